@@ -1,0 +1,179 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Run in a container that has the reference tree (default /root/reference) and the
+reference library built by oracle/Makefile (oracle/_ref/libmoldyn_ref.so):
+
+    python tests/golden/make_golden.py [REF_ROOT]
+
+Inputs come from the reference's own data files (data/nist/...), the published
+NIST values are read out of the reference's own test sources
+(tests/test_nist_lj.cpp, tests/test_nist_spce.cpp), and every computed output
+is produced by calling the compiled reference (not the restatement), so the
+fixtures pin both the restatement and the GPU path to the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402  (test infrastructure)
+
+
+def _p(a):
+    return O._p(a)
+
+
+def published_lj(ref_root):
+    """kRefs of tests/test_nist_lj.cpp:26-39 and kPressureTailPoints (:67-72)."""
+    src = open(os.path.join(ref_root, "tests", "test_nist_lj.cpp")).read()
+    rows = re.findall(r"\{(\d),\s*Truncation::(Truncated|LinearForceShift),\s*([-\d.e]+),"
+                      r"\s*([-\d.e]+),\s*([-\d.e]+),\s*([-\d.e]+)\s*\}", src)
+    table = np.array([[int(c), 0 if t == "Truncated" else 1, float(rc), float(u), float(w),
+                       float(l)] for c, t, rc, u, w, l in rows])
+    tail = re.findall(r"\{([\d.]+),\s*([\d.]+),\s*(-[\d.]+),\s*(-[\d.]+)\}", src)
+    tail = np.array([[float(v) for v in r] for r in tail])
+    assert table.shape == (12, 6), table.shape
+    assert tail.shape == (4, 4), tail.shape
+    return table, tail
+
+
+def published_spce(ref_root):
+    """kRefs of tests/test_nist_spce.cpp:64-69: config, Edisp, ELRC, Ereal,
+    Efourier, Eself, Eintra, Etotal (K)."""
+    src = open(os.path.join(ref_root, "tests", "test_nist_spce.cpp")).read()
+    rows = re.findall(r"\{(\d),((?:\s*-?[\d.]+e-?\d+,?){7})\}", src)
+    table = np.array([[int(c)] + [float(v) for v in vals.replace(" ", "").split(",") if v]
+                      for c, vals in rows])
+    assert table.shape == (4, 8), table.shape
+    return table
+
+
+def _grow(call, n):
+    """Calls a pair-enumerating reference entry point until its buffer fits."""
+    cap = 64 * n
+    while True:
+        pi = np.zeros(cap, np.int64)
+        pj = np.zeros(cap, np.int64)
+        cnt = call(pi, pj, cap)
+        if cnt <= cap:
+            return np.stack([pi[:cnt], pj[:cnt]], 1)
+        cap = int(cnt)
+
+
+def lj_fixture(ref_root, R):
+    out = {}
+    table, tail = published_lj(ref_root)
+    out["published"] = table
+    out["lrc_points"] = tail
+    computed = []
+    for c in (1, 2, 3, 4):
+        box, pos, _ = O.read_nist_config(
+            os.path.join(ref_root, "data", "nist", "lj", f"lj_sample_config_periodic{c}.txt"))
+        n = len(pos)
+        out[f"box{c}"] = box
+        out[f"pos{c}"] = pos
+        x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+        for rc, tr in ((3.0, 0), (4.0, 0), (3.0, 1)):
+            f = [np.zeros(n) for _ in range(3)]
+            e = C.c_double()
+            w = C.c_double()
+            R.ref_lj_compute(n, _p(box), _p(x), _p(y), _p(z), 1.0, 1.0, rc, tr, 1, 0.0,
+                             *[_p(a) for a in f], C.byref(e), C.byref(w))
+            ul = C.c_double()
+            pl = C.c_double()
+            R.ref_lj_lrc(n, _p(box), 1.0, 1.0, rc, tr, C.byref(ul), C.byref(pl))
+            computed.append([c, tr, rc, e.value, w.value, ul.value, pl.value])
+            tag = f"{c}_{int(rc)}_{tr}"
+            out[f"forces{tag}"] = np.stack(f, 1)
+        # Verlet pairs at rc=3, skin=0.3 (tests/test_neighbor.cpp:100-104), reference order.
+        out[f"verlet{c}"] = _grow(lambda pi, pj, cap: R.ref_verlet_pairs(
+            n, _p(box), _p(x), _p(y), _p(z), 3.0, 0.3, _p(pi), _p(pj), cap), n)
+        dims = (C.c_int * 3)()
+        cells = _grow(lambda pi, pj, cap: R.ref_cells_pairs(
+            n, _p(box), _p(x), _p(y), _p(z), 3.0, _p(pi), _p(pj), cap, dims), n)
+        out[f"celldims{c}"] = np.array(list(dims))
+        out[f"ncellpairs{c}"] = np.array(len(cells))
+        if n <= 200:  # keep the fixture small: full candidate lists for the small configs
+            out[f"cells{c}"] = cells
+    out["computed"] = np.array(computed)
+    return out
+
+
+def spce_fixture(ref_root, R):
+    out = {"published": published_spce(ref_root), "coulomb": np.array(R.ref_coulomb_prefactor())}
+    qh = 0.42380
+    for c in (1, 2, 3, 4):
+        box, pos, types = O.read_nist_config(
+            os.path.join(ref_root, "data", "nist", "spce", f"spce_sample_config_periodic{c}.txt"))
+        n = len(pos)
+        q = np.array([-2.0 * qh if t == "O" else qh for t in types])
+        m = np.array([15.9994 if t == "O" else 1.008 for t in types])
+        mol = np.arange(n, dtype=np.int64) // 3
+        out[f"box{c}"] = box
+        out[f"pos{c}"] = pos
+        out[f"isO{c}"] = np.array([t == "O" for t in types])
+        x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+        f = [np.zeros(n) for _ in range(3)]
+        terms = np.zeros(4)
+        R.ref_ewald(n, _p(box), _p(x), _p(y), _p(z), _p(q), _p(mol), 10.0, 5, 1,
+                    *[_p(a) for a in f], _p(terms))
+        out[f"ewald_terms{c}"] = terms
+        out[f"ewald_forces{c}"] = np.stack(f, 1)
+        f2 = [np.zeros(n) for _ in range(3)]
+        e = R.ref_spce(n, _p(box), _p(x), _p(y), _p(z), _p(m), _p(q), _p(mol), 10.0, 5, 1,
+                       *[_p(a) for a in f2])
+        out[f"spce_energy{c}"] = np.array(e)
+        out[f"spce_forces{c}"] = np.stack(f2, 1)
+    return out
+
+
+def fcc_fixture(R):
+    """fccLattice states and a short moldyn_run-style VV trajectory (reference)."""
+    out = {}
+    for tag, (cells, rho, temp, seed) in {"c6": (6, 0.8442, 0.722, 1),
+                                          "c3": (3, 0.80, 1.0, 12345)}.items():
+        n = 4 * cells ** 3
+        arrs = [np.zeros(n) for _ in range(7)]
+        box = np.zeros(3)
+        R.ref_fcc_lattice(cells, rho, temp, seed, *[_p(a) for a in arrs], _p(box))
+        out[f"{tag}_pos"] = np.stack(arrs[0:3], 1)
+        out[f"{tag}_vel"] = np.stack(arrs[3:6], 1)
+        out[f"{tag}_box"] = box
+    # 25 NVE steps of the N=864 drop-in configuration (rc 2.5 Truncated, skin 0.3, dt 0.005).
+    n = 864
+    st = [np.ascontiguousarray(out["c6_pos"][:, k]) for k in range(3)] + \
+         [np.ascontiguousarray(out["c6_vel"][:, k]) for k in range(3)] + [np.zeros(n) for _ in range(3)]
+    info = np.zeros(5)
+    R.ref_run(0, n, _p(out["c6_box"]), *[_p(a) for a in st], _p(np.ones(n)), 1.0, 1.0, 2.5, 0,
+              0.3, 0.005, 25, 0.0, 0.0, 0, 0.0, 1, 0, _p(info))
+    out["vv25_pos"] = np.stack(st[0:3], 1)
+    out["vv25_vel"] = np.stack(st[3:6], 1)
+    out["vv25_frc"] = np.stack(st[6:9], 1)
+    out["vv25_info"] = info[:4]
+    return out
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    O.build(ref_root)
+    R = O.ref()
+    if R is None:
+        raise SystemExit("reference library not built (oracle/_ref/libmoldyn_ref.so missing)")
+    np.savez_compressed(os.path.join(HERE, "nist_lj.npz"), **lj_fixture(ref_root, R))
+    np.savez_compressed(os.path.join(HERE, "nist_spce.npz"), **spce_fixture(ref_root, R))
+    np.savez_compressed(os.path.join(HERE, "fcc_lj.npz"), **fcc_fixture(R))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
+
+
+if __name__ == "__main__":
+    main()
