@@ -1,0 +1,221 @@
+/*
+ * moldyn_b200.h -- C ABI of the B200-native moldyn force / neighbour / integrator path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.  Every
+ * entry point names the reference interface it replaces (path:line inside the
+ * moldyn project); the C++ drop-in headers (moleculardynamics_b200/include/
+ * moldyn/...) wrap these calls behind the reference's own class names.
+ *
+ * Conventions
+ *  - Status: MD_OK (0) on success, a negative MD_ERR_* otherwise; the message is
+ *    in md_last_error() (thread-local).  MD_ERR_INVALID_ARGUMENT and
+ *    MD_ERR_RUNTIME map to the reference's std::invalid_argument and
+ *    std::runtime_error.
+ *  - Host arrays are in the caller's atom order ("original order"), one double
+ *    per atom per component.  On the device atoms are kept sorted by cell; the
+ *    library permutes on the way in and out.
+ *  - Each context owns one CUDA stream.  Handles are not thread-safe; distinct
+ *    contexts may be used from distinct host threads.
+ *  - Device-side failures (neighbour-list overflow, constraint non-convergence,
+ *    non-finite forces) are recorded in a per-context status word and reported
+ *    at the next call that synchronises.  No kernel traps or waits unboundedly.
+ */
+#ifndef MOLDYN_B200_H
+#define MOLDYN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+/* Only the md_* entry points are exported from libmoldyn_b200.so. */
+#if defined(__GNUC__)
+#define MD_API __attribute__((visibility("default")))
+#else
+#define MD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MD_OK 0
+#define MD_ERR_INVALID_ARGUMENT (-1) /* reference: std::invalid_argument */
+#define MD_ERR_RUNTIME (-2)          /* reference: std::runtime_error */
+#define MD_ERR_CUDA (-3)             /* CUDA runtime error (no reference counterpart) */
+#define MD_ERR_OUT_OF_MEMORY (-4)
+#define MD_ERR_DEVICE (-5)           /* device status word set (see md_context_status) */
+
+/* Device status bits (md_context_status). */
+#define MD_STATUS_NEIGHBOR_OVERFLOW 0x1u /* a per-atom neighbour row overflowed */
+#define MD_STATUS_SHAKE_DIVERGED 0x2u    /* SHAKE did not converge in maxIterations */
+#define MD_STATUS_RATTLE_DIVERGED 0x4u   /* RATTLE did not converge in maxIterations */
+#define MD_STATUS_SHAKE_SINGULAR 0x8u    /* SHAKE denominator below 1e-30 */
+#define MD_STATUS_NONFINITE 0x10u        /* a non-finite energy appeared */
+
+/* System fields (core/system.hpp:54-59). */
+#define MD_FIELD_X 0
+#define MD_FIELD_Y 1
+#define MD_FIELD_Z 2
+#define MD_FIELD_VX 3
+#define MD_FIELD_VY 4
+#define MD_FIELD_VZ 5
+#define MD_FIELD_FX 6
+#define MD_FIELD_FY 7
+#define MD_FIELD_FZ 8
+#define MD_FIELD_MASS 9
+#define MD_FIELD_CHARGE 10
+
+/* Truncation (forcefield/lennard_jones.hpp:11). */
+#define MD_TRUNCATED 0
+#define MD_LINEAR_FORCE_SHIFT 1
+
+/* Precision of the pair arithmetic. */
+#define MD_PRECISION_FP64 0  /* drop-in path: reference arithmetic in FP64 */
+#define MD_PRECISION_MIXED 1 /* FP32 pair terms, FP64 displacement and accumulation */
+
+typedef struct md_context md_context;
+typedef struct md_system md_system;
+typedef struct md_cells md_cells;
+typedef struct md_verlet md_verlet;
+typedef struct md_lj md_lj;
+typedef struct md_integrator md_integrator;
+
+/* ------------------------------------------------------------------ library */
+/* Message of the last failing call on this thread ("" if none). */
+MD_API const char* md_last_error(void);
+/* ABI version of this header (major*10000 + minor*100 + patch). */
+MD_API int md_abi_version(void);
+
+/* ------------------------------------------------------------------ context */
+/* No reference counterpart: the reference is one CPU thread.  One context =
+ * one device + one stream + the device status word + reusable scratch. */
+MD_API int md_context_create(int device, md_context** out);
+MD_API int md_context_destroy(md_context* ctx);
+MD_API int md_context_synchronize(md_context* ctx);
+/* Reads (and with clear != 0, clears) the device status word; synchronises. */
+MD_API int md_context_status(md_context* ctx, uint32_t* status, int clear);
+/* Number of kernels this context has launched (instrumentation). */
+MD_API int md_context_launch_count(md_context* ctx, int64_t* count);
+
+/* ------------------------------------------------------------------- system */
+/* System(Box) + addAtom (core/system.hpp:15-27).  Positions, velocities,
+ * forces and charges start at 0, masses at 1, molecule ids at the atom's own
+ * index (system.cpp:17-22). */
+MD_API int md_system_create(md_context* ctx, int64_t n, const double box[3], md_system** out);
+MD_API int md_system_destroy(md_system* sys);
+MD_API int64_t md_system_size(const md_system* sys);                  /* system.hpp:17 */
+MD_API int md_system_box(const md_system* sys, double box[3]);        /* box.hpp:14-15 */
+/* Set or get one field: n doubles in original order (system.hpp:29-43). */
+MD_API int md_system_set(md_system* sys, int field, const double* src);
+MD_API int md_system_get(md_system* sys, int field, double* dst);
+MD_API int md_system_set_molecule_ids(md_system* sys, const int64_t* ids); /* system.hpp:43 */
+MD_API int md_system_get_molecule_ids(md_system* sys, int64_t* ids);       /* system.hpp:34 */
+MD_API int md_system_zero_forces(md_system* sys);                          /* system.cpp:116-122 */
+MD_API int md_system_kinetic_energy(md_system* sys, double* ke);           /* system.cpp:124-131 */
+MD_API int md_system_total_momentum(md_system* sys, double p[3]);          /* system.cpp:137-145 */
+MD_API int md_system_remove_com_motion(md_system* sys);                    /* system.cpp:147-164 */
+/* Potential energy and virial of the last force evaluation on this system. */
+MD_API int md_system_last_energy(md_system* sys, double* energy, double* virial);
+
+/* --------------------------------------------------------------- cell list */
+/* CellList(box, cutoff) (neighbor/cell_list.hpp:28, cell_list.cpp:8-14). */
+MD_API int md_cells_create(md_context* ctx, const double box[3], double cutoff, md_cells** out);
+MD_API int md_cells_destroy(md_cells* cells);
+MD_API int md_cells_dims(const md_cells* cells, int dims[3]);  /* cell_list.hpp:36 */
+MD_API int md_cells_usable(const md_cells* cells);             /* cell_list.hpp:37: 1/0 */
+MD_API int md_cells_build(md_cells* cells, md_system* sys);    /* cell_list.cpp:16-43 */
+/* forEachPair (cell_list.hpp:55-108) as an exported candidate-pair set: every
+ * (i<j), original indices, each unordered pair once, in unspecified order.
+ * *count receives the total; at most cap pairs are written.  Requires usable(). */
+MD_API int md_cells_pairs(md_cells* cells, int64_t* pi, int64_t* pj, int64_t cap, int64_t* count);
+
+/* ------------------------------------------------------------- Verlet list */
+/* VerletList(box, cutoff, skin) (neighbor/verlet_list.hpp:28, verlet_list.cpp:5-6). */
+MD_API int md_verlet_create(md_context* ctx, const double box[3], double cutoff, double skin,
+                     md_verlet** out);
+MD_API int md_verlet_destroy(md_verlet* list);
+/* build (verlet_list.cpp:8-42): re-sorts the system's device order by cell. */
+MD_API int md_verlet_build(md_verlet* list, md_system* sys);
+/* needsRebuild (verlet_list.cpp:44-63): *flag = 1/0. */
+MD_API int md_verlet_needs_rebuild(md_verlet* list, md_system* sys, int* flag);
+/* rebuildIfNeeded (verlet_list.cpp:65-69).  *rebuilt (nullable) = 1/0. */
+MD_API int md_verlet_rebuild_if_needed(md_verlet* list, md_system* sys, int* rebuilt);
+MD_API int md_verlet_rebuild_count(md_verlet* list, int64_t* count); /* verlet_list.hpp:32 */
+/* forEachPair (verlet_list.hpp:52-57) as an exported set: pairs (i<j), original
+ * indices, sorted by (i, j). */
+MD_API int md_verlet_pairs(md_verlet* list, int64_t* pi, int64_t* pj, int64_t cap, int64_t* count);
+/* Rebuild criterion: 0 = reference (sum of the two largest displacements >
+ * skin, verlet_list.cpp:44-63), 1 = largest displacement > skin/2. */
+MD_API int md_verlet_set_criterion(md_verlet* list, int criterion);
+/* Largest and second-largest displacement since the last build (diagnostics). */
+MD_API int md_verlet_displacements(md_verlet* list, md_system* sys, double* largest, double* second);
+
+/* ----------------------------------------------------------- Lennard-Jones */
+/* LennardJones(sigma, epsilon, cutoff, truncation) (lennard_jones.hpp:26,
+ * lennard_jones.cpp:32-48) plus the pair precision. */
+MD_API int md_lj_create(double sigma, double epsilon, double cutoff, int truncation, int precision,
+                 md_lj** out);
+MD_API int md_lj_destroy(md_lj* lj);
+/* computeEnergyVirial (lennard_jones.cpp:90-92): brute force, forces untouched. */
+MD_API int md_lj_energy_virial(md_lj* lj, md_system* sys, double* energy, double* virial);
+/* computeForces(sys) (lennard_jones.cpp:94-97): brute force, zeroes forces first. */
+MD_API int md_lj_forces(md_lj* lj, md_system* sys, double* energy, double* virial);
+/* computeForces(sys, CellList) (lennard_jones.cpp:99-114): MD_ERR_INVALID_ARGUMENT
+ * when the cell list is not usable. */
+MD_API int md_lj_forces_cells(md_lj* lj, md_system* sys, md_cells* cells, double* energy,
+                       double* virial);
+/* computeForces(sys, VerletList) (lennard_jones.cpp:116-119). */
+MD_API int md_lj_forces_verlet(md_lj* lj, md_system* sys, md_verlet* list, double* energy,
+                        double* virial);
+/* longRangeCorrection / longRangeCorrectionPressure (lennard_jones.cpp:121-151). */
+MD_API int md_lj_lrc(const md_lj* lj, int64_t n, const double box[3], double* u_lrc, double* p_lrc);
+/* Threads per atom of the Verlet-list force kernel: 1, 2, 4, 8 or 16 (process-wide
+ * tuning knob, default 4; no reference counterpart -- the reference is scalar). */
+MD_API int md_lj_set_threads_per_atom(int tpa);
+
+/* -------------------------------------------------------------- integrators */
+/* VelocityVerlet(dt) (integrate/velocity_verlet.hpp:41). */
+MD_API int md_integrator_create_vv(double dt, md_integrator** out);
+/* LangevinBAOAB(dt, friction, temperature, seed) (integrate/langevin.hpp:29).
+ * The O-step noise is Philox4x32-10 keyed by seed, counter (step, atom). */
+MD_API int md_integrator_create_baoab(double dt, double friction, double temperature, uint64_t seed,
+                               md_integrator** out);
+/* NoseHooverChain(dt, T, tau, chainLength, dof) (integrate/nose_hoover.hpp:27-28);
+ * MD_ERR_INVALID_ARGUMENT when chainLength < 1 (nose_hoover.cpp:36-38). */
+MD_API int md_integrator_create_nhc(double dt, double temperature, double tau, int chain_length,
+                             int64_t dof, md_integrator** out);
+MD_API int md_integrator_destroy(md_integrator* integ);
+/* The step is split around the force call so a host ForceFn can run between
+ * (velocity_verlet.hpp:43-47: called exactly once per step):
+ *   pre_force  -- everything before computeForces (B, A[, O, A] / chain, B, A);
+ *   post_force -- everything after it (B[, chain]). */
+MD_API int md_integrator_pre_force(md_integrator* integ, md_system* sys);
+MD_API int md_integrator_post_force(md_integrator* integ, md_system* sys);
+/* conservedQuantityContribution (nose_hoover.cpp:45-54); 0 for VV and BAOAB. */
+MD_API int md_integrator_conserved(md_integrator* integ, double* value);
+/* BAOAB only: take the O-step normals from xi[3*i + {0,1,2}] (original atom
+ * order, n*steps values, one block of 3n per step) instead of Philox.  Lets a
+ * test replay the reference's exact mt19937_64 stream.  NULL restores Philox. */
+MD_API int md_integrator_set_noise(md_integrator* integ, const double* xi, int64_t count);
+
+/* Fused device loop: `steps` steps of integ with LJ forces on the Verlet list
+ * (rebuildIfNeeded + computeForces, apps/moldyn_run.cpp:581-587), without a
+ * host synchronisation per step.  Forces must be current on entry.  thermo
+ * (nullable, steps*4 doubles) receives per step: pair energy, virial, kinetic
+ * energy, conserved-quantity contribution. */
+MD_API int md_run_lj(md_integrator* integ, md_system* sys, md_verlet* list, md_lj* lj, int64_t steps,
+              double* thermo);
+
+/* -------------------------------------------------------------------- setup */
+/* fccLattice(cells, density, temperature, seed) (util/lattice.cpp:15-64), on the
+ * host: writes 4*cells^3 atoms into caller arrays (original order) and the cubic
+ * box; velocities from std::mt19937_64 with the reference's polar Box-Muller
+ * (util/random.hpp:52-69).  Returns the atom count, or MD_ERR_INVALID_ARGUMENT. */
+MD_API int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed, double* x,
+                   double* y, double* z, double* vx, double* vy, double* vz, double* mass,
+                   double box[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOLDYN_B200_H */

@@ -1,0 +1,551 @@
+"""moleculardynamics_b200 -- B200-native moldyn force / neighbour / integrator path.
+
+A thin Python binding over the C ABI in ``include/moldyn_b200.h`` (library:
+``libmoldyn_b200.so`` next to this file).  Class and method names follow the
+reference's C++ API (``moldyn::System``, ``CellList``, ``VerletList``,
+``LennardJones``, ``VelocityVerlet``, ``LangevinBAOAB``, ``NoseHooverChain``) so
+code and tests read like the reference's own.
+
+There is no CPU fallback: importing works anywhere, but constructing a
+``Context`` raises unless the CUDA library is built and a GPU is present.
+Arrays cross the boundary in the caller's atom order as float64 numpy arrays of
+shape (N, 3) (positions, velocities, forces) or (N,) (masses, charges).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmoldyn_b200.so")
+
+# C ABI constants (include/moldyn_b200.h)
+MD_OK = 0
+MD_ERR_INVALID_ARGUMENT = -1
+MD_ERR_RUNTIME = -2
+MD_ERR_CUDA = -3
+MD_ERR_OUT_OF_MEMORY = -4
+MD_ERR_DEVICE = -5
+FIELD_X, FIELD_Y, FIELD_Z, FIELD_VX, FIELD_VY, FIELD_VZ = range(6)
+FIELD_FX, FIELD_FY, FIELD_FZ, FIELD_MASS, FIELD_CHARGE = range(6, 11)
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class Truncation:
+    """forcefield/lennard_jones.hpp:11"""
+    Truncated = 0
+    LinearForceShift = 1
+
+
+class MDError(RuntimeError):
+    code = 0
+
+
+class InvalidArgument(MDError, ValueError):
+    """The reference's std::invalid_argument."""
+
+
+class DeviceError(MDError):
+    """A device status bit (neighbour overflow, constraint divergence, ...)."""
+
+
+_ERRORS = {MD_ERR_INVALID_ARGUMENT: InvalidArgument, MD_ERR_RUNTIME: MDError,
+           MD_ERR_CUDA: MDError, MD_ERR_OUT_OF_MEMORY: MemoryError, MD_ERR_DEVICE: DeviceError}
+
+_lib = None
+_vp = C.c_void_p
+_d = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `make -C moleculardynamics_b200/csrc` "
+            "(or __graft_entry__.build()).  There is no CPU fallback.")
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        "md_last_error": (C.c_char_p, []),
+        "md_abi_version": (C.c_int, []),
+        "md_context_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+        "md_context_destroy": (C.c_int, [_vp]),
+        "md_context_synchronize": (C.c_int, [_vp]),
+        "md_context_status": (C.c_int, [_vp, C.POINTER(C.c_uint32), C.c_int]),
+        "md_context_launch_count": (C.c_int, [_vp, _i64p]),
+        "md_system_create": (C.c_int, [_vp, C.c_int64, _d, C.POINTER(_vp)]),
+        "md_system_destroy": (C.c_int, [_vp]),
+        "md_system_size": (C.c_int64, [_vp]),
+        "md_system_box": (C.c_int, [_vp, _d]),
+        "md_system_set": (C.c_int, [_vp, C.c_int, _d]),
+        "md_system_get": (C.c_int, [_vp, C.c_int, _d]),
+        "md_system_set_molecule_ids": (C.c_int, [_vp, _i64p]),
+        "md_system_get_molecule_ids": (C.c_int, [_vp, _i64p]),
+        "md_system_zero_forces": (C.c_int, [_vp]),
+        "md_system_kinetic_energy": (C.c_int, [_vp, _d]),
+        "md_system_total_momentum": (C.c_int, [_vp, _d]),
+        "md_system_remove_com_motion": (C.c_int, [_vp]),
+        "md_system_last_energy": (C.c_int, [_vp, _d, _d]),
+        "md_cells_create": (C.c_int, [_vp, _d, C.c_double, C.POINTER(_vp)]),
+        "md_cells_destroy": (C.c_int, [_vp]),
+        "md_cells_dims": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+        "md_cells_usable": (C.c_int, [_vp]),
+        "md_cells_build": (C.c_int, [_vp, _vp]),
+        "md_cells_pairs": (C.c_int, [_vp, _i64p, _i64p, C.c_int64, _i64p]),
+        "md_verlet_create": (C.c_int, [_vp, _d, C.c_double, C.c_double, C.POINTER(_vp)]),
+        "md_verlet_destroy": (C.c_int, [_vp]),
+        "md_verlet_build": (C.c_int, [_vp, _vp]),
+        "md_verlet_needs_rebuild": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+        "md_verlet_rebuild_if_needed": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+        "md_verlet_rebuild_count": (C.c_int, [_vp, _i64p]),
+        "md_verlet_pairs": (C.c_int, [_vp, _i64p, _i64p, C.c_int64, _i64p]),
+        "md_verlet_set_criterion": (C.c_int, [_vp, C.c_int]),
+        "md_verlet_displacements": (C.c_int, [_vp, _vp, _d, _d]),
+        "md_lj_create": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                   C.POINTER(_vp)]),
+        "md_lj_destroy": (C.c_int, [_vp]),
+        "md_lj_energy_virial": (C.c_int, [_vp, _vp, _d, _d]),
+        "md_lj_forces": (C.c_int, [_vp, _vp, _d, _d]),
+        "md_lj_forces_cells": (C.c_int, [_vp, _vp, _vp, _d, _d]),
+        "md_lj_forces_verlet": (C.c_int, [_vp, _vp, _vp, _d, _d]),
+        "md_lj_lrc": (C.c_int, [_vp, C.c_int64, _d, _d, _d]),
+        "md_lj_set_threads_per_atom": (C.c_int, [C.c_int]),
+        "md_integrator_create_vv": (C.c_int, [C.c_double, C.POINTER(_vp)]),
+        "md_integrator_create_baoab": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                                 C.POINTER(_vp)]),
+        "md_integrator_create_nhc": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int,
+                                               C.c_int64, C.POINTER(_vp)]),
+        "md_integrator_destroy": (C.c_int, [_vp]),
+        "md_integrator_pre_force": (C.c_int, [_vp, _vp]),
+        "md_integrator_post_force": (C.c_int, [_vp, _vp]),
+        "md_integrator_conserved": (C.c_int, [_vp, _d]),
+        "md_integrator_set_noise": (C.c_int, [_vp, _d, C.c_int64]),
+        "md_run_lj": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _d]),
+        "md_fcc_lattice": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_uint64] + [_d] * 8),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def lib():
+    return _load()
+
+
+def _check(rc):
+    if rc != MD_OK:
+        msg = _load().md_last_error().decode(errors="replace")
+        exc = _ERRORS.get(rc, MDError)(f"[{rc}] {msg}")
+        if isinstance(exc, MDError):
+            exc.code = rc
+        raise exc
+    return rc
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_d)
+
+
+# ---------------------------------------------------------------- context
+_default_ctx = None
+
+
+class Context:
+    """One device, one stream, one device status word."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(_load().md_context_create(device, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def synchronize(self):
+        _check(lib().md_context_synchronize(self._h))
+
+    def status(self, clear=False):
+        st = C.c_uint32()
+        _check(lib().md_context_status(self._h, C.byref(st), 1 if clear else 0))
+        return st.value
+
+    def launch_count(self):
+        c = C.c_int64()
+        _check(lib().md_context_launch_count(self._h, C.byref(c)))
+        return c.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().md_context_destroy(self._h)
+            self._h = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def require_gpu() -> None:
+    """Raises unless the CUDA library loads and a device context can be created."""
+    default_context()
+
+
+# ---------------------------------------------------------------- system
+class System:
+    """core/system.hpp:11-60 on the device.  Arrays in the caller's atom order."""
+
+    def __init__(self, n, box, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        box = _f64(box).reshape(3)
+        h = _vp()
+        _check(lib().md_system_create(self.ctx.handle, int(n), _ptr(box), C.byref(h)))
+        self._h = h
+        self.n = int(n)
+        self.box = box.copy()
+
+    @classmethod
+    def from_arrays(cls, pos, box, vel=None, mass=None, charge=None, mol=None, ctx=None):
+        pos = _f64(pos).reshape(-1, 3)
+        s = cls(pos.shape[0], box, ctx)
+        s.positions = pos
+        if vel is not None:
+            s.velocities = vel
+        if mass is not None:
+            s.masses = mass
+        if charge is not None:
+            s.charges = charge
+        if mol is not None:
+            s.molecule_ids = mol
+        return s
+
+    @property
+    def handle(self):
+        return self._h
+
+    def size(self):
+        return self.n
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_system_destroy(self._h)
+            self._h = None
+
+    def _get3(self, f0):
+        out = np.empty((3, self.n))
+        for k in range(3):
+            _check(lib().md_system_get(self._h, f0 + k, _ptr(out[k])))
+        return out.T.copy()
+
+    def _set3(self, f0, a):
+        a = _f64(a).reshape(self.n, 3)
+        for k in range(3):
+            col = np.ascontiguousarray(a[:, k])
+            _check(lib().md_system_set(self._h, f0 + k, _ptr(col)))
+
+    def _get1(self, f):
+        out = np.empty(self.n)
+        _check(lib().md_system_get(self._h, f, _ptr(out)))
+        return out
+
+    def _set1(self, f, a):
+        a = _f64(a).reshape(self.n)
+        _check(lib().md_system_set(self._h, f, _ptr(a)))
+
+    positions = property(lambda s: s._get3(FIELD_X), lambda s, a: s._set3(FIELD_X, a))
+    velocities = property(lambda s: s._get3(FIELD_VX), lambda s, a: s._set3(FIELD_VX, a))
+    forces = property(lambda s: s._get3(FIELD_FX), lambda s, a: s._set3(FIELD_FX, a))
+    masses = property(lambda s: s._get1(FIELD_MASS), lambda s, a: s._set1(FIELD_MASS, a))
+    charges = property(lambda s: s._get1(FIELD_CHARGE), lambda s, a: s._set1(FIELD_CHARGE, a))
+
+    @property
+    def molecule_ids(self):
+        out = np.empty(self.n, dtype=np.int64)
+        _check(lib().md_system_get_molecule_ids(self._h, out.ctypes.data_as(_i64p)))
+        return out
+
+    @molecule_ids.setter
+    def molecule_ids(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.int64).reshape(self.n)
+        _check(lib().md_system_set_molecule_ids(self._h, ids.ctypes.data_as(_i64p)))
+
+    def zero_forces(self):
+        _check(lib().md_system_zero_forces(self._h))
+
+    def kinetic_energy(self):
+        v = C.c_double()
+        _check(lib().md_system_kinetic_energy(self._h, C.byref(v)))
+        return v.value
+
+    def temperature(self, dof):
+        """system.cpp:133-135"""
+        return 2.0 * self.kinetic_energy() / float(dof)
+
+    def total_momentum(self):
+        p = np.zeros(3)
+        _check(lib().md_system_total_momentum(self._h, _ptr(p)))
+        return p
+
+    def remove_center_of_mass_motion(self):
+        _check(lib().md_system_remove_com_motion(self._h))
+
+    def volume(self):
+        return float(self.box[0] * self.box[1] * self.box[2])
+
+    def last_energy_virial(self):
+        e = C.c_double()
+        w = C.c_double()
+        _check(lib().md_system_last_energy(self._h, C.byref(e), C.byref(w)))
+        return e.value, w.value
+
+
+# ---------------------------------------------------------------- neighbours
+def _pairs(fn, h):
+    cnt = C.c_int64()
+    _check(fn(h, None, None, 0, C.byref(cnt)))
+    n = cnt.value
+    pi = np.zeros(max(n, 1), np.int64)
+    pj = np.zeros(max(n, 1), np.int64)
+    _check(fn(h, pi.ctypes.data_as(_i64p), pj.ctypes.data_as(_i64p), n, C.byref(cnt)))
+    return np.stack([pi[:n], pj[:n]], 1)
+
+
+class CellList:
+    """neighbor/cell_list.hpp:26-37"""
+
+    def __init__(self, box, cutoff, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = _vp()
+        _check(lib().md_cells_create(self.ctx.handle, _ptr(_f64(box).reshape(3)), float(cutoff),
+                                     C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_cells_destroy(self._h)
+            self._h = None
+
+    def build(self, sys: System):
+        _check(lib().md_cells_build(self._h, sys.handle))
+
+    def cells_per_side(self, dim):
+        d = (C.c_int * 3)()
+        _check(lib().md_cells_dims(self._h, d))
+        return d[dim]
+
+    def usable(self):
+        return bool(lib().md_cells_usable(self._h))
+
+    def pairs(self):
+        """Candidate pairs (i<j) of forEachPair, as an (M, 2) array (any order)."""
+        return _pairs(lib().md_cells_pairs, self._h)
+
+
+class VerletList:
+    """neighbor/verlet_list.hpp:26-39"""
+
+    def __init__(self, box, cutoff, skin, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = _vp()
+        _check(lib().md_verlet_create(self.ctx.handle, _ptr(_f64(box).reshape(3)), float(cutoff),
+                                      float(skin), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_verlet_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def build(self, sys: System):
+        _check(lib().md_verlet_build(self._h, sys.handle))
+
+    def needs_rebuild(self, sys: System) -> bool:
+        f = C.c_int()
+        _check(lib().md_verlet_needs_rebuild(self._h, sys.handle, C.byref(f)))
+        return bool(f.value)
+
+    def rebuild_if_needed(self, sys: System) -> bool:
+        f = C.c_int()
+        _check(lib().md_verlet_rebuild_if_needed(self._h, sys.handle, C.byref(f)))
+        return bool(f.value)
+
+    def rebuild_count(self) -> int:
+        c = C.c_int64()
+        _check(lib().md_verlet_rebuild_count(self._h, C.byref(c)))
+        return c.value
+
+    def pairs(self):
+        """Pairs (i<j) held in the list, sorted by (i, j)."""
+        return _pairs(lib().md_verlet_pairs, self._h)
+
+    def set_criterion(self, criterion: int):
+        _check(lib().md_verlet_set_criterion(self._h, int(criterion)))
+
+    def displacements(self, sys: System):
+        a = C.c_double()
+        b = C.c_double()
+        _check(lib().md_verlet_displacements(self._h, sys.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
+# ---------------------------------------------------------------- forces
+class LennardJones:
+    """forcefield/lennard_jones.hpp:24-100.  Energy-returning calls give
+    (energy, virial) like EnergyVirial."""
+
+    def __init__(self, sigma, epsilon, cutoff, truncation=Truncation.Truncated,
+                 precision=PRECISION_FP64):
+        h = _vp()
+        _check(lib().md_lj_create(float(sigma), float(epsilon), float(cutoff), int(truncation),
+                                  int(precision), C.byref(h)))
+        self._h = h
+        self.sigma, self.epsilon, self.cutoff = float(sigma), float(epsilon), float(cutoff)
+        self.truncation = int(truncation)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_lj_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _ev(self, fn, *args):
+        e = C.c_double()
+        w = C.c_double()
+        _check(fn(self._h, *args, C.byref(e), C.byref(w)))
+        return e.value, w.value
+
+    def compute_energy_virial(self, sys: System):
+        return self._ev(lib().md_lj_energy_virial, sys.handle)
+
+    def compute_forces(self, sys: System, source=None):
+        """Brute force (source None), a CellList or a VerletList."""
+        if source is None:
+            return self._ev(lib().md_lj_forces, sys.handle)
+        if isinstance(source, CellList):
+            return self._ev(lib().md_lj_forces_cells, sys.handle, source._h)
+        return self._ev(lib().md_lj_forces_verlet, sys.handle, source.handle)
+
+    def long_range_correction(self, sys: System):
+        u = C.c_double()
+        _check(lib().md_lj_lrc(self._h, sys.n, _ptr(_f64(sys.box)), C.byref(u), None))
+        return u.value
+
+    def long_range_correction_pressure(self, sys: System):
+        p = C.c_double()
+        _check(lib().md_lj_lrc(self._h, sys.n, _ptr(_f64(sys.box)), None, C.byref(p)))
+        return p.value
+
+
+def set_threads_per_atom(tpa: int):
+    _check(lib().md_lj_set_threads_per_atom(int(tpa)))
+
+
+# ---------------------------------------------------------------- integrators
+class _Integrator:
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_integrator_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def step(self, sys: System, compute_forces):
+        """template<class ForceFn> step(System&, ForceFn&&): compute_forces(sys)
+        is called exactly once, between the pre- and post-force halves."""
+        _check(lib().md_integrator_pre_force(self._h, sys.handle))
+        result = compute_forces(sys)
+        _check(lib().md_integrator_post_force(self._h, sys.handle))
+        return result
+
+    def run(self, sys: System, verlet: VerletList, lj: LennardJones, steps: int, thermo=False):
+        """Fused device loop with the moldyn_run ForceFn (rebuildIfNeeded + LJ).
+        Returns a (steps, 4) array [energy, virial, kinetic, conserved] if thermo."""
+        out = np.zeros((steps, 4)) if thermo and steps > 0 else None
+        _check(lib().md_run_lj(self._h, sys.handle, verlet.handle, lj.handle, int(steps),
+                               _ptr(out) if out is not None else None))
+        return out
+
+    def conserved_quantity_contribution(self):
+        v = C.c_double()
+        _check(lib().md_integrator_conserved(self._h, C.byref(v)))
+        return v.value
+
+
+class VelocityVerlet(_Integrator):
+    """integrate/velocity_verlet.hpp:39-80"""
+
+    def __init__(self, dt):
+        h = _vp()
+        _check(lib().md_integrator_create_vv(float(dt), C.byref(h)))
+        self._h = h
+        self.dt = float(dt)
+
+
+class LangevinBAOAB(_Integrator):
+    """integrate/langevin.hpp:27-97"""
+
+    def __init__(self, dt, friction, temperature, seed):
+        h = _vp()
+        _check(lib().md_integrator_create_baoab(float(dt), float(friction), float(temperature),
+                                                int(seed), C.byref(h)))
+        self._h = h
+        self.dt = float(dt)
+
+    def set_noise(self, xi):
+        """Replay caller-supplied normals (3N per step, atom-major x,y,z) instead of Philox."""
+        if xi is None:
+            _check(lib().md_integrator_set_noise(self._h, None, 0))
+            return
+        xi = _f64(xi).reshape(-1)
+        _check(lib().md_integrator_set_noise(self._h, _ptr(xi), xi.size))
+
+
+class NoseHooverChain(_Integrator):
+    """integrate/nose_hoover.hpp:24-67"""
+
+    def __init__(self, dt, temperature, tau, chain_length, dof):
+        h = _vp()
+        _check(lib().md_integrator_create_nhc(float(dt), float(temperature), float(tau),
+                                              int(chain_length), int(dof), C.byref(h)))
+        self._h = h
+        self.dt = float(dt)
+
+
+# ---------------------------------------------------------------- setup
+def fcc_lattice(cells, density, temperature, seed):
+    """util/lattice.cpp:15-64 (host-side setup).  Returns dict(pos, vel, mass, box)."""
+    n = 4 * int(cells) ** 3
+    arrs = [np.zeros(n) for _ in range(7)]
+    box = np.zeros(3)
+    rc = lib().md_fcc_lattice(int(cells), float(density), float(temperature), int(seed),
+                              *[_ptr(a) for a in arrs], _ptr(box))
+    if rc < 0:
+        _check(rc)
+    x, y, z, vx, vy, vz, m = arrs
+    return dict(pos=np.stack([x, y, z], 1), vel=np.stack([vx, vy, vz], 1), mass=m, box=box)

@@ -1,0 +1,477 @@
+// integrate.cu -- velocity-Verlet, BAOAB Langevin and Nose-Hoover-chain steps.
+//
+// Per-atom updates follow the reference's arithmetic exactly (std::fma ->
+// fma(), wrap -> bit-exact fold), so one step from the same forces reproduces the
+// reference's positions and velocities bit-for-bit.  The Nose-Hoover chain keeps
+// its scalars on the device and tracks the kinetic energy analytically through
+// the velocity rescalings (KE * s^2) instead of re-summing it after each of the six
+// rescalings per step; the rescalings are folded into one factor applied by the
+// next kick.
+#include <cmath>
+#include <new>
+
+#include "md_device.cuh"
+#include "md_internal.cuh"
+
+namespace mdb {
+int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
+int verlet_ensure_capacity(md_verlet* v, md_system* sys);
+}  // namespace mdb
+
+namespace mdb {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+struct StepArgs {
+    Box3 box;
+    double dt, half_dt;
+    // BAOAB
+    double c1, c2, temperature;
+    uint32_t key0, key1;
+    uint64_t step;
+    const double* noise;  // replayed normals for this step (original order), or null
+};
+
+// velocity_verlet.hpp:55-65 (+ an optional NHC pending scale applied first).
+__global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
+    if (nhc) {
+        const double sc = nhc->scale;
+        vx = __dmul_rn(vx, sc);
+        vy = __dmul_rn(vy, sc);
+        vz = __dmul_rn(vz, sc);
+    }
+    const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
+    vx = fma(c, a.fx[k], vx);
+    vy = fma(c, a.fy[k], vy);
+    vz = fma(c, a.fz[k], vz);
+    double4 p = a.pos[k];
+    p.x = fold_exact(fma(s.dt, vx, p.x), s.box.L[0], s.box.inv[0]);
+    p.y = fold_exact(fma(s.dt, vy, p.y), s.box.L[1], s.box.inv[1]);
+    p.z = fold_exact(fma(s.dt, vz, p.z), s.box.L[2], s.box.inv[2]);
+    a.pos[k] = p;
+    a.vx[k] = vx;
+    a.vy[k] = vy;
+    a.vz[k] = vz;
+}
+
+// langevin.hpp:55-80: B, A (wrap), O, A (wrap).
+__global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
+    double vx = fma(c, a.fx[k], a.vx[k]);
+    double vy = fma(c, a.fy[k], a.vy[k]);
+    double vz = fma(c, a.fz[k], a.vz[k]);
+    double4 p = a.pos[k];
+    p.x = fold_exact(fma(s.half_dt, vx, p.x), s.box.L[0], s.box.inv[0]);
+    p.y = fold_exact(fma(s.half_dt, vy, p.y), s.box.L[1], s.box.inv[1]);
+    p.z = fold_exact(fma(s.half_dt, vz, p.z), s.box.L[2], s.box.inv[2]);
+    // O: v = c1*v + (c2*sqrt(T/m)) * xi
+    const int o = a.orig[k];
+    double x0, x1, x2;
+    if (s.noise) {
+        x0 = s.noise[3 * static_cast<int64_t>(o) + 0];
+        x1 = s.noise[3 * static_cast<int64_t>(o) + 1];
+        x2 = s.noise[3 * static_cast<int64_t>(o) + 2];
+    } else {
+        const U4 r0 = philox4x32_10(U4{static_cast<uint32_t>(o), 0u, static_cast<uint32_t>(s.step),
+                                       static_cast<uint32_t>(s.step >> 32)},
+                                    s.key0, s.key1);
+        const U4 r1 = philox4x32_10(U4{static_cast<uint32_t>(o), 1u, static_cast<uint32_t>(s.step),
+                                       static_cast<uint32_t>(s.step >> 32)},
+                                    s.key0, s.key1);
+        double x3;
+        normal2(r0, x0, x1);
+        normal2(r1, x2, x3);
+    }
+    const double sig = __dsqrt_rn(__ddiv_rn(s.temperature, a.mass[k]));
+    const double sc = __dmul_rn(s.c2, sig);
+    vx = __dadd_rn(__dmul_rn(s.c1, vx), __dmul_rn(x0, sc));
+    vy = __dadd_rn(__dmul_rn(s.c1, vy), __dmul_rn(x1, sc));
+    vz = __dadd_rn(__dmul_rn(s.c1, vz), __dmul_rn(x2, sc));
+    p.x = fold_exact(fma(s.half_dt, vx, p.x), s.box.L[0], s.box.inv[0]);
+    p.y = fold_exact(fma(s.half_dt, vy, p.y), s.box.L[1], s.box.inv[1]);
+    p.z = fold_exact(fma(s.half_dt, vz, p.z), s.box.L[2], s.box.inv[2]);
+    a.pos[k] = p;
+    a.vx[k] = vx;
+    a.vy[k] = vy;
+    a.vz[k] = vz;
+}
+
+// Second half-kick (velocity_verlet.hpp:70-73), fused with the kinetic-energy sum.
+__global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsigned* ticket,
+                          double* out) {
+    double ke[1] = {0.0};
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
+        const double vx = fma(c, a.fx[k], a.vx[k]);
+        const double vy = fma(c, a.fy[k], a.vy[k]);
+        const double vz = fma(c, a.fz[k], a.vz[k]);
+        a.vx[k] = vx;
+        a.vy[k] = vy;
+        a.vz[k] = vz;
+        ke[0] += 0.5 * a.mass[k] * (vx * vx + vy * vy + vz * vz);
+    }
+    grid_reduce<1>(ke, part, ticket, out);
+}
+
+__global__ void k_scale(md_atoms a, int64_t n, NhcState* nhc) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const double sc = nhc->scale;
+    if (k < n) {
+        a.vx[k] = __dmul_rn(a.vx[k], sc);
+        a.vy[k] = __dmul_rn(a.vy[k], sc);
+        a.vz[k] = __dmul_rn(a.vz[k], sc);
+    }
+}
+
+__global__ void k_reset_scale(NhcState* nhc) { nhc->scale = 1.0; }
+
+// nose_hoover.cpp:89-108 for link j; ke is the current kinetic energy.
+__device__ void nhc_link(NhcState& c, int j, double d2, double d4, double ke) {
+    const bool next = j < c.chain - 1;
+    if (next) c.pxi[j] *= exp(-d4 * c.pxi[j + 1] / c.Q[j + 1]);
+    double g;
+    if (j == 0) g = 2.0 * ke - c.dof * c.temperature;
+    else g = c.pxi[j - 1] * c.pxi[j - 1] / c.Q[j - 1] - c.temperature;
+    c.pxi[j] += d2 * g;
+    if (next) c.pxi[j] *= exp(-d4 * c.pxi[j + 1] / c.Q[j + 1]);
+}
+
+// integrateChain(delta) (nose_hoover.cpp:59-124) with weights w[3]; returns the
+// product of the velocity scale factors and updates ke to KE * scale^2.
+__device__ double nhc_half(NhcState& c, double delta, const double* w, double& ke) {
+    double total = 1.0;
+    for (int s = 0; s < 3; ++s) {
+        const double d = w[s] * delta;
+        const double d2 = 0.5 * d, d4 = 0.25 * d;
+        for (int j = c.chain - 1; j >= 0; --j) nhc_link(c, j, d2, d4, ke);
+        for (int k = 0; k < c.chain; ++k) c.xi[k] += d * c.pxi[k] / c.Q[k];
+        const double f = exp(-d * c.pxi[0] / c.Q[0]);
+        total *= f;
+        ke = ke * f * f;
+        for (int j = 0; j < c.chain; ++j) nhc_link(c, j, d2, d4, ke);
+    }
+    return total;
+}
+
+struct Weights {
+    double w[3];
+};
+
+// Start-of-step chain half: KE of the current velocities (pending scale included).
+__global__ void k_nhc_pre(NhcState* st, const double* ke_now, Weights w) {
+    NhcState c = *st;
+    double ke = ke_now ? *ke_now * c.scale * c.scale : c.ke;
+    const double f = nhc_half(c, 0.5 * c.dt, w.w, ke);
+    c.scale *= f;
+    c.ke = ke;
+    *st = c;
+}
+
+// End-of-step chain half using the freshly summed KE; leaves its scale pending.
+__global__ void k_nhc_post(NhcState* st, const double* ke_sum, Weights w) {
+    NhcState c = *st;
+    double ke = *ke_sum;
+    c.scale = nhc_half(c, 0.5 * c.dt, w.w, ke);
+    c.ke = ke;
+    *st = c;
+}
+
+__device__ double nhc_conserved(const NhcState& c) {
+    // nose_hoover.cpp:45-54
+    double sum = c.dof * c.temperature * c.xi[0];
+    for (int k = 1; k < c.chain; ++k) sum += c.temperature * c.xi[k];
+    for (int k = 0; k < c.chain; ++k) sum += 0.5 * c.pxi[k] * c.pxi[k] / c.Q[k];
+    return sum;
+}
+
+// thermo row: energy, virial, kinetic energy, conserved contribution.
+__global__ void k_record(const double* ev, const double* ke, const NhcState* nhc, double* row) {
+    row[0] = ev[0];
+    row[1] = ev[1];
+    row[2] = nhc ? nhc->ke : *ke;
+    row[3] = nhc ? nhc_conserved(*nhc) : 0.0;
+}
+
+__global__ void k_conserved(const NhcState* nhc, double* out) { *out = nhc_conserved(*nhc); }
+
+Weights yoshida() {
+    // nose_hoover.cpp:15-18
+    const double w1 = 1.0 / (2.0 - std::cbrt(2.0));
+    return Weights{{w1, 1.0 - 2.0 * w1, w1}};
+}
+
+StepArgs step_args(const md_integrator* it, const md_system* sys) {
+    StepArgs s{};
+    for (int d = 0; d < 3; ++d) {
+        s.box.L[d] = sys->box[d];
+        s.box.inv[d] = sys->inv_box[d];
+    }
+    s.dt = it->dt;
+    s.half_dt = 0.5 * it->dt;
+    s.c1 = std::exp(-it->friction * it->dt);  // langevin.hpp:39-40
+    s.c2 = std::sqrt(1.0 - s.c1 * s.c1);
+    s.temperature = it->temperature;
+    s.key0 = static_cast<uint32_t>(it->seed);
+    s.key1 = static_cast<uint32_t>(it->seed >> 32);
+    s.step = it->step;
+    s.noise = nullptr;
+    return s;
+}
+
+int kick_grid(const md_system* sys) {
+    const int64_t want = (sys->n + kBlock - 1) / kBlock;
+    const int cap = sys->ctx->sm_count * 8;
+    return static_cast<int>(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+NhcState* nhc_of(md_integrator* it) {
+    return it->kind == 2 ? it->chain_state.as<NhcState>() : nullptr;
+}
+
+int pre_force(md_integrator* it, md_system* sys) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    if (n == 0) return MD_OK;
+    StepArgs s = step_args(it, sys);
+    if (it->kind == 1) {
+        if (it->noise.ptr) {
+            if (it->noise_used + 3 * n > it->noise_count)
+                return fail(MD_ERR_INVALID_ARGUMENT, "BAOAB: replayed noise exhausted");
+            s.noise = it->noise.as<double>() + it->noise_used;
+            it->noise_used += 3 * n;
+        }
+        k_baoab_pre<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, n, s);
+        ++it->step;
+    } else {
+        NhcState* nhc = nhc_of(it);
+        if (nhc) {
+            // start-of-step chain half needs the current kinetic energy
+            MDB_TRY(system_kinetic_async(sys, kResKE));
+            k_nhc_pre<<<1, 1, 0, ctx->stream>>>(nhc, ctx_result(ctx, kResKE), yoshida());
+            ctx->launches += 1;
+        }
+        k_kick_drift<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc);
+    }
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    StepArgs s = step_args(it, sys);
+    const int g = kick_grid(sys);
+    double* part;
+    MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
+    if (n > 0) {
+        k_kick_ke<<<g, kBlock, 0, ctx->stream>>>(sys->cur, n, s, part, ctx_counter(ctx, 3),
+                                                ctx_result(ctx, kResKE));
+        ++ctx->launches;
+    }
+    NhcState* nhc = nhc_of(it);
+    if (nhc) {
+        k_nhc_post<<<1, 1, 0, ctx->stream>>>(nhc, ctx_result(ctx, kResKE), yoshida());
+        ++ctx->launches;
+        if (apply_scale) {
+            if (n > 0) {
+                k_scale<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, n, nhc);
+                ++ctx->launches;
+            }
+            k_reset_scale<<<1, 1, 0, ctx->stream>>>(nhc);
+            ++ctx->launches;
+        }
+    }
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+}  // namespace
+
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
+int verlet_check(md_verlet* v, md_system* sys);
+int verlet_build(md_verlet* v, md_system* sys, bool conditional);
+
+}  // namespace mdb
+
+using namespace mdb;
+
+extern "C" {
+
+int md_integrator_create_vv(double dt, md_integrator** out) {
+    if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_vv: NULL");
+    md_integrator* it = new (std::nothrow) md_integrator();
+    if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_vv: host allocation");
+    it->kind = 0;
+    it->dt = dt;
+    *out = it;
+    return MD_OK;
+}
+
+int md_integrator_create_baoab(double dt, double friction, double temperature, uint64_t seed,
+                               md_integrator** out) {
+    if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_baoab: NULL");
+    md_integrator* it = new (std::nothrow) md_integrator();
+    if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_baoab: host allocation");
+    it->kind = 1;
+    it->dt = dt;
+    it->friction = friction;
+    it->temperature = temperature;
+    it->seed = seed;
+    *out = it;
+    return MD_OK;
+}
+
+int md_integrator_create_nhc(double dt, double temperature, double tau, int chain_length,
+                             int64_t dof, md_integrator** out) {
+    if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_nhc: NULL");
+    if (chain_length < 1)  // nose_hoover.cpp:36-38
+        return fail(MD_ERR_INVALID_ARGUMENT, "NoseHooverChain: chainLength must be >= 1");
+    if (chain_length > kMaxChain)
+        return fail(MD_ERR_INVALID_ARGUMENT, "NoseHooverChain: chainLength must be <= %d", kMaxChain);
+    md_integrator* it = new (std::nothrow) md_integrator();
+    if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_nhc: host allocation");
+    it->kind = 2;
+    it->dt = dt;
+    it->temperature = temperature;
+    it->tau = tau;
+    it->chain = chain_length;
+    it->dof = dof;
+    NhcState st{};
+    st.chain = chain_length;
+    st.dt = dt;
+    st.temperature = temperature;
+    st.dof = static_cast<double>(dof);
+    st.Q[0] = static_cast<double>(dof) * temperature * tau * tau;  // nose_hoover.cpp:39-42
+    for (int k = 1; k < chain_length; ++k) st.Q[k] = temperature * tau * tau;
+    st.scale = 1.0;
+    int rc = it->chain_state.ensure(sizeof(NhcState));
+    if (rc == MD_OK && cudaMemcpy(it->chain_state.ptr, &st, sizeof(NhcState),
+                                  cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(MD_ERR_CUDA, "md_integrator_create_nhc: upload failed");
+    if (rc != MD_OK) {
+        it->chain_state.release();
+        delete it;
+        return rc;
+    }
+    *out = it;
+    return MD_OK;
+}
+
+int md_integrator_destroy(md_integrator* it) {
+    if (!it) return MD_OK;
+    cudaDeviceSynchronize();
+    it->chain_state.release();
+    it->noise.release();
+    delete it;
+    return MD_OK;
+}
+
+int md_integrator_pre_force(md_integrator* it, md_system* sys) {
+    if (!it || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_pre_force: NULL");
+    return pre_force(it, sys);
+}
+
+int md_integrator_post_force(md_integrator* it, md_system* sys) {
+    if (!it || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_post_force: NULL");
+    return post_force_async(it, sys, true);
+}
+
+int md_integrator_conserved(md_integrator* it, double* value) {
+    if (!it || !value) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_conserved: NULL");
+    if (it->kind != 2) {
+        *value = 0.0;
+        return MD_OK;
+    }
+    // A tiny read on the default stream after all work on every stream finished.
+    MDB_CUDA(cudaDeviceSynchronize());
+    double* d;
+    MDB_CUDA(cudaMalloc(&d, sizeof(double)));
+    k_conserved<<<1, 1>>>(it->chain_state.as<NhcState>(), d);
+    MDB_CUDA(cudaMemcpy(value, d, sizeof(double), cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    return MD_OK;
+}
+
+int md_integrator_set_noise(md_integrator* it, const double* xi, int64_t count) {
+    if (!it) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_set_noise: NULL");
+    if (it->kind != 1) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_set_noise: not BAOAB");
+    if (!xi) {
+        it->noise.release();
+        it->noise_count = it->noise_used = 0;
+        return MD_OK;
+    }
+    MDB_TRY(it->noise.ensure(sizeof(double) * static_cast<size_t>(count)));
+    MDB_CUDA(cudaMemcpy(it->noise.ptr, xi, sizeof(double) * static_cast<size_t>(count),
+                        cudaMemcpyHostToDevice));
+    it->noise_count = count;
+    it->noise_used = 0;
+    return MD_OK;
+}
+
+int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_t steps,
+              double* thermo) {
+    if (!it || !sys || !v || !lj) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: NULL argument");
+    if (steps < 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: steps < 0");
+    MDB_TRY(verlet_ensure_ready(v, sys, "md_run_lj"));
+    md_context* ctx = sys->ctx;
+    DevBuf rows;
+    if (thermo && steps > 0) MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
+    NhcState* nhc = nhc_of(it);
+    if (nhc && sys->n > 0) {
+        // kinetic energy of the entry velocities for the first chain half
+        MDB_TRY(system_kinetic_async(sys, kResKE));
+    }
+    for (int64_t k = 0; k < steps; ++k) {
+        if (nhc) {
+            k_nhc_pre<<<1, 1, 0, ctx->stream>>>(nhc, k == 0 ? ctx_result(ctx, kResKE) : nullptr,
+                                                yoshida());
+            ++ctx->launches;
+        }
+        if (it->kind == 1) {
+            MDB_TRY(pre_force(it, sys));
+        } else if (sys->n > 0) {
+            StepArgs s = step_args(it, sys);
+            k_kick_drift<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n, s,
+                                                                              nhc);
+            ++ctx->launches;
+        }
+        // ForceFn of apps/moldyn_run.cpp:581-587, decided on the device.
+        MDB_TRY(verlet_check(v, sys));
+        MDB_TRY(verlet_build(v, sys, true));
+        MDB_TRY(lj_forces_verlet_async(lj, sys, v));
+        MDB_TRY(post_force_async(it, sys, false));
+        if (rows.ptr) {
+            k_record<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE),
+                                               nhc, rows.as<double>() + 4 * k);
+            ++ctx->launches;
+        }
+        MDB_CHECK_LAUNCH();
+    }
+    if (nhc && steps > 0 && sys->n > 0) {
+        k_scale<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n, nhc);
+        k_reset_scale<<<1, 1, 0, ctx->stream>>>(nhc);
+        ctx->launches += 2;
+    }
+    if (rows.ptr)
+        MDB_CUDA(cudaMemcpyAsync(thermo, rows.ptr, sizeof(double) * 4 * static_cast<size_t>(steps),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    rows.release();
+    MDB_TRY(ctx_check_status(ctx));
+    double r[2];
+    MDB_TRY(ctx_read_results(ctx, kResEnergy, 2, r));
+    sys->last_energy = r[0];
+    sys->last_virial = r[1];
+    return MD_OK;
+}
+
+}  // extern "C"

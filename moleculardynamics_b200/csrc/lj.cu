@@ -1,0 +1,464 @@
+// lj.cu -- Lennard-Jones pair forces, energy and virial (forcefield/lennard_jones.cpp).
+//
+// FP64 path: every pair term is computed with the reference's operation order
+// (lennard_jones.cpp:56-86) using non-contracting intrinsics, so each pair's
+// contribution is bit-identical to the reference's; only the order in which
+// per-atom sums are accumulated differs (full neighbour list, no atomics).
+// Mixed path: FP64 minimum-image displacement, FP32 r^2, r^-6 and force terms,
+// FP64 accumulation of forces, energy and virial.
+#include <algorithm>
+#include <new>
+
+#include "md_device.cuh"
+#include "md_internal.cuh"
+
+namespace mdb {
+int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
+}
+
+namespace mdb {
+
+namespace {
+
+struct LJArgs {
+    double sig2, rc2, rc, uc, dudrc, four_eps, tf_eps;
+    float sig2f, rc2f, rcf, ucf, dudrcf, four_epsf, tf_epsf;
+};
+
+LJArgs make_lj_args(const md_lj* lj) {
+    LJArgs a;
+    a.sig2 = lj->sigma * lj->sigma;
+    a.rc2 = lj->cutoff * lj->cutoff;
+    a.rc = lj->cutoff;
+    a.uc = lj->u_at_cutoff;
+    a.dudrc = lj->dudr_at_cutoff;
+    a.four_eps = 4.0 * lj->epsilon;
+    a.tf_eps = 24.0 * lj->epsilon;
+    a.sig2f = static_cast<float>(a.sig2);
+    a.rc2f = static_cast<float>(a.rc2);
+    a.rcf = static_cast<float>(a.rc);
+    a.ucf = static_cast<float>(a.uc);
+    a.dudrcf = static_cast<float>(a.dudrc);
+    a.four_epsf = static_cast<float>(a.four_eps);
+    a.tf_epsf = static_cast<float>(a.tf_eps);
+    return a;
+}
+
+// lennard_jones.cpp:62-79 with exact operation order.  Returns false outside rc.
+template <bool LFS>
+__device__ __forceinline__ bool pair_exact(const LJArgs& a, double r2, double& u, double& w,
+                                           double& s) {
+    if (!(r2 < a.rc2)) return false;
+    const double s2 = __ddiv_rn(a.sig2, r2);
+    const double s6 = __dmul_rn(__dmul_rn(s2, s2), s2);
+    const double uLJ = __dmul_rn(a.four_eps, __dsub_rn(__dmul_rn(s6, s6), s6));
+    const double wLJ = __dmul_rn(a.tf_eps, __dsub_rn(__dmul_rn(__dmul_rn(2.0, s6), s6), s6));
+    if (LFS) {
+        const double r = __dsqrt_rn(r2);
+        u = __dsub_rn(__dsub_rn(uLJ, a.uc), __dmul_rn(__dsub_rn(r, a.rc), a.dudrc));
+        w = __dadd_rn(wLJ, __dmul_rn(r, a.dudrc));
+    } else {
+        u = uLJ;
+        w = wLJ;
+    }
+    s = __ddiv_rn(w, r2);
+    return true;
+}
+
+// Accumulates the pair (i, j) into atom i's force (FP64 reference arithmetic).
+// The displacement is always r_lo - r_hi by original index, as the reference's
+// i<j pair sources produce it; atom lo gains +f, atom hi gains -f.
+template <bool LFS>
+__device__ __forceinline__ void accumulate_exact(const LJArgs& a, const Box3& box, double4 pi,
+                                                 double4 pj, double& fx, double& fy, double& fz,
+                                                 double& e, double& vir) {
+    const bool lo = pi.w < pj.w;
+    double dx, dy, dz;
+    if (lo) min_image_exact(box, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+    else min_image_exact(box, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+    double u, w, s;
+    if (!pair_exact<LFS>(a, norm2_exact(dx, dy, dz), u, w, s)) return;
+    const double gx = __dmul_rn(dx, s), gy = __dmul_rn(dy, s), gz = __dmul_rn(dz, s);
+    if (lo) {
+        fx = __dadd_rn(fx, gx);
+        fy = __dadd_rn(fy, gy);
+        fz = __dadd_rn(fz, gz);
+        e = __dadd_rn(e, u);
+        vir = __dadd_rn(vir, w);
+    } else {
+        fx = __dsub_rn(fx, gx);
+        fy = __dsub_rn(fy, gy);
+        fz = __dsub_rn(fz, gz);
+    }
+}
+
+// Mixed precision: FP64 displacement (fast fold), FP32 pair terms, FP64 sums.
+template <bool LFS>
+__device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Box3& box, double4 pi,
+                                                 double4 pj, double& fx, double& fy, double& fz,
+                                                 double& e, double& vir) {
+    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    dx -= box.L[0] * rint(dx * box.inv[0]);
+    dy -= box.L[1] * rint(dy * box.inv[1]);
+    dz -= box.L[2] * rint(dz * box.inv[2]);
+    const float xf = static_cast<float>(dx), yf = static_cast<float>(dy), zf = static_cast<float>(dz);
+    const float r2 = xf * xf + yf * yf + zf * zf;
+    if (!(r2 < a.rc2f)) return;
+    const float inv = __frcp_rn(r2);
+    const float s2 = a.sig2f * inv;
+    const float s6 = s2 * s2 * s2;
+    float u = a.four_epsf * (s6 * s6 - s6);
+    float w = a.tf_epsf * (2.0f * s6 * s6 - s6);
+    if (LFS) {
+        const float r = sqrtf(r2);
+        u = u - a.ucf - (r - a.rcf) * a.dudrcf;
+        w = w + r * a.dudrcf;
+    }
+    const float s = w * inv;
+    fx += static_cast<double>(xf * s);
+    fy += static_cast<double>(yf * s);
+    fz += static_cast<double>(zf * s);
+    if (pi.w < pj.w) {
+        e += static_cast<double>(u);
+        vir += static_cast<double>(w);
+    }
+}
+
+constexpr int kBlock = 256;
+
+// Full Verlet list, TPA lanes per atom; rows are nbr[i*stride .. +count[i]).
+template <int TPA, bool MIXED, bool LFS>
+__global__ void __launch_bounds__(kBlock)
+k_lj_verlet(const double4* __restrict__ pos, const int* __restrict__ nbr,
+            const int* __restrict__ count, int stride, int64_t n, Box3 box, LJArgs a,
+            double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
+            double* part, unsigned* ticket, double* out) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t i = t / TPA;
+    const int g = static_cast<int>(t % TPA);
+    double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
+    if (i < n) {
+        const double4 pi = pos[i];
+        const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
+        const int* row = nbr + i * static_cast<int64_t>(stride);
+        for (int k = g; k < cnt; k += TPA) {
+            const double4 pj = ldg4(pos + __ldg(row + k));
+            if (MIXED) accumulate_mixed<LFS>(a, box, pi, pj, fx, fy, fz, e, vir);
+            else accumulate_exact<LFS>(a, box, pi, pj, fx, fy, fz, e, vir);
+        }
+    }
+#pragma unroll
+    for (int o = TPA / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (i < n && g == 0) {
+        fxo[i] = fx;
+        fyo[i] = fy;
+        fzo[i] = fz;
+    }
+    double v[2] = {e, vir};
+    grid_reduce<2>(v, part, ticket, out);
+}
+
+// Brute force (lennard_jones.cpp:90-97): every atom against every other atom,
+// positions staged through shared memory in tiles.
+template <bool LFS>
+__global__ void __launch_bounds__(kBlock)
+k_lj_brute(const double4* __restrict__ pos, int64_t n, Box3 box, LJArgs a, int write_forces,
+           double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
+           double* part, unsigned* ticket, double* out) {
+    __shared__ double4 tile[kBlock];
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
+    const double4 pi = i < n ? pos[i] : make_double4(0, 0, 0, -1.0);
+    for (int64_t base = 0; base < n; base += kBlock) {
+        __syncthreads();
+        if (base + threadIdx.x < n) tile[threadIdx.x] = pos[base + threadIdx.x];
+        __syncthreads();
+        const int lim = static_cast<int>(n - base < kBlock ? n - base : kBlock);
+        if (i < n) {
+            for (int t = 0; t < lim; ++t) {
+                if (base + t == i) continue;
+                accumulate_exact<LFS>(a, box, pi, tile[t], fx, fy, fz, e, vir);
+            }
+        }
+    }
+    if (i < n && write_forces) {
+        fxo[i] = fx;
+        fyo[i] = fy;
+        fzo[i] = fz;
+    }
+    double v[2] = {e, vir};
+    grid_reduce<2>(v, part, ticket, out);
+}
+
+// CellList source (lennard_jones.cpp:99-114): for every atom, the atoms of the 27
+// cells around the cell it was binned into at build time.
+struct CellArgs {
+    int nx, ny, nz, ncells;
+    const int* rank_of_cell;
+    const int* cell_of_rank;
+    const int* start;
+    const int* sorted_orig;
+    const int* slot;
+};
+
+template <bool LFS>
+__global__ void __launch_bounds__(kBlock)
+k_lj_cells(const double4* __restrict__ pos, int64_t n, Box3 box, LJArgs a, CellArgs c,
+           double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
+           double* part, unsigned* ticket, double* out) {
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
+    if (s < n) {
+        // rank of sorted position s: binary search in start[]
+        int lo = 0, hi = c.ncells;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (c.start[mid] <= s) lo = mid;
+            else hi = mid;
+        }
+        const int cell = c.cell_of_rank[lo];
+        const int i = c.slot[c.sorted_orig[s]];
+        const double4 pi = pos[i];
+        const int cx = cell % c.nx, cy = (cell / c.nx) % c.ny, cz = cell / (c.nx * c.ny);
+        for (int q = 0; q < 27; ++q) {
+            int jx = cx + (q % 3) - 1, jy = cy + ((q / 3) % 3) - 1, jz = cz + (q / 9) - 1;
+            jx = jx < 0 ? jx + c.nx : (jx >= c.nx ? jx - c.nx : jx);
+            jy = jy < 0 ? jy + c.ny : (jy >= c.ny ? jy - c.ny : jy);
+            jz = jz < 0 ? jz + c.nz : (jz >= c.nz ? jz - c.nz : jz);
+            const int rr = c.rank_of_cell[jx + c.nx * (jy + c.ny * jz)];
+            for (int t = c.start[rr]; t < c.start[rr + 1]; ++t) {
+                if (t == s) continue;
+                const int j = c.slot[c.sorted_orig[t]];
+                accumulate_exact<LFS>(a, box, pi, pos[j], fx, fy, fz, e, vir);
+            }
+        }
+        fxo[i] = fx;
+        fyo[i] = fy;
+        fzo[i] = fz;
+    }
+    double v[2] = {e, vir};
+    grid_reduce<2>(v, part, ticket, out);
+}
+
+Box3 box_of(const md_system* sys) {
+    Box3 b;
+    for (int d = 0; d < 3; ++d) {
+        b.L[d] = sys->box[d];
+        b.inv[d] = sys->inv_box[d];
+    }
+    return b;
+}
+
+template <int TPA, bool MIXED, bool LFS>
+void launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
+                   double* out) {
+    const int64_t threads = sys->n * TPA;
+    k_lj_verlet<TPA, MIXED, LFS><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
+        sys->cur.pos, v->nbr.as<int>(), v->count.as<int>(), v->stride, sys->n, box_of(sys), a,
+        sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+}
+
+template <bool MIXED, bool LFS>
+void launch_verlet_tpa(int tpa, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                       unsigned* ticket, double* out) {
+    switch (tpa) {
+        case 1: launch_verlet<1, MIXED, LFS>(sys, v, a, part, ticket, out); break;
+        case 2: launch_verlet<2, MIXED, LFS>(sys, v, a, part, ticket, out); break;
+        case 8: launch_verlet<8, MIXED, LFS>(sys, v, a, part, ticket, out); break;
+        case 16: launch_verlet<16, MIXED, LFS>(sys, v, a, part, ticket, out); break;
+        default: launch_verlet<4, MIXED, LFS>(sys, v, a, part, ticket, out); break;
+    }
+}
+
+}  // namespace
+
+int g_lj_tpa = 4;  // threads per atom of the Verlet force kernel (tunable)
+
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
+    md_context* ctx = sys->ctx;
+    const LJArgs a = make_lj_args(lj);
+    const int64_t threads = std::max<int64_t>(sys->n * g_lj_tpa, 1);
+    const int blocks = grid_for(threads, kBlock);
+    double* part;
+    MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+    unsigned* ticket = ctx_counter(ctx, 2);
+    double* out = ctx_result(ctx, kResEnergy);
+    const bool lfs = lj->truncation == MD_LINEAR_FORCE_SHIFT;
+    const bool mixed = lj->precision == MD_PRECISION_MIXED;
+    if (mixed) {
+        if (lfs) launch_verlet_tpa<true, true>(g_lj_tpa, sys, v, a, part, ticket, out);
+        else launch_verlet_tpa<true, false>(g_lj_tpa, sys, v, a, part, ticket, out);
+    } else {
+        if (lfs) launch_verlet_tpa<false, true>(g_lj_tpa, sys, v, a, part, ticket, out);
+        else launch_verlet_tpa<false, false>(g_lj_tpa, sys, v, a, part, ticket, out);
+    }
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int lj_forces_brute_async(md_lj* lj, md_system* sys, bool forces) {
+    md_context* ctx = sys->ctx;
+    const LJArgs a = make_lj_args(lj);
+    const int blocks = grid_for(std::max<int64_t>(sys->n, 1), kBlock);
+    double* part;
+    MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+    if (lj->truncation == MD_LINEAR_FORCE_SHIFT)
+        k_lj_brute<true><<<blocks, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->n, box_of(sys), a, forces ? 1 : 0, sys->cur.fx, sys->cur.fy,
+            sys->cur.fz, part, ctx_counter(ctx, 2), ctx_result(ctx, kResEnergy));
+    else
+        k_lj_brute<false><<<blocks, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->n, box_of(sys), a, forces ? 1 : 0, sys->cur.fx, sys->cur.fy,
+            sys->cur.fz, part, ctx_counter(ctx, 2), ctx_result(ctx, kResEnergy));
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int lj_forces_cells_async(md_lj* lj, md_system* sys, md_cells* cells) {
+    md_context* ctx = sys->ctx;
+    const LJArgs a = make_lj_args(lj);
+    const int blocks = grid_for(std::max<int64_t>(sys->n, 1), kBlock);
+    double* part;
+    MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+    CellArgs c;
+    c.nx = cells->grid.nx;
+    c.ny = cells->grid.ny;
+    c.nz = cells->grid.nz;
+    c.ncells = cells->grid.ncells;
+    c.rank_of_cell = cells->grid.rank_of_cell;
+    c.cell_of_rank = cells->grid.cell_of_rank;
+    c.start = cells->start.as<int>();
+    c.sorted_orig = cells->sorted_orig.as<int>();
+    c.slot = sys->slot;
+    if (lj->truncation == MD_LINEAR_FORCE_SHIFT)
+        k_lj_cells<true><<<blocks, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->n, box_of(sys), a, c, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
+            ctx_counter(ctx, 2), ctx_result(ctx, kResEnergy));
+    else
+        k_lj_cells<false><<<blocks, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->n, box_of(sys), a, c, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
+            ctx_counter(ctx, 2), ctx_result(ctx, kResEnergy));
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+}  // namespace mdb
+
+using namespace mdb;
+
+namespace {
+int finish_energy(md_system* sys, double* energy, double* virial) {
+    double r[2];
+    MDB_TRY(ctx_read_results(sys->ctx, kResEnergy, 2, r));
+    sys->last_energy = r[0];
+    sys->last_virial = r[1];
+    if (energy) *energy = r[0];
+    if (virial) *virial = r[1];
+    return MD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int md_lj_create(double sigma, double epsilon, double cutoff, int truncation, int precision,
+                 md_lj** out) {
+    if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_create: out is NULL");
+    if (truncation != MD_TRUNCATED && truncation != MD_LINEAR_FORCE_SHIFT)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_create: unknown truncation %d", truncation);
+    if (precision != MD_PRECISION_FP64 && precision != MD_PRECISION_MIXED)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_create: unknown precision %d", precision);
+    md_lj* lj = new (std::nothrow) md_lj();
+    if (!lj) return fail(MD_ERR_OUT_OF_MEMORY, "md_lj_create: host allocation");
+    lj->sigma = sigma;
+    lj->epsilon = epsilon;
+    lj->cutoff = cutoff;
+    lj->truncation = truncation;
+    lj->precision = precision;
+    // lennard_jones.cpp:32-48
+    const double sig2 = sigma * sigma;
+    const double rc2 = cutoff * cutoff;
+    const double s2 = sig2 / rc2;
+    const double s6 = s2 * s2 * s2;
+    lj->u_at_cutoff = 4.0 * epsilon * (s6 * s6 - s6);
+    const double w_at_cutoff = 24.0 * epsilon * (2.0 * s6 * s6 - s6);
+    lj->dudr_at_cutoff = -w_at_cutoff / cutoff;
+    *out = lj;
+    return MD_OK;
+}
+
+int md_lj_destroy(md_lj* lj) {
+    delete lj;
+    return MD_OK;
+}
+
+int md_lj_energy_virial(md_lj* lj, md_system* sys, double* energy, double* virial) {
+    if (!lj || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_energy_virial: NULL argument");
+    MDB_TRY(lj_forces_brute_async(lj, sys, false));
+    return finish_energy(sys, energy, virial);
+}
+
+int md_lj_forces(md_lj* lj, md_system* sys, double* energy, double* virial) {
+    if (!lj || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_forces: NULL argument");
+    MDB_TRY(lj_forces_brute_async(lj, sys, true));
+    return finish_energy(sys, energy, virial);
+}
+
+int md_lj_forces_cells(md_lj* lj, md_system* sys, md_cells* cells, double* energy,
+                       double* virial) {
+    if (!lj || !sys || !cells) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_forces_cells: NULL argument");
+    // lennard_jones.cpp:107-111
+    if (!cells->grid.usable)
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "LennardJones::computeForces: CellList is not usable (fewer than 3 cells per "
+                    "side); fall back to the brute-force overload");
+    if (!cells->built || cells->sys != sys || cells->n != sys->n)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_forces_cells: cell list not built for this system");
+    MDB_TRY(lj_forces_cells_async(lj, sys, cells));
+    return finish_energy(sys, energy, virial);
+}
+
+int md_lj_forces_verlet(md_lj* lj, md_system* sys, md_verlet* list, double* energy,
+                        double* virial) {
+    if (!lj || !sys || !list) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_forces_verlet: NULL argument");
+    MDB_TRY(verlet_ensure_ready(list, sys, "md_lj_forces_verlet"));
+    MDB_TRY(lj_forces_verlet_async(lj, sys, list));
+    return finish_energy(sys, energy, virial);
+}
+
+int md_lj_lrc(const md_lj* lj, int64_t n, const double box[3], double* u_lrc, double* p_lrc) {
+    if (!lj || !box) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_lrc: NULL argument");
+    // lennard_jones.cpp:121-151 (host scalars, O(1))
+    const double kPi = 3.14159265358979323846;
+    if (lj->truncation == MD_LINEAR_FORCE_SHIFT) {
+        if (u_lrc) *u_lrc = 0.0;
+        if (p_lrc) *p_lrc = 0.0;
+        return MD_OK;
+    }
+    const double nd = static_cast<double>(n);
+    const double rho = nd / (box[0] * box[1] * box[2]);
+    const double sr = lj->sigma / lj->cutoff;
+    const double sr3 = sr * sr * sr;
+    const double sr9 = sr3 * sr3 * sr3;
+    const double sig3 = lj->sigma * lj->sigma * lj->sigma;
+    if (u_lrc) *u_lrc = (8.0 / 3.0) * kPi * nd * rho * lj->epsilon * sig3 * ((1.0 / 3.0) * sr9 - sr3);
+    if (p_lrc)
+        *p_lrc = (16.0 / 3.0) * kPi * rho * rho * lj->epsilon * sig3 * ((2.0 / 3.0) * sr9 - sr3);
+    return MD_OK;
+}
+
+// Threads per atom of the Verlet force kernel (1, 2, 4, 8 or 16); autotuning hook.
+int md_lj_set_threads_per_atom(int tpa) {
+    if (tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8 && tpa != 16)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_threads_per_atom: %d not in {1,2,4,8,16}", tpa);
+    g_lj_tpa = tpa;
+    return MD_OK;
+}
+
+}  // extern "C"

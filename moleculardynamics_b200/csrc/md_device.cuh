@@ -1,0 +1,173 @@
+// md_device.cuh -- device helpers shared by the kernels.
+//
+// Exact-arithmetic helpers: the FP64 drop-in path must reproduce the reference's
+// pair membership bit-for-bit, so every operation that decides whether a pair is
+// inside a cutoff is written with explicit round-to-nearest intrinsics (__dmul_rn,
+// __dadd_rn, __dsub_rn, __ddiv_rn), which the compiler may not contract into FMAs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace mdb {
+
+// core/box.cpp:12-15: value - L * floor(value / L + 0.5), bit-exact.
+// value/L is first approximated by value * (1/L); only when that lands within
+// 1e-9 of a rounding boundary of floor(. + 0.5) -- where the one-ulp difference
+// between value*(1/L) and value/L could matter -- is the IEEE division used.
+__device__ __forceinline__ double fold_exact(double v, double L, double invL) {
+    const double s = __dadd_rn(__dmul_rn(v, invL), 0.5);
+    double k = floor(s);
+    const double frac = __dsub_rn(s, k);
+    if (frac < 1e-9 || frac > 1.0 - 1e-9) k = floor(__dadd_rn(__ddiv_rn(v, L), 0.5));
+    return __dsub_rn(v, __dmul_rn(L, k));
+}
+
+// core/vec3.hpp:59-65: x*x + y*y + z*z, left to right, no contraction.
+__device__ __forceinline__ double norm2_exact(double x, double y, double z) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+struct Box3 {
+    double L[3];
+    double inv[3];
+};
+
+// Minimum-image displacement r_a - r_b with the reference's operation order.
+__device__ __forceinline__ void min_image_exact(const Box3& b, double ax, double ay, double az,
+                                                double bx, double by, double bz, double& dx,
+                                                double& dy, double& dz) {
+    dx = fold_exact(__dsub_rn(ax, bx), b.L[0], b.inv[0]);
+    dy = fold_exact(__dsub_rn(ay, by), b.L[1], b.inv[1]);
+    dz = fold_exact(__dsub_rn(az, bz), b.L[2], b.inv[2]);
+}
+
+// Read-only 32-byte load through the non-coherent path (two 16-byte loads).
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// ----------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic grid reduction of K doubles per thread.  Each block reduces its
+// values with a fixed shuffle tree and writes part[block*K + k]; the last block
+// to arrive (atomic ticket) re-reduces all partials in block order and writes
+// out[k], then resets the ticket.  Must be called by every thread of the block;
+// blockDim.x must be a multiple of 32 and <= 1024.
+template <int K>
+__device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out) {
+    __shared__ double sm[K][32];
+    __shared__ bool is_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const double s = warp_sum(v[k]);
+        if (lane == 0) sm[k][warp] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < nw ? sm[k][lane] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) part[static_cast<size_t>(blockIdx.x) * K + k] = s;
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += __ldcg(part + static_cast<size_t>(b) * K + k);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const double s = warp_sum(acc[k]);
+        if (lane == 0) sm[k][warp] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < nw ? sm[k][lane] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out[k] = s;
+        }
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Top-2 of a multiset (verlet_list.cpp:44-63): (a1 >= a2), merge with (b1 >= b2).
+__device__ __forceinline__ void top2_merge(double& a1, double& a2, double b1, double b2) {
+    if (b1 > a1) {
+        a2 = fmax(a1, b2);
+        a1 = b1;
+    } else {
+        a2 = fmax(a2, b1);
+    }
+}
+
+__device__ __forceinline__ void top2_insert(double& a1, double& a2, double d) {
+    if (d > a1) {
+        a2 = a1;
+        a1 = d;
+    } else if (d > a2) {
+        a2 = d;
+    }
+}
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), counter-based RNG.
+struct U4 {
+    uint32_t x, y, z, w;
+};
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+        k0 += W0;
+        k1 += W1;
+    }
+    return c;
+}
+
+// Uniform in (0, 1] from 53 random bits.
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+    const uint64_t v = (static_cast<uint64_t>(a) << 21) ^ static_cast<uint64_t>(b >> 11);
+    return (static_cast<double>(v & ((1ull << 53) - 1)) + 1.0) * (1.0 / 9007199254740992.0);
+}
+
+// Two standard normals by Box-Muller from one Philox block.
+__device__ __forceinline__ void normal2(U4 r, double& n0, double& n1) {
+    const double u1 = u53(r.x, r.y);
+    const double u2 = u53(r.z, r.w);
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincospi(2.0 * u2, &s, &c);
+    n0 = rad * c;
+    n1 = rad * s;
+}
+
+}  // namespace mdb

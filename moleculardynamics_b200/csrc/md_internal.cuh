@@ -1,0 +1,237 @@
+// md_internal.cuh -- shared internals of the moldyn B200 library.
+//
+// Device layout (one md_system):
+//   pos   double4  (x, y, z, original index as a double)  -- gathered by pair kernels
+//   vx vy vz fx fy fz mass inv_mass charge   double SoA   -- streamed by integrators
+//   mol   int64 molecule id; orig (device slot -> original index), slot (inverse)
+// Atoms are stored sorted by Morton-ranked cell (re-sorted at each Verlet rebuild).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/moldyn_b200.h"
+
+namespace mdb {
+
+// ------------------------------------------------------------------ errors
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+
+#define MDB_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return ::mdb::fail(MD_ERR_CUDA, "%s:%d: %s: %s", __FILE__, __LINE__, #call,  \
+                               cudaGetErrorString(e_));                                  \
+    } while (0)
+
+#define MDB_CHECK_LAUNCH() MDB_CUDA(cudaGetLastError())
+
+#define MDB_TRY(call)            \
+    do {                         \
+        int rc_ = (call);        \
+        if (rc_ != MD_OK) return rc_; \
+    } while (0)
+
+// ------------------------------------------------------------ device buffers
+// Grow-only device allocation (bytes), freed by the owner.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want);
+    void release();
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+}  // namespace mdb
+
+// ------------------------------------------------------------------ context
+struct md_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t* d_status = nullptr;        // device status word
+    unsigned* d_counter = nullptr;       // last-block counters (zeroed; reset by the last block)
+    mdb::DevBuf partials;                // per-block reduction partials
+    mdb::DevBuf scratch;                 // general scratch (staging, scans)
+    mdb::DevBuf result;                  // small device results (energy, virial, ...)
+    double* h_result = nullptr;          // pinned host mirror of `result`
+    int64_t launches = 0;
+    int sm_count = 148;
+};
+
+namespace mdb {
+
+constexpr int kMaxResults = 64;      // doubles in context->result
+constexpr int kCounterSlots = 64;    // independent last-block counters
+
+// Result slot layout inside ctx->result (doubles).
+enum ResultSlot : int {
+    kResEnergy = 0,
+    kResVirial = 1,
+    kResKE = 2,
+    kResTop2 = 4,      // 2 doubles: largest, second
+    kResMomentum = 8,  // 4 doubles: px, py, pz, total mass
+    kResFlag = 12,     // rebuild flag (as double)
+    kResEwald = 16,    // 8 doubles: real, recip, self, intra, virial
+    kResScratch = 32,
+};
+
+int ctx_partials(md_context* ctx, size_t doubles, double** out);
+int ctx_scratch(md_context* ctx, size_t bytes, void** out);
+int ctx_read_results(md_context* ctx, int first, int count, double* out);  // synchronises
+int ctx_check_status(md_context* ctx);  // synchronises; MD_ERR_DEVICE if status set
+inline unsigned* ctx_counter(md_context* ctx, int slot) { return ctx->d_counter + slot; }
+inline double* ctx_result(md_context* ctx, int slot) {
+    return ctx->result.as<double>() + slot;
+}
+
+inline int grid_for(int64_t threads, int block) {
+    int64_t g = (threads + block - 1) / block;
+    return static_cast<int>(g < 1 ? 1 : g);
+}
+
+}  // namespace mdb
+
+// ------------------------------------------------------------------- system
+struct md_atoms {
+    double4* pos = nullptr;  // x, y, z, (double) original index
+    double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    double *fx = nullptr, *fy = nullptr, *fz = nullptr;
+    double *mass = nullptr, *inv_mass = nullptr, *charge = nullptr;
+    int64_t* mol = nullptr;
+    int* orig = nullptr;
+};
+
+struct md_system {
+    md_context* ctx = nullptr;
+    int64_t n = 0;
+    double box[3] = {0, 0, 0};
+    double inv_box[3] = {0, 0, 0};
+    md_atoms cur, alt;        // current device order and the permutation target
+    int* slot = nullptr;      // original index -> device slot
+    uint64_t epoch = 1;       // bumped by every re-sort
+    bool has_molecules = false;  // molecule ids differ from the atom's own index
+    double last_energy = 0.0, last_virial = 0.0;
+};
+
+namespace mdb {
+
+int system_alloc_atoms(md_system* sys, md_atoms* a);
+void system_free_atoms(md_atoms* a);
+// Applies a gather permutation: new slot s takes old slot perm[s].
+int system_permute(md_system* sys, const int* d_perm);
+
+// ------------------------------------------------------------- cell grid
+struct CellGrid {
+    int nx = 1, ny = 1, nz = 1;
+    int ncells = 1;
+    double cutoff = 0.0;
+    double width[3] = {0, 0, 0};
+    bool usable = false;
+    int* rank_of_cell = nullptr;   // device: reference cell id -> Morton rank
+    int* cell_of_rank = nullptr;   // device: rank -> reference cell id
+    int init(const double box[3], double cutoff);
+    void release();
+};
+
+// Counting sort of the system's atoms by (Morton rank of cell, original index).
+// d_sorted receives, for sorted position s, the current device slot; d_start
+// (ncells+1) the start of each rank's range.  Pure function of the positions.
+int cell_sort(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_start);
+
+}  // namespace mdb
+
+struct md_cells {
+    md_context* ctx = nullptr;
+    double box[3] = {0, 0, 0};
+    mdb::CellGrid grid;
+    mdb::DevBuf sorted_orig;  // original index per sorted position
+    mdb::DevBuf start;        // ncells + 1
+    md_system* sys = nullptr; // system it was last built from
+    int64_t n = 0;
+    bool built = false;
+};
+
+struct md_verlet {
+    md_context* ctx = nullptr;
+    double box[3] = {0, 0, 0};
+    double cutoff = 0.0, skin = 0.0;
+    int criterion = 0;            // 0 reference top-2 sum, 1 max > skin/2
+    mdb::CellGrid grid;
+    mdb::DevBuf start;            // ncells + 1 (device order == sorted order)
+    mdb::DevBuf perm;             // scratch for the sort
+    mdb::DevBuf nbr;              // n * stride device indices
+    mdb::DevBuf count;            // n neighbour counts
+    mdb::DevBuf ref;              // n double4 positions at the last build
+    int stride = 0;               // row capacity
+    int64_t n = 0;
+    int64_t rebuilds = 0;
+    uint64_t epoch = 0;           // system epoch the list refers to
+    md_system* sys = nullptr;
+    int* d_rebuild_flag = nullptr; // device: set by the displacement check
+    int* d_rebuild_total = nullptr; // device: rebuilds done inside fused loops
+    int* d_max_count = nullptr;     // device: largest row seen by the last build
+};
+
+namespace mdb {
+int verlet_build(md_verlet* v, md_system* sys, bool conditional);
+int verlet_check(md_verlet* v, md_system* sys);  // device flag <- needs rebuild
+int verlet_ensure_capacity(md_verlet* v, md_system* sys);
+}  // namespace mdb
+
+// --------------------------------------------------------------- potentials
+struct md_lj {
+    double sigma = 1, epsilon = 1, cutoff = 2.5;
+    int truncation = MD_TRUNCATED;
+    int precision = MD_PRECISION_FP64;
+    double u_at_cutoff = 0, dudr_at_cutoff = 0;
+};
+
+namespace mdb {
+// Pair-force kernels over the Verlet list; results land in the context result
+// slots kResEnergy / kResVirial (device), no synchronisation.
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
+int lj_forces_brute_async(md_lj* lj, md_system* sys, bool forces);
+int lj_forces_cells_async(md_lj* lj, md_system* sys, md_cells* cells);
+int system_kinetic_async(md_system* sys, int slot);
+}  // namespace mdb
+
+// ------------------------------------------------------------- integrators
+struct md_integrator {
+    int kind = 0;                 // 0 VV, 1 BAOAB, 2 NHC
+    double dt = 0.005;
+    // BAOAB
+    double friction = 1.0, temperature = 1.0;
+    uint64_t seed = 0;
+    uint64_t step = 0;            // O-step counter for Philox
+    mdb::DevBuf noise;            // optional replayed normals (original order)
+    int64_t noise_count = 0;
+    int64_t noise_used = 0;
+    // NHC
+    double tau = 0.5;
+    int chain = 3;
+    int64_t dof = 0;
+    mdb::DevBuf chain_state;      // device: NhcState
+    md_context* ctx = nullptr;
+};
+
+namespace mdb {
+// Chain-of-thermostats state kept on the device (nose_hoover.hpp:63-65).
+constexpr int kMaxChain = 16;
+struct NhcState {
+    double Q[kMaxChain];
+    double xi[kMaxChain];
+    double pxi[kMaxChain];
+    double dt, temperature;
+    double dof;
+    int chain;
+    double scale;       // pending velocity scale (applied by the next kick)
+    double ke;          // kinetic energy of the scaled velocities
+};
+}  // namespace mdb

@@ -1,0 +1,958 @@
+// neighbor.cu -- cell binning (CellList) and Verlet lists (VerletList) on the device.
+//
+// Binning (neighbor/cell_list.cpp:16-43) assigns each atom the reference's cell
+// (wrap, floor((r + L/2) / w), clamp) with bit-identical arithmetic, then counting-
+// sorts atoms by the Morton rank of their cell and, within a cell, by original
+// index, so the resulting order is a pure function of the positions.
+//
+// Verlet build (neighbor/verlet_list.cpp:8-42): one warp per cell scans the 27
+// neighbouring cells (>= 3 cells per side; the stencil then visits every unordered
+// cell pair exactly once from each side) or, for smaller boxes, every atom, and
+// compacts hits with __ballot_sync into a fixed-stride row per atom.  Membership
+// uses the reference's exact min-image r^2 with the pair ordered by original index
+// (r_lo - r_hi), so the pair set is bit-identical to the reference's.
+#include <algorithm>
+#include <cmath>
+#include <new>
+
+#include "md_device.cuh"
+#include "md_internal.cuh"
+
+namespace mdb {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kBuildWarps = 8;
+constexpr int kMaxCand = 1024;   // candidates staged per warp window
+
+__device__ __forceinline__ bool gate(const int* flag) { return flag == nullptr || *flag != 0; }
+
+// Reference cell id of a position (cell_list.cpp:29-39), exact arithmetic.
+__device__ __forceinline__ int cell_of(double x, double y, double z, const Box3& b, double wx,
+                                       double wy, double wz, int nx, int ny, int nz) {
+    const double rx = fold_exact(x, b.L[0], b.inv[0]);
+    const double ry = fold_exact(y, b.L[1], b.inv[1]);
+    const double rz = fold_exact(z, b.L[2], b.inv[2]);
+    int ix = static_cast<int>(floor(__ddiv_rn(__dadd_rn(rx, __dmul_rn(0.5, b.L[0])), wx)));
+    int iy = static_cast<int>(floor(__ddiv_rn(__dadd_rn(ry, __dmul_rn(0.5, b.L[1])), wy)));
+    int iz = static_cast<int>(floor(__ddiv_rn(__dadd_rn(rz, __dmul_rn(0.5, b.L[2])), wz)));
+    ix = ix < 0 ? 0 : (ix >= nx ? nx - 1 : ix);
+    iy = iy < 0 ? 0 : (iy >= ny ? ny - 1 : iy);
+    iz = iz < 0 ? 0 : (iz >= nz ? nz - 1 : iz);
+    return ix + nx * (iy + ny * iz);
+}
+
+struct GridArgs {
+    Box3 box;
+    double wx, wy, wz;
+    int nx, ny, nz, ncells;
+    const int* rank_of_cell;
+    const int* cell_of_rank;
+};
+
+__global__ void k_zero_int(int* a, int64_t n, const int* flag) {
+    if (!gate(flag)) return;
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        a[k] = 0;
+}
+
+__global__ void k_bin(const double4* __restrict__ pos, int64_t n, GridArgs g, int* atom_rank,
+                      int* counts, const int* flag) {
+    if (!gate(flag)) return;
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const double4 p = pos[k];
+    const int c = cell_of(p.x, p.y, p.z, g.box, g.wx, g.wy, g.wz, g.nx, g.ny, g.nz);
+    const int r = g.rank_of_cell[c];
+    atom_rank[k] = r;
+    atomicAdd(counts + r, 1);
+}
+
+// Single-block exclusive scan of counts[0..m) into start[0..m] (start[m] = total).
+__global__ void k_scan(const int* __restrict__ counts, int* start, int m, const int* flag) {
+    if (!gate(flag)) return;
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < m; base += blockDim.x) {
+        const int i = base + tid;
+        const int v = i < m ? counts[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_tot[lane] = w;
+        }
+        __syncthreads();
+        const int before = (warp > 0 ? warp_tot[warp - 1] : 0) + carry;
+        if (i < m) start[i] = before + x - v;
+        __syncthreads();
+        if (tid == blockDim.x - 1) carry = before + x;
+        __syncthreads();
+    }
+    if (tid == 0) start[m] = carry;
+}
+
+__global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const int* __restrict__ start,
+                          int* fill, int* sorted, const int* flag) {
+    if (!gate(flag)) return;
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const int r = atom_rank[k];
+    const int at = atomicAdd(fill + r, 1);
+    sorted[start[r] + at] = static_cast<int>(k);
+}
+
+// Within each cell, order atoms by original index (insertion sort; cells are small).
+__global__ void k_cell_order(int* sorted, const int* __restrict__ start, int m,
+                             const int* __restrict__ orig, const int* flag) {
+    if (!gate(flag)) return;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    const int s0 = start[r], s1 = start[r + 1];
+    for (int a = s0 + 1; a < s1; ++a) {
+        const int v = sorted[a];
+        const int key = orig[v];
+        int b = a - 1;
+        while (b >= s0 && orig[sorted[b]] > key) {
+            sorted[b + 1] = sorted[b];
+            --b;
+        }
+        sorted[b + 1] = v;
+    }
+}
+
+__global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restrict__ perm,
+                                int* slot, int64_t n, const int* flag) {
+    if (!gate(flag)) return;
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s >= n) return;
+    const int k = perm[s];
+    dst.pos[s] = src.pos[k];
+    dst.vx[s] = src.vx[k];
+    dst.vy[s] = src.vy[k];
+    dst.vz[s] = src.vz[k];
+    dst.fx[s] = src.fx[k];
+    dst.fy[s] = src.fy[k];
+    dst.fz[s] = src.fz[k];
+    dst.mass[s] = src.mass[k];
+    dst.inv_mass[s] = src.inv_mass[k];
+    dst.charge[s] = src.charge[k];
+    dst.mol[s] = src.mol[k];
+    const int o = src.orig[k];
+    dst.orig[s] = o;
+    slot[o] = static_cast<int>(s);
+}
+
+__global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* flag) {
+    if (!gate(flag)) return;
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s >= n) return;
+    dst.pos[s] = src.pos[s];
+    dst.vx[s] = src.vx[s];
+    dst.vy[s] = src.vy[s];
+    dst.vz[s] = src.vz[s];
+    dst.fx[s] = src.fx[s];
+    dst.fy[s] = src.fy[s];
+    dst.fz[s] = src.fz[s];
+    dst.mass[s] = src.mass[s];
+    dst.inv_mass[s] = src.inv_mass[s];
+    dst.charge[s] = src.charge[s];
+    dst.mol[s] = src.mol[s];
+    dst.orig[s] = src.orig[s];
+}
+
+// Exact candidate test with the pair ordered by original index.
+__device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, double rl2) {
+    double dx, dy, dz;
+    if (pi.w < pj.w) min_image_exact(b, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+    else min_image_exact(b, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+    return norm2_exact(dx, dy, dz) < rl2;
+}
+
+// One warp per (Morton-ranked) cell; device order == sorted order, so cell r holds
+// atoms [start[r], start[r+1]).
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
+               double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
+               uint32_t* status, int* max_count, const int* flag) {
+    if (!gate(flag)) return;
+    __shared__ int s_idx[kBuildWarps][kMaxCand];
+    __shared__ int s_cnt[kBuildWarps][32];
+    __shared__ int s_beg[kBuildWarps][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = blockIdx.x * kBuildWarps + warp;
+    if (r >= g.ncells) return;
+    const int cell = g.cell_of_rank[r];
+    const int cx = cell % g.nx, cy = (cell / g.nx) % g.ny, cz = cell / (g.nx * g.ny);
+    int beg = 0, cnt = 0;
+    if (lane < 27) {
+        int jx = cx + (lane % 3) - 1, jy = cy + ((lane / 3) % 3) - 1, jz = cz + (lane / 9) - 1;
+        jx = jx < 0 ? jx + g.nx : (jx >= g.nx ? jx - g.nx : jx);
+        jy = jy < 0 ? jy + g.ny : (jy >= g.ny ? jy - g.ny : jy);
+        jz = jz < 0 ? jz + g.nz : (jz >= g.nz ? jz - g.nz : jz);
+        const int rr = g.rank_of_cell[jx + g.nx * (jy + g.ny * jz)];
+        beg = start[rr];
+        cnt = start[rr + 1] - beg;
+    }
+    // inclusive scan of cnt over the 27 lanes
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    s_cnt[warp][lane] = incl - cnt;  // exclusive offset
+    s_beg[warp][lane] = beg;
+    __syncwarp();
+    const int a0 = start[r], a1 = start[r + 1];
+    for (int wb = 0; wb < total; wb += kMaxCand) {
+        const int wlen = min(kMaxCand, total - wb);
+        // stage candidate indices of this window
+        for (int t = lane; t < wlen; t += 32) {
+            const int gt = wb + t;
+            int q = 0;
+            while (q < 26 && s_cnt[warp][q + 1] <= gt) ++q;
+            s_idx[warp][t] = s_beg[warp][q] + (gt - s_cnt[warp][q]);
+        }
+        __syncwarp();
+        for (int i = a0; i < a1; ++i) {
+            const double4 pi = pos[i];
+            int base = (wb == 0) ? 0 : count[i];
+            for (int t0 = 0; t0 < wlen; t0 += 32) {
+                const int t = t0 + lane;
+                bool hit = false;
+                int j = -1;
+                if (t < wlen) {
+                    j = s_idx[warp][t];
+                    if (j != i) hit = within(g.box, pi, ldg4(pos + j), rl2);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (hit) {
+                    const int at = base + __popc(m & ((1u << lane) - 1u));
+                    if (at < stride) nbr[static_cast<int64_t>(i) * stride + at] = j;
+                }
+                base += __popc(m);
+            }
+            if (lane == 0) count[i] = base;
+            __syncwarp();
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        int mx = 0;
+        for (int i = a0; i < a1; ++i) mx = max(mx, count[i]);
+        if (mx > 0) atomicMax(max_count, mx);
+        if (mx > stride) atomicOr(status, MD_STATUS_NEIGHBOR_OVERFLOW);
+    }
+}
+
+// Boxes with fewer than 3 cells per side (verlet_list.cpp:26-33): one warp per atom
+// scans every other atom.
+__global__ void k_verlet_brute(const double4* __restrict__ pos, int64_t n, Box3 box, double rl2,
+                               int* __restrict__ nbr, int* __restrict__ count, int stride,
+                               uint32_t* status, int* max_count, const int* flag) {
+    if (!gate(flag)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t i = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const double4 pi = pos[i];
+    int base = 0;
+    for (int64_t t0 = 0; t0 < n; t0 += 32) {
+        const int64_t j = t0 + lane;
+        bool hit = false;
+        if (j < n && j != i) hit = within(box, pi, ldg4(pos + j), rl2);
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const int at = base + __popc(m & ((1u << lane) - 1u));
+            if (at < stride) nbr[i * stride + at] = static_cast<int>(j);
+        }
+        base += __popc(m);
+    }
+    if (lane == 0) {
+        count[i] = base;
+        atomicMax(max_count, base);
+        if (base > stride) atomicOr(status, MD_STATUS_NEIGHBOR_OVERFLOW);
+    }
+}
+
+__global__ void k_store_ref(const double4* __restrict__ pos, double4* ref, int64_t n,
+                            const int* flag, int* total) {
+    if (!gate(flag)) return;
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k < n) ref[k] = pos[k];
+    if (k == 0 && total) ++*total;
+}
+
+// verlet_list.cpp:44-63: top-2 min-image displacement norms; decides on device.
+__global__ void k_displacement(const double4* __restrict__ pos, const double4* __restrict__ ref,
+                               int64_t n, Box3 box, double skin, int criterion, double* part,
+                               unsigned* ticket, int* flag, double* top2_out) {
+    double a1 = 0.0, a2 = 0.0;
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double4 p = pos[k], q = ref[k];
+        double dx, dy, dz;
+        min_image_exact(box, p.x, p.y, p.z, q.x, q.y, q.z, dx, dy, dz);
+        top2_insert(a1, a2, __dsqrt_rn(norm2_exact(dx, dy, dz)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b1 = __shfl_xor_sync(0xffffffffu, a1, o);
+        const double b2 = __shfl_xor_sync(0xffffffffu, a2, o);
+        top2_merge(a1, a2, b1, b2);
+    }
+    __shared__ double s1[32], s2[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        s1[warp] = a1;
+        s2[warp] = a2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b1 = s1[0], b2 = s2[0];
+        for (int w = 1; w < nw; ++w) top2_merge(b1, b2, s1[w], s2[w]);
+        part[2 * blockIdx.x] = b1;
+        part[2 * blockIdx.x + 1] = b2;
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+        if (last) {
+            __threadfence();
+            double c1 = 0.0, c2 = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b)
+                top2_merge(c1, c2, __ldcg(part + 2 * b), __ldcg(part + 2 * b + 1));
+            top2_out[0] = c1;
+            top2_out[1] = c2;
+            const bool rebuild = criterion == 0 ? (c1 + c2) > skin : c1 > 0.5 * skin;
+            *flag = rebuild ? 1 : 0;
+            *ticket = 0u;
+        }
+    }
+}
+
+inline uint32_t spread3(uint32_t v) {
+    uint32_t x = v & 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+GridArgs make_args(const CellGrid& gr, const md_system* sys) {
+    GridArgs g;
+    for (int d = 0; d < 3; ++d) {
+        g.box.L[d] = sys->box[d];
+        g.box.inv[d] = sys->inv_box[d];
+    }
+    g.wx = gr.width[0];
+    g.wy = gr.width[1];
+    g.wz = gr.width[2];
+    g.nx = gr.nx;
+    g.ny = gr.ny;
+    g.nz = gr.nz;
+    g.ncells = gr.ncells;
+    g.rank_of_cell = gr.rank_of_cell;
+    g.cell_of_rank = gr.cell_of_rank;
+    return g;
+}
+
+Box3 make_box(const md_system* sys) {
+    Box3 b;
+    for (int d = 0; d < 3; ++d) {
+        b.L[d] = sys->box[d];
+        b.inv[d] = sys->inv_box[d];
+    }
+    return b;
+}
+
+// Scratch for one sort: atom_rank (n) + counts (m) + fill (m).
+int sort_scratch(md_context* ctx, int64_t n, int m, int** atom_rank, int** counts, int** fill) {
+    void* p;
+    const size_t bytes = (static_cast<size_t>(n) + 2 * static_cast<size_t>(m) + 64) * sizeof(int);
+    MDB_TRY(ctx_scratch(ctx, bytes, &p));
+    *atom_rank = static_cast<int*>(p);
+    *counts = *atom_rank + n;
+    *fill = *counts + m;
+    return MD_OK;
+}
+
+// Counting sort (see cell_sort), optionally gated by a device flag.
+int cell_sort_gated(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_start,
+                    const int* flag) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    const int m = grid.ncells;
+    int *atom_rank, *counts, *fill;
+    MDB_TRY(sort_scratch(ctx, n, m, &atom_rank, &counts, &fill));
+    const GridArgs g = make_args(grid, sys);
+    const int zb = std::min<int64_t>(grid_for(2 * static_cast<int64_t>(m), kBlock), 4096);
+    k_zero_int<<<zb, kBlock, 0, ctx->stream>>>(counts, 2 * static_cast<int64_t>(m), flag);
+    if (n > 0)
+        k_bin<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur.pos, n, g, atom_rank,
+                                                               counts, flag);
+    k_scan<<<1, 1024, 0, ctx->stream>>>(counts, d_start, m, flag);
+    if (n > 0)
+        k_scatter<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(atom_rank, n, d_start, fill,
+                                                                   d_sorted, flag);
+    k_cell_order<<<grid_for(m, 128), 128, 0, ctx->stream>>>(d_sorted, d_start, m, sys->cur.orig,
+                                                           flag);
+    ctx->launches += 3 + (n > 0 ? 2 : 0);
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ CellGrid
+int CellGrid::init(const double box[3], double cut) {
+    release();
+    cutoff = cut;
+    // cell_list.cpp:8-14: n = max(1, floor(L / cutoff)), width = L / n.
+    int dims[3];
+    for (int d = 0; d < 3; ++d) {
+        const double f = std::floor(box[d] / cut);
+        dims[d] = f < 1.0 ? 1 : (f > 1024.0 ? 1024 : static_cast<int>(f));
+        width[d] = box[d] / static_cast<double>(dims[d]);
+    }
+    nx = dims[0];
+    ny = dims[1];
+    nz = dims[2];
+    ncells = nx * ny * nz;
+    usable = nx >= 3 && ny >= 3 && nz >= 3;  // cell_list.cpp:51-53
+    // Morton rank of every cell, so sorted atoms of nearby cells sit nearby in HBM.
+    std::vector<std::pair<uint32_t, int>> keyed(static_cast<size_t>(ncells));
+    for (int c = 0; c < ncells; ++c) {
+        const uint32_t ix = c % nx, iy = (c / nx) % ny, iz = c / (nx * ny);
+        keyed[c] = {spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2), c};
+    }
+    std::sort(keyed.begin(), keyed.end());
+    std::vector<int> rank(static_cast<size_t>(ncells)), cell(static_cast<size_t>(ncells));
+    for (int r = 0; r < ncells; ++r) {
+        cell[r] = keyed[r].second;
+        rank[keyed[r].second] = r;
+    }
+    MDB_CUDA(cudaMalloc(&rank_of_cell, sizeof(int) * ncells));
+    MDB_CUDA(cudaMalloc(&cell_of_rank, sizeof(int) * ncells));
+    MDB_CUDA(cudaMemcpy(rank_of_cell, rank.data(), sizeof(int) * ncells, cudaMemcpyHostToDevice));
+    MDB_CUDA(cudaMemcpy(cell_of_rank, cell.data(), sizeof(int) * ncells, cudaMemcpyHostToDevice));
+    return MD_OK;
+}
+
+void CellGrid::release() {
+    if (rank_of_cell) cudaFree(rank_of_cell);
+    if (cell_of_rank) cudaFree(cell_of_rank);
+    rank_of_cell = cell_of_rank = nullptr;
+}
+
+int cell_sort(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_start) {
+    return cell_sort_gated(sys, grid, d_sorted, d_start, nullptr);
+}
+
+// ---------------------------------------------------------------- Verlet
+static int verlet_alloc(md_verlet* v, md_system* sys) {
+    const int64_t n = sys->n;
+    if (v->n != n || !v->count.ptr) {
+        MDB_TRY(v->count.ensure(sizeof(int) * static_cast<size_t>(n > 0 ? n : 1)));
+        MDB_TRY(v->ref.ensure(sizeof(double4) * static_cast<size_t>(n > 0 ? n : 1)));
+        MDB_TRY(v->perm.ensure(sizeof(int) * static_cast<size_t>(n > 0 ? n : 1)));
+        v->n = n;
+    }
+    if (v->stride == 0) {
+        // Expected full-list neighbours at this density, doubled, plus slack.
+        const double vol = sys->box[0] * sys->box[1] * sys->box[2];
+        const double rl = v->cutoff + v->skin;
+        const double expect = (n / vol) * 4.18879020478639 * rl * rl * rl;
+        int s = static_cast<int>(2.0 * expect) + 48;
+        s = std::min<int64_t>(s, std::max<int64_t>(n, 1));
+        v->stride = (s + 7) & ~7;
+    }
+    MDB_TRY(v->nbr.ensure(sizeof(int) * static_cast<size_t>(n > 0 ? n : 1) * v->stride));
+    return MD_OK;
+}
+
+int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    const Box3 box = make_box(sys);
+    const double rl2 = (v->cutoff + v->skin) * (v->cutoff + v->skin);  // verlet_list.cpp:11
+    MDB_CUDA(cudaMemsetAsync(v->d_max_count, 0, sizeof(int), ctx->stream));
+    if (v->grid.usable) {
+        int* start = v->start.as<int>();
+        MDB_TRY(cell_sort_gated(sys, v->grid, v->perm.as<int>(), start, flag));
+        // Re-sort the system into cell order: permute into alt, copy back, so the
+        // device pointers of the current arrays never change.
+        if (n > 0) {
+            k_permute_gated<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+                sys->cur, sys->alt, v->perm.as<int>(), sys->slot, n, flag);
+            k_copy_atoms<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->alt, sys->cur, n,
+                                                                         flag);
+            ctx->launches += 2;
+        }
+        const GridArgs g = make_args(v->grid, sys);
+        k_verlet_cells<<<grid_for(v->grid.ncells, kBuildWarps), kBuildWarps * 32, 0, ctx->stream>>>(
+            sys->cur.pos, start, g, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
+            ctx->d_status, v->d_max_count, flag);
+        ++ctx->launches;
+    } else if (n > 0) {
+        k_verlet_brute<<<grid_for(n * 32, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, n, box, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
+            ctx->d_status, v->d_max_count, flag);
+        ++ctx->launches;
+    }
+    if (n > 0) {
+        k_store_ref<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, v->ref.as<double4>(), n, flag, flag ? v->d_rebuild_total : nullptr);
+        ++ctx->launches;
+    }
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
+    MDB_TRY(verlet_alloc(v, sys));
+    if (!conditional) {
+        // Host-driven build: retry with a larger stride until no row overflows.
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            MDB_TRY(verlet_build_impl(v, sys, nullptr));
+            int mx = 0;
+            MDB_CUDA(cudaMemcpyAsync(&mx, v->d_max_count, sizeof(int), cudaMemcpyDeviceToHost,
+                                     sys->ctx->stream));
+            MDB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+            if (mx <= v->stride) break;
+            uint32_t st = 0;
+            md_context_status(sys->ctx, &st, 1);  // clear the overflow bit we resolve here
+            v->stride = ((mx + mx / 4 + 16) + 7) & ~7;
+            MDB_TRY(v->nbr.ensure(sizeof(int) * static_cast<size_t>(sys->n) * v->stride));
+            // positions are already sorted; the re-sort below is a no-op permutation
+        }
+        ++v->rebuilds;
+        v->epoch = sys->epoch;
+        v->sys = sys;
+        return MD_OK;
+    }
+    return verlet_build_impl(v, sys, v->d_rebuild_flag);
+}
+
+int verlet_check(md_verlet* v, md_system* sys) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    const int g = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid_for(n, kBlock),
+                                                                      ctx->sm_count * 4)));
+    double* part;
+    MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(g), &part));
+    k_displacement<<<g, kBlock, 0, ctx->stream>>>(sys->cur.pos, v->ref.as<double4>(), n,
+                                                 make_box(sys), v->skin, v->criterion, part,
+                                                 ctx_counter(ctx, 1), v->d_rebuild_flag,
+                                                 ctx_result(ctx, kResTop2));
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+}  // namespace mdb
+
+// --------------------------------------------------------------- pair export
+namespace mdb {
+namespace {
+
+__global__ void k_to_orig(const int* __restrict__ sorted, const int* __restrict__ orig, int* out,
+                          int64_t n) {
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s < n) out[s] = orig[sorted[s]];
+}
+
+__global__ void k_verlet_pair_count(const int* __restrict__ nbr, const int* __restrict__ count,
+                                    const double4* __restrict__ pos, int64_t n, int stride,
+                                    int* out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const double oi = pos[i].w;
+    int c = 0;
+    const int cnt = min(count[i], stride);
+    for (int k = 0; k < cnt; ++k)
+        if (pos[nbr[i * stride + k]].w > oi) ++c;
+    out[i] = c;
+}
+
+__global__ void k_verlet_pair_write(const int* __restrict__ nbr, const int* __restrict__ count,
+                                    const double4* __restrict__ pos, int64_t n, int stride,
+                                    const int64_t* __restrict__ offset, int64_t* pi, int64_t* pj) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const double oi = pos[i].w;
+    int64_t at = offset[i];
+    const int cnt = min(count[i], stride);
+    for (int k = 0; k < cnt; ++k) {
+        const double oj = pos[nbr[i * stride + k]].w;
+        if (oj > oi) {
+            pi[at] = static_cast<int64_t>(oi);
+            pj[at] = static_cast<int64_t>(oj);
+            ++at;
+        }
+    }
+}
+
+// Candidate pairs of a CellList: for each atom (sorted position s) every atom of
+// the 27 neighbouring cells with a larger original index.
+__device__ __forceinline__ int cells_neighbor_rank(const GridArgs& g, int cell, int q) {
+    const int cx = cell % g.nx, cy = (cell / g.nx) % g.ny, cz = cell / (g.nx * g.ny);
+    int jx = cx + (q % 3) - 1, jy = cy + ((q / 3) % 3) - 1, jz = cz + (q / 9) - 1;
+    jx = jx < 0 ? jx + g.nx : (jx >= g.nx ? jx - g.nx : jx);
+    jy = jy < 0 ? jy + g.ny : (jy >= g.ny ? jy - g.ny : jy);
+    jz = jz < 0 ? jz + g.nz : (jz >= g.nz ? jz - g.nz : jz);
+    return g.rank_of_cell[jx + g.nx * (jy + g.ny * jz)];
+}
+
+__global__ void k_cell_pairs(const int* __restrict__ sorted_orig, const int* __restrict__ start,
+                             GridArgs g, int64_t n, const int64_t* __restrict__ offset, int* counts,
+                             int64_t* pi, int64_t* pj) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.ncells) return;
+    const int cell = g.cell_of_rank[r];
+    int64_t at = offset ? offset[r] : 0;
+    int64_t c = 0;
+    for (int s = start[r]; s < start[r + 1]; ++s) {
+        const int oi = sorted_orig[s];
+        for (int q = 0; q < 27; ++q) {
+            const int rr = cells_neighbor_rank(g, cell, q);
+            for (int t = start[rr]; t < start[rr + 1]; ++t) {
+                const int oj = sorted_orig[t];
+                if (oj > oi) {
+                    if (pi) {
+                        pi[at] = oi;
+                        pj[at] = oj;
+                        ++at;
+                    }
+                    ++c;
+                }
+            }
+        }
+    }
+    if (counts) counts[r] = static_cast<int>(c);
+}
+
+int exclusive_offsets(const std::vector<int>& counts, std::vector<int64_t>& off) {
+    off.resize(counts.size() + 1);
+    int64_t acc = 0;
+    for (size_t k = 0; k < counts.size(); ++k) {
+        off[k] = acc;
+        acc += counts[k];
+    }
+    off[counts.size()] = acc;
+    return MD_OK;
+}
+
+}  // namespace
+}  // namespace mdb
+
+using namespace mdb;
+
+namespace {
+
+int check_box_match(const double a[3], const md_system* sys, const char* who) {
+    for (int d = 0; d < 3; ++d)
+        if (a[d] != sys->box[d])
+            return fail(MD_ERR_INVALID_ARGUMENT, "%s: box differs from the system's box", who);
+    return MD_OK;
+}
+
+int verlet_ready(md_verlet* v, md_system* sys, const char* who) {
+    if (!v->sys) return fail(MD_ERR_INVALID_ARGUMENT, "%s: Verlet list was never built", who);
+    if (v->sys != sys || v->n != sys->n)
+        return fail(MD_ERR_INVALID_ARGUMENT, "%s: Verlet list was built for another system", who);
+    if (v->epoch != sys->epoch)
+        return fail(MD_ERR_INVALID_ARGUMENT, "%s: system was re-sorted since this list was built",
+                    who);
+    return MD_OK;
+}
+
+}  // namespace
+
+namespace mdb {
+int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who) {
+    return verlet_ready(v, sys, who);
+}
+}  // namespace mdb
+
+extern "C" {
+
+// ------------------------------------------------------------------ CellList
+int md_cells_create(md_context* ctx, const double box[3], double cutoff, md_cells** out) {
+    if (!ctx || !box || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_create: NULL argument");
+    if (!(cutoff > 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_create: cutoff must be > 0");
+    md_cells* c = new (std::nothrow) md_cells();
+    if (!c) return fail(MD_ERR_OUT_OF_MEMORY, "md_cells_create: host allocation");
+    c->ctx = ctx;
+    for (int d = 0; d < 3; ++d) c->box[d] = box[d];
+    const int rc = c->grid.init(box, cutoff);
+    if (rc != MD_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return MD_OK;
+}
+
+int md_cells_destroy(md_cells* c) {
+    if (!c) return MD_OK;
+    c->grid.release();
+    c->sorted_orig.release();
+    c->start.release();
+    delete c;
+    return MD_OK;
+}
+
+int md_cells_dims(const md_cells* c, int dims[3]) {
+    if (!c || !dims) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_dims: NULL argument");
+    dims[0] = c->grid.nx;
+    dims[1] = c->grid.ny;
+    dims[2] = c->grid.nz;
+    return MD_OK;
+}
+
+int md_cells_usable(const md_cells* c) { return c && c->grid.usable ? 1 : 0; }
+
+
+int md_cells_build(md_cells* c, md_system* sys) {
+    if (!c || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_build: NULL argument");
+    MDB_TRY(check_box_match(c->box, sys, "md_cells_build"));
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    MDB_TRY(c->sorted_orig.ensure(sizeof(int) * static_cast<size_t>(2 * (n > 0 ? n : 1))));
+    MDB_TRY(c->start.ensure(sizeof(int) * static_cast<size_t>(c->grid.ncells + 1)));
+    int* sorted = c->sorted_orig.as<int>() + (n > 0 ? n : 1);  // second half: device slots
+    MDB_TRY(cell_sort(sys, c->grid, sorted, c->start.as<int>()));
+    if (n > 0) {
+        k_to_orig<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sorted, sys->cur.orig,
+                                                                   c->sorted_orig.as<int>(), n);
+        ++ctx->launches;
+        MDB_CHECK_LAUNCH();
+    }
+    c->sys = sys;
+    c->n = n;
+    c->built = true;
+    return MD_OK;
+}
+
+// ---------------------------------------------------------------- VerletList
+int md_verlet_create(md_context* ctx, const double box[3], double cutoff, double skin,
+                     md_verlet** out) {
+    if (!ctx || !box || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_create: NULL argument");
+    if (!(cutoff > 0.0) || !(skin >= 0.0))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_create: cutoff must be > 0 and skin >= 0");
+    md_verlet* v = new (std::nothrow) md_verlet();
+    if (!v) return fail(MD_ERR_OUT_OF_MEMORY, "md_verlet_create: host allocation");
+    v->ctx = ctx;
+    for (int d = 0; d < 3; ++d) v->box[d] = box[d];
+    v->cutoff = cutoff;
+    v->skin = skin;
+    int rc = v->grid.init(box, cutoff + skin);  // verlet_list.cpp:6: CellList at rc+skin
+    if (rc == MD_OK) rc = v->start.ensure(sizeof(int) * static_cast<size_t>(v->grid.ncells + 1));
+    if (rc == MD_OK) {
+        int* flags = nullptr;
+        if (cudaMalloc(&flags, 4 * sizeof(int)) != cudaSuccess ||
+            cudaMemset(flags, 0, 4 * sizeof(int)) != cudaSuccess) {
+            rc = fail(MD_ERR_OUT_OF_MEMORY, "md_verlet_create: device flags");
+        } else {
+            v->d_rebuild_flag = flags;
+            v->d_rebuild_total = flags + 1;
+            v->d_max_count = flags + 2;
+        }
+    }
+    if (rc != MD_OK) {
+        md_verlet_destroy(v);
+        return rc;
+    }
+    *out = v;
+    return MD_OK;
+}
+
+int md_verlet_destroy(md_verlet* v) {
+    if (!v) return MD_OK;
+    if (v->ctx) cudaStreamSynchronize(v->ctx->stream);
+    v->grid.release();
+    v->start.release();
+    v->perm.release();
+    v->nbr.release();
+    v->count.release();
+    v->ref.release();
+    if (v->d_rebuild_flag) cudaFree(v->d_rebuild_flag);
+    delete v;
+    return MD_OK;
+}
+
+int md_verlet_build(md_verlet* v, md_system* sys) {
+    if (!v || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_build: NULL argument");
+    MDB_TRY(check_box_match(v->box, sys, "md_verlet_build"));
+    return verlet_build(v, sys, false);
+}
+
+int md_verlet_needs_rebuild(md_verlet* v, md_system* sys, int* flag) {
+    if (!v || !sys || !flag) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_needs_rebuild: NULL");
+    MDB_TRY(verlet_ready(v, sys, "md_verlet_needs_rebuild"));
+    MDB_TRY(verlet_check(v, sys));
+    int f = 0;
+    MDB_CUDA(cudaMemcpyAsync(&f, v->d_rebuild_flag, sizeof(int), cudaMemcpyDeviceToHost,
+                             sys->ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+    *flag = f;
+    return MD_OK;
+}
+
+int md_verlet_rebuild_if_needed(md_verlet* v, md_system* sys, int* rebuilt) {
+    int f = 0;
+    MDB_TRY(md_verlet_needs_rebuild(v, sys, &f));
+    if (f) MDB_TRY(verlet_build(v, sys, false));
+    if (rebuilt) *rebuilt = f;
+    return MD_OK;
+}
+
+int md_verlet_rebuild_count(md_verlet* v, int64_t* count) {
+    if (!v || !count) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_rebuild_count: NULL");
+    int dev = 0;
+    MDB_CUDA(cudaMemcpyAsync(&dev, v->d_rebuild_total, sizeof(int), cudaMemcpyDeviceToHost,
+                             v->ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(v->ctx->stream));
+    *count = v->rebuilds + dev;
+    return MD_OK;
+}
+
+int md_verlet_set_criterion(md_verlet* v, int criterion) {
+    if (!v || (criterion != 0 && criterion != 1))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_criterion: criterion must be 0 or 1");
+    v->criterion = criterion;
+    return MD_OK;
+}
+
+int md_verlet_displacements(md_verlet* v, md_system* sys, double* largest, double* second) {
+    if (!v || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_displacements: NULL");
+    MDB_TRY(verlet_ready(v, sys, "md_verlet_displacements"));
+    MDB_TRY(verlet_check(v, sys));
+    double r[2];
+    MDB_TRY(ctx_read_results(sys->ctx, kResTop2, 2, r));
+    if (largest) *largest = r[0];
+    if (second) *second = r[1];
+    return MD_OK;
+}
+
+}  // extern "C"
+
+
+extern "C" {
+
+int md_verlet_pairs(md_verlet* v, int64_t* pi, int64_t* pj, int64_t cap, int64_t* count) {
+    if (!v || !count) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_pairs: NULL argument");
+    md_system* sys = v->sys;
+    if (!sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_pairs: list was never built");
+    MDB_TRY(verlet_ready(v, sys, "md_verlet_pairs"));
+    md_context* ctx = v->ctx;
+    const int64_t n = sys->n;
+    if (n == 0) {
+        *count = 0;
+        return MD_OK;
+    }
+    DevBuf cnt;
+    MDB_TRY(cnt.ensure(sizeof(int) * n));
+    k_verlet_pair_count<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+        v->nbr.as<int>(), v->count.as<int>(), sys->cur.pos, n, v->stride, cnt.as<int>());
+    ++ctx->launches;
+    std::vector<int> hc(static_cast<size_t>(n));
+    MDB_CUDA(cudaMemcpyAsync(hc.data(), cnt.ptr, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<int64_t> off;
+    exclusive_offsets(hc, off);
+    const int64_t total = off[n];
+    *count = total;
+    if (pi && pj && cap >= total && total > 0) {
+        DevBuf doff, dpi, dpj;
+        MDB_TRY(doff.ensure(sizeof(int64_t) * (n + 1)));
+        MDB_TRY(dpi.ensure(sizeof(int64_t) * total));
+        MDB_TRY(dpj.ensure(sizeof(int64_t) * total));
+        MDB_CUDA(cudaMemcpyAsync(doff.ptr, off.data(), sizeof(int64_t) * (n + 1),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+        k_verlet_pair_write<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+            v->nbr.as<int>(), v->count.as<int>(), sys->cur.pos, n, v->stride, doff.as<int64_t>(),
+            dpi.as<int64_t>(), dpj.as<int64_t>());
+        ++ctx->launches;
+        MDB_CUDA(cudaMemcpyAsync(pi, dpi.ptr, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, ctx->stream));
+        MDB_CUDA(cudaMemcpyAsync(pj, dpj.ptr, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, ctx->stream));
+        MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+        doff.release();
+        dpi.release();
+        dpj.release();
+        // sort by (i, j) on the host for a canonical export order
+        std::vector<std::pair<int64_t, int64_t>> pr(static_cast<size_t>(total));
+        for (int64_t k = 0; k < total; ++k) pr[k] = {pi[k], pj[k]};
+        std::sort(pr.begin(), pr.end());
+        for (int64_t k = 0; k < total; ++k) {
+            pi[k] = pr[k].first;
+            pj[k] = pr[k].second;
+        }
+    }
+    cnt.release();
+    return ctx_check_status(ctx);
+}
+
+int md_cells_pairs(md_cells* c, int64_t* pi, int64_t* pj, int64_t cap, int64_t* count) {
+    if (!c || !count) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_pairs: NULL argument");
+    if (!c->built) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_pairs: cell list was never built");
+    if (!c->grid.usable)
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "md_cells_pairs: CellList is not usable (fewer than 3 cells per side)");
+    md_context* ctx = c->ctx;
+    const int m = c->grid.ncells;
+    GridArgs g = make_args(c->grid, c->sys);
+    DevBuf cnt;
+    MDB_TRY(cnt.ensure(sizeof(int) * m));
+    k_cell_pairs<<<grid_for(m, 64), 64, 0, ctx->stream>>>(c->sorted_orig.as<int>(),
+                                                         c->start.as<int>(), g, c->n, nullptr,
+                                                         cnt.as<int>(), nullptr, nullptr);
+    ++ctx->launches;
+    std::vector<int> hc(static_cast<size_t>(m));
+    MDB_CUDA(cudaMemcpyAsync(hc.data(), cnt.ptr, sizeof(int) * m, cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<int64_t> off;
+    exclusive_offsets(hc, off);
+    const int64_t total = off[m];
+    *count = total;
+    if (pi && pj && cap >= total && total > 0) {
+        DevBuf doff, dpi, dpj;
+        MDB_TRY(doff.ensure(sizeof(int64_t) * (m + 1)));
+        MDB_TRY(dpi.ensure(sizeof(int64_t) * total));
+        MDB_TRY(dpj.ensure(sizeof(int64_t) * total));
+        MDB_CUDA(cudaMemcpyAsync(doff.ptr, off.data(), sizeof(int64_t) * (m + 1),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+        k_cell_pairs<<<grid_for(m, 64), 64, 0, ctx->stream>>>(
+            c->sorted_orig.as<int>(), c->start.as<int>(), g, c->n, doff.as<int64_t>(), nullptr,
+            dpi.as<int64_t>(), dpj.as<int64_t>());
+        ++ctx->launches;
+        MDB_CUDA(cudaMemcpyAsync(pi, dpi.ptr, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, ctx->stream));
+        MDB_CUDA(cudaMemcpyAsync(pj, dpj.ptr, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, ctx->stream));
+        MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+        doff.release();
+        dpi.release();
+        dpj.release();
+    }
+    cnt.release();
+    return ctx_check_status(ctx);
+}
+
+}  // extern "C"

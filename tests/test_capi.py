@@ -1,0 +1,61 @@
+"""CPU-only checks of the C ABI boundary: the library loads without a GPU and
+exports every entry point include/moldyn_b200.h declares; host-side setup code
+(md_fcc_lattice) reproduces the reference's lattice bit-for-bit."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from conftest import ROOT, load_golden
+
+HEADER = os.path.join(ROOT, "include", "moldyn_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(md_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    syms = declared_symbols()
+    for required in ("md_context_create", "md_system_create", "md_verlet_build",
+                     "md_lj_forces_verlet", "md_run_lj", "md_integrator_create_nhc"):
+        assert required in syms
+
+
+def test_library_exports_every_declared_symbol():
+    import moleculardynamics_b200 as md
+    lib = C.CDLL(md.library_path())
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_library_hides_internal_symbols():
+    # only md_* entry points are visible; kernels and helpers stay hidden
+    out = os.popen(f"nm -D --defined-only {__import__('moleculardynamics_b200').library_path()}").read()
+    exported = [l.split()[-1] for l in out.splitlines() if " T " in l]
+    assert exported and all(s.startswith("md_") for s in exported), exported[:10]
+
+
+def test_lattice_setup_bit_exact_on_host():
+    import moleculardynamics_b200 as md
+    fcc = load_golden("fcc_lj.npz")
+    st = md.fcc_lattice(6, 0.8442, 0.722, 1)
+    assert np.array_equal(st["pos"], fcc["c6_pos"])
+    assert np.array_equal(st["vel"], fcc["c6_vel"])
+    assert np.array_equal(st["box"], fcc["c6_box"])
+    st = md.fcc_lattice(3, 0.80, 1.0, 12345)
+    assert np.array_equal(st["pos"], fcc["c3_pos"])
+
+
+def test_invalid_arguments_map_to_reference_exceptions():
+    import moleculardynamics_b200 as md
+    import pytest
+    with pytest.raises(md.InvalidArgument):
+        md.LennardJones(1.0, 1.0, 2.5, truncation=7)
+    h = C.c_void_p()
+    rc = md.lib().md_integrator_create_nhc(0.002, 1.0, 0.5, 0, 10, C.byref(h))
+    assert rc == md.MD_ERR_INVALID_ARGUMENT
+    assert b"chainLength" in md.lib().md_last_error()

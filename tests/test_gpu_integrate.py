@@ -1,0 +1,263 @@
+"""GPU parity of the integrators: velocity-Verlet, BAOAB and the Nose-Hoover chain
+(the reference's tests/test_integrator.cpp and test_thermostat.cpp), plus
+step-level shadow parity against the oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+FCC = load_golden("fcc_lj.npz")
+
+
+def approx_eq(a, b, eps):
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    return np.all(np.abs(a - b) < eps * (1.0 + np.maximum(np.abs(a), np.abs(b))))
+
+
+def lattice_system(md, cells, rho, temp, seed):
+    st = md.fcc_lattice(cells, rho, temp, seed)
+    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"])
+    return s, st
+
+
+def test_vv_one_step_bit_exact_from_same_forces(md):
+    """One VV step from identical state and forces reproduces the oracle's
+    positions exactly (fma kick, fma drift, bit-exact wrap)."""
+    s, st = lattice_system(md, 6, 0.8442, 0.722, 1)
+    lj = md.LennardJones(1.0, 1.0, 2.5)
+    lj.compute_forces(s)
+    f0 = s.forces
+    integ = md.VelocityVerlet(0.005)
+    pre = {}
+
+    def forces(sys_):
+        pre["pos"] = sys_.positions
+        pre["vel"] = sys_.velocities
+        return lj.compute_forces(sys_)[0]
+
+    integ.step(s, forces)
+    # oracle: same kick and drift from the same (pos, vel, f0)
+    n = len(st["mass"])
+    vx, vy, vz = (np.ascontiguousarray(st["vel"][:, k]) for k in range(3))
+    fx, fy, fz = (np.ascontiguousarray(f0[:, k]) for k in range(3))
+    x, y, z = (np.ascontiguousarray(st["pos"][:, k]) for k in range(3))
+    L = O.lib()
+    L.orc_half_kick(n, 0.005, O._p(st["mass"]), O._p(fx), O._p(fy), O._p(fz), O._p(vx), O._p(vy),
+                    O._p(vz))
+    L.orc_drift_wrap(n, O._p(st["box"]), 0.005, O._p(vx), O._p(vy), O._p(vz), O._p(x), O._p(y),
+                     O._p(z))
+    assert np.array_equal(pre["pos"], np.stack([x, y, z], 1))
+    assert np.array_equal(pre["vel"], np.stack([vx, vy, vz], 1))
+
+
+def test_vv_trajectory_shadow_parity(md):
+    """25 steps of the N=864 drop-in configuration (moldyn_run ForceFn): each
+    step's forces/energy/virial match the oracle evaluated on the GPU's state."""
+    s, st = lattice_system(md, 6, 0.8442, 0.722, 1)
+    lj = md.LennardJones(1.0, 1.0, 2.5)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.VelocityVerlet(0.005)
+
+    def forces(sys_):
+        v.rebuild_if_needed(sys_)
+        return lj.compute_forces(sys_, v)[0]
+
+    for _ in range(25):
+        integ.step(s, forces)
+        pos = s.positions
+        fo, eo, wo = O.lj_compute(pos, st["box"], rc=2.5, trunc=0)
+        e, w = s.last_energy_virial()
+        assert approx_eq(e, eo, 1e-12) and approx_eq(w, wo, 1e-12)
+        assert approx_eq(s.forces, fo, 1e-12)
+    # and the trajectory stays on the reference's to round-off after 25 steps
+    assert np.max(np.abs(s.positions - FCC["vv25_pos"])) < 1e-9
+    assert np.max(np.abs(s.velocities - FCC["vv25_vel"])) < 1e-9
+    assert v.rebuild_count() == int(FCC["vv25_info"][2])
+
+
+def test_fused_run_equals_host_loop(md):
+    """md_run_lj (device-decided rebuilds, no per-step sync) == host-driven steps."""
+    outs = []
+    for fused in (False, True):
+        s, st = lattice_system(md, 5, 0.8442, 0.722, 3)
+        lj = md.LennardJones(1.0, 1.0, 2.5)
+        v = md.VerletList(st["box"], 2.5, 0.3)
+        v.build(s)
+        lj.compute_forces(s, v)
+        integ = md.VelocityVerlet(0.005)
+        if fused:
+            th = integ.run(s, v, lj, 60, thermo=True)
+            assert th.shape == (60, 4)
+        else:
+            def forces(sys_):
+                v.rebuild_if_needed(sys_)
+                return lj.compute_forces(sys_, v)[0]
+            for _ in range(60):
+                integ.step(s, forces)
+        outs.append((s.positions, s.velocities, v.rebuild_count()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+
+
+def energy_error_slope(md, use_run):
+    dts = [0.001, 0.002, 0.004, 0.008]
+    log_dt, log_err = [], []
+    for dt in dts:
+        s, st = lattice_system(md, 3, 0.80, 1.0, 12345)
+        lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+        integ = md.VelocityVerlet(dt)
+        pe, _ = lj.compute_forces(s)
+        e0 = pe + s.kinetic_energy()
+        steps = int(round(1.0 / dt))
+        max_dev = 0.0
+        for _ in range(steps):
+            integ.step(s, lambda q: lj.compute_forces(q)[0])
+            pe, _ = lj.compute_forces(s)
+            max_dev = max(max_dev, abs(pe + s.kinetic_energy() - e0))
+        log_dt.append(np.log(dt))
+        log_err.append(np.log(max_dev / abs(e0)))
+    return np.polyfit(log_dt, log_err, 1)[0]
+
+
+def test_vv_energy_error_scales_as_dt_squared(md):
+    """tests/test_integrator.cpp:10-50"""
+    slope = energy_error_slope(md, False)
+    assert 1.85 < slope < 2.15, slope
+
+
+def test_vv_time_reversible(md):
+    """tests/test_integrator.cpp:52-83"""
+    s, st = lattice_system(md, 3, 0.80, 1.0, 999)
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    integ = md.VelocityVerlet(0.002)
+    start = s.positions
+    lj.compute_forces(s)
+    for _ in range(200):
+        integ.step(s, lambda q: lj.compute_forces(q)[0])
+    s.velocities = -s.velocities
+    for _ in range(200):
+        integ.step(s, lambda q: lj.compute_forces(q)[0])
+    d = s.positions - start
+    L = st["box"]
+    d -= L * np.floor(d / L + 0.5)
+    assert np.max(np.linalg.norm(d, axis=1)) < 1e-8
+
+
+def test_baoab_replayed_noise_matches_oracle(md):
+    """BAOAB with the reference's own mt19937_64 normals replayed: the GPU
+    trajectory tracks the oracle's to round-off."""
+    cells, rho, temp = 3, 0.80, 1.0
+    s, st = lattice_system(md, cells, rho, temp, 42)
+    n = len(st["mass"])
+    steps = 20
+    xi = O.rng_normals(777, 3 * n * steps)
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.LangevinBAOAB(0.005, 1.0, temp, 777)
+    integ.set_noise(xi)
+
+    def forces(sys_):
+        v.rebuild_if_needed(sys_)
+        return lj.compute_forces(sys_, v)[0]
+
+    for _ in range(steps):
+        integ.step(s, forces)
+    sim = O.Sim(st["pos"], st["vel"], st["mass"], st["box"], rc=2.5, trunc=1, skin=0.3, dt=0.005)
+    sim.set_langevin(1.0, temp, 777)
+    sim.prime()
+    sim.run("baoab", steps)
+    p, vel, f = sim.state()
+    assert np.max(np.abs(s.positions - p)) < 1e-10
+    assert np.max(np.abs(s.velocities - vel)) < 1e-10
+
+
+def test_baoab_equipartition(md):
+    """tests/test_thermostat.cpp:41-96 (Philox noise; statistical parity)."""
+    s, st = lattice_system(md, 3, 0.80, 1.0, 42)
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.LangevinBAOAB(0.005, 1.0, 1.0, 777)
+    integ.run(s, v, lj, 3000)
+    th = integ.run(s, v, lj, 10000, thermo=True)
+    dof = 3 * s.n
+    mean_t = np.mean(2.0 * th[:, 2] / dof)
+    assert 0.98 < mean_t < 1.02, mean_t
+
+
+def test_nhc_matches_oracle_short(md):
+    """A few NHC steps track the oracle's (analytic KE*s^2 vs re-summed KE only
+    changes rounding)."""
+    s, st = lattice_system(md, 3, 0.80, 3.0, 55)
+    n = len(st["mass"])
+    dof = 3 * n - 3
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.NoseHooverChain(0.002, 1.0, 0.5, 3, dof)
+
+    def forces(sys_):
+        v.rebuild_if_needed(sys_)
+        return lj.compute_forces(sys_, v)[0]
+
+    for _ in range(30):
+        integ.step(s, forces)
+    sim = O.Sim(st["pos"], st["vel"], st["mass"], st["box"], rc=2.5, trunc=1, skin=0.3, dt=0.002)
+    sim.set_nhc(1.0, 0.5, 3, dof)
+    sim.prime()
+    sim.run("nhc", 30)
+    p, vel, _ = sim.state()
+    assert np.max(np.abs(s.positions - p)) < 1e-10
+    assert np.max(np.abs(s.velocities - vel)) < 1e-10
+    assert abs(integ.conserved_quantity_contribution() - sim.nhc_conserved) < 1e-9
+
+
+def test_nhc_conserves_extended_hamiltonian(md):
+    """tests/test_thermostat.cpp:222-263 (20,000 steps, max relative drift < 1e-3)."""
+    s, st = lattice_system(md, 3, 0.80, 1.0, 56)
+    dof = 3 * s.n - 3
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    pe, _ = lj.compute_forces(s, v)
+    integ = md.NoseHooverChain(0.002, 1.0, 0.5, 3, dof)
+    h0 = pe + s.kinetic_energy() + integ.conserved_quantity_contribution()
+    th = integ.run(s, v, lj, 20000, thermo=True)
+    h = th[:, 0] + th[:, 2] + th[:, 3]
+    drift = np.max(np.abs(h - h0)) / abs(h0)
+    assert drift < 1e-3, drift
+    mean_t = np.mean(2.0 * th[6000:, 2] / dof)
+    assert 0.9 < mean_t < 1.1
+
+
+def test_mixed_precision_force_error(md):
+    """Mixed path: force RMS error against FP64 on identical states."""
+    s, st = lattice_system(md, 8, 0.8442, 0.722, 5)
+    lj64 = md.LennardJones(1.0, 1.0, 2.5)
+    ljmx = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    # melt the lattice a little so forces are non-trivial
+    integ = md.LangevinBAOAB(0.005, 1.0, 0.722, 9)
+    lj64.compute_forces(s, v)
+    integ.run(s, v, lj64, 200)
+    e64, w64 = lj64.compute_forces(s, v)
+    f64 = s.forces
+    emx, wmx = ljmx.compute_forces(s, v)
+    fmx = s.forces
+    rms = np.sqrt(np.sum((fmx - f64) ** 2) / np.sum(f64 ** 2))
+    assert rms < 1e-6, rms
+    assert abs(emx - e64) < 1e-6 * abs(e64)
+    assert abs(wmx - w64) < 1e-5 * abs(w64)
