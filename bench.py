@@ -1,0 +1,495 @@
+"""Benchmark: atom-steps/s of the 1,048,576-atom Lennard-Jones NVE step on one B200,
+mixed precision vs FP64 (BASELINE metric), with the reference CPU path beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (per GPU): fcc 64^3 lattice (N = 1,048,576), rho* = 0.8442, T* = 0.722,
+rc = 2.5 sigma (truncated), skin 0.3 sigma, dt* = 0.005; seeded Maxwell-Boltzmann
+velocities, equilibrated by BAOAB Langevin (gamma* = 1) before timing, then NVE
+velocity-Verlet steps with device-decided Verlet rebuilds.  One "step" = one
+velocity-Verlet step over the whole system (kick+drift, displacement check and
+any rebuild, LJ forces, kick).  The per-step working set (positions, velocities,
+forces, neighbour rows ~ 0.4 GB) exceeds the 126 MB L2, so no L2 flush is used.
+
+Multi-GPU: the path has no exchange step, so N GPUs run N independent replicas
+(weak scaling); value = total atom-steps/s over ranks, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s, 1M-atom LJ: mixed vs FP64 on 1 B200 at stated force error"
+UNIT = "atom-steps/s"
+CELLS = 64
+RHO, TEMP, RC, SKIN, DT = 0.8442, 0.722, 2.5, 0.3, 0.005
+SEED = 2026
+
+
+def config(equil):
+    return {
+        "workload": "1M-atom LJ NVE velocity-Verlet: fcc 64^3 (N=1048576), rho*=0.8442, "
+                    "T*=0.722, rc=2.5 truncated, skin=0.3, dt*=0.005",
+        "n_atoms": 4 * CELLS ** 3,
+        "equilibration": f"{equil} BAOAB steps (gamma*=1) from the seeded lattice",
+        "neighbour": "Verlet list rebuilt on device when the two largest displacements "
+                     "exceed the skin (reference criterion)",
+        "l2_policy": "no flush: per-step working set ~0.4 GB > 126 MB L2",
+        "parallelism": "replicas (one independent system per GPU)",
+    }
+
+
+# ----------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        load = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------- ranks
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Group:
+    """Host-side barrier and max/sum over ranks (plumbing only: replicas exchange
+    no simulation data)."""
+
+    def __init__(self, world):
+        self.world = world
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def reduce(self, value, op):
+        if not self.dist:
+            return value
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX if op == "max" else self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------- GPU arm
+def traffic_per_atom():
+    """DRAM bytes per atom of one mixed LJ force launch, from the committed ncu
+    summary (profiles/lj_force_mixed.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "lj_force_mixed.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_atom:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def equilibrated_state(md, ctx, equil):
+    st = md.fcc_lattice(CELLS, RHO, TEMP, SEED)
+    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"], ctx=ctx)
+    lj = md.LennardJones(1.0, 1.0, RC)
+    v = md.VerletList(st["box"], RC, SKIN, ctx=ctx)
+    v.build(s)
+    lj.compute_forces(s, v)
+    if equil > 0:
+        md.LangevinBAOAB(DT, 1.0, TEMP, SEED + 1).run(s, v, lj, equil)
+    s.remove_center_of_mass_motion()
+    lj.compute_forces(s, v)
+    return st["box"], s.positions, s.velocities, s.forces
+
+
+def timed_run(md, ctx, box, pos, vel, frc, precision, steps, warmup, group, clocks=None):
+    """W warm-up + K timed fused VV steps from the given state.  Returns
+    (device ms for K steps (max over ranks), thermo rows, force-kernel ms per launch,
+    launches in the timed region, neighbour entries per atom, rebuilds)."""
+    s = md.System.from_arrays(pos, box, vel=vel, ctx=ctx)
+    s.forces = frc
+    lj = md.LennardJones(1.0, 1.0, RC, precision=precision)
+    v = md.VerletList(box, RC, SKIN, ctx=ctx)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.VelocityVerlet(DT)
+    if warmup > 0:
+        integ.run(s, v, lj, warmup)
+    L = md.lib()
+    ctx.synchronize()
+    group.barrier()
+    launches0 = ctx.launch_count()
+    rebuild0 = v.rebuild_count()
+    _check = md._check
+    _check(L.md_context_set_timing(ctx.handle, 1))
+    L.md_context_kernel_time(ctx.handle, md.MD_KERNEL_LJ_FORCE, 1, None, None)
+    sampler = clocks.__enter__() if clocks else None
+    _check(L.md_context_span_begin(ctx.handle))
+    rows = integ.run(s, v, lj, steps, thermo=True)
+    ms = C.c_double()
+    _check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+    if sampler:
+        clocks.__exit__(None, None, None)
+    kms = C.c_double()
+    kl = C.c_int64()
+    _check(L.md_context_kernel_time(ctx.handle, md.MD_KERNEL_LJ_FORCE, 1, C.byref(kms), C.byref(kl)))
+    _check(L.md_context_set_timing(ctx.handle, 0))
+    ctx.synchronize()
+    group.barrier()
+    launches = ctx.launch_count() - launches0
+    pairs = v.pairs()
+    nbr_per_atom = 2.0 * len(pairs) / s.n
+    rebuilds = v.rebuild_count() - rebuild0
+    dev_ms = group.reduce(ms.value, "max")
+    per_launch = kms.value / max(kl.value, 1)
+    return dev_ms, rows, per_launch, launches, nbr_per_atom, rebuilds
+
+
+def e2e_run(md, ctx, box, pos, vel, frc, steps, group):
+    """The same steps through the public C ABI with host state: every step uploads
+    the state from pinned host memory, runs one step and reads back the state and
+    its thermo row.  Returns (wall seconds, max over ranks; h2d bytes/step; d2h)."""
+    n = pos.shape[0]
+    L = md.lib()
+    s = md.System(n, box, ctx=ctx)
+    s.masses = np.ones(n)
+    lj = md.LennardJones(1.0, 1.0, RC, precision=md.PRECISION_MIXED)
+    v = md.VerletList(box, RC, SKIN, ctx=ctx)
+    integ = md.VelocityVerlet(DT)
+    # pinned host buffers for the 9 state columns
+    L.md_host_alloc.restype = C.c_void_p
+    L.md_host_alloc.argtypes = [C.c_size_t]
+    L.md_host_free.argtypes = [C.c_void_p]
+    nbytes = n * 8
+    ptrs = [L.md_host_alloc(nbytes) for _ in range(9)]
+    if not all(ptrs):
+        raise MemoryError("md_host_alloc failed")
+    cols = [np.ctypeslib.as_array((C.c_double * n).from_address(p)) for p in ptrs]
+    for k in range(3):
+        cols[k][:] = pos[:, k]
+        cols[3 + k][:] = vel[:, k]
+        cols[6 + k][:] = frc[:, k]
+    thermo = np.zeros(4)
+    dp = C.POINTER(C.c_double)
+
+    def step():
+        for f in range(9):
+            md._check(L.md_system_set(s.handle, f, C.cast(ptrs[f], dp)))
+        md._check(L.md_run_lj(integ.handle, s.handle, v.handle, lj.handle, 1,
+                              thermo.ctypes.data_as(dp)))
+        for f in range(9):
+            md._check(L.md_system_get(s.handle, f, C.cast(ptrs[f], dp)))
+
+    # the list is built once from the uploaded state (rebuilds happen on device)
+    for f in range(9):
+        md._check(L.md_system_set(s.handle, f, C.cast(ptrs[f], dp)))
+    v.build(s)
+    for _ in range(2):
+        step()
+    ctx.synchronize()
+    group.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    t1 = time.perf_counter()
+    group.barrier()
+    for p in ptrs:
+        L.md_host_free(p)
+    return group.reduce(t1 - t0, "max"), 9 * nbytes, 9 * nbytes + thermo.nbytes
+
+
+# ----------------------------------------------------------------------- CPU legs
+def _ref_worker(args):
+    """One single-threaded reference process: moldyn_run's VV loop on its own
+    1M-atom system for `steps` steps; returns seconds of the stepping loop."""
+    pos, vel, box, steps = args
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    R = O.ref()
+    kind = "reference"
+    n = pos.shape[0]
+    st = [np.ascontiguousarray(pos[:, k]) for k in range(3)] + \
+         [np.ascontiguousarray(vel[:, k]) for k in range(3)] + [np.zeros(n) for _ in range(3)]
+    info = np.zeros(5)
+    if R is not None:
+        R.ref_run(0, n, O._p(np.ascontiguousarray(box)), *[O._p(a) for a in st],
+                  O._p(np.ones(n)), 1.0, 1.0, RC, 0, SKIN, DT, steps, 0.0, 0.0, 0, 0.0, 1, 0,
+                  O._p(info))
+        return kind, info[4]
+    kind = "port"
+    sim = O.Sim(pos, vel, np.ones(n), box, rc=RC, trunc=0, skin=SKIN, dt=DT)
+    sim.prime()
+    t0 = time.perf_counter()
+    sim.run("vv", steps)
+    return kind, time.perf_counter() - t0
+
+
+def cpu_reference(pos, vel, box, steps, procs):
+    n = pos.shape[0]
+    if procs <= 1:
+        kind, sec = _ref_worker((pos, vel, box, steps))
+        rates = [n * steps / sec]
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_ref_worker, [(pos, vel, box, steps)] * procs)
+        kind = res[0][0]
+        rates = [n * steps / sec for _, sec in res]
+    return kind, float(sum(rates)), rates
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def lattice_state():
+    """The seeded fcc 64^3 lattice (host setup, bit-identical to the reference's)."""
+    import oracle as O
+    st = O.fcc_lattice(CELLS, RHO, TEMP, SEED)
+    return st["pos"], st["vel"], st["box"]
+
+
+# ----------------------------------------------------------------------- main
+def run_reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, args.ref_steps))
+    procs = max(1, min(os.cpu_count() or 1, args.ref_procs))
+    pos, vel, box = lattice_state()
+    kind, value, rates = cpu_reference(pos, vel, box, steps, procs)
+    ms = 1e3 * 4 * CELLS ** 3 * procs / value
+    sample = (f"{procs} concurrent single-threaded reference processes, each its own "
+              f"{4 * CELLS ** 3}-atom system from the seeded lattice, {steps} NVE VV steps "
+              f"after its first Verlet build ({cpu_model()})")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fcc lattice)",
+        "config": config(0), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
+                         "sample": sample, "per_process": rates},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu_arm(args):
+    world, rank, local = dist_env()
+    group = Group(world)
+    import moleculardynamics_b200 as md
+    ctx = md.Context(local)
+    md.set_threads_per_atom(args.tpa)
+    md.set_unroll(args.unroll)
+    n = 4 * CELLS ** 3
+    box, pos, vel, frc = equilibrated_state(md, ctx, args.equil)
+    # identical starting state for both precisions
+    clocks = ClockSampler(local)
+    if args.precision == "mixed":
+        # profiling configuration: the mixed path alone
+        timed_run(md, ctx, box, pos, vel, frc, md.PRECISION_MIXED, args.steps, args.warmup, group)
+        group.close()
+        return 0
+    ms64, rows64, k64, launch64, nbr, reb64 = timed_run(md, ctx, box, pos, vel, frc,
+                                                        md.PRECISION_FP64, args.steps,
+                                                        args.warmup, group)
+    if args.precision == "fp64":
+        group.close()
+        return 0
+    msmx, rowsmx, kmx, launchmx, _, rebmx = timed_run(md, ctx, box, pos, vel, frc,
+                                                      md.PRECISION_MIXED, args.steps,
+                                                      args.warmup, group, clocks)
+    clk = clocks.summary()
+    value64 = world * n * args.steps / (ms64 * 1e-3)
+    valuemx = world * n * args.steps / (msmx * 1e-3)
+    # force error of mixed vs FP64 on the same (equilibrated) state
+    s = md.System.from_arrays(pos, box, vel=vel, ctx=ctx)
+    v = md.VerletList(box, RC, SKIN, ctx=ctx)
+    v.build(s)
+    e64, w64 = md.LennardJones(1.0, 1.0, RC).compute_forces(s, v)
+    f64 = s.forces
+    emx, wmx = md.LennardJones(1.0, 1.0, RC, precision=md.PRECISION_MIXED).compute_forces(s, v)
+    fmx = s.forces
+    rms = float(np.sqrt(np.sum((fmx - f64) ** 2) / np.sum(f64 ** 2)))
+    del s, v
+    # end to end through the C ABI with host buffers (mixed)
+    e2e_steps = max(3, min(args.steps, args.e2e_steps))
+    sec, h2d, d2h = e2e_run(md, ctx, box, pos, vel, frc, e2e_steps, group)
+    e2e_value = world * n * e2e_steps / sec
+
+    if rank == 0:
+        peaks, peak_src = measured_peaks()
+        # algorithmic bytes of one force launch per atom: own position (32 B) + force
+        # write (24 B) + the half neighbour list (4 B per unique pair)
+        alg_per_atom = 32.0 + 24.0 + 4.0 * nbr / 2.0
+        achieved = alg_per_atom * n / (kmx * 1e-3) / 1e9
+        tpa = traffic_per_atom()
+        e0_64 = rows64[0, 0] + rows64[0, 2]
+        e0_mx = rowsmx[0, 0] + rowsmx[0, 2]
+        drift64 = float(np.max(np.abs(rows64[:, 0] + rows64[:, 2] - e0_64)) / n)
+        driftmx = float(np.max(np.abs(rowsmx[:, 0] + rowsmx[:, 2] - e0_mx)) / n)
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            kind, cval, _ = cpu_reference(pos, vel, box, args.cpu_steps, 1)
+            cpu = {"value": cval, "unit": UNIT, "cores": 1, "kind": kind,
+                   "sample": f"{args.cpu_steps} NVE VV steps of the same equilibrated "
+                             f"{n}-atom state after the reference's first Verlet build, "
+                             f"1 thread ({cpu_model()})"}
+        line = {
+            "metric": METRIC, "value": valuemx, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": msmx / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair terms, f64 displacement/accumulation/integration (mixed)",
+            "data": "synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities, "
+                    f"{args.equil} BAOAB equilibration steps",
+            "config": config(args.equil),
+            "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
+                     "force_kernel_ms": k64, "rebuilds": reb64},
+            "mixed_over_fp64": valuemx / value64,
+            "force_rms_rel_err": rms,
+            "energy_rel_err": abs(emx - e64) / abs(e64),
+            "virial_rel_err": abs(wmx - w64) / abs(w64),
+            "nve_max_energy_dev_per_atom": {"fp64": drift64, "mixed": driftmx,
+                                            "steps": args.steps},
+            "neighbour_entries_per_atom": nbr,
+            "rebuilds_in_timed_region": rebmx,
+            "gpu_launches": int(launchmx),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "precision": "mixed",
+                    "steps": e2e_steps,
+                    "path": "md_system_set x9 (pinned host) + md_run_lj(1 step) + "
+                            "md_system_get x9 per step"},
+            "roofline": {"bound": "hbm", "kernel": "k_lj_verlet (mixed)",
+                         "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": achieved / peaks.get("hbm_gbs", 6650.0),
+                         "peak_source": f"hbm_gbs of {peak_src}",
+                         "algorithmic_bytes_per_atom": alg_per_atom,
+                         "launch_ms": kmx,
+                         "traffic": (tpa * n) if tpa else None},
+            "clocks": clk,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.synchronize()
+    group.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--equil", type=int, default=2000)
+    ap.add_argument("--tpa", type=int, default=2)
+    ap.add_argument("--unroll", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--ref-steps", type=int, default=10)
+    ap.add_argument("--ref-procs", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="'mixed'/'fp64' run only that timed loop and print nothing "
+                         "(profiling configuration)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

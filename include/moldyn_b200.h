@@ -78,6 +78,7 @@ typedef struct md_cells md_cells;
 typedef struct md_verlet md_verlet;
 typedef struct md_lj md_lj;
 typedef struct md_integrator md_integrator;
+typedef struct md_ewald md_ewald;
 
 /* ------------------------------------------------------------------ library */
 /* Message of the last failing call on this thread ("" if none). */
@@ -95,6 +96,24 @@ MD_API int md_context_synchronize(md_context* ctx);
 MD_API int md_context_status(md_context* ctx, uint32_t* status, int clear);
 /* Number of kernels this context has launched (instrumentation). */
 MD_API int md_context_launch_count(md_context* ctx, int64_t* count);
+
+/* Instrumentation, no reference counterpart.  With timing enabled, launches of
+ * the kernels below are bracketed by CUDA events on the context's stream;
+ * md_context_kernel_time returns their summed device time (synchronises). */
+#define MD_KERNEL_LJ_FORCE 0     /* Lennard-Jones pair forces over the Verlet list */
+#define MD_KERNEL_NEIGHBOR 1     /* cell binning + Verlet build (host-driven builds) */
+#define MD_KERNEL_INTEGRATE 2    /* kick / drift / thermostat kernels */
+#define MD_KERNEL_EWALD_REAL 3   /* Ewald real-space pairs */
+#define MD_KERNEL_EWALD_RECIP 4  /* Ewald structure factors and k-space forces */
+MD_API int md_context_set_timing(md_context* ctx, int enable);
+MD_API int md_context_kernel_time(md_context* ctx, int kernel, int reset, double* total_ms,
+                                  int64_t* launches);
+/* Device time between two points on the context's stream (CUDA events). */
+MD_API int md_context_span_begin(md_context* ctx);
+MD_API int md_context_span_end(md_context* ctx, double* ms);
+/* Page-locked host memory for fast host<->device copies (NULL on failure). */
+MD_API void* md_host_alloc(size_t bytes);
+MD_API int md_host_free(void* p);
 
 /* ------------------------------------------------------------------- system */
 /* System(Box) + addAtom (core/system.hpp:15-27).  Positions, velocities,
@@ -168,9 +187,42 @@ MD_API int md_lj_forces_verlet(md_lj* lj, md_system* sys, md_verlet* list, doubl
                         double* virial);
 /* longRangeCorrection / longRangeCorrectionPressure (lennard_jones.cpp:121-151). */
 MD_API int md_lj_lrc(const md_lj* lj, int64_t n, const double box[3], double* u_lrc, double* p_lrc);
-/* Threads per atom of the Verlet-list force kernel: 1, 2, 4, 8 or 16 (process-wide
- * tuning knob, default 4; no reference counterpart -- the reference is scalar). */
+/* Launch shape of the Verlet-list force kernel (process-wide tuning knobs; no
+ * reference counterpart -- the reference is scalar): threads per atom 1, 2, 4 or 8
+ * (default 2) and independent neighbour gathers in flight per thread 1, 2 or 4
+ * (default 2). */
 MD_API int md_lj_set_threads_per_atom(int tpa);
+MD_API int md_lj_set_unroll(int unroll);
+
+/* ------------------------------------------------------------------- Ewald */
+/* e^2/(4 pi eps0 kB) in K*Angstrom/e^2 (ewald.cpp:17-21). */
+MD_API double md_coulomb_prefactor(void);
+/* Ewald(cutoff, kmax) (forcefield/ewald.hpp:51) plus alpha: alpha <= 0 selects the
+ * reference's 5.6 / min(L) (ewald.cpp:40); the reference has no alpha parameter.
+ * Real space runs over an internal Verlet list at cutoff + skin (default 1.0). */
+MD_API int md_ewald_create(md_context* ctx, double cutoff, int kmax, double alpha,
+                           md_ewald** out);
+MD_API int md_ewald_destroy(md_ewald* ew);
+MD_API int md_ewald_set_skin(md_ewald* ew, double skin);
+/* mode 0 computeEnergies, 1 computeForces (zeroes first), 2 accumulateForces
+ * (ewald.cpp:177-188).  terms = EwaldTerms {real, reciprocal, self, intra}
+ * (ewald.hpp:24-31).  virial (nullable): atomic virial of the Ewald sum -- no
+ * reference counterpart (the reference computes none). */
+MD_API int md_ewald_compute(md_ewald* ew, md_system* sys, int mode, double terms[4],
+                            double* virial);
+MD_API int md_ewald_alpha(const md_ewald* ew, double* alpha);          /* last alpha used */
+MD_API int md_ewald_kvector_count(const md_ewald* ew, int* count);     /* full k set */
+
+/* SpceForceField(params, cutoff, kmax) (forcefield/spce_forcefield.hpp:31-33):
+ * O-O Lennard-Jones (sigma_o, epsilon_o, truncated, with tail) + Ewald, on O,H,H
+ * triples.  Returns an md_ewald handle usable with md_spce_compute. */
+MD_API int md_spce_create(md_context* ctx, double sigma_o, double epsilon_o, double cutoff,
+                          int kmax, double alpha, md_ewald** out);
+/* computeForces (forces != 0; zeroes forces first) or computeEnergy
+ * (spce_forcefield.cpp:26-48).  parts (nullable, 8 doubles): Edisp, ELRC, Ereal,
+ * Efourier, Eself, Eintra, atomic virial, total. */
+MD_API int md_spce_compute(md_ewald* ff, md_system* sys, int forces, double* energy,
+                           double parts[8]);
 
 /* -------------------------------------------------------------- integrators */
 /* VelocityVerlet(dt) (integrate/velocity_verlet.hpp:41). */

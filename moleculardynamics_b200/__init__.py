@@ -31,6 +31,8 @@ MD_ERR_DEVICE = -5
 FIELD_X, FIELD_Y, FIELD_Z, FIELD_VX, FIELD_VY, FIELD_VZ = range(6)
 FIELD_FX, FIELD_FY, FIELD_FZ, FIELD_MASS, FIELD_CHARGE = range(6, 11)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+MD_KERNEL_LJ_FORCE, MD_KERNEL_NEIGHBOR, MD_KERNEL_INTEGRATE = 0, 1, 2
+MD_KERNEL_EWALD_REAL, MD_KERNEL_EWALD_RECIP = 3, 4
 
 
 class Truncation:
@@ -81,6 +83,12 @@ def _load():
         "md_context_synchronize": (C.c_int, [_vp]),
         "md_context_status": (C.c_int, [_vp, C.POINTER(C.c_uint32), C.c_int]),
         "md_context_launch_count": (C.c_int, [_vp, _i64p]),
+        "md_context_set_timing": (C.c_int, [_vp, C.c_int]),
+        "md_context_kernel_time": (C.c_int, [_vp, C.c_int, C.c_int, _d, _i64p]),
+        "md_context_span_begin": (C.c_int, [_vp]),
+        "md_context_span_end": (C.c_int, [_vp, _d]),
+        "md_host_alloc": (C.c_void_p, [C.c_size_t]),
+        "md_host_free": (C.c_int, [C.c_void_p]),
         "md_system_create": (C.c_int, [_vp, C.c_int64, _d, C.POINTER(_vp)]),
         "md_system_destroy": (C.c_int, [_vp]),
         "md_system_size": (C.c_int64, [_vp]),
@@ -118,6 +126,7 @@ def _load():
         "md_lj_forces_verlet": (C.c_int, [_vp, _vp, _vp, _d, _d]),
         "md_lj_lrc": (C.c_int, [_vp, C.c_int64, _d, _d, _d]),
         "md_lj_set_threads_per_atom": (C.c_int, [C.c_int]),
+        "md_lj_set_unroll": (C.c_int, [C.c_int]),
         "md_integrator_create_vv": (C.c_int, [C.c_double, C.POINTER(_vp)]),
         "md_integrator_create_baoab": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_uint64,
                                                  C.POINTER(_vp)]),
@@ -130,6 +139,16 @@ def _load():
         "md_integrator_set_noise": (C.c_int, [_vp, _d, C.c_int64]),
         "md_run_lj": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _d]),
         "md_fcc_lattice": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_uint64] + [_d] * 8),
+        "md_coulomb_prefactor": (C.c_double, []),
+        "md_ewald_create": (C.c_int, [_vp, C.c_double, C.c_int, C.c_double, C.POINTER(_vp)]),
+        "md_ewald_destroy": (C.c_int, [_vp]),
+        "md_ewald_set_skin": (C.c_int, [_vp, C.c_double]),
+        "md_ewald_compute": (C.c_int, [_vp, _vp, C.c_int, _d, _d]),
+        "md_ewald_alpha": (C.c_int, [_vp, _d]),
+        "md_ewald_kvector_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+        "md_spce_create": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                     C.POINTER(_vp)]),
+        "md_spce_compute": (C.c_int, [_vp, _vp, C.c_int, _d, _d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -462,6 +481,125 @@ class LennardJones:
 
 def set_threads_per_atom(tpa: int):
     _check(lib().md_lj_set_threads_per_atom(int(tpa)))
+
+
+def set_unroll(unroll: int):
+    _check(lib().md_lj_set_unroll(int(unroll)))
+
+
+def coulomb_prefactor() -> float:
+    """e^2/(4 pi eps0 kB) in K*Angstrom/e^2 (forcefield/ewald.cpp:17-21)."""
+    return lib().md_coulomb_prefactor()
+
+
+class EwaldTerms(dict):
+    """forcefield/ewald.hpp:24-31 (real, reciprocal, self, intra) as a dict."""
+
+    def total(self):
+        return self["real"] + self["reciprocal"] + self["self"] + self["intra"]
+
+
+class Ewald:
+    """forcefield/ewald.hpp:49-68 plus alpha (<= 0: the reference's 5.6 / min L)."""
+
+    def __init__(self, cutoff, kmax, alpha=0.0, ctx: Context | None = None, skin=1.0):
+        self.ctx = ctx or default_context()
+        h = _vp()
+        _check(lib().md_ewald_create(self.ctx.handle, float(cutoff), int(kmax), float(alpha),
+                                     C.byref(h)))
+        self._h = h
+        if skin != 1.0:
+            _check(lib().md_ewald_set_skin(h, float(skin)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_ewald_destroy(self._h)
+            self._h = None
+
+    def _run(self, sys, mode):
+        t = np.zeros(4)
+        w = C.c_double()
+        _check(lib().md_ewald_compute(self._h, sys.handle, mode, _ptr(t), C.byref(w)))
+        self.last_virial = w.value
+        return EwaldTerms(real=t[0], reciprocal=t[1], self=t[2], intra=t[3])
+
+    def compute_energies(self, sys):
+        return self._run(sys, 0)
+
+    def compute_forces(self, sys):
+        return self._run(sys, 1)
+
+    def accumulate_forces(self, sys):
+        return self._run(sys, 2)
+
+    def alpha(self):
+        a = C.c_double()
+        _check(lib().md_ewald_alpha(self._h, C.byref(a)))
+        return a.value
+
+
+class SpceParameters:
+    """forcefield/spce.hpp:16-24"""
+    qH = 0.42380
+    sigmaO = 3.16555789
+    epsilonO = 78.19743111
+    rOH = 1.0
+    angleHOH = 109.47
+    massOxygen = 15.9994
+    massHydrogen = 1.008
+
+
+class SpceForceField:
+    """forcefield/spce_forcefield.hpp:25-41 (+ alpha)."""
+
+    def __init__(self, cutoff=10.0, kmax=5, alpha=0.0, params=SpceParameters,
+                 ctx: Context | None = None, skin=1.0):
+        self.ctx = ctx or default_context()
+        h = _vp()
+        _check(lib().md_spce_create(self.ctx.handle, params.sigmaO, params.epsilonO,
+                                    float(cutoff), int(kmax), float(alpha), C.byref(h)))
+        self._h = h
+        if skin != 1.0:
+            _check(lib().md_ewald_set_skin(h, float(skin)))
+        self.parts = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_ewald_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _run(self, sys, forces):
+        e = C.c_double()
+        parts = np.zeros(8)
+        _check(lib().md_spce_compute(self._h, sys.handle, 1 if forces else 0, C.byref(e),
+                                     _ptr(parts)))
+        self.parts = dict(disp=parts[0], lrc=parts[1], real=parts[2], reciprocal=parts[3],
+                          self=parts[4], intra=parts[5], virial=parts[6], total=parts[7])
+        return e.value
+
+    def compute_forces(self, sys):
+        return self._run(sys, True)
+
+    def compute_energy(self, sys):
+        return self._run(sys, False)
+
+
+def build_spce_system(pos, types, box, params=SpceParameters, ctx=None):
+    """forcefield/spce.cpp:8-40: O,H,H triples; molecule id = index / 3."""
+    types = list(types)
+    n = len(types)
+    if n == 0 or n % 3 != 0:
+        raise InvalidArgument("buildSpceSystem: atom count must be a positive multiple of 3")
+    q = np.array([-2.0 * params.qH if t == "O" else params.qH for t in types])
+    m = np.array([params.massOxygen if t == "O" else params.massHydrogen for t in types])
+    for t in types:
+        if t not in ("O", "H"):
+            raise InvalidArgument(f"buildSpceSystem: unrecognised atom type '{t}'")
+    return System.from_arrays(pos, box, mass=m, charge=q, mol=np.arange(n) // 3, ctx=ctx)
 
 
 # ---------------------------------------------------------------- integrators

@@ -92,6 +92,42 @@ int ctx_check_status(md_context* ctx) {
                 (st & MD_STATUS_NONFINITE) ? "non-finite energy" : "");
 }
 
+void ctx_time_begin(md_context* ctx, int kernel) {
+    if (!ctx->timing || kernel < 0 || kernel >= kTimedKernels) return;
+    KernelTimer& t = ctx->timers[kernel];
+    if (static_cast<size_t>(2 * t.used + 2) > t.ev.size()) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return;
+        t.ev.push_back(a);
+        t.ev.push_back(b);
+    }
+    cudaEventRecord(t.ev[2 * t.used], ctx->stream);
+}
+
+void ctx_time_end(md_context* ctx, int kernel) {
+    if (!ctx->timing || kernel < 0 || kernel >= kTimedKernels) return;
+    KernelTimer& t = ctx->timers[kernel];
+    if (static_cast<size_t>(2 * t.used + 2) > t.ev.size()) return;
+    cudaEventRecord(t.ev[2 * t.used + 1], ctx->stream);
+    ++t.used;
+}
+
+// Folds recorded event pairs into the running totals (synchronises).
+static int ctx_collect(md_context* ctx) {
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < kTimedKernels; ++k) {
+        KernelTimer& t = ctx->timers[k];
+        for (int u = 0; u < t.used; ++u) {
+            float ms = 0.0f;
+            MDB_CUDA(cudaEventElapsedTime(&ms, t.ev[2 * u], t.ev[2 * u + 1]));
+            t.total_ms += ms;
+            ++t.launches;
+        }
+        t.used = 0;
+    }
+    return MD_OK;
+}
+
 }  // namespace mdb
 
 using namespace mdb;
@@ -142,6 +178,10 @@ int md_context_destroy(md_context* ctx) {
     if (ctx->h_result) cudaFreeHost(ctx->h_result);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
+    for (auto& t : ctx->timers)
+        for (cudaEvent_t e : t.ev) cudaEventDestroy(e);
+    if (ctx->span_start) cudaEventDestroy(ctx->span_start);
+    if (ctx->span_stop) cudaEventDestroy(ctx->span_stop);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return MD_OK;
@@ -159,6 +199,64 @@ int md_context_status(md_context* ctx, uint32_t* status, int clear) {
                              ctx->stream));
     if (clear) MDB_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MD_OK;
+}
+
+int md_context_set_timing(md_context* ctx, int enable) {
+    if (!ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_set_timing: NULL");
+    MDB_TRY(ctx_collect(ctx));
+    ctx->timing = enable != 0;
+    return MD_OK;
+}
+
+int md_context_kernel_time(md_context* ctx, int kernel, int reset, double* total_ms,
+                           int64_t* launches) {
+    if (!ctx || kernel < 0 || kernel >= kTimedKernels)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_context_kernel_time: bad argument");
+    MDB_TRY(ctx_collect(ctx));
+    KernelTimer& t = ctx->timers[kernel];
+    if (total_ms) *total_ms = t.total_ms;
+    if (launches) *launches = t.launches;
+    if (reset) {
+        t.total_ms = 0.0;
+        t.launches = 0;
+    }
+    return MD_OK;
+}
+
+int md_context_span_begin(md_context* ctx) {
+    if (!ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_span_begin: NULL");
+    if (!ctx->span_start) {
+        MDB_CUDA(cudaEventCreate(&ctx->span_start));
+        MDB_CUDA(cudaEventCreate(&ctx->span_stop));
+    }
+    MDB_CUDA(cudaEventRecord(ctx->span_start, ctx->stream));
+    return MD_OK;
+}
+
+int md_context_span_end(md_context* ctx, double* ms) {
+    if (!ctx || !ms || !ctx->span_start)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_context_span_end: no span was begun");
+    MDB_CUDA(cudaEventRecord(ctx->span_stop, ctx->stream));
+    MDB_CUDA(cudaEventSynchronize(ctx->span_stop));
+    float f = 0.0f;
+    MDB_CUDA(cudaEventElapsedTime(&f, ctx->span_start, ctx->span_stop));
+    *ms = f;
+    return MD_OK;
+}
+
+void* md_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("md_host_alloc: cudaMallocHost(%zu) failed", bytes);
+        return nullptr;
+    }
+    return p;
+}
+
+int md_host_free(void* p) {
+    if (p) MDB_CUDA(cudaFreeHost(p));
     return MD_OK;
 }
 

@@ -1,0 +1,742 @@
+// ewald.cu -- Ewald summation and the SPC/E force field (forcefield/ewald.cpp,
+// forcefield/spce_forcefield.cpp) on the device.
+//
+//   real space   erfc(alpha r)/r over intermolecular pairs with r < cutoff, taken
+//                from a Verlet list built at cutoff + skin (the reference scans all
+//                i<j pairs; the list holds exactly the pairs that can pass r < rc,
+//                and membership uses the reference's exact min-image r^2);
+//   self         -C alpha/sqrt(pi) sum q^2;
+//   intra        -C q_i q_j erf(alpha r)/r over same-molecule pairs (min image),
+//                from per-atom partner lists built once from the molecule ids;
+//   reciprocal   S(k) = sum_j q_j exp(i k.r_j) over the half space of k vectors
+//                (S(-k) = conj S(k), so energy and force sums double), with the
+//                per-axis factors exp(i n a x) built by complex recurrence.
+// The SPC/E force field adds O-O Lennard-Jones (oxygens = atoms with original
+// index divisible by 3, as SpceForceField::gatherOxygens takes them) in the same
+// pass over the real-space list.
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <unordered_map>
+#include <vector>
+
+#include "md_device.cuh"
+#include "md_internal.cuh"
+
+namespace mdb {
+int verlet_build(md_verlet* v, md_system* sys, bool conditional);
+int verlet_check(md_verlet* v, md_system* sys);
+int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
+}  // namespace mdb
+
+namespace mdb {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kBlock = 256;
+
+// ewald.hpp:10-13, ewald.cpp:17-21
+double coulomb_prefactor() {
+    const double e = 1.602176565e-19, eps0 = 8.854187817e-12, kB = 1.3806488e-23;
+    return (e * e) / (4.0 * kPi * eps0) * 1e10 / kB;
+}
+
+struct RealArgs {
+    double rc2, alpha, coulomb, two_alpha_over_sqrt_pi, neg_alpha2;
+    int spce_lj;            // add O-O LJ (SPC/E)
+    double sig2, four_eps, tf_eps;
+};
+
+// Real-space (and SPC/E O-O LJ) pair terms over the Verlet list.  out[0..3]:
+// E_real, W_real, E_lj, W_lj.  mode 1 writes forces, mode 2 adds to them.
+template <int TPA>
+__global__ void __launch_bounds__(kBlock)
+k_ewald_real(const double4* __restrict__ pos, const double* __restrict__ q,
+             const int64_t* __restrict__ mol, const int* __restrict__ nbr,
+             const int* __restrict__ count, int stride, int64_t n, Box3 box, RealArgs a,
+             int mode, double* fxo, double* fyo, double* fzo, double* part, unsigned* ticket,
+             double* out) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t i = t / TPA;
+    const int g = static_cast<int>(t % TPA);
+    const Fold3 f3 = fold3_of(box);
+    double fx = 0.0, fy = 0.0, fz = 0.0, er = 0.0, wr = 0.0, el = 0.0, wl = 0.0;
+    if (i < n) {
+        const double4 pi = pos[i];
+        const double qi = q[i];
+        const int64_t mi = mol[i];
+        const bool oxy_i = (static_cast<int64_t>(pi.w) % 3) == 0;
+        const int cnt = min(count[i], stride);
+        const int* row = nbr + i * static_cast<int64_t>(stride);
+        for (int k = g; k < cnt; k += TPA) {
+            const int j = __ldg(row + k);
+            const double4 pj = ldg4(pos + j);
+            const bool lo = pi.w < pj.w;
+            double dx, dy, dz;
+            if (lo) min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+            else min_image_wrapped(f3, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+            const double r2 = norm2_exact(dx, dy, dz);
+            if (!(r2 < a.rc2)) continue;
+            double s = 0.0;
+            if (mol[j] != mi) {
+                // ewald.cpp:60-68
+                const double r = __dsqrt_rn(r2);
+                const double cqq = a.coulomb * (qi * q[j]);
+                const double erfc_ar = erfc(a.alpha * r);
+                const double w = cqq * (a.two_alpha_over_sqrt_pi * exp(a.neg_alpha2 * r2) + erfc_ar / r);
+                s = w / r2;
+                if (lo) {
+                    er += cqq * erfc_ar / r;
+                    wr += w;
+                }
+            }
+            if (a.spce_lj && oxy_i && (static_cast<int64_t>(pj.w) % 3) == 0) {
+                // lennard_jones.cpp:62-70 (Truncated)
+                const double s2 = a.sig2 / r2;
+                const double s6 = s2 * s2 * s2;
+                const double w = a.tf_eps * (2.0 * s6 * s6 - s6);
+                s += w / r2;
+                if (lo) {
+                    el += a.four_eps * (s6 * s6 - s6);
+                    wl += w;
+                }
+            }
+            const double sg = lo ? s : -s;
+            fx = fma(dx, sg, fx);
+            fy = fma(dy, sg, fy);
+            fz = fma(dz, sg, fz);
+        }
+    }
+#pragma unroll
+    for (int o = TPA / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (i < n && g == 0) {
+        if (mode == 1) {
+            fxo[i] = fx;
+            fyo[i] = fy;
+            fzo[i] = fz;
+        } else {
+            fxo[i] += fx;
+            fyo[i] += fy;
+            fzo[i] += fz;
+        }
+    }
+    double v[4] = {er, wr, el, wl};
+    grid_reduce<4>(v, part, ticket, out);
+}
+
+// Intramolecular correction (ewald.cpp:79-110) per atom over its molecule partners
+// (original indices, CSR); adds to forces.  out[0..1]: E_intra, W_intra.
+__global__ void k_ewald_intra(const double4* __restrict__ pos, const double* __restrict__ q,
+                              const int* __restrict__ orig, const int* __restrict__ slot,
+                              const int* __restrict__ off, const int* __restrict__ partner,
+                              int64_t n, Box3 box, RealArgs a, int add_forces, double* fxo,
+                              double* fyo, double* fzo, double* part, unsigned* ticket,
+                              double* out) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const Fold3 f3 = fold3_of(box);
+    double e = 0.0, vir = 0.0;
+    if (k < n) {
+        const double4 pi = pos[k];
+        const int oi = orig[k];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int p = off[oi]; p < off[oi + 1]; ++p) {
+            const int oj = partner[p];
+            const int j = slot[oj];
+            const double4 pj = pos[j];
+            const bool lo = oi < oj;
+            double dx, dy, dz;
+            if (lo) min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+            else min_image_wrapped(f3, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+            const double r2 = norm2_exact(dx, dy, dz);
+            const double r = __dsqrt_rn(r2);
+            const double cqq = a.coulomb * (q[k] * q[j]);
+            const double erf_ar = erf(a.alpha * r);
+            const double w = cqq * (a.two_alpha_over_sqrt_pi * exp(a.neg_alpha2 * r2) - erf_ar / r);
+            const double s = lo ? w / r2 : -(w / r2);
+            fx = fma(dx, s, fx);
+            fy = fma(dy, s, fy);
+            fz = fma(dz, s, fz);
+            if (lo) {
+                e += -cqq * erf_ar / r;
+                vir += w;
+            }
+        }
+        if (add_forces) {
+            fxo[k] += fx;
+            fyo[k] += fy;
+            fzo[k] += fz;
+        }
+    }
+    double v[2] = {e, vir};
+    grid_reduce<2>(v, part, ticket, out);
+}
+
+__global__ void k_sum_q2(const double* __restrict__ q, int64_t n, double* part, unsigned* ticket,
+                         double* out) {
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        v[0] += q[k] * q[k];
+    grid_reduce<1>(v, part, ticket, out);
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+struct KArgs {
+    const double4* kvec;  // kx, ky, kz, factor
+    const int4* kn;       // nx, ny, nz
+    int nk, kmax;
+    double a, b, c;       // 2 pi / L per axis
+};
+
+constexpr int kSiteTile = 32;
+
+// S(k) partial sums: block (kb, sb) handles k vectors [kb*256, +256) against the
+// sites of slice sb; per-site factor tables X[nx], Y[ny], Z[nz] of a tile of sites
+// are built in shared memory by complex recurrence.
+__global__ void __launch_bounds__(kBlock)
+k_structure_factor(const double4* __restrict__ pos, const double* __restrict__ q, int64_t n,
+                   KArgs ka, int64_t sites_per_slice, double2* part) {
+    extern __shared__ double2 tab[];  // kSiteTile * (kmax+1 + 2*(2kmax+1))
+    const int nX = ka.kmax + 1, nY = 2 * ka.kmax + 1;
+    const int per = nX + 2 * nY;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int4 kn = k < ka.nk ? ka.kn[k] : make_int4(0, 0, 0, 0);
+    const int64_t s0 = blockIdx.y * sites_per_slice;
+    const int64_t s1 = min(n, s0 + sites_per_slice);
+    double re = 0.0, im = 0.0;
+    for (int64_t base = s0; base < s1; base += kSiteTile) {
+        __syncthreads();
+        // build tables: thread t builds site (t % tile), one axis per 3 groups
+        for (int w = threadIdx.x; w < 3 * kSiteTile; w += blockDim.x) {
+            const int site = w % kSiteTile, axis = w / kSiteTile;
+            const int64_t sidx = base + site;
+            double2* T = tab + site * per;
+            if (sidx < s1) {
+                const double4 p = pos[sidx];
+                const double coord = axis == 0 ? p.x : (axis == 1 ? p.y : p.z);
+                const double kk = axis == 0 ? ka.a : (axis == 1 ? ka.b : ka.c);
+                double sn, cs;
+                sincos(kk * coord, &sn, &cs);
+                const double2 e1 = make_double2(cs, sn);
+                if (axis == 0) {
+                    double2 x = make_double2(1.0, 0.0);
+                    for (int m = 0; m < nX; ++m) {
+                        T[m] = x;
+                        x = cmul(x, e1);
+                    }
+                } else {
+                    double2* Y = T + nX + (axis - 1) * nY;
+                    double2 y = make_double2(1.0, 0.0);
+                    for (int m = 0; m <= ka.kmax; ++m) {
+                        Y[ka.kmax + m] = y;
+                        Y[ka.kmax - m] = make_double2(y.x, -y.y);
+                        y = cmul(y, e1);
+                    }
+                }
+            } else {
+                for (int m = 0; m < (axis == 0 ? nX : nY); ++m)
+                    (axis == 0 ? T : T + nX + (axis - 1) * nY)[m] = make_double2(0.0, 0.0);
+            }
+        }
+        __syncthreads();
+        const int lim = static_cast<int>(s1 - base < kSiteTile ? s1 - base : kSiteTile);
+        if (k < ka.nk) {
+            for (int site = 0; site < lim; ++site) {
+                const double2* T = tab + site * per;
+                const double2 e = cmul(cmul(T[kn.x], T[nX + ka.kmax + kn.y]),
+                                       T[nX + nY + ka.kmax + kn.z]);
+                const double qs = q[base + site];
+                re = fma(qs, e.x, re);
+                im = fma(qs, e.y, im);
+            }
+        }
+    }
+    if (k < ka.nk) part[static_cast<int64_t>(blockIdx.y) * ka.nk + k] = make_double2(re, im);
+}
+
+// Sums the partials (slice order), stores S(k) and reduces the reciprocal energy
+// and virial: E = sum_half 2 factor |S|^2, W = sum_half 2 factor |S|^2 (1 - k^2/(2 a^2)).
+__global__ void k_structure_final(const double2* __restrict__ part, int slices, KArgs ka,
+                                  double inv_2alpha2, double2* sk, double* rpart,
+                                  unsigned* ticket, double* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (k < ka.nk) {
+        double re = 0.0, im = 0.0;
+        for (int s = 0; s < slices; ++s) {
+            const double2 p = part[static_cast<int64_t>(s) * ka.nk + k];
+            re += p.x;
+            im += p.y;
+        }
+        sk[k] = make_double2(re, im);
+        const double4 kv = ka.kvec[k];
+        const double k2 = kv.x * kv.x + kv.y * kv.y + kv.z * kv.z;
+        const double e = 2.0 * kv.w * (re * re + im * im);
+        v[0] = e;
+        v[1] = e * (1.0 - k2 * inv_2alpha2);
+    }
+    grid_reduce<2>(v, rpart, ticket, out);
+}
+
+// Reciprocal-space forces (ewald.cpp:163-170), one thread per site, k vectors in
+// (nx, ny) lines with exp(i nz c z) stepped along each line.
+__global__ void __launch_bounds__(kBlock)
+k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int64_t n, KArgs ka,
+              const int4* __restrict__ lines, int nlines, const double2* __restrict__ sk,
+              double* fxo, double* fyo, double* fzo) {
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s >= n) return;
+    const double4 p = pos[s];
+    const double qs = q[s];
+    double sn, cs;
+    sincos(ka.a * p.x, &sn, &cs);
+    const double2 ex = make_double2(cs, sn);
+    sincos(ka.b * p.y, &sn, &cs);
+    const double2 ey = make_double2(cs, sn);
+    sincos(ka.c * p.z, &sn, &cs);
+    const double2 ez = make_double2(cs, sn);
+    sincos(-ka.kmax * ka.b * p.y, &sn, &cs);
+    const double2 ey0 = make_double2(cs, sn);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    double2 X = make_double2(1.0, 0.0), Y = ey0;
+    int cur_nx = 0, cur_ny = -ka.kmax;
+    for (int l = 0; l < nlines; ++l) {
+        const int4 L = lines[l];  // nx, ny, nz0, first k index; count in next line's .w
+        while (cur_nx < L.x) {
+            X = cmul(X, ex);
+            ++cur_nx;
+            Y = ey0;
+            cur_ny = -ka.kmax;
+        }
+        while (cur_ny < L.y) {
+            Y = cmul(Y, ey);
+            ++cur_ny;
+        }
+        const double2 XY = cmul(X, Y);
+        sincos(static_cast<double>(L.z) * ka.c * p.z, &sn, &cs);
+        double2 Z = make_double2(cs, sn);
+        const int k0 = L.w, k1 = (l + 1 < nlines) ? lines[l + 1].w : ka.nk;
+        for (int k = k0; k < k1; ++k) {
+            const double2 e = cmul(XY, Z);
+            const double4 kv = ka.kvec[k];
+            const double2 S = sk[k];
+            // 2 (half space) * factor * 2 * q * (Re S sin - Im S cos)
+            const double coeff = 4.0 * kv.w * qs * (S.x * e.y - S.y * e.x);
+            fx = fma(coeff, kv.x, fx);
+            fy = fma(coeff, kv.y, fy);
+            fz = fma(coeff, kv.z, fz);
+            Z = cmul(Z, ez);
+        }
+    }
+    fxo[s] += fx;
+    fyo[s] += fy;
+    fzo[s] += fz;
+}
+
+template <int TPA>
+void launch_real(md_system* sys, md_verlet* v, const RealArgs& a, int mode, double* part,
+                 unsigned* ticket, double* out) {
+    const int64_t threads = std::max<int64_t>(sys->n * TPA, 1);
+    k_ewald_real<TPA><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
+        sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
+        v->stride, sys->n, Box3{{sys->box[0], sys->box[1], sys->box[2]},
+                                {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}},
+        a, mode, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+}
+
+}  // namespace
+
+}  // namespace mdb
+
+// Result slots inside kResEwald (doubles).
+enum {
+    kEwReal = 0, kEwRealW, kEwLj, kEwLjW, kEwIntra, kEwIntraW, kEwRecip, kEwRecipW, kEwQ2,
+    kEwCount
+};
+
+struct md_ewald {
+    md_context* ctx = nullptr;
+    double cutoff = 10.0;
+    int kmax = 5;
+    double alpha_in = 0.0;
+    double skin = 1.0;
+    bool spce = false;
+    double sigma_o = 0, epsilon_o = 0;
+    md_verlet* list = nullptr;
+    double list_box[3] = {0, 0, 0};
+    // topology (per original index)
+    md_system* topo_sys = nullptr;
+    uint64_t topo_version = 0;
+    int64_t topo_n = -1;
+    mdb::DevBuf partner_off, partner_idx;
+    int64_t npartners = 0;
+    // k vectors
+    double kbox[3] = {0, 0, 0};
+    int k_kmax = -1;
+    double k_alpha = 0.0;
+    mdb::DevBuf kvec, kn, lines, sk, skpart;
+    int nk = 0, nlines = 0;
+    double last[kEwCount] = {0};
+    double alpha = 0.0;
+};
+
+namespace mdb {
+
+namespace {
+
+int ewald_topology(md_ewald* ew, md_system* sys) {
+    if (ew->topo_sys == sys && ew->topo_version == sys->mol_version && ew->topo_n == sys->n)
+        return MD_OK;
+    const int64_t n = sys->n;
+    std::vector<int64_t> mol(static_cast<size_t>(n));
+    if (n > 0) MDB_TRY(md_system_get_molecule_ids(sys, mol.data()));
+    // group atoms by molecule (index order within each molecule)
+    std::unordered_map<int64_t, std::vector<int>> groups;
+    groups.reserve(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) groups[mol[i]].push_back(static_cast<int>(i));
+    std::vector<int> off(static_cast<size_t>(n + 1), 0), idx;
+    for (int64_t i = 0; i < n; ++i) off[i + 1] = static_cast<int>(groups[mol[i]].size()) - 1;
+    for (int64_t i = 0; i < n; ++i) off[i + 1] += off[i];
+    idx.resize(static_cast<size_t>(off[n]));
+    for (int64_t i = 0; i < n; ++i) {
+        int at = off[i];
+        for (int j : groups[mol[i]])
+            if (j != i) idx[at++] = j;
+    }
+    MDB_TRY(ew->partner_off.ensure(sizeof(int) * (n + 1)));
+    MDB_TRY(ew->partner_idx.ensure(sizeof(int) * std::max<size_t>(idx.size(), 1)));
+    MDB_CUDA(cudaMemcpy(ew->partner_off.ptr, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    if (!idx.empty())
+        MDB_CUDA(cudaMemcpy(ew->partner_idx.ptr, idx.data(), sizeof(int) * idx.size(),
+                            cudaMemcpyHostToDevice));
+    ew->npartners = static_cast<int64_t>(idx.size());
+    ew->topo_sys = sys;
+    ew->topo_version = sys->mol_version;
+    ew->topo_n = n;
+    return MD_OK;
+}
+
+// k vectors of the half space, grouped in (nx, ny) lines (ewald.cpp:112-172): the
+// full set n in [-kmax,kmax]^3, 0 < |n|^2 < kmax^2 + 2, is {k} u {-k} of these.
+int ewald_kvectors(md_ewald* ew, const double box[3], double alpha) {
+    if (ew->k_kmax == ew->kmax && ew->k_alpha == alpha && ew->kbox[0] == box[0] &&
+        ew->kbox[1] == box[1] && ew->kbox[2] == box[2])
+        return MD_OK;
+    const int kmax = ew->kmax;
+    const double volume = box[0] * box[1] * box[2];
+    const double kx0 = 2.0 * kPi / box[0], ky0 = 2.0 * kPi / box[1], kz0 = 2.0 * kPi / box[2];
+    const int n2max = kmax * kmax + 2;
+    const double coulomb = coulomb_prefactor();
+    std::vector<double4> kv;
+    std::vector<int4> kn, lines;
+    for (int nx = 0; nx <= kmax; ++nx) {
+        for (int ny = -kmax; ny <= kmax; ++ny) {
+            if (nx == 0 && ny < 0) continue;
+            int first = -1;
+            for (int nz = -kmax; nz <= kmax; ++nz) {
+                if (nx == 0 && ny == 0 && nz <= 0) continue;
+                const int n2 = nx * nx + ny * ny + nz * nz;
+                if (n2 == 0 || n2 >= n2max) continue;
+                if (first < 0) first = nz;
+                const double kxv = kx0 * static_cast<double>(nx);
+                const double kyv = ky0 * static_cast<double>(ny);
+                const double kzv = kz0 * static_cast<double>(nz);
+                const double k2 = kxv * kxv + kyv * kyv + kzv * kzv;
+                const double factor =
+                    coulomb * (2.0 * kPi / volume) * std::exp(-k2 / (4.0 * alpha * alpha)) / k2;
+                if (first == nz) lines.push_back(make_int4(nx, ny, nz, static_cast<int>(kv.size())));
+                kv.push_back(make_double4(kxv, kyv, kzv, factor));
+                kn.push_back(make_int4(nx, ny, nz, 0));
+            }
+        }
+    }
+    ew->nk = static_cast<int>(kv.size());
+    ew->nlines = static_cast<int>(lines.size());
+    const size_t nk = std::max<size_t>(kv.size(), 1);
+    MDB_TRY(ew->kvec.ensure(sizeof(double4) * nk));
+    MDB_TRY(ew->kn.ensure(sizeof(int4) * nk));
+    MDB_TRY(ew->lines.ensure(sizeof(int4) * std::max<size_t>(lines.size(), 1)));
+    MDB_TRY(ew->sk.ensure(sizeof(double2) * nk));
+    if (!kv.empty()) {
+        MDB_CUDA(cudaMemcpy(ew->kvec.ptr, kv.data(), sizeof(double4) * kv.size(), cudaMemcpyHostToDevice));
+        MDB_CUDA(cudaMemcpy(ew->kn.ptr, kn.data(), sizeof(int4) * kn.size(), cudaMemcpyHostToDevice));
+        MDB_CUDA(cudaMemcpy(ew->lines.ptr, lines.data(), sizeof(int4) * lines.size(),
+                            cudaMemcpyHostToDevice));
+    }
+    ew->k_kmax = kmax;
+    ew->k_alpha = alpha;
+    for (int d = 0; d < 3; ++d) ew->kbox[d] = box[d];
+    return MD_OK;
+}
+
+int ewald_list(md_ewald* ew, md_system* sys) {
+    if (ew->list && (ew->list_box[0] != sys->box[0] || ew->list_box[1] != sys->box[1] ||
+                     ew->list_box[2] != sys->box[2])) {
+        md_verlet_destroy(ew->list);
+        ew->list = nullptr;
+    }
+    if (!ew->list) {
+        MDB_TRY(md_verlet_create(ew->ctx, sys->box, ew->cutoff, ew->skin, &ew->list));
+        for (int d = 0; d < 3; ++d) ew->list_box[d] = sys->box[d];
+    }
+    md_verlet* v = ew->list;
+    if (!v->sys || v->sys != sys || v->n != sys->n || v->epoch != sys->epoch) {
+        MDB_TRY(verlet_build(v, sys, false));
+        return MD_OK;
+    }
+    int f = 0;
+    MDB_TRY(md_verlet_needs_rebuild(v, sys, &f));
+    if (f) MDB_TRY(verlet_build(v, sys, false));
+    return MD_OK;
+}
+
+}  // namespace
+
+// Everything of one evaluation, asynchronously; results land in kResEwald slots.
+// mode: 0 energies only, 1 zero + accumulate forces, 2 accumulate onto forces.
+int ewald_eval_async(md_ewald* ew, md_system* sys, int mode) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    double min_len = std::min(sys->box[0], std::min(sys->box[1], sys->box[2]));
+    const double alpha = ew->alpha_in > 0.0 ? ew->alpha_in : 5.6 / min_len;  // ewald.cpp:40
+    ew->alpha = alpha;
+    MDB_TRY(ewald_topology(ew, sys));
+    MDB_TRY(ewald_kvectors(ew, sys->box, alpha));
+    MDB_TRY(ewald_list(ew, sys));
+    md_verlet* v = ew->list;
+    RealArgs a;
+    a.rc2 = ew->cutoff * ew->cutoff;
+    a.alpha = alpha;
+    a.coulomb = coulomb_prefactor();
+    a.two_alpha_over_sqrt_pi = 2.0 * alpha / std::sqrt(kPi);
+    a.neg_alpha2 = -alpha * alpha;
+    a.spce_lj = ew->spce ? 1 : 0;
+    a.sig2 = ew->sigma_o * ew->sigma_o;
+    a.four_eps = 4.0 * ew->epsilon_o;
+    a.tf_eps = 24.0 * ew->epsilon_o;
+    double* res = ctx_result(ctx, kResEwald);
+    const Box3 box{{sys->box[0], sys->box[1], sys->box[2]},
+                   {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}};
+    double* part;
+    const int64_t real_threads = std::max<int64_t>(n * 4, 1);
+    MDB_TRY(ctx_partials(ctx, 4 * static_cast<size_t>(grid_for(real_threads, kBlock)), &part));
+    // real space (+ O-O LJ): with forces it writes (mode 1) or adds (mode 2); for
+    // energies only it writes into the scratch force sink of a zero-force pass.
+    ctx_time_begin(ctx, MD_KERNEL_EWALD_REAL);
+    if (mode == 0) {
+        // energies only: run the pair pass without touching forces by pointing the
+        // sink at the partials' tail (never read back)
+        double* sink;
+        MDB_TRY(ctx_scratch(ctx, 3 * sizeof(double) * static_cast<size_t>(std::max<int64_t>(n, 1)),
+                            reinterpret_cast<void**>(&sink)));
+        const int64_t threads = std::max<int64_t>(n * 4, 1);
+        k_ewald_real<4><<<grid_for(threads, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
+            v->stride, n, box, a, 1, sink, sink + n, sink + 2 * n, part, ctx_counter(ctx, 4),
+            res + kEwReal);
+    } else {
+        launch_real<4>(sys, v, a, mode, part, ctx_counter(ctx, 4), res + kEwReal);
+    }
+    ctx_time_end(ctx, MD_KERNEL_EWALD_REAL);
+    // intramolecular correction
+    if (n > 0) {
+        k_ewald_intra<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->cur.charge, sys->cur.orig, sys->slot, ew->partner_off.as<int>(),
+            ew->partner_idx.as<int>(), n, box, a, mode != 0 ? 1 : 0, sys->cur.fx, sys->cur.fy,
+            sys->cur.fz, part, ctx_counter(ctx, 5), res + kEwIntra);
+        const int g = std::min<int>(grid_for(n, kBlock), ctx->sm_count * 4);
+        k_sum_q2<<<g, kBlock, 0, ctx->stream>>>(sys->cur.charge, n, part, ctx_counter(ctx, 6),
+                                                res + kEwQ2);
+    }
+    // reciprocal space
+    ctx_time_begin(ctx, MD_KERNEL_EWALD_RECIP);
+    KArgs ka;
+    ka.kvec = ew->kvec.as<double4>();
+    ka.kn = ew->kn.as<int4>();
+    ka.nk = ew->nk;
+    ka.kmax = ew->kmax;
+    ka.a = 2.0 * kPi / sys->box[0];
+    ka.b = 2.0 * kPi / sys->box[1];
+    ka.c = 2.0 * kPi / sys->box[2];
+    if (ew->nk > 0 && n > 0) {
+        const int kblocks = (ew->nk + kBlock - 1) / kBlock;
+        // enough site slices to give every SM a few blocks
+        int64_t slices = std::max<int64_t>(1, (4 * ctx->sm_count) / kblocks);
+        slices = std::min<int64_t>(slices, (n + kSiteTile - 1) / kSiteTile);
+        const int64_t per = ((n + slices - 1) / slices + kSiteTile - 1) / kSiteTile * kSiteTile;
+        slices = (n + per - 1) / per;
+        MDB_TRY(ew->skpart.ensure(sizeof(double2) * static_cast<size_t>(slices) * ew->nk));
+        const size_t smem =
+            sizeof(double2) * kSiteTile * static_cast<size_t>((ew->kmax + 1) + 2 * (2 * ew->kmax + 1));
+        if (smem > 48 * 1024)
+            MDB_CUDA(cudaFuncSetAttribute(k_structure_factor,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)));
+        k_structure_factor<<<dim3(kblocks, static_cast<unsigned>(slices)), kBlock, smem, ctx->stream>>>(
+            sys->cur.pos, sys->cur.charge, n, ka, per, ew->skpart.as<double2>());
+        double* rp;
+        MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(kblocks), &rp));
+        k_structure_final<<<kblocks, kBlock, 0, ctx->stream>>>(
+            ew->skpart.as<double2>(), static_cast<int>(slices), ka, 1.0 / (2.0 * alpha * alpha),
+            ew->sk.as<double2>(), rp, ctx_counter(ctx, 7), res + kEwRecip);
+        if (mode != 0)
+            k_recip_force<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+                sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines,
+                ew->sk.as<double2>(), sys->cur.fx, sys->cur.fy, sys->cur.fz);
+    } else {
+        MDB_CUDA(cudaMemsetAsync(res + kEwRecip, 0, 2 * sizeof(double), ctx->stream));
+    }
+    ctx_time_end(ctx, MD_KERNEL_EWALD_RECIP);
+    MDB_CHECK_LAUNCH();
+    ctx->launches += 6;
+    return MD_OK;
+}
+
+int ewald_read(md_ewald* ew, md_context* ctx) {
+    MDB_TRY(ctx_read_results(ctx, kResEwald, kEwCount, ew->last));
+    return MD_OK;
+}
+
+}  // namespace mdb
+
+using namespace mdb;
+
+namespace {
+
+int ewald_new(md_context* ctx, double cutoff, int kmax, double alpha, md_ewald** out) {
+    if (!ctx || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_create: NULL argument");
+    if (!(cutoff > 0.0) || kmax < 0)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_create: cutoff must be > 0 and kmax >= 0");
+    md_ewald* ew = new (std::nothrow) md_ewald();
+    if (!ew) return fail(MD_ERR_OUT_OF_MEMORY, "md_ewald_create: host allocation");
+    ew->ctx = ctx;
+    ew->cutoff = cutoff;
+    ew->kmax = kmax;
+    ew->alpha_in = alpha;
+    *out = ew;
+    return MD_OK;
+}
+
+void fill_terms(const md_ewald* ew, double terms[4], double* virial) {
+    const double coulomb = coulomb_prefactor();
+    // ewald.cpp:76: -C alpha / sqrt(pi) * sum q^2
+    const double self = -coulomb * ew->alpha / std::sqrt(kPi) * ew->last[kEwQ2];
+    if (terms) {
+        terms[0] = ew->last[kEwReal];
+        terms[1] = ew->last[kEwRecip];
+        terms[2] = self;
+        terms[3] = ew->last[kEwIntra];
+    }
+    if (virial) *virial = ew->last[kEwRealW] + ew->last[kEwIntraW] + ew->last[kEwRecipW];
+}
+
+}  // namespace
+
+extern "C" {
+
+double md_coulomb_prefactor(void) { return coulomb_prefactor(); }
+
+int md_ewald_create(md_context* ctx, double cutoff, int kmax, double alpha, md_ewald** out) {
+    return ewald_new(ctx, cutoff, kmax, alpha, out);
+}
+
+int md_ewald_destroy(md_ewald* ew) {
+    if (!ew) return MD_OK;
+    if (ew->list) md_verlet_destroy(ew->list);
+    ew->partner_off.release();
+    ew->partner_idx.release();
+    ew->kvec.release();
+    ew->kn.release();
+    ew->lines.release();
+    ew->sk.release();
+    ew->skpart.release();
+    delete ew;
+    return MD_OK;
+}
+
+int md_ewald_set_skin(md_ewald* ew, double skin) {
+    if (!ew || !(skin >= 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_skin: bad argument");
+    ew->skin = skin;
+    if (ew->list) {
+        md_verlet_destroy(ew->list);
+        ew->list = nullptr;
+    }
+    return MD_OK;
+}
+
+int md_ewald_compute(md_ewald* ew, md_system* sys, int mode, double terms[4], double* virial) {
+    if (!ew || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_compute: NULL argument");
+    if (mode < 0 || mode > 2) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_compute: mode %d", mode);
+    if (sys->ctx != ew->ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_compute: context mismatch");
+    MDB_TRY(ewald_eval_async(ew, sys, mode));
+    MDB_TRY(ewald_read(ew, sys->ctx));
+    fill_terms(ew, terms, virial);
+    return MD_OK;
+}
+
+int md_ewald_alpha(const md_ewald* ew, double* alpha) {
+    if (!ew || !alpha) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_alpha: NULL");
+    *alpha = ew->alpha;
+    return MD_OK;
+}
+
+int md_ewald_kvector_count(const md_ewald* ew, int* count) {
+    if (!ew || !count) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_kvector_count: NULL");
+    *count = 2 * ew->nk;  // the full set is the half space and its negatives
+    return MD_OK;
+}
+
+// ------------------------------------------------------------------- SPC/E
+int md_spce_create(md_context* ctx, double sigma_o, double epsilon_o, double cutoff, int kmax,
+                   double alpha, md_ewald** out) {
+    MDB_TRY(ewald_new(ctx, cutoff, kmax, alpha, out));
+    (*out)->spce = true;
+    (*out)->sigma_o = sigma_o;
+    (*out)->epsilon_o = epsilon_o;
+    return MD_OK;
+}
+
+int md_spce_compute(md_ewald* ew, md_system* sys, int forces, double* energy, double parts[8]) {
+    if (!ew || !sys || !ew->spce) return fail(MD_ERR_INVALID_ARGUMENT, "md_spce_compute: not an SPC/E force field");
+    if (sys->n % 3 != 0)  // spce_forcefield.cpp:14-17
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "SpceForceField: atom count is not a multiple of 3; expected O,H,H triples");
+    MDB_TRY(ewald_eval_async(ew, sys, forces ? 1 : 0));
+    MDB_TRY(ewald_read(ew, sys->ctx));
+    double terms[4], vir;
+    fill_terms(ew, terms, &vir);
+    // dispersion tail of the oxygen subsystem (lennard_jones.cpp:121-135 with n = N/3)
+    const double m = static_cast<double>(sys->n / 3);
+    const double rho = m / (sys->box[0] * sys->box[1] * sys->box[2]);
+    const double sr = ew->sigma_o / ew->cutoff;
+    const double sr3 = sr * sr * sr, sr9 = sr3 * sr3 * sr3;
+    const double sig3 = ew->sigma_o * ew->sigma_o * ew->sigma_o;
+    const double elrc =
+        (8.0 / 3.0) * kPi * m * rho * ew->epsilon_o * sig3 * ((1.0 / 3.0) * sr9 - sr3);
+    const double disp = ew->last[kEwLj];
+    // spce_forcefield.cpp:40: disp + elrc + total()
+    const double total = disp + elrc + (terms[0] + terms[1] + terms[2] + terms[3]);
+    if (energy) *energy = total;
+    if (parts) {
+        parts[0] = disp;
+        parts[1] = elrc;
+        parts[2] = terms[0];
+        parts[3] = terms[1];
+        parts[4] = terms[2];
+        parts[5] = terms[3];
+        parts[6] = vir + ew->last[kEwLjW];  // atomic virial, no reference counterpart
+        parts[7] = total;
+    }
+    sys->last_energy = total;
+    return MD_OK;
+}
+
+}  // extern "C"

@@ -15,7 +15,7 @@
 
 namespace mdb {
 int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
-int verlet_ensure_capacity(md_verlet* v, md_system* sys);
+DispArgs disp_args(md_verlet* v, md_context* ctx, double* part);
 }  // namespace mdb
 
 namespace mdb {
@@ -34,73 +34,95 @@ struct StepArgs {
     const double* noise;  // replayed normals for this step (original order), or null
 };
 
-// velocity_verlet.hpp:55-65 (+ an optional NHC pending scale applied first).
-__global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc) {
+// Squared min-image displacement of a freshly moved atom from its position at the
+// last Verlet build (for the fused rebuild check).
+__device__ __forceinline__ double disp2(const Fold3& f3, double4 p, double4 q) {
+    double dx, dy, dz;
+    min_image_wrapped(f3, p.x, p.y, p.z, q.x, q.y, q.z, dx, dy, dz);
+    return norm2_exact(dx, dy, dz);
+}
+
+// velocity_verlet.hpp:55-65 (+ an optional NHC pending scale applied first).  With
+// CHECK the kernel also reduces the top-2 displacement since the last Verlet build
+// and writes the device rebuild flag (verlet_list.cpp:44-63), saving a pass.
+template <bool CHECK>
+__global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc, DispArgs d) {
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (k >= n) return;
-    double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
-    if (nhc) {
-        const double sc = nhc->scale;
-        vx = __dmul_rn(vx, sc);
-        vy = __dmul_rn(vy, sc);
-        vz = __dmul_rn(vz, sc);
+    double a1 = 0.0;
+    if (k < n) {
+        double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
+        if (nhc) {
+            const double sc = nhc->scale;
+            vx = __dmul_rn(vx, sc);
+            vy = __dmul_rn(vy, sc);
+            vz = __dmul_rn(vz, sc);
+        }
+        const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
+        vx = fma(c, a.fx[k], vx);
+        vy = fma(c, a.fy[k], vy);
+        vz = fma(c, a.fz[k], vz);
+        const Fold3 f3 = fold3_of(s.box);
+        double4 p = a.pos[k];
+        p.x = fold_wrapped(fma(s.dt, vx, p.x), f3.b[0]);
+        p.y = fold_wrapped(fma(s.dt, vy, p.y), f3.b[1]);
+        p.z = fold_wrapped(fma(s.dt, vz, p.z), f3.b[2]);
+        a.pos[k] = p;
+        a.vx[k] = vx;
+        a.vy[k] = vy;
+        a.vz[k] = vz;
+        if (CHECK) a1 = disp2(f3, p, d.ref[k]);
     }
-    const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
-    vx = fma(c, a.fx[k], vx);
-    vy = fma(c, a.fy[k], vy);
-    vz = fma(c, a.fz[k], vz);
-    double4 p = a.pos[k];
-    p.x = fold_exact(fma(s.dt, vx, p.x), s.box.L[0], s.box.inv[0]);
-    p.y = fold_exact(fma(s.dt, vy, p.y), s.box.L[1], s.box.inv[1]);
-    p.z = fold_exact(fma(s.dt, vz, p.z), s.box.L[2], s.box.inv[2]);
-    a.pos[k] = p;
-    a.vx[k] = vx;
-    a.vy[k] = vy;
-    a.vz[k] = vz;
+    if (CHECK) top2_grid(a1, 0.0, d);
 }
 
 // langevin.hpp:55-80: B, A (wrap), O, A (wrap).
-__global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s) {
+template <bool CHECK>
+__global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s, DispArgs d) {
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (k >= n) return;
-    const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
-    double vx = fma(c, a.fx[k], a.vx[k]);
-    double vy = fma(c, a.fy[k], a.vy[k]);
-    double vz = fma(c, a.fz[k], a.vz[k]);
-    double4 p = a.pos[k];
-    p.x = fold_exact(fma(s.half_dt, vx, p.x), s.box.L[0], s.box.inv[0]);
-    p.y = fold_exact(fma(s.half_dt, vy, p.y), s.box.L[1], s.box.inv[1]);
-    p.z = fold_exact(fma(s.half_dt, vz, p.z), s.box.L[2], s.box.inv[2]);
-    // O: v = c1*v + (c2*sqrt(T/m)) * xi
-    const int o = a.orig[k];
-    double x0, x1, x2;
-    if (s.noise) {
-        x0 = s.noise[3 * static_cast<int64_t>(o) + 0];
-        x1 = s.noise[3 * static_cast<int64_t>(o) + 1];
-        x2 = s.noise[3 * static_cast<int64_t>(o) + 2];
-    } else {
-        const U4 r0 = philox4x32_10(U4{static_cast<uint32_t>(o), 0u, static_cast<uint32_t>(s.step),
-                                       static_cast<uint32_t>(s.step >> 32)},
-                                    s.key0, s.key1);
-        const U4 r1 = philox4x32_10(U4{static_cast<uint32_t>(o), 1u, static_cast<uint32_t>(s.step),
-                                       static_cast<uint32_t>(s.step >> 32)},
-                                    s.key0, s.key1);
-        double x3;
-        normal2(r0, x0, x1);
-        normal2(r1, x2, x3);
+    double a1 = 0.0;
+    if (k < n) {
+        const Fold3 f3 = fold3_of(s.box);
+        const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
+        double vx = fma(c, a.fx[k], a.vx[k]);
+        double vy = fma(c, a.fy[k], a.vy[k]);
+        double vz = fma(c, a.fz[k], a.vz[k]);
+        double4 p = a.pos[k];
+        p.x = fold_wrapped(fma(s.half_dt, vx, p.x), f3.b[0]);
+        p.y = fold_wrapped(fma(s.half_dt, vy, p.y), f3.b[1]);
+        p.z = fold_wrapped(fma(s.half_dt, vz, p.z), f3.b[2]);
+        // O: v = c1*v + (c2*sqrt(T/m)) * xi
+        const int o = a.orig[k];
+        double x0, x1, x2;
+        if (s.noise) {
+            x0 = s.noise[3 * static_cast<int64_t>(o) + 0];
+            x1 = s.noise[3 * static_cast<int64_t>(o) + 1];
+            x2 = s.noise[3 * static_cast<int64_t>(o) + 2];
+        } else {
+            const U4 r0 = philox4x32_10(U4{static_cast<uint32_t>(o), 0u, static_cast<uint32_t>(s.step),
+                                           static_cast<uint32_t>(s.step >> 32)},
+                                        s.key0, s.key1);
+            const U4 r1 = philox4x32_10(U4{static_cast<uint32_t>(o), 1u, static_cast<uint32_t>(s.step),
+                                           static_cast<uint32_t>(s.step >> 32)},
+                                        s.key0, s.key1);
+            double x3;
+            normal2(r0, x0, x1);
+            normal2(r1, x2, x3);
+        }
+        const double sig = __dsqrt_rn(__ddiv_rn(s.temperature, a.mass[k]));
+        const double sc = __dmul_rn(s.c2, sig);
+        vx = __dadd_rn(__dmul_rn(s.c1, vx), __dmul_rn(x0, sc));
+        vy = __dadd_rn(__dmul_rn(s.c1, vy), __dmul_rn(x1, sc));
+        vz = __dadd_rn(__dmul_rn(s.c1, vz), __dmul_rn(x2, sc));
+        p.x = fold_wrapped(fma(s.half_dt, vx, p.x), f3.b[0]);
+        p.y = fold_wrapped(fma(s.half_dt, vy, p.y), f3.b[1]);
+        p.z = fold_wrapped(fma(s.half_dt, vz, p.z), f3.b[2]);
+        a.pos[k] = p;
+        a.vx[k] = vx;
+        a.vy[k] = vy;
+        a.vz[k] = vz;
+        if (CHECK) a1 = disp2(f3, p, d.ref[k]);
     }
-    const double sig = __dsqrt_rn(__ddiv_rn(s.temperature, a.mass[k]));
-    const double sc = __dmul_rn(s.c2, sig);
-    vx = __dadd_rn(__dmul_rn(s.c1, vx), __dmul_rn(x0, sc));
-    vy = __dadd_rn(__dmul_rn(s.c1, vy), __dmul_rn(x1, sc));
-    vz = __dadd_rn(__dmul_rn(s.c1, vz), __dmul_rn(x2, sc));
-    p.x = fold_exact(fma(s.half_dt, vx, p.x), s.box.L[0], s.box.inv[0]);
-    p.y = fold_exact(fma(s.half_dt, vy, p.y), s.box.L[1], s.box.inv[1]);
-    p.z = fold_exact(fma(s.half_dt, vz, p.z), s.box.L[2], s.box.inv[2]);
-    a.pos[k] = p;
-    a.vx[k] = vx;
-    a.vy[k] = vy;
-    a.vz[k] = vz;
+    if (CHECK) top2_grid(a1, 0.0, d);
 }
 
 // Second half-kick (velocity_verlet.hpp:70-73), fused with the kinetic-energy sum.
@@ -236,11 +258,20 @@ NhcState* nhc_of(md_integrator* it) {
     return it->kind == 2 ? it->chain_state.as<NhcState>() : nullptr;
 }
 
-int pre_force(md_integrator* it, md_system* sys) {
+// The pre-force half of a step.  With `check` the rebuild test of that Verlet
+// list is fused into the position update (fused stepping loops).
+int pre_force(md_integrator* it, md_system* sys, md_verlet* check) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     if (n == 0) return MD_OK;
     StepArgs s = step_args(it, sys);
+    DispArgs d{};
+    const int blocks = grid_for(n, kBlock);
+    if (check) {
+        double* part;
+        MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+        d = disp_args(check, ctx, part);
+    }
     if (it->kind == 1) {
         if (it->noise.ptr) {
             if (it->noise_used + 3 * n > it->noise_count)
@@ -248,7 +279,8 @@ int pre_force(md_integrator* it, md_system* sys) {
             s.noise = it->noise.as<double>() + it->noise_used;
             it->noise_used += 3 * n;
         }
-        k_baoab_pre<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, n, s);
+        if (check) k_baoab_pre<true><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, d);
+        else k_baoab_pre<false><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, d);
         ++it->step;
     } else {
         NhcState* nhc = nhc_of(it);
@@ -258,7 +290,8 @@ int pre_force(md_integrator* it, md_system* sys) {
             k_nhc_pre<<<1, 1, 0, ctx->stream>>>(nhc, ctx_result(ctx, kResKE), yoshida());
             ctx->launches += 1;
         }
-        k_kick_drift<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc);
+        if (check) k_kick_drift<true><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
+        else k_kick_drift<false><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
     }
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
@@ -297,7 +330,6 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
 }  // namespace
 
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
-int verlet_check(md_verlet* v, md_system* sys);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 
 }  // namespace mdb
@@ -377,7 +409,7 @@ int md_integrator_destroy(md_integrator* it) {
 
 int md_integrator_pre_force(md_integrator* it, md_system* sys) {
     if (!it || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_pre_force: NULL");
-    return pre_force(it, sys);
+    return pre_force(it, sys, nullptr);
 }
 
 int md_integrator_post_force(md_integrator* it, md_system* sys) {
@@ -436,16 +468,9 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
                                                 yoshida());
             ++ctx->launches;
         }
-        if (it->kind == 1) {
-            MDB_TRY(pre_force(it, sys));
-        } else if (sys->n > 0) {
-            StepArgs s = step_args(it, sys);
-            k_kick_drift<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n, s,
-                                                                              nhc);
-            ++ctx->launches;
-        }
-        // ForceFn of apps/moldyn_run.cpp:581-587, decided on the device.
-        MDB_TRY(verlet_check(v, sys));
+        // Kick/drift with the rebuild test of the ForceFn (apps/moldyn_run.cpp:581-587)
+        // fused in; the rebuild itself is gated on the device flag.
+        MDB_TRY(pre_force(it, sys, v));
         MDB_TRY(verlet_build(v, sys, true));
         MDB_TRY(lj_forces_verlet_async(lj, sys, v));
         MDB_TRY(post_force_async(it, sys, false));

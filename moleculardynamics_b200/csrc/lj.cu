@@ -69,13 +69,13 @@ __device__ __forceinline__ bool pair_exact(const LJArgs& a, double r2, double& u
 // The displacement is always r_lo - r_hi by original index, as the reference's
 // i<j pair sources produce it; atom lo gains +f, atom hi gains -f.
 template <bool LFS>
-__device__ __forceinline__ void accumulate_exact(const LJArgs& a, const Box3& box, double4 pi,
+__device__ __forceinline__ void accumulate_exact(const LJArgs& a, const Fold3& f3, double4 pi,
                                                  double4 pj, double& fx, double& fy, double& fz,
                                                  double& e, double& vir) {
     const bool lo = pi.w < pj.w;
     double dx, dy, dz;
-    if (lo) min_image_exact(box, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
-    else min_image_exact(box, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+    if (lo) min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+    else min_image_wrapped(f3, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
     double u, w, s;
     if (!pair_exact<LFS>(a, norm2_exact(dx, dy, dz), u, w, s)) return;
     const double gx = __dmul_rn(dx, s), gy = __dmul_rn(dy, s), gz = __dmul_rn(dz, s);
@@ -92,32 +92,36 @@ __device__ __forceinline__ void accumulate_exact(const LJArgs& a, const Box3& bo
     }
 }
 
-// Mixed precision: FP64 displacement (fast fold), FP32 pair terms, FP64 sums.
+// Mixed precision: the minimum-image displacement and r^2 in FP64 (r^2 is the
+// quantity the r^-14 force steepness amplifies, so it is rounded to FP32 once,
+// after it is formed); r^-2, r^-6, energy and force magnitude in FP32; the force
+// vector assembled and accumulated in FP64, as are energy and virial.
 template <bool LFS>
-__device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Box3& box, double4 pi,
+__device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Fold3& f3, double4 pi,
                                                  double4 pj, double& fx, double& fy, double& fz,
                                                  double& e, double& vir) {
+    // wrapped coordinates: |d| < L, so the nearest image is one compare away
     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    dx -= box.L[0] * rint(dx * box.inv[0]);
-    dy -= box.L[1] * rint(dy * box.inv[1]);
-    dz -= box.L[2] * rint(dz * box.inv[2]);
-    const float xf = static_cast<float>(dx), yf = static_cast<float>(dy), zf = static_cast<float>(dz);
-    const float r2 = xf * xf + yf * yf + zf * zf;
-    if (!(r2 < a.rc2f)) return;
-    const float inv = __frcp_rn(r2);
+    if (fabs(dx) > f3.b[0].lo) dx -= copysign(f3.b[0].L, dx);
+    if (fabs(dy) > f3.b[1].lo) dy -= copysign(f3.b[1].L, dy);
+    if (fabs(dz) > f3.b[2].lo) dz -= copysign(f3.b[2].L, dz);
+    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+    if (!(r2 < a.rc2)) return;
+    const float r2f = static_cast<float>(r2);
+    const float inv = __frcp_rn(r2f);
     const float s2 = a.sig2f * inv;
     const float s6 = s2 * s2 * s2;
     float u = a.four_epsf * (s6 * s6 - s6);
     float w = a.tf_epsf * (2.0f * s6 * s6 - s6);
     if (LFS) {
-        const float r = sqrtf(r2);
+        const float r = sqrtf(r2f);
         u = u - a.ucf - (r - a.rcf) * a.dudrcf;
         w = w + r * a.dudrcf;
     }
-    const float s = w * inv;
-    fx += static_cast<double>(xf * s);
-    fy += static_cast<double>(yf * s);
-    fz += static_cast<double>(zf * s);
+    const double s = static_cast<double>(w * inv);
+    fx = fma(dx, s, fx);
+    fy = fma(dy, s, fy);
+    fz = fma(dz, s, fz);
     if (pi.w < pj.w) {
         e += static_cast<double>(u);
         vir += static_cast<double>(w);
@@ -127,8 +131,15 @@ __device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Box3& bo
 constexpr int kBlock = 256;
 
 // Full Verlet list, TPA lanes per atom; rows are nbr[i*stride .. +count[i]).
-template <int TPA, bool MIXED, bool LFS>
-__global__ void __launch_bounds__(kBlock)
+// Register budget per unroll factor: U gather chains per thread need ~8U more
+// registers, traded against resident blocks per SM.
+template <int U>
+struct UnrollBlocks {
+    static constexpr int value = U >= 4 ? 2 : 4;
+};
+
+template <int TPA, bool MIXED, bool LFS, int U>
+__global__ void __launch_bounds__(kBlock, UnrollBlocks<U>::value)
 k_lj_verlet(const double4* __restrict__ pos, const int* __restrict__ nbr,
             const int* __restrict__ count, int stride, int64_t n, Box3 box, LJArgs a,
             double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
@@ -136,15 +147,32 @@ k_lj_verlet(const double4* __restrict__ pos, const int* __restrict__ nbr,
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t i = t / TPA;
     const int g = static_cast<int>(t % TPA);
+    const Fold3 f3 = fold3_of(box);
     double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
     if (i < n) {
         const double4 pi = pos[i];
         const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
         const int* row = nbr + i * static_cast<int64_t>(stride);
-        for (int k = g; k < cnt; k += TPA) {
+        // U independent index->position gather chains in flight per thread; the
+        // pair terms are accumulated in list order, as in the rolled loop.
+        int k = g;
+        for (; k + (U - 1) * TPA < cnt; k += U * TPA) {
+            int j[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) j[u] = __ldg(row + k + u * TPA);
+            double4 pj[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) pj[u] = ldg4(pos + j[u]);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (MIXED) accumulate_mixed<LFS>(a, f3, pi, pj[u], fx, fy, fz, e, vir);
+                else accumulate_exact<LFS>(a, f3, pi, pj[u], fx, fy, fz, e, vir);
+            }
+        }
+        for (; k < cnt; k += TPA) {
             const double4 pj = ldg4(pos + __ldg(row + k));
-            if (MIXED) accumulate_mixed<LFS>(a, box, pi, pj, fx, fy, fz, e, vir);
-            else accumulate_exact<LFS>(a, box, pi, pj, fx, fy, fz, e, vir);
+            if (MIXED) accumulate_mixed<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
+            else accumulate_exact<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
         }
     }
 #pragma unroll
@@ -170,6 +198,7 @@ k_lj_brute(const double4* __restrict__ pos, int64_t n, Box3 box, LJArgs a, int w
            double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
            double* part, unsigned* ticket, double* out) {
     __shared__ double4 tile[kBlock];
+    const Fold3 f3 = fold3_of(box);
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
     const double4 pi = i < n ? pos[i] : make_double4(0, 0, 0, -1.0);
@@ -181,7 +210,7 @@ k_lj_brute(const double4* __restrict__ pos, int64_t n, Box3 box, LJArgs a, int w
         if (i < n) {
             for (int t = 0; t < lim; ++t) {
                 if (base + t == i) continue;
-                accumulate_exact<LFS>(a, box, pi, tile[t], fx, fy, fz, e, vir);
+                accumulate_exact<LFS>(a, f3, pi, tile[t], fx, fy, fz, e, vir);
             }
         }
     }
@@ -211,6 +240,7 @@ k_lj_cells(const double4* __restrict__ pos, int64_t n, Box3 box, LJArgs a, CellA
            double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
            double* part, unsigned* ticket, double* out) {
     const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const Fold3 f3 = fold3_of(box);
     double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
     if (s < n) {
         // rank of sorted position s: binary search in start[]
@@ -233,7 +263,7 @@ k_lj_cells(const double4* __restrict__ pos, int64_t n, Box3 box, LJArgs a, CellA
             for (int t = c.start[rr]; t < c.start[rr + 1]; ++t) {
                 if (t == s) continue;
                 const int j = c.slot[c.sorted_orig[t]];
-                accumulate_exact<LFS>(a, box, pi, pos[j], fx, fy, fz, e, vir);
+                accumulate_exact<LFS>(a, f3, pi, pos[j], fx, fy, fz, e, vir);
             }
         }
         fxo[i] = fx;
@@ -253,30 +283,40 @@ Box3 box_of(const md_system* sys) {
     return b;
 }
 
-template <int TPA, bool MIXED, bool LFS>
+template <int TPA, bool MIXED, bool LFS, int U>
 void launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
                    double* out) {
     const int64_t threads = sys->n * TPA;
-    k_lj_verlet<TPA, MIXED, LFS><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
+    k_lj_verlet<TPA, MIXED, LFS, U><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
         sys->cur.pos, v->nbr.as<int>(), v->count.as<int>(), v->stride, sys->n, box_of(sys), a,
         sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
 }
 
+template <int TPA, bool MIXED, bool LFS>
+void launch_verlet_u(int unroll, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                     unsigned* ticket, double* out) {
+    switch (unroll) {
+        case 1: launch_verlet<TPA, MIXED, LFS, 1>(sys, v, a, part, ticket, out); break;
+        case 4: launch_verlet<TPA, MIXED, LFS, 4>(sys, v, a, part, ticket, out); break;
+        default: launch_verlet<TPA, MIXED, LFS, 2>(sys, v, a, part, ticket, out); break;
+    }
+}
+
 template <bool MIXED, bool LFS>
-void launch_verlet_tpa(int tpa, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
-                       unsigned* ticket, double* out) {
+void launch_verlet_tpa(int tpa, int unroll, md_system* sys, md_verlet* v, const LJArgs& a,
+                       double* part, unsigned* ticket, double* out) {
     switch (tpa) {
-        case 1: launch_verlet<1, MIXED, LFS>(sys, v, a, part, ticket, out); break;
-        case 2: launch_verlet<2, MIXED, LFS>(sys, v, a, part, ticket, out); break;
-        case 8: launch_verlet<8, MIXED, LFS>(sys, v, a, part, ticket, out); break;
-        case 16: launch_verlet<16, MIXED, LFS>(sys, v, a, part, ticket, out); break;
-        default: launch_verlet<4, MIXED, LFS>(sys, v, a, part, ticket, out); break;
+        case 1: launch_verlet_u<1, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
+        case 4: launch_verlet_u<4, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
+        case 8: launch_verlet_u<8, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
+        default: launch_verlet_u<2, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
     }
 }
 
 }  // namespace
 
-int g_lj_tpa = 4;  // threads per atom of the Verlet force kernel (tunable)
+int g_lj_tpa = 2;     // threads per atom of the Verlet force kernel (tunable)
+int g_lj_unroll = 2;  // independent gather chains per thread (tunable)
 
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     md_context* ctx = sys->ctx;
@@ -289,13 +329,15 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     double* out = ctx_result(ctx, kResEnergy);
     const bool lfs = lj->truncation == MD_LINEAR_FORCE_SHIFT;
     const bool mixed = lj->precision == MD_PRECISION_MIXED;
+    ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     if (mixed) {
-        if (lfs) launch_verlet_tpa<true, true>(g_lj_tpa, sys, v, a, part, ticket, out);
-        else launch_verlet_tpa<true, false>(g_lj_tpa, sys, v, a, part, ticket, out);
+        if (lfs) launch_verlet_tpa<true, true>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
+        else launch_verlet_tpa<true, false>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
     } else {
-        if (lfs) launch_verlet_tpa<false, true>(g_lj_tpa, sys, v, a, part, ticket, out);
-        else launch_verlet_tpa<false, false>(g_lj_tpa, sys, v, a, part, ticket, out);
+        if (lfs) launch_verlet_tpa<false, true>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
+        else launch_verlet_tpa<false, false>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
     }
+    ctx_time_end(ctx, MD_KERNEL_LJ_FORCE);
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;
@@ -453,11 +495,19 @@ int md_lj_lrc(const md_lj* lj, int64_t n, const double box[3], double* u_lrc, do
     return MD_OK;
 }
 
-// Threads per atom of the Verlet force kernel (1, 2, 4, 8 or 16); autotuning hook.
+// Threads per atom of the Verlet force kernel (1, 2, 4 or 8); autotuning hook.
 int md_lj_set_threads_per_atom(int tpa) {
-    if (tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8 && tpa != 16)
-        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_threads_per_atom: %d not in {1,2,4,8,16}", tpa);
+    if (tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_threads_per_atom: %d not in {1,2,4,8}", tpa);
     g_lj_tpa = tpa;
+    return MD_OK;
+}
+
+// Independent neighbour gathers in flight per thread (1, 2 or 4); autotuning hook.
+int md_lj_set_unroll(int unroll) {
+    if (unroll != 1 && unroll != 2 && unroll != 4)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_unroll: %d not in {1,2,4}", unroll);
+    g_lj_unroll = unroll;
     return MD_OK;
 }
 

@@ -24,6 +24,28 @@ __device__ __forceinline__ double fold_exact(double v, double L, double invL) {
     return __dsub_rn(v, __dmul_rn(L, k));
 }
 
+// fold_exact for a difference of two wrapped coordinates (|v| < 1.5 L), with
+// the floor replaced by comparisons wherever they provably agree with it:
+// floor(v/L + 0.5) is 0 for |v| <= 0.5 L (1 - 2^-40) and sign(v) for
+// 0.5 L (1 + 2^-40) <= |v| <= 1.5 L (1 - 2^-40), whatever the rounding of v/L;
+// v - L*k with k = +-1 is then v -+ L with the same single rounding.  Only
+// values within 2^-41 L of +-L/2 (or beyond) take the reference path.
+struct FoldBounds {
+    double L, invL, lo, hi, top;
+};
+
+__host__ __device__ inline FoldBounds fold_bounds(double L, double invL) {
+    const double e = 9.094947017729282e-13;  // 2^-40
+    return FoldBounds{L, invL, 0.5 * L * (1.0 - e), 0.5 * L * (1.0 + e), 1.5 * L * (1.0 - e)};
+}
+
+__device__ __forceinline__ double fold_wrapped(double v, const FoldBounds& b) {
+    const double a = fabs(v);
+    if (a <= b.lo) return v;
+    if (a >= b.hi && a <= b.top) return v > 0.0 ? __dsub_rn(v, b.L) : __dadd_rn(v, b.L);
+    return fold_exact(v, b.L, b.invL);
+}
+
 // core/vec3.hpp:59-65: x*x + y*y + z*z, left to right, no contraction.
 __device__ __forceinline__ double norm2_exact(double x, double y, double z) {
     return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
@@ -33,6 +55,24 @@ struct Box3 {
     double L[3];
     double inv[3];
 };
+
+struct Fold3 {
+    FoldBounds b[3];
+};
+
+__host__ __device__ inline Fold3 fold3_of(const Box3& box) {
+    return Fold3{{fold_bounds(box.L[0], box.inv[0]), fold_bounds(box.L[1], box.inv[1]),
+                  fold_bounds(box.L[2], box.inv[2])}};
+}
+
+// Minimum-image displacement r_a - r_b (reference arithmetic) for wrapped positions.
+__device__ __forceinline__ void min_image_wrapped(const Fold3& f, double ax, double ay,
+                                                  double az, double bx, double by, double bz,
+                                                  double& dx, double& dy, double& dz) {
+    dx = fold_wrapped(__dsub_rn(ax, bx), f.b[0]);
+    dy = fold_wrapped(__dsub_rn(ay, by), f.b[1]);
+    dz = fold_wrapped(__dsub_rn(az, bz), f.b[2]);
+}
 
 // Minimum-image displacement r_a - r_b with the reference's operation order.
 __device__ __forceinline__ void min_image_exact(const Box3& b, double ax, double ay, double az,
@@ -130,6 +170,73 @@ __device__ __forceinline__ void top2_insert(double& a1, double& a2, double d) {
         a1 = d;
     } else if (d > a2) {
         a2 = d;
+    }
+}
+
+// Grid-wide top-2 of per-thread (a1 >= a2) pairs of SQUARED displacements; the last
+// block to arrive takes the square roots of the winners (sqrt is monotone and
+// correctly rounded, so these equal the top two of the per-atom norms) and
+// writes the rebuild flag: criterion 0 -> d1 + d2 > skin (verlet_list.cpp:44-63),
+// 1 -> d1 > skin / 2.  Called by every thread; blockDim.x <= 1024.
+struct DispArgs {
+    const double4* ref;
+    double skin;
+    int criterion;
+    double* part;
+    unsigned* ticket;
+    int* flag;
+    double* top2;
+};
+
+__device__ inline void top2_grid(double a1, double a2, const DispArgs& d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b1 = __shfl_xor_sync(0xffffffffu, a1, o);
+        const double b2 = __shfl_xor_sync(0xffffffffu, a2, o);
+        top2_merge(a1, a2, b1, b2);
+    }
+    __shared__ double s1[32], s2[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        s1[warp] = a1;
+        s2[warp] = a2;
+    }
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        double b1 = s1[0], b2 = s2[0];
+        for (int w = 1; w < nw; ++w) top2_merge(b1, b2, s1[w], s2[w]);
+        d.part[2 * blockIdx.x] = b1;
+        d.part[2 * blockIdx.x + 1] = b2;
+        __threadfence();
+        last = atomicAdd(d.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    // the last block merges all partials with every thread, then a tree
+    __threadfence();
+    double c1 = 0.0, c2 = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        top2_merge(c1, c2, __ldcg(d.part + 2 * b), __ldcg(d.part + 2 * b + 1));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b1 = __shfl_xor_sync(0xffffffffu, c1, o);
+        const double b2 = __shfl_xor_sync(0xffffffffu, c2, o);
+        top2_merge(c1, c2, b1, b2);
+    }
+    __syncthreads();
+    if (lane == 0) {
+        s1[warp] = c1;
+        s2[warp] = c2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < nw; ++w) top2_merge(c1, c2, s1[w], s2[w]);
+        const double r1 = __dsqrt_rn(c1), r2 = __dsqrt_rn(c2);
+        d.top2[0] = r1;
+        d.top2[1] = r2;
+        *d.flag = (d.criterion == 0 ? (r1 + r2) > d.skin : r1 > 0.5 * d.skin) ? 1 : 0;
+        *d.ticket = 0u;
     }
 }
 

@@ -52,6 +52,17 @@ struct DevBuf {
 }  // namespace mdb
 
 // ------------------------------------------------------------------ context
+namespace mdb {
+// CUDA-event brackets around selected kernel launches (instrumentation only).
+struct KernelTimer {
+    std::vector<cudaEvent_t> ev;  // pairs: start, stop
+    int used = 0;                 // pairs recorded since the last read
+    int64_t launches = 0;
+    double total_ms = 0.0;
+};
+constexpr int kTimedKernels = 8;
+}  // namespace mdb
+
 struct md_context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -63,6 +74,9 @@ struct md_context {
     double* h_result = nullptr;          // pinned host mirror of `result`
     int64_t launches = 0;
     int sm_count = 148;
+    bool timing = false;
+    mdb::KernelTimer timers[mdb::kTimedKernels];
+    cudaEvent_t span_start = nullptr, span_stop = nullptr;
 };
 
 namespace mdb {
@@ -86,6 +100,9 @@ int ctx_partials(md_context* ctx, size_t doubles, double** out);
 int ctx_scratch(md_context* ctx, size_t bytes, void** out);
 int ctx_read_results(md_context* ctx, int first, int count, double* out);  // synchronises
 int ctx_check_status(md_context* ctx);  // synchronises; MD_ERR_DEVICE if status set
+// Bracket a launch with events when timing is enabled (kernel ids: MD_KERNEL_*).
+void ctx_time_begin(md_context* ctx, int kernel);
+void ctx_time_end(md_context* ctx, int kernel);
 inline unsigned* ctx_counter(md_context* ctx, int slot) { return ctx->d_counter + slot; }
 inline double* ctx_result(md_context* ctx, int slot) {
     return ctx->result.as<double>() + slot;
@@ -117,6 +134,7 @@ struct md_system {
     int* slot = nullptr;      // original index -> device slot
     uint64_t epoch = 1;       // bumped by every re-sort
     bool has_molecules = false;  // molecule ids differ from the atom's own index
+    uint64_t mol_version = 1;    // bumped whenever molecule ids are set
     double last_energy = 0.0, last_virial = 0.0;
 };
 

@@ -23,8 +23,8 @@ namespace mdb {
 namespace {
 
 constexpr int kBlock = 256;
-constexpr int kBuildWarps = 8;
-constexpr int kMaxCand = 1024;   // candidates staged per warp window
+constexpr int kBuildWarps = 4;
+constexpr int kMaxCand = 576;    // candidates staged per warp window
 
 __device__ __forceinline__ bool gate(const int* flag) { return flag == nullptr || *flag != 0; }
 
@@ -70,42 +70,90 @@ __global__ void k_bin(const double4* __restrict__ pos, int64_t n, GridArgs g, in
     atomicAdd(counts + r, 1);
 }
 
-// Single-block exclusive scan of counts[0..m) into start[0..m] (start[m] = total).
-__global__ void k_scan(const int* __restrict__ counts, int* start, int m, const int* flag) {
-    if (!gate(flag)) return;
+// Exclusive scan of counts[0..m) into start[0..m] (start[m] = total) in three
+// passes: each 1024-thread block scans 4096 consecutive counts (coalesced), the
+// block totals are scanned by one block, and the block offsets are added back.
+constexpr int kScanBlock = 1024, kScanItems = 4;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
     __shared__ int warp_tot[32];
-    __shared__ int carry;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) carry = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
     __syncthreads();
-    for (int base = 0; base < m; base += blockDim.x) {
-        const int i = base + tid;
-        const int v = i < m ? counts[i] : 0;
-        int x = v;
+    if (warp == 0) {
+        int w = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-        if (lane == 31) warp_tot[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            int w = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
-            }
-            warp_tot[lane] = w;
-        }
-        __syncthreads();
-        const int before = (warp > 0 ? warp_tot[warp - 1] : 0) + carry;
-        if (i < m) start[i] = before + x - v;
-        __syncthreads();
-        if (tid == blockDim.x - 1) carry = before + x;
-        __syncthreads();
+        warp_tot[lane] = w;
     }
-    if (tid == 0) start[m] = carry;
+    __syncthreads();
+    const int excl = (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
+    *total = warp_tot[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return excl;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int* __restrict__ counts,
+                                                            int* start, int m, int* bsum,
+                                                            const int* flag) {
+    if (!gate(flag)) return;
+    const int base = blockIdx.x * kScanBlock * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int u = 0; u < kScanItems; ++u) {
+        const int i = base + u * kScanBlock + threadIdx.x;  // coalesced
+        v[u] = i < m ? counts[i] : 0;
+    }
+    // scan in item-major order: thread t owns elements base + u*1024 + t
+    int run_base = 0;
+#pragma unroll
+    for (int u = 0; u < kScanItems; ++u) {
+        int tot;
+        const int ex = block_exclusive_scan(v[u], &tot);
+        const int i = base + u * kScanBlock + threadIdx.x;
+        if (i < m) start[i] = run_base + ex;
+        run_base += tot;
+        sum += v[u];
+    }
+    (void)sum;
+    if (threadIdx.x == 0) bsum[blockIdx.x] = run_base;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_top(int* bsum, int nb, int* start, int m,
+                                                         const int* flag) {
+    if (!gate(flag)) return;
+    int carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += kScanBlock) {
+        const int b = b0 + threadIdx.x;
+        const int v = b < nb ? bsum[b] : 0;
+        int tot;
+        const int ex = block_exclusive_scan(v, &tot);
+        if (b < nb) bsum[b] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) start[m] = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_add(int* start, int m, const int* __restrict__ bsum,
+                                                         const int* flag) {
+    if (!gate(flag)) return;
+    const int base = blockIdx.x * kScanBlock * kScanItems;
+    const int off = bsum[blockIdx.x];
+#pragma unroll
+    for (int u = 0; u < kScanItems; ++u) {
+        const int i = base + u * kScanBlock + threadIdx.x;
+        if (i < m) start[i] += off;
+    }
 }
 
 __global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const int* __restrict__ start,
@@ -118,13 +166,27 @@ __global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const in
     sorted[start[r] + at] = static_cast<int>(k);
 }
 
-// Within each cell, order atoms by original index (insertion sort; cells are small).
+// Within each cell, order atoms by original index.  One warp per cell: for up to
+// 32 atoms each lane's rank is the number of smaller keys (keys are distinct); a
+// larger cell falls back to an insertion sort by lane 0.
 __global__ void k_cell_order(int* sorted, const int* __restrict__ start, int m,
                              const int* __restrict__ orig, const int* flag) {
     if (!gate(flag)) return;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (r >= m) return;
-    const int s0 = start[r], s1 = start[r + 1];
+    const int s0 = start[r], s1 = start[r + 1], c = s1 - s0;
+    if (c <= 1) return;
+    if (c <= 32) {
+        const int v = lane < c ? sorted[s0 + lane] : 0;
+        const int key = lane < c ? orig[v] : 0x7fffffff;
+        int rank = 0;
+        for (int o = 0; o < c; ++o) rank += (__shfl_sync(0xffffffffu, key, o) < key) ? 1 : 0;
+        __syncwarp();
+        if (lane < c) sorted[s0 + rank] = v;
+        return;
+    }
+    if (lane != 0) return;
     for (int a = s0 + 1; a < s1; ++a) {
         const int v = sorted[a];
         const int key = orig[v];
@@ -137,8 +199,10 @@ __global__ void k_cell_order(int* sorted, const int* __restrict__ start, int m,
     }
 }
 
+// Gathers every per-atom array into the new order.  Forces are skipped when the
+// caller recomputes them right after the rebuild (fused stepping loops).
 __global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restrict__ perm,
-                                int* slot, int64_t n, const int* flag) {
+                                int* slot, int64_t n, const int* flag, int with_forces) {
     if (!gate(flag)) return;
     const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (s >= n) return;
@@ -147,9 +211,11 @@ __global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restric
     dst.vx[s] = src.vx[k];
     dst.vy[s] = src.vy[k];
     dst.vz[s] = src.vz[k];
-    dst.fx[s] = src.fx[k];
-    dst.fy[s] = src.fy[k];
-    dst.fz[s] = src.fz[k];
+    if (with_forces) {
+        dst.fx[s] = src.fx[k];
+        dst.fy[s] = src.fy[k];
+        dst.fz[s] = src.fz[k];
+    }
     dst.mass[s] = src.mass[k];
     dst.inv_mass[s] = src.inv_mass[k];
     dst.charge[s] = src.charge[k];
@@ -159,7 +225,8 @@ __global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restric
     slot[o] = static_cast<int>(s);
 }
 
-__global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* flag) {
+__global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* flag,
+                             int with_forces) {
     if (!gate(flag)) return;
     const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (s >= n) return;
@@ -167,9 +234,11 @@ __global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* f
     dst.vx[s] = src.vx[s];
     dst.vy[s] = src.vy[s];
     dst.vz[s] = src.vz[s];
-    dst.fx[s] = src.fx[s];
-    dst.fy[s] = src.fy[s];
-    dst.fz[s] = src.fz[s];
+    if (with_forces) {
+        dst.fx[s] = src.fx[s];
+        dst.fy[s] = src.fy[s];
+        dst.fz[s] = src.fz[s];
+    }
     dst.mass[s] = src.mass[s];
     dst.inv_mass[s] = src.inv_mass[s];
     dst.charge[s] = src.charge[s];
@@ -180,26 +249,38 @@ __global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* f
 // Exact candidate test with the pair ordered by original index.
 __device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, double rl2) {
     double dx, dy, dz;
-    if (pi.w < pj.w) min_image_exact(b, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
-    else min_image_exact(b, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+    const Fold3 f = fold3_of(b);
+    if (pi.w < pj.w) min_image_wrapped(f, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+    else min_image_wrapped(f, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
     return norm2_exact(dx, dy, dz) < rl2;
 }
 
 // One warp per (Morton-ranked) cell; device order == sorted order, so cell r holds
-// atoms [start[r], start[r+1]).
+// atoms [start[r], start[r+1]).  The candidates of the 27 surrounding cells are
+// staged in shared memory once per cell as FP32 coordinates relative to the cell
+// centre (nearest periodic image); then each lane takes one atom of the cell and
+// scans the staged candidates (a broadcast read), appending hits to its own row.
+// Only a candidate whose FP32 r^2 lies within 2^-12 of the list cutoff^2 -- far
+// wider than the FP32 error of these coordinates -- is decided by the exact
+// reference arithmetic, so the pair set stays bit-identical to the reference's.
+// Rows list candidates in stencil order, atoms of a cell in sorted order.
 __global__ void __launch_bounds__(kBuildWarps * 32)
 k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
                double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
                uint32_t* status, int* max_count, const int* flag) {
     if (!gate(flag)) return;
-    __shared__ int s_idx[kBuildWarps][kMaxCand];
-    __shared__ int s_cnt[kBuildWarps][32];
-    __shared__ int s_beg[kBuildWarps][32];
+    __shared__ float4 s_p[kBuildWarps][kMaxCand];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = blockIdx.x * kBuildWarps + warp;
     if (r >= g.ncells) return;
     const int cell = g.cell_of_rank[r];
     const int cx = cell % g.nx, cy = (cell / g.nx) % g.ny, cz = cell / (g.nx * g.ny);
+    const double ox = -0.5 * g.box.L[0] + (cx + 0.5) * g.wx;
+    const double oy = -0.5 * g.box.L[1] + (cy + 0.5) * g.wy;
+    const double oz = -0.5 * g.box.L[2] + (cz + 0.5) * g.wz;
+    const float lo_thr = static_cast<float>(rl2 * (1.0 - 1.0 / 4096.0));
+    const float hi_thr = static_cast<float>(rl2 * (1.0 + 1.0 / 4096.0));
+    // the 27 neighbour cell ranges (lane q holds cell q of the stencil)
     int beg = 0, cnt = 0;
     if (lane < 27) {
         int jx = cx + (lane % 3) - 1, jy = cy + ((lane / 3) % 3) - 1, jz = cz + (lane / 9) - 1;
@@ -210,7 +291,6 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
         beg = start[rr];
         cnt = start[rr + 1] - beg;
     }
-    // inclusive scan of cnt over the 27 lanes
     int incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -218,46 +298,96 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
         if (lane >= o) incl += y;
     }
     const int total = __shfl_sync(0xffffffffu, incl, 31);
-    s_cnt[warp][lane] = incl - cnt;  // exclusive offset
-    s_beg[warp][lane] = beg;
-    __syncwarp();
+    const int excl = incl - cnt;
     const int a0 = start[r], a1 = start[r + 1];
+    int local_max = 0;
     for (int wb = 0; wb < total; wb += kMaxCand) {
         const int wlen = min(kMaxCand, total - wb);
-        // stage candidate indices of this window
-        for (int t = lane; t < wlen; t += 32) {
-            const int gt = wb + t;
-            int q = 0;
-            while (q < 26 && s_cnt[warp][q + 1] <= gt) ++q;
-            s_idx[warp][t] = s_beg[warp][q] + (gt - s_cnt[warp][q]);
-        }
         __syncwarp();
-        for (int i = a0; i < a1; ++i) {
-            const double4 pi = pos[i];
-            int base = (wb == 0) ? 0 : count[i];
-            for (int t0 = 0; t0 < wlen; t0 += 32) {
-                const int t = t0 + lane;
-                bool hit = false;
-                int j = -1;
-                if (t < wlen) {
-                    j = s_idx[warp][t];
-                    if (j != i) hit = within(g.box, pi, ldg4(pos + j), rl2);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, hit);
-                if (hit) {
-                    const int at = base + __popc(m & ((1u << lane) - 1u));
-                    if (at < stride) nbr[static_cast<int64_t>(i) * stride + at] = j;
-                }
-                base += __popc(m);
+        // stage candidates [wb, wb + wlen) cell by cell
+        for (int q = 0; q < 27; ++q) {
+            const int qb = __shfl_sync(0xffffffffu, beg, q);
+            const int qo = __shfl_sync(0xffffffffu, excl, q);
+            const int qc = __shfl_sync(0xffffffffu, cnt, q);
+            const int lo = max(qo, wb), hi = min(qo + qc, wb + wlen);
+            for (int gt = lo + lane; gt < hi; gt += 32) {
+                const int j = qb + (gt - qo);
+                const double4 pj = ldg4(pos + j);
+                double vx = pj.x - ox, vy = pj.y - oy, vz = pj.z - oz;
+                vx -= g.box.L[0] * rint(vx * g.box.inv[0]);
+                vy -= g.box.L[1] * rint(vy * g.box.inv[1]);
+                vz -= g.box.L[2] * rint(vz * g.box.inv[2]);
+                s_p[warp][gt - wb] = make_float4(static_cast<float>(vx), static_cast<float>(vy),
+                                                 static_cast<float>(vz), __int_as_float(j));
             }
-            if (lane == 0) count[i] = base;
-            __syncwarp();
         }
         __syncwarp();
+        for (int ib = a0; ib < a1; ib += 32) {
+            const int i = ib + lane;
+            const bool active = i < a1;
+            double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
+            float fx = 0.f, fy = 0.f, fz = 0.f;
+            int c = 0;
+            if (active) {
+                pi = pos[i];
+                double ux = pi.x - ox, uy = pi.y - oy, uz = pi.z - oz;
+                ux -= g.box.L[0] * rint(ux * g.box.inv[0]);
+                uy -= g.box.L[1] * rint(uy * g.box.inv[1]);
+                uz -= g.box.L[2] * rint(uz * g.box.inv[2]);
+                fx = static_cast<float>(ux);
+                fy = static_cast<float>(uy);
+                fz = static_cast<float>(uz);
+                c = wb == 0 ? 0 : count[i];
+            }
+            int* row = nbr + static_cast<int64_t>(active ? i : 0) * stride;
+            int t = 0;
+            for (; t + 4 <= wlen; t += 4) {  // four independent candidate tests in flight
+                float4 q[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) q[u] = s_p[warp][t + u];
+                bool hit[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float dx = fx - q[u].x, dy = fy - q[u].y, dz = fz - q[u].z;
+                    hit[u] = dx * dx + dy * dy + dz * dz < lo_thr;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int j = __float_as_int(q[u].w);
+                    bool h = hit[u];
+                    if (!h) {
+                        const float dx = fx - q[u].x, dy = fy - q[u].y, dz = fz - q[u].z;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 <= hi_thr && active && j != i)
+                            h = within(g.box, pi, ldg4(pos + j), rl2);
+                    }
+                    if (h && active && j != i) {
+                        if (c < stride) row[c] = j;
+                        ++c;
+                    }
+                }
+            }
+            for (; t < wlen; ++t) {
+                const float4 q = s_p[warp][t];
+                const int j = __float_as_int(q.w);
+                const float dx = fx - q.x, dy = fy - q.y, dz = fz - q.z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                bool hit = r2 < lo_thr;
+                if (!hit && r2 <= hi_thr && active && j != i)
+                    hit = within(g.box, pi, ldg4(pos + j), rl2);
+                if (hit && active && j != i) {
+                    if (c < stride) row[c] = j;
+                    ++c;
+                }
+            }
+            if (active) {
+                count[i] = c;
+                local_max = max(local_max, c);
+            }
+        }
     }
+    const int mx = __reduce_max_sync(0xffffffffu, local_max);
     if (lane == 0) {
-        int mx = 0;
-        for (int i = a0; i < a1; ++i) mx = max(mx, count[i]);
         if (mx > 0) atomicMax(max_count, mx);
         if (mx > stride) atomicOr(status, MD_STATUS_NEIGHBOR_OVERFLOW);
     }
@@ -300,51 +430,19 @@ __global__ void k_store_ref(const double4* __restrict__ pos, double4* ref, int64
     if (k == 0 && total) ++*total;
 }
 
-// verlet_list.cpp:44-63: top-2 min-image displacement norms; decides on device.
-__global__ void k_displacement(const double4* __restrict__ pos, const double4* __restrict__ ref,
-                               int64_t n, Box3 box, double skin, int criterion, double* part,
-                               unsigned* ticket, int* flag, double* top2_out) {
+// verlet_list.cpp:44-63: top-2 min-image displacements; decides on device.
+__global__ void k_displacement(const double4* __restrict__ pos, int64_t n, Box3 box,
+                               DispArgs d) {
+    const Fold3 f3 = fold3_of(box);
     double a1 = 0.0, a2 = 0.0;
     for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const double4 p = pos[k], q = ref[k];
+        const double4 p = pos[k], q = d.ref[k];
         double dx, dy, dz;
-        min_image_exact(box, p.x, p.y, p.z, q.x, q.y, q.z, dx, dy, dz);
-        top2_insert(a1, a2, __dsqrt_rn(norm2_exact(dx, dy, dz)));
+        min_image_wrapped(f3, p.x, p.y, p.z, q.x, q.y, q.z, dx, dy, dz);
+        top2_insert(a1, a2, norm2_exact(dx, dy, dz));
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double b1 = __shfl_xor_sync(0xffffffffu, a1, o);
-        const double b2 = __shfl_xor_sync(0xffffffffu, a2, o);
-        top2_merge(a1, a2, b1, b2);
-    }
-    __shared__ double s1[32], s2[32];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane == 0) {
-        s1[warp] = a1;
-        s2[warp] = a2;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double b1 = s1[0], b2 = s2[0];
-        for (int w = 1; w < nw; ++w) top2_merge(b1, b2, s1[w], s2[w]);
-        part[2 * blockIdx.x] = b1;
-        part[2 * blockIdx.x + 1] = b2;
-        __threadfence();
-        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-        if (last) {
-            __threadfence();
-            double c1 = 0.0, c2 = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b)
-                top2_merge(c1, c2, __ldcg(part + 2 * b), __ldcg(part + 2 * b + 1));
-            top2_out[0] = c1;
-            top2_out[1] = c2;
-            const bool rebuild = criterion == 0 ? (c1 + c2) > skin : c1 > 0.5 * skin;
-            *flag = rebuild ? 1 : 0;
-            *ticket = 0u;
-        }
-    }
+    top2_grid(a1, a2, d);
 }
 
 inline uint32_t spread3(uint32_t v) {
@@ -386,7 +484,8 @@ Box3 make_box(const md_system* sys) {
 // Scratch for one sort: atom_rank (n) + counts (m) + fill (m).
 int sort_scratch(md_context* ctx, int64_t n, int m, int** atom_rank, int** counts, int** fill) {
     void* p;
-    const size_t bytes = (static_cast<size_t>(n) + 2 * static_cast<size_t>(m) + 64) * sizeof(int);
+    const size_t bsums = static_cast<size_t>(m) / (4096) + 64;  // k_scan block totals
+    const size_t bytes = (static_cast<size_t>(n) + 2 * static_cast<size_t>(m) + bsums) * sizeof(int);
     MDB_TRY(ctx_scratch(ctx, bytes, &p));
     *atom_rank = static_cast<int*>(p);
     *counts = *atom_rank + n;
@@ -408,12 +507,17 @@ int cell_sort_gated(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_
     if (n > 0)
         k_bin<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur.pos, n, g, atom_rank,
                                                                counts, flag);
-    k_scan<<<1, 1024, 0, ctx->stream>>>(counts, d_start, m, flag);
+    const int nb = (m + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
+    int* bsum = fill + m;  // scratch tail (sort_scratch reserves it)
+    k_scan_blocks<<<nb, kScanBlock, 0, ctx->stream>>>(counts, d_start, m, bsum, flag);
+    k_scan_top<<<1, kScanBlock, 0, ctx->stream>>>(bsum, nb, d_start, m, flag);
+    k_scan_add<<<nb, kScanBlock, 0, ctx->stream>>>(d_start, m, bsum, flag);
+    ctx->launches += 2;
     if (n > 0)
         k_scatter<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(atom_rank, n, d_start, fill,
                                                                    d_sorted, flag);
-    k_cell_order<<<grid_for(m, 128), 128, 0, ctx->stream>>>(d_sorted, d_start, m, sys->cur.orig,
-                                                           flag);
+    k_cell_order<<<grid_for(32 * static_cast<int64_t>(m), 256), 256, 0, ctx->stream>>>(
+        d_sorted, d_start, m, sys->cur.orig, flag);
     ctx->launches += 3 + (n > 0 ? 2 : 0);
     MDB_CHECK_LAUNCH();
     return MD_OK;
@@ -500,10 +604,11 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
         // Re-sort the system into cell order: permute into alt, copy back, so the
         // device pointers of the current arrays never change.
         if (n > 0) {
+            const int with_forces = flag ? 0 : 1;  // fused loops recompute forces next
             k_permute_gated<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
-                sys->cur, sys->alt, v->perm.as<int>(), sys->slot, n, flag);
+                sys->cur, sys->alt, v->perm.as<int>(), sys->slot, n, flag, with_forces);
             k_copy_atoms<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->alt, sys->cur, n,
-                                                                         flag);
+                                                                         flag, with_forces);
             ctx->launches += 2;
         }
         const GridArgs g = make_args(v->grid, sys);
@@ -551,17 +656,27 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
     return verlet_build_impl(v, sys, v->d_rebuild_flag);
 }
 
+DispArgs disp_args(md_verlet* v, md_context* ctx, double* part) {
+    DispArgs d;
+    d.ref = v->ref.as<double4>();
+    d.skin = v->skin;
+    d.criterion = v->criterion;
+    d.part = part;
+    d.ticket = ctx_counter(ctx, 1);
+    d.flag = v->d_rebuild_flag;
+    d.top2 = ctx_result(ctx, kResTop2);
+    return d;
+}
+
 int verlet_check(md_verlet* v, md_system* sys) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     const int g = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid_for(n, kBlock),
-                                                                      ctx->sm_count * 4)));
+                                                                      ctx->sm_count * 8)));
     double* part;
     MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(g), &part));
-    k_displacement<<<g, kBlock, 0, ctx->stream>>>(sys->cur.pos, v->ref.as<double4>(), n,
-                                                 make_box(sys), v->skin, v->criterion, part,
-                                                 ctx_counter(ctx, 1), v->d_rebuild_flag,
-                                                 ctx_result(ctx, kResTop2));
+    k_displacement<<<g, kBlock, 0, ctx->stream>>>(sys->cur.pos, n, make_box(sys),
+                                                 disp_args(v, ctx, part));
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;

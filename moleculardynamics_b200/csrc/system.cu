@@ -300,6 +300,7 @@ int md_system_set_molecule_ids(md_system* sys, const int64_t* ids) {
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    ++sys->mol_version;
     sys->has_molecules = false;
     for (int64_t i = 0; i < sys->n; ++i)
         if (ids[i] != i) {

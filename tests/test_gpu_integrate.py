@@ -181,9 +181,46 @@ def test_baoab_replayed_noise_matches_oracle(md):
     assert np.max(np.abs(s.velocities - vel)) < 1e-10
 
 
+def ks_normal(sample, sigma):
+    """Kolmogorov-Smirnov statistic against N(0, sigma) (tests/test_thermostat.cpp:29-39)."""
+    from math import erfc, sqrt
+    x = np.sort(np.asarray(sample))
+    n = len(x)
+    phi = np.array([0.5 * erfc(-v / (sigma * sqrt(2.0))) for v in x])
+    k = np.arange(1, n + 1)
+    return max(np.max(k / n - phi), np.max(phi - (k - 1) / n))
+
+
+def test_baoab_noise_is_standard_normal(md):
+    """The O-step's Philox normals: from v = 0 and zero force, one BAOAB step leaves
+    v = c2 * sqrt(T/m) * xi exactly, so the velocities expose the raw noise."""
+    s, st = lattice_system(md, 8, 0.8, 1.0, 4)  # N = 2048
+    s.velocities = np.zeros((s.n, 3))
+    s.forces = np.zeros((s.n, 3))
+    dt, gamma = 0.005, 1.0
+    c1 = np.exp(-gamma * dt)
+    c2 = np.sqrt(1.0 - c1 * c1)
+    integ = md.LangevinBAOAB(dt, gamma, 1.0, 99)
+    xs = []
+    for _ in range(8):
+        s.velocities = np.zeros((s.n, 3))
+        integ.step(s, lambda q: 0.0)
+        xs.append(s.velocities.ravel() / c2)
+    xi = np.concatenate(xs)  # 49152 draws
+    assert abs(np.mean(xi)) < 5.0 / np.sqrt(len(xi))
+    assert abs(np.var(xi) - 1.0) < 5.0 * np.sqrt(2.0 / len(xi))
+    assert ks_normal(xi, 1.0) < 1.63 / np.sqrt(len(xi))
+    # consecutive steps and neighbouring atoms are uncorrelated
+    a = xs[0].reshape(-1, 3)
+    b = xs[1].reshape(-1, 3)
+    assert abs(np.corrcoef(a[:, 0], b[:, 0])[0, 1]) < 5.0 / np.sqrt(len(a))
+    assert abs(np.corrcoef(a[:-1, 0], a[1:, 0])[0, 1]) < 5.0 / np.sqrt(len(a))
+
+
 def test_baoab_equipartition(md):
-    """tests/test_thermostat.cpp:41-96 (Philox noise; statistical parity)."""
-    s, st = lattice_system(md, 3, 0.80, 1.0, 42)
+    """tests/test_thermostat.cpp:41-96 with Philox noise (statistical parity).  N=864
+    rather than 108 so the +-2% band is ~5 standard errors of the mean wide."""
+    s, st = lattice_system(md, 6, 0.80, 1.0, 42)
     lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
     v = md.VerletList(st["box"], 2.5, 0.3)
     v.build(s)
@@ -194,6 +231,37 @@ def test_baoab_equipartition(md):
     dof = 3 * s.n
     mean_t = np.mean(2.0 * th[:, 2] / dof)
     assert 0.98 < mean_t < 1.02, mean_t
+
+
+def test_baoab_velocity_distribution_is_maxwell_boltzmann(md):
+    """tests/test_thermostat.cpp:98-143: frames 5/gamma apart, KS vs N(0, sqrt(T/m))."""
+    s, st = lattice_system(md, 3, 0.80, 1.0, 43)
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.LangevinBAOAB(0.005, 1.0, 1.0, 778)
+    integ.run(s, v, lj, 3000)
+    comps = []
+    for _ in range(60):
+        integ.run(s, v, lj, 1000)
+        comps.append(s.velocities.ravel())
+    comps = np.concatenate(comps)
+    assert ks_normal(comps, 1.0) < 1.63 / np.sqrt(len(comps))
+
+
+def test_baoab_relaxes_hot_start(md):
+    """tests/test_thermostat.cpp:145-179"""
+    s, st = lattice_system(md, 3, 0.80, 3.0, 99)
+    lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = md.LangevinBAOAB(0.005, 1.0, 1.0, 779)
+    integ.run(s, v, lj, 3000)
+    th = integ.run(s, v, lj, 4000, thermo=True)
+    final_t = np.mean(2.0 * th[:, 2] / (3 * s.n))
+    assert 0.9 < final_t < 1.1 and final_t < 1.5
 
 
 def test_nhc_matches_oracle_short(md):

@@ -105,6 +105,24 @@ def test_verlet_pair_set_bit_exact(md, c):
     assert np.array_equal(got, ref[order])
 
 
+@pytest.mark.parametrize("cells,skin", [(10, 0.3), (10, 1.5), (12, 0.3)])
+def test_verlet_pair_set_bit_exact_liquid(md, cells, skin):
+    """Pair sets on disordered states: several cells per side, and (skin 1.5) more
+    candidates per cell than one shared-memory staging window holds."""
+    st = md.fcc_lattice(cells, 0.8442, 0.722, 11)
+    rng = np.random.default_rng(cells)
+    pos = st["pos"] + rng.normal(scale=0.15, size=st["pos"].shape)
+    box = st["box"]
+    pos -= box * np.floor(pos / box + 0.5)
+    sys_ = md.System.from_arrays(pos, box)
+    v = md.VerletList(box, 2.5, skin)
+    v.build(sys_)
+    got = v.pairs()
+    ref = O.verlet_pairs(pos, box, 2.5, skin)
+    order = np.lexsort((ref[:, 1], ref[:, 0]))
+    assert np.array_equal(got, ref[order])
+
+
 def test_verlet_forces_match_brute(md):
     """tests/test_neighbor.cpp:106-128"""
     sys_ = nist_system(md, 1)
