@@ -257,6 +257,27 @@ MD_API int md_integrator_set_noise(md_integrator* integ, const double* xi, int64
 MD_API int md_run_lj(md_integrator* integ, md_system* sys, md_verlet* list, md_lj* lj, int64_t steps,
               double* thermo);
 
+/* Lennard-Jones forces, energy and virial by brute force (the arithmetic of
+ * md_lj_forces) for callers that must not allocate device memory -- no counterpart
+ * in the reference.  Callers such as a host framework that owns all device memory
+ * through its own pool, code running inside a stream capture, or latency-critical
+ * loops that cannot afford cudaMalloc's device-wide synchronisation pass their
+ * own device buffers: positions d_x/d_y/d_z (n doubles each, atom order), force
+ * outputs d_fx/d_fy/d_fz and d_energy_virial (2 doubles: pair energy, virial),
+ * and the CUDA stream to run on (NULL = legacy default stream).  The call
+ * allocates nothing: its reduction scratch is a fixed 16 KiB array in the
+ * library's device image, held by every GPU that loads the library until the
+ * process exits, which limits n to 262,144 atoms (larger n is rejected with
+ * MD_ERR_INVALID_ARGUMENT).  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  All calls share the array: calls that may overlap on the GPU
+ * (different streams, or different host threads on one device) race and must be
+ * serialised by the caller.  The call returns once the work is enqueued. */
+MD_API int md_lj_forces_static(const double* d_x, const double* d_y, const double* d_z,
+                               int64_t n, const double box[3], double sigma, double epsilon,
+                               double cutoff, int truncation, double* d_fx, double* d_fy,
+                               double* d_fz, double* d_energy_virial, void* stream);
+
 /* -------------------------------------------------------------------- setup */
 /* fccLattice(cells, density, temperature, seed) (util/lattice.cpp:15-64), on the
  * host: writes 4*cells^3 atoms into caller arrays (original order) and the cubic

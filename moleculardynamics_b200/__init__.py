@@ -140,6 +140,10 @@ def _load():
         "md_run_lj": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _d]),
         "md_fcc_lattice": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_uint64] + [_d] * 8),
         "md_coulomb_prefactor": (C.c_double, []),
+        "md_lj_forces_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, _d,
+                                          C.c_double, C.c_double, C.c_double, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
         "md_ewald_create": (C.c_int, [_vp, C.c_double, C.c_int, C.c_double, C.POINTER(_vp)]),
         "md_ewald_destroy": (C.c_int, [_vp]),
         "md_ewald_set_skin": (C.c_int, [_vp, C.c_double]),
