@@ -152,8 +152,8 @@ class Group:
 # ----------------------------------------------------------------------- GPU arm
 def traffic_per_atom():
     """DRAM bytes per atom of one mixed LJ force launch, from the committed ncu
-    summary (profiles/lj_force_mixed.txt), or None."""
-    path = os.path.join(ROOT, "profiles", "lj_force_mixed.txt")
+    summary (profiles/k_lj_verlet_mixed_lj1m.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "k_lj_verlet_mixed_lj1m.txt")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_atom:"):

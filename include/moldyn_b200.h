@@ -79,6 +79,7 @@ typedef struct md_verlet md_verlet;
 typedef struct md_lj md_lj;
 typedef struct md_integrator md_integrator;
 typedef struct md_ewald md_ewald;
+typedef struct md_rigid md_rigid;
 
 /* ------------------------------------------------------------------ library */
 /* Message of the last failing call on this thread ("" if none). */
@@ -224,6 +225,29 @@ MD_API int md_spce_create(md_context* ctx, double sigma_o, double epsilon_o, dou
 MD_API int md_spce_compute(md_ewald* ff, md_system* sys, int forces, double* energy,
                            double parts[8]);
 
+/* O-O Lennard-Jones truncation of an SPC/E force field: MD_TRUNCATED (default,
+ * with the analytic tail, spce_forcefield.cpp:9) or MD_LINEAR_FORCE_SHIFT (no
+ * tail; the continuous force tests/test_rigid_water.cpp:189-190 use). */
+MD_API int md_spce_set_lj_truncation(md_ewald* ff, int truncation);
+
+/* ------------------------------------------------------------- rigid water */
+/* RigidWater(ohDistance, hohAngleDegrees, tolerance, maxIterations)
+ * (constrain/rigid_water.hpp:32-35, rigid_water.cpp:30-53); invalid arguments give
+ * MD_ERR_INVALID_ARGUMENT like the reference's std::invalid_argument. */
+MD_API int md_rigid_create(double oh, double hoh_degrees, double tolerance, int max_iterations,
+                           md_rigid** out);
+MD_API int md_rigid_destroy(md_rigid* rw);
+MD_API int md_rigid_distances(const md_rigid* rw, double* oh, double* hh);
+/* degreesOfFreedom(molecules, comRemoved) (rigid_water.cpp:55-59). */
+MD_API int64_t md_rigid_degrees_of_freedom(int64_t molecules, int com_removed);
+/* constrainPositions(sys, reference) (rigid_water.cpp:61-116): reference positions
+ * as host arrays in original order.  constrainVelocities (rigid_water.cpp:118-161).
+ * *iterations receives the sweep count; non-convergence or a singular constraint
+ * returns MD_ERR_RUNTIME (the reference's std::runtime_error). */
+MD_API int md_rigid_constrain_positions(md_rigid* rw, md_system* sys, const double* rx,
+                                        const double* ry, const double* rz, int* iterations);
+MD_API int md_rigid_constrain_velocities(md_rigid* rw, md_system* sys, int* iterations);
+
 /* -------------------------------------------------------------- integrators */
 /* VelocityVerlet(dt) (integrate/velocity_verlet.hpp:41). */
 MD_API int md_integrator_create_vv(double dt, md_integrator** out);
@@ -235,6 +259,16 @@ MD_API int md_integrator_create_baoab(double dt, double friction, double tempera
  * MD_ERR_INVALID_ARGUMENT when chainLength < 1 (nose_hoover.cpp:36-38). */
 MD_API int md_integrator_create_nhc(double dt, double temperature, double tau, int chain_length,
                              int64_t dof, md_integrator** out);
+/* ConstrainedVelocityVerlet(dt, RigidWater) (integrate/constrained_velocity_verlet.hpp:25-26). */
+MD_API int md_integrator_create_rattle(double dt, const md_rigid* rw, md_integrator** out);
+/* The Nose-Hoover chain around the constrained step -- no reference counterpart
+ * (the reference has no thermostatted rigid-water integrator); dof = 6M - 3 for M
+ * molecules with the centre of mass fixed. */
+MD_API int md_integrator_create_rattle_nhc(double dt, const md_rigid* rw, double temperature,
+                                           double tau, int chain_length, int64_t dof,
+                                           md_integrator** out);
+/* Largest SHAKE / RATTLE sweep counts seen by a constrained integrator. */
+MD_API int md_integrator_iterations(md_integrator* integ, int* shake, int* rattle);
 MD_API int md_integrator_destroy(md_integrator* integ);
 /* The step is split around the force call so a host ForceFn can run between
  * (velocity_verlet.hpp:43-47: called exactly once per step):
@@ -286,6 +320,13 @@ MD_API int md_lj_forces_static(const double* d_x, const double* d_y, const doubl
 MD_API int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed, double* x,
                    double* y, double* z, double* vx, double* vy, double* vz, double* mass,
                    double box[3]);
+
+/* Fused device loop of a constrained integrator with SPC/E forces (the
+ * water_rdf-style NVE / NHC production loop): forces are (re)computed on entry,
+ * neighbour rebuilds are decided on the device.  thermo (nullable, steps*4):
+ * potential energy (K), virial, kinetic energy, conserved contribution. */
+MD_API int md_run_spce(md_integrator* integ, md_system* sys, md_ewald* ff, int64_t steps,
+                       double* thermo);
 
 #ifdef __cplusplus
 }

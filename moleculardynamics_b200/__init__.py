@@ -153,6 +153,19 @@ def _load():
         "md_spce_create": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                      C.POINTER(_vp)]),
         "md_spce_compute": (C.c_int, [_vp, _vp, C.c_int, _d, _d]),
+        "md_spce_set_lj_truncation": (C.c_int, [_vp, C.c_int]),
+        "md_rigid_create": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int,
+                                      C.POINTER(_vp)]),
+        "md_rigid_destroy": (C.c_int, [_vp]),
+        "md_rigid_distances": (C.c_int, [_vp, _d, _d]),
+        "md_rigid_degrees_of_freedom": (C.c_int64, [C.c_int64, C.c_int]),
+        "md_rigid_constrain_positions": (C.c_int, [_vp, _vp, _d, _d, _d, C.POINTER(C.c_int)]),
+        "md_rigid_constrain_velocities": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+        "md_integrator_create_rattle": (C.c_int, [C.c_double, _vp, C.POINTER(_vp)]),
+        "md_integrator_create_rattle_nhc": (C.c_int, [C.c_double, _vp, C.c_double, C.c_double,
+                                                      C.c_int, C.c_int64, C.POINTER(_vp)]),
+        "md_integrator_iterations": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "md_run_spce": (C.c_int, [_vp, _vp, _vp, C.c_int64, _d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -557,7 +570,9 @@ class SpceForceField:
     """forcefield/spce_forcefield.hpp:25-41 (+ alpha)."""
 
     def __init__(self, cutoff=10.0, kmax=5, alpha=0.0, params=SpceParameters,
-                 ctx: Context | None = None, skin=1.0):
+                 ctx: Context | None = None, skin=1.0, truncation=Truncation.Truncated):
+        """truncation applies to the O-O Lennard-Jones term: Truncated (the
+        reference's, with the analytic tail) or LinearForceShift (no tail)."""
         self.ctx = ctx or default_context()
         h = _vp()
         _check(lib().md_spce_create(self.ctx.handle, params.sigmaO, params.epsilonO,
@@ -565,6 +580,8 @@ class SpceForceField:
         self._h = h
         if skin != 1.0:
             _check(lib().md_ewald_set_skin(h, float(skin)))
+        if truncation != Truncation.Truncated:
+            _check(lib().md_spce_set_lj_truncation(h, int(truncation)))
         self.parts = None
 
     def __del__(self):
@@ -677,6 +694,100 @@ class NoseHooverChain(_Integrator):
                                               int(chain_length), int(dof), C.byref(h)))
         self._h = h
         self.dt = float(dt)
+
+
+# ---------------------------------------------------------------- rigid water
+class RigidWater:
+    """constrain/rigid_water.hpp:29-67: SHAKE/RATTLE on O-H1, O-H2, H1-H2 of each
+    consecutive (O, H, H) triple, one GPU thread per molecule."""
+
+    def __init__(self, oh_distance, hoh_angle_degrees, tolerance=1e-12, max_iterations=500):
+        h = _vp()
+        _check(lib().md_rigid_create(float(oh_distance), float(hoh_angle_degrees),
+                                     float(tolerance), int(max_iterations), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_rigid_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _distances(self):
+        oh, hh = C.c_double(), C.c_double()
+        _check(lib().md_rigid_distances(self._h, C.byref(oh), C.byref(hh)))
+        return oh.value, hh.value
+
+    def oh_distance(self):
+        return self._distances()[0]
+
+    def hh_distance(self):
+        return self._distances()[1]
+
+    @staticmethod
+    def degrees_of_freedom(molecules, com_removed):
+        return int(lib().md_rigid_degrees_of_freedom(int(molecules), 1 if com_removed else 0))
+
+    def constrain_positions(self, sys: System, reference) -> int:
+        """Reset positions onto the constraint surface along the bonds of
+        `reference` (an (N, 3) array in the system's atom order).  Returns the
+        sweep count; raises MDError (std::runtime_error) on non-convergence."""
+        ref = _f64(reference).reshape(-1, 3)
+        if ref.shape[0] != sys.n:
+            raise InvalidArgument("RigidWater: reference size differs from the system")
+        cols = [np.ascontiguousarray(ref[:, k]) for k in range(3)]
+        it = C.c_int()
+        _check(lib().md_rigid_constrain_positions(self._h, sys.handle, *[_ptr(c) for c in cols],
+                                                  C.byref(it)))
+        return it.value
+
+    def constrain_velocities(self, sys: System) -> int:
+        it = C.c_int()
+        _check(lib().md_rigid_constrain_velocities(self._h, sys.handle, C.byref(it)))
+        return it.value
+
+
+class ConstrainedVelocityVerlet(_Integrator):
+    """integrate/constrained_velocity_verlet.hpp:22-66 (RATTLE form)."""
+
+    def __init__(self, dt, constraint: RigidWater):
+        h = _vp()
+        _check(lib().md_integrator_create_rattle(float(dt), constraint.handle, C.byref(h)))
+        self._h = h
+        self.dt = float(dt)
+        self.constraint = constraint
+
+    def run(self, sys: System, ff: SpceForceField, steps: int, thermo=False):
+        """Fused device loop with SPC/E forces.  Forces are recomputed on entry.
+        Returns a (steps, 4) array [energy, virial, kinetic, conserved] if thermo."""
+        out = np.zeros((steps, 4)) if thermo and steps > 0 else None
+        _check(lib().md_run_spce(self._h, sys.handle, ff.handle, int(steps),
+                                 _ptr(out) if out is not None else None))
+        return out
+
+    def iterations(self):
+        """Largest (SHAKE, RATTLE) sweep counts seen so far."""
+        a, b = C.c_int(), C.c_int()
+        _check(lib().md_integrator_iterations(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
+class ConstrainedNoseHooverChain(ConstrainedVelocityVerlet):
+    """A Nose-Hoover chain (integrate/nose_hoover.hpp) around the constrained
+    step; the reference has no thermostatted rigid-water integrator.  dof is
+    RigidWater.degrees_of_freedom(molecules, True) for a system at rest."""
+
+    def __init__(self, dt, constraint: RigidWater, temperature, tau, chain_length, dof):
+        h = _vp()
+        _check(lib().md_integrator_create_rattle_nhc(float(dt), constraint.handle,
+                                                     float(temperature), float(tau),
+                                                     int(chain_length), int(dof), C.byref(h)))
+        self._h = h
+        self.dt = float(dt)
+        self.constraint = constraint
 
 
 # ---------------------------------------------------------------- setup

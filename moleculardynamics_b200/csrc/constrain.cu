@@ -1,0 +1,597 @@
+// constrain.cu -- rigid three-site water (constrain/rigid_water.cpp) and the
+// constrained velocity-Verlet step (integrate/constrained_velocity_verlet.hpp) on
+// the device, plus its Nose-Hoover-chain variant (no reference counterpart).
+//
+// SHAKE/RATTLE run one thread per molecule.  The reference sweeps all molecules
+// Gauss-Seidel style until the worst violation over the whole system is below the
+// tolerance; molecules share no atoms and a molecule whose three violations are
+// already within tolerance is left untouched by every later sweep, so iterating
+// each molecule to its own convergence gives identical positions and velocities,
+// and the reference's iteration count is the maximum over molecules.  Each update
+// uses the reference's operation order, so results are bit-identical to it.
+#include <cmath>
+#include <new>
+
+#include "md_device.cuh"
+#include "md_internal.cuh"
+
+namespace mdb {
+int nhc_pre_async(md_integrator* it, md_context* ctx, const double* ke_now);
+int nhc_post_async(md_integrator* it, md_context* ctx, const double* ke_sum);
+int nhc_apply_scale_async(md_integrator* it, md_system* sys);
+int record_async(md_context* ctx, const double* ev, const double* ke, const NhcState* nhc,
+                 double* row);
+int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated);
+int system_kinetic_async(md_system* sys, int slot);
+}  // namespace mdb
+
+namespace mdb {
+namespace {
+
+constexpr int kBlock = 128;
+constexpr double kPi = 3.14159265358979323846;
+__device__ __constant__ int kCons[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+
+struct RigidArgs {
+    double target2[3];  // squared O-H, O-H, H-H distances
+    double tolerance;
+    int max_iterations;
+};
+
+RigidArgs rigid_args(const md_rigid& rw) {
+    RigidArgs a;
+    a.target2[0] = rw.oh * rw.oh;
+    a.target2[1] = rw.oh * rw.oh;
+    a.target2[2] = rw.hh * rw.hh;
+    a.tolerance = rw.tolerance;
+    a.max_iterations = rw.max_iterations;
+    return a;
+}
+
+__device__ __forceinline__ double dot_exact(double ax, double ay, double az, double bx, double by,
+                                            double bz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
+}
+
+struct Mol {
+    double x[3], y[3], z[3];
+};
+
+// rigid_water.cpp:61-116 for one molecule.  Returns iterations, -1 (no
+// convergence) or -2 (singular denominator).
+__device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const RigidArgs& a,
+                              const Fold3& f3) {
+    for (int it = 0; it < a.max_iterations; ++it) {
+        double worst = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int i = kCons[c][0], j = kCons[c][1];
+            const double d2 = a.target2[c];
+            double ax, ay, az;
+            min_image_wrapped(f3, r.x[i], r.y[i], r.z[i], r.x[j], r.y[j], r.z[j], ax, ay, az);
+            const double s = __dsub_rn(norm2_exact(ax, ay, az), d2);
+            const double violation = __ddiv_rn(fabs(s), d2);
+            if (violation > worst) worst = violation;
+            if (violation <= a.tolerance) continue;
+            double bx, by, bz;
+            min_image_wrapped(f3, ref.x[i], ref.y[i], ref.z[i], ref.x[j], ref.y[j], ref.z[j], bx,
+                              by, bz);
+            const double inv_mass_sum = __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j]));
+            const double denom =
+                __dmul_rn(__dmul_rn(2.0, inv_mass_sum), dot_exact(ax, ay, az, bx, by, bz));
+            if (fabs(denom) < 1e-30) return -2;
+            const double g = __ddiv_rn(s, denom);
+            const double gi = __ddiv_rn(g, m[i]), gj = __ddiv_rn(g, m[j]);
+            r.x[i] = __dsub_rn(r.x[i], __dmul_rn(bx, gi));
+            r.y[i] = __dsub_rn(r.y[i], __dmul_rn(by, gi));
+            r.z[i] = __dsub_rn(r.z[i], __dmul_rn(bz, gi));
+            r.x[j] = __dadd_rn(r.x[j], __dmul_rn(bx, gj));
+            r.y[j] = __dadd_rn(r.y[j], __dmul_rn(by, gj));
+            r.z[j] = __dadd_rn(r.z[j], __dmul_rn(bz, gj));
+        }
+        if (worst <= a.tolerance) return it + 1;
+    }
+    return -1;
+}
+
+// rigid_water.cpp:118-161 for one molecule.
+__device__ int rattle_molecule(const Mol& r, Mol& v, const double m[3], const RigidArgs& a,
+                               const Fold3& f3) {
+    for (int it = 0; it < a.max_iterations; ++it) {
+        double worst = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int i = kCons[c][0], j = kCons[c][1];
+            const double d2 = a.target2[c];
+            double ax, ay, az;
+            min_image_wrapped(f3, r.x[i], r.y[i], r.z[i], r.x[j], r.y[j], r.z[j], ax, ay, az);
+            const double ux = __dsub_rn(v.x[i], v.x[j]), uy = __dsub_rn(v.y[i], v.y[j]),
+                         uz = __dsub_rn(v.z[i], v.z[j]);
+            const double rv = dot_exact(ax, ay, az, ux, uy, uz);
+            const double scaled = __ddiv_rn(fabs(rv), d2);
+            if (scaled > worst) worst = scaled;
+            if (scaled <= a.tolerance) continue;
+            const double inv_mass_sum = __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j]));
+            const double k = __ddiv_rn(rv, __dmul_rn(inv_mass_sum, norm2_exact(ax, ay, az)));
+            const double ki = __ddiv_rn(k, m[i]), kj = __ddiv_rn(k, m[j]);
+            v.x[i] = __dsub_rn(v.x[i], __dmul_rn(ax, ki));
+            v.y[i] = __dsub_rn(v.y[i], __dmul_rn(ay, ki));
+            v.z[i] = __dsub_rn(v.z[i], __dmul_rn(az, ki));
+            v.x[j] = __dadd_rn(v.x[j], __dmul_rn(ax, kj));
+            v.y[j] = __dadd_rn(v.y[j], __dmul_rn(ay, kj));
+            v.z[j] = __dadd_rn(v.z[j], __dmul_rn(az, kj));
+        }
+        if (worst <= a.tolerance) return it + 1;
+    }
+    return -1;
+}
+
+struct MolSlots {
+    int s[3];
+};
+
+__device__ __forceinline__ MolSlots mol_slots(const int* slot, int64_t m) {
+    return MolSlots{{slot[3 * m], slot[3 * m + 1], slot[3 * m + 2]}};
+}
+
+__device__ __forceinline__ void load_pos(const md_atoms& a, const MolSlots& ms, Mol& r) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double4 p = a.pos[ms.s[k]];
+        r.x[k] = p.x;
+        r.y[k] = p.y;
+        r.z[k] = p.z;
+    }
+}
+
+__device__ __forceinline__ void store_pos(md_atoms& a, const MolSlots& ms, const Mol& r) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double4 p = a.pos[ms.s[k]];
+        p.x = r.x[k];
+        p.y = r.y[k];
+        p.z = r.z[k];
+        a.pos[ms.s[k]] = p;
+    }
+}
+
+__device__ __forceinline__ void load_vel(const md_atoms& a, const MolSlots& ms, Mol& v) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v.x[k] = a.vx[ms.s[k]];
+        v.y[k] = a.vy[ms.s[k]];
+        v.z[k] = a.vz[ms.s[k]];
+    }
+}
+
+__device__ __forceinline__ void store_vel(md_atoms& a, const MolSlots& ms, const Mol& v) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a.vx[ms.s[k]] = v.x[k];
+        a.vy[ms.s[k]] = v.y[k];
+        a.vz[ms.s[k]] = v.z[k];
+    }
+}
+
+__device__ __forceinline__ void report(int it, int* max_it, uint32_t* status, uint32_t fail_bit) {
+    if (it > 0) atomicMax(max_it, it);
+    else atomicOr(status, it == -2 ? MD_STATUS_SHAKE_SINGULAR : fail_bit);
+}
+
+// constrainPositions with reference positions given in original order.
+__global__ void k_shake(md_atoms a, const int* __restrict__ slot, int64_t nmol,
+                        const double* __restrict__ rx, const double* __restrict__ ry,
+                        const double* __restrict__ rz, RigidArgs ra, Box3 box, int* max_it,
+                        uint32_t* status) {
+    const int64_t m = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (m >= nmol) return;
+    const Fold3 f3 = fold3_of(box);
+    const MolSlots ms = mol_slots(slot, m);
+    Mol r, ref;
+    load_pos(a, ms, r);
+    double mass[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        ref.x[k] = rx[3 * m + k];
+        ref.y[k] = ry[3 * m + k];
+        ref.z[k] = rz[3 * m + k];
+        mass[k] = a.mass[ms.s[k]];
+    }
+    const int it = shake_molecule(r, ref, mass, ra, f3);
+    report(it, max_it, status, MD_STATUS_SHAKE_DIVERGED);
+    store_pos(a, ms, r);
+}
+
+__global__ void k_rattle(md_atoms a, const int* __restrict__ slot, int64_t nmol, RigidArgs ra,
+                         Box3 box, int* max_it, uint32_t* status) {
+    const int64_t m = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (m >= nmol) return;
+    const Fold3 f3 = fold3_of(box);
+    const MolSlots ms = mol_slots(slot, m);
+    Mol r, v;
+    load_pos(a, ms, r);
+    load_vel(a, ms, v);
+    double mass[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) mass[k] = a.mass[ms.s[k]];
+    const int it = rattle_molecule(r, v, mass, ra, f3);
+    report(it, max_it, status, MD_STATUS_RATTLE_DIVERGED);
+    store_vel(a, ms, v);
+}
+
+struct CvvArgs {
+    double dt, half_dt, inv_dt;
+    RigidArgs ra;
+    Box3 box;
+};
+
+// constrained_velocity_verlet.hpp:31-52: reference = r; kick; drift (no wrap);
+// SHAKE along the reference bonds; velocity correction shift / dt.  An NHC
+// pending scale (if any) is applied to the velocities first.
+__global__ void k_cvv_pre(md_atoms a, const int* __restrict__ slot, int64_t nmol, CvvArgs c,
+                          const NhcState* nhc, int* max_it, uint32_t* status) {
+    const int64_t m = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (m >= nmol) return;
+    const Fold3 f3 = fold3_of(c.box);
+    const MolSlots ms = mol_slots(slot, m);
+    Mol r, v, ref, unc;
+    load_pos(a, ms, r);
+    load_vel(a, ms, v);
+    ref = r;
+    double mass[3];
+    const double sc = nhc ? nhc->scale : 1.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int s = ms.s[k];
+        mass[k] = a.mass[s];
+        if (nhc) {
+            v.x[k] = __dmul_rn(v.x[k], sc);
+            v.y[k] = __dmul_rn(v.y[k], sc);
+            v.z[k] = __dmul_rn(v.z[k], sc);
+        }
+        const double kc = __ddiv_rn(c.half_dt, mass[k]);  // 0.5 * dt_ / mass
+        v.x[k] = __dadd_rn(v.x[k], __dmul_rn(a.fx[s], kc));
+        v.y[k] = __dadd_rn(v.y[k], __dmul_rn(a.fy[s], kc));
+        v.z[k] = __dadd_rn(v.z[k], __dmul_rn(a.fz[s], kc));
+        r.x[k] = __dadd_rn(r.x[k], __dmul_rn(v.x[k], c.dt));
+        r.y[k] = __dadd_rn(r.y[k], __dmul_rn(v.y[k], c.dt));
+        r.z[k] = __dadd_rn(r.z[k], __dmul_rn(v.z[k], c.dt));
+    }
+    unc = r;
+    const int it = shake_molecule(r, ref, mass, c.ra, f3);
+    report(it, max_it, status, MD_STATUS_SHAKE_DIVERGED);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double sx, sy, sz;
+        min_image_wrapped(f3, r.x[k], r.y[k], r.z[k], unc.x[k], unc.y[k], unc.z[k], sx, sy, sz);
+        v.x[k] = __dadd_rn(v.x[k], __dmul_rn(sx, c.inv_dt));
+        v.y[k] = __dadd_rn(v.y[k], __dmul_rn(sy, c.inv_dt));
+        v.z[k] = __dadd_rn(v.z[k], __dmul_rn(sz, c.inv_dt));
+    }
+    store_pos(a, ms, r);
+    store_vel(a, ms, v);
+}
+
+// constrained_velocity_verlet.hpp:54-56: kick; RATTLE; kinetic-energy sum.
+__global__ void __launch_bounds__(kBlock)
+k_cvv_post(md_atoms a, const int* __restrict__ slot, int64_t nmol, CvvArgs c, int* max_it,
+           uint32_t* status, double* part, unsigned* ticket, double* ke_out) {
+    const int64_t m = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double ke[1] = {0.0};
+    if (m < nmol) {
+        const Fold3 f3 = fold3_of(c.box);
+        const MolSlots ms = mol_slots(slot, m);
+        Mol r, v;
+        load_pos(a, ms, r);
+        load_vel(a, ms, v);
+        double mass[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int s = ms.s[k];
+            mass[k] = a.mass[s];
+            const double kc = __ddiv_rn(c.half_dt, mass[k]);
+            v.x[k] = __dadd_rn(v.x[k], __dmul_rn(a.fx[s], kc));
+            v.y[k] = __dadd_rn(v.y[k], __dmul_rn(a.fy[s], kc));
+            v.z[k] = __dadd_rn(v.z[k], __dmul_rn(a.fz[s], kc));
+        }
+        const int it = rattle_molecule(r, v, mass, c.ra, f3);
+        report(it, max_it, status, MD_STATUS_RATTLE_DIVERGED);
+        store_vel(a, ms, v);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            ke[0] += 0.5 * mass[k] * (v.x[k] * v.x[k] + v.y[k] * v.y[k] + v.z[k] * v.z[k]);
+    }
+    grid_reduce<1>(ke, part, ticket, ke_out);
+}
+
+// SPC/E potential energy from the Ewald result slots (spce_forcefield.cpp:40):
+// disp + elrc + (real + reciprocal + self + intra); self = self_coef * sum q^2.
+__global__ void k_spce_total(const double* ew, double elrc, double self_coef, double* ev) {
+    // ew slots: 0 real, 1 W real, 2 lj, 3 W lj, 4 intra, 5 W intra, 6 recip, 7 W recip, 8 sum q^2
+    const double self = self_coef * ew[8];
+    ev[0] = ew[2] + elrc + (ew[0] + ew[6] + self + ew[4]);
+    ev[1] = ew[1] + ew[3] + ew[5] + ew[7];
+}
+
+Box3 box_of(const md_system* sys) {
+    Box3 b;
+    for (int d = 0; d < 3; ++d) {
+        b.L[d] = sys->box[d];
+        b.inv[d] = sys->inv_box[d];
+    }
+    return b;
+}
+
+CvvArgs cvv_args(const md_integrator* it, const md_system* sys) {
+    CvvArgs c;
+    c.dt = it->dt;
+    c.half_dt = 0.5 * it->dt;
+    c.inv_dt = 1.0 / it->dt;
+    c.ra = rigid_args(it->rigid);
+    c.box = box_of(sys);
+    return c;
+}
+
+int check_triples(const md_system* sys, const char* who) {
+    if (sys->n % 3 != 0)  // rigid_water.cpp:63-68
+        return fail(MD_ERR_RUNTIME, "%s: atom count is not a multiple of 3", who);
+    return MD_OK;
+}
+
+int ensure_counters(md_integrator* it) {
+    if (!it->counters.ptr) {
+        MDB_TRY(it->counters.ensure(4 * sizeof(int)));
+        MDB_CUDA(cudaMemset(it->counters.ptr, 0, 4 * sizeof(int)));
+    }
+    return MD_OK;
+}
+
+int status_to_error(md_context* ctx) {
+    uint32_t st = 0;
+    MDB_CUDA(cudaMemcpyAsync(&st, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    const uint32_t bits = MD_STATUS_SHAKE_DIVERGED | MD_STATUS_RATTLE_DIVERGED | MD_STATUS_SHAKE_SINGULAR;
+    if (st & bits) {
+        const uint32_t keep = st & ~bits;
+        MDB_CUDA(cudaMemcpyAsync(ctx->d_status, &keep, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+        MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+        // rigid_water.cpp:63-68, 100-104, 114-115, 159-160 throw std::runtime_error
+        if (st & MD_STATUS_SHAKE_SINGULAR)
+            return fail(MD_ERR_RUNTIME, "RigidWater: constraint became singular (bond rotated ~90 "
+                                        "degrees in one step); the timestep is far too large");
+        if (st & MD_STATUS_SHAKE_DIVERGED)
+            return fail(MD_ERR_RUNTIME, "RigidWater: SHAKE failed to converge");
+        return fail(MD_ERR_RUNTIME, "RigidWater: RATTLE failed to converge");
+    }
+    return MD_OK;
+}
+
+}  // namespace
+
+int constrained_pre_force(md_integrator* it, md_system* sys) {
+    MDB_TRY(check_triples(sys, "ConstrainedVelocityVerlet"));
+    MDB_TRY(ensure_counters(it));
+    md_context* ctx = sys->ctx;
+    const int64_t nmol = sys->n / 3;
+    NhcState* nhc = it->kind == 4 ? it->chain_state.as<NhcState>() : nullptr;
+    if (nhc) {
+        MDB_TRY(system_kinetic_async(sys, kResKE));
+        MDB_TRY(nhc_pre_async(it, ctx, ctx_result(ctx, kResKE)));
+    }
+    if (nmol > 0) {
+        k_cvv_pre<<<grid_for(nmol, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur, sys->slot, nmol, cvv_args(it, sys), nhc, it->counters.as<int>(), ctx->d_status);
+        ++ctx->launches;
+        MDB_CHECK_LAUNCH();
+    }
+    return status_to_error(ctx);
+}
+
+int constrained_post_force(md_integrator* it, md_system* sys, bool apply_scale) {
+    MDB_TRY(ensure_counters(it));
+    md_context* ctx = sys->ctx;
+    const int64_t nmol = sys->n / 3;
+    const int g = grid_for(std::max<int64_t>(nmol, 1), kBlock);
+    double* part;
+    MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
+    k_cvv_post<<<g, kBlock, 0, ctx->stream>>>(sys->cur, sys->slot, nmol, cvv_args(it, sys),
+                                             it->counters.as<int>() + 1, ctx->d_status, part,
+                                             ctx_counter(ctx, 8), ctx_result(ctx, kResKE));
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    if (it->kind == 4) {
+        MDB_TRY(nhc_post_async(it, ctx, ctx_result(ctx, kResKE)));
+        if (apply_scale) MDB_TRY(nhc_apply_scale_async(it, sys));
+    }
+    if (apply_scale) return status_to_error(ctx);
+    return MD_OK;
+}
+
+}  // namespace mdb
+
+using namespace mdb;
+
+extern "C" {
+
+int md_rigid_create(double oh, double hoh_degrees, double tolerance, int max_iterations,
+                    md_rigid** out) {
+    if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_create: NULL");
+    // rigid_water.cpp:38-49
+    if (!(oh > 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "RigidWater: ohDistance must be positive");
+    if (!(hoh_degrees > 0.0) || !(hoh_degrees < 180.0))
+        return fail(MD_ERR_INVALID_ARGUMENT, "RigidWater: hohAngleDegrees must lie in (0, 180)");
+    if (!(tolerance > 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "RigidWater: tolerance must be positive");
+    if (max_iterations < 1)
+        return fail(MD_ERR_INVALID_ARGUMENT, "RigidWater: maxIterations must be at least 1");
+    md_rigid* rw = new (std::nothrow) md_rigid();
+    if (!rw) return fail(MD_ERR_OUT_OF_MEMORY, "md_rigid_create: host allocation");
+    rw->oh = oh;
+    rw->tolerance = tolerance;
+    rw->max_iterations = max_iterations;
+    const double half_angle = 0.5 * hoh_degrees * kPi / 180.0;  // rigid_water.cpp:51-52
+    rw->hh = 2.0 * oh * std::sin(half_angle);
+    *out = rw;
+    return MD_OK;
+}
+
+int md_rigid_destroy(md_rigid* rw) {
+    delete rw;
+    return MD_OK;
+}
+
+int md_rigid_distances(const md_rigid* rw, double* oh, double* hh) {
+    if (!rw) return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_distances: NULL");
+    if (oh) *oh = rw->oh;
+    if (hh) *hh = rw->hh;
+    return MD_OK;
+}
+
+int64_t md_rigid_degrees_of_freedom(int64_t molecules, int com_removed) {
+    // rigid_water.cpp:55-59
+    const int64_t total = 6 * molecules;
+    return com_removed ? (total >= 3 ? total - 3 : 0) : total;
+}
+
+int md_rigid_constrain_positions(md_rigid* rw, md_system* sys, const double* rx,
+                                 const double* ry, const double* rz, int* iterations) {
+    if (!rw || !sys || !rx || !ry || !rz)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_constrain_positions: NULL argument");
+    MDB_TRY(check_triples(sys, "RigidWater"));
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n, nmol = n / 3;
+    DevBuf ref, cnt;
+    MDB_TRY(ref.ensure(3 * sizeof(double) * static_cast<size_t>(n > 0 ? n : 1)));
+    MDB_TRY(cnt.ensure(sizeof(int)));
+    double* d = ref.as<double>();
+    MDB_CUDA(cudaMemcpyAsync(d, rx, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    MDB_CUDA(cudaMemcpyAsync(d + n, ry, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    MDB_CUDA(cudaMemcpyAsync(d + 2 * n, rz, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    MDB_CUDA(cudaMemsetAsync(cnt.ptr, 0, sizeof(int), ctx->stream));
+    if (nmol > 0) {
+        k_shake<<<grid_for(nmol, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur, sys->slot, nmol, d, d + n, d + 2 * n, rigid_args(*rw), box_of(sys),
+            cnt.as<int>(), ctx->d_status);
+        ++ctx->launches;
+        MDB_CHECK_LAUNCH();
+    }
+    int it = 0;
+    MDB_CUDA(cudaMemcpyAsync(&it, cnt.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    const int rc = status_to_error(ctx);
+    ref.release();
+    cnt.release();
+    if (rc != MD_OK) return rc;
+    if (iterations) *iterations = nmol > 0 ? it : 1;
+    return MD_OK;
+}
+
+int md_rigid_constrain_velocities(md_rigid* rw, md_system* sys, int* iterations) {
+    if (!rw || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_constrain_velocities: NULL");
+    MDB_TRY(check_triples(sys, "RigidWater"));
+    md_context* ctx = sys->ctx;
+    const int64_t nmol = sys->n / 3;
+    DevBuf cnt;
+    MDB_TRY(cnt.ensure(sizeof(int)));
+    MDB_CUDA(cudaMemsetAsync(cnt.ptr, 0, sizeof(int), ctx->stream));
+    if (nmol > 0) {
+        k_rattle<<<grid_for(nmol, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur, sys->slot, nmol, rigid_args(*rw), box_of(sys), cnt.as<int>(), ctx->d_status);
+        ++ctx->launches;
+        MDB_CHECK_LAUNCH();
+    }
+    int it = 0;
+    MDB_CUDA(cudaMemcpyAsync(&it, cnt.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    const int rc = status_to_error(ctx);
+    cnt.release();
+    if (rc != MD_OK) return rc;
+    if (iterations) *iterations = nmol > 0 ? it : 1;
+    return MD_OK;
+}
+
+int md_integrator_create_rattle(double dt, const md_rigid* rw, md_integrator** out) {
+    if (!rw || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_rattle: NULL");
+    md_integrator* it = new (std::nothrow) md_integrator();
+    if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_rattle: host allocation");
+    it->kind = 3;
+    it->dt = dt;
+    it->rigid = *rw;
+    *out = it;
+    return MD_OK;
+}
+
+int md_integrator_create_rattle_nhc(double dt, const md_rigid* rw, double temperature, double tau,
+                                    int chain_length, int64_t dof, md_integrator** out) {
+    if (!rw || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_rattle_nhc: NULL");
+    MDB_TRY(md_integrator_create_nhc(dt, temperature, tau, chain_length, dof, out));
+    (*out)->kind = 4;
+    (*out)->rigid = *rw;
+    return MD_OK;
+}
+
+int md_integrator_iterations(md_integrator* it, int* shake, int* rattle) {
+    if (!it) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_iterations: NULL");
+    int h[2] = {0, 0};
+    if (it->counters.ptr) {
+        MDB_CUDA(cudaDeviceSynchronize());
+        MDB_CUDA(cudaMemcpy(h, it->counters.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    if (shake) *shake = h[0];
+    if (rattle) *rattle = h[1];
+    return MD_OK;
+}
+
+// Fused device loop of a constrained integrator with SPC/E forces.
+int md_run_spce(md_integrator* it, md_system* sys, md_ewald* ff, int64_t steps, double* thermo) {
+    if (!it || !sys || !ff) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_spce: NULL argument");
+    if (it->kind < 3) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_spce: needs a constrained integrator");
+    if (steps < 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_spce: steps < 0");
+    MDB_TRY(check_triples(sys, "md_run_spce"));
+    md_context* ctx = sys->ctx;
+    // Forces are made current on entry; this also builds the force field's
+    // neighbour list and topology once, host-side.
+    double e0, parts[8];
+    MDB_TRY(md_spce_compute(ff, sys, 1, &e0, parts));
+    MDB_TRY(ensure_counters(it));
+    double alpha = 0.0;
+    MDB_TRY(md_ewald_alpha(ff, &alpha));
+    const double elrc = parts[1];
+    const double self_coef = -md_coulomb_prefactor() * alpha / std::sqrt(kPi);
+    DevBuf rows;
+    if (thermo && steps > 0) MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
+    NhcState* nhc = it->kind == 4 ? it->chain_state.as<NhcState>() : nullptr;
+    const int64_t nmol = sys->n / 3;
+    if (nhc) MDB_TRY(system_kinetic_async(sys, kResKE));
+    const int g = grid_for(std::max<int64_t>(nmol, 1), kBlock);
+    double* part;
+    MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
+    for (int64_t k = 0; k < steps; ++k) {
+        if (nhc) MDB_TRY(nhc_pre_async(it, ctx, k == 0 ? ctx_result(ctx, kResKE) : nullptr));
+        if (nmol > 0) {
+            k_cvv_pre<<<grid_for(nmol, kBlock), kBlock, 0, ctx->stream>>>(
+                sys->cur, sys->slot, nmol, cvv_args(it, sys), nhc, it->counters.as<int>(),
+                ctx->d_status);
+            ++ctx->launches;
+        }
+        MDB_TRY(ewald_eval_async(ff, sys, 1, true));
+        k_spce_total<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEwald), elrc, self_coef,
+                                               ctx_result(ctx, kResEnergy));
+        k_cvv_post<<<g, kBlock, 0, ctx->stream>>>(sys->cur, sys->slot, nmol, cvv_args(it, sys),
+                                                 it->counters.as<int>() + 1, ctx->d_status, part,
+                                                 ctx_counter(ctx, 8), ctx_result(ctx, kResKE));
+        ctx->launches += 2;
+        if (nhc) MDB_TRY(nhc_post_async(it, ctx, ctx_result(ctx, kResKE)));
+        if (rows.ptr)
+            MDB_TRY(record_async(ctx, ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE), nhc,
+                                 rows.as<double>() + 4 * k));
+        MDB_CHECK_LAUNCH();
+    }
+    if (nhc && steps > 0) MDB_TRY(nhc_apply_scale_async(it, sys));
+    if (rows.ptr)
+        MDB_CUDA(cudaMemcpyAsync(thermo, rows.ptr, sizeof(double) * 4 * static_cast<size_t>(steps),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    rows.release();
+    MDB_TRY(status_to_error(ctx));
+    return ctx_check_status(ctx);
+}
+
+}  // extern "C"

@@ -46,6 +46,8 @@ struct RealArgs {
     double rc2, alpha, coulomb, two_alpha_over_sqrt_pi, neg_alpha2;
     int spce_lj;            // add O-O LJ (SPC/E)
     double sig2, four_eps, tf_eps;
+    int lj_lfs;             // O-O LJ with linear force shift at the cutoff
+    double rc, uc, dudrc;
 };
 
 // Real-space (and SPC/E O-O LJ) pair terms over the Verlet list.  out[0..3]:
@@ -95,10 +97,16 @@ k_ewald_real(const double4* __restrict__ pos, const double* __restrict__ q,
                 // lennard_jones.cpp:62-70 (Truncated)
                 const double s2 = a.sig2 / r2;
                 const double s6 = s2 * s2 * s2;
-                const double w = a.tf_eps * (2.0 * s6 * s6 - s6);
+                double w = a.tf_eps * (2.0 * s6 * s6 - s6);
+                double u = a.four_eps * (s6 * s6 - s6);
+                if (a.lj_lfs) {  // lennard_jones.cpp:73-77
+                    const double r = sqrt(r2);
+                    u = u - a.uc - (r - a.rc) * a.dudrc;
+                    w = w + r * a.dudrc;
+                }
                 s += w / r2;
                 if (lo) {
-                    el += a.four_eps * (s6 * s6 - s6);
+                    el += u;
                     wl += w;
                 }
             }
@@ -370,6 +378,7 @@ struct md_ewald {
     double skin = 1.0;
     bool spce = false;
     double sigma_o = 0, epsilon_o = 0;
+    int lj_truncation = MD_TRUNCATED;
     md_verlet* list = nullptr;
     double list_box[3] = {0, 0, 0};
     // topology (per original index)
@@ -477,6 +486,11 @@ int ewald_kvectors(md_ewald* ew, const double box[3], double alpha) {
     return MD_OK;
 }
 
+int ewald_list_gated(md_ewald* ew, md_system* sys) {
+    MDB_TRY(verlet_check(ew->list, sys));
+    return verlet_build(ew->list, sys, true);
+}
+
 int ewald_list(md_ewald* ew, md_system* sys) {
     if (ew->list && (ew->list_box[0] != sys->box[0] || ew->list_box[1] != sys->box[1] ||
                      ew->list_box[2] != sys->box[2])) {
@@ -502,15 +516,21 @@ int ewald_list(md_ewald* ew, md_system* sys) {
 
 // Everything of one evaluation, asynchronously; results land in kResEwald slots.
 // mode: 0 energies only, 1 zero + accumulate forces, 2 accumulate onto forces.
-int ewald_eval_async(md_ewald* ew, md_system* sys, int mode) {
+// gated: the neighbour list is maintained by device-decided rebuilds (no host
+// synchronisation; the list must already be built for this system).
+int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     double min_len = std::min(sys->box[0], std::min(sys->box[1], sys->box[2]));
     const double alpha = ew->alpha_in > 0.0 ? ew->alpha_in : 5.6 / min_len;  // ewald.cpp:40
     ew->alpha = alpha;
-    MDB_TRY(ewald_topology(ew, sys));
-    MDB_TRY(ewald_kvectors(ew, sys->box, alpha));
-    MDB_TRY(ewald_list(ew, sys));
+    if (gated) {
+        MDB_TRY(ewald_list_gated(ew, sys));
+    } else {
+        MDB_TRY(ewald_topology(ew, sys));
+        MDB_TRY(ewald_kvectors(ew, sys->box, alpha));
+        MDB_TRY(ewald_list(ew, sys));
+    }
     md_verlet* v = ew->list;
     RealArgs a;
     a.rc2 = ew->cutoff * ew->cutoff;
@@ -522,6 +542,14 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode) {
     a.sig2 = ew->sigma_o * ew->sigma_o;
     a.four_eps = 4.0 * ew->epsilon_o;
     a.tf_eps = 24.0 * ew->epsilon_o;
+    a.lj_lfs = ew->lj_truncation == MD_LINEAR_FORCE_SHIFT ? 1 : 0;
+    a.rc = ew->cutoff;
+    {
+        // lennard_jones.cpp:32-48
+        const double s2 = a.sig2 / a.rc2, s6 = s2 * s2 * s2;
+        a.uc = 4.0 * ew->epsilon_o * (s6 * s6 - s6);
+        a.dudrc = -(24.0 * ew->epsilon_o * (2.0 * s6 * s6 - s6)) / ew->cutoff;
+    }
     double* res = ctx_result(ctx, kResEwald);
     const Box3 box{{sys->box[0], sys->box[1], sys->box[2]},
                    {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}};
@@ -676,7 +704,7 @@ int md_ewald_compute(md_ewald* ew, md_system* sys, int mode, double terms[4], do
     if (!ew || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_compute: NULL argument");
     if (mode < 0 || mode > 2) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_compute: mode %d", mode);
     if (sys->ctx != ew->ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_compute: context mismatch");
-    MDB_TRY(ewald_eval_async(ew, sys, mode));
+    MDB_TRY(ewald_eval_async(ew, sys, mode, false));
     MDB_TRY(ewald_read(ew, sys->ctx));
     fill_terms(ew, terms, virial);
     return MD_OK;
@@ -704,12 +732,19 @@ int md_spce_create(md_context* ctx, double sigma_o, double epsilon_o, double cut
     return MD_OK;
 }
 
+int md_spce_set_lj_truncation(md_ewald* ew, int truncation) {
+    if (!ew || !ew->spce || (truncation != MD_TRUNCATED && truncation != MD_LINEAR_FORCE_SHIFT))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_spce_set_lj_truncation: bad argument");
+    ew->lj_truncation = truncation;
+    return MD_OK;
+}
+
 int md_spce_compute(md_ewald* ew, md_system* sys, int forces, double* energy, double parts[8]) {
     if (!ew || !sys || !ew->spce) return fail(MD_ERR_INVALID_ARGUMENT, "md_spce_compute: not an SPC/E force field");
     if (sys->n % 3 != 0)  // spce_forcefield.cpp:14-17
         return fail(MD_ERR_INVALID_ARGUMENT,
                     "SpceForceField: atom count is not a multiple of 3; expected O,H,H triples");
-    MDB_TRY(ewald_eval_async(ew, sys, forces ? 1 : 0));
+    MDB_TRY(ewald_eval_async(ew, sys, forces ? 1 : 0, false));
     MDB_TRY(ewald_read(ew, sys->ctx));
     double terms[4], vir;
     fill_terms(ew, terms, &vir);
@@ -719,8 +754,10 @@ int md_spce_compute(md_ewald* ew, md_system* sys, int forces, double* energy, do
     const double sr = ew->sigma_o / ew->cutoff;
     const double sr3 = sr * sr * sr, sr9 = sr3 * sr3 * sr3;
     const double sig3 = ew->sigma_o * ew->sigma_o * ew->sigma_o;
-    const double elrc =
-        (8.0 / 3.0) * kPi * m * rho * ew->epsilon_o * sig3 * ((1.0 / 3.0) * sr9 - sr3);
+    const double elrc = ew->lj_truncation == MD_LINEAR_FORCE_SHIFT
+                            ? 0.0
+                            : (8.0 / 3.0) * kPi * m * rho * ew->epsilon_o * sig3 *
+                                  ((1.0 / 3.0) * sr9 - sr3);
     const double disp = ew->last[kEwLj];
     // spce_forcefield.cpp:40: disp + elrc + total()
     const double total = disp + elrc + (terms[0] + terms[1] + terms[2] + terms[3]);

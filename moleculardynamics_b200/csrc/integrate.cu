@@ -255,7 +255,7 @@ int kick_grid(const md_system* sys) {
 }
 
 NhcState* nhc_of(md_integrator* it) {
-    return it->kind == 2 ? it->chain_state.as<NhcState>() : nullptr;
+    return (it->kind == 2 || it->kind == 4) ? it->chain_state.as<NhcState>() : nullptr;
 }
 
 // The pre-force half of a step.  With `check` the rebuild test of that Verlet
@@ -332,6 +332,45 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 
+// Chain-of-thermostats pieces shared with the constrained integrators.
+int nhc_pre_async(md_integrator* it, md_context* ctx, const double* ke_now) {
+    k_nhc_pre<<<1, 1, 0, ctx->stream>>>(it->chain_state.as<NhcState>(), ke_now, yoshida());
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int nhc_post_async(md_integrator* it, md_context* ctx, const double* ke_sum) {
+    k_nhc_post<<<1, 1, 0, ctx->stream>>>(it->chain_state.as<NhcState>(), ke_sum, yoshida());
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int nhc_apply_scale_async(md_integrator* it, md_system* sys) {
+    md_context* ctx = sys->ctx;
+    NhcState* nhc = it->chain_state.as<NhcState>();
+    if (sys->n > 0) {
+        k_scale<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n, nhc);
+        ++ctx->launches;
+    }
+    k_reset_scale<<<1, 1, 0, ctx->stream>>>(nhc);
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int record_async(md_context* ctx, const double* ev, const double* ke, const NhcState* nhc,
+                 double* row) {
+    k_record<<<1, 1, 0, ctx->stream>>>(ev, ke, nhc, row);
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int constrained_pre_force(md_integrator* it, md_system* sys);
+int constrained_post_force(md_integrator* it, md_system* sys, bool apply_scale);
+
 }  // namespace mdb
 
 using namespace mdb;
@@ -403,23 +442,27 @@ int md_integrator_destroy(md_integrator* it) {
     cudaDeviceSynchronize();
     it->chain_state.release();
     it->noise.release();
+    it->mol_state.release();
+    it->counters.release();
     delete it;
     return MD_OK;
 }
 
 int md_integrator_pre_force(md_integrator* it, md_system* sys) {
     if (!it || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_pre_force: NULL");
+    if (it->kind >= 3) return constrained_pre_force(it, sys);
     return pre_force(it, sys, nullptr);
 }
 
 int md_integrator_post_force(md_integrator* it, md_system* sys) {
     if (!it || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_post_force: NULL");
+    if (it->kind >= 3) return constrained_post_force(it, sys, true);
     return post_force_async(it, sys, true);
 }
 
 int md_integrator_conserved(md_integrator* it, double* value) {
     if (!it || !value) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_conserved: NULL");
-    if (it->kind != 2) {
+    if (it->kind != 2 && it->kind != 4) {
         *value = 0.0;
         return MD_OK;
     }
@@ -454,6 +497,8 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
     if (!it || !sys || !v || !lj) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: NULL argument");
     if (steps < 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: steps < 0");
     MDB_TRY(verlet_ensure_ready(v, sys, "md_run_lj"));
+    if (it->kind >= 3)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: constrained integrators run with md_run_spce");
     md_context* ctx = sys->ctx;
     DevBuf rows;
     if (thermo && steps > 0) MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));

@@ -221,8 +221,16 @@ int system_kinetic_async(md_system* sys, int slot);
 }  // namespace mdb
 
 // ------------------------------------------------------------- integrators
+struct md_rigid {
+    double oh = 1.0, hh = 0.0, tolerance = 1e-12;
+    int max_iterations = 500;
+};
+
 struct md_integrator {
-    int kind = 0;                 // 0 VV, 1 BAOAB, 2 NHC
+    int kind = 0;                 // 0 VV, 1 BAOAB, 2 NHC, 3 constrained VV, 4 constrained VV + NHC
+    md_rigid rigid;               // constraint of kinds 3 and 4
+    mdb::DevBuf mol_state;        // kinds 3/4: per-molecule scratch (unconstrained positions)
+    mdb::DevBuf counters;         // kinds 3/4: device iteration maxima
     double dt = 0.005;
     // BAOAB
     double friction = 1.0, temperature = 1.0;

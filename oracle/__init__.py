@@ -63,6 +63,12 @@ class OrcEwaldTerms(C.Structure):
                 ("intra", C.c_double)]
 
 
+class OrcNhc(C.Structure):
+    _fields_ = [("dt", C.c_double), ("temperature", C.c_double), ("tau", C.c_double),
+                ("chain_length", C.c_int), ("dof", C.c_int64), ("Q", C.c_double * 16),
+                ("xi", C.c_double * 16), ("pxi", C.c_double * 16)]
+
+
 class OrcRigidWater(C.Structure):
     _fields_ = [("oh", C.c_double), ("hh", C.c_double), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int)]
@@ -147,6 +153,13 @@ def lib():
         L.orc_rigid_water_velocities.restype = C.c_int
         L.orc_rigid_water_velocities.argtypes = [C.POINTER(OrcRigidWater), C.c_int64, _d, _d,
                                                  _d, _d, _d, _d, _d, _d]
+        L.orc_nhc_init.restype = C.c_int
+        L.orc_nhc_init.argtypes = [C.POINTER(OrcNhc), C.c_double, C.c_double, C.c_double,
+                                   C.c_int, C.c_int64]
+        L.orc_nhc_chain.restype = None
+        L.orc_nhc_chain.argtypes = [C.POINTER(OrcNhc), C.c_int64, _d, _d, _d, _d, C.c_double]
+        L.orc_nhc_conserved.restype = C.c_double
+        L.orc_nhc_conserved.argtypes = [C.POINTER(OrcNhc)]
         _lib = L
     return _lib
 
@@ -427,6 +440,26 @@ def rattle(rw, pos, vel, mass, box):
     it = lib().orc_rigid_water_velocities(C.byref(rw), n, _p(_f64(box)), _p(_f64(mass)),
                                           *[_p(c) for c in pcols], *[_p(c) for c in vcols])
     return np.stack(vcols, 1), it
+
+
+def nhc(dt, temperature, tau, chain_length, dof):
+    """NoseHooverChain state (nose_hoover.cpp:15-43)."""
+    c = OrcNhc()
+    if lib().orc_nhc_init(C.byref(c), dt, temperature, tau, chain_length, dof) != 0:
+        raise ValueError("NoseHooverChain: chainLength must be >= 1")
+    return c
+
+
+def nhc_chain(c, vel, mass, delta):
+    """integrateChain(delta) (nose_hoover.cpp:59-124) on a copy of vel; returns it."""
+    vel = _f64(vel)
+    cols = [np.ascontiguousarray(vel[:, k]) for k in range(3)]
+    lib().orc_nhc_chain(C.byref(c), vel.shape[0], _p(_f64(mass)), *[_p(a) for a in cols], delta)
+    return np.stack(cols, 1)
+
+
+def nhc_conserved(c):
+    return lib().orc_nhc_conserved(C.byref(c))
 
 
 def read_nist_config(path):

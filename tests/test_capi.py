@@ -59,3 +59,24 @@ def test_invalid_arguments_map_to_reference_exceptions():
     rc = md.lib().md_integrator_create_nhc(0.002, 1.0, 0.5, 0, 10, C.byref(h))
     assert rc == md.MD_ERR_INVALID_ARGUMENT
     assert b"chainLength" in md.lib().md_last_error()
+
+
+def test_rigid_water_host_side():
+    """RigidWater's constructor checks and target distances (rigid_water.cpp:30-59)
+    run on the host: invalid parameters raise InvalidArgument, the H-H target
+    and the degrees of freedom match the oracle."""
+    import moleculardynamics_b200 as md
+    import pytest
+
+    import oracle as O
+    for bad in ((0.0, 109.47), (1.0, 0.0), (1.0, 180.0)):
+        with pytest.raises(md.InvalidArgument):
+            md.RigidWater(*bad)
+    with pytest.raises(md.InvalidArgument):
+        md.RigidWater(1.0, 109.47, 0.0)
+    with pytest.raises(md.InvalidArgument):
+        md.RigidWater(1.0, 109.47, 1e-12, 0)
+    rw, orw = md.RigidWater(1.0, 109.47), O.rigid_water(1.0, 109.47)
+    assert rw.oh_distance() == orw.oh and rw.hh_distance() == orw.hh
+    assert md.RigidWater.degrees_of_freedom(100, True) == 597
+    assert md.RigidWater.degrees_of_freedom(0, True) == 0
