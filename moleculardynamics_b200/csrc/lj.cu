@@ -23,6 +23,8 @@ namespace {
 struct LJArgs {
     double sig2, rc2, rc, uc, dudrc, four_eps, tf_eps;
     float sig2f, rc2f, rcf, ucf, dudrcf, four_epsf, tf_epsf;
+    double res[3];  // fixed-point resolution per axis, L / 2^32 (mixed path)
+    double band;    // |r^2 - rc^2| below which the mixed path decides exactly
 };
 
 LJArgs make_lj_args(const md_lj* lj) {
@@ -41,6 +43,8 @@ LJArgs make_lj_args(const md_lj* lj) {
     a.dudrcf = static_cast<float>(a.dudrc);
     a.four_epsf = static_cast<float>(a.four_eps);
     a.tf_epsf = static_cast<float>(a.tf_eps);
+    a.res[0] = a.res[1] = a.res[2] = 0.0;
+    a.band = 0.0;
     return a;
 }
 
@@ -92,21 +96,53 @@ __device__ __forceinline__ void accumulate_exact(const LJArgs& a, const Fold3& f
     }
 }
 
-// Mixed precision: the minimum-image displacement and r^2 in FP64 (r^2 is the
-// quantity the r^-14 force steepness amplifies, so it is rounded to FP32 once,
-// after it is formed); r^-2, r^-6, energy and force magnitude in FP32; the force
-// vector assembled and accumulated in FP64, as are energy and virial.
-template <bool LFS>
-__device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Fold3& f3, double4 pi,
-                                                 double4 pj, double& fx, double& fy, double& fz,
-                                                 double& e, double& vir) {
-    // wrapped coordinates: |d| < L, so the nearest image is one compare away
-    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    if (fabs(dx) > f3.b[0].lo) dx -= copysign(f3.b[0].L, dx);
-    if (fabs(dy) > f3.b[1].lo) dy -= copysign(f3.b[1].L, dy);
-    if (fabs(dz) > f3.b[2].lo) dz -= copysign(f3.b[2].L, dz);
+// Mixed precision.  Positions are gathered as int32 fixed point with the box
+// length mapped to 2^32 per axis (resolution L / 2^32: 2.5e-8 for the
+// 1,048,576-atom liquid's L = 107.5), so the minimum image is the wrap-around of
+// an int32 difference and a neighbour is one 16-byte load.  The displacement and
+// r^2 are formed in FP64 from the exact integer difference (r^2 is the quantity
+// the r^-14 force steepness amplifies, so it is rounded to FP32 once, after it
+// is formed); r^-2, r^-6, energy and force magnitude in FP32; the force vector
+// assembled and accumulated in FP64, as are energy and virial.
+__device__ __forceinline__ int wrap_diff(int a, int b) {
+    return static_cast<int>(static_cast<unsigned>(a) - static_cast<unsigned>(b));
+}
+
+// A pair whose fixed-point r^2 lies within a.band of rc^2 could fall on the other
+// side of the cutoff than in the FP64 path (a truncated potential jumps there),
+// so it is decided by the reference arithmetic on the FP64 positions: the mixed
+// path sums exactly the FP64 path's pairs.  The band is several times the
+// largest r^2 change the quantisation can cause, so such pairs are rare; the
+// main loop only flags them (keeping its register budget) and a second pass
+// over the thread's share of the row settles them.
+__device__ __forceinline__ bool inside_exact(const LJArgs& a, const Fold3& f3,
+                                             const double4* __restrict__ pd, int i, int j) {
+    const double4 p = ldg4(pd + i), q = ldg4(pd + j);
+    double dx, dy, dz;
+    if (p.w < q.w) min_image_wrapped(f3, p.x, p.y, p.z, q.x, q.y, q.z, dx, dy, dz);
+    else min_image_wrapped(f3, q.x, q.y, q.z, p.x, p.y, p.z, dx, dy, dz);
+    return norm2_exact(dx, dy, dz) < a.rc2;
+}
+
+// NEAR = false: the main loop (pairs in the band are skipped and flagged);
+// NEAR = true: the second pass (only pairs in the band, decided exactly).
+template <bool LFS, bool NEAR>
+__device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Fold3& f3,
+                                                 const double4* __restrict__ pd, int i, int j,
+                                                 int4 qi, int4 qj, double& fx, double& fy,
+                                                 double& fz, double& e, double& vir, bool& near) {
+    const double dx = static_cast<double>(wrap_diff(qi.x, qj.x)) * a.res[0];
+    const double dy = static_cast<double>(wrap_diff(qi.y, qj.y)) * a.res[1];
+    const double dz = static_cast<double>(wrap_diff(qi.z, qj.z)) * a.res[2];
     const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-    if (!(r2 < a.rc2)) return;
+    if (!(r2 < a.rc2 + a.band)) return;
+    const bool in_band = r2 > a.rc2 - a.band;
+    if (NEAR) {
+        if (!in_band || !inside_exact(a, f3, pd, i, j)) return;
+    } else if (in_band) {
+        near = true;
+        return;
+    }
     const float r2f = static_cast<float>(r2);
     const float inv = __frcp_rn(r2f);
     const float s2 = a.sig2f * inv;
@@ -122,7 +158,7 @@ __device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Fold3& f
     fx = fma(dx, s, fx);
     fy = fma(dy, s, fy);
     fz = fma(dz, s, fz);
-    if (pi.w < pj.w) {
+    if (qi.w < qj.w) {
         e += static_cast<double>(u);
         vir += static_cast<double>(w);
     }
@@ -138,19 +174,34 @@ struct UnrollBlocks {
     static constexpr int value = U >= 4 ? 2 : 4;
 };
 
+// Position source of the pair kernel: FP64 double4 for the reference arithmetic,
+// int32 fixed point for the mixed path.
+template <bool MIXED>
+struct PosOf {
+    using T = double4;
+    static __device__ __forceinline__ T load(const T* p) { return ldg4(p); }
+};
+template <>
+struct PosOf<true> {
+    using T = int4;
+    static __device__ __forceinline__ T load(const T* p) { return __ldg(p); }
+};
+
 template <int TPA, bool MIXED, bool LFS, int U>
 __global__ void __launch_bounds__(kBlock, UnrollBlocks<U>::value)
-k_lj_verlet(const double4* __restrict__ pos, const int* __restrict__ nbr,
-            const int* __restrict__ count, int stride, int64_t n, Box3 box, LJArgs a,
-            double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
-            double* part, unsigned* ticket, double* out) {
+k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
+            const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
+            Box3 box, LJArgs a, double* __restrict__ fxo, double* __restrict__ fyo,
+            double* __restrict__ fzo, double* part, unsigned* ticket, double* out) {
+    using P = PosOf<MIXED>;
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t i = t / TPA;
     const int g = static_cast<int>(t % TPA);
     const Fold3 f3 = fold3_of(box);
     double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
+    bool near = false;
     if (i < n) {
-        const double4 pi = pos[i];
+        const typename P::T pi = P::load(pos + i);
         const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
         const int* row = nbr + i * static_cast<int64_t>(stride);
         // U independent index->position gather chains in flight per thread; the
@@ -160,19 +211,33 @@ k_lj_verlet(const double4* __restrict__ pos, const int* __restrict__ nbr,
             int j[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) j[u] = __ldg(row + k + u * TPA);
-            double4 pj[U];
+            typename P::T pj[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) pj[u] = ldg4(pos + j[u]);
+            for (int u = 0; u < U; ++u) pj[u] = P::load(pos + j[u]);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (MIXED) accumulate_mixed<LFS>(a, f3, pi, pj[u], fx, fy, fz, e, vir);
+                if constexpr (MIXED)
+                    accumulate_mixed<LFS, false>(a, f3, pd, static_cast<int>(i), j[u], pi, pj[u],
+                                                 fx, fy, fz, e, vir, near);
                 else accumulate_exact<LFS>(a, f3, pi, pj[u], fx, fy, fz, e, vir);
             }
         }
         for (; k < cnt; k += TPA) {
-            const double4 pj = ldg4(pos + __ldg(row + k));
-            if (MIXED) accumulate_mixed<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
+            const int j = __ldg(row + k);
+            const typename P::T pj = P::load(pos + j);
+            if constexpr (MIXED)
+                accumulate_mixed<LFS, false>(a, f3, pd, static_cast<int>(i), j, pi, pj, fx, fy, fz,
+                                             e, vir, near);
             else accumulate_exact<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
+        }
+        if constexpr (MIXED) {
+            if (near) {  // rare: settle the pairs next to the cutoff
+                for (int kk = g; kk < cnt; kk += TPA) {
+                    const int j = __ldg(row + kk);
+                    accumulate_mixed<LFS, true>(a, f3, pd, static_cast<int>(i), j, pi,
+                                                P::load(pos + j), fx, fy, fz, e, vir, near);
+                }
+            }
         }
     }
 #pragma unroll
@@ -287,9 +352,26 @@ template <int TPA, bool MIXED, bool LFS, int U>
 void launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
                    double* out) {
     const int64_t threads = sys->n * TPA;
+    const typename PosOf<MIXED>::T* pos;
+    if constexpr (MIXED) pos = sys->qpos.as<int4>();
+    else pos = sys->cur.pos;
     k_lj_verlet<TPA, MIXED, LFS, U><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
-        sys->cur.pos, v->nbr.as<int>(), v->count.as<int>(), v->stride, sys->n, box_of(sys), a,
+        pos, sys->cur.pos, v->nbr.as<int>(), v->count.as<int>(), v->stride, sys->n, box_of(sys), a,
         sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+}
+
+// Fixed-point positions for the mixed pair kernel: q = round(x 2^32 / L) taken
+// modulo 2^32 (so unwrapped coordinates land on their periodic image), w = the
+// original index.
+__global__ void k_quantize(const double4* __restrict__ pos, int64_t n, double sx, double sy,
+                           double sz, int4* __restrict__ q) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const double4 p = pos[k];
+    q[k] = make_int4(static_cast<int>(static_cast<unsigned>(llrint(p.x * sx))),
+                     static_cast<int>(static_cast<unsigned>(llrint(p.y * sy))),
+                     static_cast<int>(static_cast<unsigned>(llrint(p.z * sz))),
+                     static_cast<int>(p.w));
 }
 
 template <int TPA, bool MIXED, bool LFS>
@@ -320,7 +402,14 @@ int g_lj_unroll = 2;  // independent gather chains per thread (tunable)
 
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     md_context* ctx = sys->ctx;
-    const LJArgs a = make_lj_args(lj);
+    LJArgs a = make_lj_args(lj);
+    double res_max = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        a.res[d] = sys->box[d] / 4294967296.0;
+        res_max = std::max(res_max, a.res[d]);
+    }
+    // |r^2 error| <= 2 r |d error| + rounding, |d error| <= sqrt(3) res: 4x margin
+    a.band = 8.0 * 1.7320508075688772 * a.rc * res_max + 1e-12 * a.rc2;
     const int64_t threads = std::max<int64_t>(sys->n * g_lj_tpa, 1);
     const int blocks = grid_for(threads, kBlock);
     double* part;
@@ -329,6 +418,14 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     double* out = ctx_result(ctx, kResEnergy);
     const bool lfs = lj->truncation == MD_LINEAR_FORCE_SHIFT;
     const bool mixed = lj->precision == MD_PRECISION_MIXED;
+    if (mixed && sys->n > 0) {
+        MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(sys->n)));
+        const double two32 = 4294967296.0;
+        k_quantize<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->n, two32 / sys->box[0], two32 / sys->box[1], two32 / sys->box[2],
+            sys->qpos.as<int4>());
+        ++ctx->launches;
+    }
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     if (mixed) {
         if (lfs) launch_verlet_tpa<true, true>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);

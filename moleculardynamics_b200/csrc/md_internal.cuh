@@ -136,6 +136,10 @@ struct md_system {
     bool has_molecules = false;  // molecule ids differ from the atom's own index
     uint64_t mol_version = 1;    // bumped whenever molecule ids are set
     double last_energy = 0.0, last_virial = 0.0;
+    // Fixed-point copy of the positions for the mixed-precision pair kernel: per
+    // axis the box length maps to 2^32, so x, y, z are int32 (w = original index)
+    // and one 16-byte load fetches a neighbour; written before each mixed launch.
+    mdb::DevBuf qpos;
 };
 
 namespace mdb {

@@ -340,45 +340,25 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                 c = wb == 0 ? 0 : count[i];
             }
             int* row = nbr + static_cast<int64_t>(active ? i : 0) * stride;
-            int t = 0;
-            for (; t + 4 <= wlen; t += 4) {  // four independent candidate tests in flight
-                float4 q[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) q[u] = s_p[warp][t + u];
-                bool hit[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const float dx = fx - q[u].x, dy = fy - q[u].y, dz = fz - q[u].z;
-                    hit[u] = dx * dx + dy * dy + dz * dz < lo_thr;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int j = __float_as_int(q[u].w);
-                    bool h = hit[u];
-                    if (!h) {
-                        const float dx = fx - q[u].x, dy = fy - q[u].y, dz = fz - q[u].z;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 <= hi_thr && active && j != i)
-                            h = within(g.box, pi, ldg4(pos + j), rl2);
-                    }
-                    if (h && active && j != i) {
-                        if (c < stride) row[c] = j;
-                        ++c;
-                    }
-                }
-            }
-            for (; t < wlen; ++t) {
+            // Per candidate: an FP32 distance test and a predicated append.  The
+            // few candidates within the 2^-12 band around the cutoff are decided
+            // by the exact reference arithmetic in place (so rows keep stencil
+            // order); the band check is one warp vote, taken only when some lane
+            // of the warp has such a candidate.
+#pragma unroll 4
+            for (int t = 0; t < wlen; ++t) {
                 const float4 q = s_p[warp][t];
                 const int j = __float_as_int(q.w);
                 const float dx = fx - q.x, dy = fy - q.y, dz = fz - q.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 bool hit = r2 < lo_thr;
-                if (!hit && r2 <= hi_thr && active && j != i)
-                    hit = within(g.box, pi, ldg4(pos + j), rl2);
-                if (hit && active && j != i) {
-                    if (c < stride) row[c] = j;
-                    ++c;
+                const bool near = active && !hit && r2 <= hi_thr;
+                if (__any_sync(0xffffffffu, near)) {
+                    if (near) hit = within(g.box, pi, ldg4(pos + j), rl2);
                 }
+                hit = hit && active && j != i;
+                if (hit && c < stride) row[c] = j;
+                c += hit ? 1 : 0;
             }
             if (active) {
                 count[i] = c;

@@ -238,6 +238,7 @@ int md_system_destroy(md_system* sys) {
     system_free_atoms(&sys->cur);
     system_free_atoms(&sys->alt);
     if (sys->slot) cudaFree(sys->slot);
+    sys->qpos.release();
     delete sys;
     return MD_OK;
 }
