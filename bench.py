@@ -204,8 +204,6 @@ def timed_run(md, ctx, box, pos, vel, frc, precision, steps, warmup, group, cloc
     launches0 = ctx.launch_count()
     rebuild0 = v.rebuild_count()
     _check = md._check
-    _check(L.md_context_set_timing(ctx.handle, 1))
-    L.md_context_kernel_time(ctx.handle, md.MD_KERNEL_LJ_FORCE, 1, None, None)
     sampler = clocks.__enter__() if clocks else None
     _check(L.md_context_span_begin(ctx.handle))
     rows = integ.run(s, v, lj, steps, thermo=True)
@@ -213,16 +211,23 @@ def timed_run(md, ctx, box, pos, vel, frc, precision, steps, warmup, group, cloc
     _check(L.md_context_span_end(ctx.handle, C.byref(ms)))
     if sampler:
         clocks.__exit__(None, None, None)
+    ctx.synchronize()
+    group.barrier()
+    launches = ctx.launch_count() - launches0
+    rebuilds = v.rebuild_count() - rebuild0
+    # The force kernel's own duration: CUDA events around each of its launches on
+    # the context stream, over a further run of the same loop with per-kernel
+    # timing on (that run launches every kernel from the host, so it is not the
+    # timed region above).
+    _check(L.md_context_set_timing(ctx.handle, 1))
+    L.md_context_kernel_time(ctx.handle, md.MD_KERNEL_LJ_FORCE, 1, None, None)
+    integ.run(s, v, lj, min(steps, 50))
     kms = C.c_double()
     kl = C.c_int64()
     _check(L.md_context_kernel_time(ctx.handle, md.MD_KERNEL_LJ_FORCE, 1, C.byref(kms), C.byref(kl)))
     _check(L.md_context_set_timing(ctx.handle, 0))
-    ctx.synchronize()
-    group.barrier()
-    launches = ctx.launch_count() - launches0
     pairs = v.pairs()
     nbr_per_atom = 2.0 * len(pairs) / s.n
-    rebuilds = v.rebuild_count() - rebuild0
     dev_ms = group.reduce(ms.value, "max")
     per_launch = kms.value / max(kl.value, 1)
     return dev_ms, rows, per_launch, launches, nbr_per_atom, rebuilds
@@ -409,9 +414,10 @@ def run_gpu_arm(args):
 
     if rank == 0:
         peaks, peak_src = measured_peaks()
-        # algorithmic bytes of one force launch per atom: own position (32 B) + force
-        # write (24 B) + the half neighbour list (4 B per unique pair)
-        alg_per_atom = 32.0 + 24.0 + 4.0 * nbr / 2.0
+        # algorithmic bytes of one mixed force launch per atom: own fixed-point
+        # position (16 B) + force write (24 B) + the half neighbour list (4 B per
+        # unique pair)
+        alg_per_atom = 16.0 + 24.0 + 4.0 * nbr / 2.0
         achieved = alg_per_atom * n / (kmx * 1e-3) / 1e9
         tpa = traffic_per_atom()
         e0_64 = rows64[0, 0] + rows64[0, 2]

@@ -107,6 +107,11 @@ MD_API int md_context_launch_count(md_context* ctx, int64_t* count);
 #define MD_KERNEL_EWALD_REAL 3   /* Ewald real-space pairs */
 #define MD_KERNEL_EWALD_RECIP 4  /* Ewald structure factors and k-space forces */
 MD_API int md_context_set_timing(md_context* ctx, int enable);
+/* Fused device loops (md_run_lj) replay one captured CUDA graph per step, the
+ * device-decided neighbour rebuild being a conditional node, when enabled
+ * (default) and timing is off; 0 launches every kernel from the host instead.
+ * Results are identical either way.  No reference counterpart. */
+MD_API int md_context_set_graphs(md_context* ctx, int enable);
 MD_API int md_context_kernel_time(md_context* ctx, int kernel, int reset, double* total_ms,
                                   int64_t* launches);
 /* Device time between two points on the context's stream (CUDA events). */

@@ -84,6 +84,7 @@ def _load():
         "md_context_status": (C.c_int, [_vp, C.POINTER(C.c_uint32), C.c_int]),
         "md_context_launch_count": (C.c_int, [_vp, _i64p]),
         "md_context_set_timing": (C.c_int, [_vp, C.c_int]),
+        "md_context_set_graphs": (C.c_int, [_vp, C.c_int]),
         "md_context_kernel_time": (C.c_int, [_vp, C.c_int, C.c_int, _d, _i64p]),
         "md_context_span_begin": (C.c_int, [_vp]),
         "md_context_span_end": (C.c_int, [_vp, _d]),
@@ -225,6 +226,11 @@ class Context:
         c = C.c_int64()
         _check(lib().md_context_launch_count(self._h, C.byref(c)))
         return c.value
+
+    def set_graphs(self, enable: bool):
+        """Fused loops replay one captured CUDA graph per step (default) or launch
+        every kernel from the host; results are identical."""
+        _check(lib().md_context_set_graphs(self._h, 1 if enable else 0))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -209,6 +209,12 @@ int md_context_set_timing(md_context* ctx, int enable) {
     return MD_OK;
 }
 
+int md_context_set_graphs(md_context* ctx, int enable) {
+    if (!ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_set_graphs: NULL");
+    ctx->graphs = enable != 0;
+    return MD_OK;
+}
+
 int md_context_kernel_time(md_context* ctx, int kernel, int reset, double* total_ms,
                            int64_t* launches) {
     if (!ctx || kernel < 0 || kernel >= kTimedKernels)

@@ -9,6 +9,7 @@
 // next kick.
 #include <cmath>
 #include <new>
+#include <vector>
 
 #include "md_device.cuh"
 #include "md_internal.cuh"
@@ -224,6 +225,22 @@ __global__ void k_record(const double* ev, const double* ke, const NhcState* nhc
 
 __global__ void k_conserved(const NhcState* nhc, double* out) { *out = nhc_conserved(*nhc); }
 
+// Thermo row at a device-held index (graph replays cannot change a pointer).
+__global__ void k_record_at(const double* ev, const double* ke, const NhcState* nhc, double* rows,
+                            int* idx) {
+    double* row = rows + 4 * static_cast<int64_t>(*idx);
+    row[0] = ev[0];
+    row[1] = ev[1];
+    row[2] = nhc ? nhc->ke : *ke;
+    row[3] = nhc ? nhc_conserved(*nhc) : 0.0;
+    ++*idx;
+}
+
+// Opens the rebuild branch of a step graph when the fused check asked for one.
+__global__ void k_set_rebuild(cudaGraphConditionalHandle h, const int* flag) {
+    cudaGraphSetConditional(h, *flag != 0 ? 1u : 0u);
+}
+
 Weights yoshida() {
     // nose_hoover.cpp:15-18
     const double w1 = 1.0 / (2.0 - std::cbrt(2.0));
@@ -260,7 +277,10 @@ NhcState* nhc_of(md_integrator* it) {
 
 // The pre-force half of a step.  With `check` the rebuild test of that Verlet
 // list is fused into the position update (fused stepping loops).
-int pre_force(md_integrator* it, md_system* sys, md_verlet* check) {
+// fresh_ke: the chain half of a Nose-Hoover step sums the kinetic energy of the
+// current velocities; otherwise it uses the value the chain tracked through the
+// previous step's rescalings (fused loops, after their first step).
+int pre_force(md_integrator* it, md_system* sys, md_verlet* check, bool fresh_ke = true) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     if (n == 0) return MD_OK;
@@ -285,9 +305,10 @@ int pre_force(md_integrator* it, md_system* sys, md_verlet* check) {
     } else {
         NhcState* nhc = nhc_of(it);
         if (nhc) {
-            // start-of-step chain half needs the current kinetic energy
-            MDB_TRY(system_kinetic_async(sys, kResKE));
-            k_nhc_pre<<<1, 1, 0, ctx->stream>>>(nhc, ctx_result(ctx, kResKE), yoshida());
+            // start-of-step chain half (integrateChain(dt/2), nose_hoover.hpp:37-42)
+            if (fresh_ke) MDB_TRY(system_kinetic_async(sys, kResKE));
+            k_nhc_pre<<<1, 1, 0, ctx->stream>>>(nhc, fresh_ke ? ctx_result(ctx, kResKE) : nullptr,
+                                                yoshida());
             ctx->launches += 1;
         }
         if (check) k_kick_drift<true><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
@@ -331,6 +352,111 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
 
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
+
+// ------------------------------------------------------------ step graphs
+// One fused LJ step captured as a CUDA graph: [chain half,] kick/drift with the
+// displacement check, a conditional node whose body is the gated neighbour
+// rebuild (opened by k_set_rebuild from the device flag, so steps without a
+// rebuild launch none of its kernels), forces, the closing kick and the thermo
+// row.  Replaying it runs the same kernels with the same arguments as the host
+// loop.
+struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t main_launches = 0;  // kernels outside the rebuild branch
+    int64_t body_launches = 0;  // kernels inside it
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+};
+
+// Captures work() on the context stream into graph g after the given nodes; on
+// return the stream is out of capture whatever happened.  leaves (optional)
+// receives the last captured nodes.
+template <class F>
+int capture_into(md_context* ctx, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
+                 F&& work, std::vector<cudaGraphNode_t>* leaves) {
+    MDB_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, g, deps, nullptr, ndeps,
+                                           cudaStreamCaptureModeThreadLocal));
+    int rc = work();
+    if (rc == MD_OK && leaves) {
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* out = nullptr;
+        size_t nout = 0;
+        const cudaError_t e =
+            cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, nullptr, &out, &nout);
+        if (e != cudaSuccess) rc = fail(MD_ERR_CUDA, "capture info: %s", cudaGetErrorString(e));
+        else leaves->assign(out, out + nout);
+    }
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
+    if (rc != MD_OK) return rc;
+    if (e != cudaSuccess) return fail(MD_ERR_CUDA, "step graph capture: %s", cudaGetErrorString(e));
+    return MD_OK;
+}
+
+int capture_lj_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
+                    int* idx, StepGraph& sg) {
+    md_context* ctx = sys->ctx;
+    NhcState* nhc = nhc_of(it);
+    const int64_t l0 = ctx->launches;
+    int rc = MD_OK;
+    if (cudaGraphCreate(&sg.graph, 0) != cudaSuccess)
+        return fail(MD_ERR_CUDA, "cudaGraphCreate failed");
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, sg.graph, 0, cudaGraphCondAssignDefault) !=
+        cudaSuccess) {
+        sg.release();
+        return fail(MD_ERR_CUDA, "cudaGraphConditionalHandleCreate failed");
+    }
+    std::vector<cudaGraphNode_t> leaves;
+    rc = capture_into(ctx, sg.graph, nullptr, 0, [&]() -> int {
+        MDB_TRY(pre_force(it, sys, v, false));
+        k_set_rebuild<<<1, 1, 0, ctx->stream>>>(h, v->d_rebuild_flag);
+        ++ctx->launches;
+        MDB_CHECK_LAUNCH();
+        return MD_OK;
+    }, &leaves);
+    const int64_t l1 = ctx->launches;
+    cudaGraphNode_t cond = nullptr;
+    cudaGraph_t body = nullptr;
+    if (rc == MD_OK) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        const cudaError_t e = cudaGraphAddNode(&cond, sg.graph, leaves.data(), leaves.size(), &cp);
+        if (e != cudaSuccess) rc = fail(MD_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
+        else body = cp.conditional.phGraph_out[0];
+    }
+    if (rc == MD_OK)
+        rc = capture_into(ctx, body, nullptr, 0, [&]() -> int { return verlet_build(v, sys, true); },
+                          nullptr);
+    const int64_t l2 = ctx->launches;
+    if (rc == MD_OK)
+        rc = capture_into(ctx, sg.graph, &cond, 1, [&]() -> int {
+            MDB_TRY(lj_forces_verlet_async(lj, sys, v));
+            MDB_TRY(post_force_async(it, sys, false));
+            if (rows) {
+                k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy),
+                                                      ctx_result(ctx, kResKE), nhc, rows, idx);
+                ++ctx->launches;
+            }
+            MDB_CHECK_LAUNCH();
+            return MD_OK;
+        }, nullptr);
+    sg.main_launches = (l1 - l0) + (ctx->launches - l2);
+    sg.body_launches = l2 - l1;
+    ctx->launches = l0;  // counted per replay by the caller
+    if (rc == MD_OK && cudaGraphInstantiate(&sg.exec, sg.graph, 0) != cudaSuccess)
+        rc = fail(MD_ERR_CUDA, "step graph instantiation failed");
+    if (rc != MD_OK) sg.release();
+    return rc;
+}
 
 // Chain-of-thermostats pieces shared with the constrained integrators.
 int nhc_pre_async(md_integrator* it, md_context* ctx, const double* ke_now) {
@@ -500,31 +626,52 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
     if (it->kind >= 3)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: constrained integrators run with md_run_spce");
     md_context* ctx = sys->ctx;
-    DevBuf rows;
-    if (thermo && steps > 0) MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
-    NhcState* nhc = nhc_of(it);
-    if (nhc && sys->n > 0) {
-        // kinetic energy of the entry velocities for the first chain half
-        MDB_TRY(system_kinetic_async(sys, kResKE));
+    DevBuf rows, idx;
+    if (thermo && steps > 0) {
+        MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
+        MDB_TRY(idx.ensure(sizeof(int)));
+        MDB_CUDA(cudaMemsetAsync(idx.ptr, 0, sizeof(int), ctx->stream));
     }
+    NhcState* nhc = nhc_of(it);
+    // The first step runs from the host: it sums the entry kinetic energy for
+    // the chain and sizes every buffer, so that the captured step graph needs
+    // no allocation.  Later steps replay the graph when that is possible
+    // (BAOAB's noise counter is a host-side launch argument, so it never is).
+    const bool want_graph = ctx->graphs && !ctx->timing && it->kind != 1 && steps >= 4 && sys->n > 0;
+    StepGraph sg;
     for (int64_t k = 0; k < steps; ++k) {
-        if (nhc) {
-            k_nhc_pre<<<1, 1, 0, ctx->stream>>>(nhc, k == 0 ? ctx_result(ctx, kResKE) : nullptr,
-                                                yoshida());
-            ++ctx->launches;
-        }
         // Kick/drift with the rebuild test of the ForceFn (apps/moldyn_run.cpp:581-587)
         // fused in; the rebuild itself is gated on the device flag.
-        MDB_TRY(pre_force(it, sys, v));
+        MDB_TRY(pre_force(it, sys, v, k == 0));
         MDB_TRY(verlet_build(v, sys, true));
         MDB_TRY(lj_forces_verlet_async(lj, sys, v));
         MDB_TRY(post_force_async(it, sys, false));
         if (rows.ptr) {
-            k_record<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE),
-                                               nhc, rows.as<double>() + 4 * k);
+            k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy),
+                                                  ctx_result(ctx, kResKE), nhc, rows.as<double>(),
+                                                  idx.as<int>());
             ++ctx->launches;
         }
         MDB_CHECK_LAUNCH();
+        if (k == 0 && want_graph) {
+            if (capture_lj_step(it, sys, v, lj, rows.as<double>(), idx.as<int>(), sg) != MD_OK) {
+                cudaGetLastError();  // no graph: the remaining steps run from the host
+                continue;
+            }
+            const int64_t graph_steps = steps - 1;
+            int rebuilt0 = 0;
+            MDB_CUDA(cudaMemcpyAsync(&rebuilt0, v->d_rebuild_total, sizeof(int),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+            MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+            for (int64_t g = 0; g < graph_steps; ++g) MDB_CUDA(cudaGraphLaunch(sg.exec, ctx->stream));
+            int rebuilt1 = 0;
+            MDB_CUDA(cudaMemcpyAsync(&rebuilt1, v->d_rebuild_total, sizeof(int),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+            MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+            ctx->launches += graph_steps * sg.main_launches +
+                             static_cast<int64_t>(rebuilt1 - rebuilt0) * sg.body_launches;
+            break;
+        }
     }
     if (nhc && steps > 0 && sys->n > 0) {
         k_scale<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n, nhc);
@@ -535,7 +682,9 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
         MDB_CUDA(cudaMemcpyAsync(thermo, rows.ptr, sizeof(double) * 4 * static_cast<size_t>(steps),
                                  cudaMemcpyDeviceToHost, ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    sg.release();
     rows.release();
+    idx.release();
     MDB_TRY(ctx_check_status(ctx));
     double r[2];
     MDB_TRY(ctx_read_results(ctx, kResEnergy, 2, r));

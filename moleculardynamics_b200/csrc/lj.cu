@@ -204,16 +204,26 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
         const typename P::T pi = P::load(pos + i);
         const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
         const int* row = nbr + i * static_cast<int64_t>(stride);
-        // U independent index->position gather chains in flight per thread; the
-        // pair terms are accumulated in list order, as in the rolled loop.
+        // U independent index->position gather chains in flight per thread, and
+        // the next U list indices are fetched while the current pairs are
+        // computed.  Pair terms are accumulated in list order.
         int k = g;
+        int jn[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) jn[u] = k + u * TPA < cnt ? __ldg(row + k + u * TPA) : 0;
         for (; k + (U - 1) * TPA < cnt; k += U * TPA) {
             int j[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) j[u] = __ldg(row + k + u * TPA);
             typename P::T pj[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) pj[u] = P::load(pos + j[u]);
+            for (int u = 0; u < U; ++u) {
+                j[u] = jn[u];
+                pj[u] = P::load(pos + j[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int kn = k + (U + u) * TPA;
+                jn[u] = kn < cnt ? __ldg(row + kn) : 0;
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if constexpr (MIXED)
@@ -222,13 +232,16 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
                 else accumulate_exact<LFS>(a, f3, pi, pj[u], fx, fy, fz, e, vir);
             }
         }
-        for (; k < cnt; k += TPA) {
-            const int j = __ldg(row + k);
-            const typename P::T pj = P::load(pos + j);
-            if constexpr (MIXED)
-                accumulate_mixed<LFS, false>(a, f3, pd, static_cast<int>(i), j, pi, pj, fx, fy, fz,
-                                             e, vir, near);
-            else accumulate_exact<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
+        // fewer than U entries left; their indices are already in jn
+#pragma unroll
+        for (int u = 0; u < U - 1; ++u) {
+            if (k + u * TPA < cnt) {
+                const typename P::T pj = P::load(pos + jn[u]);
+                if constexpr (MIXED)
+                    accumulate_mixed<LFS, false>(a, f3, pd, static_cast<int>(i), jn[u], pi, pj, fx,
+                                                 fy, fz, e, vir, near);
+                else accumulate_exact<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
+            }
         }
         if constexpr (MIXED) {
             if (near) {  // rare: settle the pairs next to the cutoff

@@ -75,6 +75,7 @@ struct md_context {
     int64_t launches = 0;
     int sm_count = 148;
     bool timing = false;
+    bool graphs = true;                  // fused loops replay a captured step graph
     mdb::KernelTimer timers[mdb::kTimedKernels];
     cudaEvent_t span_start = nullptr, span_stop = nullptr;
 };

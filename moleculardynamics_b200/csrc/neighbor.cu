@@ -24,7 +24,7 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kBuildWarps = 4;
-constexpr int kMaxCand = 576;    // candidates staged per warp window
+constexpr int kMaxCand = 576;    // candidates staged per warp window (even)
 
 __device__ __forceinline__ bool gate(const int* flag) { return flag == nullptr || *flag != 0; }
 
@@ -259,7 +259,8 @@ __device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, do
 // atoms [start[r], start[r+1]).  The candidates of the 27 surrounding cells are
 // staged in shared memory once per cell as FP32 coordinates relative to the cell
 // centre (nearest periodic image); then each lane takes one atom of the cell and
-// scans the staged candidates (a broadcast read), appending hits to its own row.
+// scans the staged candidates (broadcast reads, two candidates per packed FP32x2
+// step), appending hits to its own row.
 // Only a candidate whose FP32 r^2 lies within 2^-12 of the list cutoff^2 -- far
 // wider than the FP32 error of these coordinates -- is decided by the exact
 // reference arithmetic, so the pair set stays bit-identical to the reference's.
@@ -269,7 +270,11 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
                uint32_t* status, int* max_count, const int* flag) {
     if (!gate(flag)) return;
-    __shared__ float4 s_p[kBuildWarps][kMaxCand];
+    // Candidates in pairs, structure-of-arrays within a pair so that two
+    // candidates are tested with one packed FP32x2 instruction per step:
+    // s_a[p] = (-x0, -x1, -y0, -y1), s_b[p] = (-z0, -z1, j0, j1).
+    __shared__ float4 s_a[kBuildWarps][kMaxCand / 2];
+    __shared__ float4 s_b[kBuildWarps][kMaxCand / 2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = blockIdx.x * kBuildWarps + warp;
     if (r >= g.ncells) return;
@@ -317,9 +322,20 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                 vx -= g.box.L[0] * rint(vx * g.box.inv[0]);
                 vy -= g.box.L[1] * rint(vy * g.box.inv[1]);
                 vz -= g.box.L[2] * rint(vz * g.box.inv[2]);
-                s_p[warp][gt - wb] = make_float4(static_cast<float>(vx), static_cast<float>(vy),
-                                                 static_cast<float>(vz), __int_as_float(j));
+                const int tt = gt - wb, pr = tt >> 1, h = tt & 1;
+                float* A = reinterpret_cast<float*>(&s_a[warp][pr]);
+                float* B = reinterpret_cast<float*>(&s_b[warp][pr]);
+                A[h] = -static_cast<float>(vx);
+                A[2 + h] = -static_cast<float>(vy);
+                B[h] = -static_cast<float>(vz);
+                B[2 + h] = __int_as_float(j);
             }
+        }
+        if ((wlen & 1) && lane == 0) {  // pad the odd slot: infinitely far, no atom
+            float* A = reinterpret_cast<float*>(&s_a[warp][wlen >> 1]);
+            float* B = reinterpret_cast<float*>(&s_b[warp][wlen >> 1]);
+            A[1] = A[3] = B[1] = 1e30f;
+            B[3] = __int_as_float(-1);
         }
         __syncwarp();
         for (int ib = a0; ib < a1; ib += 32) {
@@ -340,25 +356,35 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                 c = wb == 0 ? 0 : count[i];
             }
             int* row = nbr + static_cast<int64_t>(active ? i : 0) * stride;
-            // Per candidate: an FP32 distance test and a predicated append.  The
-            // few candidates within the 2^-12 band around the cutoff are decided
-            // by the exact reference arithmetic in place (so rows keep stencil
-            // order); the band check is one warp vote, taken only when some lane
-            // of the warp has such a candidate.
-#pragma unroll 4
-            for (int t = 0; t < wlen; ++t) {
-                const float4 q = s_p[warp][t];
-                const int j = __float_as_int(q.w);
-                const float dx = fx - q.x, dy = fy - q.y, dz = fz - q.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                bool hit = r2 < lo_thr;
-                const bool near = active && !hit && r2 <= hi_thr;
-                if (__any_sync(0xffffffffu, near)) {
-                    if (near) hit = within(g.box, pi, ldg4(pos + j), rl2);
+            // Per candidate pair: packed FP32x2 distances and predicated appends.
+            // The few candidates within the 2^-12 band around the cutoff are
+            // decided by the exact reference arithmetic in place (so rows keep
+            // stencil order); the band check is one warp vote per pair, taken
+            // only when some lane of the warp has such a candidate.
+            const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy),
+                         fz2 = make_float2(fz, fz);
+            const int npairs = (wlen + 1) >> 1;
+#pragma unroll 2
+            for (int pr = 0; pr < npairs; ++pr) {
+                const float4 A = s_a[warp][pr], B = s_b[warp][pr];
+                const float2 dx = __fadd2_rn(fx2, make_float2(A.x, A.y));
+                const float2 dy = __fadd2_rn(fy2, make_float2(A.z, A.w));
+                const float2 dz = __fadd2_rn(fz2, make_float2(B.x, B.y));
+                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                const int j0 = __float_as_int(B.z), j1 = __float_as_int(B.w);
+                bool h0 = r2.x < lo_thr, h1 = r2.y < lo_thr;
+                const bool n0 = active && !h0 && r2.x <= hi_thr;
+                const bool n1 = active && !h1 && r2.y <= hi_thr;
+                if (__any_sync(0xffffffffu, n0 || n1)) {
+                    if (n0 && j0 != i) h0 = within(g.box, pi, ldg4(pos + j0), rl2);
+                    if (n1 && j1 != i) h1 = within(g.box, pi, ldg4(pos + j1), rl2);
                 }
-                hit = hit && active && j != i;
-                if (hit && c < stride) row[c] = j;
-                c += hit ? 1 : 0;
+                h0 = h0 && active && j0 != i;
+                h1 = h1 && active && j1 != i;
+                if (h0 && c < stride) row[c] = j0;
+                c += h0 ? 1 : 0;
+                if (h1 && c < stride) row[c] = j1;
+                c += h1 ? 1 : 0;
             }
             if (active) {
                 count[i] = c;

@@ -107,6 +107,60 @@ def test_fused_run_equals_host_loop(md):
     assert outs[0][2] == outs[1][2]
 
 
+@pytest.mark.parametrize("kind", ["vv", "nhc"])
+def test_step_graph_replay_equals_host_launches(md, kind):
+    """md_run_lj replaying the captured step graph (conditional rebuild node) and
+    launching every kernel from the host give bit-identical trajectories, thermo
+    rows and rebuild counts; 300 steps of a hot liquid rebuild many times."""
+    outs = []
+    ctx = md.default_context()
+    for graphs in (False, True):
+        ctx.set_graphs(graphs)
+        try:
+            s, st = lattice_system(md, 5, 0.8442, 1.5, 7)
+            lj = md.LennardJones(1.0, 1.0, 2.5)
+            v = md.VerletList(st["box"], 2.5, 0.3)
+            v.build(s)
+            lj.compute_forces(s, v)
+            integ = (md.VelocityVerlet(0.005) if kind == "vv"
+                     else md.NoseHooverChain(0.005, 1.0, 0.5, 3, 3 * s.n - 3))
+            th = integ.run(s, v, lj, 300, thermo=True)
+            outs.append((s.positions, s.velocities, th, v.rebuild_count()))
+        finally:
+            ctx.set_graphs(True)
+    assert outs[0][3] == outs[1][3] and outs[0][3] > 5
+    for a, b in zip(outs[0][:3], outs[1][:3]):
+        assert np.array_equal(a, b)
+
+
+def test_nhc_fused_run_follows_host_steps(md):
+    """The fused Nose-Hoover loop applies integrateChain(dt/2) exactly twice per
+    step, as NoseHooverChain::step does (nose_hoover.hpp:37-42): it tracks the
+    host-driven steps to round-off (it reuses the chain's tracked kinetic energy
+    instead of re-summing it)."""
+    outs = []
+    for fused in (False, True):
+        s, st = lattice_system(md, 4, 0.80, 1.2, 21)
+        dof = 3 * s.n - 3
+        lj = md.LennardJones(1.0, 1.0, 2.5, md.Truncation.LinearForceShift)
+        v = md.VerletList(st["box"], 2.5, 0.3)
+        v.build(s)
+        lj.compute_forces(s, v)
+        integ = md.NoseHooverChain(0.002, 1.0, 0.5, 3, dof)
+        if fused:
+            integ.run(s, v, lj, 100)
+        else:
+            def forces(sys_):
+                v.rebuild_if_needed(sys_)
+                return lj.compute_forces(sys_, v)[0]
+            for _ in range(100):
+                integ.step(s, forces)
+        outs.append((s.positions, s.velocities, integ.conserved_quantity_contribution()))
+    assert np.max(np.abs(outs[0][0] - outs[1][0])) < 1e-10
+    assert np.max(np.abs(outs[0][1] - outs[1][1])) < 1e-10
+    assert abs(outs[0][2] - outs[1][2]) < 1e-10 * (1 + abs(outs[0][2]))
+
+
 def energy_error_slope(md, use_run):
     dts = [0.001, 0.002, 0.004, 0.008]
     log_dt, log_err = [], []
