@@ -472,8 +472,154 @@ def run_gpu_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ batch workload
+BATCH_METRIC = "aggregate atom-steps/s, 48 LJ replicas (NHC, mixed) on 1 B200"
+BATCH_TABLE = os.path.join(ROOT, "moleculardynamics_b200", "data", "replicas_48.json")
+
+
+def batch_table():
+    with open(BATCH_TABLE) as fh:
+        return json.load(fh)["replicas"]
+
+
+def batch_config():
+    rows = batch_table()
+    return {"workload": "48 independent LJ replicas (table moleculardynamics_b200/data/"
+                        "replicas_48.json): fcc n ~ U{4..20}, rho in {0.1..0.9}, T ~ U[1,2]; "
+                        "NHC M=3 tau=0.5 dt=0.005, rc=2.5 truncated, skin 0.3, mixed precision",
+            "replicas": len(rows), "atoms": sum(r["atoms"] for r in rows),
+            "l2_policy": "no flush: replicas hold ~0.2 GB > 126 MB L2",
+            "parallelism": "replicas (one CUDA graph per step holds every replica's kernels)"}
+
+
+def _batch_ref_worker(args):
+    """One single-threaded reference process stepping the given replicas with
+    NoseHooverChain; returns (kind, atom-steps, seconds)."""
+    rows, steps = args
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    R = O.ref()
+    done, sec = 0, 0.0
+    for r in rows:
+        st = O.fcc_lattice(r["cells"], r["density"], r["temperature"], r["seed"])
+        pos, vel, box = st["pos"], st["vel"], st["box"]
+        n = pos.shape[0]
+        cols = [np.ascontiguousarray(pos[:, k]) for k in range(3)] + \
+               [np.ascontiguousarray(vel[:, k]) for k in range(3)] + [np.zeros(n) for _ in range(3)]
+        info = np.zeros(5)
+        if R is None:
+            raise RuntimeError("reference library not built")
+        R.ref_run(2, n, O._p(np.ascontiguousarray(box)), *[O._p(a) for a in cols],
+                  O._p(np.ones(n)), 1.0, 1.0, RC, 0, SKIN, DT, steps, 0.0, r["temperature"], 0,
+                  0.5, 3, 3 * n - 3, O._p(info))
+        done += n * steps
+        sec += info[4]
+    return "reference", done, sec
+
+
+def batch_cpu_reference(steps, procs):
+    """The 48 replicas spread over `procs` concurrent single-threaded reference
+    processes (largest first, round robin); aggregate = all atom-steps / the
+    slowest process's stepping time."""
+    rows = sorted(batch_table(), key=lambda r: -r["atoms"])
+    shares = [rows[k::procs] for k in range(procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_batch_ref_worker, [(sh, steps) for sh in shares])
+    total = sum(r[1] for r in res)
+    return total / max(r[2] for r in res), procs
+
+
+def run_batch_arm(args):
+    world, rank, local = dist_env()
+    group = Group(world)
+    if args.impl == "reference":
+        if rank == 0:
+            steps = max(1, min(args.steps, args.ref_steps))
+            procs = max(1, min(os.cpu_count() or 1, args.ref_procs))
+            value, procs = batch_cpu_reference(steps, procs)
+            print(json.dumps({
+                "metric": BATCH_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded fcc lattices)", "config": batch_config(),
+                "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs,
+                                 "kind": "reference",
+                                 "sample": f"all 48 replicas over {procs} concurrent single-threaded "
+                                           f"reference processes, {steps} NHC steps each "
+                                           f"({cpu_model()})"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}), flush=True)
+        group.close()
+        return 0
+    import moleculardynamics_b200 as md
+    rows = batch_table()
+    batch = md.Batch()
+    parts = []
+    for r in rows:
+        ctx = md.Context(local)
+        st = md.fcc_lattice(r["cells"], r["density"], r["temperature"], r["seed"])
+        s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"], ctx=ctx)
+        lj = md.LennardJones(1.0, 1.0, RC, precision=md.PRECISION_MIXED)
+        v = md.VerletList(st["box"], RC, SKIN, ctx=ctx)
+        v.build(s)
+        pe, _ = lj.compute_forces(s, v)
+        integ = md.NoseHooverChain(DT, r["temperature"], 0.5, 3, 3 * s.n - 3)
+        parts.append((ctx, s, v, lj, integ, pe + s.kinetic_energy()))
+        batch.add(integ, s, v, lj)
+    n_atoms = sum(p[1].n for p in parts)
+    batch.run(args.warmup)
+    lead = parts[0][0]
+    L = md.lib()
+    launches0 = sum(p[0].launch_count() for p in parts)
+    group.barrier()
+    clocks = ClockSampler(local)
+    clocks.__enter__()
+    md._check(L.md_context_span_begin(lead.handle))
+    th = batch.run(args.steps, thermo=True)
+    ms = C.c_double()
+    md._check(L.md_context_span_end(lead.handle, C.byref(ms)))
+    clocks.__exit__(None, None, None)
+    group.barrier()
+    launches = sum(p[0].launch_count() for p in parts) - launches0
+    dev_ms = group.reduce(ms.value, "max")
+    value = world * n_atoms * args.steps / (dev_ms * 1e-3)
+    h = th[:, :, 0] + th[:, :, 2] + th[:, :, 3]
+    dev = np.max(np.abs(h - h[:, :1]), axis=1)
+    drift = dev / np.abs(h[:, 0])
+    per_atom = dev / np.array([p[1].n for p in parts])
+    if rank == 0:
+        line = {
+            "metric": BATCH_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair terms, f64 displacement/accumulation/integration (mixed)",
+            "data": "synthetic: seeded fcc lattices, Maxwell-Boltzmann velocities",
+            "config": batch_config(), "gpu_launches": int(launches),
+            "nhc_extended_energy_drift": {
+                "steps": args.steps, "note": "truncated LJ: cutoff crossings step the energy",
+                "relative_max": float(drift.max()), "relative_median": float(np.median(drift)),
+                "per_atom_max": float(per_atom.max()), "per_atom_median": float(np.median(per_atom))},
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            cval, procs = batch_cpu_reference(max(1, args.cpu_steps), args.ref_procs)
+            line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": procs,
+                                    "kind": "reference",
+                                    "sample": f"all 48 replicas over {procs} concurrent "
+                                              f"single-threaded reference processes, "
+                                              f"{max(1, args.cpu_steps)} NHC steps each "
+                                              f"({cpu_model()})"}
+        print(json.dumps(line), flush=True)
+    group.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--workload", default="lj1m", choices=["lj1m", "batch"],
+                    help="lj1m: the headline 1M-atom run; batch: 48 NHC replicas")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
@@ -492,6 +638,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.workload == "batch":
+        return run_batch_arm(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

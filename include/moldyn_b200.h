@@ -80,6 +80,7 @@ typedef struct md_lj md_lj;
 typedef struct md_integrator md_integrator;
 typedef struct md_ewald md_ewald;
 typedef struct md_rigid md_rigid;
+typedef struct md_batch md_batch;
 
 /* ------------------------------------------------------------------ library */
 /* Message of the last failing call on this thread ("" if none). */
@@ -325,6 +326,22 @@ MD_API int md_lj_forces_static(const double* d_x, const double* d_y, const doubl
 MD_API int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed, double* x,
                    double* y, double* z, double* vx, double* vy, double* vz, double* mass,
                    double box[3]);
+
+/* ------------------------------------------------------------ replica batches */
+/* Many independent LJ replicas stepped together; no reference counterpart (the
+ * reference runs one system per moldyn_run process).  Each replica is an
+ * integrator (velocity Verlet or Nose-Hoover chain), a system on its own context,
+ * its Verlet list (built) and an LJ force field.  md_batch_run advances every
+ * replica by `steps` fused steps, replaying one CUDA graph per step that holds
+ * all replicas' kernels as independent chains; each replica's trajectory equals
+ * the one md_run_lj gives it alone.  thermo (nullable): replicas x steps x 4
+ * doubles (potential energy, virial, kinetic energy, chain contribution). */
+MD_API int md_batch_create(md_batch** out);
+MD_API int md_batch_destroy(md_batch* batch);
+MD_API int md_batch_add(md_batch* batch, md_integrator* integ, md_system* sys, md_verlet* list,
+                        md_lj* lj, int* index);
+MD_API int md_batch_size(const md_batch* batch);
+MD_API int md_batch_run(md_batch* batch, int64_t steps, double* thermo);
 
 /* Fused device loop of a constrained integrator with SPC/E forces (the
  * water_rdf-style NVE / NHC production loop): forces are (re)computed on entry,

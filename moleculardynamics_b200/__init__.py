@@ -167,6 +167,11 @@ def _load():
                                                       C.c_int, C.c_int64, C.POINTER(_vp)]),
         "md_integrator_iterations": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "md_run_spce": (C.c_int, [_vp, _vp, _vp, C.c_int64, _d]),
+        "md_batch_create": (C.c_int, [C.POINTER(_vp)]),
+        "md_batch_destroy": (C.c_int, [_vp]),
+        "md_batch_add": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int)]),
+        "md_batch_size": (C.c_int, [_vp]),
+        "md_batch_run": (C.c_int, [_vp, C.c_int64, _d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -794,6 +799,41 @@ class ConstrainedNoseHooverChain(ConstrainedVelocityVerlet):
         self._h = h
         self.dt = float(dt)
         self.constraint = constraint
+
+
+# ---------------------------------------------------------------- batches
+class Batch:
+    """Independent LJ replicas stepped together (no reference counterpart).  Each
+    replica is (integrator, system, Verlet list, LennardJones) with the system on
+    its own Context; run() replays one CUDA graph per step over all replicas."""
+
+    def __init__(self):
+        h = _vp()
+        _check(lib().md_batch_create(C.byref(h)))
+        self._h = h
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_batch_destroy(self._h)
+            self._h = None
+
+    def add(self, integrator, sys: System, verlet: VerletList, lj: LennardJones) -> int:
+        idx = C.c_int()
+        _check(lib().md_batch_add(self._h, integrator.handle, sys.handle, verlet.handle,
+                                  lj.handle, C.byref(idx)))
+        self._keep.append((integrator, sys, verlet, lj))
+        return idx.value
+
+    def __len__(self):
+        return lib().md_batch_size(self._h)
+
+    def run(self, steps: int, thermo=False):
+        """Returns a (replicas, steps, 4) array [energy, virial, kinetic, conserved]
+        if thermo."""
+        out = np.zeros((len(self), steps, 4)) if thermo and steps > 0 else None
+        _check(lib().md_batch_run(self._h, int(steps), _ptr(out) if out is not None else None))
+        return out
 
 
 # ---------------------------------------------------------------- setup

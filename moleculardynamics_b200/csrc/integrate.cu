@@ -354,6 +354,8 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 
 // ------------------------------------------------------------ step graphs
+namespace {
+
 // One fused LJ step captured as a CUDA graph: [chain half,] kick/drift with the
 // displacement check, a conditional node whose body is the gated neighbour
 // rebuild (opened by k_set_rebuild from the device flag, so steps without a
@@ -398,22 +400,38 @@ int capture_into(md_context* ctx, cudaGraph_t g, const cudaGraphNode_t* deps, si
     return MD_OK;
 }
 
-int capture_lj_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
-                    int* idx, StepGraph& sg) {
+}  // namespace (the step graph helpers above are private to this file)
+
+int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
+                  int* idx, bool first) {
+    md_context* ctx = sys->ctx;
+    // Kick/drift with the rebuild test of the ForceFn (apps/moldyn_run.cpp:581-587)
+    // fused in; the rebuild itself is gated on the device flag.
+    MDB_TRY(pre_force(it, sys, v, first));
+    MDB_TRY(verlet_build(v, sys, true));
+    MDB_TRY(lj_forces_verlet_async(lj, sys, v));
+    MDB_TRY(post_force_async(it, sys, false));
+    if (rows) {
+        k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE),
+                                              nhc_of(it), rows, idx);
+        ++ctx->launches;
+    }
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj,
+                         double* rows, int* idx, cudaGraph_t graph, int64_t* main_launches,
+                         int64_t* body_launches) {
     md_context* ctx = sys->ctx;
     NhcState* nhc = nhc_of(it);
     const int64_t l0 = ctx->launches;
     int rc = MD_OK;
-    if (cudaGraphCreate(&sg.graph, 0) != cudaSuccess)
-        return fail(MD_ERR_CUDA, "cudaGraphCreate failed");
     cudaGraphConditionalHandle h;
-    if (cudaGraphConditionalHandleCreate(&h, sg.graph, 0, cudaGraphCondAssignDefault) !=
-        cudaSuccess) {
-        sg.release();
+    if (cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
         return fail(MD_ERR_CUDA, "cudaGraphConditionalHandleCreate failed");
-    }
     std::vector<cudaGraphNode_t> leaves;
-    rc = capture_into(ctx, sg.graph, nullptr, 0, [&]() -> int {
+    rc = capture_into(ctx, graph, nullptr, 0, [&]() -> int {
         MDB_TRY(pre_force(it, sys, v, false));
         k_set_rebuild<<<1, 1, 0, ctx->stream>>>(h, v->d_rebuild_flag);
         ++ctx->launches;
@@ -429,7 +447,7 @@ int capture_lj_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, 
         cp.conditional.handle = h;
         cp.conditional.type = cudaGraphCondTypeIf;
         cp.conditional.size = 1;
-        const cudaError_t e = cudaGraphAddNode(&cond, sg.graph, leaves.data(), leaves.size(), &cp);
+        const cudaError_t e = cudaGraphAddNode(&cond, graph, leaves.data(), leaves.size(), &cp);
         if (e != cudaSuccess) rc = fail(MD_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
         else body = cp.conditional.phGraph_out[0];
     }
@@ -438,7 +456,7 @@ int capture_lj_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, 
                           nullptr);
     const int64_t l2 = ctx->launches;
     if (rc == MD_OK)
-        rc = capture_into(ctx, sg.graph, &cond, 1, [&]() -> int {
+        rc = capture_into(ctx, graph, &cond, 1, [&]() -> int {
             MDB_TRY(lj_forces_verlet_async(lj, sys, v));
             MDB_TRY(post_force_async(it, sys, false));
             if (rows) {
@@ -449,14 +467,27 @@ int capture_lj_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, 
             MDB_CHECK_LAUNCH();
             return MD_OK;
         }, nullptr);
-    sg.main_launches = (l1 - l0) + (ctx->launches - l2);
-    sg.body_launches = l2 - l1;
+    if (main_launches) *main_launches = (l1 - l0) + (ctx->launches - l2);
+    if (body_launches) *body_launches = l2 - l1;
     ctx->launches = l0;  // counted per replay by the caller
+    return rc;
+}
+
+namespace {
+
+int capture_lj_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
+                    int* idx, StepGraph& sg) {
+    if (cudaGraphCreate(&sg.graph, 0) != cudaSuccess)
+        return fail(MD_ERR_CUDA, "cudaGraphCreate failed");
+    int rc = capture_lj_step_into(it, sys, v, lj, rows, idx, sg.graph, &sg.main_launches,
+                                  &sg.body_launches);
     if (rc == MD_OK && cudaGraphInstantiate(&sg.exec, sg.graph, 0) != cudaSuccess)
         rc = fail(MD_ERR_CUDA, "step graph instantiation failed");
     if (rc != MD_OK) sg.release();
     return rc;
 }
+
+}  // namespace
 
 // Chain-of-thermostats pieces shared with the constrained integrators.
 int nhc_pre_async(md_integrator* it, md_context* ctx, const double* ke_now) {
@@ -640,19 +671,7 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
     const bool want_graph = ctx->graphs && !ctx->timing && it->kind != 1 && steps >= 4 && sys->n > 0;
     StepGraph sg;
     for (int64_t k = 0; k < steps; ++k) {
-        // Kick/drift with the rebuild test of the ForceFn (apps/moldyn_run.cpp:581-587)
-        // fused in; the rebuild itself is gated on the device flag.
-        MDB_TRY(pre_force(it, sys, v, k == 0));
-        MDB_TRY(verlet_build(v, sys, true));
-        MDB_TRY(lj_forces_verlet_async(lj, sys, v));
-        MDB_TRY(post_force_async(it, sys, false));
-        if (rows.ptr) {
-            k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy),
-                                                  ctx_result(ctx, kResKE), nhc, rows.as<double>(),
-                                                  idx.as<int>());
-            ++ctx->launches;
-        }
-        MDB_CHECK_LAUNCH();
+        MDB_TRY(lj_fused_step(it, sys, v, lj, rows.as<double>(), idx.as<int>(), k == 0));
         if (k == 0 && want_graph) {
             if (capture_lj_step(it, sys, v, lj, rows.as<double>(), idx.as<int>(), sg) != MD_OK) {
                 cudaGetLastError();  // no graph: the remaining steps run from the host

@@ -217,6 +217,19 @@ struct md_lj {
 };
 
 namespace mdb {
+// Adds one fused LJ step (kick/drift with the displacement check, a conditional
+// node holding the gated neighbour rebuild, forces, kick, thermo row at rows +
+// 4 * (*idx)) to `graph`, captured on the system's context stream.  The kernel
+// counts outside / inside the rebuild branch are returned for launch accounting.
+// One fused LJ step launched from the host (first: the chain half sums the
+// current kinetic energy instead of using the tracked value).
+int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
+                  int* idx, bool first);
+int nhc_apply_scale_async(md_integrator* it, md_system* sys);
+int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj,
+                         double* rows, int* idx, cudaGraph_t graph, int64_t* main_launches,
+                         int64_t* body_launches);
+
 // Pair-force kernels over the Verlet list; results land in the context result
 // slots kResEnergy / kResVirial (device), no synchronisation.
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);

@@ -1,0 +1,63 @@
+"""Replica batches: every replica of a batch run follows exactly the trajectory
+md_run_lj gives it alone (same kernels, same arguments, replayed as independent
+chains of one CUDA graph per step)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# (cells, density, temperature, seed, integrator): a 2-cells-per-side replica
+# (brute-force list build), a dilute gas, dense liquids, a mixed-precision one
+REPLICAS = [(4, 0.9, 1.3, 11, "nhc", 0), (5, 0.1, 1.8, 12, "nhc", 0), (6, 0.8, 1.0, 13, "vv", 0),
+            (8, 0.5, 1.5, 14, "nhc", 1), (7, 0.3, 2.0, 15, "vv", 0)]
+
+
+def replica(md, cells, rho, temp, seed, kind, prec):
+    ctx = md.Context(0)
+    st = md.fcc_lattice(cells, rho, temp, seed)
+    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"], ctx=ctx)
+    lj = md.LennardJones(1.0, 1.0, 2.5, precision=prec)
+    v = md.VerletList(st["box"], 2.5, 0.3, ctx=ctx)
+    v.build(s)
+    lj.compute_forces(s, v)
+    integ = (md.NoseHooverChain(0.005, temp, 0.5, 3, 3 * s.n - 3) if kind == "nhc"
+             else md.VelocityVerlet(0.005))
+    return ctx, s, v, lj, integ
+
+
+def test_batch_equals_replicas_run_alone(md):
+    steps = 80
+    alone = []
+    for r in REPLICAS:
+        ctx, s, v, lj, integ = replica(md, *r)
+        th = integ.run(s, v, lj, steps, thermo=True)
+        alone.append((s.positions, s.velocities, th, v.rebuild_count()))
+    batch = md.Batch()
+    parts = [replica(md, *r) for r in REPLICAS]
+    for ctx, s, v, lj, integ in parts:
+        batch.add(integ, s, v, lj)
+    assert len(batch) == len(REPLICAS)
+    th = batch.run(steps, thermo=True)
+    assert th.shape == (len(REPLICAS), steps, 4)
+    for k, (ctx, s, v, lj, integ) in enumerate(parts):
+        pos, vel, th_alone, rebuilds = alone[k]
+        assert np.array_equal(s.positions, pos), k
+        assert np.array_equal(s.velocities, vel), k
+        assert np.array_equal(th[k], th_alone), k
+        assert v.rebuild_count() == rebuilds, k
+    assert sum(alone[k][3] for k in range(len(REPLICAS))) > len(REPLICAS)
+
+
+def test_batch_rejects_shared_context_and_langevin(md):
+    ctx, s, v, lj, integ = replica(md, 4, 0.8, 1.0, 3, "vv", 0)
+    batch = md.Batch()
+    batch.add(integ, s, v, lj)
+    st = md.fcc_lattice(4, 0.8, 1.0, 4)
+    s2 = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], ctx=ctx)
+    v2 = md.VerletList(st["box"], 2.5, 0.3, ctx=ctx)
+    v2.build(s2)
+    with pytest.raises(md.InvalidArgument, match="own context"):
+        batch.add(md.VelocityVerlet(0.005), s2, v2, lj)
+    ctx3, s3, v3, lj3, _ = replica(md, 4, 0.8, 1.0, 5, "vv", 0)
+    with pytest.raises(md.InvalidArgument, match="Nose-Hoover"):
+        batch.add(md.LangevinBAOAB(0.005, 1.0, 1.0, 7), s3, v3, lj3)
