@@ -81,6 +81,7 @@ typedef struct md_integrator md_integrator;
 typedef struct md_ewald md_ewald;
 typedef struct md_rigid md_rigid;
 typedef struct md_batch md_batch;
+typedef struct md_adjoint md_adjoint;
 
 /* ------------------------------------------------------------------ library */
 /* Message of the last failing call on this thread ("" if none). */
@@ -342,6 +343,30 @@ MD_API int md_batch_add(md_batch* batch, md_integrator* integ, md_system* sys, m
                         md_lj* lj, int* index);
 MD_API int md_batch_size(const md_batch* batch);
 MD_API int md_batch_run(md_batch* batch, int64_t steps, double* thermo);
+
+/* ------------------------------------------------ differentiable trajectories */
+/* No reference counterpart.  A velocity-Verlet LJ trajectory (FP64) with a
+ * hand-written adjoint, in torch.autograd.Function form: md_adjoint_forward runs
+ * `steps` steps from the system's state, saves the state every `every` steps
+ * (the save-for-backward) and writes rows (steps x 3: potential energy, virial
+ * W = sum of w, kinetic energy after each step).  Its Verlet list (cutoff + skin)
+ * is rebuilt only at the saved states; a step whose list the reference rebuild
+ * criterion would reject fails the call (MD_ERR_RUNTIME: raise the skin or save
+ * more often).  md_adjoint_backward takes dL/d(row) (steps x 3), recomputes each
+ * segment from its saved state and returns dL/d(epsilon, sigma), and optionally
+ * dL/d(initial positions) and dL/d(initial velocities) (n x 3, caller's order).
+ * The system is left where the forward left it. */
+MD_API int md_adjoint_create(md_context* ctx, md_adjoint** out);
+MD_API int md_adjoint_destroy(md_adjoint* adj);
+MD_API int md_adjoint_forward(md_adjoint* adj, md_system* sys, const md_lj* lj, double dt,
+                              int64_t steps, int every, double skin, double* rows);
+MD_API int md_adjoint_backward(md_adjoint* adj, const double* grad_rows, double grad_theta[2],
+                               double* grad_x0, double* grad_v0);
+/* Hessian-vector product of the LJ forces: out = (dF/dx)^T u for a per-atom
+ * field u (n x 3, caller's order), and dtheta = (u . dF/d epsilon, u . dF/d sigma).
+ * FP64, over a built Verlet list.  No reference counterpart. */
+MD_API int md_lj_hvp(const md_lj* lj, md_system* sys, md_verlet* list, const double* u, double* out,
+                     double dtheta[2]);
 
 /* Fused device loop of a constrained integrator with SPC/E forces (the
  * water_rdf-style NVE / NHC production loop): forces are (re)computed on entry,

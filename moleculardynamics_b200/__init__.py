@@ -172,6 +172,12 @@ def _load():
         "md_batch_add": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int)]),
         "md_batch_size": (C.c_int, [_vp]),
         "md_batch_run": (C.c_int, [_vp, C.c_int64, _d]),
+        "md_adjoint_create": (C.c_int, [_vp, C.POINTER(_vp)]),
+        "md_adjoint_destroy": (C.c_int, [_vp]),
+        "md_adjoint_forward": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_int64, C.c_int,
+                                         C.c_double, _d]),
+        "md_adjoint_backward": (C.c_int, [_vp, _d, _d, _d, _d]),
+        "md_lj_hvp": (C.c_int, [_vp, _vp, _vp, _d, _d, _d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -496,6 +502,15 @@ class LennardJones:
             return self._ev(lib().md_lj_forces_cells, sys.handle, source._h)
         return self._ev(lib().md_lj_forces_verlet, sys.handle, source.handle)
 
+    def hessian_vector_product(self, sys: System, verlet: VerletList, u):
+        """(dF/dx)^T u for a per-atom field u (N, 3), and (u . dF/d epsilon,
+        u . dF/d sigma).  FP64 over a built Verlet list."""
+        u = _f64(u).reshape(sys.n, 3)
+        out = np.zeros((sys.n, 3))
+        th = np.zeros(2)
+        _check(lib().md_lj_hvp(self._h, sys.handle, verlet.handle, _ptr(u), _ptr(out), _ptr(th)))
+        return out, th
+
     def long_range_correction(self, sys: System):
         u = C.c_double()
         _check(lib().md_lj_lrc(self._h, sys.n, _ptr(_f64(sys.box)), C.byref(u), None))
@@ -799,6 +814,42 @@ class ConstrainedNoseHooverChain(ConstrainedVelocityVerlet):
         self._h = h
         self.dt = float(dt)
         self.constraint = constraint
+
+
+# ---------------------------------------------------------------- adjoint
+class AdjointTrajectory:
+    """A differentiable FP64 velocity-Verlet LJ trajectory with a hand-written
+    adjoint (no reference counterpart).  forward() saves the state every `every`
+    steps and returns rows (steps, 3) = [U, W, KE] after each step; backward(g)
+    with g = dL/d(rows) returns (dL/d epsilon, dL/d sigma, dL/dx0, dL/dv0)."""
+
+    def __init__(self, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = _vp()
+        _check(lib().md_adjoint_create(self.ctx.handle, C.byref(h)))
+        self._h = h
+        self.n = 0
+        self.steps = 0
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_adjoint_destroy(self._h)
+            self._h = None
+
+    def forward(self, sys: System, lj: LennardJones, dt, steps, every=50, skin=1.0):
+        rows = np.zeros((int(steps), 3))
+        _check(lib().md_adjoint_forward(self._h, sys.handle, lj.handle, float(dt), int(steps),
+                                        int(every), float(skin), _ptr(rows)))
+        self.n, self.steps = sys.n, int(steps)
+        return rows
+
+    def backward(self, grad_rows):
+        g = _f64(grad_rows).reshape(self.steps, 3)
+        th = np.zeros(2)
+        gx = np.zeros((self.n, 3))
+        gv = np.zeros((self.n, 3))
+        _check(lib().md_adjoint_backward(self._h, _ptr(g), _ptr(th), _ptr(gx), _ptr(gv)))
+        return th[0], th[1], gx, gv
 
 
 # ---------------------------------------------------------------- batches

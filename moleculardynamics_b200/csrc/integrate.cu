@@ -402,6 +402,12 @@ int capture_into(md_context* ctx, cudaGraph_t g, const cudaGraphNode_t* deps, si
 
 }  // namespace (the step graph helpers above are private to this file)
 
+int vv_pre_async(md_integrator* it, md_system* sys, md_verlet* check) {
+    return pre_force(it, sys, check, true);
+}
+
+int vv_post_async(md_integrator* it, md_system* sys) { return post_force_async(it, sys, true); }
+
 int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
                   int* idx, bool first) {
     md_context* ctx = sys->ctx;

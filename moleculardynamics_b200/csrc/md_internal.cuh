@@ -226,6 +226,10 @@ namespace mdb {
 int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
                   int* idx, bool first);
 int nhc_apply_scale_async(md_integrator* it, md_system* sys);
+// The two halves of one host-driven step (pre_force with an optional fused
+// displacement check against `check`'s reference positions; post_force).
+int vv_pre_async(md_integrator* it, md_system* sys, md_verlet* check);
+int vv_post_async(md_integrator* it, md_system* sys);
 int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj,
                          double* rows, int* idx, cudaGraph_t graph, int64_t* main_launches,
                          int64_t* body_launches);
