@@ -616,10 +616,125 @@ def run_batch_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- adjoint workload
+ADJ_METRIC = "atom-steps/s of forward + adjoint backward, 32,000-atom LJ trajectory (FP64)"
+
+
+def adjoint_config(steps, every, skin):
+    return {"workload": f"differentiable LJ trajectory: fcc 20^3 (N=32000), rho*=0.8442, "
+                        f"T*=0.722, rc=2.5 force-shifted (continuous, so finite differences "
+                        f"see no cutoff jumps), {steps} FP64 velocity-Verlet steps, dt*=0.005, "
+                        f"states saved every {every} steps, list skin {skin}",
+            "loss": "(mean virial pressure - 1)^2 + (mean potential energy per atom + 5)^2",
+            "n_atoms": 32000, "parallelism": "one system"}
+
+
+def run_adjoint_arm(args):
+    world, rank, local = dist_env()
+    group = Group(world)
+    steps, every, skin = args.steps, 50, args.adj_skin
+    if args.impl == "reference":
+        if rank == 0:
+            import oracle as O
+            st = O.fcc_lattice(20, RHO, TEMP, SEED)
+            nsteps = max(1, min(args.steps, args.ref_steps))
+            kind, value, _ = cpu_reference(st["pos"], st["vel"], st["box"], nsteps, 1)
+            print(json.dumps({
+                "metric": ADJ_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * 32000 / value,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded fcc lattice)",
+                "config": adjoint_config(steps, every, skin), "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+                                 "sample": f"{nsteps} reference NVE VV steps (the forward only: "
+                                           f"the reference has no backward) of the 32000-atom "
+                                           f"lattice, 1 thread ({cpu_model()})"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}), flush=True)
+        group.close()
+        return 0
+    import moleculardynamics_b200 as md
+    ctx = md.Context(local)
+    st = md.fcc_lattice(20, RHO, TEMP, SEED)
+    pos, vel, mass, box = st["pos"], st["vel"], st["mass"], st["box"]
+    n, vol = pos.shape[0], float(np.prod(box))
+    dof = 3 * n - 3
+    L = md.lib()
+
+    def loss_rows(rows):
+        p = n / vol * 2 * rows[:, 2] / dof + rows[:, 1] / (3 * vol)
+        u = rows[:, 0] / n
+        return (p.mean() - 1.0) ** 2 + (u.mean() + 5.0) ** 2, p.mean(), u.mean()
+
+    def run_forward(sigma=1.0, eps=1.0, timed=False):
+        s = md.System.from_arrays(pos, box, vel=vel, mass=mass, ctx=ctx)
+        traj = md.AdjointTrajectory(ctx)
+        lj = md.LennardJones(sigma, eps, RC, md.Truncation.LinearForceShift)
+        ms = C.c_double()
+        md._check(L.md_context_span_begin(ctx.handle))
+        rows = traj.forward(s, lj, DT, steps, every, skin)
+        md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+        return rows, traj, s, ms.value
+
+    run_forward()  # warm-up: allocations, module load
+    rows, traj, s, fwd_ms = run_forward(timed=True)
+    loss, pm, um = loss_rows(rows)
+    g = np.zeros_like(rows)
+    g[:, 0] = 2 * (um + 5.0) / (n * steps)
+    g[:, 1] = 2 * (pm - 1.0) / (3 * vol * steps)
+    g[:, 2] = 2 * (pm - 1.0) * (n / vol) * 2 / (dof * steps)
+    ms = C.c_double()
+    md._check(L.md_context_span_begin(ctx.handle))
+    d_eps, d_sig, gx, gv = traj.backward(g)
+    md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+    bwd_ms = ms.value
+    def fd(h):
+        e = (loss_rows(run_forward(eps=1 + h)[0])[0] - loss_rows(run_forward(eps=1 - h)[0])[0]) / (2 * h)
+        s_ = (loss_rows(run_forward(sigma=1 + h)[0])[0] -
+              loss_rows(run_forward(sigma=1 - h)[0])[0]) / (2 * h)
+        return e, s_
+
+    fd_eps, fd_sig = fd(1e-6)
+    fd_eps9, fd_sig9 = fd(1e-9)
+    total_ms = group.reduce(fwd_ms + bwd_ms, "max")
+    value = world * n * steps / (total_ms * 1e-3)
+    if rank == 0:
+        line = {
+            "metric": ADJ_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": 1, "ms_per_step": total_ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities",
+            "config": adjoint_config(steps, every, skin),
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+            "loss": loss,
+            "grad": {"d_epsilon": d_eps, "d_sigma": d_sig,
+                     "fd_epsilon": fd_eps, "fd_sigma": fd_sig,
+                     "rel_err_epsilon": abs(d_eps - fd_eps) / abs(fd_eps),
+                     "rel_err_sigma": abs(d_sig - fd_sig) / abs(fd_sig),
+                     "fd_step": "central, h = 1e-6 relative",
+                     "fd_h1e-9": {"fd_epsilon": fd_eps9, "fd_sigma": fd_sig9,
+                                  "rel_err_epsilon": abs(d_eps - fd_eps9) / abs(fd_eps9),
+                                  "rel_err_sigma": abs(d_sig - fd_sig9) / abs(fd_sig9)},
+                     "d_x0_norm": float(np.linalg.norm(gx))},
+        }
+        if world == 1 and not args.no_cpu:
+            kind, cval, _ = cpu_reference(pos, vel, box, max(1, args.cpu_steps) * 4, 1)
+            line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": 1, "kind": kind,
+                                    "sample": f"{max(1, args.cpu_steps) * 4} reference NVE VV "
+                                              f"steps (forward only) of the same 32000-atom state, "
+                                              f"1 thread ({cpu_model()})"}
+        print(json.dumps(line), flush=True)
+    group.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--workload", default="lj1m", choices=["lj1m", "batch"],
-                    help="lj1m: the headline 1M-atom run; batch: 48 NHC replicas")
+    ap.add_argument("--workload", default="lj1m", choices=["lj1m", "batch", "adjoint"],
+                    help="lj1m: the headline 1M-atom run; batch: 48 NHC replicas; adjoint: "
+                         "forward + backward of a 32,000-atom differentiable trajectory "
+                         "(--steps is its length)")
+    ap.add_argument("--adj-skin", type=float, default=2.0)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
@@ -640,6 +755,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.workload == "batch":
         return run_batch_arm(args)
+    if args.workload == "adjoint":
+        return run_adjoint_arm(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

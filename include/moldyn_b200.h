@@ -368,6 +368,13 @@ MD_API int md_adjoint_backward(md_adjoint* adj, const double* grad_rows, double 
 MD_API int md_lj_hvp(const md_lj* lj, md_system* sys, md_verlet* list, const double* u, double* out,
                      double dtheta[2]);
 
+/* Derivatives of the Ewald sum (no reference counterpart).  Charge gradient of
+ * the Coulomb energy, real + reciprocal + self + intramolecular terms
+ * (ewald.cpp:33-175): dedq[i] = dE/dq_i (n, caller's order).  Hessian-vector
+ * product of the real-space Coulomb forces: out = (dF_real/dx)^T u (n x 3). */
+MD_API int md_ewald_charge_gradient(md_ewald* ff, md_system* sys, double* dedq);
+MD_API int md_ewald_real_hvp(md_ewald* ff, md_system* sys, const double* u, double* out);
+
 /* Fused device loop of a constrained integrator with SPC/E forces (the
  * water_rdf-style NVE / NHC production loop): forces are (re)computed on entry,
  * neighbour rebuilds are decided on the device.  thermo (nullable, steps*4):

@@ -178,6 +178,8 @@ def _load():
                                          C.c_double, _d]),
         "md_adjoint_backward": (C.c_int, [_vp, _d, _d, _d, _d]),
         "md_lj_hvp": (C.c_int, [_vp, _vp, _vp, _d, _d, _d]),
+        "md_ewald_charge_gradient": (C.c_int, [_vp, _vp, _d]),
+        "md_ewald_real_hvp": (C.c_int, [_vp, _vp, _d, _d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -574,6 +576,19 @@ class Ewald:
 
     def accumulate_forces(self, sys):
         return self._run(sys, 2)
+
+    def charge_gradient(self, sys):
+        """dE/dq_i of the Coulomb energy (real + reciprocal + self + intramolecular)."""
+        out = np.zeros(sys.n)
+        _check(lib().md_ewald_charge_gradient(self._h, sys.handle, _ptr(out)))
+        return out
+
+    def real_space_hvp(self, sys, u):
+        """(dF_real/dx)^T u for a per-atom field u (N, 3)."""
+        u = _f64(u).reshape(sys.n, 3)
+        out = np.zeros((sys.n, 3))
+        _check(lib().md_ewald_real_hvp(self._h, sys.handle, _ptr(u), _ptr(out)))
+        return out
 
     def alpha(self):
         a = C.c_double()

@@ -296,10 +296,13 @@ __global__ void k_structure_final(const double2* __restrict__ part, int slices, 
 
 // Reciprocal-space forces (ewald.cpp:163-170), one thread per site, k vectors in
 // (nx, ny) lines with exp(i nz c z) stepped along each line.
+// CHARGE: instead of forces, dE_recip/dq_s = sum over the half space of
+// 4 factor Re(conj(S) e^{i k.r_s}) into dq[s] (added).
+template <bool CHARGE>
 __global__ void __launch_bounds__(kBlock)
 k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int64_t n, KArgs ka,
               const int4* __restrict__ lines, int nlines, const double2* __restrict__ sk,
-              double* fxo, double* fyo, double* fzo) {
+              double* fxo, double* fyo, double* fzo, double* dq) {
     const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (s >= n) return;
     const double4 p = pos[s];
@@ -336,17 +339,124 @@ k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int
             const double2 e = cmul(XY, Z);
             const double4 kv = ka.kvec[k];
             const double2 S = sk[k];
-            // 2 (half space) * factor * 2 * q * (Re S sin - Im S cos)
-            const double coeff = 4.0 * kv.w * qs * (S.x * e.y - S.y * e.x);
-            fx = fma(coeff, kv.x, fx);
-            fy = fma(coeff, kv.y, fy);
-            fz = fma(coeff, kv.z, fz);
+            if (CHARGE) {
+                fx += 4.0 * kv.w * (S.x * e.x + S.y * e.y);
+            } else {
+                // 2 (half space) * factor * 2 * q * (Re S sin - Im S cos)
+                const double coeff = 4.0 * kv.w * qs * (S.x * e.y - S.y * e.x);
+                fx = fma(coeff, kv.x, fx);
+                fy = fma(coeff, kv.y, fy);
+                fz = fma(coeff, kv.z, fz);
+            }
             Z = cmul(Z, ez);
         }
     }
-    fxo[s] += fx;
-    fyo[s] += fy;
-    fzo[s] += fz;
+    if (CHARGE) {
+        dq[s] += fx;
+    } else {
+        fxo[s] += fx;
+        fyo[s] += fy;
+        fzo[s] += fz;
+    }
+}
+
+__global__ void k_to_slot4(const int* __restrict__ slot, int64_t n, const double4* in, double4* out) {
+    const int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (o < n) out[slot[o]] = in[o];
+}
+
+__global__ void k_to_orig4(const int* __restrict__ orig, int64_t n, const double4* in, double4* out) {
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s < n) out[orig[s]] = in[s];
+}
+
+__global__ void k_to_orig1(const int* __restrict__ orig, int64_t n, const double* in, double* out) {
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s < n) out[orig[s]] = in[s];
+}
+
+// Charge gradient of the real-space and intramolecular terms, plus the self
+// term, per atom (device order):
+//   dE/dq_i = sum_j C q_j erfc(a r)/r (other molecules, r < rc)
+//           - sum_j C q_j erf(a r)/r (same molecule) - 2 C a/sqrt(pi) q_i
+__global__ void __launch_bounds__(kBlock)
+k_ewald_dq(const double4* __restrict__ pos, const double* __restrict__ q,
+           const int64_t* __restrict__ mol, const int* __restrict__ nbr,
+           const int* __restrict__ count, int stride, const int* __restrict__ orig,
+           const int* __restrict__ slot, const int* __restrict__ off,
+           const int* __restrict__ partner, int64_t n, Box3 box, RealArgs a, double* dq) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const Fold3 f3 = fold3_of(box);
+    const double4 pi = pos[i];
+    const int64_t mi = mol[i];
+    double acc = 0.0;
+    const int cnt = min(count[i], stride);
+    const int* row = nbr + i * static_cast<int64_t>(stride);
+    for (int k = 0; k < cnt; ++k) {
+        const int j = __ldg(row + k);
+        if (mol[j] == mi) continue;
+        const double4 pj = ldg4(pos + j);
+        double dx, dy, dz;
+        min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < a.rc2)) continue;
+        const double r = sqrt(r2);
+        acc += a.coulomb * q[j] * erfc(a.alpha * r) / r;
+    }
+    const int oi = orig[i];
+    for (int p = off[oi]; p < off[oi + 1]; ++p) {
+        const int j = slot[partner[p]];
+        const double4 pj = pos[j];
+        double dx, dy, dz;
+        min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        acc -= a.coulomb * q[j] * erf(a.alpha * r) / r;
+    }
+    acc -= a.coulomb * a.two_alpha_over_sqrt_pi * q[i];  // 2 C a / sqrt(pi) q_i
+    dq[i] = acc;
+}
+
+// Hessian-vector product of the real-space Coulomb forces (other molecules,
+// r < rc): out_i = sum_j [g (u_i - u_j) + 2 g' d (d . (u_i - u_j))] with
+// F_i = sum_j g(r^2) d, g = C q_i q_j (A e^{-a^2 r^2}/r^2 + erfc(a r)/r^3), A = 2a/sqrt(pi).
+__global__ void __launch_bounds__(kBlock)
+k_ewald_real_hvp(const double4* __restrict__ pos, const double* __restrict__ q,
+                 const int64_t* __restrict__ mol, const int* __restrict__ nbr,
+                 const int* __restrict__ count, int stride, int64_t n, Box3 box, RealArgs a,
+                 const double4* __restrict__ u, double4* out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const Fold3 f3 = fold3_of(box);
+    const double4 pi = pos[i], ui = u[i];
+    const int64_t mi = mol[i];
+    const double qi = q[i];
+    const double a3 = a.alpha * a.alpha * a.two_alpha_over_sqrt_pi;  // 2 a^3 / sqrt(pi)
+    const double a1 = 1.5 * a.two_alpha_over_sqrt_pi;                 // 3 a / sqrt(pi)
+    double hx = 0.0, hy = 0.0, hz = 0.0;
+    const int cnt = min(count[i], stride);
+    const int* row = nbr + i * static_cast<int64_t>(stride);
+    for (int k = 0; k < cnt; ++k) {
+        const int j = __ldg(row + k);
+        if (mol[j] == mi) continue;
+        const double4 pj = ldg4(pos + j);
+        double dx, dy, dz;
+        min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
+        const double s = dx * dx + dy * dy + dz * dz;
+        if (!(s < a.rc2)) continue;
+        const double r = sqrt(s);
+        const double cqq = a.coulomb * qi * q[j];
+        const double ex = exp(a.neg_alpha2 * s), ec = erfc(a.alpha * r);
+        const double g = cqq * (a.two_alpha_over_sqrt_pi * ex / s + ec / (s * r));
+        const double gs = -cqq * (a3 * ex / s + a1 * ex / (s * s) + 1.5 * ec / (s * s * r));
+        const double4 uj = u[j];
+        const double ux = ui.x - uj.x, uy = ui.y - uj.y, uz = ui.z - uj.z;
+        const double dm = dx * ux + dy * uy + dz * uz;
+        hx += g * ux + 2.0 * gs * dx * dm;
+        hy += g * uy + 2.0 * gs * dy * dm;
+        hz += g * uz + 2.0 * gs * dz * dm;
+    }
+    out[i] = make_double4(hx, hy, hz, 0.0);
 }
 
 template <int TPA>
@@ -518,6 +628,38 @@ int ewald_list(md_ewald* ew, md_system* sys) {
 // mode: 0 energies only, 1 zero + accumulate forces, 2 accumulate onto forces.
 // gated: the neighbour list is maintained by device-decided rebuilds (no host
 // synchronisation; the list must already be built for this system).
+RealArgs real_args_of(const md_ewald* ew, double alpha) {
+    RealArgs a;
+    a.rc2 = ew->cutoff * ew->cutoff;
+    a.alpha = alpha;
+    a.coulomb = coulomb_prefactor();
+    a.two_alpha_over_sqrt_pi = 2.0 * alpha / std::sqrt(kPi);
+    a.neg_alpha2 = -alpha * alpha;
+    a.spce_lj = ew->spce ? 1 : 0;
+    a.sig2 = ew->sigma_o * ew->sigma_o;
+    a.four_eps = 4.0 * ew->epsilon_o;
+    a.tf_eps = 24.0 * ew->epsilon_o;
+    a.lj_lfs = ew->lj_truncation == MD_LINEAR_FORCE_SHIFT ? 1 : 0;
+    a.rc = ew->cutoff;
+    // lennard_jones.cpp:32-48
+    const double s2 = a.sig2 / a.rc2, s6 = s2 * s2 * s2;
+    a.uc = 4.0 * ew->epsilon_o * (s6 * s6 - s6);
+    a.dudrc = -(24.0 * ew->epsilon_o * (2.0 * s6 * s6 - s6)) / ew->cutoff;
+    return a;
+}
+
+KArgs kargs_of(md_ewald* ew, const md_system* sys) {
+    KArgs ka;
+    ka.kvec = ew->kvec.as<double4>();
+    ka.kn = ew->kn.as<int4>();
+    ka.nk = ew->nk;
+    ka.kmax = ew->kmax;
+    ka.a = 2.0 * kPi / sys->box[0];
+    ka.b = 2.0 * kPi / sys->box[1];
+    ka.c = 2.0 * kPi / sys->box[2];
+    return ka;
+}
+
 int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
@@ -532,24 +674,7 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
         MDB_TRY(ewald_list(ew, sys));
     }
     md_verlet* v = ew->list;
-    RealArgs a;
-    a.rc2 = ew->cutoff * ew->cutoff;
-    a.alpha = alpha;
-    a.coulomb = coulomb_prefactor();
-    a.two_alpha_over_sqrt_pi = 2.0 * alpha / std::sqrt(kPi);
-    a.neg_alpha2 = -alpha * alpha;
-    a.spce_lj = ew->spce ? 1 : 0;
-    a.sig2 = ew->sigma_o * ew->sigma_o;
-    a.four_eps = 4.0 * ew->epsilon_o;
-    a.tf_eps = 24.0 * ew->epsilon_o;
-    a.lj_lfs = ew->lj_truncation == MD_LINEAR_FORCE_SHIFT ? 1 : 0;
-    a.rc = ew->cutoff;
-    {
-        // lennard_jones.cpp:32-48
-        const double s2 = a.sig2 / a.rc2, s6 = s2 * s2 * s2;
-        a.uc = 4.0 * ew->epsilon_o * (s6 * s6 - s6);
-        a.dudrc = -(24.0 * ew->epsilon_o * (2.0 * s6 * s6 - s6)) / ew->cutoff;
-    }
+    const RealArgs a = real_args_of(ew, alpha);
     double* res = ctx_result(ctx, kResEwald);
     const Box3 box{{sys->box[0], sys->box[1], sys->box[2]},
                    {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}};
@@ -586,14 +711,7 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
     }
     // reciprocal space
     ctx_time_begin(ctx, MD_KERNEL_EWALD_RECIP);
-    KArgs ka;
-    ka.kvec = ew->kvec.as<double4>();
-    ka.kn = ew->kn.as<int4>();
-    ka.nk = ew->nk;
-    ka.kmax = ew->kmax;
-    ka.a = 2.0 * kPi / sys->box[0];
-    ka.b = 2.0 * kPi / sys->box[1];
-    ka.c = 2.0 * kPi / sys->box[2];
+    const KArgs ka = kargs_of(ew, sys);
     if (ew->nk > 0 && n > 0) {
         const int kblocks = (ew->nk + kBlock - 1) / kBlock;
         // enough site slices to give every SM a few blocks
@@ -616,9 +734,9 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
             ew->skpart.as<double2>(), static_cast<int>(slices), ka, 1.0 / (2.0 * alpha * alpha),
             ew->sk.as<double2>(), rp, ctx_counter(ctx, 7), res + kEwRecip);
         if (mode != 0)
-            k_recip_force<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+            k_recip_force<false><<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
                 sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines,
-                ew->sk.as<double2>(), sys->cur.fx, sys->cur.fy, sys->cur.fz);
+                ew->sk.as<double2>(), sys->cur.fx, sys->cur.fy, sys->cur.fz, nullptr);
     } else {
         MDB_CUDA(cudaMemsetAsync(res + kEwRecip, 0, 2 * sizeof(double), ctx->stream));
     }
@@ -708,6 +826,94 @@ int md_ewald_compute(md_ewald* ew, md_system* sys, int mode, double terms[4], do
     MDB_TRY(ewald_read(ew, sys->ctx));
     fill_terms(ew, terms, virial);
     return MD_OK;
+}
+
+namespace {
+
+// per-atom vectors between the caller's order (n x 3 host) and device double4
+int upload_vec(md_system* sys, const double* u, double4* dev_orig, double4* dev) {
+    const int64_t n = sys->n;
+    std::vector<double4> h(static_cast<size_t>(n));
+    for (int64_t o = 0; o < n; ++o) h[o] = make_double4(u[3 * o], u[3 * o + 1], u[3 * o + 2], 0.0);
+    MDB_CUDA(cudaMemcpyAsync(dev_orig, h.data(), sizeof(double4) * n, cudaMemcpyHostToDevice,
+                             sys->ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+    k_to_slot4<<<grid_for(n, kBlock), kBlock, 0, sys->ctx->stream>>>(sys->slot, n, dev_orig, dev);
+    return MD_OK;
+}
+
+}  // namespace
+
+int md_ewald_charge_gradient(md_ewald* ew, md_system* sys, double* dedq) {
+    if (!ew || !sys || !dedq) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_charge_gradient: NULL");
+    if (sys->ctx != ew->ctx)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_charge_gradient: context mismatch");
+    const int64_t n = sys->n;
+    if (n == 0) return MD_OK;
+    md_context* ctx = sys->ctx;
+    // energies (also builds the list, topology, k vectors and S(k))
+    MDB_TRY(ewald_eval_async(ew, sys, 0, false));
+    DevBuf buf;
+    MDB_TRY(buf.ensure(2 * sizeof(double) * static_cast<size_t>(n)));
+    double* dq = buf.as<double>();
+    double* dq_o = dq + n;
+    const Box3 box{{sys->box[0], sys->box[1], sys->box[2]},
+                   {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}};
+    const RealArgs a = real_args_of(ew, ew->alpha);
+    md_verlet* v = ew->list;
+    const int g = grid_for(n, kBlock);
+    k_ewald_dq<<<g, kBlock, 0, ctx->stream>>>(
+        sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
+        v->stride, sys->cur.orig, sys->slot, ew->partner_off.as<int>(), ew->partner_idx.as<int>(),
+        n, box, a, dq);
+    if (ew->nk > 0)
+        k_recip_force<true><<<g, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->cur.charge, n, kargs_of(ew, sys), ew->lines.as<int4>(), ew->nlines,
+            ew->sk.as<double2>(), nullptr, nullptr, nullptr, dq);
+    k_to_orig1<<<g, kBlock, 0, ctx->stream>>>(sys->cur.orig, n, dq, dq_o);
+    ctx->launches += 3;
+    MDB_CHECK_LAUNCH();
+    MDB_CUDA(cudaMemcpyAsync(dedq, dq_o, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    buf.release();
+    return ctx_check_status(ctx);
+}
+
+int md_ewald_real_hvp(md_ewald* ew, md_system* sys, const double* u, double* out) {
+    if (!ew || !sys || !u || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_real_hvp: NULL");
+    if (sys->ctx != ew->ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_real_hvp: context mismatch");
+    const int64_t n = sys->n;
+    if (n == 0) return MD_OK;
+    md_context* ctx = sys->ctx;
+    MDB_TRY(ewald_eval_async(ew, sys, 0, false));  // list and alpha for this state
+    DevBuf buf;
+    MDB_TRY(buf.ensure(4 * sizeof(double4) * static_cast<size_t>(n)));
+    double4* uo = buf.as<double4>();
+    double4* ud = uo + n;
+    double4* res = uo + 2 * n;
+    double4* res_o = uo + 3 * n;
+    MDB_TRY(upload_vec(sys, u, uo, ud));
+    const Box3 box{{sys->box[0], sys->box[1], sys->box[2]},
+                   {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}};
+    md_verlet* v = ew->list;
+    const int g = grid_for(n, kBlock);
+    k_ewald_real_hvp<<<g, kBlock, 0, ctx->stream>>>(sys->cur.pos, sys->cur.charge, sys->cur.mol,
+                                                   v->nbr.as<int>(), v->count.as<int>(), v->stride,
+                                                   n, box, real_args_of(ew, ew->alpha), ud, res);
+    k_to_orig4<<<g, kBlock, 0, ctx->stream>>>(sys->cur.orig, n, res, res_o);
+    ctx->launches += 3;
+    MDB_CHECK_LAUNCH();
+    std::vector<double4> h(static_cast<size_t>(n));
+    MDB_CUDA(cudaMemcpyAsync(h.data(), res_o, sizeof(double4) * n, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    buf.release();
+    for (int64_t o = 0; o < n; ++o) {
+        out[3 * o] = h[o].x;
+        out[3 * o + 1] = h[o].y;
+        out[3 * o + 2] = h[o].z;
+    }
+    return ctx_check_status(ctx);
 }
 
 int md_ewald_alpha(const md_ewald* ew, double* alpha) {

@@ -137,3 +137,48 @@ def test_ewald_alpha_override_matches_oracle(md):
                        kmax=7, alpha=0.3, forces=False)
     for k in ("real", "reciprocal", "self", "intra"):
         assert approx_eq(t[k], ot[k], 1e-12), (k, t[k], ot[k])
+
+
+def test_charge_gradient_matches_differences(md):
+    """dE/dq_i of the Coulomb energy (real + reciprocal + self + intra) against
+    central differences; the energy is quadratic in each charge, so the
+    differences are exact up to rounding."""
+    s = water(md, 1)
+    ew = md.Ewald(10.0, 5)
+    dedq = ew.charge_gradient(s)
+    q0 = s.charges
+    rng = np.random.default_rng(3)
+    for i in rng.integers(0, s.n, 6):
+        h = 1e-3 * abs(q0[i])
+        e = []
+        for sign in (1, -1):
+            q = q0.copy()
+            q[i] += sign * h
+            s.charges = q
+            e.append(ew.compute_energies(s).total())
+        s.charges = q0
+        fd = (e[0] - e[1]) / (2 * h)
+        assert abs(dedq[i] - fd) < 1e-8 * abs(fd), (i, dedq[i], fd)
+
+
+def test_real_space_hvp_matches_force_differences(md):
+    """With every site its own molecule and no k vectors the Ewald force is the
+    real-space force alone; its Hessian-vector product against differences."""
+    rng = np.random.default_rng(5)
+    pos = SPCE["pos1"][::3].copy()  # oxygens: no two sites closer than ~2.5 A
+    n = pos.shape[0]
+    box = SPCE["box1"]
+    q = rng.choice([-0.8, 0.8], size=n)
+    s = md.System.from_arrays(pos, box, charge=q, mol=np.arange(n))
+    ew = md.Ewald(8.0, 0)
+    u = rng.normal(size=(n, 3))
+    hvp = ew.real_space_hvp(s, u)
+    h = 1e-5
+
+    def forces(p):
+        t = md.System.from_arrays(p, box, charge=q, mol=np.arange(n))
+        md.Ewald(8.0, 0).compute_forces(t)
+        return t.forces
+
+    fd = (forces(pos + h * u) - forces(pos - h * u)) / (2 * h)
+    assert np.max(np.abs(hvp - fd)) < 1e-6 * np.max(np.abs(fd))
