@@ -728,13 +728,113 @@ def run_adjoint_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- water workload
+WATER_METRIC = "site-steps/s, 4096 rigid SPC/E molecules, Ewald, Nose-Hoover 298 K, 1 B200"
+WATER_ALPHA, WATER_KMAX, WATER_RC, WATER_L = 0.34, 18, 10.0, 49.72
+TAU_PS = 1.0966875353  # internal time unit in ps (core/units.hpp:33)
+
+
+def water_config(steps):
+    return {"workload": f"4096 rigid SPC/E molecules (12,288 sites) on a seeded random-orientation "
+                        f"lattice at 0.997 g/cm^3, L={WATER_L} A; Ewald rc={WATER_RC} A, "
+                        f"alpha={WATER_ALPHA}/A, kmax={WATER_KMAX} (half space |n|^2 < kmax^2+2); "
+                        f"O-O LJ truncated + tail; RATTLE velocity Verlet + Nose-Hoover chain "
+                        f"(M=3, tau=0.1 ps) at 298 K, dt=2 fs, {steps} steps after equilibration",
+            "sites": 12288, "precision": "FP64 (real and reciprocal space)",
+            "parallelism": "one system"}
+
+
+def run_water_arm(args):
+    world, rank, local = dist_env()
+    group = Group(world)
+    import moleculardynamics_b200 as md
+    fs = lambda x: x * 1e-3 / TAU_PS
+    w = md.water_lattice(16, WATER_L, SEED)
+    if args.impl == "reference" or (rank == 0 and not args.no_cpu):
+        import oracle as O
+        q = np.array([-0.8476 if t == "O" else 0.4238 for t in w["types"]])
+        mol = np.arange(len(w["types"])) // 3
+        t0 = time.perf_counter()
+        O.spce(w["pos"], w["box"], q, mol, cutoff=WATER_RC, kmax=WATER_KMAX, alpha=WATER_ALPHA)
+        cpu_sec = time.perf_counter() - t0
+        cpu = {"value": 12288 / cpu_sec, "unit": "site-steps/s", "cores": 1, "kind": "port",
+               "sample": "one SPC/E force evaluation (the oracle's C restatement of "
+                         "SpceForceField with the alpha override, brute-force real space) on the "
+                         f"12,288-site lattice, 1 thread ({cpu_model()}); forces only, no step"}
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({
+                    "metric": WATER_METRIC, "value": cpu["value"], "unit": "site-steps/s",
+                    "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * cpu_sec,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f64", "data": "synthetic water lattice", "config": water_config(1),
+                    "impl": "reference", "cpu_baseline": cpu,
+                    "e2e": {"value": cpu["value"], "unit": "site-steps/s",
+                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+            group.close()
+            return 0
+    ctx = md.Context(local)
+    s = md.build_spce_system(w["pos"], w["types"], w["box"], ctx=ctx)
+    m = s.masses
+    rng = np.random.default_rng(SEED)
+    s.velocities = np.sqrt(298.0 / m)[:, None] * rng.normal(size=(s.n, 3))
+    s.remove_center_of_mass_motion()
+    rw = md.RigidWater(1.0, 109.47)
+    rw.constrain_velocities(s)
+    ff = md.SpceForceField(cutoff=WATER_RC, kmax=WATER_KMAX, alpha=WATER_ALPHA, ctx=ctx)
+    dof = md.RigidWater.degrees_of_freedom(4096, True)
+    md.ConstrainedNoseHooverChain(fs(0.5), rw, 298.0, fs(50.0), 3, dof).run(s, ff, args.equil_water)
+    integ = md.ConstrainedNoseHooverChain(fs(2.0), rw, 298.0, fs(100.0), 3, dof)
+    integ.run(s, ff, args.warmup)
+    L = md.lib()
+    launches0 = ctx.launch_count()
+    clocks = ClockSampler(local)
+    clocks.__enter__()
+    ms = C.c_double()
+    md._check(L.md_context_span_begin(ctx.handle))
+    th = integ.run(s, ff, args.steps, thermo=True)
+    md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+    clocks.__exit__(None, None, None)
+    launches = ctx.launch_count() - launches0
+    dev_ms = group.reduce(ms.value, "max")
+    value = world * 12288 * args.steps / (dev_ms * 1e-3)
+    h = th[:, 0] + th[:, 2] + th[:, 3]
+    # reciprocal truncation: forces at kmax against kmax + 8 on the final state
+    f_ref = None
+    ff.compute_forces(s)
+    f_run = s.forces
+    md.SpceForceField(cutoff=WATER_RC, kmax=WATER_KMAX + 8, alpha=WATER_ALPHA, ctx=ctx).compute_forces(s)
+    f_ref = s.forces
+    ferr = float(np.sqrt(np.sum((f_run - f_ref) ** 2) / np.sum(f_ref ** 2)))
+    if rank == 0:
+        line = {
+            "metric": WATER_METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded rigid-water lattice, Maxwell-Boltzmann velocities, "
+                    f"{args.equil_water} NHC steps of 0.5 fs",
+            "config": water_config(args.steps), "gpu_launches": int(launches),
+            "nhc_extended_energy_drift_K": {"max_abs": float(np.max(np.abs(h - h[0]))),
+                                            "relative": float(np.max(np.abs(h - h[0])) / abs(h[0]))},
+            "mean_temperature_K": float(np.mean(2 * th[:, 2] / dof)),
+            "force_rel_rms_vs_kmax+8": ferr,
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    group.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--workload", default="lj1m", choices=["lj1m", "batch", "adjoint"],
+    ap.add_argument("--workload", default="lj1m", choices=["lj1m", "batch", "adjoint", "water"],
                     help="lj1m: the headline 1M-atom run; batch: 48 NHC replicas; adjoint: "
                          "forward + backward of a 32,000-atom differentiable trajectory "
                          "(--steps is its length)")
     ap.add_argument("--adj-skin", type=float, default=2.0)
+    ap.add_argument("--equil-water", type=int, default=1000)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
@@ -757,6 +857,8 @@ def main():
         return run_batch_arm(args)
     if args.workload == "adjoint":
         return run_adjoint_arm(args)
+    if args.workload == "water":
+        return run_water_arm(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

@@ -903,6 +903,36 @@ class Batch:
 
 
 # ---------------------------------------------------------------- setup
+def water_lattice(per_side, box_length, seed, params=SpceParameters):
+    """A simple cubic lattice of rigid SPC/E molecules (per_side^3 molecules in a
+    cubic box of side box_length, oxygens at the cell centres, each molecule
+    turned by a seeded random rotation); O, H, H order, rOH and the HOH angle of
+    `params`.  Host-side setup, no reference counterpart (the reference reads
+    its water from the NIST configuration files)."""
+    rng = np.random.default_rng(seed)
+    a = box_length / per_side
+    half = 0.5 * np.radians(params.angleHOH)
+    local = np.array([[0.0, 0.0, 0.0],
+                      [params.rOH * np.sin(half), 0.0, params.rOH * np.cos(half)],
+                      [-params.rOH * np.sin(half), 0.0, params.rOH * np.cos(half)]])
+    m = per_side ** 3
+    q = rng.normal(size=(m, 4))
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    w, x, y, z = q.T
+    rot = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+    idx = np.arange(m)
+    centre = (np.stack([idx % per_side, (idx // per_side) % per_side, idx // per_side ** 2], 1)
+              + 0.5) * a - 0.5 * box_length
+    pos = centre[:, None, :] + np.einsum("mij,kj->mki", rot, local)
+    pos = pos.reshape(-1, 3)
+    pos -= box_length * np.floor(pos / box_length + 0.5)
+    types = ["O", "H", "H"] * m
+    return dict(pos=pos, types=types, box=np.full(3, float(box_length)))
+
+
 def fcc_lattice(cells, density, temperature, seed):
     """util/lattice.cpp:15-64 (host-side setup).  Returns dict(pos, vel, mass, box)."""
     n = 4 * int(cells) ** 3
