@@ -15,6 +15,7 @@
 // index divisible by 3, as SpceForceField::gatherOxygens takes them) in the same
 // pass over the real-space list.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <new>
 #include <unordered_map>
@@ -296,15 +297,21 @@ __global__ void k_structure_final(const double2* __restrict__ part, int slices, 
 
 // Reciprocal-space forces (ewald.cpp:163-170), one thread per site, k vectors in
 // (nx, ny) lines with exp(i nz c z) stepped along each line.
-// CHARGE: instead of forces, dE_recip/dq_s = sum over the half space of
-// 4 factor Re(conj(S) e^{i k.r_s}) into dq[s] (added).
+// k-space forces (or, with CHARGE, dE_recip/dq_s = sum over the half space of
+// 4 factor Re(conj(S) e^{i k.r_s})) over a 2-D grid: blockIdx.x picks 256 sites,
+// blockIdx.y a slice of the (nx, ny) lines of k vectors, so small systems still
+// fill the GPU.  Each slice starts its e^{i nx a x}, e^{i ny b y} factors with
+// sincos and continues by complex recurrence along its lines; its partial sums go
+// to part[slice][site] and k_recip_sum adds the slices in order (deterministic).
 template <bool CHARGE>
 __global__ void __launch_bounds__(kBlock)
 k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int64_t n, KArgs ka,
-              const int4* __restrict__ lines, int nlines, const double2* __restrict__ sk,
-              double* fxo, double* fyo, double* fzo, double* dq) {
+              const int4* __restrict__ lines, int nlines, int lines_per_slice,
+              const double2* __restrict__ sk, double4* __restrict__ part) {
     const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (s >= n) return;
+    const int l0 = blockIdx.y * lines_per_slice;
+    const int l1 = min(nlines, l0 + lines_per_slice);
     const double4 p = pos[s];
     const double qs = q[s];
     double sn, cs;
@@ -314,22 +321,29 @@ k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int
     const double2 ey = make_double2(cs, sn);
     sincos(ka.c * p.z, &sn, &cs);
     const double2 ez = make_double2(cs, sn);
-    sincos(-ka.kmax * ka.b * p.y, &sn, &cs);
-    const double2 ey0 = make_double2(cs, sn);
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    double2 X = make_double2(1.0, 0.0), Y = ey0;
-    int cur_nx = 0, cur_ny = -ka.kmax;
-    for (int l = 0; l < nlines; ++l) {
+    double2 X = make_double2(1.0, 0.0), Y = make_double2(1.0, 0.0);
+    int cur_nx = INT_MIN, cur_ny = INT_MIN;
+    for (int l = l0; l < l1; ++l) {
         const int4 L = lines[l];  // nx, ny, nz0, first k index; count in next line's .w
-        while (cur_nx < L.x) {
-            X = cmul(X, ex);
-            ++cur_nx;
-            Y = ey0;
-            cur_ny = -ka.kmax;
+        if (L.x != cur_nx) {
+            if (cur_nx != INT_MIN && L.x == cur_nx + 1) {
+                X = cmul(X, ex);
+            } else {
+                sincos(static_cast<double>(L.x) * ka.a * p.x, &sn, &cs);
+                X = make_double2(cs, sn);
+            }
+            cur_nx = L.x;
+            cur_ny = INT_MIN;
         }
-        while (cur_ny < L.y) {
-            Y = cmul(Y, ey);
-            ++cur_ny;
+        if (L.y != cur_ny) {
+            if (cur_ny != INT_MIN && L.y == cur_ny + 1) {
+                Y = cmul(Y, ey);
+            } else {
+                sincos(static_cast<double>(L.y) * ka.b * p.y, &sn, &cs);
+                Y = make_double2(cs, sn);
+            }
+            cur_ny = L.y;
         }
         const double2 XY = cmul(X, Y);
         sincos(static_cast<double>(L.z) * ka.c * p.z, &sn, &cs);
@@ -351,6 +365,22 @@ k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int
             Z = cmul(Z, ez);
         }
     }
+    part[blockIdx.y * n + s] = make_double4(fx, fy, fz, 0.0);
+}
+
+// Adds the slices' partial k-space forces (CHARGE: charge gradients) in order.
+template <bool CHARGE>
+__global__ void k_recip_sum(const double4* __restrict__ part, int slices, int64_t n, double* fxo,
+                            double* fyo, double* fzo, double* dq) {
+    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (s >= n) return;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int k = 0; k < slices; ++k) {
+        const double4 v = part[k * n + s];
+        fx += v.x;
+        fy += v.y;
+        fz += v.z;
+    }
     if (CHARGE) {
         dq[s] += fx;
     } else {
@@ -358,6 +388,14 @@ k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int
         fyo[s] += fy;
         fzo[s] += fz;
     }
+}
+
+// Grid of the k-space force pass: enough line slices to give every SM a few
+// blocks (one slice for large systems).
+int recip_slices(const md_context* ctx, int64_t n, int nlines) {
+    const int64_t site_blocks = (n + kBlock - 1) / kBlock;
+    int64_t slices = (4 * static_cast<int64_t>(ctx->sm_count) + site_blocks - 1) / site_blocks;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(slices, nlines)));
 }
 
 __global__ void k_to_slot4(const int* __restrict__ slot, int64_t n, const double4* in, double4* out) {
@@ -502,6 +540,7 @@ struct md_ewald {
     int k_kmax = -1;
     double k_alpha = 0.0;
     mdb::DevBuf kvec, kn, lines, sk, skpart;
+    mdb::DevBuf rpart;            // per line slice k-space force partials
     int nk = 0, nlines = 0;
     double last[kEwCount] = {0};
     double alpha = 0.0;
@@ -628,6 +667,35 @@ int ewald_list(md_ewald* ew, md_system* sys) {
 // mode: 0 energies only, 1 zero + accumulate forces, 2 accumulate onto forces.
 // gated: the neighbour list is maintained by device-decided rebuilds (no host
 // synchronisation; the list must already be built for this system).
+// k-space forces added to the system's forces (charge = false), or
+// dE_recip/dq added to dq (device order); S(k) must be current.
+int recip_force_async(md_ewald* ew, md_system* sys, const KArgs& ka, bool charge, double* dq) {
+    md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
+    if (n == 0 || ew->nk == 0) return MD_OK;
+    const int slices = recip_slices(ctx, n, ew->nlines);
+    const int per = (ew->nlines + slices - 1) / slices;
+    MDB_TRY(ew->rpart.ensure(sizeof(double4) * static_cast<size_t>(slices) * n));
+    const dim3 grid(static_cast<unsigned>((n + kBlock - 1) / kBlock), static_cast<unsigned>(slices));
+    double4* part = ew->rpart.as<double4>();
+    if (charge) {
+        k_recip_force<true><<<grid, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines, per,
+            ew->sk.as<double2>(), part);
+        k_recip_sum<true><<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+            part, slices, n, nullptr, nullptr, nullptr, dq);
+    } else {
+        k_recip_force<false><<<grid, kBlock, 0, ctx->stream>>>(
+            sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines, per,
+            ew->sk.as<double2>(), part);
+        k_recip_sum<false><<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+            part, slices, n, sys->cur.fx, sys->cur.fy, sys->cur.fz, nullptr);
+    }
+    ctx->launches += 2;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
 RealArgs real_args_of(const md_ewald* ew, double alpha) {
     RealArgs a;
     a.rc2 = ew->cutoff * ew->cutoff;
@@ -733,10 +801,7 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
         k_structure_final<<<kblocks, kBlock, 0, ctx->stream>>>(
             ew->skpart.as<double2>(), static_cast<int>(slices), ka, 1.0 / (2.0 * alpha * alpha),
             ew->sk.as<double2>(), rp, ctx_counter(ctx, 7), res + kEwRecip);
-        if (mode != 0)
-            k_recip_force<false><<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
-                sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines,
-                ew->sk.as<double2>(), sys->cur.fx, sys->cur.fy, sys->cur.fz, nullptr);
+        if (mode != 0) MDB_TRY(recip_force_async(ew, sys, ka, false, nullptr));
     } else {
         MDB_CUDA(cudaMemsetAsync(res + kEwRecip, 0, 2 * sizeof(double), ctx->stream));
     }
@@ -802,6 +867,7 @@ int md_ewald_destroy(md_ewald* ew) {
     ew->kvec.release();
     ew->kn.release();
     ew->lines.release();
+    ew->rpart.release();
     ew->sk.release();
     ew->skpart.release();
     delete ew;
@@ -866,10 +932,7 @@ int md_ewald_charge_gradient(md_ewald* ew, md_system* sys, double* dedq) {
         sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
         v->stride, sys->cur.orig, sys->slot, ew->partner_off.as<int>(), ew->partner_idx.as<int>(),
         n, box, a, dq);
-    if (ew->nk > 0)
-        k_recip_force<true><<<g, kBlock, 0, ctx->stream>>>(
-            sys->cur.pos, sys->cur.charge, n, kargs_of(ew, sys), ew->lines.as<int4>(), ew->nlines,
-            ew->sk.as<double2>(), nullptr, nullptr, nullptr, dq);
+    MDB_TRY(recip_force_async(ew, sys, kargs_of(ew, sys), true, dq));
     k_to_orig1<<<g, kBlock, 0, ctx->stream>>>(sys->cur.orig, n, dq, dq_o);
     ctx->launches += 3;
     MDB_CHECK_LAUNCH();

@@ -166,10 +166,15 @@ __global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const in
     sorted[start[r] + at] = static_cast<int>(k);
 }
 
-// Within each cell, order atoms by original index.  One warp per cell: for up to
-// 32 atoms each lane's rank is the number of smaller keys (keys are distinct); a
-// larger cell falls back to an insertion sort by lane 0.
-__global__ void k_cell_order(int* sorted, const int* __restrict__ start, int m,
+// Within each cell, order atoms by original index.  One warp per cell: each atom's
+// rank is the number of smaller keys (keys are distinct), taken from registers
+// for up to 32 atoms and from shared memory up to kOrderMax; a cell beyond that
+// falls back to an insertion sort by lane 0.
+constexpr int kOrderWarps = 8;   // k_cell_order runs 256-thread blocks
+constexpr int kOrderMax = 512;   // atoms per cell ordered in shared memory
+
+__global__ void __launch_bounds__(32 * kOrderWarps)
+k_cell_order(int* sorted, const int* __restrict__ start, int m,
                              const int* __restrict__ orig, const int* flag) {
     if (!gate(flag)) return;
     const int lane = threadIdx.x & 31;
@@ -186,7 +191,26 @@ __global__ void k_cell_order(int* sorted, const int* __restrict__ start, int m,
         if (lane < c) sorted[s0 + rank] = v;
         return;
     }
-    if (lane != 0) return;
+    if (c <= kOrderMax) {
+        // rank sort by the warp: stage (key, atom) in shared memory, each lane
+        // ranks every 32nd element against all of the cell's keys
+        __shared__ int s_key[kOrderWarps][kOrderMax], s_val[kOrderWarps][kOrderMax];
+        const int w = threadIdx.x >> 5;
+        for (int t = lane; t < c; t += 32) {
+            const int v = sorted[s0 + t];
+            s_val[w][t] = v;
+            s_key[w][t] = orig[v];
+        }
+        __syncwarp();
+        for (int t = lane; t < c; t += 32) {
+            const int key = s_key[w][t];
+            int rank = 0;
+            for (int o = 0; o < c; ++o) rank += s_key[w][o] < key ? 1 : 0;
+            sorted[s0 + rank] = s_val[w][t];
+        }
+        return;
+    }
+    if (lane != 0) return;  // very crowded cells: insertion sort by one thread
     for (int a = s0 + 1; a < s1; ++a) {
         const int v = sorted[a];
         const int key = orig[v];
@@ -268,7 +292,7 @@ __device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, do
 __global__ void __launch_bounds__(kBuildWarps * 32)
 k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
                double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
-               uint32_t* status, int* max_count, const int* flag) {
+               uint32_t* status, int* max_count, const int* flag, int groups) {
     if (!gate(flag)) return;
     // Candidates in pairs, structure-of-arrays within a pair so that two
     // candidates are tested with one packed FP32x2 instruction per step:
@@ -276,7 +300,9 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     __shared__ float4 s_a[kBuildWarps][kMaxCand / 2];
     __shared__ float4 s_b[kBuildWarps][kMaxCand / 2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = blockIdx.x * kBuildWarps + warp;
+    // `groups` warps share a crowded cell, each taking every groups-th run of 32 atoms
+    const int wid = blockIdx.x * kBuildWarps + warp;
+    const int r = wid / groups, grp = wid % groups;
     if (r >= g.ncells) return;
     const int cell = g.cell_of_rank[r];
     const int cx = cell % g.nx, cy = (cell / g.nx) % g.ny, cz = cell / (g.nx * g.ny);
@@ -338,7 +364,7 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
             B[3] = __int_as_float(-1);
         }
         __syncwarp();
-        for (int ib = a0; ib < a1; ib += 32) {
+        for (int ib = a0 + 32 * grp; ib < a1; ib += 32 * groups) {
             const int i = ib + lane;
             const bool active = i < a1;
             double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -618,9 +644,13 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
             ctx->launches += 2;
         }
         const GridArgs g = make_args(v->grid, sys);
-        k_verlet_cells<<<grid_for(v->grid.ncells, kBuildWarps), kBuildWarps * 32, 0, ctx->stream>>>(
+        // warps per cell from the mean occupancy (crowded cells, e.g. a long cutoff)
+        const double mean = static_cast<double>(n) / v->grid.ncells;
+        const int groups = static_cast<int>(std::min(16.0, std::max(1.0, std::ceil(1.5 * mean / 32.0))));
+        const int64_t warps = static_cast<int64_t>(v->grid.ncells) * groups;
+        k_verlet_cells<<<grid_for(warps, kBuildWarps), kBuildWarps * 32, 0, ctx->stream>>>(
             sys->cur.pos, start, g, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
-            ctx->d_status, v->d_max_count, flag);
+            ctx->d_status, v->d_max_count, flag, groups);
         ++ctx->launches;
     } else if (n > 0) {
         k_verlet_brute<<<grid_for(n * 32, kBlock), kBlock, 0, ctx->stream>>>(
