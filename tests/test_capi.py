@@ -80,3 +80,18 @@ def test_rigid_water_host_side():
     assert rw.oh_distance() == orw.oh and rw.hh_distance() == orw.hh
     assert md.RigidWater.degrees_of_freedom(100, True) == 597
     assert md.RigidWater.degrees_of_freedom(0, True) == 0
+
+
+def test_cxx_api_header_compiles_and_links(tmp_path):
+    """include/moldyn_b200.hpp (the reference's C++ class API over the C ABI)
+    compiles cleanly and links against the library; running it needs a GPU."""
+    import subprocess
+
+    import moleculardynamics_b200 as md
+    libdir = os.path.dirname(md.library_path())
+    exe = tmp_path / "shim_run"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "shim_run.cpp"),
+                    f"-L{libdir}", "-lmoldyn_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                   check=True)
+    assert exe.exists()
