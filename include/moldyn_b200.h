@@ -95,6 +95,8 @@ MD_API int md_abi_version(void);
 MD_API int md_context_create(int device, md_context** out);
 MD_API int md_context_destroy(md_context* ctx);
 MD_API int md_context_synchronize(md_context* ctx);
+/* The device's name and SM count, e.g. for keying tuned launch shapes. */
+MD_API int md_context_device_name(const md_context* ctx, char* name, int len);
 /* Reads (and with clear != 0, clears) the device status word; synchronises. */
 MD_API int md_context_status(md_context* ctx, uint32_t* status, int clear);
 /* Number of kernels this context has launched (instrumentation). */
@@ -201,6 +203,10 @@ MD_API int md_lj_lrc(const md_lj* lj, int64_t n, const double box[3], double* u_
  * (default 2). */
 MD_API int md_lj_set_threads_per_atom(int tpa);
 MD_API int md_lj_set_unroll(int unroll);
+/* Launch shape of this LJ object's Verlet force kernel (threads per atom 1/2/4/8,
+ * gathers in flight 1/2/4; 0 = the library default).  Set by the autotuner
+ * (moleculardynamics_b200/autotune.py); no reference counterpart. */
+MD_API int md_lj_set_launch(md_lj* lj, int tpa, int unroll);
 
 /* ------------------------------------------------------------------- Ewald */
 /* e^2/(4 pi eps0 kB) in K*Angstrom/e^2 (ewald.cpp:17-21). */

@@ -85,6 +85,7 @@ def _load():
         "md_context_launch_count": (C.c_int, [_vp, _i64p]),
         "md_context_set_timing": (C.c_int, [_vp, C.c_int]),
         "md_context_set_graphs": (C.c_int, [_vp, C.c_int]),
+        "md_context_device_name": (C.c_int, [_vp, C.c_char_p, C.c_int]),
         "md_context_kernel_time": (C.c_int, [_vp, C.c_int, C.c_int, _d, _i64p]),
         "md_context_span_begin": (C.c_int, [_vp]),
         "md_context_span_end": (C.c_int, [_vp, _d]),
@@ -128,6 +129,7 @@ def _load():
         "md_lj_lrc": (C.c_int, [_vp, C.c_int64, _d, _d, _d]),
         "md_lj_set_threads_per_atom": (C.c_int, [C.c_int]),
         "md_lj_set_unroll": (C.c_int, [C.c_int]),
+        "md_lj_set_launch": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_integrator_create_vv": (C.c_int, [C.c_double, C.POINTER(_vp)]),
         "md_integrator_create_baoab": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_uint64,
                                                  C.POINTER(_vp)]),
@@ -239,6 +241,11 @@ class Context:
         c = C.c_int64()
         _check(lib().md_context_launch_count(self._h, C.byref(c)))
         return c.value
+
+    def device_name(self) -> str:
+        buf = C.create_string_buffer(256)
+        _check(lib().md_context_device_name(self._h, buf, 256))
+        return buf.value.decode()
 
     def set_graphs(self, enable: bool):
         """Fused loops replay one captured CUDA graph per step (default) or launch
@@ -477,6 +484,7 @@ class LennardJones:
         self._h = h
         self.sigma, self.epsilon, self.cutoff = float(sigma), float(epsilon), float(cutoff)
         self.truncation = int(truncation)
+        self.precision = int(precision)
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -503,6 +511,11 @@ class LennardJones:
         if isinstance(source, CellList):
             return self._ev(lib().md_lj_forces_cells, sys.handle, source._h)
         return self._ev(lib().md_lj_forces_verlet, sys.handle, source.handle)
+
+    def set_launch(self, tpa=0, unroll=0):
+        """Threads per atom and gathers in flight of this object's Verlet force
+        kernel (0 = library default); see moleculardynamics_b200.autotune."""
+        _check(lib().md_lj_set_launch(self._h, int(tpa), int(unroll)))
 
     def hessian_vector_product(self, sys: System, verlet: VerletList, u):
         """(dF/dx)^T u for a per-atom field u (N, 3), and (u . dF/d epsilon,

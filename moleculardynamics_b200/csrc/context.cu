@@ -1,4 +1,5 @@
 // context.cu -- error state, device context, scratch management.
+#include <cstdio>
 #include <cstdarg>
 #include <cstring>
 #include <new>
@@ -191,6 +192,14 @@ int md_context_synchronize(md_context* ctx) {
     if (!ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_synchronize: NULL context");
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
     return ctx_check_status(ctx);
+}
+
+int md_context_device_name(const md_context* ctx, char* name, int len) {
+    if (!ctx || !name || len < 1) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_device_name: bad argument");
+    cudaDeviceProp prop;
+    MDB_CUDA(cudaGetDeviceProperties(&prop, ctx->device));
+    std::snprintf(name, static_cast<size_t>(len), "%s (%d SMs)", prop.name, prop.multiProcessorCount);
+    return MD_OK;
 }
 
 int md_context_status(md_context* ctx, uint32_t* status, int clear) {

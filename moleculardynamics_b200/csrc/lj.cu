@@ -168,10 +168,13 @@ constexpr int kBlock = 256;
 
 // Full Verlet list, TPA lanes per atom; rows are nbr[i*stride .. +count[i]).
 // Register budget per unroll factor: U gather chains per thread need ~8U more
-// registers, traded against resident blocks per SM.
-template <int U>
+// registers, traded against resident blocks per SM.  The mixed kernel is bound by
+// gather latency, so it takes 5 blocks (48 registers, a few spilled) -- measured
+// 0.266 ms against 0.282 ms at 4 blocks on the 1M-atom liquid; 6 blocks spill too
+// much (0.390 ms).
+template <int U, bool MIXED>
 struct UnrollBlocks {
-    static constexpr int value = U >= 4 ? 2 : 4;
+    static constexpr int value = U >= 4 ? 2 : (MIXED ? 5 : 4);
 };
 
 // Position source of the pair kernel: FP64 double4 for the reference arithmetic,
@@ -188,7 +191,7 @@ struct PosOf<true> {
 };
 
 template <int TPA, bool MIXED, bool LFS, int U>
-__global__ void __launch_bounds__(kBlock, UnrollBlocks<U>::value)
+__global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
 k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
             const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
             Box3 box, LJArgs a, double* __restrict__ fxo, double* __restrict__ fyo,
@@ -423,7 +426,8 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     }
     // |r^2 error| <= 2 r |d error| + rounding, |d error| <= sqrt(3) res: 4x margin
     a.band = 8.0 * 1.7320508075688772 * a.rc * res_max + 1e-12 * a.rc2;
-    const int64_t threads = std::max<int64_t>(sys->n * g_lj_tpa, 1);
+    const int tpa = lj->tpa ? lj->tpa : g_lj_tpa, unroll = lj->unroll ? lj->unroll : g_lj_unroll;
+    const int64_t threads = std::max<int64_t>(sys->n * tpa, 1);
     const int blocks = grid_for(threads, kBlock);
     double* part;
     MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
@@ -441,11 +445,11 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     }
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     if (mixed) {
-        if (lfs) launch_verlet_tpa<true, true>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
-        else launch_verlet_tpa<true, false>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
+        if (lfs) launch_verlet_tpa<true, true>(tpa, unroll, sys, v, a, part, ticket, out);
+        else launch_verlet_tpa<true, false>(tpa, unroll, sys, v, a, part, ticket, out);
     } else {
-        if (lfs) launch_verlet_tpa<false, true>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
-        else launch_verlet_tpa<false, false>(g_lj_tpa, g_lj_unroll, sys, v, a, part, ticket, out);
+        if (lfs) launch_verlet_tpa<false, true>(tpa, unroll, sys, v, a, part, ticket, out);
+        else launch_verlet_tpa<false, false>(tpa, unroll, sys, v, a, part, ticket, out);
     }
     ctx_time_end(ctx, MD_KERNEL_LJ_FORCE);
     ++ctx->launches;
@@ -610,6 +614,18 @@ int md_lj_set_threads_per_atom(int tpa) {
     if (tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_threads_per_atom: %d not in {1,2,4,8}", tpa);
     g_lj_tpa = tpa;
+    return MD_OK;
+}
+
+// Launch shape of one LJ object's Verlet force kernel (0 = the library default).
+int md_lj_set_launch(md_lj* lj, int tpa, int unroll) {
+    if (!lj) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: NULL");
+    if (tpa != 0 && tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: tpa %d not in {0,1,2,4,8}", tpa);
+    if (unroll != 0 && unroll != 1 && unroll != 2 && unroll != 4)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: unroll %d not in {0,1,2,4}", unroll);
+    lj->tpa = tpa;
+    lj->unroll = unroll;
     return MD_OK;
 }
 

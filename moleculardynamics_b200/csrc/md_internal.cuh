@@ -214,6 +214,7 @@ struct md_lj {
     int truncation = MD_TRUNCATED;
     int precision = MD_PRECISION_FP64;
     double u_at_cutoff = 0, dudr_at_cutoff = 0;
+    int tpa = 0, unroll = 0;   // launch shape of the Verlet force kernel (0: library default)
 };
 
 namespace mdb {
