@@ -12,7 +12,9 @@ pytestmark = pytest.mark.gpu
 def test_tune_force_kernel_applies_and_caches(md, tmp_path, monkeypatch):
     monkeypatch.setenv("MOLDYN_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     st = md.fcc_lattice(8, 0.8442, 0.722, 3)
-    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"])
+    pos = st["pos"] + np.random.default_rng(3).normal(scale=0.1, size=st["pos"].shape)
+    pos -= st["box"] * np.floor(pos / st["box"] + 0.5)
+    s = md.System.from_arrays(pos, st["box"], vel=st["vel"])
     v = md.VerletList(st["box"], 2.5, 0.3)
     v.build(s)
     ref_lj = md.LennardJones(1.0, 1.0, 2.5)
