@@ -49,7 +49,7 @@ extern "C" {
 #define MD_STATUS_SHAKE_DIVERGED 0x2u    /* SHAKE did not converge in maxIterations */
 #define MD_STATUS_RATTLE_DIVERGED 0x4u   /* RATTLE did not converge in maxIterations */
 #define MD_STATUS_SHAKE_SINGULAR 0x8u    /* SHAKE denominator below 1e-30 */
-#define MD_STATUS_NONFINITE 0x10u        /* a non-finite energy appeared */
+#define MD_STATUS_NONFINITE 0x10u        /* a position or the kinetic energy stopped being finite */
 
 /* System fields (core/system.hpp:54-59). */
 #define MD_FIELD_X 0
@@ -177,6 +177,13 @@ MD_API int md_verlet_pairs(md_verlet* list, int64_t* pi, int64_t* pj, int64_t ca
 MD_API int md_verlet_set_criterion(md_verlet* list, int criterion);
 /* Largest and second-largest displacement since the last build (diagnostics). */
 MD_API int md_verlet_displacements(md_verlet* list, md_system* sys, double* largest, double* second);
+/* Row capacity (neighbours per atom) of the list; no reference counterpart (the
+ * reference's list is a growing vector of pairs).  Host-driven builds grow a row
+ * capacity that overflows and build again, unless `fixed` is set, in which case
+ * the build fails with MD_ERR_RUNTIME; a rebuild decided on the device inside a
+ * fused loop cannot grow it and reports MD_ERR_DEVICE (neighbour overflow).  The
+ * list must be built again before its next use. */
+MD_API int md_verlet_set_capacity(md_verlet* list, int capacity, int fixed);
 
 /* ----------------------------------------------------------- Lennard-Jones */
 /* LennardJones(sigma, epsilon, cutoff, truncation) (lennard_jones.hpp:26,

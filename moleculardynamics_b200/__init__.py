@@ -119,6 +119,7 @@ def _load():
         "md_verlet_pairs": (C.c_int, [_vp, _i64p, _i64p, C.c_int64, _i64p]),
         "md_verlet_set_criterion": (C.c_int, [_vp, C.c_int]),
         "md_verlet_displacements": (C.c_int, [_vp, _vp, _d, _d]),
+        "md_verlet_set_capacity": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_lj_create": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                    C.POINTER(_vp)]),
         "md_lj_destroy": (C.c_int, [_vp]),
@@ -463,6 +464,11 @@ class VerletList:
 
     def set_criterion(self, criterion: int):
         _check(lib().md_verlet_set_criterion(self._h, int(criterion)))
+
+    def set_capacity(self, capacity: int, fixed: bool = False):
+        """Neighbours per atom the rows hold; host builds grow it on overflow
+        unless fixed.  The list must be built again."""
+        _check(lib().md_verlet_set_capacity(self._h, int(capacity), 1 if fixed else 0))
 
     def displacements(self, sys: System):
         a = C.c_double()

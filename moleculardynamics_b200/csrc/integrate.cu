@@ -33,7 +33,12 @@ struct StepArgs {
     uint32_t key0, key1;
     uint64_t step;
     const double* noise;  // replayed normals for this step (original order), or null
+    uint32_t* status;     // MD_STATUS_NONFINITE when a position stops being finite
 };
+
+__device__ __forceinline__ void check_finite(const double4& p, uint32_t* status) {
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(status, MD_STATUS_NONFINITE);
+}
 
 // Squared min-image displacement of a freshly moved atom from its position at the
 // last Verlet build (for the fused rebuild check).
@@ -67,6 +72,7 @@ __global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* 
         p.x = fold_wrapped(fma(s.dt, vx, p.x), f3.b[0]);
         p.y = fold_wrapped(fma(s.dt, vy, p.y), f3.b[1]);
         p.z = fold_wrapped(fma(s.dt, vz, p.z), f3.b[2]);
+        check_finite(p, s.status);
         a.pos[k] = p;
         a.vx[k] = vx;
         a.vy[k] = vy;
@@ -117,6 +123,7 @@ __global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s, DispArgs d) {
         p.x = fold_wrapped(fma(s.half_dt, vx, p.x), f3.b[0]);
         p.y = fold_wrapped(fma(s.half_dt, vy, p.y), f3.b[1]);
         p.z = fold_wrapped(fma(s.half_dt, vz, p.z), f3.b[2]);
+        check_finite(p, s.status);
         a.pos[k] = p;
         a.vx[k] = vx;
         a.vy[k] = vy;
@@ -128,7 +135,7 @@ __global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s, DispArgs d) {
 
 // Second half-kick (velocity_verlet.hpp:70-73), fused with the kinetic-energy sum.
 __global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsigned* ticket,
-                          double* out) {
+                          double* out, uint32_t* status) {
     double ke[1] = {0.0};
     for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -141,7 +148,7 @@ __global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsig
         a.vz[k] = vz;
         ke[0] += 0.5 * a.mass[k] * (vx * vx + vy * vy + vz * vz);
     }
-    grid_reduce<1>(ke, part, ticket, out);
+    grid_reduce<1>(ke, part, ticket, out, status);  // a NaN anywhere reaches the kinetic energy
 }
 
 __global__ void k_scale(md_atoms a, int64_t n, NhcState* nhc) {
@@ -262,6 +269,7 @@ StepArgs step_args(const md_integrator* it, const md_system* sys) {
     s.key1 = static_cast<uint32_t>(it->seed >> 32);
     s.step = it->step;
     s.noise = nullptr;
+    s.status = sys->ctx->d_status;
     return s;
 }
 
@@ -328,7 +336,7 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
     MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
     if (n > 0) {
         k_kick_ke<<<g, kBlock, 0, ctx->stream>>>(sys->cur, n, s, part, ctx_counter(ctx, 3),
-                                                ctx_result(ctx, kResKE));
+                                                ctx_result(ctx, kResKE), ctx->d_status);
         ++ctx->launches;
     }
     NhcState* nhc = nhc_of(it);

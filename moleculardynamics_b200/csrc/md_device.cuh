@@ -10,6 +10,8 @@
 
 #include <cstdint>
 
+#include "../../include/moldyn_b200.h"
+
 namespace mdb {
 
 // core/box.cpp:12-15: value - L * floor(value / L + 0.5), bit-exact.
@@ -102,8 +104,12 @@ __device__ __forceinline__ double warp_sum(double v) {
 // to arrive (atomic ticket) re-reduces all partials in block order and writes
 // out[k], then resets the ticket.  Must be called by every thread of the block;
 // blockDim.x must be a multiple of 32 and <= 1024.
+// Deterministic grid-wide sums: per-block partials, then the last block to
+// arrive (ticket) sums them in block order into out[0..K).  With `status`, a
+// non-finite sum (an atom that blew up) also sets MD_STATUS_NONFINITE there.
 template <int K>
-__device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out) {
+__device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out,
+                            uint32_t* status = nullptr) {
     __shared__ double sm[K][32];
     __shared__ bool is_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -148,7 +154,10 @@ __device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, doub
         for (int k = 0; k < K; ++k) {
             double s = lane < nw ? sm[k][lane] : 0.0;
             s = warp_sum(s);
-            if (lane == 0) out[k] = s;
+            if (lane == 0) {
+                out[k] = s;
+                if (status && !isfinite(s)) atomicOr(status, MD_STATUS_NONFINITE);
+            }
         }
     }
     if (threadIdx.x == 0) *ticket = 0u;

@@ -193,6 +193,7 @@ struct md_verlet {
     mdb::DevBuf count;            // n neighbour counts
     mdb::DevBuf ref;              // n double4 positions at the last build
     int stride = 0;               // row capacity
+    bool stride_fixed = false;    // host builds fail instead of growing it
     int64_t n = 0;
     int64_t rebuilds = 0;
     uint64_t epoch = 0;           // system epoch the list refers to

@@ -680,6 +680,12 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
             if (mx <= v->stride) break;
             uint32_t st = 0;
             md_context_status(sys->ctx, &st, 1);  // clear the overflow bit we resolve here
+            if (v->stride_fixed) {
+                v->sys = nullptr;
+                return fail(MD_ERR_RUNTIME,
+                            "VerletList: an atom has %d neighbours within the list cutoff, more "
+                            "than the fixed row capacity %d", mx, v->stride);
+            }
             v->stride = ((mx + mx / 4 + 16) + 7) & ~7;
             MDB_TRY(v->nbr.ensure(sizeof(int) * static_cast<size_t>(sys->n) * v->stride));
             // positions are already sorted; the re-sort below is a no-op permutation
@@ -983,6 +989,15 @@ int md_verlet_rebuild_count(md_verlet* v, int64_t* count) {
                              v->ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(v->ctx->stream));
     *count = v->rebuilds + dev;
+    return MD_OK;
+}
+
+int md_verlet_set_capacity(md_verlet* v, int capacity, int fixed) {
+    if (!v || capacity < 1) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_capacity: bad argument");
+    if (v->ctx) MDB_CUDA(cudaStreamSynchronize(v->ctx->stream));
+    v->stride = capacity;
+    v->stride_fixed = fixed != 0;
+    v->sys = nullptr;  // rows of the old capacity are no longer readable
     return MD_OK;
 }
 
