@@ -214,6 +214,16 @@ MD_API int md_lj_set_unroll(int unroll);
  * gathers in flight 1/2/4; 0 = the library default).  Set by the autotuner
  * (moleculardynamics_b200/autotune.py); no reference counterpart. */
 MD_API int md_lj_set_launch(md_lj* lj, int tpa, int unroll);
+/* Mixed precision only: read neighbours through halo tiles (on = 1, the
+ * default) or gather them through the int32 rows (0).  A halo tile holds a block
+ * of 128 cell-sorted atoms and every atom of the cells around them in shared
+ * memory; rows then hold 16-bit tile slots.  Forces are identical either way.
+ * No reference counterpart. */
+MD_API int md_lj_set_halo(md_lj* lj, int on);
+/* Halo tiles of a Verlet list: how many of its tiles are staged in shared memory
+ * (the rest gather through the int32 rows), out of how many (both 0 until a
+ * mixed-precision force call has used the list).  Diagnostics; synchronises. */
+MD_API int md_verlet_halo_tiles(md_verlet* v, int64_t* staged, int64_t* tiles);
 
 /* ------------------------------------------------------------------- Ewald */
 /* e^2/(4 pi eps0 kB) in K*Angstrom/e^2 (ewald.cpp:17-21). */

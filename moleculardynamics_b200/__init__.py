@@ -131,6 +131,8 @@ def _load():
         "md_lj_set_threads_per_atom": (C.c_int, [C.c_int]),
         "md_lj_set_unroll": (C.c_int, [C.c_int]),
         "md_lj_set_launch": (C.c_int, [_vp, C.c_int, C.c_int]),
+        "md_lj_set_halo": (C.c_int, [_vp, C.c_int]),
+        "md_verlet_halo_tiles": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "md_integrator_create_vv": (C.c_int, [C.c_double, C.POINTER(_vp)]),
         "md_integrator_create_baoab": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_uint64,
                                                  C.POINTER(_vp)]),
@@ -470,6 +472,13 @@ class VerletList:
         unless fixed.  The list must be built again."""
         _check(lib().md_verlet_set_capacity(self._h, int(capacity), 1 if fixed else 0))
 
+    def halo_tiles(self):
+        """(staged, total) halo tiles of this list (0, 0 before a mixed-precision
+        force call has used it)."""
+        a, b = C.c_int64(), C.c_int64()
+        _check(lib().md_verlet_halo_tiles(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def displacements(self, sys: System):
         a = C.c_double()
         b = C.c_double()
@@ -522,6 +531,11 @@ class LennardJones:
         """Threads per atom and gathers in flight of this object's Verlet force
         kernel (0 = library default); see moleculardynamics_b200.autotune."""
         _check(lib().md_lj_set_launch(self._h, int(tpa), int(unroll)))
+
+    def set_halo(self, on=True):
+        """Mixed precision: read neighbours through shared-memory halo tiles (the
+        default) or gather them through the int32 rows; forces are identical."""
+        _check(lib().md_lj_set_halo(self._h, 1 if on else 0))
 
     def hessian_vector_product(self, sys: System, verlet: VerletList, u):
         """(dF/dx)^T u for a per-atom field u (N, 3), and (u . dF/d epsilon,

@@ -25,6 +25,8 @@ struct LJArgs {
     float sig2f, rc2f, rcf, ucf, dudrcf, four_epsf, tf_epsf;
     double res[3];  // fixed-point resolution per axis, L / 2^32 (mixed path)
     double band;    // |r^2 - rc^2| below which the mixed path decides exactly
+    double res2;    // res^2 (cubic boxes)
+    double rc2_lo, rc2_hi;  // rc^2 -/+ band
 };
 
 LJArgs make_lj_args(const md_lj* lj) {
@@ -45,6 +47,8 @@ LJArgs make_lj_args(const md_lj* lj) {
     a.tf_epsf = static_cast<float>(a.tf_eps);
     a.res[0] = a.res[1] = a.res[2] = 0.0;
     a.band = 0.0;
+    a.res2 = 0.0;
+    a.rc2_lo = a.rc2_hi = a.rc2;
     return a;
 }
 
@@ -103,9 +107,30 @@ __device__ __forceinline__ void accumulate_exact(const LJArgs& a, const Fold3& f
 // r^2 are formed in FP64 from the exact integer difference (r^2 is the quantity
 // the r^-14 force steepness amplifies, so it is rounded to FP32 once, after it
 // is formed); r^-2, r^-6, energy and force magnitude in FP32; the force vector
-// assembled and accumulated in FP64, as are energy and virial.
+// assembled and accumulated in FP64.  Energy and virial terms are summed in FP32
+// per thread (a few dozen terms; the grid sum is FP64).
 __device__ __forceinline__ int wrap_diff(int a, int b) {
     return static_cast<int>(static_cast<unsigned>(a) - static_cast<unsigned>(b));
+}
+
+// Exact int32 -> FP64 on the FP64 pipe instead of the conversion unit: the bit
+// pattern (0x43300000, x + 2^31) is the double 2^52 + 2^31 + x, and subtracting
+// 2^52 + 2^31 from it is exact.
+__device__ __forceinline__ double int_to_double(int x) {
+    return __hiloint2double(0x43300000, x ^ static_cast<int>(0x80000000u)) - 4503601774854144.0;
+}
+
+// The same for the wrapped difference a - b: (a - b + 2^31) mod 2^32 in one add.
+__device__ __forceinline__ double diff_to_double(int a, int b) {
+    const unsigned biased = static_cast<unsigned>(a) - static_cast<unsigned>(b) + 0x80000000u;
+    return __hiloint2double(0x43300000, static_cast<int>(biased)) - 4503601774854144.0;
+}
+
+// Reciprocal by the special-function unit alone (PTX rcp.approx, <= 1 ulp).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 // A pair whose fixed-point r^2 lies within a.band of rc^2 could fall on the other
@@ -124,44 +149,87 @@ __device__ __forceinline__ bool inside_exact(const LJArgs& a, const Fold3& f3,
     return norm2_exact(dx, dy, dz) < a.rc2;
 }
 
-// NEAR = false: the main loop (pairs in the band are skipped and flagged);
-// NEAR = true: the second pass (only pairs in the band, decided exactly).
-template <bool LFS, bool NEAR>
-__device__ __forceinline__ void accumulate_mixed(const LJArgs& a, const Fold3& f3,
-                                                 const double4* __restrict__ pd, int i, int j,
-                                                 int4 qi, int4 qj, double& fx, double& fy,
-                                                 double& fz, double& e, double& vir, bool& near) {
-    const double dx = static_cast<double>(wrap_diff(qi.x, qj.x)) * a.res[0];
-    const double dy = static_cast<double>(wrap_diff(qi.y, qj.y)) * a.res[1];
-    const double dz = static_cast<double>(wrap_diff(qi.z, qj.z)) * a.res[2];
-    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-    if (!(r2 < a.rc2 + a.band)) return;
-    const bool in_band = r2 > a.rc2 - a.band;
-    if (NEAR) {
-        if (!in_band || !inside_exact(a, f3, pd, i, j)) return;
-    } else if (in_band) {
-        near = true;
-        return;
+// Main-loop pair term, branch-free: a pair beyond the band contributes zero, a
+// pair inside the band contributes zero and flags `near` (settled by
+// near_pair below).  Energy and virial take every list entry, so each pair
+// twice; the kernels halve them.  CUBIC: one resolution for all axes, so r^2 is
+// the integer-unit r^2 scaled once and the force is the integer-unit
+// displacement times (F/r) res.
+template <bool LFS, bool CUBIC>
+__device__ __forceinline__ void pair_mixed(const LJArgs& a, int4 qi, int4 qj, double& fx,
+                                           double& fy, double& fz, float& e, float& vir,
+                                           bool& near) {
+    double dx = diff_to_double(qi.x, qj.x);
+    double dy = diff_to_double(qi.y, qj.y);
+    double dz = diff_to_double(qi.z, qj.z);
+    double r2;
+    if constexpr (CUBIC) {
+        r2 = fma(dz, dz, fma(dy, dy, dx * dx)) * a.res2;
+    } else {
+        dx *= a.res[0];
+        dy *= a.res[1];
+        dz *= a.res[2];
+        r2 = fma(dz, dz, fma(dy, dy, dx * dx));
     }
+    const bool in_range = r2 < a.rc2_hi;
+    const bool in_band = r2 > a.rc2_lo;
+    near = near || (in_range && in_band);
+    const bool take = in_range && !in_band;
     const float r2f = static_cast<float>(r2);
-    const float inv = __frcp_rn(r2f);
+    const float inv = rcp_approx(r2f);
     const float s2 = a.sig2f * inv;
     const float s6 = s2 * s2 * s2;
-    float u = a.four_epsf * (s6 * s6 - s6);
-    float w = a.tf_epsf * (2.0f * s6 * s6 - s6);
+    const float t6 = fmaf(s6, s6, -s6);  // s6^2 - s6
+    float u = a.four_epsf * t6;
+    float w = a.tf_epsf * fmaf(s6, s6, t6);  // 24 eps (2 s6^2 - s6)
     if (LFS) {
         const float r = sqrtf(r2f);
         u = u - a.ucf - (r - a.rcf) * a.dudrcf;
         w = w + r * a.dudrcf;
     }
-    const double s = static_cast<double>(w * inv);
-    fx = fma(dx, s, fx);
-    fy = fma(dy, s, fy);
-    fz = fma(dz, s, fz);
-    if (qi.w < qj.w) {
-        e += static_cast<double>(u);
-        vir += static_cast<double>(w);
+    float sf = 0.f;
+    if (take) {
+        sf = w * inv;
+        e += u;
+        vir += w;
     }
+    double sd = static_cast<double>(sf);
+    if constexpr (CUBIC) sd *= a.res[0];
+    fx = fma(dx, sd, fx);
+    fy = fma(dy, sd, fy);
+    fz = fma(dz, sd, fz);
+}
+
+// A pair next to the cutoff (second pass): decided by the reference arithmetic
+// on the FP64 positions, then the same terms as pair_mixed (non-cubic form).
+template <bool LFS>
+__device__ __forceinline__ void near_pair(const LJArgs& a, const Fold3& f3,
+                                          const double4* __restrict__ pd, int i, int j, int4 qi,
+                                          int4 qj, double& fx, double& fy, double& fz, float& e,
+                                          float& vir) {
+    const double dx = int_to_double(wrap_diff(qi.x, qj.x)) * a.res[0];
+    const double dy = int_to_double(wrap_diff(qi.y, qj.y)) * a.res[1];
+    const double dz = int_to_double(wrap_diff(qi.z, qj.z)) * a.res[2];
+    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+    if (!(r2 < a.rc2_hi) || !(r2 > a.rc2_lo) || !inside_exact(a, f3, pd, i, j)) return;
+    const float r2f = static_cast<float>(r2);
+    const float inv = rcp_approx(r2f);
+    const float s2 = a.sig2f * inv;
+    const float s6 = s2 * s2 * s2;
+    const float t6 = fmaf(s6, s6, -s6);
+    float u = a.four_epsf * t6;
+    float w = a.tf_epsf * fmaf(s6, s6, t6);
+    if (LFS) {
+        const float r = sqrtf(r2f);
+        u = u - a.ucf - (r - a.rcf) * a.dudrcf;
+        w = w + r * a.dudrcf;
+    }
+    const double sd = static_cast<double>(w * inv);
+    fx = fma(dx, sd, fx);
+    fy = fma(dy, sd, fy);
+    fz = fma(dz, sd, fz);
+    e += u;
+    vir += w;
 }
 
 constexpr int kBlock = 256;
@@ -190,7 +258,7 @@ struct PosOf<true> {
     static __device__ __forceinline__ T load(const T* p) { return __ldg(p); }
 };
 
-template <int TPA, bool MIXED, bool LFS, int U>
+template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
 __global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
 k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
             const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
@@ -202,6 +270,7 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
     const int g = static_cast<int>(t % TPA);
     const Fold3 f3 = fold3_of(box);
     double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, vir = 0.0;
+    float ef = 0.f, vf = 0.f;  // mixed path: energy and virial terms
     bool near = false;
     if (i < n) {
         const typename P::T pi = P::load(pos + i);
@@ -230,8 +299,7 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if constexpr (MIXED)
-                    accumulate_mixed<LFS, false>(a, f3, pd, static_cast<int>(i), j[u], pi, pj[u],
-                                                 fx, fy, fz, e, vir, near);
+                    pair_mixed<LFS, CUBIC>(a, pi, pj[u], fx, fy, fz, ef, vf, near);
                 else accumulate_exact<LFS>(a, f3, pi, pj[u], fx, fy, fz, e, vir);
             }
         }
@@ -241,8 +309,7 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
             if (k + u * TPA < cnt) {
                 const typename P::T pj = P::load(pos + jn[u]);
                 if constexpr (MIXED)
-                    accumulate_mixed<LFS, false>(a, f3, pd, static_cast<int>(i), jn[u], pi, pj, fx,
-                                                 fy, fz, e, vir, near);
+                    pair_mixed<LFS, CUBIC>(a, pi, pj, fx, fy, fz, ef, vf, near);
                 else accumulate_exact<LFS>(a, f3, pi, pj, fx, fy, fz, e, vir);
             }
         }
@@ -250,12 +317,213 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
             if (near) {  // rare: settle the pairs next to the cutoff
                 for (int kk = g; kk < cnt; kk += TPA) {
                     const int j = __ldg(row + kk);
-                    accumulate_mixed<LFS, true>(a, f3, pd, static_cast<int>(i), j, pi,
-                                                P::load(pos + j), fx, fy, fz, e, vir, near);
+                    near_pair<LFS>(a, f3, pd, static_cast<int>(i), j, pi, P::load(pos + j), fx, fy,
+                                   fz, ef, vf);
                 }
             }
+            e = 0.5 * static_cast<double>(ef);  // every pair was taken from both sides
+            vir = 0.5 * static_cast<double>(vf);
         }
     }
+#pragma unroll
+    for (int o = TPA / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (i < n && g == 0) {
+        fxo[i] = fx;
+        fyo[i] = fy;
+        fzo[i] = fz;
+    }
+    double v[2] = {e, vir};
+    grid_reduce<2>(v, part, ticket, out);
+}
+
+// One thread's share of a row (entries g, g + TPA, ...): U position loads in
+// flight and the next U indices read one iteration ahead; pairs are accumulated
+// in row order.  row(k) gives entry k, load(j) the fixed-point position of j.
+template <int TPA, int U, class Row, class Load, class Pair>
+__device__ __forceinline__ void walk_row(int g, int cnt, Row row, Load load, Pair pair) {
+    int k = g;
+    int jn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) jn[u] = k + u * TPA < cnt ? row(k + u * TPA) : 0;
+    for (; k + (U - 1) * TPA < cnt; k += U * TPA) {
+        int4 pj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) pj[u] = load(jn[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int kn = k + (U + u) * TPA;
+            jn[u] = kn < cnt ? row(kn) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) pair(pj[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U - 1; ++u)
+        if (k + u * TPA < cnt) pair(load(jn[u]));
+}
+
+// Pair sums of one thread's share of a row (mixed path).
+struct PairSums {
+    double fx, fy, fz;
+    float e, vir;
+};
+
+// The rare paths of k_lj_halo, out of line so that the staged main loop keeps its
+// registers.  Pairs of a staged row next to the cutoff, decided exactly and
+// added in row order to the sums so far:
+template <bool LFS>
+__device__ __noinline__ PairSums near_pairs_tile(LJArgs a, Box3 box, const double4* pd,
+                                                 const uint16_t* row, int cnt, int g, int ii,
+                                                 int4 pi, const int4* s_q, const int* s_beg,
+                                                 const int* s_base, int nr, PairSums acc) {
+    constexpr int TPA = kBlock / kHaloAtoms;
+    const Fold3 f3 = fold3_of(box);
+    for (int kk = g; kk < cnt; kk += TPA) {
+        const int sl = row[kk] >> 4;  // rows hold byte offsets of 16-byte slots
+        int lo = 0, hi = nr;  // the last run whose first slot is <= sl
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_base[mid] <= sl) lo = mid;
+            else hi = mid;
+        }
+        near_pair<LFS>(a, f3, pd, ii, s_beg[lo] + (sl - s_base[lo]), pi, s_q[sl], acc.fx, acc.fy,
+                       acc.fz, acc.e, acc.vir);
+    }
+    return acc;
+}
+
+// and a whole row of a tile that was not staged, gathered through the int32 row
+// exactly as k_lj_verlet's mixed path walks it.
+template <bool LFS, bool CUBIC, int U, int TPA>
+__device__ __noinline__ PairSums gathered_row(LJArgs a, Box3 box, const double4* pd, const int4* q,
+                                              const int* row, int cnt, int g, int ii, int4 pi) {
+    PairSums acc = {0.0, 0.0, 0.0, 0.f, 0.f};
+    bool near = false;
+    walk_row<TPA, U>(g, cnt, [&](int k) { return __ldg(row + k); },
+                     [&](int j) { return __ldg(q + j); },
+                     [&](int4 pj) {
+                         pair_mixed<LFS, CUBIC>(a, pi, pj, acc.fx, acc.fy, acc.fz, acc.e, acc.vir,
+                                                near);
+                     });
+    if (near) {
+        const Fold3 f3 = fold3_of(box);
+        for (int kk = g; kk < cnt; kk += TPA) {
+            const int j = __ldg(row + kk);
+            near_pair<LFS>(a, f3, pd, ii, j, pi, __ldg(q + j), acc.fx, acc.fy, acc.fz, acc.e,
+                           acc.vir);
+        }
+    }
+    return acc;
+}
+
+// Mixed-precision forces over halo tiles (one CTA per tile of kHaloAtoms sorted
+// atoms, two threads per atom).  The CTA copies the fixed-point positions of its
+// tile's cell runs into shared memory -- contiguous, coalesced reads of an array
+// that stays in L2 -- and then reads each row as 16-bit tile slots: a neighbour
+// costs a 2-byte list read and a shared-memory load instead of a 4-byte read and
+// a gather through L1/L2.  A tile that was not staged (too many cells or atoms
+// around it) walks its int32 row with global gathers.  Pair arithmetic, the
+// exact decision of pairs next to the cutoff and the accumulation order are
+// those of k_lj_verlet's mixed path.
+template <bool LFS, int U, bool CUBIC>
+__global__ void __launch_bounds__(kBlock, 4)
+k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int* __restrict__ nbr,
+          const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride, int64_t n,
+          const int2* __restrict__ runs, const int2* __restrict__ meta, Box3 box, LJArgs a,
+          double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
+          double* part, unsigned* ticket, double* out) {
+    constexpr int TPA = kBlock / kHaloAtoms;
+    extern __shared__ int4 s_q[];  // kHaloCap slots
+    __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int2 m = meta[blockIdx.x];
+    const bool staged = m.x > 0;
+    if (staged) {
+        if (tid < m.x) {
+            const int2 r = runs[static_cast<int64_t>(blockIdx.x) * kHaloRuns + tid];
+            s_beg[tid] = r.x;
+            s_base[tid] = r.y;
+        }
+        if (tid == 0) s_base[m.x] = m.y;
+        __syncthreads();
+        // every copy is issued before any is waited on (asynchronous 16-byte
+        // global->shared copies through L2), so the tile costs one L2 latency
+        for (int t = warp; t < m.x; t += kBlock / 32) {
+            const int4* src = q + s_beg[t];
+            const int base = s_base[t], len = s_base[t + 1] - base;
+            for (int k = lane; k < len; k += 32) {
+                const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(s_q + base + k));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src + k)
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+    }
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kHaloAtoms + tid / TPA;
+    const int g = tid % TPA;
+    PairSums acc = {0.0, 0.0, 0.0, 0.f, 0.f};
+    if (i < n) {
+        const int4 pi = __ldg(q + i);
+        const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
+        const int ii = static_cast<int>(i);
+        if (staged) {
+            // eight slots per 16-byte read (rows start 16-byte aligned: the stride is
+            // a multiple of 8), the next read issued before the current pairs; this
+            // thread takes the entries g, g + 2, ... of each chunk -- the row order
+            // of the gathered walk.  Slots are stored as byte offsets into the tile.
+            const uint16_t* row = nbr16 + i * stride;
+            const uint4* rowv = reinterpret_cast<const uint4*>(row);
+            const char* tile = reinterpret_cast<const char*>(s_q);
+            const unsigned sel = g ? 0x4432u : 0x4410u;  // this thread's 16-bit halves
+            const int nfull = cnt >> 3, nch = (cnt + 7) >> 3;
+            bool near = false;
+            uint4 cur = nch > 0 ? __ldg(rowv) : make_uint4(0u, 0u, 0u, 0u);
+            auto chunk = [&](const uint4& v) {
+                const unsigned w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    pair_mixed<LFS, CUBIC>(
+                        a, pi, *reinterpret_cast<const int4*>(tile + __byte_perm(w4[t], 0u, sel)),
+                        acc.fx, acc.fy, acc.fz, acc.e, acc.vir, near);
+            };
+            int c = 0;
+            for (; c + 1 < nfull; c += 2) {  // two chunks per trip: no register copies
+                const uint4 nxt = __ldg(rowv + c + 1);
+                chunk(cur);
+                cur = c + 2 < nch ? __ldg(rowv + c + 2) : nxt;
+                chunk(nxt);
+            }
+            if (c < nfull) {
+                const uint4 nxt = c + 1 < nch ? __ldg(rowv + c + 1) : cur;
+                chunk(cur);
+                cur = nxt;
+            }
+            const int rem = cnt & 7;  // the last, partial chunk
+            if (rem > g) {
+                const unsigned w4[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (g + 2 * t < rem)
+                        pair_mixed<LFS, CUBIC>(
+                            a, pi,
+                            *reinterpret_cast<const int4*>(tile + __byte_perm(w4[t], 0u, sel)),
+                            acc.fx, acc.fy, acc.fz, acc.e, acc.vir, near);
+            }
+            if (near)  // rare: settle the pairs next to the cutoff
+                acc = near_pairs_tile<LFS>(a, box, pd, row, cnt, g, ii, pi, s_q, s_beg, s_base, m.x,
+                                           acc);
+        } else {
+            acc = gathered_row<LFS, CUBIC, U, TPA>(a, box, pd, q, nbr + i * stride, cnt, g, ii, pi);
+        }
+    }
+    double fx = acc.fx, fy = acc.fy, fz = acc.fz;
+    const double e = 0.5 * static_cast<double>(acc.e);  // every pair was taken from both sides
+    const double vir = 0.5 * static_cast<double>(acc.vir);
 #pragma unroll
     for (int o = TPA / 2; o > 0; o >>= 1) {
         fx += __shfl_xor_sync(0xffffffffu, fx, o);
@@ -371,7 +639,10 @@ void launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, 
     const typename PosOf<MIXED>::T* pos;
     if constexpr (MIXED) pos = sys->qpos.as<int4>();
     else pos = sys->cur.pos;
-    k_lj_verlet<TPA, MIXED, LFS, U><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
+    const bool cubic = MIXED && a.res[0] == a.res[1] && a.res[0] == a.res[2];
+    auto kernel = cubic ? k_lj_verlet<TPA, MIXED, LFS, U, MIXED>
+                        : k_lj_verlet<TPA, MIXED, LFS, U, false>;
+    kernel<<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
         pos, sys->cur.pos, v->nbr.as<int>(), v->count.as<int>(), v->stride, sys->n, box_of(sys), a,
         sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
 }
@@ -388,6 +659,28 @@ __global__ void k_quantize(const double4* __restrict__ pos, int64_t n, double sx
                      static_cast<int>(static_cast<unsigned>(llrint(p.y * sy))),
                      static_cast<int>(static_cast<unsigned>(llrint(p.z * sz))),
                      static_cast<int>(p.w));
+}
+
+template <bool LFS, int U>
+void launch_halo(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
+                 double* out) {
+    const unsigned blocks = static_cast<unsigned>(halo_blocks(sys->n));
+    const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
+    auto kernel = cubic ? k_lj_halo<LFS, U, true> : k_lj_halo<LFS, U, false>;
+    kernel<<<blocks, kBlock, kHaloCap * sizeof(int4), sys->ctx->stream>>>(
+        sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
+        v->count.as<int>(), v->stride, sys->n, v->halo_runs.as<int2>(), v->halo_meta.as<int2>(),
+        box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+}
+
+template <bool LFS>
+void launch_halo_u(int unroll, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                   unsigned* ticket, double* out) {
+    switch (unroll) {
+        case 1: launch_halo<LFS, 1>(sys, v, a, part, ticket, out); break;
+        case 4: launch_halo<LFS, 4>(sys, v, a, part, ticket, out); break;
+        default: launch_halo<LFS, 2>(sys, v, a, part, ticket, out); break;
+    }
 }
 
 template <int TPA, bool MIXED, bool LFS>
@@ -426,9 +719,12 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
     }
     // |r^2 error| <= 2 r |d error| + rounding, |d error| <= sqrt(3) res: 4x margin
     a.band = 8.0 * 1.7320508075688772 * a.rc * res_max + 1e-12 * a.rc2;
+    a.res2 = a.res[0] * a.res[0];
+    a.rc2_lo = a.rc2 - a.band;
+    a.rc2_hi = a.rc2 + a.band;
     const int tpa = lj->tpa ? lj->tpa : g_lj_tpa, unroll = lj->unroll ? lj->unroll : g_lj_unroll;
     const int64_t threads = std::max<int64_t>(sys->n * tpa, 1);
-    const int blocks = grid_for(threads, kBlock);
+    const int64_t blocks = std::max<int64_t>(grid_for(threads, kBlock), halo_blocks(sys->n));
     double* part;
     MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
     unsigned* ticket = ctx_counter(ctx, 2);
@@ -443,8 +739,14 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
             sys->qpos.as<int4>());
         ++ctx->launches;
     }
+    // halo tiles need the list's cell grid; they are built once here and then with
+    // every rebuild of this list
+    const bool halo = mixed && lj->halo && sys->n > 0 && verlet_halo_ready(v, sys);
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
-    if (mixed) {
+    if (halo) {
+        if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out);
+        else launch_halo_u<false>(unroll, sys, v, a, part, ticket, out);
+    } else if (mixed) {
         if (lfs) launch_verlet_tpa<true, true>(tpa, unroll, sys, v, a, part, ticket, out);
         else launch_verlet_tpa<true, false>(tpa, unroll, sys, v, a, part, ticket, out);
     } else {
@@ -626,6 +928,12 @@ int md_lj_set_launch(md_lj* lj, int tpa, int unroll) {
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: unroll %d not in {0,1,2,4}", unroll);
     lj->tpa = tpa;
     lj->unroll = unroll;
+    return MD_OK;
+}
+
+int md_lj_set_halo(md_lj* lj, int on) {
+    if (!lj) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_halo: NULL");
+    lj->halo = on != 0;
     return MD_OK;
 }
 

@@ -201,9 +201,27 @@ struct md_verlet {
     int* d_rebuild_flag = nullptr; // device: set by the displacement check
     int* d_rebuild_total = nullptr; // device: rebuilds done inside fused loops
     int* d_max_count = nullptr;     // device: largest row seen by the last build
+    // Halo tiles (mixed-precision force path): per block of kHaloAtoms sorted
+    // atoms, runs of the cells around them and the rows as 16-bit halo slots.
+    bool halo_on = false;
+    mdb::DevBuf halo_runs;          // blocks * kHaloRuns int2 (first atom, slot base)
+    mdb::DevBuf halo_meta;          // blocks int2 (runs or -1 when not staged, atoms)
+    mdb::DevBuf nbr16;              // n * stride halo slots
 };
 
 namespace mdb {
+// A halo tile: kHaloAtoms consecutive sorted atoms (one force block) and every
+// atom of the cells around their cells, staged in at most kHaloCap slots of
+// shared memory; blocks that span more than kHaloSpan cells or need more runs or
+// slots than that keep gathering through the int32 rows.
+constexpr int kHaloAtoms = 128;
+constexpr int kHaloRuns = 64;
+constexpr int kHaloCap = 2560;
+constexpr int kHaloSpan = 16;
+inline int64_t halo_blocks(int64_t n) { return (n + kHaloAtoms - 1) / kHaloAtoms; }
+// Turns the halo tiles on for this list (built right away from the current list
+// unless the stream is capturing); false when they cannot be used.
+bool verlet_halo_ready(md_verlet* v, md_system* sys);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 int verlet_check(md_verlet* v, md_system* sys);  // device flag <- needs rebuild
 int verlet_ensure_capacity(md_verlet* v, md_system* sys);
@@ -216,6 +234,7 @@ struct md_lj {
     int precision = MD_PRECISION_FP64;
     double u_at_cutoff = 0, dudr_at_cutoff = 0;
     int tpa = 0, unroll = 0;   // launch shape of the Verlet force kernel (0: library default)
+    bool halo = true;          // mixed precision: staged halo tiles where the list allows
 };
 
 namespace mdb {

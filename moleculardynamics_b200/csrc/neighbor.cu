@@ -285,9 +285,13 @@ __device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, do
 // centre (nearest periodic image); then each lane takes one atom of the cell and
 // scans the staged candidates (broadcast reads, two candidates per packed FP32x2
 // step), appending hits to its own row.
-// Only a candidate whose FP32 r^2 lies within 2^-12 of the list cutoff^2 -- far
-// wider than the FP32 error of these coordinates -- is decided by the exact
-// reference arithmetic, so the pair set stays bit-identical to the reference's.
+// A candidate is listed when its FP32 r^2 is below the list cutoff^2 widened by
+// 2^-12 -- far more than the FP32 error of these coordinates -- so the rows hold
+// every pair the reference lists plus, at most, pairs within a 1.2e-4 relative
+// shell outside the list cutoff.  Every consumer tests its own cutoff, which is
+// below the list cutoff, so the extra entries never contribute; the exported
+// pair set (forEachPair) applies the reference's exact test to the positions of
+// the build and is bit-identical to the reference's.
 // Rows list candidates in stencil order, atoms of a cell in sorted order.
 __global__ void __launch_bounds__(kBuildWarps * 32)
 k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
@@ -309,7 +313,6 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     const double ox = -0.5 * g.box.L[0] + (cx + 0.5) * g.wx;
     const double oy = -0.5 * g.box.L[1] + (cy + 0.5) * g.wy;
     const double oz = -0.5 * g.box.L[2] + (cz + 0.5) * g.wz;
-    const float lo_thr = static_cast<float>(rl2 * (1.0 - 1.0 / 4096.0));
     const float hi_thr = static_cast<float>(rl2 * (1.0 + 1.0 / 4096.0));
     // the 27 neighbour cell ranges (lane q holds cell q of the stencil)
     int beg = 0, cnt = 0;
@@ -383,10 +386,6 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
             }
             int* row = nbr + static_cast<int64_t>(active ? i : 0) * stride;
             // Per candidate pair: packed FP32x2 distances and predicated appends.
-            // The few candidates within the 2^-12 band around the cutoff are
-            // decided by the exact reference arithmetic in place (so rows keep
-            // stencil order); the band check is one warp vote per pair, taken
-            // only when some lane of the warp has such a candidate.
             const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy),
                          fz2 = make_float2(fz, fz);
             const int npairs = (wlen + 1) >> 1;
@@ -398,15 +397,8 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                 const float2 dz = __fadd2_rn(fz2, make_float2(B.x, B.y));
                 const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
                 const int j0 = __float_as_int(B.z), j1 = __float_as_int(B.w);
-                bool h0 = r2.x < lo_thr, h1 = r2.y < lo_thr;
-                const bool n0 = active && !h0 && r2.x <= hi_thr;
-                const bool n1 = active && !h1 && r2.y <= hi_thr;
-                if (__any_sync(0xffffffffu, n0 || n1)) {
-                    if (n0 && j0 != i) h0 = within(g.box, pi, ldg4(pos + j0), rl2);
-                    if (n1 && j1 != i) h1 = within(g.box, pi, ldg4(pos + j1), rl2);
-                }
-                h0 = h0 && active && j0 != i;
-                h1 = h1 && active && j1 != i;
+                const bool h0 = active && r2.x < hi_thr && j0 != i;
+                const bool h1 = active && r2.y < hi_thr && j1 != i;
                 if (h0 && c < stride) row[c] = j0;
                 c += h0 ? 1 : 0;
                 if (h1 && c < stride) row[c] = j1;
@@ -452,6 +444,195 @@ __global__ void k_verlet_brute(const double4* __restrict__ pos, int64_t n, Box3 
         atomicMax(max_count, base);
         if (base > stride) atomicOr(status, MD_STATUS_NEIGHBOR_OVERFLOW);
     }
+}
+
+// ---------------------------------------------------------------- halo tiles
+constexpr int kPlanEntries = 512;  // >= kHaloSpan * 27, a power of two
+
+// Rank of the cell holding sorted atom a (the largest r with start[r] <= a), by a
+// 32-way search of the warp: four rounds of one coalesced probe per lane for
+// 50k cells.  Every lane returns it.
+__device__ __forceinline__ int cell_rank_of(const int* __restrict__ start, int m, int64_t a,
+                                            int lane) {
+    int lo = 0, hi = m;  // start[lo] <= a < start[hi] (start[m] = n)
+    while (hi - lo > 1) {
+        const int step = (hi - lo + 31) / 32;
+        const int p = lo + (lane + 1) * step;
+        const bool le = p < hi && start[p] <= a;
+        const int k = __popc(__ballot_sync(0xffffffffu, le));  // probes are monotone
+        hi = min(hi, lo + (k + 1) * step);
+        lo += k * step;
+    }
+    return lo;
+}
+
+// One CTA per halo tile (kHaloAtoms consecutive sorted atoms).  Plan: the cell
+// ranks the tile's atoms span, their 27-cell neighbourhoods sorted (bitonic) and
+// merged into runs of consecutive ranks -- each run one contiguous range of
+// sorted atoms -- and each run's first slot in the staged tile.  A tile spanning
+// more than kHaloSpan cells, needing more than kHaloRuns runs or kHaloCap slots,
+// or lying inside one crowded cell, is not staged.  Rows: each int32 row entry j
+// becomes the 16-bit byte offset of its slot (base of the run holding j + j -
+// the run's first atom), eight entries per 16-byte access, with the last run
+// found cached per thread (entries come in stencil order).  A neighbour outside
+// the tile's runs (not possible for a list built from the same cells) un-stages
+// the tile.
+__global__ void __launch_bounds__(kBlock)
+k_halo_tiles(const int* __restrict__ start, GridArgs g, int64_t n, const int* __restrict__ nbr,
+             const int* __restrict__ count, int stride, int2* __restrict__ runs,
+             int2* __restrict__ meta, uint16_t* __restrict__ nbr16, const int* flag) {
+    if (!gate(flag)) return;
+    __shared__ int s_ent[kPlanEntries];
+    __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
+    __shared__ int s_rank[2], s_nr;
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+    const int64_t a0 = static_cast<int64_t>(b) * kHaloAtoms;
+    const int64_t a1 = min(n, a0 + kHaloAtoms) - 1;
+    if (tid < 32) {
+        const int r0 = cell_rank_of(start, g.ncells, a0, lane);
+        const int r1 = cell_rank_of(start, g.ncells, a1, lane);
+        if (lane == 0) {
+            s_rank[0] = r0;
+            s_rank[1] = r1;
+            // inside one cell whose atoms run past both ends of the tile: the
+            // list build writes slots for a cell's first and last tile only
+            const bool inner = r0 == r1 && start[r0] < a0 && start[r0 + 1] - 1 > a1;
+            s_nr = inner || r1 - r0 + 1 > kHaloSpan ? -1 : 0;
+        }
+    }
+    __syncthreads();
+    if (s_nr < 0) {
+        if (tid == 0) meta[b] = make_int2(-1, 0);
+        return;
+    }
+    const int r0 = s_rank[0], ne = (s_rank[1] - r0 + 1) * 27;
+    for (int e = tid; e < kPlanEntries; e += blockDim.x) {
+        int v = 0x7fffffff;
+        if (e < ne) {
+            const int cell = g.cell_of_rank[r0 + e / 27], q = e % 27;
+            const int cx = cell % g.nx, cy = (cell / g.nx) % g.ny, cz = cell / (g.nx * g.ny);
+            int jx = cx + (q % 3) - 1, jy = cy + ((q / 3) % 3) - 1, jz = cz + (q / 9) - 1;
+            jx = jx < 0 ? jx + g.nx : (jx >= g.nx ? jx - g.nx : jx);
+            jy = jy < 0 ? jy + g.ny : (jy >= g.ny ? jy - g.ny : jy);
+            jz = jz < 0 ? jz + g.nz : (jz >= g.nz ? jz - g.nz : jz);
+            v = g.rank_of_cell[jx + g.nx * (jy + g.ny * jz)];
+        }
+        s_ent[e] = v;
+    }
+    __syncthreads();
+    const int np2 = ne <= 256 ? 256 : kPlanEntries;  // sort only the filled power of two
+    for (int k = 2; k <= np2; k <<= 1) {  // bitonic sort, ascending
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int e = tid; e < np2; e += blockDim.x) {
+                const int p = e ^ j;
+                if (p > e) {
+                    const int x = s_ent[e], y = s_ent[p];
+                    if ((x > y) == ((e & k) == 0)) {
+                        s_ent[e] = y;
+                        s_ent[p] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (tid < 32) {
+        // runs of consecutive distinct ranks (duplicates neither open nor close one)
+        int nopen = 0, nclose = 0;
+        for (int c = 0; c < ne; c += 32) {
+            const int e = c + lane;
+            const int v = e < ne ? s_ent[e] : 0;
+            const bool opens = e < ne && (e == 0 || v > s_ent[e - 1] + 1);
+            const bool closes = e < ne && (e == ne - 1 || s_ent[e + 1] > v + 1);
+            const unsigned mo = __ballot_sync(0xffffffffu, opens);
+            const unsigned mc = __ballot_sync(0xffffffffu, closes);
+            const unsigned below = (1u << lane) - 1u;
+            const int io = nopen + __popc(mo & below), ic = nclose + __popc(mc & below);
+            // first atom of an opening rank; one past the last atom of a closing one
+            if (opens && io < kHaloRuns) s_beg[io] = start[v];
+            if (closes && ic < kHaloRuns) s_base[ic] = start[v + 1];
+            nopen += __popc(mo);
+            nclose += __popc(mc);
+        }
+        __syncwarp();
+        const int nr = nopen;
+        int total = 0;
+        if (nr <= kHaloRuns) {
+            // run lengths -> slot bases (exclusive scan, two runs per lane)
+            int len[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int t = 2 * lane + h;
+                len[h] = t < nr ? s_base[t] - s_beg[t] : 0;
+            }
+            const int pair = len[0] + len[1];
+            int incl = pair;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+            const int base0 = incl - pair;
+            int2* out = runs + static_cast<int64_t>(b) * kHaloRuns;
+            if (2 * lane < nr) {
+                s_base[2 * lane] = base0;
+                out[2 * lane] = make_int2(s_beg[2 * lane], base0);
+            }
+            if (2 * lane + 1 < nr) {
+                s_base[2 * lane + 1] = base0 + len[0];
+                out[2 * lane + 1] = make_int2(s_beg[2 * lane + 1], base0 + len[0]);
+            }
+        }
+        const bool staged = nr <= kHaloRuns && total <= kHaloCap;
+        if (lane == 0) {
+            s_base[staged ? nr : 0] = total;
+            s_nr = staged ? nr : -1;
+            meta[b] = make_int2(staged ? nr : -1, total);
+        }
+    }
+    __syncthreads();
+    const int nr = s_nr;
+    if (nr <= 0) return;
+    // rows: thread t converts chunks (t & 1), (t & 1) + 2, ... of atom t >> 1
+    const int64_t i = a0 + (tid >> 1);
+    bool bad = false;
+    if (i <= a1) {
+        const int c = min(count[i], stride);
+        const int4* src = reinterpret_cast<const int4*>(nbr + i * stride);
+        uint4* dst = reinterpret_cast<uint4*>(nbr16 + i * stride);
+        int t = 0, beg = s_beg[0], len = s_base[1] - s_base[0];
+        for (int ch = tid & 1; 8 * ch < c; ch += 2) {
+            const int4 lo4 = __ldg(src + 2 * ch), hi4 = __ldg(src + 2 * ch + 1);
+            const int js[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
+            unsigned off[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                off[k] = 0u;
+                if (8 * ch + k < c) {
+                    const int j = js[k];
+                    if (static_cast<unsigned>(j - beg) >= static_cast<unsigned>(len)) {
+                        int lo = 0, hi = nr;  // the last run whose first atom is <= j
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (s_beg[mid] <= j) lo = mid;
+                            else hi = mid;
+                        }
+                        t = lo;
+                        beg = s_beg[t];
+                        len = s_base[t + 1] - s_base[t];
+                    }
+                    const bool ok = static_cast<unsigned>(j - beg) < static_cast<unsigned>(len);
+                    bad = bad || !ok;
+                    off[k] = ok ? static_cast<unsigned>(s_base[t] + (j - beg)) << 4 : 0u;
+                }
+            }
+            dst[ch] = make_uint4(off[0] | (off[1] << 16), off[2] | (off[3] << 16),
+                                 off[4] | (off[5] << 16), off[6] | (off[7] << 16));
+        }
+    }
+    if (__syncthreads_or(bad) && tid == 0) meta[b].x = -1;
 }
 
 __global__ void k_store_ref(const double4* __restrict__ pos, double4* ref, int64_t n,
@@ -624,6 +805,26 @@ static int verlet_alloc(md_verlet* v, md_system* sys) {
     return MD_OK;
 }
 
+// Halo tiles of the current list (gated by the rebuild flag inside fused loops).
+int halo_build(md_verlet* v, md_system* sys, const int* flag) {
+    md_context* ctx = sys->ctx;
+    if (v->stride % 8 != 0) {  // rows are converted and read 16 bytes at a time
+        v->halo_on = false;
+        return MD_OK;
+    }
+    const int64_t n = sys->n, blocks = halo_blocks(n);
+    MDB_TRY(v->halo_runs.ensure(sizeof(int2) * static_cast<size_t>(blocks) * kHaloRuns));
+    MDB_TRY(v->halo_meta.ensure(sizeof(int2) * static_cast<size_t>(blocks)));
+    MDB_TRY(v->nbr16.ensure(sizeof(uint16_t) * static_cast<size_t>(n) * v->stride));
+    const GridArgs g = make_args(v->grid, sys);
+    k_halo_tiles<<<static_cast<unsigned>(blocks), kBlock, 0, ctx->stream>>>(
+        v->start.as<int>(), g, n, v->nbr.as<int>(), v->count.as<int>(), v->stride,
+        v->halo_runs.as<int2>(), v->halo_meta.as<int2>(), v->nbr16.as<uint16_t>(), flag);
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
 int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
@@ -663,6 +864,7 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
             sys->cur.pos, v->ref.as<double4>(), n, flag, flag ? v->d_rebuild_total : nullptr);
         ++ctx->launches;
     }
+    if (v->halo_on && v->grid.usable && n > 0) MDB_TRY(halo_build(v, sys, flag));
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
@@ -696,6 +898,22 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
         return MD_OK;
     }
     return verlet_build_impl(v, sys, v->d_rebuild_flag);
+}
+
+bool verlet_halo_ready(md_verlet* v, md_system* sys) {
+    if (v->stride % 8 != 0) return false;  // the force kernel reads rows 16 bytes at a time
+    if (v->halo_on) return true;
+    if (!v->grid.usable || sys->n <= 0 || v->sys != sys) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(sys->ctx->stream, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone)
+        return false;
+    if (halo_build(v, sys, nullptr) != MD_OK) {
+        cudaGetLastError();
+        return false;
+    }
+    v->halo_on = true;
+    return true;
 }
 
 DispArgs disp_args(md_verlet* v, md_context* ctx, double* part) {
@@ -736,32 +954,37 @@ __global__ void k_to_orig(const int* __restrict__ sorted, const int* __restrict_
     if (s < n) out[s] = orig[sorted[s]];
 }
 
+// The exported pairs: rows entries (i, j) with orig(i) < orig(j) that pass the
+// reference's exact test on the positions of the build (`ref`).
 __global__ void k_verlet_pair_count(const int* __restrict__ nbr, const int* __restrict__ count,
-                                    const double4* __restrict__ pos, int64_t n, int stride,
-                                    int* out) {
+                                    const double4* __restrict__ ref, int64_t n, int stride,
+                                    Box3 box, double rl2, int* out) {
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
-    const double oi = pos[i].w;
+    const double4 pi = ref[i];
     int c = 0;
     const int cnt = min(count[i], stride);
-    for (int k = 0; k < cnt; ++k)
-        if (pos[nbr[i * stride + k]].w > oi) ++c;
+    for (int k = 0; k < cnt; ++k) {
+        const double4 pj = ref[nbr[i * stride + k]];
+        if (pj.w > pi.w && within(box, pi, pj, rl2)) ++c;
+    }
     out[i] = c;
 }
 
 __global__ void k_verlet_pair_write(const int* __restrict__ nbr, const int* __restrict__ count,
-                                    const double4* __restrict__ pos, int64_t n, int stride,
-                                    const int64_t* __restrict__ offset, int64_t* pi, int64_t* pj) {
+                                    const double4* __restrict__ ref, int64_t n, int stride,
+                                    Box3 box, double rl2, const int64_t* __restrict__ offset,
+                                    int64_t* pi, int64_t* pj) {
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
-    const double oi = pos[i].w;
+    const double4 p = ref[i];
     int64_t at = offset[i];
     const int cnt = min(count[i], stride);
     for (int k = 0; k < cnt; ++k) {
-        const double oj = pos[nbr[i * stride + k]].w;
-        if (oj > oi) {
-            pi[at] = static_cast<int64_t>(oi);
-            pj[at] = static_cast<int64_t>(oj);
+        const double4 q = ref[nbr[i * stride + k]];
+        if (q.w > p.w && within(box, p, q, rl2)) {
+            pi[at] = static_cast<int64_t>(p.w);
+            pj[at] = static_cast<int64_t>(q.w);
             ++at;
         }
     }
@@ -951,6 +1174,9 @@ int md_verlet_destroy(md_verlet* v) {
     v->nbr.release();
     v->count.release();
     v->ref.release();
+    v->halo_runs.release();
+    v->halo_meta.release();
+    v->nbr16.release();
     if (v->d_rebuild_flag) cudaFree(v->d_rebuild_flag);
     delete v;
     return MD_OK;
@@ -998,6 +1224,21 @@ int md_verlet_set_capacity(md_verlet* v, int capacity, int fixed) {
     v->stride = capacity;
     v->stride_fixed = fixed != 0;
     v->sys = nullptr;  // rows of the old capacity are no longer readable
+    v->halo_on = false;
+    return MD_OK;
+}
+
+int md_verlet_halo_tiles(md_verlet* v, int64_t* staged, int64_t* tiles) {
+    if (!v || !staged || !tiles) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_halo_tiles: NULL");
+    *staged = *tiles = 0;
+    if (!v->halo_on || v->n <= 0) return MD_OK;
+    const int64_t blocks = halo_blocks(v->n);
+    std::vector<int2> meta(static_cast<size_t>(blocks));
+    MDB_CUDA(cudaStreamSynchronize(v->ctx->stream));
+    MDB_CUDA(cudaMemcpy(meta.data(), v->halo_meta.ptr, sizeof(int2) * meta.size(),
+                        cudaMemcpyDeviceToHost));
+    for (const int2& m : meta) *staged += m.x > 0 ? 1 : 0;
+    *tiles = blocks;
     return MD_OK;
 }
 
@@ -1037,8 +1278,11 @@ int md_verlet_pairs(md_verlet* v, int64_t* pi, int64_t* pj, int64_t cap, int64_t
     }
     DevBuf cnt;
     MDB_TRY(cnt.ensure(sizeof(int) * n));
+    const Box3 box = make_box(sys);
+    const double rl2 = (v->cutoff + v->skin) * (v->cutoff + v->skin);  // verlet_list.cpp:11
     k_verlet_pair_count<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
-        v->nbr.as<int>(), v->count.as<int>(), sys->cur.pos, n, v->stride, cnt.as<int>());
+        v->nbr.as<int>(), v->count.as<int>(), v->ref.as<double4>(), n, v->stride, box, rl2,
+        cnt.as<int>());
     ++ctx->launches;
     std::vector<int> hc(static_cast<size_t>(n));
     MDB_CUDA(cudaMemcpyAsync(hc.data(), cnt.ptr, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1055,8 +1299,8 @@ int md_verlet_pairs(md_verlet* v, int64_t* pi, int64_t* pj, int64_t cap, int64_t
         MDB_CUDA(cudaMemcpyAsync(doff.ptr, off.data(), sizeof(int64_t) * (n + 1),
                                  cudaMemcpyHostToDevice, ctx->stream));
         k_verlet_pair_write<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
-            v->nbr.as<int>(), v->count.as<int>(), sys->cur.pos, n, v->stride, doff.as<int64_t>(),
-            dpi.as<int64_t>(), dpj.as<int64_t>());
+            v->nbr.as<int>(), v->count.as<int>(), v->ref.as<double4>(), n, v->stride, box, rl2,
+            doff.as<int64_t>(), dpi.as<int64_t>(), dpj.as<int64_t>());
         ++ctx->launches;
         MDB_CUDA(cudaMemcpyAsync(pi, dpi.ptr, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, ctx->stream));
         MDB_CUDA(cudaMemcpyAsync(pj, dpj.ptr, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, ctx->stream));

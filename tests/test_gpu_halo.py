@@ -1,0 +1,98 @@
+"""Halo tiles of the mixed-precision Verlet force kernel.
+
+Reading a neighbour through a tile staged in shared memory (16-bit slots) or
+gathering it through the int32 row must give bit-identical forces, energy and
+virial: the pair arithmetic and the accumulation order are the same.  Covered:
+a liquid where every tile is staged, a dilute gas where no tile is (a block of
+128 atoms spans more than 16 cells), a two-phase box where both kinds of tile
+occur in one launch, the linear-force-shift truncation, and a fused run with
+neighbour rebuilds inside the replayed step graph.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def melt(md, cells, rho, seed, steps=100):
+    st = md.fcc_lattice(cells, rho, 0.722, seed)
+    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"])
+    lj = md.LennardJones(1.0, 1.0, 2.5)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    md.LangevinBAOAB(0.005, 1.0, 0.722, seed).run(s, v, lj, steps)
+    return s, v, st
+
+
+def both_ways(md, s, v, trunc=0):
+    on = md.LennardJones(1.0, 1.0, 2.5, trunc, precision=md.PRECISION_MIXED)
+    off = md.LennardJones(1.0, 1.0, 2.5, trunc, precision=md.PRECISION_MIXED)
+    off.set_halo(False)
+    e0, w0 = off.compute_forces(s, v)
+    f0 = s.forces
+    e1, w1 = on.compute_forces(s, v)
+    f1 = s.forces
+    return (e0, w0, f0), (e1, w1, f1)
+
+
+@pytest.mark.parametrize("trunc", [0, 1])
+def test_liquid_tiles_staged_and_identical(md, trunc):
+    s, v, _ = melt(md, 12, 0.8442, 3)  # 6912 atoms
+    (e0, w0, f0), (e1, w1, f1) = both_ways(md, s, v, trunc)
+    staged, tiles = v.halo_tiles()
+    assert tiles == (s.n + 127) // 128 and staged == tiles
+    assert np.array_equal(f0, f1)
+    assert e0 == e1 and w0 == w1
+
+
+def test_dilute_gas_falls_back_identically(md):
+    st = md.fcc_lattice(10, 0.02, 1.5, 4)  # 4000 atoms, ~0.4 per cell
+    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"])
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    rng = np.random.default_rng(4)
+    s.positions = st["pos"] + rng.normal(0, 0.5, st["pos"].shape)
+    v.build(s)
+    (e0, w0, f0), (e1, w1, f1) = both_ways(md, s, v)
+    staged, tiles = v.halo_tiles()
+    assert tiles > 0 and staged == 0
+    assert np.array_equal(f0, f1) and e0 == e1 and w0 == w1
+
+
+def test_two_phase_box_mixes_staged_and_gathered_tiles(md):
+    # a dense slab and a dilute gas in one box
+    st = md.fcc_lattice(12, 0.8442, 0.722, 5)
+    pos = st["pos"].copy()
+    box = st["box"].copy()
+    box[2] *= 3.0
+    rng = np.random.default_rng(5)
+    gas = rng.uniform(-0.5, 0.5, size=(300, 3)) * box
+    gas[:, 2] = np.where(gas[:, 2] > 0, gas[:, 2] * 0.5 + box[2] / 4, gas[:, 2] * 0.5 - box[2] / 4)
+    pos = np.concatenate([pos, gas])  # gas at |z| > 0.75 Lz, the slab at |z| < 0.5 Lz
+    s = md.System.from_arrays(pos, box, vel=np.zeros_like(pos), mass=np.ones(len(pos)))
+    v = md.VerletList(box, 2.5, 0.3)
+    v.build(s)
+    (e0, w0, f0), (e1, w1, f1) = both_ways(md, s, v)
+    staged, tiles = v.halo_tiles()
+    assert 0 < staged < tiles
+    assert np.array_equal(f0, f1) and e0 == e1 and w0 == w1
+
+
+def test_fused_run_with_rebuilds_is_identical(md):
+    s, v, st = melt(md, 10, 0.8442, 6, steps=50)
+    x, vel = s.positions, s.velocities
+    out = []
+    for halo in (False, True):
+        sys_ = md.System.from_arrays(x, st["box"], vel=vel, mass=st["mass"])
+        lj = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+        lj.set_halo(halo)
+        vl = md.VerletList(st["box"], 2.5, 0.3)
+        vl.build(sys_)
+        lj.compute_forces(sys_, vl)
+        th = md.VelocityVerlet(0.005).run(sys_, vl, lj, 300, thermo=True)
+        assert vl.rebuild_count() > 3
+        out.append((sys_.positions, sys_.velocities, th, vl.halo_tiles()))
+    assert out[1][3][0] == out[1][3][1] > 0
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
