@@ -449,64 +449,64 @@ __global__ void k_verlet_brute(const double4* __restrict__ pos, int64_t n, Box3 
 // ---------------------------------------------------------------- halo tiles
 constexpr int kPlanEntries = 512;  // >= kHaloSpan * 27, a power of two
 
-// Rank of the cell holding sorted atom a (the largest r with start[r] <= a), by a
-// 32-way search of the warp: four rounds of one coalesced probe per lane for
-// 50k cells.  Every lane returns it.
-__device__ __forceinline__ int cell_rank_of(const int* __restrict__ start, int m, int64_t a,
-                                            int lane) {
-    int lo = 0, hi = m;  // start[lo] <= a < start[hi] (start[m] = n)
-    while (hi - lo > 1) {
-        const int step = (hi - lo + 31) / 32;
-        const int p = lo + (lane + 1) * step;
-        const bool le = p < hi && start[p] <= a;
-        const int k = __popc(__ballot_sync(0xffffffffu, le));  // probes are monotone
-        hi = min(hi, lo + (k + 1) * step);
-        lo += k * step;
-    }
-    return lo;
-}
-
-// One CTA per halo tile (kHaloAtoms consecutive sorted atoms).  Plan: the cell
-// ranks the tile's atoms span, their 27-cell neighbourhoods sorted (bitonic) and
-// merged into runs of consecutive ranks -- each run one contiguous range of
-// sorted atoms -- and each run's first slot in the staged tile.  A tile spanning
-// more than kHaloSpan cells, needing more than kHaloRuns runs or kHaloCap slots,
-// or lying inside one crowded cell, is not staged.  Rows: each int32 row entry j
-// becomes the 16-bit byte offset of its slot (base of the run holding j + j -
-// the run's first atom), eight entries per 16-byte access, with the last run
-// found cached per thread (entries come in stencil order).  A neighbour outside
-// the tile's runs (not possible for a list built from the same cells) un-stages
-// the tile.
-__global__ void __launch_bounds__(kBlock)
-k_halo_tiles(const int* __restrict__ start, GridArgs g, int64_t n, const int* __restrict__ nbr,
-             const int* __restrict__ count, int stride, int2* __restrict__ runs,
-             int2* __restrict__ meta, uint16_t* __restrict__ nbr16, const int* flag) {
-    if (!gate(flag)) return;
-    __shared__ int s_ent[kPlanEntries];
-    __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
-    __shared__ int s_rank[2], s_nr;
-    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
-    const int64_t a0 = static_cast<int64_t>(b) * kHaloAtoms;
-    const int64_t a1 = min(n, a0 + kHaloAtoms) - 1;
-    if (tid < 32) {
-        const int r0 = cell_rank_of(start, g.ncells, a0, lane);
-        const int r1 = cell_rank_of(start, g.ncells, a1, lane);
-        if (lane == 0) {
-            s_rank[0] = r0;
-            s_rank[1] = r1;
-            // inside one cell whose atoms run past both ends of the tile: the
-            // list build writes slots for a cell's first and last tile only
-            const bool inner = r0 == r1 && start[r0] < a0 && start[r0 + 1] - 1 > a1;
-            s_nr = inner || r1 - r0 + 1 > kHaloSpan ? -1 : 0;
+// Ranks of the cells holding sorted atoms a and b (the largest r with
+// start[r] <= a), one 16-way search per half warp: four rounds of one coalesced
+// probe per lane for 50k cells.  Every lane returns both.
+__device__ __forceinline__ int2 cell_ranks_of(const int* __restrict__ start, int m, int64_t a,
+                                              int64_t b, int lane) {
+    const int half = lane >> 4, hl = lane & 15;
+    const int64_t x = half ? b : a;
+    int lo = 0, hi = m;  // start[lo] <= x < start[hi] (start[m] = n)
+    while (__any_sync(0xffffffffu, hi - lo > 1)) {
+        const bool open = hi - lo > 1;
+        const int step = (hi - lo + 15) / 16;
+        const int p = lo + (hl + 1) * step;
+        const bool le = open && p < hi && start[p] <= x;
+        const unsigned mask = __ballot_sync(0xffffffffu, le);
+        const int k = __popc((mask >> (16 * half)) & 0xffffu);  // probes are monotone
+        if (open) {
+            hi = min(hi, lo + (k + 1) * step);
+            lo += k * step;
         }
     }
-    __syncthreads();
-    if (s_nr < 0) {
-        if (tid == 0) meta[b] = make_int2(-1, 0);
+    return make_int2(__shfl_sync(0xffffffffu, lo, 0), __shfl_sync(0xffffffffu, lo, 16));
+}
+
+// Plan of the halo tiles, one warp per tile (kHaloAtoms consecutive sorted
+// atoms): the cell ranks the tile's atoms span, their 27-cell neighbourhoods
+// sorted (bitonic, in shared memory) and merged into runs of consecutive ranks --
+// each run one contiguous range of sorted atoms -- and each run's first slot in
+// the staged tile.  A tile spanning more than kHaloSpan cells, needing more than
+// kHaloRuns runs or kHaloCap slots, or lying inside one crowded cell, is not
+// staged (meta.x = -1).
+constexpr int kPlanWarps = 8;
+
+__global__ void __launch_bounds__(32 * kPlanWarps)
+k_halo_plan(const int* __restrict__ start, GridArgs g, int64_t n, int64_t tiles,
+            int2* __restrict__ runs, int2* __restrict__ meta, const int* flag) {
+    if (!gate(flag)) return;
+    __shared__ int s_ent[kPlanWarps][kPlanEntries];
+    __shared__ int s_beg[kPlanWarps][kHaloRuns], s_end[kPlanWarps][kHaloRuns];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = static_cast<int64_t>(blockIdx.x) * kPlanWarps + warp;
+    if (b >= tiles) return;  // the whole warp; no block-wide barrier follows
+    const int64_t a0 = b * kHaloAtoms, a1 = min(n, a0 + kHaloAtoms) - 1;
+    const int2 rr = cell_ranks_of(start, g.ncells, a0, a1, lane);
+    const int r0 = rr.x, r1 = rr.y;
+    // inside one cell whose atoms run past both ends of the tile: the list build
+    // writes slots for a cell's first and last tile only
+    const bool inner = r0 == r1 && start[r0] < a0 && start[r0 + 1] - 1 > a1;
+    if (inner || r1 - r0 + 1 > kHaloSpan) {
+        if (lane == 0) meta[b] = make_int2(-1, 0);
         return;
     }
-    const int r0 = s_rank[0], ne = (s_rank[1] - r0 + 1) * 27;
-    for (int e = tid; e < kPlanEntries; e += blockDim.x) {
+    int* ent = s_ent[warp];
+    const int ne = (r1 - r0 + 1) * 27;
+    const int np2 = ne <= 256 ? 256 : kPlanEntries;  // sort only the filled power of two
+#pragma unroll
+    for (int k = 0; k < kPlanEntries / 32; ++k) {  // unrolled: the loads go out together
+        const int e = lane + 32 * k;
+        if (e >= np2) break;
         int v = 0x7fffffff;
         if (e < ne) {
             const int cell = g.cell_of_rank[r0 + e / 27], q = e % 27;
@@ -517,119 +517,138 @@ k_halo_tiles(const int* __restrict__ start, GridArgs g, int64_t n, const int* __
             jz = jz < 0 ? jz + g.nz : (jz >= g.nz ? jz - g.nz : jz);
             v = g.rank_of_cell[jx + g.nx * (jy + g.ny * jz)];
         }
-        s_ent[e] = v;
+        ent[e] = v;
     }
-    __syncthreads();
-    const int np2 = ne <= 256 ? 256 : kPlanEntries;  // sort only the filled power of two
+    __syncwarp();
     for (int k = 2; k <= np2; k <<= 1) {  // bitonic sort, ascending
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int e = tid; e < np2; e += blockDim.x) {
+            for (int e = lane; e < np2; e += 32) {
                 const int p = e ^ j;
                 if (p > e) {
-                    const int x = s_ent[e], y = s_ent[p];
+                    const int x = ent[e], y = ent[p];
                     if ((x > y) == ((e & k) == 0)) {
-                        s_ent[e] = y;
-                        s_ent[p] = x;
+                        ent[e] = y;
+                        ent[p] = x;
                     }
                 }
             }
-            __syncthreads();
-        }
-    }
-    if (tid < 32) {
-        // runs of consecutive distinct ranks (duplicates neither open nor close one)
-        int nopen = 0, nclose = 0;
-        for (int c = 0; c < ne; c += 32) {
-            const int e = c + lane;
-            const int v = e < ne ? s_ent[e] : 0;
-            const bool opens = e < ne && (e == 0 || v > s_ent[e - 1] + 1);
-            const bool closes = e < ne && (e == ne - 1 || s_ent[e + 1] > v + 1);
-            const unsigned mo = __ballot_sync(0xffffffffu, opens);
-            const unsigned mc = __ballot_sync(0xffffffffu, closes);
-            const unsigned below = (1u << lane) - 1u;
-            const int io = nopen + __popc(mo & below), ic = nclose + __popc(mc & below);
-            // first atom of an opening rank; one past the last atom of a closing one
-            if (opens && io < kHaloRuns) s_beg[io] = start[v];
-            if (closes && ic < kHaloRuns) s_base[ic] = start[v + 1];
-            nopen += __popc(mo);
-            nclose += __popc(mc);
-        }
-        __syncwarp();
-        const int nr = nopen;
-        int total = 0;
-        if (nr <= kHaloRuns) {
-            // run lengths -> slot bases (exclusive scan, two runs per lane)
-            int len[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int t = 2 * lane + h;
-                len[h] = t < nr ? s_base[t] - s_beg[t] : 0;
-            }
-            const int pair = len[0] + len[1];
-            int incl = pair;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            total = __shfl_sync(0xffffffffu, incl, 31);
             __syncwarp();
-            const int base0 = incl - pair;
-            int2* out = runs + static_cast<int64_t>(b) * kHaloRuns;
-            if (2 * lane < nr) {
-                s_base[2 * lane] = base0;
-                out[2 * lane] = make_int2(s_beg[2 * lane], base0);
-            }
-            if (2 * lane + 1 < nr) {
-                s_base[2 * lane + 1] = base0 + len[0];
-                out[2 * lane + 1] = make_int2(s_beg[2 * lane + 1], base0 + len[0]);
-            }
-        }
-        const bool staged = nr <= kHaloRuns && total <= kHaloCap;
-        if (lane == 0) {
-            s_base[staged ? nr : 0] = total;
-            s_nr = staged ? nr : -1;
-            meta[b] = make_int2(staged ? nr : -1, total);
         }
     }
+    // runs of consecutive distinct ranks (duplicates neither open nor close one)
+    int nopen = 0, nclose = 0;
+    for (int c = 0; c < ne; c += 32) {
+        const int e = c + lane;
+        const int v = e < ne ? ent[e] : 0;
+        const bool opens = e < ne && (e == 0 || v > ent[e - 1] + 1);
+        const bool closes = e < ne && (e == ne - 1 || ent[e + 1] > v + 1);
+        const unsigned mo = __ballot_sync(0xffffffffu, opens);
+        const unsigned mc = __ballot_sync(0xffffffffu, closes);
+        const unsigned below = (1u << lane) - 1u;
+        const int io = nopen + __popc(mo & below), ic = nclose + __popc(mc & below);
+        if (opens && io < kHaloRuns) s_beg[warp][io] = v;   // first rank of a run
+        if (closes && ic < kHaloRuns) s_end[warp][ic] = v;  // last rank of a run
+        nopen += __popc(mo);
+        nclose += __popc(mc);
+    }
+    __syncwarp();
+    const int nr = nopen;
+    if (nr > kHaloRuns) {
+        if (lane == 0) meta[b] = make_int2(-1, 0);
+        return;
+    }
+    // run atoms [start[first rank], start[last rank + 1]) -> slot bases (exclusive
+    // scan, two runs per lane)
+    int len[2], beg[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int t = 2 * lane + h;
+        beg[h] = t < nr ? start[s_beg[warp][t]] : 0;
+        len[h] = t < nr ? start[s_end[warp][t] + 1] - beg[h] : 0;
+    }
+    const int pair = len[0] + len[1];
+    int incl = pair;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int base0 = incl - pair;
+    int2* out = runs + b * kHaloRuns;
+    if (2 * lane < nr) out[2 * lane] = make_int2(beg[0], base0);
+    if (2 * lane + 1 < nr) out[2 * lane + 1] = make_int2(beg[1], base0 + len[0]);
+    if (lane == 0) meta[b] = make_int2(total <= kHaloCap ? nr : -1, total);
+}
+
+// Rows of a planned tile as 16-bit byte offsets of 16-byte slots (slot = base of
+// the run holding j + j - the run's first atom; kHaloCap * 16 < 2^16): four
+// threads per atom, eight entries per 16-byte access, two accesses in flight.  A
+// neighbour outside the tile's runs (not possible for a list built from the same
+// cells) un-stages the tile.
+constexpr int kRowsThreads = 4 * kHaloAtoms;
+
+// The run holding j by a fixed six-step search (kHaloRuns = 64), predicated rather
+// than branched so that the lanes of a warp stay together.
+__device__ __forceinline__ unsigned halo_slot(int j, int nr, const int* s_beg, const int* s_base,
+                                              bool& bad) {
+    int t = 0;
+#pragma unroll
+    for (int step = kHaloRuns / 2; step > 0; step >>= 1) {
+        const int mid = t + step;
+        t = mid < nr && s_beg[mid] <= j ? mid : t;
+    }
+    const int off = j - s_beg[t];
+    const bool ok = off >= 0 && off < s_base[t + 1] - s_base[t];
+    bad = bad || !ok;
+    return ok ? static_cast<unsigned>(s_base[t] + off) << 4 : 0u;
+}
+
+__global__ void __launch_bounds__(kRowsThreads)
+k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
+            const int2* __restrict__ runs, int2* meta, uint16_t* __restrict__ nbr16,
+            const int* flag) {
+    if (!gate(flag)) return;
+    __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const int2 m = meta[b];
+    if (m.x <= 0) return;
+    const int nr = m.x;
+    if (tid < nr) {
+        const int2 r = runs[static_cast<int64_t>(b) * kHaloRuns + tid];
+        s_beg[tid] = r.x;
+        s_base[tid] = r.y;
+    }
+    if (tid == 0) s_base[nr] = m.y;
     __syncthreads();
-    const int nr = s_nr;
-    if (nr <= 0) return;
-    // rows: thread t converts chunks (t & 1), (t & 1) + 2, ... of atom t >> 1
-    const int64_t i = a0 + (tid >> 1);
+    const int64_t i = static_cast<int64_t>(b) * kHaloAtoms + (tid >> 2);
     bool bad = false;
-    if (i <= a1) {
+    if (i < n) {  // thread t converts chunks (t & 3), (t & 3) + 4, ... of atom t >> 2
         const int c = min(count[i], stride);
         const int4* src = reinterpret_cast<const int4*>(nbr + i * stride);
         uint4* dst = reinterpret_cast<uint4*>(nbr16 + i * stride);
-        int t = 0, beg = s_beg[0], len = s_base[1] - s_base[0];
-        for (int ch = tid & 1; 8 * ch < c; ch += 2) {
-            const int4 lo4 = __ldg(src + 2 * ch), hi4 = __ldg(src + 2 * ch + 1);
-            const int js[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
-            unsigned off[8];
+        for (int ch = tid & 3; 8 * ch < c; ch += 8) {
+            const int ch2 = ch + 4;
+            const bool two = 8 * ch2 < c;
+            const int4 a0 = __ldg(src + 2 * ch), a1 = __ldg(src + 2 * ch + 1);
+            int4 b0 = make_int4(0, 0, 0, 0), b1 = b0;
+            if (two) {
+                b0 = __ldg(src + 2 * ch2);
+                b1 = __ldg(src + 2 * ch2 + 1);
+            }
+            const int js[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                                b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            unsigned off[16];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                off[k] = 0u;
-                if (8 * ch + k < c) {
-                    const int j = js[k];
-                    if (static_cast<unsigned>(j - beg) >= static_cast<unsigned>(len)) {
-                        int lo = 0, hi = nr;  // the last run whose first atom is <= j
-                        while (hi - lo > 1) {
-                            const int mid = (lo + hi) >> 1;
-                            if (s_beg[mid] <= j) lo = mid;
-                            else hi = mid;
-                        }
-                        t = lo;
-                        beg = s_beg[t];
-                        len = s_base[t + 1] - s_base[t];
-                    }
-                    const bool ok = static_cast<unsigned>(j - beg) < static_cast<unsigned>(len);
-                    bad = bad || !ok;
-                    off[k] = ok ? static_cast<unsigned>(s_base[t] + (j - beg)) << 4 : 0u;
-                }
+            for (int k = 0; k < 16; ++k) {
+                const int e = 8 * (k < 8 ? ch : ch2) + (k & 7);
+                off[k] = e < c ? halo_slot(js[k], nr, s_beg, s_base, bad) : 0u;
             }
             dst[ch] = make_uint4(off[0] | (off[1] << 16), off[2] | (off[3] << 16),
                                  off[4] | (off[5] << 16), off[6] | (off[7] << 16));
+            if (two)
+                dst[ch2] = make_uint4(off[8] | (off[9] << 16), off[10] | (off[11] << 16),
+                                      off[12] | (off[13] << 16), off[14] | (off[15] << 16));
         }
     }
     if (__syncthreads_or(bad) && tid == 0) meta[b].x = -1;
@@ -805,21 +824,37 @@ static int verlet_alloc(md_verlet* v, md_system* sys) {
     return MD_OK;
 }
 
-// Halo tiles of the current list (gated by the rebuild flag inside fused loops).
+// Halo tile buffers for the current size and row capacity.
+int halo_alloc(md_verlet* v, int64_t n) {
+    const int64_t tiles = halo_blocks(n);
+    MDB_TRY(v->halo_runs.ensure(sizeof(int2) * static_cast<size_t>(tiles) * kHaloRuns));
+    MDB_TRY(v->halo_meta.ensure(sizeof(int2) * static_cast<size_t>(tiles)));
+    MDB_TRY(v->nbr16.ensure(sizeof(uint16_t) * static_cast<size_t>(n) * v->stride));
+    return MD_OK;
+}
+
+void halo_plan(md_verlet* v, md_system* sys, const int* flag) {
+    const int64_t n = sys->n, tiles = halo_blocks(n);
+    k_halo_plan<<<static_cast<unsigned>((tiles + kPlanWarps - 1) / kPlanWarps), 32 * kPlanWarps, 0,
+                  sys->ctx->stream>>>(v->start.as<int>(), make_args(v->grid, sys), n, tiles,
+                                      v->halo_runs.as<int2>(), v->halo_meta.as<int2>(), flag);
+    ++sys->ctx->launches;
+}
+
+// Halo tiles of the current list: plan, then convert its rows (gated by the
+// rebuild flag inside fused loops).
 int halo_build(md_verlet* v, md_system* sys, const int* flag) {
     md_context* ctx = sys->ctx;
+    const int64_t n = sys->n;
     if (v->stride % 8 != 0) {  // rows are converted and read 16 bytes at a time
         v->halo_on = false;
         return MD_OK;
     }
-    const int64_t n = sys->n, blocks = halo_blocks(n);
-    MDB_TRY(v->halo_runs.ensure(sizeof(int2) * static_cast<size_t>(blocks) * kHaloRuns));
-    MDB_TRY(v->halo_meta.ensure(sizeof(int2) * static_cast<size_t>(blocks)));
-    MDB_TRY(v->nbr16.ensure(sizeof(uint16_t) * static_cast<size_t>(n) * v->stride));
-    const GridArgs g = make_args(v->grid, sys);
-    k_halo_tiles<<<static_cast<unsigned>(blocks), kBlock, 0, ctx->stream>>>(
-        v->start.as<int>(), g, n, v->nbr.as<int>(), v->count.as<int>(), v->stride,
-        v->halo_runs.as<int2>(), v->halo_meta.as<int2>(), v->nbr16.as<uint16_t>(), flag);
+    MDB_TRY(halo_alloc(v, n));
+    halo_plan(v, sys, flag);
+    k_halo_rows<<<static_cast<unsigned>(halo_blocks(n)), kRowsThreads, 0, ctx->stream>>>(
+        v->nbr.as<int>(), v->count.as<int>(), v->stride, n, v->halo_runs.as<int2>(),
+        v->halo_meta.as<int2>(), v->nbr16.as<uint16_t>(), flag);
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;
@@ -853,6 +888,7 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
             sys->cur.pos, start, g, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
             ctx->d_status, v->d_max_count, flag, groups);
         ++ctx->launches;
+        if (v->halo_on && n > 0) MDB_TRY(halo_build(v, sys, flag));
     } else if (n > 0) {
         k_verlet_brute<<<grid_for(n * 32, kBlock), kBlock, 0, ctx->stream>>>(
             sys->cur.pos, n, box, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
@@ -864,7 +900,6 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
             sys->cur.pos, v->ref.as<double4>(), n, flag, flag ? v->d_rebuild_total : nullptr);
         ++ctx->launches;
     }
-    if (v->halo_on && v->grid.usable && n > 0) MDB_TRY(halo_build(v, sys, flag));
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
