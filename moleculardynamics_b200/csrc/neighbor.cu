@@ -314,6 +314,11 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     const double oy = -0.5 * g.box.L[1] + (cy + 0.5) * g.wy;
     const double oz = -0.5 * g.box.L[2] + (cz + 0.5) * g.wz;
     const float hi_thr = static_cast<float>(rl2 * (1.0 + 1.0 / 4096.0));
+    // half widths of the cell's box, widened a little (its atoms were binned with
+    // the reference arithmetic, their offsets here are FP64 then FP32)
+    const float hwx = static_cast<float>(0.5 * g.wx * (1.0 + 1e-6)) + 1e-6f;
+    const float hwy = static_cast<float>(0.5 * g.wy * (1.0 + 1e-6)) + 1e-6f;
+    const float hwz = static_cast<float>(0.5 * g.wz * (1.0 + 1e-6)) + 1e-6f;
     // the 27 neighbour cell ranges (lane q holds cell q of the stencil)
     int beg = 0, cnt = 0;
     if (lane < 27) {
@@ -338,31 +343,49 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     for (int wb = 0; wb < total; wb += kMaxCand) {
         const int wlen = min(kMaxCand, total - wb);
         __syncwarp();
-        // stage candidates [wb, wb + wlen) cell by cell
+        // stage candidates [wb, wb + wlen) cell by cell, keeping only those within
+        // the list cutoff of the cell's own box (a quarter of the 27-cell volume is
+        // farther from every atom of the cell); order is kept
+        int ns = 0;
         for (int q = 0; q < 27; ++q) {
             const int qb = __shfl_sync(0xffffffffu, beg, q);
             const int qo = __shfl_sync(0xffffffffu, excl, q);
             const int qc = __shfl_sync(0xffffffffu, cnt, q);
             const int lo = max(qo, wb), hi = min(qo + qc, wb + wlen);
-            for (int gt = lo + lane; gt < hi; gt += 32) {
+            for (int gb = lo; gb < hi; gb += 32) {
+                const int gt = gb + lane;
                 const int j = qb + (gt - qo);
-                const double4 pj = ldg4(pos + j);
-                double vx = pj.x - ox, vy = pj.y - oy, vz = pj.z - oz;
-                vx -= g.box.L[0] * rint(vx * g.box.inv[0]);
-                vy -= g.box.L[1] * rint(vy * g.box.inv[1]);
-                vz -= g.box.L[2] * rint(vz * g.box.inv[2]);
-                const int tt = gt - wb, pr = tt >> 1, h = tt & 1;
-                float* A = reinterpret_cast<float*>(&s_a[warp][pr]);
-                float* B = reinterpret_cast<float*>(&s_b[warp][pr]);
-                A[h] = -static_cast<float>(vx);
-                A[2 + h] = -static_cast<float>(vy);
-                B[h] = -static_cast<float>(vz);
-                B[2 + h] = __int_as_float(j);
+                double vx = 0.0, vy = 0.0, vz = 0.0;
+                bool keep = false;
+                if (gt < hi) {
+                    const double4 pj = ldg4(pos + j);
+                    vx = pj.x - ox;
+                    vy = pj.y - oy;
+                    vz = pj.z - oz;
+                    vx -= g.box.L[0] * rint(vx * g.box.inv[0]);
+                    vy -= g.box.L[1] * rint(vy * g.box.inv[1]);
+                    vz -= g.box.L[2] * rint(vz * g.box.inv[2]);
+                    const float ex = fmaxf(fabsf(static_cast<float>(vx)) - hwx, 0.f);
+                    const float ey = fmaxf(fabsf(static_cast<float>(vy)) - hwy, 0.f);
+                    const float ez = fmaxf(fabsf(static_cast<float>(vz)) - hwz, 0.f);
+                    keep = fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < hi_thr;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int tt = ns + __popc(m & ((1u << lane) - 1u)), pr = tt >> 1, h = tt & 1;
+                    float* A = reinterpret_cast<float*>(&s_a[warp][pr]);
+                    float* B = reinterpret_cast<float*>(&s_b[warp][pr]);
+                    A[h] = -static_cast<float>(vx);
+                    A[2 + h] = -static_cast<float>(vy);
+                    B[h] = -static_cast<float>(vz);
+                    B[2 + h] = __int_as_float(j);
+                }
+                ns += __popc(m);
             }
         }
-        if ((wlen & 1) && lane == 0) {  // pad the odd slot: infinitely far, no atom
-            float* A = reinterpret_cast<float*>(&s_a[warp][wlen >> 1]);
-            float* B = reinterpret_cast<float*>(&s_b[warp][wlen >> 1]);
+        if ((ns & 1) && lane == 0) {  // pad the odd slot: infinitely far, no atom
+            float* A = reinterpret_cast<float*>(&s_a[warp][ns >> 1]);
+            float* B = reinterpret_cast<float*>(&s_b[warp][ns >> 1]);
             A[1] = A[3] = B[1] = 1e30f;
             B[3] = __int_as_float(-1);
         }
@@ -388,7 +411,7 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
             // Per candidate pair: packed FP32x2 distances and predicated appends.
             const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy),
                          fz2 = make_float2(fz, fz);
-            const int npairs = (wlen + 1) >> 1;
+            const int npairs = (ns + 1) >> 1;
 #pragma unroll 2
             for (int pr = 0; pr < npairs; ++pr) {
                 const float4 A = s_a[warp][pr], B = s_b[warp][pr];
