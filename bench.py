@@ -152,8 +152,8 @@ class Group:
 # ----------------------------------------------------------------------- GPU arm
 def traffic_per_atom():
     """DRAM bytes per atom of one mixed LJ force launch, from the committed ncu
-    summary (profiles/k_lj_verlet_mixed_lj1m.txt), or None."""
-    path = os.path.join(ROOT, "profiles", "k_lj_verlet_mixed_lj1m.txt")
+    summary (profiles/k_lj_halo_mixed_lj1m.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "k_lj_halo_mixed_lj1m.txt")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_atom:"):
@@ -415,9 +415,9 @@ def run_gpu_arm(args):
     if rank == 0:
         peaks, peak_src = measured_peaks()
         # algorithmic bytes of one mixed force launch per atom: own fixed-point
-        # position (16 B) + force write (24 B) + the half neighbour list (4 B per
-        # unique pair)
-        alg_per_atom = 16.0 + 24.0 + 4.0 * nbr / 2.0
+        # position (16 B) + force write (24 B) + its row of the full neighbour list
+        # as 16-bit halo-tile slots (2 B per entry)
+        alg_per_atom = 16.0 + 24.0 + 2.0 * nbr
         achieved = alg_per_atom * n / (kmx * 1e-3) / 1e9
         tpa = traffic_per_atom()
         e0_64 = rows64[0, 0] + rows64[0, 2]
@@ -455,7 +455,7 @@ def run_gpu_arm(args):
                     "steps": e2e_steps,
                     "path": "md_system_set x9 (pinned host) + md_run_lj(1 step) + "
                             "md_system_get x9 per step"},
-            "roofline": {"bound": "hbm", "kernel": "k_lj_verlet (mixed)",
+            "roofline": {"bound": "hbm", "kernel": "k_lj_halo (mixed, halo tiles)",
                          "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": achieved / peaks.get("hbm_gbs", 6650.0),
                          "peak_source": f"hbm_gbs of {peak_src}",

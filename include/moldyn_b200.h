@@ -214,15 +214,21 @@ MD_API int md_lj_set_unroll(int unroll);
  * gathers in flight 1/2/4; 0 = the library default).  Set by the autotuner
  * (moleculardynamics_b200/autotune.py); no reference counterpart. */
 MD_API int md_lj_set_launch(md_lj* lj, int tpa, int unroll);
-/* Mixed precision only: read neighbours through halo tiles (on = 1, the
- * default) or gather them through the int32 rows (0).  A halo tile holds a block
- * of 128 cell-sorted atoms and every atom of the cells around them in shared
- * memory; rows then hold 16-bit tile slots.  Forces are identical either way.
- * No reference counterpart. */
+/* Mixed precision only: read neighbours through the list's halo tiles when it
+ * keeps them (on = 1, the default) or always gather them through the int32 rows
+ * (0).  A halo tile holds a block of 128 cell-sorted atoms and every atom of the
+ * cells around them in shared memory; rows then also exist as 16-bit tile slots.
+ * Forces are identical either way.  No reference counterpart. */
 MD_API int md_lj_set_halo(md_lj* lj, int on);
-/* Halo tiles of a Verlet list: how many of its tiles are staged in shared memory
- * (the rest gather through the int32 rows), out of how many (both 0 until a
- * mixed-precision force call has used the list).  Diagnostics; synchronises. */
+/* Halo tiles of a Verlet list: built now from the current list and again at
+ * every rebuild (on = 1), or dropped (0).  md_run_lj and md_batch_run turn them on
+ * by themselves for mixed-precision runs of >= 16 steps on >= 65,536 atoms, where
+ * the faster force kernel pays for building them.  Lists without a cell grid
+ * (fewer than 3 cells per side) keep none.  No reference counterpart. */
+MD_API int md_verlet_set_halo(md_verlet* v, int on);
+/* How many of a list's halo tiles are staged in shared memory (the rest gather
+ * through the int32 rows), out of how many (0, 0 without tiles).  Diagnostics;
+ * synchronises. */
 MD_API int md_verlet_halo_tiles(md_verlet* v, int64_t* staged, int64_t* tiles);
 
 /* ------------------------------------------------------------------- Ewald */

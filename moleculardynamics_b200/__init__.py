@@ -133,6 +133,7 @@ def _load():
         "md_lj_set_launch": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_lj_set_halo": (C.c_int, [_vp, C.c_int]),
         "md_verlet_halo_tiles": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "md_verlet_set_halo": (C.c_int, [_vp, C.c_int]),
         "md_integrator_create_vv": (C.c_int, [C.c_double, C.POINTER(_vp)]),
         "md_integrator_create_baoab": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_uint64,
                                                  C.POINTER(_vp)]),
@@ -472,9 +473,13 @@ class VerletList:
         unless fixed.  The list must be built again."""
         _check(lib().md_verlet_set_capacity(self._h, int(capacity), 1 if fixed else 0))
 
+    def set_halo(self, on=True):
+        """Keep halo tiles for the mixed-precision force kernel (built now and at
+        every rebuild), or drop them.  Fused runs of large systems turn them on."""
+        _check(lib().md_verlet_set_halo(self._h, 1 if on else 0))
+
     def halo_tiles(self):
-        """(staged, total) halo tiles of this list (0, 0 before a mixed-precision
-        force call has used it)."""
+        """(staged, total) halo tiles of this list ((0, 0) without tiles)."""
         a, b = C.c_int64(), C.c_int64()
         _check(lib().md_verlet_halo_tiles(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value

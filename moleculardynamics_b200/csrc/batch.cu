@@ -100,6 +100,7 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     for (auto& r : b->reps) {
         MDB_TRY(verlet_ensure_ready(r.list, r.sys, "md_batch_run"));
         if (r.sys->n == 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_batch_run: empty replica");
+        verlet_halo_for_run(r.list, r.sys, r.lj, steps);
     }
     MDB_CUDA(cudaSetDevice(b->device));
     std::vector<Run> run(nr);

@@ -683,6 +683,7 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
     // no allocation.  Later steps replay the graph when that is possible
     // (BAOAB's noise counter is a host-side launch argument, so it never is).
     const bool want_graph = ctx->graphs && !ctx->timing && it->kind != 1 && steps >= 4 && sys->n > 0;
+    verlet_halo_for_run(v, sys, lj, steps);
     StepGraph sg;
     for (int64_t k = 0; k < steps; ++k) {
         MDB_TRY(lj_fused_step(it, sys, v, lj, rows.as<double>(), idx.as<int>(), k == 0));

@@ -739,9 +739,9 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
             sys->qpos.as<int4>());
         ++ctx->launches;
     }
-    // halo tiles need the list's cell grid; they are built once here and then with
-    // every rebuild of this list
-    const bool halo = mixed && lj->halo && sys->n > 0 && verlet_halo_ready(v, sys);
+    // halo tiles, when the list keeps them (fused runs of large systems turn them on,
+    // or md_verlet_set_halo)
+    const bool halo = mixed && lj->halo && sys->n > 0 && v->halo_on && v->stride % 8 == 0;
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     if (halo) {
         if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out);

@@ -218,10 +218,17 @@ constexpr int kHaloAtoms = 128;
 constexpr int kHaloRuns = 64;
 constexpr int kHaloCap = 2560;
 constexpr int kHaloSpan = 16;
+// Fused runs keep halo tiles for systems of at least this many atoms and runs of at
+// least kHaloMinSteps steps: below that, building the tiles at each rebuild costs
+// more than the faster force kernel saves.
+constexpr int64_t kHaloMinAtoms = 65536;
+constexpr int64_t kHaloMinSteps = 16;
 inline int64_t halo_blocks(int64_t n) { return (n + kHaloAtoms - 1) / kHaloAtoms; }
 // Turns the halo tiles on for this list (built right away from the current list
 // unless the stream is capturing); false when they cannot be used.
 bool verlet_halo_ready(md_verlet* v, md_system* sys);
+// The fused-run policy above, for a mixed-precision LJ force field.
+void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj, int64_t steps);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 int verlet_check(md_verlet* v, md_system* sys);  // device flag <- needs rebuild
 int verlet_ensure_capacity(md_verlet* v, md_system* sys);

@@ -974,6 +974,12 @@ bool verlet_halo_ready(md_verlet* v, md_system* sys) {
     return true;
 }
 
+void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj, int64_t steps) {
+    if (lj->precision == MD_PRECISION_MIXED && lj->halo && sys->n >= kHaloMinAtoms &&
+        steps >= kHaloMinSteps)
+        verlet_halo_ready(v, sys);
+}
+
 DispArgs disp_args(md_verlet* v, md_context* ctx, double* part) {
     DispArgs d;
     d.ref = v->ref.as<double4>();
@@ -1284,6 +1290,18 @@ int md_verlet_set_capacity(md_verlet* v, int capacity, int fixed) {
     v->sys = nullptr;  // rows of the old capacity are no longer readable
     v->halo_on = false;
     return MD_OK;
+}
+
+int md_verlet_set_halo(md_verlet* v, int on) {
+    if (!v) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_halo: NULL");
+    if (!on) {
+        v->halo_on = false;
+        return MD_OK;
+    }
+    if (!v->sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_halo: list was never built");
+    MDB_TRY(verlet_ready(v, v->sys, "md_verlet_set_halo"));
+    verlet_halo_ready(v, v->sys);  // a list without a cell grid keeps gathering
+    return ctx_check_status(v->ctx);
 }
 
 int md_verlet_halo_tiles(md_verlet* v, int64_t* staged, int64_t* tiles) {

@@ -31,6 +31,7 @@ def both_ways(md, s, v, trunc=0):
     off.set_halo(False)
     e0, w0 = off.compute_forces(s, v)
     f0 = s.forces
+    v.set_halo(True)
     e1, w1 = on.compute_forces(s, v)
     f1 = s.forces
     return (e0, w0, f0), (e1, w1, f1)
@@ -89,6 +90,7 @@ def test_fused_run_with_rebuilds_is_identical(md):
         lj.set_halo(halo)
         vl = md.VerletList(st["box"], 2.5, 0.3)
         vl.build(sys_)
+        vl.set_halo(halo)  # 4000 atoms: below the size fused runs turn tiles on at
         lj.compute_forces(sys_, vl)
         th = md.VelocityVerlet(0.005).run(sys_, vl, lj, 300, thermo=True)
         assert vl.rebuild_count() > 3
@@ -96,3 +98,18 @@ def test_fused_run_with_rebuilds_is_identical(md):
     assert out[1][3][0] == out[1][3][1] > 0
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2])
+
+
+def test_tile_policy(md):
+    """Tiles are kept only where they pay: a fused mixed run of a small system or a
+    single force call leaves a list without them; set_halo(False) drops them."""
+    s, v, st = melt(md, 8, 0.8442, 7, steps=20)  # 2048 atoms
+    lj = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+    lj.compute_forces(s, v)
+    md.VelocityVerlet(0.005).run(s, v, lj, 40)
+    assert v.halo_tiles() == (0, 0)
+    v.set_halo(True)
+    staged, tiles = v.halo_tiles()
+    assert tiles == 16 and staged == tiles
+    v.set_halo(False)
+    assert v.halo_tiles() == (0, 0)
