@@ -36,7 +36,6 @@
 
 namespace mdb {
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
-int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
 int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
 }
 

@@ -34,6 +34,8 @@ struct StepArgs {
     uint64_t step;
     const double* noise;  // replayed normals for this step (original order), or null
     uint32_t* status;     // MD_STATUS_NONFINITE when a position stops being finite
+    int4* q;              // fixed-point copy of the new positions for the mixed force, or null
+    double qs[3];         // 2^32 / L per axis
 };
 
 __device__ __forceinline__ void check_finite(const double4& p, uint32_t* status) {
@@ -77,6 +79,7 @@ __global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* 
         a.vx[k] = vx;
         a.vy[k] = vy;
         a.vz[k] = vz;
+        if (s.q) s.q[k] = quantize_position(p, s.qs[0], s.qs[1], s.qs[2]);
         if (CHECK) a1 = disp2(f3, p, d.ref[k]);
     }
     if (CHECK) top2_grid(a1, 0.0, d);
@@ -270,6 +273,7 @@ StepArgs step_args(const md_integrator* it, const md_system* sys) {
     s.step = it->step;
     s.noise = nullptr;
     s.status = sys->ctx->d_status;
+    s.q = nullptr;
     return s;
 }
 
@@ -288,11 +292,20 @@ NhcState* nhc_of(md_integrator* it) {
 // fresh_ke: the chain half of a Nose-Hoover step sums the kinetic energy of the
 // current velocities; otherwise it uses the value the chain tracked through the
 // previous step's rescalings (fused loops, after their first step).
-int pre_force(md_integrator* it, md_system* sys, md_verlet* check, bool fresh_ke = true) {
+// q: also write the fixed-point positions for a mixed-precision force (kick/drift
+// integrators only; pre_force_quantizes says whether it does).
+bool pre_force_quantizes(const md_integrator* it) { return it->kind != 1; }
+
+int pre_force(md_integrator* it, md_system* sys, md_verlet* check, bool fresh_ke = true,
+              int4* q = nullptr) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     if (n == 0) return MD_OK;
     StepArgs s = step_args(it, sys);
+    if (q && pre_force_quantizes(it)) {
+        s.q = q;
+        for (int d = 0; d < 3; ++d) s.qs[d] = 4294967296.0 / sys->box[d];
+    }
     DispArgs d{};
     const int blocks = grid_for(n, kBlock);
     if (check) {
@@ -358,7 +371,6 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
 
 }  // namespace
 
-int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 
 // ------------------------------------------------------------ step graphs
@@ -416,14 +428,29 @@ int vv_pre_async(md_integrator* it, md_system* sys, md_verlet* check) {
 
 int vv_post_async(md_integrator* it, md_system* sys) { return post_force_async(it, sys, true); }
 
+// The fixed-point position buffer the step's kick/drift fills for a mixed force
+// (null when the force is FP64 or the integrator has no kick/drift kernel).
+int step_quantize_target(md_integrator* it, md_system* sys, const md_lj* lj, int4** q) {
+    *q = nullptr;
+    if (lj->precision != MD_PRECISION_MIXED || !pre_force_quantizes(it) || sys->n <= 0)
+        return MD_OK;
+    MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(sys->n)));
+    *q = sys->qpos.as<int4>();
+    return MD_OK;
+}
+
 int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, double* rows,
                   int* idx, bool first) {
     md_context* ctx = sys->ctx;
     // Kick/drift with the rebuild test of the ForceFn (apps/moldyn_run.cpp:581-587)
-    // fused in; the rebuild itself is gated on the device flag.
-    MDB_TRY(pre_force(it, sys, v, first));
+    // fused in; the rebuild itself is gated on the device flag.  A mixed force
+    // takes the fixed-point positions the kick/drift wrote, re-quantized only after
+    // a rebuild re-sorted the atoms.
+    int4* q = nullptr;
+    MDB_TRY(step_quantize_target(it, sys, lj, &q));
+    MDB_TRY(pre_force(it, sys, v, first, q));
     MDB_TRY(verlet_build(v, sys, true));
-    MDB_TRY(lj_forces_verlet_async(lj, sys, v));
+    MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr));
     MDB_TRY(post_force_async(it, sys, false));
     if (rows) {
         k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE),
@@ -445,8 +472,10 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
     if (cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
         return fail(MD_ERR_CUDA, "cudaGraphConditionalHandleCreate failed");
     std::vector<cudaGraphNode_t> leaves;
+    int4* q = nullptr;
+    MDB_TRY(step_quantize_target(it, sys, lj, &q));  // allocated by the first, eager step
     rc = capture_into(ctx, graph, nullptr, 0, [&]() -> int {
-        MDB_TRY(pre_force(it, sys, v, false));
+        MDB_TRY(pre_force(it, sys, v, false, q));
         k_set_rebuild<<<1, 1, 0, ctx->stream>>>(h, v->d_rebuild_flag);
         ++ctx->launches;
         MDB_CHECK_LAUNCH();
@@ -471,7 +500,7 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
     const int64_t l2 = ctx->launches;
     if (rc == MD_OK)
         rc = capture_into(ctx, graph, &cond, 1, [&]() -> int {
-            MDB_TRY(lj_forces_verlet_async(lj, sys, v));
+            MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr));
             MDB_TRY(post_force_async(it, sys, false));
             if (rows) {
                 k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy),

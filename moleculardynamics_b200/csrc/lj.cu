@@ -647,18 +647,15 @@ void launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, 
         sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
 }
 
-// Fixed-point positions for the mixed pair kernel: q = round(x 2^32 / L) taken
-// modulo 2^32 (so unwrapped coordinates land on their periodic image), w = the
-// original index.
+// Fixed-point positions for the mixed pair kernels (quantize_position), skipped
+// when `flag` is given and zero: the step's kick/drift already wrote them and no
+// rebuild re-sorted the atoms since.
 __global__ void k_quantize(const double4* __restrict__ pos, int64_t n, double sx, double sy,
-                           double sz, int4* __restrict__ q) {
+                           double sz, int4* __restrict__ q, const int* flag) {
+    if (flag && *flag == 0) return;
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (k >= n) return;
-    const double4 p = pos[k];
-    q[k] = make_int4(static_cast<int>(static_cast<unsigned>(llrint(p.x * sx))),
-                     static_cast<int>(static_cast<unsigned>(llrint(p.y * sy))),
-                     static_cast<int>(static_cast<unsigned>(llrint(p.z * sz))),
-                     static_cast<int>(p.w));
+    q[k] = quantize_position(pos[k], sx, sy, sz);
 }
 
 template <bool LFS, int U>
@@ -709,7 +706,7 @@ void launch_verlet_tpa(int tpa, int unroll, md_system* sys, md_verlet* v, const 
 int g_lj_tpa = 2;     // threads per atom of the Verlet force kernel (tunable)
 int g_lj_unroll = 2;  // independent gather chains per thread (tunable)
 
-int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q_gate) {
     md_context* ctx = sys->ctx;
     LJArgs a = make_lj_args(lj);
     double res_max = 0.0;
@@ -736,7 +733,7 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v) {
         const double two32 = 4294967296.0;
         k_quantize<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(
             sys->cur.pos, sys->n, two32 / sys->box[0], two32 / sys->box[1], two32 / sys->box[2],
-            sys->qpos.as<int4>());
+            sys->qpos.as<int4>(), q_gate);
         ++ctx->launches;
     }
     // halo tiles, when the list keeps them (fused runs of large systems turn them on,

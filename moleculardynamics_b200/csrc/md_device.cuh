@@ -107,6 +107,17 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Deterministic grid-wide sums: per-block partials, then the last block to
 // arrive (ticket) sums them in block order into out[0..K).  With `status`, a
 // non-finite sum (an atom that blew up) also sets MD_STATUS_NONFINITE there.
+// Fixed-point position for the mixed pair kernels: q = round(x 2^32 / L) taken
+// modulo 2^32 (so unwrapped coordinates land on their periodic image), w = the
+// original index.
+__device__ __forceinline__ int4 quantize_position(const double4& p, double sx, double sy,
+                                                  double sz) {
+    return make_int4(static_cast<int>(static_cast<unsigned>(llrint(p.x * sx))),
+                     static_cast<int>(static_cast<unsigned>(llrint(p.y * sy))),
+                     static_cast<int>(static_cast<unsigned>(llrint(p.z * sz))),
+                     static_cast<int>(p.w));
+}
+
 template <int K>
 __device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out,
                             uint32_t* status = nullptr) {

@@ -264,7 +264,11 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
 
 // Pair-force kernels over the Verlet list; results land in the context result
 // slots kResEnergy / kResVirial (device), no synchronisation.
-int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v);
+// q_gate: the fixed-point positions were written by the step's kick/drift; they
+// are re-quantized only when this device flag says a rebuild re-sorted the atoms
+// (null: always quantize).
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v,
+                           const int* q_gate = nullptr);
 int lj_forces_brute_async(md_lj* lj, md_system* sys, bool forces);
 int lj_forces_cells_async(md_lj* lj, md_system* sys, md_cells* cells);
 int system_kinetic_async(md_system* sys, int slot);
