@@ -82,6 +82,9 @@ typedef struct md_ewald md_ewald;
 typedef struct md_rigid md_rigid;
 typedef struct md_batch md_batch;
 typedef struct md_adjoint md_adjoint;
+typedef struct md_rdf md_rdf;
+typedef struct md_msd md_msd;
+typedef struct md_vacf md_vacf;
 
 /* ------------------------------------------------------------------ library */
 /* Message of the last failing call on this thread ("" if none). */
@@ -410,6 +413,51 @@ MD_API int md_ewald_real_hvp(md_ewald* ff, md_system* sys, const double* u, doub
  * potential energy (K), virial, kinetic energy, conserved contribution. */
 MD_API int md_run_spce(md_integrator* integ, md_system* sys, md_ewald* ff, int64_t steps,
                        double* thermo);
+
+/* ---------------------------------------------------------------- analysis */
+/* Radial distribution function, analyze/rdf.hpp:16-34 (Rdf(rMax, bins)).
+ * md_rdf_accumulate adds one frame (rdf.cpp:55-82): every pair i < j with
+ * minimum-image distance r < rMax counted into bin (size_t)(r / (rMax / bins)),
+ * MD_ERR_INVALID_ARGUMENT (the reference's std::invalid_argument) when rMax
+ * exceeds half the smallest box length.  Pairs are found through a cell grid of
+ * width >= rMax on the device; the distance and bin use the reference's
+ * arithmetic, so md_rdf_histogram (bins doubles: the raw pair counts) equals the
+ * reference's histogram.  md_rdf_g is Rdf::g (rdf.cpp:92-107), md_rdf_bin_centres
+ * Rdf::binCentres (rdf.cpp:84-90), md_rdf_frames Rdf::frames. */
+MD_API int md_rdf_create(md_context* ctx, double rmax, int64_t bins, md_rdf** out);
+MD_API int md_rdf_destroy(md_rdf* rdf);
+MD_API int md_rdf_accumulate(md_rdf* rdf, md_system* sys);
+MD_API int md_rdf_histogram(const md_rdf* rdf, double* hist);
+MD_API int md_rdf_g(const md_rdf* rdf, double* g);
+MD_API int md_rdf_bin_centres(const md_rdf* rdf, double* centres);
+MD_API int md_rdf_frames(const md_rdf* rdf, int64_t* frames);
+
+/* Mean-squared displacement, analyze/msd.hpp:19-42 (Msd(natoms, maxLag)).
+ * md_msd_push (msd.cpp:66-96) unwraps incrementally with the minimum image of
+ * each step and adds |u_i(t) - u_i(t - lag)|^2 over atoms for every available lag;
+ * the ring of maxLag + 1 frames lives on the device (24 bytes per atom per frame).
+ * The per-lag sum over atoms is a fixed-order tree sum (the reference sums in atom
+ * order), so values agree with the reference to ~1e-13 relative.  The system must
+ * have natoms atoms (MD_ERR_INVALID_ARGUMENT otherwise).  md_msd_values writes
+ * maxLag + 1 doubles (Msd::msd, msd.cpp:98-106); md_msd_diffusion is
+ * Msd::diffusionCoefficient (msd.cpp:108-136). */
+MD_API int md_msd_create(md_context* ctx, int64_t natoms, int64_t max_lag, md_msd** out);
+MD_API int md_msd_destroy(md_msd* msd);
+MD_API int md_msd_push(md_msd* msd, md_system* sys);
+MD_API int md_msd_values(const md_msd* msd, double* out);
+MD_API int md_msd_diffusion(const md_msd* msd, double dt, int64_t fit_from, int64_t fit_to,
+                            double* d);
+
+/* Velocity autocorrelation, analyze/vacf.hpp:151-174 (Vacf(natoms, maxLag)):
+ * md_vacf_push as vacf.cpp:195-216 (v_i(t) . v_i(t - lag), same sums as MSD),
+ * md_vacf_values(normalised = 1: Vacf::vacf, vacf.cpp:228-239; 0: the
+ * unnormalised means), md_vacf_diffusion the Green-Kubo integral
+ * (vacf.cpp:241-261). */
+MD_API int md_vacf_create(md_context* ctx, int64_t natoms, int64_t max_lag, md_vacf** out);
+MD_API int md_vacf_destroy(md_vacf* vacf);
+MD_API int md_vacf_push(md_vacf* vacf, md_system* sys);
+MD_API int md_vacf_values(const md_vacf* vacf, int normalised, double* out);
+MD_API int md_vacf_diffusion(const md_vacf* vacf, double dt, double* d);
 
 #ifdef __cplusplus
 }

@@ -132,6 +132,23 @@ def _load():
         "md_lj_set_unroll": (C.c_int, [C.c_int]),
         "md_lj_set_launch": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_lj_set_halo": (C.c_int, [_vp, C.c_int]),
+        "md_rdf_create": (C.c_int, [_vp, C.c_double, C.c_int64, C.POINTER(_vp)]),
+        "md_rdf_destroy": (C.c_int, [_vp]),
+        "md_rdf_accumulate": (C.c_int, [_vp, _vp]),
+        "md_rdf_histogram": (C.c_int, [_vp, _d]),
+        "md_rdf_g": (C.c_int, [_vp, _d]),
+        "md_rdf_bin_centres": (C.c_int, [_vp, _d]),
+        "md_rdf_frames": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+        "md_msd_create": (C.c_int, [_vp, C.c_int64, C.c_int64, C.POINTER(_vp)]),
+        "md_msd_destroy": (C.c_int, [_vp]),
+        "md_msd_push": (C.c_int, [_vp, _vp]),
+        "md_msd_values": (C.c_int, [_vp, _d]),
+        "md_msd_diffusion": (C.c_int, [_vp, C.c_double, C.c_int64, C.c_int64, _d]),
+        "md_vacf_create": (C.c_int, [_vp, C.c_int64, C.c_int64, C.POINTER(_vp)]),
+        "md_vacf_destroy": (C.c_int, [_vp]),
+        "md_vacf_push": (C.c_int, [_vp, _vp]),
+        "md_vacf_values": (C.c_int, [_vp, C.c_int, _d]),
+        "md_vacf_diffusion": (C.c_int, [_vp, C.c_double, _d]),
         "md_verlet_halo_tiles": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "md_verlet_set_halo": (C.c_int, [_vp, C.c_int]),
         "md_integrator_create_vv": (C.c_int, [C.c_double, C.POINTER(_vp)]),
@@ -870,6 +887,96 @@ class ConstrainedNoseHooverChain(ConstrainedVelocityVerlet):
 
 
 # ---------------------------------------------------------------- adjoint
+# ---------------------------------------------------------------- analysis
+class Rdf:
+    """analyze/rdf.hpp:16-34: g(r) accumulated over frames, on the device."""
+
+    def __init__(self, r_max, bins, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.bins = int(bins)
+        h = _vp()
+        _check(lib().md_rdf_create(self.ctx.handle, float(r_max), self.bins, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.md_rdf_destroy(self._h)
+            self._h = None
+
+    def accumulate(self, sys: System):
+        _check(lib().md_rdf_accumulate(self._h, sys.handle))
+
+    def _vec(self, fn):
+        out = np.zeros(self.bins)
+        _check(fn(self._h, _ptr(out)))
+        return out
+
+    def histogram(self):
+        """Pair counts per bin (i < j), summed over the frames."""
+        return self._vec(lib().md_rdf_histogram)
+
+    def g(self):
+        return self._vec(lib().md_rdf_g)
+
+    def bin_centres(self):
+        return self._vec(lib().md_rdf_bin_centres)
+
+    def frames(self) -> int:
+        f = C.c_int64()
+        _check(lib().md_rdf_frames(self._h, C.byref(f)))
+        return f.value
+
+
+class _Corr:
+    _pre = ""
+
+    def __init__(self, natoms, max_lag, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.max_lag = int(max_lag)
+        h = _vp()
+        _check(getattr(lib(), f"md_{self._pre}_create")(self.ctx.handle, int(natoms), self.max_lag,
+                                                        C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            getattr(_lib, f"md_{self._pre}_destroy")(self._h)
+            self._h = None
+
+    def push(self, sys: System):
+        _check(getattr(lib(), f"md_{self._pre}_push")(self._h, sys.handle))
+
+
+class Msd(_Corr):
+    """analyze/msd.hpp:19-42: mean-squared displacement over all time origins."""
+    _pre = "msd"
+
+    def msd(self):
+        out = np.zeros(self.max_lag + 1)
+        _check(lib().md_msd_values(self._h, _ptr(out)))
+        return out
+
+    def diffusion_coefficient(self, dt, fit_from, fit_to):
+        d = np.zeros(1)
+        _check(lib().md_msd_diffusion(self._h, float(dt), int(fit_from), int(fit_to), _ptr(d)))
+        return float(d[0])
+
+
+class Vacf(_Corr):
+    """analyze/vacf.hpp:151-174: velocity autocorrelation over all time origins."""
+    _pre = "vacf"
+
+    def vacf(self, normalised=True):
+        out = np.zeros(self.max_lag + 1)
+        _check(lib().md_vacf_values(self._h, 1 if normalised else 0, _ptr(out)))
+        return out
+
+    def diffusion_coefficient(self, dt):
+        d = np.zeros(1)
+        _check(lib().md_vacf_diffusion(self._h, float(dt), _ptr(d)))
+        return float(d[0])
+
+
 class AdjointTrajectory:
     """A differentiable FP64 velocity-Verlet LJ trajectory with a hand-written
     adjoint (no reference counterpart).  forward() saves the state every `every`

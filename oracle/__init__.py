@@ -160,6 +160,11 @@ def lib():
         L.orc_nhc_chain.argtypes = [C.POINTER(OrcNhc), C.c_int64, _d, _d, _d, _d, C.c_double]
         L.orc_nhc_conserved.restype = C.c_double
         L.orc_nhc_conserved.argtypes = [C.POINTER(OrcNhc)]
+        L.orc_rdf_accumulate.restype = C.c_int
+        L.orc_rdf_accumulate.argtypes = [C.c_int64, _d, _d, _d, _d, C.c_double, C.c_int64, _d]
+        L.orc_rdf_g.argtypes = [_d, C.c_int64, C.c_double, C.c_int64, C.c_int64, C.c_double, _d]
+        L.orc_msd.argtypes = [C.c_int64, C.c_int64, _d, _d, C.c_int64, _d]
+        L.orc_vacf.argtypes = [C.c_int64, C.c_int64, _d, C.c_int64, _d]
         _lib = L
     return _lib
 
@@ -208,6 +213,11 @@ def ref():
         R.ref_spce_cvv.restype = C.c_double
         R.ref_spce_cvv.argtypes = ([C.c_int64, _d] + [_d] * 9 + [_d, _d, _i64] +
                                    [C.c_double, C.c_int, C.c_double, C.c_int64])
+        R.ref_rdf.restype = C.c_int
+        R.ref_rdf.argtypes = [C.c_int64, C.c_int64, _d, _d, C.c_double, C.c_int64, _d, _d]
+        R.ref_msd.argtypes = [C.c_int64, C.c_int64, _d, _d, C.c_int64, _d, C.c_double, C.c_int64,
+                              C.c_int64, _d]
+        R.ref_vacf.argtypes = [C.c_int64, C.c_int64, _d, _d, C.c_int64, _d, C.c_double, _d]
         _ref = R
     return _ref
 
@@ -476,3 +486,68 @@ def read_nist_config(path):
         pos.append([float(f[1]), float(f[2]), float(f[3])])
         types.append(f[4] if len(f) > 4 else "")
     return box, np.array(pos), types
+
+
+# ---------------------------------------------------------------------------
+# analyze/: RDF, MSD, VACF (restatement, and the reference itself)
+# ---------------------------------------------------------------------------
+
+def _frames_soa(frames):
+    """(F, N, 3) -> contiguous F x (x[N] | y[N] | z[N])."""
+    a = np.asarray(frames, dtype=np.float64)
+    return np.ascontiguousarray(np.transpose(a, (0, 2, 1)))
+
+
+def rdf(frames, box, rmax, bins):
+    """rdf.cpp:55-107 over (F, N, 3) wrapped positions: (histogram, g)."""
+    a = np.asarray(frames, dtype=np.float64)
+    box = _f64(box)
+    hist = np.zeros(bins)
+    sum_rho = 0.0
+    for f in a:
+        x, y, z = (np.ascontiguousarray(f[:, d]) for d in range(3))
+        if lib().orc_rdf_accumulate(len(f), _p(box), _p(x), _p(y), _p(z), rmax, bins,
+                                    _p(hist)) != 0:
+            raise ValueError("Rdf: rMax exceeds half the smallest box length")
+        sum_rho += len(f) / (box[0] * box[1] * box[2])
+    g = np.zeros(bins)
+    lib().orc_rdf_g(_p(hist), bins, rmax, len(a), a.shape[1], sum_rho, _p(g))
+    return hist, g
+
+
+def msd(frames, box, max_lag):
+    a = _frames_soa(frames)
+    out = np.zeros(max_lag + 1)
+    lib().orc_msd(a.shape[0], a.shape[2], _p(_f64(box)), _p(a), max_lag, _p(out))
+    return out
+
+
+def vacf_unnormalised(frames, max_lag):
+    a = _frames_soa(frames)
+    out = np.zeros(max_lag + 1)
+    lib().orc_vacf(a.shape[0], a.shape[2], _p(a), max_lag, _p(out))
+    return out
+
+
+def ref_rdf(frames, box, rmax, bins):
+    a = _frames_soa(frames)
+    g, c = np.zeros(bins), np.zeros(bins)
+    rc = ref().ref_rdf(a.shape[0], a.shape[2], _p(_f64(box)), _p(a), rmax, bins, _p(g), _p(c))
+    if rc != 0:
+        raise ValueError("Rdf: rMax exceeds half the smallest box length")
+    return g, c
+
+
+def ref_msd(frames, box, max_lag, dt, fit_from, fit_to):
+    a = _frames_soa(frames)
+    out, d = np.zeros(max_lag + 1), np.zeros(1)
+    ref().ref_msd(a.shape[0], a.shape[2], _p(_f64(box)), _p(a), max_lag, _p(out), dt, fit_from,
+                  fit_to, _p(d))
+    return out, d[0]
+
+
+def ref_vacf(frames, box, max_lag, dt):
+    a = _frames_soa(frames)
+    out, d = np.zeros(max_lag + 1), np.zeros(1)
+    ref().ref_vacf(a.shape[0], a.shape[2], _p(_f64(box)), _p(a), max_lag, _p(out), dt, _p(d))
+    return out, d[0]

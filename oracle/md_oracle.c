@@ -1032,3 +1032,104 @@ int orc_rigid_water_velocities(const orc_rigid_water* rw, int64_t n, const doubl
     }
     return -1;
 }
+
+/* ---- analyze/ ------------------------------------------------------------ */
+/* analyze/rdf.cpp:55-82 */
+int orc_rdf_accumulate(int64_t n, const double box[3], const double* x, const double* y,
+                       const double* z, double rmax, int64_t bins, double* hist) {
+    double smallest = box[0];
+    if (box[1] < smallest) smallest = box[1];
+    if (box[2] < smallest) smallest = box[2];
+    if (rmax > 0.5 * smallest) return -1;
+    const double width = rmax / (double)bins; /* rdf.cpp:53 */
+    for (int64_t i = 0; i < n; ++i) {
+        for (int64_t j = i + 1; j < n; ++j) {
+            const double dx = orc_fold(x[i] - x[j], box[0]);
+            const double dy = orc_fold(y[i] - y[j], box[1]);
+            const double dz = orc_fold(z[i] - z[j], box[2]);
+            const double r = sqrt(norm2(dx, dy, dz));
+            if (r < rmax) {
+                const uint64_t bin = (uint64_t)(r / width);
+                if (bin < (uint64_t)bins) hist[bin] += 1.0;
+            }
+        }
+    }
+    return 0;
+}
+
+/* analyze/rdf.cpp:92-107 */
+void orc_rdf_g(const double* hist, int64_t bins, double rmax, int64_t frames, int64_t natoms,
+               double sum_rho, double* g) {
+    const double pi = 3.14159265358979323846;
+    const double width = rmax / (double)bins;
+    for (int64_t k = 0; k < bins; ++k) g[k] = 0.0;
+    if (frames == 0) return;
+    const double rho = sum_rho / (double)frames;
+    for (int64_t k = 0; k < bins; ++k) {
+        const double lo = (double)k * width;
+        const double hi = (double)(k + 1) * width;
+        const double shell = (4.0 / 3.0) * pi * (hi * hi * hi - lo * lo * lo);
+        const double denom = (double)frames * 0.5 * (double)natoms * rho * shell;
+        g[k] = denom > 0.0 ? hist[k] / denom : 0.0;
+    }
+}
+
+/* Shared ring-buffer loop of analyze/msd.cpp:66-106 (DIFF = 1) and
+ * analyze/vacf.cpp:195-226 (DIFF = 0). */
+static void orc_corr(int64_t frames, int64_t n, const double* a, int64_t max_lag, int diff,
+                     double* out) {
+    const int64_t period = max_lag + 1;
+    double* sum = (double*)calloc((size_t)period, sizeof(double));
+    int64_t* count = (int64_t*)calloc((size_t)period, sizeof(int64_t));
+    for (int64_t f = 0; f < frames; ++f) {
+        const int64_t avail = f < max_lag ? f : max_lag;
+        const double* cur = a + f * 3 * n;
+        for (int64_t lag = 0; lag <= avail; ++lag) {
+            const double* org = a + (f - lag) * 3 * n;
+            double s = 0.0;
+            for (int64_t i = 0; i < n; ++i) {
+                if (diff) {
+                    s += norm2(cur[i] - org[i], cur[n + i] - org[n + i],
+                               cur[2 * n + i] - org[2 * n + i]);
+                } else {
+                    s += cur[i] * org[i] + cur[n + i] * org[n + i] + cur[2 * n + i] * org[2 * n + i];
+                }
+            }
+            sum[lag] += s;
+            count[lag] += n;
+        }
+    }
+    for (int64_t lag = 0; lag < period; ++lag)
+        out[lag] = count[lag] > 0 ? sum[lag] / (double)count[lag] : 0.0;
+    free(sum);
+    free(count);
+}
+
+/* analyze/msd.cpp:66-96: incremental unwrapping by the minimum image of each step,
+ * then the ring loop over unwrapped positions. */
+void orc_msd(int64_t frames, int64_t n, const double box[3], const double* pos,
+             int64_t max_lag, double* out) {
+    double* unw = (double*)malloc(sizeof(double) * (size_t)(frames * 3 * n + 1));
+    for (int64_t f = 0; f < frames; ++f) {
+        const double* p = pos + f * 3 * n;
+        double* u = unw + f * 3 * n;
+        for (int64_t i = 0; i < n; ++i) {
+            for (int d = 0; d < 3; ++d) {
+                if (f == 0) {
+                    u[d * n + i] = p[d * n + i];
+                } else {
+                    const double* q = pos + (f - 1) * 3 * n;
+                    const double step = orc_fold(p[d * n + i] - q[d * n + i], box[d]);
+                    u[d * n + i] = unw[(f - 1) * 3 * n + d * n + i] + step;
+                }
+            }
+        }
+    }
+    orc_corr(frames, n, unw, max_lag, 1, out);
+    free(unw);
+}
+
+/* analyze/vacf.cpp:195-226 */
+void orc_vacf(int64_t frames, int64_t n, const double* vel, int64_t max_lag, double* out) {
+    orc_corr(frames, n, vel, max_lag, 0, out);
+}

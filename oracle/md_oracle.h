@@ -204,6 +204,23 @@ int orc_rigid_water_velocities(const orc_rigid_water* rw, int64_t n, const doubl
                                const double* mass, const double* x, const double* y,
                                const double* z, double* vx, double* vy, double* vz);
 
+/* ---- analyze/ ------------------------------------------------------------ */
+/* rdf.cpp:55-82: one frame's pairs i < j into hist (bins doubles, accumulated).
+ * Returns -1 (std::invalid_argument) when rmax exceeds half the smallest box
+ * length, else 0. */
+int orc_rdf_accumulate(int64_t n, const double box[3], const double* x, const double* y,
+                       const double* z, double rmax, int64_t bins, double* hist);
+/* rdf.cpp:92-107: g(r) from the accumulated histogram. */
+void orc_rdf_g(const double* hist, int64_t bins, double rmax, int64_t frames, int64_t natoms,
+               double sum_rho, double* g);
+/* msd.cpp:66-106 over a whole trajectory: pos holds frames x (x[n] | y[n] | z[n])
+ * wrapped positions in atom order; out receives max_lag + 1 values. */
+void orc_msd(int64_t frames, int64_t n, const double box[3], const double* pos,
+             int64_t max_lag, double* out);
+/* vacf.cpp:195-226: vel as pos above; out receives the max_lag + 1 unnormalised
+ * means. */
+void orc_vacf(int64_t frames, int64_t n, const double* vel, int64_t max_lag, double* out);
+
 #ifdef __cplusplus
 }
 #endif

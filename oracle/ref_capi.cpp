@@ -15,6 +15,9 @@
 #include <utility>
 #include <vector>
 
+#include "moldyn/analyze/msd.hpp"
+#include "moldyn/analyze/rdf.hpp"
+#include "moldyn/analyze/vacf.hpp"
 #include "moldyn/constrain/rigid_water.hpp"
 #include "moldyn/core/box.hpp"
 #include "moldyn/core/system.hpp"
@@ -303,6 +306,61 @@ double ref_spce_cvv(int64_t n, const double* box, double* x, double* y, double* 
     for (int64_t k = 0; k < steps; ++k) integ.step(sys, forces);
     dumpState(sys, x, y, z, vx, vy, vz, fx, fy, fz);
     return pe;
+}
+
+// Rdf over `frames` frames (pos: frames x (x[n] | y[n] | z[n])): g and the bin
+// centres (bins each).  Returns 0, or -2 for std::invalid_argument.
+int ref_rdf(int64_t frames, int64_t n, const double* box, const double* pos, double rmax,
+            int64_t bins, double* g, double* centres) {
+    try {
+        Rdf rdf(rmax, static_cast<std::size_t>(bins));
+        for (int64_t f = 0; f < frames; ++f) {
+            const double* p = pos + f * 3 * n;
+            const System sys = makeSystem(n, box, p, p + n, p + 2 * n, nullptr, nullptr, nullptr,
+                                          nullptr, nullptr, nullptr);
+            rdf.accumulate(sys);
+        }
+        const std::vector<double> gv = rdf.g(), cv = rdf.binCentres();
+        for (int64_t k = 0; k < bins; ++k) {
+            g[k] = gv[k];
+            centres[k] = cv[k];
+        }
+        return 0;
+    } catch (const std::invalid_argument&) {
+        return -2;
+    }
+}
+
+// Msd over a trajectory of wrapped positions (as ref_rdf): max_lag + 1 values and
+// the Einstein diffusion coefficient over [fit_from, fit_to).
+void ref_msd(int64_t frames, int64_t n, const double* box, const double* pos, int64_t max_lag,
+             double* out, double dt, int64_t fit_from, int64_t fit_to, double* d) {
+    Msd msd(static_cast<std::size_t>(n), static_cast<std::size_t>(max_lag));
+    for (int64_t f = 0; f < frames; ++f) {
+        const double* p = pos + f * 3 * n;
+        msd.push(makeSystem(n, box, p, p + n, p + 2 * n, nullptr, nullptr, nullptr, nullptr,
+                            nullptr, nullptr));
+    }
+    const std::vector<double> m = msd.msd();
+    for (int64_t k = 0; k <= max_lag; ++k) out[k] = m[k];
+    *d = msd.diffusionCoefficient(dt, static_cast<std::size_t>(fit_from),
+                                  static_cast<std::size_t>(fit_to));
+}
+
+// Vacf over a trajectory of velocities: the normalised values and the Green-Kubo
+// diffusion coefficient.
+void ref_vacf(int64_t frames, int64_t n, const double* box, const double* vel, int64_t max_lag,
+              double* out, double dt, double* d) {
+    Vacf vacf(static_cast<std::size_t>(n), static_cast<std::size_t>(max_lag));
+    std::vector<double> zero(static_cast<std::size_t>(n), 0.0);
+    for (int64_t f = 0; f < frames; ++f) {
+        const double* v = vel + f * 3 * n;
+        vacf.push(makeSystem(n, box, zero.data(), zero.data(), zero.data(), v, v + n, v + 2 * n,
+                             nullptr, nullptr, nullptr));
+    }
+    const std::vector<double> c = vacf.vacf();
+    for (int64_t k = 0; k <= max_lag; ++k) out[k] = c[k];
+    *d = vacf.diffusionCoefficient(dt);
 }
 
 }  // extern "C"

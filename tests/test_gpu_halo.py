@@ -113,3 +113,62 @@ def test_tile_policy(md):
     assert tiles == 16 and staged == tiles
     v.set_halo(False)
     assert v.halo_tiles() == (0, 0)
+
+
+def test_list_with_tiles_serves_other_consumers(md):
+    """A list that keeps halo tiles (rebuilt inside a fused run and by host builds)
+    still exports the reference's pair set and serves an FP64 force call exactly."""
+    s, v, st = melt(md, 10, 0.8442, 8, steps=20)  # 4000 atoms
+    lj = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+    v.set_halo(True)
+    lj.compute_forces(s, v)
+    md.VelocityVerlet(0.005).run(s, v, lj, 200)
+    assert v.rebuild_count() > 3 and v.halo_tiles()[0] > 0
+    v.build(s)  # a host build with tiles on
+    fresh = md.VerletList(st["box"], 2.5, 0.3)
+    fresh.build(s)
+    assert np.array_equal(v.pairs(), fresh.pairs())
+    v.build(s)
+    lj64 = md.LennardJones(1.0, 1.0, 2.5)
+    e1, w1 = lj64.compute_forces(s, v)
+    f1 = s.forces
+    e2, w2 = lj64.compute_forces(s, fresh)
+    f2 = s.forces
+    assert e1 == e2 and w1 == w2 and np.array_equal(f1, f2)
+
+
+def test_fused_run_over_staged_and_gathered_tiles(md):
+    """A dense slab beside a dilute gas: rebuilds inside the fused run write slot
+    rows, int32 rows, or both (cells touching both kinds of tile); the trajectory
+    equals the one without tiles."""
+    st = md.fcc_lattice(12, 0.8442, 0.722, 9)
+    box = st["box"].copy()
+    box[2] *= 3.0
+    rng = np.random.default_rng(9)
+    gas = rng.uniform(-0.5, 0.5, size=(300, 3)) * box
+    gas[:, 2] = np.where(gas[:, 2] > 0, gas[:, 2] * 0.5 + box[2] / 4, gas[:, 2] * 0.5 - box[2] / 4)
+    keep = []  # no two gas atoms closer than 1.0 (minimum image)
+    for k in range(len(gas)):
+        d = gas[keep] - gas[k]
+        d -= box * np.round(d / box)
+        if not keep or np.min(np.sum(d * d, axis=1)) > 1.0:
+            keep.append(k)
+    gas = gas[keep]
+    pos = np.concatenate([st["pos"], gas])
+    vel = np.concatenate([st["vel"], rng.normal(0.0, 0.8, size=gas.shape)])
+    out = []
+    for halo in (False, True):
+        s = md.System.from_arrays(pos, box, vel=vel, mass=np.ones(len(pos)))
+        lj = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+        lj.set_halo(halo)
+        v = md.VerletList(box, 2.5, 0.3)
+        v.build(s)
+        v.set_halo(halo)
+        lj.compute_forces(s, v)
+        th = md.VelocityVerlet(0.002).run(s, v, lj, 150, thermo=True)
+        staged, tiles = v.halo_tiles()
+        if halo:
+            assert v.rebuild_count() >= 1 and 0 < staged < tiles
+        out.append((s.positions, th, v.pairs()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])

@@ -275,3 +275,48 @@ def test_rng_matches_reference():
     b = np.zeros(5001)
     R.ref_rng_normals(2026, O._p(b), 5001)
     assert np.array_equal(a, b)
+
+
+# ------------------------------------------------------------------ analyze/
+def random_walk(n, frames, box, step, seed):
+    """Seeded wrapped positions and velocities, (frames, n, 3) each; steps of
+    `step` per frame cross the periodic boundaries often."""
+    rng = np.random.default_rng(seed)
+    box = np.asarray(box, dtype=float)
+    p = (rng.random((n, 3)) - 0.5) * box
+    pos, vel = [], []
+    for _ in range(frames):
+        v = rng.normal(0.0, 1.0, (n, 3))
+        p = p + step * v
+        p = p - box * np.floor(p / box + 0.5)
+        pos.append(p.copy())
+        vel.append(v)
+    return np.array(pos), np.array(vel)
+
+
+def test_rdf_restatement_matches_reference():
+    need_ref()
+    box = np.array([7.0, 7.5, 8.0])
+    pos, _ = random_walk(200, 4, box, 0.3, 11)
+    hist, g = O.rdf(pos, box, 3.4, 40)
+    g_ref, centres = O.ref_rdf(pos, box, 3.4, 40)
+    assert np.array_equal(g, g_ref)
+    assert np.array_equal(centres, (np.arange(40) + 0.5) * (3.4 / 40))
+    assert hist.sum() > 0 and np.all(hist == np.round(hist))
+    with pytest.raises(ValueError):
+        O.ref_rdf(pos, box, 3.6, 40)  # rMax > L/2
+    with pytest.raises(ValueError):
+        O.rdf(pos, box, 3.6, 40)
+
+
+def test_msd_vacf_restatement_matches_reference():
+    need_ref()
+    box = np.array([5.0, 5.0, 6.0])
+    pos, vel = random_walk(64, 30, box, 0.8, 12)
+    m = O.msd(pos, box, 10)
+    m_ref, _ = O.ref_msd(pos, box, 10, 0.01, 1, 10)
+    assert np.array_equal(m, m_ref)
+    u = O.vacf_unnormalised(vel, 10)
+    c_ref, _ = O.ref_vacf(vel, box, 10, 0.01)
+    assert np.array_equal(u / u[0], c_ref)
+    assert m[0] == 0.0 and np.all(m[1:] > 0)
