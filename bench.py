@@ -827,9 +827,141 @@ def run_water_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ analysis
+ANALYSIS_METRIC = "RDF frames/s, 1M-atom LJ liquid (rMax 4.0, 200 bins) on 1 B200"
+RDF_RMAX, RDF_BINS, CORR_LAGS = 4.0, 200, 100
+
+
+def analysis_config(steps):
+    return {"workload": "radial distribution function of the equilibrated 1M-atom LJ liquid "
+                        f"(fcc 64^3, rho*=0.8442): rMax {RDF_RMAX}, {RDF_BINS} bins, every pair "
+                        "i<j counted (analyze/rdf.cpp); MSD and VACF pushes with "
+                        f"{CORR_LAGS + 1} lags (analyze/msd.cpp, vacf.cpp)",
+            "frames": steps, "n_atoms": 4 * CELLS ** 3,
+            "l2_policy": "no flush: positions 32 MB, MSD/VACF rings 2.5 GB each > 126 MB L2",
+            "parallelism": "replicas (one independent system per GPU)"}
+
+
+def reference_rdf_rate(cells=20, frames=1):
+    """The reference's Rdf (brute force, all pairs) on one seeded frame of a
+    cells^3 fcc liquid, 1 thread: pair evaluations per second."""
+    import oracle as O
+    st = O.fcc_lattice(cells, RHO, TEMP, SEED)
+    n = len(st["pos"])
+    t0 = time.perf_counter()
+    O.ref_rdf(st["pos"][None], st["box"], RDF_RMAX, RDF_BINS)
+    sec = time.perf_counter() - t0
+    return frames * n * (n - 1) / 2 / sec, n, sec
+
+
+def run_analysis_arm(args):
+    world, rank, local = dist_env()
+    group = Group(world)
+    n = 4 * CELLS ** 3
+    pairs_1m = n * (n - 1) / 2
+    cpu = None
+    if args.impl == "reference" or (rank == 0 and world == 1 and not args.no_cpu):
+        rate, n_s, sec = reference_rdf_rate()
+        cpu = {"value": rate / pairs_1m, "unit": "frames/s", "cores": 1, "kind": "reference",
+               "sample": f"the reference's Rdf::accumulate on one {n_s}-atom frame of the same "
+                         f"liquid ({sec:.2f} s, {rate:.3g} pair evaluations/s), projected to the "
+                         f"{n}-atom frame's {pairs_1m:.3g} pairs; 1 thread ({cpu_model()})"}
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({
+                    "metric": ANALYSIS_METRIC, "value": cpu["value"], "unit": "frames/s",
+                    "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                    "ms_per_step": 1e3 / cpu["value"], "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic: seeded fcc lattice", "config": analysis_config(1),
+                    "impl": "reference", "cpu_baseline": cpu,
+                    "e2e": {"value": cpu["value"], "unit": "frames/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}), flush=True)
+            group.close()
+            return 0
+    import moleculardynamics_b200 as md
+    ctx = md.Context(local)
+    box, pos, vel, frc = equilibrated_state(md, ctx, args.equil)
+    s = md.System.from_arrays(pos, box, vel=vel, ctx=ctx)
+    L = md.lib()
+    rdf = md.Rdf(RDF_RMAX, RDF_BINS, ctx=ctx)
+    for _ in range(args.warmup):
+        rdf.accumulate(s)
+    ctx.synchronize()
+    group.barrier()
+    launches0 = ctx.launch_count()
+    clocks = ClockSampler(local)
+    clocks.__enter__()
+    ms = C.c_double()
+    md._check(L.md_context_span_begin(ctx.handle))
+    for _ in range(args.steps):
+        rdf.accumulate(s)
+    md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+    clocks.__exit__(None, None, None)
+    launches = ctx.launch_count() - launches0
+    dev_ms = group.reduce(ms.value, "max")
+    value = world * args.steps / (dev_ms * 1e-3)
+    # MSD / VACF pushes with every lag available
+    msd, vacf = md.Msd(n, CORR_LAGS, ctx=ctx), md.Vacf(n, CORR_LAGS, ctx=ctx)
+    for _ in range(CORR_LAGS + 1):
+        msd.push(s)
+        vacf.push(s)
+    t = {}
+    for name, obj in (("msd", msd), ("vacf", vacf)):
+        md._check(L.md_context_span_begin(ctx.handle))
+        for _ in range(10):
+            obj.push(s)
+        md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+        t[name] = ms.value / 10
+    # end to end through the public C ABI: positions from pinned host memory each
+    # frame, the frame accumulated, g(r) read back
+    hpos = [np.ascontiguousarray(pos[:, d]) for d in range(3)]
+    g = np.zeros(RDF_BINS)
+    e2e_frames = max(3, min(args.steps, 10))
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_frames):
+        for d, f in enumerate((md.FIELD_X, md.FIELD_X + 1, md.FIELD_X + 2)):
+            md._check(L.md_system_set(s.handle, f, hpos[d].ctypes.data_as(C.POINTER(C.c_double))))
+        md._check(L.md_rdf_accumulate(rdf._h, s.handle))
+        md._check(L.md_rdf_g(rdf._h, g.ctypes.data_as(C.POINTER(C.c_double))))
+    e2e_sec = group.reduce(time.perf_counter() - t0, "max")
+    if rank == 0:
+        peaks, peak_src = measured_peaks()
+        # algorithmic bytes of a frame: every atom's position read once (32 B)
+        achieved = 32.0 * n / (dev_ms / args.steps * 1e-3) / 1e9
+        line = {
+            "metric": ANALYSIS_METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities, "
+                    f"{args.equil} BAOAB equilibration steps",
+            "config": analysis_config(args.steps), "gpu_launches": int(launches),
+            "pairs_within_rmax_per_frame": float(rdf.histogram().sum() / rdf.frames()),
+            "msd_push_ms": t["msd"], "vacf_push_ms": t["vacf"],
+            "e2e": {"value": world * e2e_frames / e2e_sec, "unit": "frames/s",
+                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 8 * RDF_BINS,
+                    "path": "md_system_set x3 (host positions) + md_rdf_accumulate + md_rdf_g "
+                            "per frame"},
+            "roofline": {"bound": "hbm", "kernel": "k_rdf_cells", "achieved": achieved,
+                         "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": achieved / peaks.get("hbm_gbs", 6650.0),
+                         "peak_source": f"hbm_gbs of {peak_src}",
+                         "algorithmic_bytes_per_atom": 32.0, "traffic": None,
+                         "note": "FP64 pair arithmetic (exact fold, sqrt, divide) bounds it"},
+            "clocks": clocks.summary(),
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    group.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--workload", default="lj1m", choices=["lj1m", "batch", "adjoint", "water"],
+    ap.add_argument("--workload", default="lj1m",
+                    choices=["lj1m", "batch", "adjoint", "water", "analysis"],
                     help="lj1m: the headline 1M-atom run; batch: 48 NHC replicas; adjoint: "
                          "forward + backward of a 32,000-atom differentiable trajectory "
                          "(--steps is its length)")
@@ -859,6 +991,8 @@ def main():
         return run_adjoint_arm(args)
     if args.workload == "water":
         return run_water_arm(args)
+    if args.workload == "analysis":
+        return run_analysis_arm(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

@@ -627,4 +627,88 @@ inline System fccLattice(int cells, double density, double temperature, uint64_t
     return sys;
 }
 
+// analyze/rdf.hpp:16-34 on the device (md_rdf_*).
+class Rdf {
+public:
+    Rdf(double rMax, std::size_t bins, md_context* ctx = nullptr) : bins_(bins) {
+        detail::check(md_rdf_create(ctx ? ctx : detail::context(), rMax,
+                                    static_cast<int64_t>(bins), &h_));
+    }
+    Rdf(const Rdf&) = delete;
+    Rdf& operator=(const Rdf&) = delete;
+    ~Rdf() { md_rdf_destroy(h_); }
+    void accumulate(const System& sys) { detail::check(md_rdf_accumulate(h_, sys.device())); }
+    std::vector<double> binCentres() const { return vec(md_rdf_bin_centres); }
+    std::vector<double> g() const { return vec(md_rdf_g); }
+    std::size_t frames() const {
+        int64_t f = 0;
+        detail::check(md_rdf_frames(h_, &f));
+        return static_cast<std::size_t>(f);
+    }
+
+private:
+    std::vector<double> vec(int (*fn)(const md_rdf*, double*)) const {
+        std::vector<double> out(bins_);
+        detail::check(fn(h_, out.data()));
+        return out;
+    }
+    std::size_t bins_;
+    md_rdf* h_ = nullptr;
+};
+
+// analyze/msd.hpp:19-42 on the device (md_msd_*).
+class Msd {
+public:
+    Msd(std::size_t natoms, std::size_t maxLag, md_context* ctx = nullptr) : lags_(maxLag + 1) {
+        detail::check(md_msd_create(ctx ? ctx : detail::context(), static_cast<int64_t>(natoms),
+                                    static_cast<int64_t>(maxLag), &h_));
+    }
+    Msd(const Msd&) = delete;
+    Msd& operator=(const Msd&) = delete;
+    ~Msd() { md_msd_destroy(h_); }
+    void push(const System& sys) { detail::check(md_msd_push(h_, sys.device())); }
+    std::vector<double> msd() const {
+        std::vector<double> out(lags_);
+        detail::check(md_msd_values(h_, out.data()));
+        return out;
+    }
+    double diffusionCoefficient(double dt, std::size_t fitFrom, std::size_t fitTo) const {
+        double d = 0.0;
+        detail::check(md_msd_diffusion(h_, dt, static_cast<int64_t>(fitFrom),
+                                       static_cast<int64_t>(fitTo), &d));
+        return d;
+    }
+
+private:
+    std::size_t lags_;
+    md_msd* h_ = nullptr;
+};
+
+// analyze/vacf.hpp:151-174 on the device (md_vacf_*).
+class Vacf {
+public:
+    Vacf(std::size_t natoms, std::size_t maxLag, md_context* ctx = nullptr) : lags_(maxLag + 1) {
+        detail::check(md_vacf_create(ctx ? ctx : detail::context(), static_cast<int64_t>(natoms),
+                                     static_cast<int64_t>(maxLag), &h_));
+    }
+    Vacf(const Vacf&) = delete;
+    Vacf& operator=(const Vacf&) = delete;
+    ~Vacf() { md_vacf_destroy(h_); }
+    void push(const System& sys) { detail::check(md_vacf_push(h_, sys.device())); }
+    std::vector<double> vacf() const {
+        std::vector<double> out(lags_);
+        detail::check(md_vacf_values(h_, 1, out.data()));
+        return out;
+    }
+    double diffusionCoefficient(double dt) const {
+        double d = 0.0;
+        detail::check(md_vacf_diffusion(h_, dt, &d));
+        return d;
+    }
+
+private:
+    std::size_t lags_;
+    md_vacf* h_ = nullptr;
+};
+
 }  // namespace moldyn_b200
