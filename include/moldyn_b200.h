@@ -85,6 +85,7 @@ typedef struct md_adjoint md_adjoint;
 typedef struct md_rdf md_rdf;
 typedef struct md_msd md_msd;
 typedef struct md_vacf md_vacf;
+typedef struct md_thermo_csv md_thermo_csv;
 
 /* ------------------------------------------------------------------ library */
 /* Message of the last failing call on this thread ("" if none). */
@@ -458,6 +459,41 @@ MD_API int md_vacf_destroy(md_vacf* vacf);
 MD_API int md_vacf_push(md_vacf* vacf, md_system* sys);
 MD_API int md_vacf_values(const md_vacf* vacf, int normalised, double* out);
 MD_API int md_vacf_diffusion(const md_vacf* vacf, double dt, double* d);
+
+/* ----------------------------------------------------------------- formats */
+/* moldyn_run's thermo CSV (apps/moldyn_run.cpp:229-245, 600-617): opens path and
+ * writes the header -- "# command", "# git_sha" and "# host" carry the caller's
+ * strings (revision/host NULL: "unknown"), the units, truncation and
+ * temperature_dof lines -- and the column names.  md_thermo_csv_append writes one
+ * row per thermo row of md_run_lj (4 doubles: pair energy, virial, kinetic
+ * energy, conserved), as StepSampler::record (moldyn_run.cpp:497-511): step =
+ * first_step + k * step_stride, time = step * dt, potential energy with the tail
+ * correction, temperature 2 KE / dof, pressure rho T + W / (3V) + P_LRC, numbers
+ * at std::setprecision(10).  MD_ERR_RUNTIME when the file cannot be written. */
+MD_API int md_thermo_csv_open(const char* path, const char* command_line, const char* revision,
+                              const char* host, int truncation, int64_t dof_langevin,
+                              int64_t dof_nve, md_thermo_csv** out);
+MD_API int md_thermo_csv_append(md_thermo_csv* csv, const md_lj* lj, int64_t n,
+                                const double box[3], int64_t first_step, int64_t step_stride,
+                                double dt, const char* phase, int64_t dof, const double* rows,
+                                int64_t count);
+MD_API int md_thermo_csv_close(md_thermo_csv* csv);
+/* One XYZ trajectory frame appended to path (moldyn_run.cpp:519-533): the atom
+ * count, the "step= time= phase= git_sha= host= command=" comment line and one
+ * "Ar x y z" line per atom in original order, default stream precision. */
+MD_API int md_xyz_append(const char* path, md_system* sys, int64_t step, double time,
+                         const char* phase, const char* revision, const char* host,
+                         const char* command_line);
+/* Restartable binary checkpoint (no reference counterpart): every per-atom field
+ * in original order, molecule ids, the box, and -- when integ is given -- the
+ * integrator's parameters, step counter (BAOAB's noise stream) and chain state,
+ * with a checksum.  md_checkpoint_load creates the system on ctx and, when integ
+ * is given, restores it into an integrator of the same kind (MD_ERR_INVALID_ARGUMENT
+ * for another kind, a damaged or foreign file).  A run continued from the loaded
+ * state after a fresh Verlet build equals the saved run continued after one. */
+MD_API int md_checkpoint_save(md_system* sys, const md_integrator* integ, const char* path);
+MD_API int md_checkpoint_load(md_context* ctx, const char* path, md_system** sys,
+                              md_integrator* integ);
 
 #ifdef __cplusplus
 }

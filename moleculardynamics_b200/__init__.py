@@ -132,6 +132,15 @@ def _load():
         "md_lj_set_unroll": (C.c_int, [C.c_int]),
         "md_lj_set_launch": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_lj_set_halo": (C.c_int, [_vp, C.c_int]),
+        "md_thermo_csv_open": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
+                                        C.c_int64, C.c_int64, C.POINTER(_vp)]),
+        "md_thermo_csv_append": (C.c_int, [_vp, _vp, C.c_int64, _d, C.c_int64, C.c_int64,
+                                          C.c_double, C.c_char_p, C.c_int64, _d, C.c_int64]),
+        "md_thermo_csv_close": (C.c_int, [_vp]),
+        "md_xyz_append": (C.c_int, [C.c_char_p, _vp, C.c_int64, C.c_double, C.c_char_p,
+                                   C.c_char_p, C.c_char_p, C.c_char_p]),
+        "md_checkpoint_save": (C.c_int, [_vp, _vp, C.c_char_p]),
+        "md_checkpoint_load": (C.c_int, [_vp, C.c_char_p, C.POINTER(_vp), _vp]),
         "md_rdf_create": (C.c_int, [_vp, C.c_double, C.c_int64, C.POINTER(_vp)]),
         "md_rdf_destroy": (C.c_int, [_vp]),
         "md_rdf_accumulate": (C.c_int, [_vp, _vp]),
@@ -303,6 +312,18 @@ class System:
         self._h = h
         self.n = int(n)
         self.box = box.copy()
+
+    @classmethod
+    def _adopt(cls, h, ctx):
+        """Wrap a system handle created by the library (checkpoint_load)."""
+        s = cls.__new__(cls)
+        s.ctx = ctx
+        s._h = h
+        s.n = int(lib().md_system_size(h))
+        box = np.zeros(3)
+        _check(lib().md_system_box(h, _ptr(box)))
+        s.box = box
+        return s
 
     @classmethod
     def from_arrays(cls, pos, box, vel=None, mass=None, charge=None, mol=None, ctx=None):
@@ -887,6 +908,61 @@ class ConstrainedNoseHooverChain(ConstrainedVelocityVerlet):
 
 
 # ---------------------------------------------------------------- adjoint
+# ----------------------------------------------------------------- formats
+def _b(x):
+    return None if x is None else str(x).encode()
+
+
+class ThermoCsv:
+    """moldyn_run's thermo CSV (apps/moldyn_run.cpp:229-245, 497-511, 600-617):
+    header on open, one row per thermo row of a fused run on append()."""
+
+    def __init__(self, path, command_line="", revision=None, host=None, truncation=0,
+                 dof_langevin=0, dof_nve=0):
+        h = _vp()
+        _check(lib().md_thermo_csv_open(_b(path), _b(command_line), _b(revision), _b(host),
+                                        int(truncation), int(dof_langevin), int(dof_nve),
+                                        C.byref(h)))
+        self._h = h
+
+    def append(self, lj, n, box, rows, first_step, dt, phase, dof, step_stride=1):
+        rows = _f64(rows).reshape(-1, 4)
+        _check(lib().md_thermo_csv_append(self._h, lj.handle, int(n), _ptr(_f64(box)),
+                                          int(first_step), int(step_stride), float(dt),
+                                          _b(phase), int(dof), _ptr(rows), len(rows)))
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            h, self._h = self._h, None
+            _check(_lib.md_thermo_csv_close(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def xyz_append(path, sys, step, time, phase, command_line="", revision=None, host=None):
+    """One XYZ frame (moldyn_run.cpp:519-533) appended to path."""
+    _check(lib().md_xyz_append(_b(path), sys.handle, int(step), float(time), _b(phase),
+                               _b(revision), _b(host), _b(command_line)))
+
+
+def checkpoint_save(sys, path, integrator=None):
+    _check(lib().md_checkpoint_save(sys.handle, integrator.handle if integrator else None,
+                                    _b(path)))
+
+
+def checkpoint_load(path, integrator=None, ctx=None):
+    """A System restored from a checkpoint (and the integrator's state, when given)."""
+    ctx = ctx or default_context()
+    h = _vp()
+    _check(lib().md_checkpoint_load(ctx.handle, _b(path), C.byref(h),
+                                    integrator.handle if integrator else None))
+    return System._adopt(h, ctx)
+
+
 # ---------------------------------------------------------------- analysis
 class Rdf:
     """analyze/rdf.hpp:16-34: g(r) accumulated over frames, on the device."""
