@@ -779,7 +779,7 @@ def run_water_arm(args):
     rng = np.random.default_rng(SEED)
     s.velocities = np.sqrt(298.0 / m)[:, None] * rng.normal(size=(s.n, 3))
     s.remove_center_of_mass_motion()
-    rw = md.RigidWater(1.0, 109.47)
+    rw = md.RigidWater(1.0, 109.47, settle=args.settle)
     rw.constrain_velocities(s)
     ff = md.SpceForceField(cutoff=WATER_RC, kmax=WATER_KMAX, alpha=WATER_ALPHA, ctx=ctx)
     dof = md.RigidWater.degrees_of_freedom(4096, True)
@@ -813,7 +813,9 @@ def run_water_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded rigid-water lattice, Maxwell-Boltzmann velocities, "
                     f"{args.equil_water} NHC steps of 0.5 fs",
-            "config": water_config(args.steps), "gpu_launches": int(launches),
+            "config": dict(water_config(args.steps),
+                           constraints="SETTLE" if args.settle else "SHAKE/RATTLE"),
+            "gpu_launches": int(launches),
             "nhc_extended_energy_drift_K": {"max_abs": float(np.max(np.abs(h - h[0]))),
                                             "relative": float(np.max(np.abs(h - h[0])) / abs(h[0]))},
             "mean_temperature_K": float(np.mean(2 * th[:, 2] / dof)),
@@ -967,6 +969,8 @@ def main():
                          "(--steps is its length)")
     ap.add_argument("--adj-skin", type=float, default=2.0)
     ap.add_argument("--equil-water", type=int, default=1000)
+    ap.add_argument("--settle", action="store_true",
+                    help="water: SETTLE instead of SHAKE/RATTLE iterations")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)

@@ -276,6 +276,13 @@ MD_API int md_spce_set_lj_truncation(md_ewald* ff, int truncation);
  * MD_ERR_INVALID_ARGUMENT like the reference's std::invalid_argument. */
 MD_API int md_rigid_create(double oh, double hoh_degrees, double tolerance, int max_iterations,
                            md_rigid** out);
+/* Solve the constraints in closed form (on = 1) with SETTLE (Miyamoto &
+ * Kollman 1992) -- the specialisation rigid_water.hpp:20-24 plans -- instead of
+ * SHAKE / RATTLE iterations: the same fixed point, reached without iterating
+ * (positions agree with SHAKE to its tolerance; molecules with unequal hydrogen
+ * masses, or configurations SETTLE cannot solve, still take SHAKE).  Applies to
+ * md_rigid_constrain_* and to integrators created from this object afterwards. */
+MD_API int md_rigid_set_settle(md_rigid* rw, int on);
 MD_API int md_rigid_destroy(md_rigid* rw);
 MD_API int md_rigid_distances(const md_rigid* rw, double* oh, double* hh);
 /* degreesOfFreedom(molecules, comRemoved) (rigid_water.cpp:55-59). */

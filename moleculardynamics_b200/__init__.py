@@ -187,6 +187,7 @@ def _load():
                                      C.POINTER(_vp)]),
         "md_spce_compute": (C.c_int, [_vp, _vp, C.c_int, _d, _d]),
         "md_spce_set_lj_truncation": (C.c_int, [_vp, C.c_int]),
+        "md_rigid_set_settle": (C.c_int, [_vp, C.c_int]),
         "md_rigid_create": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int,
                                       C.POINTER(_vp)]),
         "md_rigid_destroy": (C.c_int, [_vp]),
@@ -818,11 +819,19 @@ class RigidWater:
     """constrain/rigid_water.hpp:29-67: SHAKE/RATTLE on O-H1, O-H2, H1-H2 of each
     consecutive (O, H, H) triple, one GPU thread per molecule."""
 
-    def __init__(self, oh_distance, hoh_angle_degrees, tolerance=1e-12, max_iterations=500):
+    def __init__(self, oh_distance, hoh_angle_degrees, tolerance=1e-12, max_iterations=500,
+                 settle=False):
         h = _vp()
         _check(lib().md_rigid_create(float(oh_distance), float(hoh_angle_degrees),
                                      float(tolerance), int(max_iterations), C.byref(h)))
         self._h = h
+        if settle:
+            self.set_settle(True)
+
+    def set_settle(self, on=True):
+        """Closed-form SETTLE instead of SHAKE / RATTLE iterations (the same fixed
+        point); integrators created afterwards inherit it."""
+        _check(lib().md_rigid_set_settle(self._h, 1 if on else 0))
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

@@ -36,6 +36,8 @@ struct RigidArgs {
     double target2[3];  // squared O-H, O-H, H-H distances
     double tolerance;
     int max_iterations;
+    int settle;         // closed-form SETTLE instead of SHAKE / RATTLE iterations
+    double oh, hh;
 };
 
 RigidArgs rigid_args(const md_rigid& rw) {
@@ -45,6 +47,9 @@ RigidArgs rigid_args(const md_rigid& rw) {
     a.target2[2] = rw.hh * rw.hh;
     a.tolerance = rw.tolerance;
     a.max_iterations = rw.max_iterations;
+    a.settle = rw.settle ? 1 : 0;
+    a.oh = rw.oh;
+    a.hh = rw.hh;
     return a;
 }
 
@@ -92,6 +97,152 @@ __device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const R
         if (worst <= a.tolerance) return it + 1;
     }
     return -1;
+}
+
+// SETTLE (Miyamoto & Kollman, J. Comput. Chem. 13, 952 (1992)): the positions
+// SHAKE converges to, in closed form.  The three corrections act along the
+// reference bonds, so they lie in the reference molecular plane: in a frame whose
+// z axis is that plane's normal the z coordinates keep their unconstrained values,
+// which fixes the two tilts (phi about x, psi about y) of the canonical triangle,
+// and the in-plane rotation theta makes the corrections' torque vanish,
+// alpha sin(theta) + beta cos(theta) = gamma.  Work is local to the molecule
+// (bond vectors by minimum image from the oxygen), and the corrections are added
+// to the original coordinates as SHAKE's are.  Needs equal hydrogen masses;
+// returns 1, or 0 when the configuration has no solution (then SHAKE runs).
+__device__ int settle_molecule(Mol& r, const Mol& ref, const double m[3], const RigidArgs& a,
+                               const Fold3& f3) {
+    if (m[1] != m[2]) return 0;
+    const double mo = m[0], mh = m[1], M = mo + 2.0 * mh;
+    const double rc = 0.5 * a.hh;
+    const double h = sqrt(a.oh * a.oh - rc * rc);  // O above the H-H midpoint
+    const double ra = 2.0 * mh * h / M;             // centre of mass to O
+    const double rb = h - ra;                       // centre of mass to the H-H midpoint
+    // reference bonds from O, and the unconstrained positions relative to O
+    double b0[3], c0[3], p1[3][3];
+    min_image_wrapped(f3, ref.x[1], ref.y[1], ref.z[1], ref.x[0], ref.y[0], ref.z[0], b0[0], b0[1], b0[2]);
+    min_image_wrapped(f3, ref.x[2], ref.y[2], ref.z[2], ref.x[0], ref.y[0], ref.z[0], c0[0], c0[1], c0[2]);
+    p1[0][0] = p1[0][1] = p1[0][2] = 0.0;
+    min_image_wrapped(f3, r.x[1], r.y[1], r.z[1], r.x[0], r.y[0], r.z[0], p1[1][0], p1[1][1], p1[1][2]);
+    min_image_wrapped(f3, r.x[2], r.y[2], r.z[2], r.x[0], r.y[0], r.z[0], p1[2][0], p1[2][1], p1[2][2]);
+    double d[3];  // centre of mass of the unconstrained molecule
+    for (int k = 0; k < 3; ++k) d[k] = (mh * p1[1][k] + mh * p1[2][k]) / M;
+    double A1[3], B1[3], C1[3];
+    for (int k = 0; k < 3; ++k) {
+        A1[k] = p1[0][k] - d[k];
+        B1[k] = p1[1][k] - d[k];
+        C1[k] = p1[2][k] - d[k];
+    }
+    // frame: ez normal to the reference plane, ex perpendicular to ez and A1
+    double ez[3] = {b0[1] * c0[2] - b0[2] * c0[1], b0[2] * c0[0] - b0[0] * c0[2],
+                    b0[0] * c0[1] - b0[1] * c0[0]};
+    double ex[3] = {A1[1] * ez[2] - A1[2] * ez[1], A1[2] * ez[0] - A1[0] * ez[2],
+                    A1[0] * ez[1] - A1[1] * ez[0]};
+    const double nz = sqrt(ez[0] * ez[0] + ez[1] * ez[1] + ez[2] * ez[2]);
+    const double nx = sqrt(ex[0] * ex[0] + ex[1] * ex[1] + ex[2] * ex[2]);
+    if (!(nz > 0.0) || !(nx > 0.0)) return 0;
+    for (int k = 0; k < 3; ++k) {
+        ez[k] /= nz;
+        ex[k] /= nx;
+    }
+    const double ey[3] = {ez[1] * ex[2] - ez[2] * ex[1], ez[2] * ex[0] - ez[0] * ex[2],
+                          ez[0] * ex[1] - ez[1] * ex[0]};
+    auto px = [&](const double* v) { return v[0] * ex[0] + v[1] * ex[1] + v[2] * ex[2]; };
+    auto py = [&](const double* v) { return v[0] * ey[0] + v[1] * ey[1] + v[2] * ey[2]; };
+    auto pz = [&](const double* v) { return v[0] * ez[0] + v[1] * ez[1] + v[2] * ez[2]; };
+    // tilts from the out-of-plane coordinates
+    const double sphi = pz(A1) / ra;
+    const double cphi2 = 1.0 - sphi * sphi;
+    if (!(cphi2 > 0.0)) return 0;
+    const double cphi = sqrt(cphi2);
+    const double spsi = (pz(B1) - pz(C1)) / (2.0 * rc * cphi);
+    const double cpsi2 = 1.0 - spsi * spsi;
+    if (!(cpsi2 > 0.0)) return 0;
+    const double cpsi = sqrt(cpsi2);
+    // the tilted canonical triangle (O on +y, H1 at -x, H2 at +x), in-plane coordinates
+    const double x2[3] = {0.0, -rc * cpsi, rc * cpsi};
+    const double y2[3] = {ra * cphi, -rb * cphi - rc * spsi * sphi, -rb * cphi + rc * spsi * sphi};
+    // reference (x0, y0) and unconstrained (x1, y1) in-plane coordinates; the torque
+    // about any point is the same since the corrections sum to zero
+    const double x0[3] = {0.0, px(b0), px(c0)}, y0[3] = {0.0, py(b0), py(c0)};
+    const double x1[3] = {px(A1), px(B1), px(C1)}, y1[3] = {py(A1), py(B1), py(C1)};
+    double alpha = 0.0, beta = 0.0, gamma = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        alpha += m[k] * (x0[k] * x2[k] + y0[k] * y2[k]);
+        beta += m[k] * (x0[k] * y2[k] - y0[k] * x2[k]);
+        gamma += m[k] * (x0[k] * y1[k] - y0[k] * x1[k]);
+    }
+    const double r2 = alpha * alpha + beta * beta;
+    const double disc = r2 - gamma * gamma;
+    if (!(r2 > 0.0) || !(disc >= 0.0)) return 0;
+    const double sq = sqrt(disc);
+    const double sth = (alpha * gamma - beta * sq) / r2;  // the root near theta = 0
+    const double cth = (alpha * sq + beta * gamma) / r2;
+    // constrained positions relative to the centre of mass, then the corrections
+    for (int k = 0; k < 3; ++k) {
+        const double x3 = x2[k] * cth - y2[k] * sth;
+        const double y3 = x2[k] * sth + y2[k] * cth;
+        const double z3 = pz(k == 0 ? A1 : (k == 1 ? B1 : C1));
+        const double* q1 = k == 0 ? A1 : (k == 1 ? B1 : C1);
+        const double dx = x3 - px(q1), dy = y3 - py(q1), dz = z3 - pz(q1);
+        r.x[k] += dx * ex[0] + dy * ey[0] + dz * ez[0];
+        r.y[k] += dx * ex[1] + dy * ey[1] + dz * ez[1];
+        r.z[k] += dx * ex[2] + dy * ey[2] + dz * ez[2];
+    }
+    return 1;
+}
+
+// The velocity half of SETTLE: the multipliers of the three bond constraints
+// solve one 3x3 linear system (RATTLE's fixed point), by Cramer's rule.
+// Returns 1, or 0 for a singular system (then RATTLE runs).
+__device__ int settle_velocities(const Mol& r, Mol& v, const double m[3], const Fold3& f3) {
+    double rab[3], rac[3], rbc[3];
+    min_image_wrapped(f3, r.x[0], r.y[0], r.z[0], r.x[1], r.y[1], r.z[1], rab[0], rab[1], rab[2]);
+    min_image_wrapped(f3, r.x[0], r.y[0], r.z[0], r.x[2], r.y[2], r.z[2], rac[0], rac[1], rac[2]);
+    min_image_wrapped(f3, r.x[1], r.y[1], r.z[1], r.x[2], r.y[2], r.z[2], rbc[0], rbc[1], rbc[2]);
+    auto dot3 = [](const double* p, const double* q) { return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]; };
+    const double vab[3] = {v.x[0] - v.x[1], v.y[0] - v.y[1], v.z[0] - v.z[1]};
+    const double vac[3] = {v.x[0] - v.x[2], v.y[0] - v.y[2], v.z[0] - v.z[2]};
+    const double vbc[3] = {v.x[1] - v.x[2], v.y[1] - v.y[2], v.z[1] - v.z[2]};
+    const double ia = 1.0 / m[0], ib = 1.0 / m[1], ic = 1.0 / m[2];
+    const double abab = dot3(rab, rab), acac = dot3(rac, rac), bcbc = dot3(rbc, rbc);
+    const double abac = dot3(rab, rac), abbc = dot3(rab, rbc), acbc = dot3(rac, rbc);
+    // rows: (dv_a - dv_b).r_ab, (dv_a - dv_c).r_ac, (dv_b - dv_c).r_bc = -(v_ij . r_ij)
+    const double A[3][3] = {{(ia + ib) * abab, ia * abac, -ib * abbc},
+                            {ia * abac, (ia + ic) * acac, ic * acbc},
+                            {-ib * abbc, ic * acbc, (ib + ic) * bcbc}};
+    const double b[3] = {-dot3(vab, rab), -dot3(vac, rac), -dot3(vbc, rbc)};
+    const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                       A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                       A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    if (!(fabs(det) > 1e-300)) return 0;
+    double lam[3];
+    for (int c = 0; c < 3; ++c) {
+        double Mc[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) Mc[i][j] = j == c ? b[i] : A[i][j];
+        lam[c] = (Mc[0][0] * (Mc[1][1] * Mc[2][2] - Mc[1][2] * Mc[2][1]) -
+                  Mc[0][1] * (Mc[1][0] * Mc[2][2] - Mc[1][2] * Mc[2][0]) +
+                  Mc[0][2] * (Mc[1][0] * Mc[2][1] - Mc[1][1] * Mc[2][0])) / det;
+    }
+    // dv_a = (l_ab r_ab + l_ac r_ac)/m_a, dv_b = (-l_ab r_ab + l_bc r_bc)/m_b,
+    // dv_c = (-l_ac r_ac - l_bc r_bc)/m_c
+    const double da[3] = {(lam[0] * rab[0] + lam[1] * rac[0]) * ia, (lam[0] * rab[1] + lam[1] * rac[1]) * ia,
+                          (lam[0] * rab[2] + lam[1] * rac[2]) * ia};
+    const double db[3] = {(-lam[0] * rab[0] + lam[2] * rbc[0]) * ib, (-lam[0] * rab[1] + lam[2] * rbc[1]) * ib,
+                          (-lam[0] * rab[2] + lam[2] * rbc[2]) * ib};
+    const double dc[3] = {(-lam[1] * rac[0] - lam[2] * rbc[0]) * ic, (-lam[1] * rac[1] - lam[2] * rbc[1]) * ic,
+                          (-lam[1] * rac[2] - lam[2] * rbc[2]) * ic};
+    v.x[0] += da[0]; v.y[0] += da[1]; v.z[0] += da[2];
+    v.x[1] += db[0]; v.y[1] += db[1]; v.z[1] += db[2];
+    v.x[2] += dc[0]; v.y[2] += dc[1]; v.z[2] += dc[2];
+    return 1;
+}
+
+// Position and velocity constraints of one molecule by the configured method.
+__device__ __forceinline__ int constrain_positions(Mol& r, const Mol& ref, const double m[3],
+                                                   const RigidArgs& a, const Fold3& f3) {
+    if (a.settle && settle_molecule(r, ref, m, a, f3)) return 1;
+    return shake_molecule(r, ref, m, a, f3);
 }
 
 // rigid_water.cpp:118-161 for one molecule.
@@ -197,7 +348,7 @@ __global__ void k_shake(md_atoms a, const int* __restrict__ slot, int64_t nmol,
         ref.z[k] = rz[3 * m + k];
         mass[k] = a.mass[ms.s[k]];
     }
-    const int it = shake_molecule(r, ref, mass, ra, f3);
+    const int it = constrain_positions(r, ref, mass, ra, f3);
     report(it, max_it, status, MD_STATUS_SHAKE_DIVERGED);
     store_pos(a, ms, r);
 }
@@ -214,7 +365,7 @@ __global__ void k_rattle(md_atoms a, const int* __restrict__ slot, int64_t nmol,
     double mass[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) mass[k] = a.mass[ms.s[k]];
-    const int it = rattle_molecule(r, v, mass, ra, f3);
+    const int it = ra.settle && settle_velocities(r, v, mass, f3) ? 1 : rattle_molecule(r, v, mass, ra, f3);
     report(it, max_it, status, MD_STATUS_RATTLE_DIVERGED);
     store_vel(a, ms, v);
 }
@@ -258,7 +409,7 @@ __global__ void k_cvv_pre(md_atoms a, const int* __restrict__ slot, int64_t nmol
         r.z[k] = __dadd_rn(r.z[k], __dmul_rn(v.z[k], c.dt));
     }
     unc = r;
-    const int it = shake_molecule(r, ref, mass, c.ra, f3);
+    const int it = constrain_positions(r, ref, mass, c.ra, f3);
     report(it, max_it, status, MD_STATUS_SHAKE_DIVERGED);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -294,7 +445,7 @@ k_cvv_post(md_atoms a, const int* __restrict__ slot, int64_t nmol, CvvArgs c, in
             v.y[k] = __dadd_rn(v.y[k], __dmul_rn(a.fy[s], kc));
             v.z[k] = __dadd_rn(v.z[k], __dmul_rn(a.fz[s], kc));
         }
-        const int it = rattle_molecule(r, v, mass, c.ra, f3);
+        const int it = c.ra.settle && settle_velocities(r, v, mass, f3) ? 1 : rattle_molecule(r, v, mass, c.ra, f3);
         report(it, max_it, status, MD_STATUS_RATTLE_DIVERGED);
         store_vel(a, ms, v);
 #pragma unroll
@@ -431,6 +582,12 @@ int md_rigid_create(double oh, double hoh_degrees, double tolerance, int max_ite
     const double half_angle = 0.5 * hoh_degrees * kPi / 180.0;  // rigid_water.cpp:51-52
     rw->hh = 2.0 * oh * std::sin(half_angle);
     *out = rw;
+    return MD_OK;
+}
+
+int md_rigid_set_settle(md_rigid* rw, int on) {
+    if (!rw) return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_set_settle: NULL");
+    rw->settle = on != 0;
     return MD_OK;
 }
 

@@ -278,6 +278,7 @@ int system_kinetic_async(md_system* sys, int slot);
 struct md_rigid {
     double oh = 1.0, hh = 0.0, tolerance = 1e-12;
     int max_iterations = 500;
+    bool settle = false;  // closed-form SETTLE instead of SHAKE / RATTLE iterations
 };
 
 struct md_integrator {

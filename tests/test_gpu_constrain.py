@@ -329,3 +329,73 @@ def test_nhc_constrained_thermostats_and_conserves(md):
     t = 2.0 * rows[2000:, 2] / dof
     assert abs(t.mean() - 298.0) < 0.1 * 298.0, t.mean()
     assert worst_geometry(s.positions, SPCE["box1"], rw.oh_distance(), rw.hh_distance()) < 1e-10
+
+
+# ----------------------------------------------------------------- SETTLE
+def settle_constraint(md):
+    p = md.SpceParameters
+    return md.RigidWater(p.rOH, p.angleHOH, settle=True)
+
+
+@pytest.mark.parametrize("c", [1, 2])
+def test_settle_positions_are_shakes_fixed_point(md, c):
+    """rigid_water.hpp:20-24: SETTLE must reproduce SHAKE to machine precision --
+    here to SHAKE's own tolerance (1e-12 relative on r^2) -- on the displaced
+    NIST sites, without iterating and without moving any centre of mass."""
+    rw = settle_constraint(md)
+    _, orw = constraint(md)
+    s = water(md, c)
+    box = SPCE[f"box{c}"]
+    ref = s.positions
+    i = np.arange(s.n)
+    sh = 0.01 * (i % 7) - 0.03
+    disp = ref + np.stack([sh, -0.5 * sh, 0.25 * sh], 1)
+    s.positions = disp
+    m = s.masses
+    it = rw.constrain_positions(s, ref)
+    got = s.positions
+    want, _ = O.shake(orw, disp, ref, m, box)
+    assert it == 1
+    assert np.max(np.abs(got - want)) < 1e-11
+    assert worst_geometry(got, box, rw.oh_distance(), rw.hh_distance()) < 1e-13
+    com = lambda p: np.add.reduceat(p * m[:, None], np.arange(0, s.n, 3)) / np.add.reduceat(
+        m, np.arange(0, s.n, 3))[:, None]
+    assert np.max(np.linalg.norm(com(got) - com(disp), axis=1)) < 1e-12
+
+
+def test_settle_velocities_are_rattles_fixed_point(md):
+    rw = settle_constraint(md)
+    _, orw = constraint(md)
+    s = water(md)
+    thermal_velocities(md, s, 298.0, 21)
+    vel = s.velocities
+    it = rw.constrain_velocities(s)
+    got = s.velocities
+    want, _ = O.rattle(orw, s.positions, vel, s.masses, SPCE["box1"])
+    assert it == 1
+    assert np.max(np.abs(got - want)) < 1e-10 * np.max(np.abs(want))
+    # no velocity left along any bond
+    pos = s.positions
+    for i, j in ((0, 1), (0, 2), (1, 2)):
+        d = fold(pos[i::3] - pos[j::3], SPCE["box1"])
+        rel = np.sum((got[i::3] - got[j::3]) * d, axis=1)
+        assert np.max(np.abs(rel)) < 1e-12 * np.max(np.abs(got))
+
+
+def test_settle_trajectory_tracks_shake(md):
+    """50 constrained steps of 2 fs under full SPC/E forces: SETTLE and SHAKE/RATTLE
+    stay within roundoff of each other over the run, and SETTLE holds the geometry
+    to 1e-12."""
+    rw_s = settle_constraint(md)
+    rw, _ = constraint(md)
+    runs = []
+    for r in (rw, rw_s):
+        s = water(md)
+        thermal_velocities(md, s, 298.0, 5)
+        r.constrain_velocities(s)
+        ff = md.SpceForceField()
+        ff.compute_forces(s)
+        md.ConstrainedVelocityVerlet(femtoseconds(2.0), r).run(s, ff, 50)
+        runs.append(s.positions)
+    assert np.max(np.abs(runs[0] - runs[1])) < 1e-6
+    assert worst_geometry(runs[1], SPCE["box1"], rw.oh_distance(), rw.hh_distance()) < 1e-12
