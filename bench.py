@@ -829,6 +829,194 @@ def run_water_arm(args):
     return 0
 
 
+# ------------------------------------------------------------- water_rdf protocol
+WRDF_METRIC = ("site-steps/s, SPC/E water_rdf protocol: 300 rigid molecules (900 sites), "
+               "15,000 + 10,000 steps, 1 B200")
+WRDF_SITES, WRDF_EQUIL, WRDF_PROD, WRDF_SAMPLE = 900, 15000, 10000, 10
+WRDF_PUBLISHED_SEC = 434.687  # the reference's recorded wall time for this protocol
+
+
+def water_rdf_config(runs, equil=15000, prod=10000):
+    return {"workload": "apps/water_rdf.cpp protocol: NIST SPC/E configuration 3 (300 molecules) "
+                        "expanded rigidly to 0.997 g/cm^3 (L = 20.802 A); Ewald alpha=5.6/L, "
+                        f"kmax=5, rc=10 A; RATTLE velocity Verlet, dt=2 fs; {equil:,} equilibration "
+                        f"steps rescaled to 298 K every 50, {prod:,} NVE steps with an O-O RDF "
+                        "(10 A, 200 bins) every 10; one bench step = the whole protocol",
+            "sites": WRDF_SITES, "protocol_runs": runs, "precision": "FP64",
+            "l2_policy": "no flush: the working set (about 2 MB) is L2-resident by design",
+            "parallelism": "replicas (one independent system per GPU)"}
+
+
+def water_rdf_inputs():
+    """NIST SPC/E configuration 3 (the reference's data file, carried as a test
+    fixture) at the app's state point, with its Rng(7001) velocities."""
+    from moleculardynamics_b200 import water_rdf as W
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                             "nist_spce.npz"))
+    types = ["O" if o else "H" for o in d["isO3"]]
+    return d["pos3"], types, d["box3"]
+
+
+def reference_water_rdf_rate(steps):
+    """The reference's ConstrainedVelocityVerlet + SpceForceField (compiled from
+    its sources) for `steps` steps of the protocol's state point, 1 thread."""
+    import oracle as O
+    from moleculardynamics_b200 import water_rdf as W
+    pos, types, box = water_rdf_inputs()
+    pos, types, box, _ = W.state_point(pos, types, box)
+    m = np.array([15.9994 if t == "O" else 1.008 for t in types])
+    q = np.array([-0.8476 if t == "O" else 0.4238 for t in types])
+    vel = W.thermal_velocities(m, 298.0, 7001)
+    R = O.ref()
+    if R is None:
+        return None
+    cols = [np.ascontiguousarray(a[:, k]) for a in (pos, vel) for k in range(3)]
+    f = [np.zeros(len(m)) for _ in range(3)]
+    mol = (np.arange(len(m)) // 3).astype(np.int64)
+    p = O._p
+    t0 = time.perf_counter()
+    R.ref_spce_cvv(len(m), p(box), *[p(c) for c in cols], *[p(c) for c in f], p(m), p(q),
+                   mol.ctypes.data_as(C.POINTER(C.c_int64)), 10.0, 5, 2e-3 / TAU_PS, int(steps))
+    sec = time.perf_counter() - t0
+    return WRDF_SITES * steps / sec, sec
+
+
+def run_water_rdf_arm(args):
+    world, rank, local = dist_env()
+    group = Group(world)
+    cpu = None
+    if args.impl == "reference" or (rank == 0 and world == 1 and not args.no_cpu):
+        if rank == 0:
+            steps = max(args.ref_steps, 1)
+            got = reference_water_rdf_rate(steps)
+            if got is not None:
+                rate, sec = got
+                cpu = {"value": rate, "unit": "site-steps/s", "cores": 1, "kind": "reference",
+                       "sample": f"{steps} constrained steps (+1 priming force call) of the "
+                                 f"protocol's state point through the reference's "
+                                 f"ConstrainedVelocityVerlet and SpceForceField, compiled from "
+                                 f"its sources ({sec:.2f} s, 1 thread, {cpu_model()}); no RDF"}
+        if args.impl == "reference":
+            if rank == 0:
+                if cpu is None:
+                    print(json.dumps({"impl": "reference",
+                                      "unavailable": "reference library not built"}), flush=True)
+                else:
+                    print(json.dumps({
+                        "metric": WRDF_METRIC, "value": cpu["value"], "unit": "site-steps/s",
+                        "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                        "ms_per_step": 1e3 * WRDF_SITES * (WRDF_EQUIL + WRDF_PROD) / cpu["value"],
+                        "higher_is_better": True, "scaling": "weak",
+                        "vs_baseline": cpu["value"] / (WRDF_SITES * (WRDF_EQUIL + WRDF_PROD)
+                                                        / WRDF_PUBLISHED_SEC),
+                        "dtype": "f64", "data": "NIST SPC/E configuration 3 (reference data)",
+                        "config": water_rdf_config(1), "impl": "reference", "cpu_baseline": cpu,
+                        "e2e": {"value": cpu["value"], "unit": "site-steps/s",
+                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+            group.close()
+            return 0
+    import moleculardynamics_b200 as md
+    from moleculardynamics_b200 import water_rdf as W
+    equil, prod = args.wrdf_steps
+    ctx = md.Context(local)
+    pos0, types0, box0 = water_rdf_inputs()
+    pos, types, box, molecules = W.state_point(pos0, types0, box0)
+    dof = md.RigidWater.degrees_of_freedom(molecules, True)
+    s = md.build_spce_system(pos, types, box, ctx=ctx)
+    m = s.masses
+    v0 = W.thermal_velocities(m, 298.0, 7001)
+    rigid = md.RigidWater(1.0, 109.47, settle=args.settle)
+    ff = md.SpceForceField(ctx=ctx)
+    L = md.lib()
+    mean_t = C.c_double()
+
+    def protocol(rdf):
+        integ = md.ConstrainedVelocityVerlet(md.units.femtoseconds(2.0), rigid)
+        s.positions = pos
+        s.velocities = v0
+        s.remove_center_of_mass_motion()
+        rigid.constrain_velocities(s)
+        ctx.synchronize()
+        l0 = ctx.launch_count()
+        ms = C.c_double()
+        md._check(L.md_context_span_begin(ctx.handle))
+        md._check(L.md_water_rdf_run(integ.handle, s.handle, ff.handle, rdf.handle, 298.0, dof,
+                                     equil, 50, prod, WRDF_SAMPLE, C.byref(mean_t)))
+        md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+        return ms.value, ctx.launch_count() - l0
+
+    for _ in range(args.warmup):
+        protocol(md.Rdf(10.0, 200, ctx=ctx))
+    ctx.synchronize()
+    group.barrier()
+    # the timed region: the fused protocol alone (state reset outside it)
+    total_ms, launches = 0.0, 0
+    clocks = ClockSampler(local)
+    clocks.__enter__()
+    rdf = md.Rdf(10.0, 200, ctx=ctx)
+    for _ in range(args.steps):
+        ms, n_launch = protocol(rdf)  # state reset and synchronised before the span
+        total_ms += ms
+        launches += n_launch
+    clocks.__exit__(None, None, None)
+    dev_ms = group.reduce(total_ms, "max")
+    md_steps = equil + prod
+    value = world * WRDF_SITES * md_steps * args.steps / (dev_ms * 1e-3)
+    # end to end through the public API: host arrays in, the finished g(r) out
+    group.barrier()
+    t0 = time.perf_counter()
+    res = W.run(pos0, types0, box0, equilibrate=equil, production=prod, settle=args.settle,
+                ctx=ctx)
+    e2e_sec = group.reduce(time.perf_counter() - t0, "max")
+    g = rdf.g()
+    r = rdf.bin_centres()
+    peak = W.first_peak(r, g)
+    if rank == 0:
+        peaks, peak_src = measured_peaks()
+        us_step = 1e3 * dev_ms / (args.steps * md_steps)
+        # algorithmic bytes of a step: each site's position, velocity and force
+        # read and position and velocity written by the two halves (5 x 24 B),
+        # plus position and charge read by the force pass (32 B)
+        alg = 152.0 * WRDF_SITES
+        achieved = alg / (us_step * 1e-6) / 1e9
+        h2d = sum(a.nbytes for a in (pos0, box0)) + 8 * 900 * 5  # positions, box; m, q, mol, v
+        line = {
+            "metric": WRDF_METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / world / (WRDF_SITES * (WRDF_EQUIL + WRDF_PROD)
+                                            / WRDF_PUBLISHED_SEC),
+            "dtype": "f64",
+            "data": "NIST SPC/E configuration 3 (reference data file) at the app's state point, "
+                    "Rng(7001) velocities",
+            "config": dict(water_rdf_config(args.steps, equil, prod),
+                           constraints="SETTLE" if args.settle else "SHAKE/RATTLE"),
+            "gpu_launches": int(launches), "us_per_md_step": us_step,
+            "launches_per_md_step": launches / (args.steps * md_steps),
+            "result": {"mean_production_temperature_K": mean_t.value,
+                       "first_peak_r_angstrom": peak[2], "first_peak_g": peak[3],
+                       "tail_mean_g_beyond_8.5A": W.tail_mean(r, g), "rdf_frames": rdf.frames()},
+            "e2e": {"value": world * WRDF_SITES * md_steps / e2e_sec, "unit": "site-steps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * 200 * 3,
+                    "wall_seconds": e2e_sec,
+                    "path": "water_rdf.run: host configuration -> state point -> device system, "
+                            "md_water_rdf_run, g(r) read back"},
+            "roofline": {"bound": "hbm", "kernel": "whole MD step", "achieved": achieved,
+                         "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": achieved / peaks.get("hbm_gbs", 6650.0),
+                         "peak_source": f"hbm_gbs of {peak_src}",
+                         "algorithmic_bytes_per_site": 152.0, "traffic": None,
+                         "note": "latency bound: 900 sites, about 2 MB of state and lists held "
+                                 "in L2; the step is a chain of dependent launches"},
+            "clocks": clocks.summary(),
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    group.close()
+    return 0
+
+
 # ------------------------------------------------------------------ analysis
 ANALYSIS_METRIC = "RDF frames/s, 1M-atom LJ liquid (rMax 4.0, 200 bins) on 1 B200"
 RDF_RMAX, RDF_BINS, CORR_LAGS = 4.0, 200, 100
@@ -963,7 +1151,7 @@ def run_analysis_arm(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--workload", default="lj1m",
-                    choices=["lj1m", "batch", "adjoint", "water", "analysis"],
+                    choices=["lj1m", "batch", "adjoint", "water", "analysis", "water_rdf"],
                     help="lj1m: the headline 1M-atom run; batch: 48 NHC replicas; adjoint: "
                          "forward + backward of a 32,000-atom differentiable trajectory "
                          "(--steps is its length)")
@@ -971,6 +1159,10 @@ def main():
     ap.add_argument("--equil-water", type=int, default=1000)
     ap.add_argument("--settle", action="store_true",
                     help="water: SETTLE instead of SHAKE/RATTLE iterations")
+    ap.add_argument("--wrdf-steps", type=int, nargs=2, default=[WRDF_EQUIL, WRDF_PROD],
+                    metavar=("EQUIL", "PROD"),
+                    help="water_rdf: protocol lengths (profiling configurations only; the "
+                         "metric is quoted on the default 15000 10000)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
@@ -997,6 +1189,8 @@ def main():
         return run_water_arm(args)
     if args.workload == "analysis":
         return run_analysis_arm(args)
+    if args.workload == "water_rdf":
+        return run_water_rdf_arm(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

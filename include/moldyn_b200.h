@@ -146,6 +146,10 @@ MD_API int md_system_zero_forces(md_system* sys);                          /* sy
 MD_API int md_system_kinetic_energy(md_system* sys, double* ke);           /* system.cpp:124-131 */
 MD_API int md_system_total_momentum(md_system* sys, double p[3]);          /* system.cpp:137-145 */
 MD_API int md_system_remove_com_motion(md_system* sys);                    /* system.cpp:147-164 */
+/* Velocity rescale toward `target` on the device, no host round trip:
+ * t = 2 KE / dof, and v *= sqrt(target / t) when t > 0 (the equilibration
+ * rescale of apps/water_rdf.cpp:186-195, system.cpp:133-135). */
+MD_API int md_system_rescale_temperature(md_system* sys, int64_t dof, double target);
 /* Potential energy and virial of the last force evaluation on this system. */
 MD_API int md_system_last_energy(md_system* sys, double* energy, double* virial);
 
@@ -367,6 +371,10 @@ MD_API int md_lj_forces_static(const double* d_x, const double* d_y, const doubl
 MD_API int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed, double* x,
                    double* y, double* z, double* vx, double* vy, double* vz, double* mass,
                    double box[3]);
+/* `count` consecutive normal draws of Rng(seed) (util/random.hpp:37-76):
+ * std::mt19937_64 and the polar Box-Muller transform, host-side setup.
+ * Returns count or MD_ERR_INVALID_ARGUMENT. */
+MD_API int64_t md_rng_normals(uint64_t seed, int64_t count, double* out);
 
 /* ------------------------------------------------------------ replica batches */
 /* Many independent LJ replicas stepped together; no reference counterpart (the
@@ -435,10 +443,29 @@ MD_API int md_run_spce(md_integrator* integ, md_system* sys, md_ewald* ff, int64
 MD_API int md_rdf_create(md_context* ctx, double rmax, int64_t bins, md_rdf** out);
 MD_API int md_rdf_destroy(md_rdf* rdf);
 MD_API int md_rdf_accumulate(md_rdf* rdf, md_system* sys);
+/* The frame of the atoms with original index first, first + stride, ... alone,
+ * as Rdf::accumulate of a System holding just those atoms in that order (e.g.
+ * the oxygens of consecutive O, H, H water molecules: first 0, stride 3, as
+ * apps/water_rdf.cpp:90-97 gathers them). */
+MD_API int md_rdf_accumulate_subset(md_rdf* rdf, md_system* sys, int64_t first, int64_t stride);
 MD_API int md_rdf_histogram(const md_rdf* rdf, double* hist);
 MD_API int md_rdf_g(const md_rdf* rdf, double* g);
 MD_API int md_rdf_bin_centres(const md_rdf* rdf, double* centres);
 MD_API int md_rdf_frames(const md_rdf* rdf, int64_t* frames);
+
+/* The simulation of apps/water_rdf.cpp:159-216 in one call, on the device:
+ * forces on entry, `equilibrate` constrained steps with the velocities scaled
+ * toward `temperature` (T = 2 KE / dof) and re-constrained every
+ * `rescale_every` steps (:188-200), then `production` NVE steps whose
+ * temperatures are averaged into *mean_temperature (nullable, :207-211) while
+ * the oxygens (atoms 0, 3, 6, ...) are accumulated into `rdf` every
+ * `sample_every` steps (:212-215).  `integ` is a ConstrainedVelocityVerlet
+ * (md_integrator_create_rattle); the system is O, H, H triples.  One host
+ * synchronisation at the end; the histogram is read when rdf is queried. */
+MD_API int md_water_rdf_run(md_integrator* integ, md_system* sys, md_ewald* ff, md_rdf* rdf,
+                            double temperature, int64_t dof, int64_t equilibrate,
+                            int64_t rescale_every, int64_t production, int64_t sample_every,
+                            double* mean_temperature);
 
 /* Mean-squared displacement, analyze/msd.hpp:19-42 (Msd(natoms, maxLag)).
  * md_msd_push (msd.cpp:66-96) unwraps incrementally with the minimum image of

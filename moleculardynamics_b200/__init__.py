@@ -103,6 +103,7 @@ def _load():
         "md_system_kinetic_energy": (C.c_int, [_vp, _d]),
         "md_system_total_momentum": (C.c_int, [_vp, _d]),
         "md_system_remove_com_motion": (C.c_int, [_vp]),
+        "md_system_rescale_temperature": (C.c_int, [_vp, C.c_int64, C.c_double]),
         "md_system_last_energy": (C.c_int, [_vp, _d, _d]),
         "md_cells_create": (C.c_int, [_vp, _d, C.c_double, C.POINTER(_vp)]),
         "md_cells_destroy": (C.c_int, [_vp]),
@@ -144,6 +145,7 @@ def _load():
         "md_rdf_create": (C.c_int, [_vp, C.c_double, C.c_int64, C.POINTER(_vp)]),
         "md_rdf_destroy": (C.c_int, [_vp]),
         "md_rdf_accumulate": (C.c_int, [_vp, _vp]),
+        "md_rdf_accumulate_subset": (C.c_int, [_vp, _vp, C.c_int64, C.c_int64]),
         "md_rdf_histogram": (C.c_int, [_vp, _d]),
         "md_rdf_g": (C.c_int, [_vp, _d]),
         "md_rdf_bin_centres": (C.c_int, [_vp, _d]),
@@ -173,6 +175,7 @@ def _load():
         "md_run_lj": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _d]),
         "md_fcc_lattice": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_uint64] + [_d] * 8),
         "md_coulomb_prefactor": (C.c_double, []),
+        "md_rng_normals": (C.c_int64, [C.c_uint64, C.c_int64, _d]),
         "md_lj_forces_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, _d,
                                           C.c_double, C.c_double, C.c_double, C.c_int,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -200,6 +203,8 @@ def _load():
                                                       C.c_int, C.c_int64, C.POINTER(_vp)]),
         "md_integrator_iterations": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "md_run_spce": (C.c_int, [_vp, _vp, _vp, C.c_int64, _d]),
+        "md_water_rdf_run": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int64, C.c_int64,
+                                       C.c_int64, C.c_int64, C.c_int64, _d]),
         "md_batch_create": (C.c_int, [C.POINTER(_vp)]),
         "md_batch_destroy": (C.c_int, [_vp]),
         "md_batch_add": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int)]),
@@ -410,6 +415,11 @@ class System:
 
     def remove_center_of_mass_motion(self):
         _check(lib().md_system_remove_com_motion(self._h))
+
+    def rescale_temperature(self, dof, target):
+        """v *= sqrt(target / T), T = 2 KE / dof, if T > 0; on the device,
+        asynchronous (apps/water_rdf.cpp:186-195)."""
+        _check(lib().md_system_rescale_temperature(self._h, int(dof), float(target)))
 
     def volume(self):
         return float(self.box[0] * self.box[1] * self.box[2])
@@ -988,8 +998,17 @@ class Rdf:
             _lib.md_rdf_destroy(self._h)
             self._h = None
 
-    def accumulate(self, sys: System):
-        _check(lib().md_rdf_accumulate(self._h, sys.handle))
+    @property
+    def handle(self):
+        return self._h
+
+    def accumulate(self, sys: System, first=0, stride=1):
+        """One frame; first/stride select the atoms with original index first,
+        first + stride, ... (e.g. the oxygens of O, H, H water: 0, 3)."""
+        if first == 0 and stride == 1:
+            _check(lib().md_rdf_accumulate(self._h, sys.handle))
+        else:
+            _check(lib().md_rdf_accumulate_subset(self._h, sys.handle, int(first), int(stride)))
 
     def _vec(self, fn):
         out = np.zeros(self.bins)
@@ -1133,6 +1152,74 @@ class Batch:
 
 
 # ---------------------------------------------------------------- setup
+class units:
+    """core/units.hpp:33-40: the water side's time unit, tau = A sqrt(amu / kB)."""
+    TAU_IN_PICOSECONDS = 1.0966875353
+
+    @staticmethod
+    def picoseconds(ps):
+        return ps / units.TAU_IN_PICOSECONDS
+
+    @staticmethod
+    def femtoseconds(fs):
+        return units.picoseconds(fs * 1.0e-3)
+
+    @staticmethod
+    def to_picoseconds(tau):
+        return tau * units.TAU_IN_PICOSECONDS
+
+
+def read_nist_config(path):
+    """readNistConfig (io/nist_config.cpp:30-86): line 1 the box lengths, line 2
+    a count (not trusted: the SPC/E files give molecules), then `index x y z
+    [type]` lines until end of file, blank lines skipped.  Returns dict(pos,
+    box, types); types is empty unless some line has the fifth column.  Raises
+    MDError (std::runtime_error) on a missing file or a malformed line."""
+    try:
+        f = open(path)
+    except OSError:
+        raise MDError(f"readNistConfig: cannot open file {path}") from None
+    with f:
+        lines = f.read().split("\n")
+    if lines and lines[-1] == "":
+        lines.pop()
+    if not lines:
+        raise MDError(f"readNistConfig: empty file {path}")
+
+    def numbers(text, count, conv):
+        parts = text.split()
+        if len(parts) < count:
+            raise ValueError
+        return [conv(x) for x in parts[:count]]
+
+    try:
+        box = np.array(numbers(lines[0], 3, float))
+    except ValueError:
+        raise MDError(f"readNistConfig: malformed box line in {path}") from None
+    if len(lines) < 2:
+        raise MDError(f"readNistConfig: missing count line in {path}")
+    try:
+        numbers(lines[1], 1, int)
+    except ValueError:
+        raise MDError(f"readNistConfig: malformed count line in {path}") from None
+    pos, types, any_typed = [], [], False
+    for line in lines[2:]:
+        if not line.strip(" \t\r\n"):
+            continue
+        parts = line.split()
+        try:
+            int(parts[0])
+            xyz = [float(v) for v in parts[1:4]]
+            if len(xyz) < 3:
+                raise ValueError
+        except (ValueError, IndexError):
+            raise MDError(f"readNistConfig: malformed atom line in {path}") from None
+        pos.append(xyz)
+        types.append(parts[4] if len(parts) > 4 else "")
+        any_typed = any_typed or len(parts) > 4
+    return dict(pos=np.array(pos).reshape(-1, 3), box=box, types=types if any_typed else [])
+
+
 def water_lattice(per_side, box_length, seed, params=SpceParameters):
     """A simple cubic lattice of rigid SPC/E molecules (per_side^3 molecules in a
     cubic box of side box_length, oxygens at the cell centres, each molecule

@@ -29,8 +29,9 @@ struct md_rdf {
     md_context* ctx = nullptr;
     double rmax = 0.0, width = 0.0;
     int64_t bins = 0;
-    DevBuf hist;                 // unsigned long long[bins]
-    std::vector<double> host;    // running pair counts (rdf.cpp:73)
+    DevBuf hist;                 // unsigned long long[bins]: pair counts of every frame so far
+    mutable std::vector<double> host;  // host copy of hist (rdf.cpp:73), refreshed on demand
+    mutable bool stale = false;        // hist has frames that host does not
     int64_t frames = 0, natoms = 0;
     double sum_rho = 0.0;
     CellGrid grid;
@@ -60,7 +61,13 @@ struct RdfArgs {
     double rmax, rmax2_hi, width;
     int bins;
     int use_shared;
+    int64_t first, stride;  // atoms counted: original index first + k * stride
 };
+
+__device__ __forceinline__ bool rdf_selected(const RdfArgs& a, double w) {
+    const int64_t o = static_cast<int64_t>(w) - a.first;
+    return o >= 0 && o % a.stride == 0;
+}
 
 // rdf.cpp:68-74 for the pair (a, b), a holding the lower original index: the bin
 // of r = |minimumImage(r_a - r_b)|, or -1 when r >= rMax or past the last bin.
@@ -126,6 +133,7 @@ k_rdf_cells(const double4* __restrict__ pos, int64_t n, RdfGrid g, RdfArgs a,
         const int cell = g.cell_of_rank[lo];
         const int cx = cell % g.nx, cy = (cell / g.nx) % g.ny, cz = cell / (g.nx * g.ny);
         const double4 p = ldg4(pos + g.sorted[s]);
+        if (!rdf_selected(a, p.w)) goto done;
         for (int q = 0; q < 27; ++q) {
             int jx = cx + (q % 3) - 1, jy = cy + ((q / 3) % 3) - 1, jz = cz + (q / 9) - 1;
             jx = jx < 0 ? jx + g.nx : (jx >= g.nx ? jx - g.nx : jx);
@@ -135,10 +143,12 @@ k_rdf_cells(const double4* __restrict__ pos, int64_t n, RdfGrid g, RdfArgs a,
             const int t1 = g.start[rr + 1];
             for (int t = g.start[rr]; t < t1; ++t) {
                 const double4 qd = ldg4(pos + g.sorted[t]);
-                if (qd.w > p.w) rdf_count(a, s_hist, hist, rdf_bin(a, f3, p, qd));
+                if (qd.w > p.w && rdf_selected(a, qd.w))
+                    rdf_count(a, s_hist, hist, rdf_bin(a, f3, p, qd));
             }
         }
     }
+done:
     rdf_flush(a, s_hist, hist);
 }
 
@@ -157,9 +167,10 @@ k_rdf_brute(const double4* __restrict__ pos, int64_t n, RdfArgs a, unsigned long
         if (base + threadIdx.x < n) tile[threadIdx.x] = pos[base + threadIdx.x];
         __syncthreads();
         const int lim = static_cast<int>(n - base < kRdfBlock ? n - base : kRdfBlock);
-        if (i < n)
+        if (i < n && rdf_selected(a, p.w))
             for (int t = 0; t < lim; ++t)
-                if (tile[t].w > p.w) rdf_count(a, s_hist, hist, rdf_bin(a, f3, p, tile[t]));
+                if (tile[t].w > p.w && rdf_selected(a, tile[t].w))
+                    rdf_count(a, s_hist, hist, rdf_bin(a, f3, p, tile[t]));
     }
     rdf_flush(a, s_hist, hist);
 }
@@ -362,9 +373,12 @@ int md_rdf_create(md_context* ctx, double rmax, int64_t bins, md_rdf** out) {
     r->bins = bins;
     r->width = rmax / static_cast<double>(bins);  // rdf.cpp:53
     r->host.assign(static_cast<size_t>(bins), 0.0);
-    if (bins > 0 && r->hist.ensure(sizeof(unsigned long long) * static_cast<size_t>(bins)) != MD_OK) {
+    if (bins > 0 && (r->hist.ensure(sizeof(unsigned long long) * static_cast<size_t>(bins)) != MD_OK ||
+                     cudaMemsetAsync(r->hist.ptr, 0, sizeof(unsigned long long) * static_cast<size_t>(bins),
+                                     ctx->stream) != cudaSuccess)) {
+        r->hist.release();
         delete r;
-        return MD_ERR_CUDA;
+        return fail(MD_ERR_CUDA, "md_rdf_create: device histogram");
     }
     *out = r;
     return MD_OK;
@@ -381,8 +395,32 @@ int md_rdf_destroy(md_rdf* r) {
     return MD_OK;
 }
 
-int md_rdf_accumulate(md_rdf* r, md_system* sys) {
+int md_rdf_accumulate(md_rdf* r, md_system* sys) { return md_rdf_accumulate_subset(r, sys, 0, 1); }
+
+int md_rdf_accumulate_subset(md_rdf* r, md_system* sys, int64_t first, int64_t stride) {
+    MDB_TRY(rdf_accumulate_async(r, sys, first, stride));
+    return ctx_check_status(r->ctx);
+}
+
+int md_rdf_histogram(const md_rdf* r, double* hist) {
+    if (!r || (!hist && r->bins > 0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_histogram: NULL argument");
+    MDB_TRY(rdf_sync(r));
+    std::copy(r->host.begin(), r->host.end(), hist);
+    return MD_OK;
+}
+
+}  // extern "C"
+
+namespace mdb {
+
+// One frame's pair counts are added to the device histogram; nothing is read
+// back (the host copy is refreshed by rdf_sync when the counts are asked for).
+// Counts are integers, so summing them per bin on the device over frames equals
+// the reference's running double sum (rdf.cpp:73) exactly.
+int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t stride) {
     if (!r || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_accumulate: NULL argument");
+    if (first < 0 || stride < 1)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_accumulate_subset: first >= 0, stride >= 1");
     if (sys->ctx != r->ctx)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_accumulate: the system lives on another context");
     const double smallest = std::min({sys->box[0], sys->box[1], sys->box[2]});
@@ -392,8 +430,8 @@ int md_rdf_accumulate(md_rdf* r, md_system* sys) {
                     "beyond that are ambiguous");
     md_context* ctx = r->ctx;
     const int64_t n = sys->n;
-    if (n > 1 && r->bins > 0 && r->rmax > 0.0) {
-        MDB_CUDA(cudaMemsetAsync(r->hist.ptr, 0, sizeof(unsigned long long) * r->bins, ctx->stream));
+    const int64_t selected = n > first ? (n - first + stride - 1) / stride : 0;
+    if (selected > 1 && r->bins > 0 && r->rmax > 0.0) {
         RdfArgs a;
         a.box = box_of_system(sys);
         a.rmax = r->rmax;
@@ -401,6 +439,8 @@ int md_rdf_accumulate(md_rdf* r, md_system* sys) {
         a.width = r->width;
         a.bins = static_cast<int>(std::min<int64_t>(r->bins, 0x7fffffff));
         a.use_shared = r->bins <= kRdfSharedBins ? 1 : 0;
+        a.first = first;
+        a.stride = stride;
         const size_t shm = a.use_shared ? sizeof(unsigned) * static_cast<size_t>(r->bins) : 0;
         if (!r->grid.rank_of_cell || r->grid_box[0] != sys->box[0] ||
             r->grid_box[1] != sys->box[1] || r->grid_box[2] != sys->box[2]) {
@@ -421,23 +461,28 @@ int md_rdf_accumulate(md_rdf* r, md_system* sys) {
         }
         ++ctx->launches;
         MDB_CHECK_LAUNCH();
-        std::vector<unsigned long long> h(static_cast<size_t>(r->bins));
-        MDB_CUDA(cudaMemcpyAsync(h.data(), r->hist.ptr, sizeof(unsigned long long) * r->bins,
-                                 cudaMemcpyDeviceToHost, ctx->stream));
-        MDB_CUDA(cudaStreamSynchronize(ctx->stream));
-        for (int64_t k = 0; k < r->bins; ++k) r->host[k] += static_cast<double>(h[k]);
+        r->stale = true;
     }
-    r->natoms = n;  // rdf.cpp:79-81
-    r->sum_rho += static_cast<double>(n) / (sys->box[0] * sys->box[1] * sys->box[2]);
+    r->natoms = selected;  // rdf.cpp:79-81
+    r->sum_rho += static_cast<double>(selected) / (sys->box[0] * sys->box[1] * sys->box[2]);
     ++r->frames;
-    return ctx_check_status(ctx);
-}
-
-int md_rdf_histogram(const md_rdf* r, double* hist) {
-    if (!r || (!hist && r->bins > 0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_histogram: NULL argument");
-    std::copy(r->host.begin(), r->host.end(), hist);
     return MD_OK;
 }
+
+int rdf_sync(const md_rdf* r) {
+    if (!r->stale) return MD_OK;
+    std::vector<unsigned long long> h(static_cast<size_t>(r->bins));
+    MDB_CUDA(cudaMemcpyAsync(h.data(), r->hist.ptr, sizeof(unsigned long long) * r->bins,
+                             cudaMemcpyDeviceToHost, r->ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(r->ctx->stream));
+    for (int64_t k = 0; k < r->bins; ++k) r->host[k] = static_cast<double>(h[k]);
+    r->stale = false;
+    return MD_OK;
+}
+
+}  // namespace mdb
+
+extern "C" {
 
 int md_rdf_bin_centres(const md_rdf* r, double* centres) {
     if (!r || (!centres && r->bins > 0))
@@ -450,6 +495,7 @@ int md_rdf_bin_centres(const md_rdf* r, double* centres) {
 int md_rdf_g(const md_rdf* r, double* g) {
     if (!r || (!g && r->bins > 0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_g: NULL argument");
     const double pi = 3.14159265358979323846;
+    MDB_TRY(rdf_sync(r));
     for (int64_t k = 0; k < r->bins; ++k) g[k] = 0.0;
     if (r->frames == 0) return MD_OK;
     const double rho = r->sum_rho / static_cast<double>(r->frames);  // rdf.cpp:97-105

@@ -30,7 +30,10 @@ namespace {
 
 constexpr int kBlock = 128;
 constexpr double kPi = 3.14159265358979323846;
-__device__ __constant__ int kCons[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+// The constraints' atom pairs (O-H1, O-H2, H1-H2), as compile-time indices so
+// that a molecule's coordinates stay in registers in the unrolled sweeps.
+__host__ __device__ constexpr int cons_i(int c) { return c == 2 ? 1 : 0; }
+__host__ __device__ constexpr int cons_j(int c) { return c == 0 ? 1 : 2; }
 
 struct RigidArgs {
     double target2[3];  // squared O-H, O-H, H-H distances
@@ -64,13 +67,23 @@ struct Mol {
 
 // rigid_water.cpp:61-116 for one molecule.  Returns iterations, -1 (no
 // convergence) or -2 (singular denominator).
+// The reference bond vectors and the inverse-mass sums do not change during the
+// iterations; they are formed once, with the same operations, before the sweeps.
 __device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const RigidArgs& a,
                               const Fold3& f3) {
+    double b[3][3], two_inv_mass[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int i = cons_i(c), j = cons_j(c);
+        min_image_wrapped(f3, ref.x[i], ref.y[i], ref.z[i], ref.x[j], ref.y[j], ref.z[j], b[c][0],
+                          b[c][1], b[c][2]);
+        two_inv_mass[c] = __dmul_rn(2.0, __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j])));
+    }
     for (int it = 0; it < a.max_iterations; ++it) {
         double worst = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const int i = kCons[c][0], j = kCons[c][1];
+            const int i = cons_i(c), j = cons_j(c);
             const double d2 = a.target2[c];
             double ax, ay, az;
             min_image_wrapped(f3, r.x[i], r.y[i], r.z[i], r.x[j], r.y[j], r.z[j], ax, ay, az);
@@ -78,12 +91,8 @@ __device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const R
             const double violation = __ddiv_rn(fabs(s), d2);
             if (violation > worst) worst = violation;
             if (violation <= a.tolerance) continue;
-            double bx, by, bz;
-            min_image_wrapped(f3, ref.x[i], ref.y[i], ref.z[i], ref.x[j], ref.y[j], ref.z[j], bx,
-                              by, bz);
-            const double inv_mass_sum = __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j]));
-            const double denom =
-                __dmul_rn(__dmul_rn(2.0, inv_mass_sum), dot_exact(ax, ay, az, bx, by, bz));
+            const double bx = b[c][0], by = b[c][1], bz = b[c][2];
+            const double denom = __dmul_rn(two_inv_mass[c], dot_exact(ax, ay, az, bx, by, bz));
             if (fabs(denom) < 1e-30) return -2;
             const double g = __ddiv_rn(s, denom);
             const double gi = __ddiv_rn(g, m[i]), gj = __ddiv_rn(g, m[j]);
@@ -246,24 +255,33 @@ __device__ __forceinline__ int constrain_positions(Mol& r, const Mol& ref, const
 }
 
 // rigid_water.cpp:118-161 for one molecule.
+// Positions are fixed during the iterations: the bond vectors, their squared
+// lengths times the inverse-mass sums, are formed once before the sweeps.
 __device__ int rattle_molecule(const Mol& r, Mol& v, const double m[3], const RigidArgs& a,
                                const Fold3& f3) {
+    double b[3][3], mass_norm[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int i = cons_i(c), j = cons_j(c);
+        min_image_wrapped(f3, r.x[i], r.y[i], r.z[i], r.x[j], r.y[j], r.z[j], b[c][0], b[c][1],
+                          b[c][2]);
+        const double inv_mass_sum = __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j]));
+        mass_norm[c] = __dmul_rn(inv_mass_sum, norm2_exact(b[c][0], b[c][1], b[c][2]));
+    }
     for (int it = 0; it < a.max_iterations; ++it) {
         double worst = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const int i = kCons[c][0], j = kCons[c][1];
+            const int i = cons_i(c), j = cons_j(c);
             const double d2 = a.target2[c];
-            double ax, ay, az;
-            min_image_wrapped(f3, r.x[i], r.y[i], r.z[i], r.x[j], r.y[j], r.z[j], ax, ay, az);
+            const double ax = b[c][0], ay = b[c][1], az = b[c][2];
             const double ux = __dsub_rn(v.x[i], v.x[j]), uy = __dsub_rn(v.y[i], v.y[j]),
                          uz = __dsub_rn(v.z[i], v.z[j]);
             const double rv = dot_exact(ax, ay, az, ux, uy, uz);
             const double scaled = __ddiv_rn(fabs(rv), d2);
             if (scaled > worst) worst = scaled;
             if (scaled <= a.tolerance) continue;
-            const double inv_mass_sum = __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j]));
-            const double k = __ddiv_rn(rv, __dmul_rn(inv_mass_sum, norm2_exact(ax, ay, az)));
+            const double k = __ddiv_rn(rv, mass_norm[c]);
             const double ki = __ddiv_rn(k, m[i]), kj = __ddiv_rn(k, m[j]);
             v.x[i] = __dsub_rn(v.x[i], __dmul_rn(ax, ki));
             v.y[i] = __dsub_rn(v.y[i], __dmul_rn(ay, ki));
@@ -517,6 +535,76 @@ int status_to_error(md_context* ctx) {
     return MD_OK;
 }
 
+// A fused loop of constrained steps with SPC/E forces
+// (constrained_velocity_verlet.hpp:27-57, the Ewald sum between the halves),
+// every launch on the context's stream and no host synchronisation per step.
+struct SpceLoop {
+    md_integrator* it = nullptr;
+    md_system* sys = nullptr;
+    md_ewald* ff = nullptr;
+    NhcState* nhc = nullptr;
+    int64_t nmol = 0;
+    int g = 1;
+    double elrc = 0.0, self_coef = 0.0;
+};
+
+int spce_loop_begin(md_integrator* it, md_system* sys, md_ewald* ff, const char* who, SpceLoop& L) {
+    if (it->kind < 3) return fail(MD_ERR_INVALID_ARGUMENT, "%s: needs a constrained integrator", who);
+    MDB_TRY(check_triples(sys, who));
+    // Forces are made current on entry; this also builds the force field's
+    // neighbour list and topology once, host-side.
+    double e0, parts[8];
+    MDB_TRY(md_spce_compute(ff, sys, 1, &e0, parts));
+    MDB_TRY(ensure_counters(it));
+    double alpha = 0.0;
+    MDB_TRY(md_ewald_alpha(ff, &alpha));
+    L.it = it;
+    L.sys = sys;
+    L.ff = ff;
+    L.elrc = parts[1];
+    L.self_coef = -md_coulomb_prefactor() * alpha / std::sqrt(kPi);
+    L.nhc = it->kind == 4 ? it->chain_state.as<NhcState>() : nullptr;
+    L.nmol = sys->n / 3;
+    L.g = grid_for(std::max<int64_t>(L.nmol, 1), kBlock);
+    if (L.nhc) MDB_TRY(system_kinetic_async(sys, kResKE));
+    return MD_OK;
+}
+
+// One step; `first` feeds the chain the entry kinetic energy, `row` (device,
+// or null) receives [energy, virial, kinetic, conserved].  The step's kinetic
+// energy is left in the kResKE result slot.
+int spce_step_async(SpceLoop& L, bool first, double* row) {
+    md_system* sys = L.sys;
+    md_integrator* it = L.it;
+    md_context* ctx = sys->ctx;
+    if (L.nhc) MDB_TRY(nhc_pre_async(it, ctx, first ? ctx_result(ctx, kResKE) : nullptr));
+    if (L.nmol > 0) {
+        k_cvv_pre<<<grid_for(L.nmol, kBlock), kBlock, 0, ctx->stream>>>(
+            sys->cur, sys->slot, L.nmol, cvv_args(it, sys), L.nhc, it->counters.as<int>(),
+            ctx->d_status);
+        ++ctx->launches;
+    }
+    MDB_TRY(ewald_eval_async(L.ff, sys, 1, true));
+    k_spce_total<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEwald), L.elrc, L.self_coef,
+                                           ctx_result(ctx, kResEnergy));
+    double* part;  // fetched after the Ewald sum, which may grow the partials
+    MDB_TRY(ctx_partials(ctx, static_cast<size_t>(L.g), &part));
+    k_cvv_post<<<L.g, kBlock, 0, ctx->stream>>>(sys->cur, sys->slot, L.nmol, cvv_args(it, sys),
+                                               it->counters.as<int>() + 1, ctx->d_status, part,
+                                               ctx_counter(ctx, 8), ctx_result(ctx, kResKE));
+    ctx->launches += 2;
+    if (L.nhc) MDB_TRY(nhc_post_async(it, ctx, ctx_result(ctx, kResKE)));
+    if (row) MDB_TRY(record_async(ctx, ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE), L.nhc, row));
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+// apps/water_rdf.cpp:211 summed on the device: acc += 2 KE / dof (system.cpp:133-135),
+// one launch per step so the additions run in step order.
+__global__ void k_sum_temperature(const double* __restrict__ ke, double dof, double* acc) {
+    acc[0] += 2.0 * ke[0] / dof;
+}
+
 }  // namespace
 
 int constrained_pre_force(md_integrator* it, md_system* sys) {
@@ -699,54 +787,72 @@ int md_integrator_iterations(md_integrator* it, int* shake, int* rattle) {
 // Fused device loop of a constrained integrator with SPC/E forces.
 int md_run_spce(md_integrator* it, md_system* sys, md_ewald* ff, int64_t steps, double* thermo) {
     if (!it || !sys || !ff) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_spce: NULL argument");
-    if (it->kind < 3) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_spce: needs a constrained integrator");
     if (steps < 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_run_spce: steps < 0");
-    MDB_TRY(check_triples(sys, "md_run_spce"));
+    SpceLoop L;
+    MDB_TRY(spce_loop_begin(it, sys, ff, "md_run_spce", L));
     md_context* ctx = sys->ctx;
-    // Forces are made current on entry; this also builds the force field's
-    // neighbour list and topology once, host-side.
-    double e0, parts[8];
-    MDB_TRY(md_spce_compute(ff, sys, 1, &e0, parts));
-    MDB_TRY(ensure_counters(it));
-    double alpha = 0.0;
-    MDB_TRY(md_ewald_alpha(ff, &alpha));
-    const double elrc = parts[1];
-    const double self_coef = -md_coulomb_prefactor() * alpha / std::sqrt(kPi);
     DevBuf rows;
     if (thermo && steps > 0) MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
-    NhcState* nhc = it->kind == 4 ? it->chain_state.as<NhcState>() : nullptr;
-    const int64_t nmol = sys->n / 3;
-    if (nhc) MDB_TRY(system_kinetic_async(sys, kResKE));
-    const int g = grid_for(std::max<int64_t>(nmol, 1), kBlock);
-    double* part;
-    MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
-    for (int64_t k = 0; k < steps; ++k) {
-        if (nhc) MDB_TRY(nhc_pre_async(it, ctx, k == 0 ? ctx_result(ctx, kResKE) : nullptr));
-        if (nmol > 0) {
-            k_cvv_pre<<<grid_for(nmol, kBlock), kBlock, 0, ctx->stream>>>(
-                sys->cur, sys->slot, nmol, cvv_args(it, sys), nhc, it->counters.as<int>(),
-                ctx->d_status);
-            ++ctx->launches;
-        }
-        MDB_TRY(ewald_eval_async(ff, sys, 1, true));
-        k_spce_total<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEwald), elrc, self_coef,
-                                               ctx_result(ctx, kResEnergy));
-        k_cvv_post<<<g, kBlock, 0, ctx->stream>>>(sys->cur, sys->slot, nmol, cvv_args(it, sys),
-                                                 it->counters.as<int>() + 1, ctx->d_status, part,
-                                                 ctx_counter(ctx, 8), ctx_result(ctx, kResKE));
-        ctx->launches += 2;
-        if (nhc) MDB_TRY(nhc_post_async(it, ctx, ctx_result(ctx, kResKE)));
-        if (rows.ptr)
-            MDB_TRY(record_async(ctx, ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE), nhc,
-                                 rows.as<double>() + 4 * k));
-        MDB_CHECK_LAUNCH();
-    }
-    if (nhc && steps > 0) MDB_TRY(nhc_apply_scale_async(it, sys));
+    for (int64_t k = 0; k < steps; ++k)
+        MDB_TRY(spce_step_async(L, k == 0, rows.ptr ? rows.as<double>() + 4 * k : nullptr));
+    if (L.nhc && steps > 0) MDB_TRY(nhc_apply_scale_async(it, sys));
     if (rows.ptr)
         MDB_CUDA(cudaMemcpyAsync(thermo, rows.ptr, sizeof(double) * 4 * static_cast<size_t>(steps),
                                  cudaMemcpyDeviceToHost, ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
     rows.release();
+    MDB_TRY(status_to_error(ctx));
+    return ctx_check_status(ctx);
+}
+
+int md_water_rdf_run(md_integrator* it, md_system* sys, md_ewald* ff, md_rdf* rdf,
+                     double temperature, int64_t dof, int64_t equilibrate, int64_t rescale_every,
+                     int64_t production, int64_t sample_every, double* mean_temperature) {
+    if (!it || !sys || !ff || !rdf)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_water_rdf_run: NULL argument");
+    if (it->kind != 3)
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "md_water_rdf_run: needs a ConstrainedVelocityVerlet integrator");
+    if (dof < 1 || equilibrate < 0 || production < 0 || rescale_every < 1 || sample_every < 1)
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "md_water_rdf_run: dof, rescale_every, sample_every >= 1; step counts >= 0");
+    SpceLoop L;
+    MDB_TRY(spce_loop_begin(it, sys, ff, "md_water_rdf_run", L));
+    md_context* ctx = sys->ctx;
+    DevBuf acc;
+    MDB_TRY(acc.ensure(sizeof(double)));
+    MDB_CUDA(cudaMemsetAsync(acc.ptr, 0, sizeof(double), ctx->stream));
+    // apps/water_rdf.cpp:188-200: every rescale_every steps the velocities are
+    // scaled toward the target and put back on the constraint surface (RATTLE's
+    // velocity half, rigid_water.cpp:107-162, as constrainVelocities does).
+    for (int64_t step = 0; step < equilibrate; ++step) {
+        MDB_TRY(spce_step_async(L, step == 0, nullptr));
+        if ((step + 1) % rescale_every == 0) {
+            MDB_TRY(md_system_rescale_temperature(sys, dof, temperature));
+            if (L.nmol > 0) {
+                k_rattle<<<grid_for(L.nmol, kBlock), kBlock, 0, ctx->stream>>>(
+                    sys->cur, sys->slot, L.nmol, rigid_args(it->rigid), box_of(sys),
+                    it->counters.as<int>() + 1, ctx->d_status);
+                ++ctx->launches;
+                MDB_CHECK_LAUNCH();
+            }
+        }
+    }
+    // apps/water_rdf.cpp:207-216: NVE production; the temperature of every
+    // step is summed, and the oxygens (first site of each O, H, H triple) are
+    // binned every sample_every steps.
+    for (int64_t step = 0; step < production; ++step) {
+        MDB_TRY(spce_step_async(L, equilibrate == 0 && step == 0, nullptr));
+        k_sum_temperature<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResKE), static_cast<double>(dof),
+                                                    acc.as<double>());
+        ++ctx->launches;
+        if ((step + 1) % sample_every == 0) MDB_TRY(rdf_accumulate_async(rdf, sys, 0, 3));
+    }
+    double sum = 0.0;
+    MDB_CUDA(cudaMemcpyAsync(&sum, acc.ptr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    acc.release();
+    if (mean_temperature) *mean_temperature = production > 0 ? sum / static_cast<double>(production) : 0.0;
     MDB_TRY(status_to_error(ctx));
     return ctx_check_status(ctx);
 }

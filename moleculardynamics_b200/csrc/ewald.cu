@@ -368,19 +368,29 @@ k_recip_force(const double4* __restrict__ pos, const double* __restrict__ q, int
     part[blockIdx.y * n + s] = make_double4(fx, fy, fz, 0.0);
 }
 
-// Adds the slices' partial k-space forces (CHARGE: charge gradients) in order.
+// Adds the slices' partial k-space forces (CHARGE: charge gradients), one warp
+// per site: lane l sums slices l, l + 32, ... in order, then the lanes combine
+// by a fixed butterfly, so the result does not depend on scheduling.
 template <bool CHARGE>
 __global__ void k_recip_sum(const double4* __restrict__ part, int slices, int64_t n, double* fxo,
                             double* fyo, double* fzo, double* dq) {
-    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (s >= n) return;
+    const int64_t s = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= n) return;  // whole warps leave together
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int k = 0; k < slices; ++k) {
+    for (int k = lane; k < slices; k += 32) {
         const double4 v = part[k * n + s];
         fx += v.x;
         fy += v.y;
         fz += v.z;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (lane != 0) return;
     if (CHARGE) {
         dq[s] += fx;
     } else {
@@ -497,15 +507,36 @@ k_ewald_real_hvp(const double4* __restrict__ pos, const double* __restrict__ q,
     out[i] = make_double4(hx, hy, hz, 0.0);
 }
 
+// Threads per atom of the real-space pass: the fewest (at least 4) that put
+// about a thousand threads on every SM, so that a few thousand sites still
+// spread over the whole GPU instead of a dozen SMs; at most a warp.
+int real_tpa(const md_context* ctx, int64_t n) {
+    const int64_t want = 1024 * static_cast<int64_t>(ctx->sm_count);
+    int tpa = 4;
+    while (tpa < 32 && n * tpa < want) tpa *= 2;
+    return tpa;
+}
+
 template <int TPA>
-void launch_real(md_system* sys, md_verlet* v, const RealArgs& a, int mode, double* part,
-                 unsigned* ticket, double* out) {
+void launch_real_t(md_system* sys, md_verlet* v, const RealArgs& a, int mode, double* fx,
+                   double* fy, double* fz, double* part, unsigned* ticket, double* out) {
     const int64_t threads = std::max<int64_t>(sys->n * TPA, 1);
     k_ewald_real<TPA><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
         sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
         v->stride, sys->n, Box3{{sys->box[0], sys->box[1], sys->box[2]},
                                 {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}},
-        a, mode, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+        a, mode, fx, fy, fz, part, ticket, out);
+}
+
+// mode 1 writes (fx, fy, fz), 2 adds to them; part holds 4 doubles per block.
+void launch_real(md_system* sys, md_verlet* v, const RealArgs& a, int mode, int tpa, double* fx,
+                 double* fy, double* fz, double* part, unsigned* ticket, double* out) {
+    switch (tpa) {
+        case 32: launch_real_t<32>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        case 16: launch_real_t<16>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        case 8: launch_real_t<8>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        default: launch_real_t<4>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+    }
 }
 
 }  // namespace
@@ -682,13 +713,13 @@ int recip_force_async(md_ewald* ew, md_system* sys, const KArgs& ka, bool charge
         k_recip_force<true><<<grid, kBlock, 0, ctx->stream>>>(
             sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines, per,
             ew->sk.as<double2>(), part);
-        k_recip_sum<true><<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+        k_recip_sum<true><<<grid_for(32 * n, kBlock), kBlock, 0, ctx->stream>>>(
             part, slices, n, nullptr, nullptr, nullptr, dq);
     } else {
         k_recip_force<false><<<grid, kBlock, 0, ctx->stream>>>(
             sys->cur.pos, sys->cur.charge, n, ka, ew->lines.as<int4>(), ew->nlines, per,
             ew->sk.as<double2>(), part);
-        k_recip_sum<false><<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+        k_recip_sum<false><<<grid_for(32 * n, kBlock), kBlock, 0, ctx->stream>>>(
             part, slices, n, sys->cur.fx, sys->cur.fy, sys->cur.fz, nullptr);
     }
     ctx->launches += 2;
@@ -747,24 +778,23 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
     const Box3 box{{sys->box[0], sys->box[1], sys->box[2]},
                    {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}};
     double* part;
-    const int64_t real_threads = std::max<int64_t>(n * 4, 1);
+    const int tpa = real_tpa(ctx, n);
+    const int64_t real_threads = std::max<int64_t>(n * tpa, 1);
     MDB_TRY(ctx_partials(ctx, 4 * static_cast<size_t>(grid_for(real_threads, kBlock)), &part));
     // real space (+ O-O LJ): with forces it writes (mode 1) or adds (mode 2); for
     // energies only it writes into the scratch force sink of a zero-force pass.
     ctx_time_begin(ctx, MD_KERNEL_EWALD_REAL);
     if (mode == 0) {
         // energies only: run the pair pass without touching forces by pointing the
-        // sink at the partials' tail (never read back)
+        // sink at scratch (never read back)
         double* sink;
         MDB_TRY(ctx_scratch(ctx, 3 * sizeof(double) * static_cast<size_t>(std::max<int64_t>(n, 1)),
                             reinterpret_cast<void**>(&sink)));
-        const int64_t threads = std::max<int64_t>(n * 4, 1);
-        k_ewald_real<4><<<grid_for(threads, kBlock), kBlock, 0, ctx->stream>>>(
-            sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
-            v->stride, n, box, a, 1, sink, sink + n, sink + 2 * n, part, ctx_counter(ctx, 4),
-            res + kEwReal);
+        launch_real(sys, v, a, 1, tpa, sink, sink + n, sink + 2 * n, part, ctx_counter(ctx, 4),
+                    res + kEwReal);
     } else {
-        launch_real<4>(sys, v, a, mode, part, ctx_counter(ctx, 4), res + kEwReal);
+        launch_real(sys, v, a, mode, tpa, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
+                    ctx_counter(ctx, 4), res + kEwReal);
     }
     ctx_time_end(ctx, MD_KERNEL_EWALD_REAL);
     // intramolecular correction

@@ -168,6 +168,11 @@ struct CellGrid {
 // (ncells+1) the start of each rank's range.  Pure function of the positions.
 int cell_sort(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_start);
 
+// One RDF frame of the atoms first, first + stride, ... added to the device
+// histogram, no host synchronisation; rdf_sync refreshes the host counts.
+int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t stride);
+int rdf_sync(const md_rdf* r);
+
 }  // namespace mdb
 
 struct md_cells {

@@ -97,4 +97,15 @@ int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed,
     return n;
 }
 
+// `count` consecutive Rng(seed).normal() draws (util/random.hpp:37-76), e.g.
+// the thermal velocities v_i = sqrt(T / m_i) * (n0, n1, n2) that
+// apps/water_rdf.cpp:167-170 draws atom by atom.  Returns count or
+// MD_ERR_INVALID_ARGUMENT.
+int64_t md_rng_normals(uint64_t seed, int64_t count, double* out) {
+    if (count < 0 || (count > 0 && !out)) return MD_ERR_INVALID_ARGUMENT;
+    LatticeRng rng(seed);
+    for (int64_t k = 0; k < count; ++k) out[k] = rng.normal();
+    return count;
+}
+
 }  // extern "C"

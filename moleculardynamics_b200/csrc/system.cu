@@ -137,6 +137,21 @@ __global__ void k_sub_com(md_atoms a, int64_t n, const double* __restrict__ pm) 
     a.vz[k] -= pm[2] / total;
 }
 
+// apps/water_rdf.cpp:186-195: t = 2 KE / dof (system.cpp:133-135); when t > 0,
+// v *= sqrt(target / t).  KE comes from the device result slot of k_kinetic,
+// so the rescale needs no host round trip.
+__global__ void k_rescale_temperature(md_atoms a, int64_t n, const double* __restrict__ ke,
+                                      double dof, double target) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const double t = 2.0 * ke[0] / dof;
+    if (!(t > 0.0)) return;
+    const double scale = sqrt(target / t);
+    a.vx[k] *= scale;
+    a.vy[k] *= scale;
+    a.vz[k] *= scale;
+}
+
 int reduce_grid(md_system* sys) {
     // Enough blocks to fill the GPU, few enough partials to re-reduce cheaply.
     const int64_t want = (sys->n + kBlock - 1) / kBlock;
@@ -380,6 +395,19 @@ int md_system_remove_com_motion(md_system* sys) {
     k_sub_com<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n,
                                                                     ctx_result(ctx, kResMomentum));
     ctx->launches += 2;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int md_system_rescale_temperature(md_system* sys, int64_t dof, double target) {
+    if (!sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_system_rescale_temperature: NULL");
+    if (dof < 1 || !(target >= 0.0))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_system_rescale_temperature: dof >= 1, target >= 0");
+    if (sys->n == 0) return MD_OK;
+    MDB_TRY(system_kinetic_async(sys, kResKE));
+    k_rescale_temperature<<<grid_for(sys->n, kBlock), kBlock, 0, sys->ctx->stream>>>(
+        sys->cur, sys->n, ctx_result(sys->ctx, kResKE), static_cast<double>(dof), target);
+    ++sys->ctx->launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }

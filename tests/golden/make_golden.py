@@ -161,15 +161,51 @@ def fcc_fixture(R):
     return out
 
 
+def water_rdf_fixture(ref_root, R):
+    """The reference's recorded water_rdf run (results/water_rdf.csv, written by
+    apps/water_rdf.cpp:274-297): its header values and g_OO(r), plus the first
+    normals of Rng(7001) (the app's velocity seed) from the compiled reference."""
+    head, rows = {}, []
+    for line in open(os.path.join(ref_root, "results", "water_rdf.csv")):
+        line = line.strip()
+        if line.startswith("# "):
+            key, _, val = line[2:].partition(": ")
+            try:
+                head[key] = float(val)
+            except ValueError:
+                pass
+        elif line and line[0].isdigit():
+            rows.append([float(v) for v in line.split(",")])
+    rows = np.array(rows)
+    assert rows.shape == (200, 2), rows.shape
+    keys = ["molecules", "box_length_angstrom", "density_g_per_cm3", "target_temperature_K",
+            "mean_production_temperature_K", "dt_fs", "equilibration_steps", "production_steps",
+            "rdf_frames", "bin_width_angstrom", "first_peak_bin_r_angstrom", "first_peak_bin_g",
+            "first_peak_r_angstrom", "first_peak_g", "tail_mean_g_beyond_8.5A", "wall_seconds"]
+    normals = np.zeros(2700)
+    R.ref_rng_normals(7001, _p(normals), normals.size)
+    return {"r": rows[:, 0], "g": rows[:, 1], "keys": np.array(keys),
+            "values": np.array([head[k] for k in keys]), "normals7001": normals}
+
+
+FIXTURES = {
+    "nist_lj.npz": lambda root, R: lj_fixture(root, R),
+    "nist_spce.npz": lambda root, R: spce_fixture(root, R),
+    "fcc_lj.npz": lambda root, R: fcc_fixture(R),
+    "water_rdf_ref.npz": water_rdf_fixture,
+}
+
+
 def main():
+    """make_golden.py [REF_ROOT [FIXTURE ...]]: every fixture, or the named ones."""
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    names = sys.argv[2:] or sorted(FIXTURES)
     O.build(ref_root)
     R = O.ref()
     if R is None:
         raise SystemExit("reference library not built (oracle/_ref/libmoldyn_ref.so missing)")
-    np.savez_compressed(os.path.join(HERE, "nist_lj.npz"), **lj_fixture(ref_root, R))
-    np.savez_compressed(os.path.join(HERE, "nist_spce.npz"), **spce_fixture(ref_root, R))
-    np.savez_compressed(os.path.join(HERE, "fcc_lj.npz"), **fcc_fixture(R))
+    for name in names:
+        np.savez_compressed(os.path.join(HERE, name), **FIXTURES[name](ref_root, R))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
