@@ -152,26 +152,27 @@ done:
     rdf_flush(a, s_hist, hist);
 }
 
-// Small boxes (fewer than 3 cells of width rMax per side): every pair, atoms of
-// the other side staged through shared memory in tiles.
+// Small boxes (fewer than 3 cells of width rMax per side): every pair.  Block
+// (x, y) pairs the atoms of block x with one span of the other side, staged in
+// shared memory; the spans are short enough to give every SM work even for a
+// few hundred atoms.
 __global__ void __launch_bounds__(kRdfBlock)
-k_rdf_brute(const double4* __restrict__ pos, int64_t n, RdfArgs a, unsigned long long* hist) {
+k_rdf_brute(const double4* __restrict__ pos, int64_t n, int span, RdfArgs a,
+            unsigned long long* hist) {
     extern __shared__ unsigned s_hist[];
     __shared__ double4 tile[kRdfBlock];
     rdf_zero(a, s_hist);
     const Fold3 f3 = fold3_of(a.box);
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const double4 p = i < n ? pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
-    for (int64_t base = 0; base < n; base += kRdfBlock) {
-        __syncthreads();
-        if (base + threadIdx.x < n) tile[threadIdx.x] = pos[base + threadIdx.x];
-        __syncthreads();
-        const int lim = static_cast<int>(n - base < kRdfBlock ? n - base : kRdfBlock);
-        if (i < n && rdf_selected(a, p.w))
-            for (int t = 0; t < lim; ++t)
-                if (tile[t].w > p.w && rdf_selected(a, tile[t].w))
-                    rdf_count(a, s_hist, hist, rdf_bin(a, f3, p, tile[t]));
-    }
+    const int64_t base = blockIdx.y * static_cast<int64_t>(span);
+    const int lim = static_cast<int>(n - base < span ? n - base : span);
+    if (threadIdx.x < lim) tile[threadIdx.x] = pos[base + threadIdx.x];
+    __syncthreads();
+    if (i < n && rdf_selected(a, p.w))
+        for (int t = 0; t < lim; ++t)
+            if (tile[t].w > p.w && rdf_selected(a, tile[t].w))
+                rdf_count(a, s_hist, hist, rdf_bin(a, f3, p, tile[t]));
     rdf_flush(a, s_hist, hist);
 }
 
@@ -456,8 +457,19 @@ int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t strid
             k_rdf_cells<<<grid_for(n, kRdfBlock), kRdfBlock, shm, ctx->stream>>>(
                 sys->cur.pos, n, g, a, r->hist.as<unsigned long long>());
         } else {
-            k_rdf_brute<<<grid_for(n, kRdfBlock), kRdfBlock, shm, ctx->stream>>>(
-                sys->cur.pos, n, a, r->hist.as<unsigned long long>());
+            // spans of a multiple of 32 atoms, enough of them for two blocks per SM
+            const int64_t xblocks = grid_for(n, kRdfBlock);
+            const int64_t want = (2 * static_cast<int64_t>(ctx->sm_count) + xblocks - 1) / xblocks;
+            int64_t span = (n + want - 1) / want;
+            span = std::min<int64_t>(kRdfBlock, std::max<int64_t>(32, (span + 31) / 32 * 32));
+            const int64_t spans = (n + span - 1) / span;
+            if (spans > 65535)
+                return fail(MD_ERR_INVALID_ARGUMENT,
+                            "Rdf: %lld atoms in a box under 3 rMax wide exceed the all-pairs pass",
+                            static_cast<long long>(n));
+            k_rdf_brute<<<dim3(static_cast<unsigned>(xblocks), static_cast<unsigned>(spans)),
+                          kRdfBlock, shm, ctx->stream>>>(sys->cur.pos, n, static_cast<int>(span), a,
+                                                         r->hist.as<unsigned long long>());
         }
         ++ctx->launches;
         MDB_CHECK_LAUNCH();

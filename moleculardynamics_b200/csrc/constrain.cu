@@ -10,6 +10,7 @@
 // and the reference's iteration count is the maximum over molecules.  Each update
 // uses the reference's operation order, so results are bit-identical to it.
 #include <cmath>
+#include <limits>
 #include <new>
 
 #include "md_device.cuh"
@@ -37,17 +38,39 @@ __host__ __device__ constexpr int cons_j(int c) { return c == 0 ? 1 : 2; }
 
 struct RigidArgs {
     double target2[3];  // squared O-H, O-H, H-H distances
+    // within[c]: the largest x >= 0 whose rounded quotient x / target2[c] is at
+    // most the tolerance, so that |s| / d2 <= tolerance (rigid_water.cpp:85-91,
+    // 139-146) is decided by |s| <= within[c] without the division
+    double within[3];
     double tolerance;
     int max_iterations;
     int settle;         // closed-form SETTLE instead of SHAKE / RATTLE iterations
     double oh, hh;
 };
 
+// Largest x >= 0 with RN(x / d2) <= tol (IEEE division on the host, rounded to
+// nearest like __ddiv_rn).  x -> RN(x / d2) is non-decreasing, so the set of
+// such x is an interval [0, within] and |s| / d2 <= tol exactly when
+// |s| <= within; a NaN fails both tests, an infinity fails both.
+double tolerance_bound(double d2, double tol) {
+    if (!(d2 > 0.0) || !(tol >= 0.0)) return -1.0;  // nothing passes; the division decides
+    double x = tol * d2;
+    if (!std::isfinite(x)) x = std::numeric_limits<double>::max();
+    for (int k = 0; k < 64 && x > 0.0 && x / d2 > tol; ++k) x = std::nextafter(x, 0.0);
+    for (int k = 0; k < 64; ++k) {
+        const double up = std::nextafter(x, std::numeric_limits<double>::infinity());
+        if (!std::isfinite(up) || up / d2 > tol) break;
+        x = up;
+    }
+    return x / d2 <= tol ? x : -1.0;
+}
+
 RigidArgs rigid_args(const md_rigid& rw) {
     RigidArgs a;
     a.target2[0] = rw.oh * rw.oh;
     a.target2[1] = rw.oh * rw.oh;
     a.target2[2] = rw.hh * rw.hh;
+    for (int c = 0; c < 3; ++c) a.within[c] = tolerance_bound(a.target2[c], rw.tolerance);
     a.tolerance = rw.tolerance;
     a.max_iterations = rw.max_iterations;
     a.settle = rw.settle ? 1 : 0;
@@ -80,7 +103,7 @@ __device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const R
         two_inv_mass[c] = __dmul_rn(2.0, __dadd_rn(__ddiv_rn(1.0, m[i]), __ddiv_rn(1.0, m[j])));
     }
     for (int it = 0; it < a.max_iterations; ++it) {
-        double worst = 0.0;
+        bool open = false;  // some violation above the tolerance (worst > tolerance)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const int i = cons_i(c), j = cons_j(c);
@@ -88,9 +111,8 @@ __device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const R
             double ax, ay, az;
             min_image_wrapped(f3, r.x[i], r.y[i], r.z[i], r.x[j], r.y[j], r.z[j], ax, ay, az);
             const double s = __dsub_rn(norm2_exact(ax, ay, az), d2);
-            const double violation = __ddiv_rn(fabs(s), d2);
-            if (violation > worst) worst = violation;
-            if (violation <= a.tolerance) continue;
+            if (fabs(s) > a.within[c]) open = true;
+            if (fabs(s) <= a.within[c]) continue;
             const double bx = b[c][0], by = b[c][1], bz = b[c][2];
             const double denom = __dmul_rn(two_inv_mass[c], dot_exact(ax, ay, az, bx, by, bz));
             if (fabs(denom) < 1e-30) return -2;
@@ -103,7 +125,7 @@ __device__ int shake_molecule(Mol& r, const Mol& ref, const double m[3], const R
             r.y[j] = __dadd_rn(r.y[j], __dmul_rn(by, gj));
             r.z[j] = __dadd_rn(r.z[j], __dmul_rn(bz, gj));
         }
-        if (worst <= a.tolerance) return it + 1;
+        if (!open) return it + 1;
     }
     return -1;
 }
@@ -269,18 +291,16 @@ __device__ int rattle_molecule(const Mol& r, Mol& v, const double m[3], const Ri
         mass_norm[c] = __dmul_rn(inv_mass_sum, norm2_exact(b[c][0], b[c][1], b[c][2]));
     }
     for (int it = 0; it < a.max_iterations; ++it) {
-        double worst = 0.0;
+        bool open = false;  // some |r.v| / d2 above the tolerance
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const int i = cons_i(c), j = cons_j(c);
-            const double d2 = a.target2[c];
             const double ax = b[c][0], ay = b[c][1], az = b[c][2];
             const double ux = __dsub_rn(v.x[i], v.x[j]), uy = __dsub_rn(v.y[i], v.y[j]),
                          uz = __dsub_rn(v.z[i], v.z[j]);
             const double rv = dot_exact(ax, ay, az, ux, uy, uz);
-            const double scaled = __ddiv_rn(fabs(rv), d2);
-            if (scaled > worst) worst = scaled;
-            if (scaled <= a.tolerance) continue;
+            if (fabs(rv) > a.within[c]) open = true;
+            if (fabs(rv) <= a.within[c]) continue;
             const double k = __ddiv_rn(rv, mass_norm[c]);
             const double ki = __ddiv_rn(k, m[i]), kj = __ddiv_rn(k, m[j]);
             v.x[i] = __dsub_rn(v.x[i], __dmul_rn(ax, ki));
@@ -290,7 +310,7 @@ __device__ int rattle_molecule(const Mol& r, Mol& v, const double m[3], const Ri
             v.y[j] = __dadd_rn(v.y[j], __dmul_rn(ay, kj));
             v.z[j] = __dadd_rn(v.z[j], __dmul_rn(az, kj));
         }
-        if (worst <= a.tolerance) return it + 1;
+        if (!open) return it + 1;
     }
     return -1;
 }
