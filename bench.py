@@ -782,6 +782,10 @@ def run_water_arm(args):
     rw = md.RigidWater(1.0, 109.47, settle=args.settle)
     rw.constrain_velocities(s)
     ff = md.SpceForceField(cutoff=WATER_RC, kmax=WATER_KMAX, alpha=WATER_ALPHA, ctx=ctx)
+    if args.pme > 0:
+        ff.set_pme_spacing(w["box"], args.pme, args.pme_order)
+    recip = ("smooth PME, grid %dx%dx%d, B-spline order %d" % (*ff.pme_grid()[0], args.pme_order)
+             if args.pme > 0 else f"Ewald k-vector sums, kmax={WATER_KMAX}")
     dof = md.RigidWater.degrees_of_freedom(4096, True)
     md.ConstrainedNoseHooverChain(fs(0.5), rw, 298.0, fs(50.0), 3, dof).run(s, ff, args.equil_water)
     integ = md.ConstrainedNoseHooverChain(fs(2.0), rw, 298.0, fs(100.0), 3, dof)
@@ -814,7 +818,8 @@ def run_water_arm(args):
             "data": "synthetic: seeded rigid-water lattice, Maxwell-Boltzmann velocities, "
                     f"{args.equil_water} NHC steps of 0.5 fs",
             "config": dict(water_config(args.steps),
-                           constraints="SETTLE" if args.settle else "SHAKE/RATTLE"),
+                           constraints="SETTLE" if args.settle else "SHAKE/RATTLE",
+                           reciprocal=recip),
             "gpu_launches": int(launches),
             "nhc_extended_energy_drift_K": {"max_abs": float(np.max(np.abs(h - h[0]))),
                                             "relative": float(np.max(np.abs(h - h[0])) / abs(h[0]))},
@@ -1163,6 +1168,10 @@ def main():
                     metavar=("EQUIL", "PROD"),
                     help="water_rdf: protocol lengths (profiling configurations only; the "
                          "metric is quoted on the default 15000 10000)")
+    ap.add_argument("--pme", type=float, default=0.0, metavar="SPACING",
+                    help="water: smooth PME with grid cells of at most SPACING A instead of "
+                         "the k-vector sums")
+    ap.add_argument("--pme-order", type=int, default=6)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)

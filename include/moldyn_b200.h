@@ -257,6 +257,15 @@ MD_API int md_ewald_compute(md_ewald* ew, md_system* sys, int mode, double terms
                             double* virial);
 MD_API int md_ewald_alpha(const md_ewald* ew, double* alpha);          /* last alpha used */
 MD_API int md_ewald_kvector_count(const md_ewald* ew, int* count);     /* full k set */
+/* Smooth particle-mesh Ewald (Essmann et al., J. Chem. Phys. 103, 8577 (1995))
+ * for the reciprocal term instead of the k-vector sums of ewald.cpp:112-172:
+ * a kx x ky x kz charge grid (each in [2 order, 4096]) and cardinal B-splines of
+ * order 4, 6 or 8; kx = ky = kz = 0 returns to the k-vector sums.  The
+ * reference defers PME (no counterpart); real space, self and intramolecular
+ * terms are unchanged.  md_ewald_charge_gradient needs the k-vector sums. */
+MD_API int md_ewald_set_pme(md_ewald* ew, int kx, int ky, int kz, int order);
+/* The PME grid and order, zeros when the k-vector sums are in use. */
+MD_API int md_ewald_pme_grid(const md_ewald* ew, int k[3], int* order);
 
 /* SpceForceField(params, cutoff, kmax) (forcefield/spce_forcefield.hpp:31-33):
  * O-O Lennard-Jones (sigma_o, epsilon_o, truncated, with tail) + Ewald, on O,H,H

@@ -14,6 +14,7 @@ shape (N, 3) (positions, velocities, forces) or (N,) (masses, charges).
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -186,6 +187,8 @@ def _load():
         "md_ewald_compute": (C.c_int, [_vp, _vp, C.c_int, _d, _d]),
         "md_ewald_alpha": (C.c_int, [_vp, _d]),
         "md_ewald_kvector_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+        "md_ewald_set_pme": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "md_ewald_pme_grid": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "md_spce_create": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                      C.POINTER(_vp)]),
         "md_spce_compute": (C.c_int, [_vp, _vp, C.c_int, _d, _d]),
@@ -631,7 +634,46 @@ class EwaldTerms(dict):
         return self["real"] + self["reciprocal"] + self["self"] + self["intra"]
 
 
-class Ewald:
+def fft_size(at_least):
+    """The smallest n >= at_least whose prime factors are 2, 3, 5 and 7 (sizes
+    the 3-D FFTs of PME handle fastest)."""
+    n = max(1, int(at_least))
+    while True:
+        m = n
+        for p in (2, 3, 5, 7):
+            while m % p == 0:
+                m //= p
+        if m == 1:
+            return n
+        n += 1
+
+
+class _PmeMixin:
+    def set_pme(self, grid, order=6):
+        """Smooth PME (Essmann et al. 1995) for the reciprocal term instead of
+        the k-vector sums: grid is (kx, ky, kz) or one size for all axes; None
+        or 0 returns to the k-vector sums."""
+        if not grid:
+            k = (0, 0, 0)
+        elif np.isscalar(grid):
+            k = (int(grid),) * 3
+        else:
+            k = tuple(int(v) for v in grid)
+        _check(lib().md_ewald_set_pme(self._h, *k, int(order)))
+
+    def set_pme_spacing(self, box, spacing=1.0, order=6):
+        """PME with FFT-friendly grid sizes of at most `spacing` per grid cell."""
+        self.set_pme([fft_size(math.ceil(float(L) / spacing)) for L in np.asarray(box)], order)
+
+    def pme_grid(self):
+        """((kx, ky, kz), order), or ((0, 0, 0), 0) with the k-vector sums."""
+        k = (C.c_int * 3)()
+        o = C.c_int()
+        _check(lib().md_ewald_pme_grid(self._h, k, C.byref(o)))
+        return tuple(k), o.value
+
+
+class Ewald(_PmeMixin):
     """forcefield/ewald.hpp:49-68 plus alpha (<= 0: the reference's 5.6 / min L)."""
 
     def __init__(self, cutoff, kmax, alpha=0.0, ctx: Context | None = None, skin=1.0):
@@ -694,7 +736,7 @@ class SpceParameters:
     massHydrogen = 1.008
 
 
-class SpceForceField:
+class SpceForceField(_PmeMixin):
     """forcefield/spce_forcefield.hpp:25-41 (+ alpha)."""
 
     def __init__(self, cutoff=10.0, kmax=5, alpha=0.0, params=SpceParameters,

@@ -575,6 +575,7 @@ struct md_ewald {
     int nk = 0, nlines = 0;
     double last[kEwCount] = {0};
     double alpha = 0.0;
+    mdb::PmeState* pme = nullptr;  // reciprocal term by smooth PME instead of k-vector sums
 };
 
 namespace mdb {
@@ -769,7 +770,7 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
         MDB_TRY(ewald_list_gated(ew, sys));
     } else {
         MDB_TRY(ewald_topology(ew, sys));
-        MDB_TRY(ewald_kvectors(ew, sys->box, alpha));
+        if (!ew->pme) MDB_TRY(ewald_kvectors(ew, sys->box, alpha));
         MDB_TRY(ewald_list(ew, sys));
     }
     md_verlet* v = ew->list;
@@ -810,7 +811,10 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
     // reciprocal space
     ctx_time_begin(ctx, MD_KERNEL_EWALD_RECIP);
     const KArgs ka = kargs_of(ew, sys);
-    if (ew->nk > 0 && n > 0) {
+    if (ew->pme) {
+        MDB_TRY(pme_eval_async(ew->pme, sys, alpha, coulomb_prefactor(), mode, res + kEwRecip,
+                               ctx_counter(ctx, 12)));
+    } else if (ew->nk > 0 && n > 0) {
         const int kblocks = (ew->nk + kBlock - 1) / kBlock;
         // enough site slices to give every SM a few blocks
         int64_t slices = std::max<int64_t>(1, (4 * ctx->sm_count) / kblocks);
@@ -892,6 +896,10 @@ int md_ewald_create(md_context* ctx, double cutoff, int kmax, double alpha, md_e
 int md_ewald_destroy(md_ewald* ew) {
     if (!ew) return MD_OK;
     if (ew->list) md_verlet_destroy(ew->list);
+    if (ew->pme) {
+        cudaStreamSynchronize(ew->ctx->stream);
+        pme_destroy(ew->pme);
+    }
     ew->partner_off.release();
     ew->partner_idx.release();
     ew->kvec.release();
@@ -940,8 +948,48 @@ int upload_vec(md_system* sys, const double* u, double4* dev_orig, double4* dev)
 
 }  // namespace
 
+int md_ewald_set_pme(md_ewald* ew, int kx, int ky, int kz, int order) {
+    if (!ew) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_pme: NULL");
+    if (kx == 0 && ky == 0 && kz == 0) {  // back to the k-vector sums
+        if (ew->pme) {
+            cudaStreamSynchronize(ew->ctx->stream);
+            pme_destroy(ew->pme);
+            ew->pme = nullptr;
+        }
+        return MD_OK;
+    }
+    if (order != 4 && order != 6 && order != 8)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_pme: order must be 4, 6 or 8");
+    const int K[3] = {kx, ky, kz};
+    for (int d = 0; d < 3; ++d)
+        if (K[d] < 2 * order || K[d] > 4096)
+            return fail(MD_ERR_INVALID_ARGUMENT,
+                        "md_ewald_set_pme: grid sizes must lie in [2 * order, 4096]");
+    mdb::PmeState* s = nullptr;
+    MDB_TRY(pme_create(ew->ctx, K, order, &s));
+    if (ew->pme) {
+        cudaStreamSynchronize(ew->ctx->stream);
+        pme_destroy(ew->pme);
+    }
+    ew->pme = s;
+    return MD_OK;
+}
+
+int md_ewald_pme_grid(const md_ewald* ew, int k[3], int* order) {
+    if (!ew || !k || !order) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_pme_grid: NULL");
+    if (!ew->pme) {
+        k[0] = k[1] = k[2] = 0;
+        *order = 0;
+        return MD_OK;
+    }
+    return pme_grid(ew->pme, k, order);
+}
+
 int md_ewald_charge_gradient(md_ewald* ew, md_system* sys, double* dedq) {
     if (!ew || !sys || !dedq) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_charge_gradient: NULL");
+    if (ew->pme)
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "md_ewald_charge_gradient: needs the k-vector reciprocal sum (PME is set)");
     if (sys->ctx != ew->ctx)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_charge_gradient: context mismatch");
     const int64_t n = sys->n;

@@ -173,6 +173,16 @@ int cell_sort(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_start)
 int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t stride);
 int rdf_sync(const md_rdf* r);
 
+// Smooth particle-mesh Ewald reciprocal term (pme.cu): grid and cuFFT plans of
+// one Ewald handle.  pme_eval_async writes the reciprocal energy and virial trace
+// to out[0..1] (device) and, for mode != 0, adds the k-space forces.
+struct PmeState;
+int pme_create(md_context* ctx, const int K[3], int order, PmeState** out);
+void pme_destroy(PmeState* s);
+int pme_grid(const PmeState* s, int K[3], int* order);
+int pme_eval_async(PmeState* s, md_system* sys, double alpha, double coulomb, int mode, double* out,
+                   unsigned* ticket);
+
 }  // namespace mdb
 
 struct md_cells {

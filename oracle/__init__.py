@@ -551,3 +551,99 @@ def ref_vacf(frames, box, max_lag, dt):
     out, d = np.zeros(max_lag + 1), np.zeros(1)
     ref().ref_vacf(a.shape[0], a.shape[2], _p(_f64(box)), _p(a), max_lag, _p(out), dt, _p(d))
     return out, d[0]
+
+
+# ---------------------------------------------------------------------------
+# Smooth particle-mesh Ewald, restated in numpy from Essmann et al., J. Chem.
+# Phys. 103, 8577 (1995).  The reference has no PME (its phase-2 plan defers
+# it); this restatement is pinned by converging to the reference-pinned Ewald
+# sum above as the grid is refined, and is the checker of the device PME.
+# ---------------------------------------------------------------------------
+
+def _bspline_weights(w, p):
+    """c[:, j] = M_p(w + j) and d[:, j] = M_p'(w + j), j = 0..p-1 (cardinal
+    B-spline recursion, Essmann eq. 4.1 and 4.2)."""
+    w = np.asarray(w, dtype=np.float64)
+    c = np.zeros((w.size, p))
+    c[:, 0] = w
+    c[:, 1] = 1.0 - w
+    d = np.zeros((w.size, p))
+    if p == 2:
+        d[:, 0], d[:, 1] = 1.0, -1.0
+    for n in range(3, p + 1):
+        if n == p:
+            d = c - np.concatenate([np.zeros((w.size, 1)), c[:, :-1]], axis=1)
+        new = np.zeros_like(c)
+        for j in range(n):
+            x = w + j
+            lo = c[:, j - 1] if j > 0 else 0.0
+            new[:, j] = (x * c[:, j] + (n - x) * lo) / (n - 1)
+        c = new
+    return c, d
+
+
+def _bspline_moduli(K, p):
+    """|b(m)|^2 = 1 / |sum_{k=0}^{p-2} M_p(k+1) exp(2 pi i m k / K)|^2 (Essmann eq. 4.4)."""
+    ints, _ = _bspline_weights(np.array([0.0]), p)  # M_p(j), j = 0..p-1
+    mk = ints[0, 1:p]                                # M_p(1..p-1)
+    m = np.arange(K)[:, None]
+    k = np.arange(p - 1)[None, :]
+    s = np.sum(mk[None, :] * np.exp(2j * np.pi * m * k / K), axis=1)
+    mag = np.abs(s) ** 2
+    out = np.where(mag > 1e-10, 1.0 / np.where(mag > 1e-10, mag, 1.0), 0.0)
+    for i in np.nonzero(out == 0.0)[0]:
+        out[i] = 0.5 * (out[(i - 1) % K] + out[(i + 1) % K])
+    return out
+
+
+def pme_recip(pos, box, q, alpha, K, order):
+    """Reciprocal-space energy, virial trace and forces of smooth PME on a
+    K[0] x K[1] x K[2] grid with B-splines of `order`.  Returns (E, W, F)."""
+    pos, box, q = _f64(pos).reshape(-1, 3), _f64(box), _f64(q)
+    K = [int(k) for k in (K if np.ndim(K) else (K, K, K))]
+    n = pos.shape[0]
+    coulomb = lib().orc_coulomb_prefactor()
+    volume = float(np.prod(box))
+    frac = pos / box
+    frac = frac - np.floor(frac)
+    u = frac * np.array(K)
+    u = np.where(u >= np.array(K), u - np.array(K), u)
+    i0 = np.floor(u).astype(np.int64)
+    w = u - i0
+    cs, ds = [], []
+    for a in range(3):
+        c, d = _bspline_weights(w[:, a], order)
+        cs.append(c)
+        ds.append(d)
+    j = np.arange(order)
+    gx = (i0[:, 0:1] - j[None, :]) % K[0]
+    gy = (i0[:, 1:2] - j[None, :]) % K[1]
+    gz = (i0[:, 2:3] - j[None, :]) % K[2]
+    Q = np.zeros(K)
+    wts = (q[:, None, None, None] * cs[0][:, :, None, None] * cs[1][:, None, :, None] *
+           cs[2][:, None, None, :])
+    ix = np.broadcast_to(gx[:, :, None, None], wts.shape)
+    iy = np.broadcast_to(gy[:, None, :, None], wts.shape)
+    iz = np.broadcast_to(gz[:, None, None, :], wts.shape)
+    np.add.at(Q, (ix.ravel(), iy.ravel(), iz.ravel()), wts.ravel())
+    F = np.fft.fftn(Q)
+    m = [np.fft.fftfreq(K[a], 1.0 / K[a]) / box[a] for a in range(3)]
+    m2 = m[0][:, None, None] ** 2 + m[1][None, :, None] ** 2 + m[2][None, None, :] ** 2
+    B = [_bspline_moduli(K[a], order) for a in range(3)]
+    Bm = B[0][:, None, None] * B[1][None, :, None] * B[2][None, None, :]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        theta = np.where(m2 > 0, np.exp(-np.pi ** 2 * m2 / alpha ** 2) / m2 * Bm, 0.0)
+    em = coulomb / (2.0 * np.pi * volume) * theta * np.abs(F) ** 2
+    energy = float(np.sum(em))
+    virial = float(np.sum(em * (1.0 - 2.0 * np.pi ** 2 * m2 / alpha ** 2)))
+    phi = coulomb / (np.pi * volume) * np.real(np.fft.ifftn(theta * F)) * float(np.prod(K))
+    grads = []
+    for a in range(3):
+        parts = [cs[0], cs[1], cs[2]]
+        parts[a] = ds[a]
+        stencil = (parts[0][:, :, None, None] * parts[1][:, None, :, None] *
+                   parts[2][:, None, None, :])
+        vals = phi[ix, iy, iz]
+        grads.append(np.sum(stencil * vals, axis=(1, 2, 3)) * K[a] / box[a])
+    forces = -q[:, None] * np.stack(grads, axis=1)
+    return energy, virial, forces
