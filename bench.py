@@ -784,6 +784,8 @@ def run_water_arm(args):
     ff = md.SpceForceField(cutoff=WATER_RC, kmax=WATER_KMAX, alpha=WATER_ALPHA, ctx=ctx)
     if args.pme > 0:
         ff.set_pme_spacing(w["box"], args.pme, args.pme_order)
+    if args.mixed:
+        ff.set_precision(md.PRECISION_MIXED)
     recip = ("smooth PME, grid %dx%dx%d, B-spline order %d" % (*ff.pme_grid()[0], args.pme_order)
              if args.pme > 0 else f"Ewald k-vector sums, kmax={WATER_KMAX}")
     dof = md.RigidWater.degrees_of_freedom(4096, True)
@@ -819,7 +821,10 @@ def run_water_arm(args):
                     f"{args.equil_water} NHC steps of 0.5 fs",
             "config": dict(water_config(args.steps),
                            constraints="SETTLE" if args.settle else "SHAKE/RATTLE",
-                           reciprocal=recip),
+                           reciprocal=recip,
+                           precision=("FP32 real-space pair terms, FP64 displacements, "
+                                      "reciprocal space and sums" if args.mixed
+                                      else "FP64 (real and reciprocal space)")),
             "gpu_launches": int(launches),
             "nhc_extended_energy_drift_K": {"max_abs": float(np.max(np.abs(h - h[0]))),
                                             "relative": float(np.max(np.abs(h - h[0])) / abs(h[0]))},
@@ -1172,6 +1177,8 @@ def main():
                     help="water: smooth PME with grid cells of at most SPACING A instead of "
                          "the k-vector sums")
     ap.add_argument("--pme-order", type=int, default=6)
+    ap.add_argument("--mixed", action="store_true",
+                    help="water: FP32 real-space pair terms (FP64 displacements and sums)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)

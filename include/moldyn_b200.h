@@ -264,6 +264,10 @@ MD_API int md_ewald_kvector_count(const md_ewald* ew, int* count);     /* full k
  * reference defers PME (no counterpart); real space, self and intramolecular
  * terms are unchanged.  md_ewald_charge_gradient needs the k-vector sums. */
 MD_API int md_ewald_set_pme(md_ewald* ew, int kx, int ky, int kz, int order);
+/* Precision of the real-space pair terms (erfc, exp, O-O LJ powers):
+ * MD_PRECISION_FP64 (default, the reference's arithmetic) or MD_PRECISION_MIXED
+ * (FP32 pair terms; displacements, cutoff test and all sums in FP64). */
+MD_API int md_ewald_set_precision(md_ewald* ew, int precision);
 /* The PME grid and order, zeros when the k-vector sums are in use. */
 MD_API int md_ewald_pme_grid(const md_ewald* ew, int k[3], int* order);
 

@@ -188,6 +188,7 @@ def _load():
         "md_ewald_alpha": (C.c_int, [_vp, _d]),
         "md_ewald_kvector_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),
         "md_ewald_set_pme": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "md_ewald_set_precision": (C.c_int, [_vp, C.c_int]),
         "md_ewald_pme_grid": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "md_spce_create": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                      C.POINTER(_vp)]),
@@ -664,6 +665,11 @@ class _PmeMixin:
     def set_pme_spacing(self, box, spacing=1.0, order=6):
         """PME with FFT-friendly grid sizes of at most `spacing` per grid cell."""
         self.set_pme([fft_size(math.ceil(float(L) / spacing)) for L in np.asarray(box)], order)
+
+    def set_precision(self, precision):
+        """PRECISION_FP64 (default) or PRECISION_MIXED: FP32 real-space pair
+        terms with FP64 displacements and sums."""
+        _check(lib().md_ewald_set_precision(self._h, int(precision)))
 
     def pme_grid(self):
         """((kx, ky, kz), order), or ((0, 0, 0), 0) with the k-vector sums."""

@@ -51,9 +51,45 @@ struct RealArgs {
     double rc, uc, dudrc;
 };
 
+// The real-space Coulomb (ewald.cpp:60-68) and O-O LJ (lennard_jones.cpp:62-77)
+// terms of one pair at r2, in FP32 (MD_PRECISION_MIXED): returns the force
+// coefficient s (F = s d) and adds the energies and virials of the pair.
+__device__ __forceinline__ float real_pair_mixed(float r2, float cqq, bool coulomb, bool lj,
+                                                 const RealArgs& a, float& er, float& wr,
+                                                 float& el, float& wl) {
+    float s = 0.0f;
+    if (coulomb) {
+        const float r = sqrtf(r2);
+        const float erfc_ar = erfcf(static_cast<float>(a.alpha) * r);
+        const float w = cqq * (static_cast<float>(a.two_alpha_over_sqrt_pi) *
+                                   expf(static_cast<float>(a.neg_alpha2) * r2) +
+                               erfc_ar / r);
+        s = w / r2;
+        er = cqq * erfc_ar / r;
+        wr = w;
+    }
+    if (lj) {
+        const float s2 = static_cast<float>(a.sig2) / r2;
+        const float s6 = s2 * s2 * s2;
+        float w = static_cast<float>(a.tf_eps) * (2.0f * s6 * s6 - s6);
+        float u = static_cast<float>(a.four_eps) * (s6 * s6 - s6);
+        if (a.lj_lfs) {
+            const float r = sqrtf(r2);
+            u = u - static_cast<float>(a.uc) - (r - static_cast<float>(a.rc)) * static_cast<float>(a.dudrc);
+            w = w + r * static_cast<float>(a.dudrc);
+        }
+        s += w / r2;
+        el = u;
+        wl = w;
+    }
+    return s;
+}
+
 // Real-space (and SPC/E O-O LJ) pair terms over the Verlet list.  out[0..3]:
 // E_real, W_real, E_lj, W_lj.  mode 1 writes forces, mode 2 adds to them.
-template <int TPA>
+// MIXED: the displacement, the cutoff test and every sum stay FP64; the pair
+// terms (erfc, exp, the LJ powers) are evaluated in FP32.
+template <int TPA, bool MIXED>
 __global__ void __launch_bounds__(kBlock)
 k_ewald_real(const double4* __restrict__ pos, const double* __restrict__ q,
              const int64_t* __restrict__ mol, const int* __restrict__ nbr,
@@ -72,16 +108,42 @@ k_ewald_real(const double4* __restrict__ pos, const double* __restrict__ q,
         const bool oxy_i = (static_cast<int64_t>(pi.w) % 3) == 0;
         const int cnt = min(count[i], stride);
         const int* row = nbr + i * static_cast<int64_t>(stride);
+        // the neighbour's position, charge and molecule are requested together, so
+        // one L2 round trip serves the cutoff test and the pair terms
+#pragma unroll 2
         for (int k = g; k < cnt; k += TPA) {
             const int j = __ldg(row + k);
             const double4 pj = ldg4(pos + j);
+            const double qj = __ldg(q + j);
+            const int64_t mj = __ldg(mol + j);
             const bool lo = pi.w < pj.w;
+            // r_lower - r_higher by original index, the reference's pair order; the
+            // operands are selected rather than branched on, so a warp runs one fold
             double dx, dy, dz;
-            if (lo) min_image_wrapped(f3, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, dx, dy, dz);
-            else min_image_wrapped(f3, pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, dx, dy, dz);
+            min_image_wrapped(f3, lo ? pi.x : pj.x, lo ? pi.y : pj.y, lo ? pi.z : pj.z,
+                              lo ? pj.x : pi.x, lo ? pj.y : pi.y, lo ? pj.z : pi.z, dx, dy, dz);
             const double r2 = norm2_exact(dx, dy, dz);
             if (!(r2 < a.rc2)) continue;
             double s = 0.0;
+            if (MIXED) {
+                const bool coul = mj != mi;
+                const bool lj = a.spce_lj && oxy_i && (static_cast<int>(pj.w) % 3) == 0;
+                float per = 0.0f, pwr = 0.0f, pel = 0.0f, pwl = 0.0f;
+                s = real_pair_mixed(static_cast<float>(r2),
+                                    coul ? static_cast<float>(a.coulomb * (qi * qj)) : 0.0f, coul,
+                                    lj, a, per, pwr, pel, pwl);
+                if (lo) {
+                    er += per;
+                    wr += pwr;
+                    el += pel;
+                    wl += pwl;
+                }
+                const double sg = lo ? s : -s;
+                fx = fma(dx, sg, fx);
+                fy = fma(dy, sg, fy);
+                fz = fma(dz, sg, fz);
+                continue;
+            }
             if (mol[j] != mi) {
                 // ewald.cpp:60-68
                 const double r = __dsqrt_rn(r2);
@@ -94,7 +156,7 @@ k_ewald_real(const double4* __restrict__ pos, const double* __restrict__ q,
                     wr += w;
                 }
             }
-            if (a.spce_lj && oxy_i && (static_cast<int64_t>(pj.w) % 3) == 0) {
+            if (a.spce_lj && oxy_i && (static_cast<int>(pj.w) % 3) == 0) {
                 // lennard_jones.cpp:62-70 (Truncated)
                 const double s2 = a.sig2 / r2;
                 const double s6 = s2 * s2 * s2;
@@ -517,11 +579,15 @@ int real_tpa(const md_context* ctx, int64_t n) {
     return tpa;
 }
 
-template <int TPA>
+// 128-thread blocks: at the kernel's ~96 registers five fit on an SM (20 warps)
+// where two 256-thread blocks would (16).
+constexpr int kRealBlock = 128;
+
+template <int TPA, bool MIXED>
 void launch_real_t(md_system* sys, md_verlet* v, const RealArgs& a, int mode, double* fx,
                    double* fy, double* fz, double* part, unsigned* ticket, double* out) {
     const int64_t threads = std::max<int64_t>(sys->n * TPA, 1);
-    k_ewald_real<TPA><<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
+    k_ewald_real<TPA, MIXED><<<grid_for(threads, kRealBlock), kRealBlock, 0, sys->ctx->stream>>>(
         sys->cur.pos, sys->cur.charge, sys->cur.mol, v->nbr.as<int>(), v->count.as<int>(),
         v->stride, sys->n, Box3{{sys->box[0], sys->box[1], sys->box[2]},
                                 {sys->inv_box[0], sys->inv_box[1], sys->inv_box[2]}},
@@ -529,14 +595,21 @@ void launch_real_t(md_system* sys, md_verlet* v, const RealArgs& a, int mode, do
 }
 
 // mode 1 writes (fx, fy, fz), 2 adds to them; part holds 4 doubles per block.
-void launch_real(md_system* sys, md_verlet* v, const RealArgs& a, int mode, int tpa, double* fx,
-                 double* fy, double* fz, double* part, unsigned* ticket, double* out) {
+template <bool MIXED>
+void launch_real_p(md_system* sys, md_verlet* v, const RealArgs& a, int mode, int tpa, double* fx,
+                   double* fy, double* fz, double* part, unsigned* ticket, double* out) {
     switch (tpa) {
-        case 32: launch_real_t<32>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
-        case 16: launch_real_t<16>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
-        case 8: launch_real_t<8>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
-        default: launch_real_t<4>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        case 32: launch_real_t<32, MIXED>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        case 16: launch_real_t<16, MIXED>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        case 8: launch_real_t<8, MIXED>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
+        default: launch_real_t<4, MIXED>(sys, v, a, mode, fx, fy, fz, part, ticket, out); break;
     }
+}
+
+void launch_real(md_system* sys, md_verlet* v, const RealArgs& a, int mode, int tpa, bool mixed,
+                 double* fx, double* fy, double* fz, double* part, unsigned* ticket, double* out) {
+    if (mixed) launch_real_p<true>(sys, v, a, mode, tpa, fx, fy, fz, part, ticket, out);
+    else launch_real_p<false>(sys, v, a, mode, tpa, fx, fy, fz, part, ticket, out);
 }
 
 }  // namespace
@@ -576,6 +649,7 @@ struct md_ewald {
     double last[kEwCount] = {0};
     double alpha = 0.0;
     mdb::PmeState* pme = nullptr;  // reciprocal term by smooth PME instead of k-vector sums
+    bool mixed = false;            // FP32 real-space pair terms (MD_PRECISION_MIXED)
 };
 
 namespace mdb {
@@ -781,7 +855,7 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
     double* part;
     const int tpa = real_tpa(ctx, n);
     const int64_t real_threads = std::max<int64_t>(n * tpa, 1);
-    MDB_TRY(ctx_partials(ctx, 4 * static_cast<size_t>(grid_for(real_threads, kBlock)), &part));
+    MDB_TRY(ctx_partials(ctx, 4 * static_cast<size_t>(grid_for(real_threads, kRealBlock)), &part));
     // real space (+ O-O LJ): with forces it writes (mode 1) or adds (mode 2); for
     // energies only it writes into the scratch force sink of a zero-force pass.
     ctx_time_begin(ctx, MD_KERNEL_EWALD_REAL);
@@ -791,11 +865,11 @@ int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated) {
         double* sink;
         MDB_TRY(ctx_scratch(ctx, 3 * sizeof(double) * static_cast<size_t>(std::max<int64_t>(n, 1)),
                             reinterpret_cast<void**>(&sink)));
-        launch_real(sys, v, a, 1, tpa, sink, sink + n, sink + 2 * n, part, ctx_counter(ctx, 4),
-                    res + kEwReal);
-    } else {
-        launch_real(sys, v, a, mode, tpa, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
+        launch_real(sys, v, a, 1, tpa, ew->mixed, sink, sink + n, sink + 2 * n, part,
                     ctx_counter(ctx, 4), res + kEwReal);
+    } else {
+        launch_real(sys, v, a, mode, tpa, ew->mixed, sys->cur.fx, sys->cur.fy, sys->cur.fz,
+                    part, ctx_counter(ctx, 4), res + kEwReal);
     }
     ctx_time_end(ctx, MD_KERNEL_EWALD_REAL);
     // intramolecular correction
@@ -972,6 +1046,13 @@ int md_ewald_set_pme(md_ewald* ew, int kx, int ky, int kz, int order) {
         pme_destroy(ew->pme);
     }
     ew->pme = s;
+    return MD_OK;
+}
+
+int md_ewald_set_precision(md_ewald* ew, int precision) {
+    if (!ew || (precision != MD_PRECISION_FP64 && precision != MD_PRECISION_MIXED))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_precision: MD_PRECISION_FP64 or _MIXED");
+    ew->mixed = precision == MD_PRECISION_MIXED;
     return MD_OK;
 }
 
