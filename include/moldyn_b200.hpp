@@ -3,8 +3,9 @@
 // Header-only.  The classes keep the names, constructors and methods of the
 // reference's hot path (core/system.hpp, core/box.hpp, core/vec3.hpp,
 // neighbor/cell_list.hpp, neighbor/verlet_list.hpp, forcefield/*.hpp,
-// constrain/rigid_water.hpp, integrate/*.hpp, util/lattice.hpp), so code written
-// against them -- apps/moldyn_run.cpp's simulation loop, for one -- compiles
+// constrain/rigid_water.hpp, integrate/*.hpp, util/lattice.hpp, util/random.hpp,
+// core/units.hpp, io/nist_config.hpp, analyze/*.hpp), so code written against
+// them -- apps/moldyn_run.cpp's simulation loop, apps/water_rdf.cpp -- compiles
 // against this header with
 //
 //     #include "moldyn_b200.hpp"
@@ -21,6 +22,9 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <fstream>
+#include <random>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -183,6 +187,12 @@ public:
     }
     void removeCenterOfMassMotion() {
         detail::check(md_system_remove_com_motion(device()));
+        device_ahead_ = true;
+    }
+    // Extension: v *= sqrt(target / T), T = 2 KE / dof, when T > 0, on the device
+    // (the equilibration rescale of apps/water_rdf.cpp:188-195).
+    void rescaleTemperature(std::size_t dof, double target) {
+        detail::check(md_system_rescale_temperature(device(), static_cast<int64_t>(dof), target));
         device_ahead_ = true;
     }
 
@@ -410,6 +420,10 @@ public:
     Ewald(const Ewald&) = delete;
     Ewald& operator=(const Ewald&) = delete;
     ~Ewald() { md_ewald_destroy(h_); }
+    // Extensions: smooth PME for the reciprocal term (0, 0, 0: the k-vector
+    // sums), FP32 real-space pair terms (MD_PRECISION_MIXED).
+    void setPme(int kx, int ky, int kz, int order = 6) { detail::check(md_ewald_set_pme(h_, kx, ky, kz, order)); }
+    void setPrecision(int precision) { detail::check(md_ewald_set_precision(h_, precision)); }
     EwaldTerms computeEnergies(const System& sys) const { return run(sys, 0); }
     EwaldTerms computeForces(System& sys) const { EwaldTerms t = run(sys, 1); sys.deviceChanged(); return t; }
     EwaldTerms accumulateForces(System& sys) const { EwaldTerms t = run(sys, 2); sys.deviceChanged(); return t; }
@@ -454,6 +468,8 @@ public:
         detail::check(md_spce_compute(h_, sys.device(), 0, &e, nullptr));
         return e;
     }
+    void setPme(int kx, int ky, int kz, int order = 6) { detail::check(md_ewald_set_pme(h_, kx, ky, kz, order)); }
+    void setPrecision(int precision) { detail::check(md_ewald_set_precision(h_, precision)); }
     md_ewald* handle() const { return h_; }
 
 private:
@@ -495,6 +511,12 @@ public:
         sys.deviceChanged();
         return it;
     }
+    // Extension: closed-form SETTLE instead of SHAKE / RATTLE iterations (the same
+    // fixed point); integrators created from this constraint afterwards use it.
+    void setSettle(bool on) {
+        detail::check(md_rigid_set_settle(h_, on ? 1 : 0));
+        settle_ = on;
+    }
     double ohDistance() const { double oh, hh; md_rigid_distances(h_, &oh, &hh); return oh; }
     double hhDistance() const { double oh, hh; md_rigid_distances(h_, &oh, &hh); return hh; }
     static std::size_t degreesOfFreedom(std::size_t molecules, bool comRemoved) {
@@ -510,10 +532,13 @@ private:
         max_it_ = o.max_it_;
         angle_ = o.angle_;
         detail::check(md_rigid_create(oh, o.angle_, o.tolerance_, o.max_it_, &h_));
+        settle_ = o.settle_;
+        if (settle_) detail::check(md_rigid_set_settle(h_, 1));
     }
     md_rigid* h_ = nullptr;
     double tolerance_ = 1e-12, angle_ = 109.47;
     int max_it_ = 500;
+    bool settle_ = false;
 };
 
 // ------------------------------------------------------------------- integrators
@@ -638,6 +663,13 @@ public:
     Rdf& operator=(const Rdf&) = delete;
     ~Rdf() { md_rdf_destroy(h_); }
     void accumulate(const System& sys) { detail::check(md_rdf_accumulate(h_, sys.device())); }
+    // Extension: the atoms first, first + stride, ... alone, as accumulate() of a
+    // System holding just those (apps/water_rdf.cpp's gatherOxygens: 0, 3).
+    void accumulateSubset(const System& sys, std::size_t first, std::size_t stride) {
+        detail::check(md_rdf_accumulate_subset(h_, sys.device(), static_cast<int64_t>(first),
+                                               static_cast<int64_t>(stride)));
+    }
+    md_rdf* handle() const { return h_; }
     std::vector<double> binCentres() const { return vec(md_rdf_bin_centres); }
     std::vector<double> g() const { return vec(md_rdf_g); }
     std::size_t frames() const {
@@ -710,5 +742,142 @@ private:
     std::size_t lags_;
     md_vacf* h_ = nullptr;
 };
+
+// ------------------------------------------------------------------ core/units.hpp
+namespace units {
+inline constexpr double kTauInPicoseconds = 1.0966875353;  // core/units.hpp:33
+inline constexpr double picoseconds(double ps) { return ps / kTauInPicoseconds; }
+inline constexpr double femtoseconds(double fs) { return picoseconds(fs * 1.0e-3); }
+inline constexpr double toPicoseconds(double tau) { return tau * kTauInPicoseconds; }
+}  // namespace units
+
+// ------------------------------------------------------------- util/random.hpp
+// Rng (util/random.hpp:37-76): std::mt19937_64, uniform deviates in (0, 1],
+// normals by Marsaglia's polar method keeping the spare -- the same stream as the
+// reference's for a seed (md_rng_normals gives the same draws from C).
+class Rng {
+public:
+    explicit Rng(uint64_t seed) : engine_(seed) {}
+    double uniform() { return 1.0 - dist_(engine_); }
+    double normal() {
+        if (have_spare_) {
+            have_spare_ = false;
+            return spare_;
+        }
+        double u = 0.0, v = 0.0, s = 0.0;
+        do {
+            u = 2.0 * uniform() - 1.0;
+            v = 2.0 * uniform() - 1.0;
+            s = u * u + v * v;
+        } while (s >= 1.0 || s == 0.0);
+        const double m = std::sqrt(-2.0 * std::log(s) / s);
+        spare_ = v * m;
+        have_spare_ = true;
+        return u * m;
+    }
+
+private:
+    std::mt19937_64 engine_;
+    std::uniform_real_distribution<double> dist_{0.0, 1.0};
+    double spare_ = 0.0;
+    bool have_spare_ = false;
+};
+
+// ------------------------------------------------------------ io/nist_config.hpp
+struct NistConfig {
+    System system;
+    std::vector<std::string> types;
+};
+
+// readNistConfig (io/nist_config.cpp:30-86): line 1 the box, line 2 a count that
+// is not trusted (the SPC/E files give molecules), then "index x y z [type]" lines
+// to the end of the file; blank lines are skipped, every atom gets mass 1 and zero
+// velocity.  Throws std::runtime_error on a missing file or a malformed line.
+inline NistConfig readNistConfig(const std::string& path) {
+    std::ifstream in(path);
+    if (!in.is_open()) throw std::runtime_error("readNistConfig: cannot open file " + path);
+    std::string line;
+    if (!std::getline(in, line)) throw std::runtime_error("readNistConfig: empty file " + path);
+    double lx = 0.0, ly = 0.0, lz = 0.0;
+    {
+        std::istringstream iss(line);
+        if (!(iss >> lx >> ly >> lz))
+            throw std::runtime_error("readNistConfig: malformed box line in " + path);
+    }
+    if (!std::getline(in, line)) throw std::runtime_error("readNistConfig: missing count line in " + path);
+    {
+        std::istringstream iss(line);
+        long declared = 0;
+        if (!(iss >> declared))
+            throw std::runtime_error("readNistConfig: malformed count line in " + path);
+    }
+    NistConfig cfg{System(Box(Vec3{lx, ly, lz})), {}};
+    std::vector<std::string> types;
+    bool typed = false;
+    while (std::getline(in, line)) {
+        if (line.find_first_not_of(" \t\r\n") == std::string::npos) continue;
+        std::istringstream iss(line);
+        long index = 0;
+        double x = 0.0, y = 0.0, z = 0.0;
+        if (!(iss >> index >> x >> y >> z))
+            throw std::runtime_error("readNistConfig: malformed atom line in " + path);
+        std::string type;
+        const bool has_type = static_cast<bool>(iss >> type);
+        cfg.system.addAtom(Vec3{x, y, z}, Vec3{0.0, 0.0, 0.0}, 1.0);
+        types.push_back(has_type ? type : std::string());
+        typed = typed || has_type;
+    }
+    if (typed) cfg.types = std::move(types);
+    return cfg;
+}
+
+// ------------------------------------------------------------ forcefield/spce.hpp
+struct SpceSystem {
+    System full;
+    System oxygens;
+    std::size_t moleculeCount = 0;
+};
+
+// buildSpceSystem (forcefield/spce.cpp:8-40): O, H, H triples with the model's
+// charges and masses, molecule id = index / 3; `oxygens` holds the O sites alone.
+inline SpceSystem buildSpceSystem(const NistConfig& cfg, const SpceParameters& params = SpceParameters()) {
+    const std::size_t n = cfg.system.size();
+    if (n == 0 || n % 3 != 0)
+        throw std::invalid_argument(
+            "buildSpceSystem: atom count must be a positive multiple of 3 (O, H, H per molecule)");
+    if (cfg.types.size() != n) throw std::invalid_argument("buildSpceSystem: config has no per-atom types");
+    const double qO = -2.0 * params.qH;
+    SpceSystem out{System(cfg.system.box()), System(cfg.system.box()), n / 3};
+    out.full.reserve(n);
+    for (std::size_t i = 0; i < n; ++i) {
+        const Vec3 r = cfg.system.position(i), v = cfg.system.velocity(i);
+        if (cfg.types[i] == "O") {
+            out.full.addAtom(r, v, params.massOxygen, qO, i / 3);
+            out.oxygens.addAtom(r, v, params.massOxygen);
+        } else if (cfg.types[i] == "H") {
+            out.full.addAtom(r, v, params.massHydrogen, params.qH, i / 3);
+        } else {
+            throw std::invalid_argument("buildSpceSystem: unrecognised atom type '" + cfg.types[i] +
+                                        "' (expected \"O\" or \"H\")");
+        }
+    }
+    return out;
+}
+
+// Extension: the simulation of apps/water_rdf.cpp:186-216 as one device call
+// (md_water_rdf_run): `equilibrate` steps rescaled toward `temperature` and
+// re-constrained every `rescaleEvery`, then `production` NVE steps with the
+// oxygens (atoms 0, 3, 6, ...) accumulated into rdf every `sampleEvery`.
+// Returns the mean production temperature.
+inline double runWaterRdf(ConstrainedVelocityVerlet& integ, System& sys, const SpceForceField& ff,
+                          Rdf& rdf, double temperature, std::size_t dof, int64_t equilibrate,
+                          int64_t rescaleEvery, int64_t production, int64_t sampleEvery) {
+    double mean = 0.0;
+    detail::check(md_water_rdf_run(integ.handle(), sys.device(), ff.handle(), rdf.handle(),
+                                   temperature, static_cast<int64_t>(dof), equilibrate, rescaleEvery,
+                                   production, sampleEvery, &mean));
+    sys.deviceChanged();
+    return mean;
+}
 
 }  // namespace moldyn_b200

@@ -165,7 +165,9 @@ def test_full_protocol_reproduces_the_reference_structure(md, settle, tmp_path):
     assert abs(res.first_peak_r - WVAL["first_peak_r_angstrom"]) < 0.03
     assert abs(res.first_peak_g - WVAL["first_peak_g"]) < 0.2
     assert abs(res.tail_mean - 1.0) < 0.01
-    assert abs(res.mean_temperature - 298.0) < 10.0
+    # NVE production after a crude rescale: the reference saw 294.4 K after 30 ps
+    # and 308.8 K after 10 ps of equilibration (apps/water_rdf.cpp:108-113)
+    assert abs(res.mean_temperature - 298.0) < 15.0
     r, g = res.r, res.g
     assert np.all(g[r < 2.2] < 0.05)  # excluded volume
     band = (r > 2.0)
@@ -178,3 +180,31 @@ def test_full_protocol_reproduces_the_reference_structure(md, settle, tmp_path):
     W.write_csv(tmp_path / "w.csv", res, "water_rdf", settle=settle)
     lines = (tmp_path / "w.csv").read_text().splitlines()
     assert lines[22] == "r_angstrom,g_oo" and len(lines) == 223
+
+
+def test_cxx_app_equals_the_python_driver(md, tmp_path):
+    """The C++ app (apps/water_rdf.cpp's drop-in on include/moldyn_b200.hpp) and
+    the Python driver, on the same NIST file: every CSV line but the provenance
+    ones (command, revision, host, wall time) is identical."""
+    import os
+    import subprocess
+    from moleculardynamics_b200 import water_rdf as W
+    pos, types, box = config3()
+    cfg_dir = tmp_path / "data" / "nist" / "spce"
+    cfg_dir.mkdir(parents=True)
+    lines = ["%25.12E%25.12E%25.12E" % tuple(box), "%12d" % (len(types) // 3)]
+    lines += ["%5d%25.12E%25.12E%25.12E    %s" % (k + 1, *p, t) for k, (p, t) in enumerate(zip(pos, types))]
+    (cfg_dir / "spce_sample_config_periodic3.txt").write_text("\n".join(lines) + "\n")
+    exe = os.path.join(os.path.dirname(md.library_path()), "bin", "water_rdf")
+    args = ["--equilibrate", "150", "--production", "60", "--sample-every", "10"]
+    res = subprocess.run([exe, "--data", str(tmp_path / "data"), "--out", str(tmp_path / "cxx.csv"),
+                          *args], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr[-2000:]
+    cfg = md.read_nist_config(cfg_dir / "spce_sample_config_periodic3.txt")
+    r = W.run(cfg["pos"], cfg["types"], cfg["box"], equilibrate=150, production=60, sample_every=10)
+    W.write_csv(tmp_path / "py.csv", r, "water_rdf")
+    skip = ("# command", "# git_sha", "# host", "# wall_seconds")
+    a = [l for l in (tmp_path / "cxx.csv").read_text().splitlines() if not l.startswith(skip)]
+    b = [l for l in (tmp_path / "py.csv").read_text().splitlines() if not l.startswith(skip)]
+    assert len(a) == len(b) == 219
+    assert a == b

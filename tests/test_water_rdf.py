@@ -157,6 +157,7 @@ def test_csv_layout(tmp_path):
     assert lines[3] == "# model: SPC/E, rigid (SHAKE/RATTLE), Ewald alpha=5.6/L kmax=5 rcut=10 A"
     assert lines[5] == "# box_length_angstrom: 20.802"
     assert lines[16] == "# first_peak_r_angstrom: 2.75167"
+    assert lines[18:20] == ["# reference_first_peak_r_angstrom: 2.75", "# reference_first_peak_g: 3.0"]
     assert lines[20] == "# tail_mean_g_beyond_8.5A: 1.00014"
     assert lines[22] == "r_angstrom,g_oo"
     assert lines[23] == "0.025,0" and lines[-1] == "9.975,%g" % g[-1]
@@ -182,3 +183,16 @@ def test_units():
     """core/units.hpp:33-40"""
     assert md.units.femtoseconds(2.0) == 2.0e-3 / 1.0966875353
     assert md.units.to_picoseconds(md.units.picoseconds(3.5)) == pytest.approx(3.5, rel=1e-15)
+
+
+def test_cxx_app_flag_errors():
+    """The C++ drop-in (moleculardynamics_b200/bin/water_rdf) rejects flags as
+    apps/water_rdf.cpp:120-142 does, before touching the device."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(md.library_path()), "bin", "water_rdf")
+    assert os.path.exists(exe), "build the package first (make -C moleculardynamics_b200/csrc)"
+    res = subprocess.run([exe, "--bogus", "1"], capture_output=True, text=True)
+    assert res.returncode == 1 and "unknown flag --bogus" in res.stderr
+    res = subprocess.run([exe, "--seed"], capture_output=True, text=True)
+    assert res.returncode == 1 and "--seed needs a value" in res.stderr
