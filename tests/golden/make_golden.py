@@ -188,11 +188,35 @@ def water_rdf_fixture(ref_root, R):
             "values": np.array([head[k] for k in keys]), "normals7001": normals}
 
 
+def exp02_fixture(ref_root, R):
+    """The reference's recorded experiment 02 (experiments/exp02_energy_conservation.sh):
+    moldyn_run NVE velocity Verlet on fcc(3), rho*=0.80, T*=1.0, seed 12345, rc 2.5,
+    skin 0.4, linear-force-shift, dt 0.001 / 0.002 / 0.004 / 0.008 to t = 1.  Every
+    thermo row (step, time, PE, KE, E, T, P) and the summary (e0, max |E - e0|,
+    relative error) as written by the reference (results/exp02_*.csv)."""
+    out = {}
+    for dt in ("0.001", "0.002", "0.004", "0.008"):
+        rows = []
+        for line in open(os.path.join(ref_root, "results", f"exp02_thermo_dt{dt}.csv")):
+            if line[:1].isdigit():
+                f = line.strip().split(",")
+                rows.append([float(f[0]), float(f[1])] + [float(v) for v in f[3:8]])
+        out["thermo_" + dt] = np.array(rows)
+    summary = []
+    for line in open(os.path.join(ref_root, "results", "exp02_energy_conservation.csv")):
+        if line[:1].isdigit():
+            summary.append([float(v) for v in line.strip().split(",")])
+    out["summary"] = np.array(summary)
+    assert out["summary"].shape == (4, 4)
+    return out
+
+
 FIXTURES = {
     "nist_lj.npz": lambda root, R: lj_fixture(root, R),
     "nist_spce.npz": lambda root, R: spce_fixture(root, R),
     "fcc_lj.npz": lambda root, R: fcc_fixture(R),
     "water_rdf_ref.npz": water_rdf_fixture,
+    "exp02_ref.npz": exp02_fixture,
 }
 
 
