@@ -211,12 +211,34 @@ def exp02_fixture(ref_root, R):
     return out
 
 
+def exp03_fixture(ref_root, R):
+    """The reference's recorded experiment 03 (experiments/exp03_argon_rdf.sh):
+    moldyn_run on fcc(6) (864 atoms), rc 2.5, skin 0.3, dt 0.005, 5000 Langevin
+    then 20000 NVE steps with g(r) (200 bins to 0.98 L/2) every production step,
+    at the Rahman (0.8177, 0.7880, seed 3001) and Verlet (0.8442, 0.7280, seed
+    3002) state points: each g(r) and the summary peak."""
+    out = {}
+    for label in ("rahman", "verlet"):
+        rows = [[float(v) for v in line.strip().split(",")]
+                for line in open(os.path.join(ref_root, "results", f"exp03_rdf_{label}.csv"))
+                if line[:1].isdigit()]
+        out["rdf_" + label] = np.array(rows)
+    summ = {}
+    for line in open(os.path.join(ref_root, "results", "exp03_argon_rdf.csv")):
+        f = line.strip().split(",")
+        if f[0] in ("rahman", "verlet"):
+            summ[f[0]] = [float(f[1]), float(f[2]), float(f[3]), float(f[4]), float(f[5])]
+    out["summary"] = np.array([summ["rahman"], summ["verlet"]])  # rho, T, seed, peak r, peak g
+    return out
+
+
 FIXTURES = {
     "nist_lj.npz": lambda root, R: lj_fixture(root, R),
     "nist_spce.npz": lambda root, R: spce_fixture(root, R),
     "fcc_lj.npz": lambda root, R: fcc_fixture(R),
     "water_rdf_ref.npz": water_rdf_fixture,
     "exp02_ref.npz": exp02_fixture,
+    "exp03_ref.npz": exp03_fixture,
 }
 
 
