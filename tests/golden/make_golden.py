@@ -232,6 +232,21 @@ def exp03_fixture(ref_root, R):
     return out
 
 
+def exp04_fixture(ref_root, R):
+    """The reference's recorded experiment 04 (experiments/exp04_argon_diffusion.sh):
+    per replica (8 seeds at the Rahman and Verlet state points) the diffusion
+    coefficients from the MSD fit and the VACF integral
+    (results/exp04_argon_diffusion.csv): rho, T, seed, D_msd, D_vacf."""
+    rows = []
+    for line in open(os.path.join(ref_root, "results", "exp04_argon_diffusion.csv")):
+        f = line.strip().split(",")
+        if f[0] in ("rahman", "verlet"):
+            rows.append([0.0 if f[0] == "rahman" else 1.0] + [float(v) for v in f[1:6]])
+    rows = np.array(rows)
+    assert rows.shape == (16, 6), rows.shape
+    return {"replicas": rows}  # state (0 Rahman, 1 Verlet), rho, T, seed, D_msd, D_vacf
+
+
 FIXTURES = {
     "nist_lj.npz": lambda root, R: lj_fixture(root, R),
     "nist_spce.npz": lambda root, R: spce_fixture(root, R),
@@ -239,6 +254,7 @@ FIXTURES = {
     "water_rdf_ref.npz": water_rdf_fixture,
     "exp02_ref.npz": exp02_fixture,
     "exp03_ref.npz": exp03_fixture,
+    "exp04_ref.npz": exp04_fixture,
 }
 
 
