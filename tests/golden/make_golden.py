@@ -247,6 +247,20 @@ def exp04_fixture(ref_root, R):
     return {"replicas": rows}  # state (0 Rahman, 1 Verlet), rho, T, seed, D_msd, D_vacf
 
 
+def exp05_fixture(ref_root, R):
+    """The reference's recorded experiment 05 (experiments/exp05_lj_eos.sh): the LJ
+    equation of state on fcc(5) (500 atoms), rc 3.0 with tail corrections, 10000
+    Langevin then 20000 Nose-Hoover steps at NIST's temperature per density
+    (results/exp05_lj_eos.csv): rho, seed, its T*, U*, p*, NIST's T*, U*, p*."""
+    rows = []
+    for line in open(os.path.join(ref_root, "results", "exp05_lj_eos.csv")):
+        if line[:1].isdigit():
+            rows.append([float(v) for v in line.strip().split(",")[:8]])
+    rows = np.array(rows)
+    assert rows.shape == (6, 8), rows.shape
+    return {"rows": rows}
+
+
 FIXTURES = {
     "nist_lj.npz": lambda root, R: lj_fixture(root, R),
     "nist_spce.npz": lambda root, R: spce_fixture(root, R),
@@ -255,6 +269,7 @@ FIXTURES = {
     "exp02_ref.npz": exp02_fixture,
     "exp03_ref.npz": exp03_fixture,
     "exp04_ref.npz": exp04_fixture,
+    "exp05_ref.npz": exp05_fixture,
 }
 
 
