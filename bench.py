@@ -259,14 +259,14 @@ def e2e_run(md, ctx, box, pos, vel, frc, steps, group):
         cols[6 + k][:] = frc[:, k]
     thermo = np.zeros(4)
     dp = C.POINTER(C.c_double)
+    fields = (C.c_int * 9)(*range(9))
+    cols_p = (dp * 9)(*[C.cast(p, dp) for p in ptrs])
 
     def step():
-        for f in range(9):
-            md._check(L.md_system_set(s.handle, f, C.cast(ptrs[f], dp)))
+        md._check(L.md_system_set_fields(s.handle, 9, fields, cols_p))
         md._check(L.md_run_lj(integ.handle, s.handle, v.handle, lj.handle, 1,
                               thermo.ctypes.data_as(dp)))
-        for f in range(9):
-            md._check(L.md_system_get(s.handle, f, C.cast(ptrs[f], dp)))
+        md._check(L.md_system_get_fields(s.handle, 9, fields, cols_p))
 
     # the list is built once from the uploaded state (rebuilds happen on device)
     for f in range(9):
@@ -453,8 +453,8 @@ def run_gpu_arm(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "precision": "mixed",
                     "steps": e2e_steps,
-                    "path": "md_system_set x9 (pinned host) + md_run_lj(1 step) + "
-                            "md_system_get x9 per step"},
+                    "path": "md_system_set_fields (9 pinned host columns) + md_run_lj(1 step) + "
+                            "md_system_get_fields (9 columns) per step"},
             "roofline": {"bound": "hbm", "kernel": "k_lj_halo (mixed, halo tiles)",
                          "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": achieved / peaks.get("hbm_gbs", 6650.0),

@@ -140,6 +140,12 @@ MD_API int md_system_box(const md_system* sys, double box[3]);        /* box.hpp
 /* Set or get one field: n doubles in original order (system.hpp:29-43). */
 MD_API int md_system_set(md_system* sys, int field, const double* src);
 MD_API int md_system_get(md_system* sys, int field, double* dst);
+/* Several fields at once (fields[k] <- src[k], dst[k] <- fields[k]): every
+ * column's copy is queued before one host synchronisation, where md_system_set
+ * and md_system_get synchronise per field.  Pinned host memory (md_host_alloc)
+ * lets the copies run as DMA. */
+MD_API int md_system_set_fields(md_system* sys, int count, const int* fields, const double* const* src);
+MD_API int md_system_get_fields(md_system* sys, int count, const int* fields, double* const* dst);
 MD_API int md_system_set_molecule_ids(md_system* sys, const int64_t* ids); /* system.hpp:43 */
 MD_API int md_system_get_molecule_ids(md_system* sys, int64_t* ids);       /* system.hpp:34 */
 MD_API int md_system_zero_forces(md_system* sys);                          /* system.cpp:116-122 */

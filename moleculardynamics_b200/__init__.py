@@ -98,6 +98,8 @@ def _load():
         "md_system_box": (C.c_int, [_vp, _d]),
         "md_system_set": (C.c_int, [_vp, C.c_int, _d]),
         "md_system_get": (C.c_int, [_vp, C.c_int, _d]),
+        "md_system_set_fields": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(_d)]),
+        "md_system_get_fields": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(_d)]),
         "md_system_set_molecule_ids": (C.c_int, [_vp, _i64p]),
         "md_system_get_molecule_ids": (C.c_int, [_vp, _i64p]),
         "md_system_zero_forces": (C.c_int, [_vp]),

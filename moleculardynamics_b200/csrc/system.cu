@@ -303,6 +303,56 @@ int md_system_get(md_system* sys, int field, double* dst) {
     return MD_OK;
 }
 
+int md_system_set_fields(md_system* sys, int count, const int* fields, const double* const* src) {
+    if (!sys || count < 0 || (count > 0 && (!fields || !src)))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_system_set_fields: NULL argument");
+    for (int k = 0; k < count; ++k)
+        if (fields[k] < MD_FIELD_X || fields[k] > MD_FIELD_CHARGE || !src[k])
+            return fail(MD_ERR_INVALID_ARGUMENT, "md_system_set_fields: bad field %d", k);
+    if (sys->n == 0 || count == 0) return MD_OK;
+    md_context* ctx = sys->ctx;
+    const size_t col = static_cast<size_t>(sys->n);
+    void* staging;
+    MDB_TRY(ctx_scratch(ctx, col * sizeof(double) * count, &staging));
+    double* st = static_cast<double*>(staging);
+    // every column's copy is queued before any scatter, so the copy engine
+    // streams them back to back; one synchronisation for all
+    for (int k = 0; k < count; ++k)
+        MDB_CUDA(cudaMemcpyAsync(st + k * col, src[k], col * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    for (int k = 0; k < count; ++k)
+        k_set_field<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, fields[k],
+                                                                         st + k * col, sys->n);
+    ctx->launches += count;
+    MDB_CHECK_LAUNCH();
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MD_OK;
+}
+
+int md_system_get_fields(md_system* sys, int count, const int* fields, double* const* dst) {
+    if (!sys || count < 0 || (count > 0 && (!fields || !dst)))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_system_get_fields: NULL argument");
+    for (int k = 0; k < count; ++k)
+        if (fields[k] < MD_FIELD_X || fields[k] > MD_FIELD_CHARGE || !dst[k])
+            return fail(MD_ERR_INVALID_ARGUMENT, "md_system_get_fields: bad field %d", k);
+    if (sys->n == 0 || count == 0) return MD_OK;
+    md_context* ctx = sys->ctx;
+    const size_t col = static_cast<size_t>(sys->n);
+    void* staging;
+    MDB_TRY(ctx_scratch(ctx, col * sizeof(double) * count, &staging));
+    double* st = static_cast<double*>(staging);
+    for (int k = 0; k < count; ++k)
+        k_get_field<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, fields[k],
+                                                                         st + k * col, sys->n);
+    ctx->launches += count;
+    MDB_CHECK_LAUNCH();
+    for (int k = 0; k < count; ++k)
+        MDB_CUDA(cudaMemcpyAsync(dst[k], st + k * col, col * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MD_OK;
+}
+
 int md_system_set_molecule_ids(md_system* sys, const int64_t* ids) {
     if (!sys || !ids) return fail(MD_ERR_INVALID_ARGUMENT, "md_system_set_molecule_ids: NULL");
     if (sys->n == 0) return MD_OK;

@@ -383,3 +383,36 @@ def test_mixed_precision_force_error(md):
     assert rms < 1e-6, rms
     assert abs(emx - e64) < 1e-6 * abs(e64)
     assert abs(wmx - w64) < 1e-5 * abs(w64)
+
+
+def test_bulk_field_transfer_equals_per_field(md):
+    """md_system_set_fields / md_system_get_fields move the same bytes as one
+    md_system_set / md_system_get per field, in original atom order, also after
+    a rebuild has re-sorted the device arrays."""
+    import ctypes as C
+    s, st = lattice_system(md, 6, 0.8442, 0.722, 4)
+    lj = md.LennardJones(1.0, 1.0, 2.5)
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj.compute_forces(s, v)
+    md.VelocityVerlet(0.005).run(s, v, lj, 60)
+    assert v.rebuild_count() > 1
+    n = s.n
+    L = md.lib()
+    dp = C.POINTER(C.c_double)
+    fields = [md.FIELD_X + k for k in range(9)] + [md.FIELD_X + 9, md.FIELD_X + 10]
+    outs = [np.zeros(n) for _ in fields]
+    md._check(L.md_system_get_fields(s.handle, len(fields), (C.c_int * len(fields))(*fields),
+                                     (dp * len(fields))(*[o.ctypes.data_as(dp) for o in outs])))
+    per = [s._get1(f) for f in fields]
+    for a, b in zip(outs, per):
+        assert np.array_equal(a, b)
+    rng = np.random.default_rng(3)
+    new = [rng.normal(size=n) for _ in range(6)]
+    md._check(L.md_system_set_fields(s.handle, 6, (C.c_int * 6)(*fields[:6]),
+                                     (dp * 6)(*[a.ctypes.data_as(dp) for a in new])))
+    assert np.array_equal(s.positions, np.stack(new[:3], 1))
+    assert np.array_equal(s.velocities, np.stack(new[3:6], 1))
+    with pytest.raises(md.InvalidArgument):
+        md._check(L.md_system_set_fields(s.handle, 1, (C.c_int * 1)(42),
+                                         (dp * 1)(new[0].ctypes.data_as(dp))))
