@@ -297,7 +297,7 @@ int pme_create(md_context* ctx, const int K[3], int order, PmeState** out) {
         (rc = s->real.ensure(sizeof(double) * cells)) != MD_OK ||
         (rc = s->spec.ensure(sizeof(double2) * half)) != MD_OK ||
         (rc = s->bmod.ensure(sizeof(double) * (K[0] + K[1] + K[2]))) != MD_OK ||
-        (rc = s->part.ensure(sizeof(double) * 2 * 4 * 148 * 4)) != MD_OK) {
+        (rc = s->part.ensure(sizeof(double) * 2 * 4 * static_cast<size_t>(ctx->sm_count))) != MD_OK) {
         delete s;
         return rc;
     }
