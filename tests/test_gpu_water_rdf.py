@@ -208,3 +208,24 @@ def test_cxx_app_equals_the_python_driver(md, tmp_path):
     b = [l for l in (tmp_path / "py.csv").read_text().splitlines() if not l.startswith(skip)]
     assert len(a) == len(b) == 219
     assert a == b
+
+
+def test_python_cli_writes_the_csv(md, tmp_path, capsys):
+    """python -m moleculardynamics_b200.water_rdf with the reference's flags on a
+    short protocol: the summary lines and the CSV (header, 200 rows)."""
+    from moleculardynamics_b200 import water_rdf as W
+    pos, types, box = config3()
+    cfg_dir = tmp_path / "data" / "nist" / "spce"
+    cfg_dir.mkdir(parents=True)
+    lines = ["%25.12E%25.12E%25.12E" % tuple(box), "%12d" % (len(types) // 3)]
+    lines += ["%5d%25.12E%25.12E%25.12E    %s" % (k + 1, *p, t) for k, (p, t) in enumerate(zip(pos, types))]
+    (cfg_dir / "spce_sample_config_periodic3.txt").write_text("\n".join(lines) + "\n")
+    out = tmp_path / "res" / "w.csv"
+    rc = W.main(["water_rdf", "--data", str(tmp_path / "data"), "--out", str(out),
+                 "--equilibrate", "100", "--production", "50", "--sample-every", "5", "--settle"])
+    assert rc == 0
+    printed = capsys.readouterr().out
+    assert "300 molecules, L = 20.8020 A" in printed and "O-O first peak" in printed
+    text = out.read_text().splitlines()
+    assert text[3] == "# model: SPC/E, rigid (SETTLE), Ewald alpha=5.6/L kmax=5 rcut=10 A"
+    assert text[12] == "# rdf_frames: 10" and text[22] == "r_angstrom,g_oo" and len(text) == 223
