@@ -419,6 +419,21 @@ namespace mdb {
 // Counts are integers, so summing them per bin on the device over frames equals
 // the reference's running double sum (rdf.cpp:73) exactly.
 int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t stride) {
+    MDB_TRY(rdf_frame_launch(r, sys, first, stride));
+    rdf_frame_note(r, sys, first, stride);
+    return MD_OK;
+}
+
+void rdf_frame_note(md_rdf* r, const md_system* sys, int64_t first, int64_t stride) {
+    const int64_t n = sys->n;
+    const int64_t selected = n > first ? (n - first + stride - 1) / stride : 0;
+    if (selected > 1 && r->bins > 0 && r->rmax > 0.0) r->stale = true;
+    r->natoms = selected;  // rdf.cpp:79-81
+    r->sum_rho += static_cast<double>(selected) / (sys->box[0] * sys->box[1] * sys->box[2]);
+    ++r->frames;
+}
+
+int rdf_frame_launch(md_rdf* r, md_system* sys, int64_t first, int64_t stride) {
     if (!r || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_accumulate: NULL argument");
     if (first < 0 || stride < 1)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_accumulate_subset: first >= 0, stride >= 1");
@@ -473,11 +488,7 @@ int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t strid
         }
         ++ctx->launches;
         MDB_CHECK_LAUNCH();
-        r->stale = true;
     }
-    r->natoms = selected;  // rdf.cpp:79-81
-    r->sum_rho += static_cast<double>(selected) / (sys->box[0] * sys->box[1] * sys->box[2]);
-    ++r->frames;
     return MD_OK;
 }
 

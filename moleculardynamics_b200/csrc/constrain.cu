@@ -24,6 +24,7 @@ int record_async(md_context* ctx, const double* ev, const double* ke, const NhcS
                  double* row);
 int ewald_eval_async(md_ewald* ew, md_system* sys, int mode, bool gated);
 int system_kinetic_async(md_system* sys, int slot);
+int record_at_async(md_context* ctx, const NhcState* nhc, double* rows, int* idx);
 }  // namespace mdb
 
 namespace mdb {
@@ -625,6 +626,43 @@ __global__ void k_sum_temperature(const double* __restrict__ ke, double dof, dou
     acc[0] += 2.0 * ke[0] / dof;
 }
 
+// A block of work captured once from the context's stream and replayed: the same
+// kernels with the same arguments as the eager launches it replaces, so results
+// are identical.  Buffers must already have their final sizes (an eager block
+// runs first).  launches counts the kernels of one replay.
+struct BlockGraph {
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+    ~BlockGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
+template <class F>
+int capture_block(md_context* ctx, F&& work, BlockGraph& bg) {
+    MDB_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t l0 = ctx->launches;
+    const int rc = work();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    bg.launches = ctx->launches - l0;
+    ctx->launches = l0;
+    if (rc != MD_OK || e != cudaSuccess || cudaGraphInstantiate(&bg.exec, graph, 0) != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        bg.exec = nullptr;
+        cudaGetLastError();  // no graph: the caller launches eagerly
+        return rc != MD_OK ? rc : MD_ERR_CUDA;
+    }
+    cudaGraphDestroy(graph);
+    return MD_OK;
+}
+
+int replay(md_context* ctx, const BlockGraph& bg) {
+    MDB_CUDA(cudaGraphLaunch(bg.exec, ctx->stream));
+    ctx->launches += bg.launches;
+    return MD_OK;
+}
+
 }  // namespace
 
 int constrained_pre_force(md_integrator* it, md_system* sys) {
@@ -811,16 +849,34 @@ int md_run_spce(md_integrator* it, md_system* sys, md_ewald* ff, int64_t steps, 
     SpceLoop L;
     MDB_TRY(spce_loop_begin(it, sys, ff, "md_run_spce", L));
     md_context* ctx = sys->ctx;
-    DevBuf rows;
-    if (thermo && steps > 0) MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
-    for (int64_t k = 0; k < steps; ++k)
-        MDB_TRY(spce_step_async(L, k == 0, rows.ptr ? rows.as<double>() + 4 * k : nullptr));
+    DevBuf rows, idx;
+    if (thermo && steps > 0) {
+        MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
+        MDB_TRY(idx.ensure(sizeof(int)));
+        MDB_CUDA(cudaMemsetAsync(idx.ptr, 0, sizeof(int), ctx->stream));
+    }
+    // One step with its thermo row at a device-held index; after the first (eager)
+    // step it is captured once and replayed, unless kernel timing is on.
+    auto one_step = [&](bool first) -> int {
+        MDB_TRY(spce_step_async(L, first, nullptr));
+        if (rows.ptr) MDB_TRY(record_at_async(ctx, L.nhc, rows.as<double>(), idx.as<int>()));
+        return MD_OK;
+    };
+    BlockGraph bg;
+    const bool want_graph = ctx->graphs && !ctx->timing && steps >= 4;
+    for (int64_t k = 0; k < steps; ++k) {
+        // a failed capture leaves no graph: the eager launches then report any error
+        if (k == 1 && want_graph) capture_block(ctx, [&] { return one_step(false); }, bg);
+        if (bg.exec) MDB_TRY(replay(ctx, bg));
+        else MDB_TRY(one_step(k == 0));
+    }
     if (L.nhc && steps > 0) MDB_TRY(nhc_apply_scale_async(it, sys));
     if (rows.ptr)
         MDB_CUDA(cudaMemcpyAsync(thermo, rows.ptr, sizeof(double) * 4 * static_cast<size_t>(steps),
                                  cudaMemcpyDeviceToHost, ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
     rows.release();
+    idx.release();
     MDB_TRY(status_to_error(ctx));
     return ctx_check_status(ctx);
 }
@@ -845,29 +901,51 @@ int md_water_rdf_run(md_integrator* it, md_system* sys, md_ewald* ff, md_rdf* rd
     // apps/water_rdf.cpp:188-200: every rescale_every steps the velocities are
     // scaled toward the target and put back on the constraint surface (RATTLE's
     // velocity half, rigid_water.cpp:107-162, as constrainVelocities does).
-    for (int64_t step = 0; step < equilibrate; ++step) {
-        MDB_TRY(spce_step_async(L, step == 0, nullptr));
-        if ((step + 1) % rescale_every == 0) {
-            MDB_TRY(md_system_rescale_temperature(sys, dof, temperature));
-            if (L.nmol > 0) {
-                k_rattle<<<grid_for(L.nmol, kBlock), kBlock, 0, ctx->stream>>>(
-                    sys->cur, sys->slot, L.nmol, rigid_args(it->rigid), box_of(sys),
-                    it->counters.as<int>() + 1, ctx->d_status);
-                ++ctx->launches;
-                MDB_CHECK_LAUNCH();
-            }
+    auto eq_block = [&](int64_t steps, bool first, bool rescale) -> int {
+        for (int64_t k = 0; k < steps; ++k) MDB_TRY(spce_step_async(L, first && k == 0, nullptr));
+        if (!rescale) return MD_OK;
+        MDB_TRY(md_system_rescale_temperature(sys, dof, temperature));
+        if (L.nmol > 0) {
+            k_rattle<<<grid_for(L.nmol, kBlock), kBlock, 0, ctx->stream>>>(
+                sys->cur, sys->slot, L.nmol, rigid_args(it->rigid), box_of(sys),
+                it->counters.as<int>() + 1, ctx->d_status);
+            ++ctx->launches;
+            MDB_CHECK_LAUNCH();
         }
-    }
+        return MD_OK;
+    };
     // apps/water_rdf.cpp:207-216: NVE production; the temperature of every
     // step is summed, and the oxygens (first site of each O, H, H triple) are
     // binned every sample_every steps.
-    for (int64_t step = 0; step < production; ++step) {
-        MDB_TRY(spce_step_async(L, equilibrate == 0 && step == 0, nullptr));
-        k_sum_temperature<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResKE), static_cast<double>(dof),
-                                                    acc.as<double>());
-        ++ctx->launches;
-        if ((step + 1) % sample_every == 0) MDB_TRY(rdf_accumulate_async(rdf, sys, 0, 3));
+    auto prod_block = [&](int64_t steps, bool first, bool frame) -> int {
+        for (int64_t k = 0; k < steps; ++k) {
+            MDB_TRY(spce_step_async(L, first && k == 0, nullptr));
+            k_sum_temperature<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResKE),
+                                                        static_cast<double>(dof), acc.as<double>());
+            ++ctx->launches;
+        }
+        if (frame) MDB_TRY(rdf_frame_launch(rdf, sys, 0, 3));
+        return MD_OK;
+    };
+    // Whole blocks after the first (eager, it sizes every buffer) replay one
+    // captured graph each: the same launches in the same order.
+    const bool want_graph = ctx->graphs && !ctx->timing;
+    const int64_t eq_blocks = equilibrate / rescale_every;
+    BlockGraph ge, gp;
+    for (int64_t b = 0; b < eq_blocks; ++b) {
+        if (b == 1 && want_graph) capture_block(ctx, [&] { return eq_block(rescale_every, false, true); }, ge);
+        if (ge.exec) MDB_TRY(replay(ctx, ge));
+        else MDB_TRY(eq_block(rescale_every, b == 0, true));
     }
+    MDB_TRY(eq_block(equilibrate % rescale_every, eq_blocks == 0, false));
+    const int64_t prod_blocks = production / sample_every;
+    for (int64_t b = 0; b < prod_blocks; ++b) {
+        if (b == 1 && want_graph) capture_block(ctx, [&] { return prod_block(sample_every, false, true); }, gp);
+        if (gp.exec) MDB_TRY(replay(ctx, gp));
+        else MDB_TRY(prod_block(sample_every, equilibrate == 0 && b == 0, true));
+        rdf_frame_note(rdf, sys, 0, 3);
+    }
+    MDB_TRY(prod_block(production % sample_every, equilibrate == 0 && prod_blocks == 0, false));
     double sum = 0.0;
     MDB_CUDA(cudaMemcpyAsync(&sum, acc.ptr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -428,6 +428,14 @@ int vv_pre_async(md_integrator* it, md_system* sys, md_verlet* check) {
 
 int vv_post_async(md_integrator* it, md_system* sys) { return post_force_async(it, sys, true); }
 
+int record_at_async(md_context* ctx, const NhcState* nhc, double* rows, int* idx) {
+    k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE), nhc,
+                                          rows, idx);
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
 // The fixed-point position buffer the step's kick/drift fills for a mixed force
 // (null when the force is FP64 or the integrator has no kick/drift kernel).
 int step_quantize_target(md_integrator* it, md_system* sys, const md_lj* lj, int4** q) {

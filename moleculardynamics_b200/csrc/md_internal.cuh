@@ -172,6 +172,11 @@ int cell_sort(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_start)
 // histogram, no host synchronisation; rdf_sync refreshes the host counts.
 int rdf_accumulate_async(md_rdf* r, md_system* sys, int64_t first, int64_t stride);
 int rdf_sync(const md_rdf* r);
+// The two halves of rdf_accumulate_async: the device work of a frame (capturable
+// into a graph once the first frame has sized every buffer) and the host
+// bookkeeping (frame count, density sum) each frame needs.
+int rdf_frame_launch(md_rdf* r, md_system* sys, int64_t first, int64_t stride);
+void rdf_frame_note(md_rdf* r, const md_system* sys, int64_t first, int64_t stride);
 
 // Smooth particle-mesh Ewald reciprocal term (pme.cu): grid and cuFFT plans of
 // one Ewald handle.  pme_eval_async writes the reciprocal energy and virial trace
