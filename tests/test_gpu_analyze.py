@@ -144,3 +144,20 @@ def test_msd_rejects_a_system_of_another_size(md):
     msd = md.Msd(s.n + 1, 3)
     with pytest.raises(md.InvalidArgument):
         msd.push(s)
+
+
+@pytest.mark.parametrize("first,stride", [(1, 2), (5, 7)])
+def test_rdf_subset_on_the_cell_path(md, first, stride):
+    """A subset frame (atoms first, first + stride, ...) through the cell grid
+    (4 cells of width rMax per side) equals the oracle's Rdf of those atoms."""
+    s, v, lj, box = liquid(md, 10, 0.8442, 9)
+    rdf = md.Rdf(4.0, 80)
+    pos, _ = frames_of(md, s, v, lj, 2, 30)
+    frames = []
+    for p in pos:
+        s.positions = p
+        rdf.accumulate(s, first, stride)
+        frames.append(p[first::stride])
+    hist, g = O.rdf(frames, box, 4.0, 80)
+    assert np.array_equal(rdf.histogram(), hist)
+    assert np.array_equal(rdf.g(), g)

@@ -50,6 +50,22 @@ def test_pme_equals_the_restatement(md, c, K, order):
     assert np.max(np.abs(f - f_or)) < 1e-9 * scale
 
 
+def test_pme_in_a_non_cubic_box(md):
+    """Configuration 1 stretched by (1, 1.25, 1.1) along the axes (the sites
+    scaled with the box): unequal box lengths and grid spacings per axis."""
+    scale = np.array([1.0, 1.25, 1.1])
+    types = ["O" if o else "H" for o in SPCE["isO1"]]
+    box = SPCE["box1"] * scale
+    s = md.build_spce_system(SPCE["pos1"] * scale, types, box)
+    ew = md.Ewald(10.0, 5, 0.3)
+    ew.set_pme((24, 30, 28), 6)
+    t, f, w = recip_forces(md, s, ew)
+    e_or, w_or, f_or = O.pme_recip(s.positions, box, s.charges, 0.3, (24, 30, 28), 6)
+    assert t["reciprocal"] == pytest.approx(e_or, rel=1e-11)
+    assert w == pytest.approx(w_or, rel=1e-9, abs=1e-9 * abs(e_or))
+    assert np.max(np.abs(f - f_or)) < 1e-9 * np.sqrt(np.mean(f_or ** 2))
+
+
 def test_pme_converges_to_the_ewald_sum(md):
     s = water(md, 1)
     ew = md.Ewald(10.0, 12)
