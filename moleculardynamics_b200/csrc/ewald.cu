@@ -89,8 +89,10 @@ __device__ __forceinline__ float real_pair_mixed(float r2, float cqq, bool coulo
 // E_real, W_real, E_lj, W_lj.  mode 1 writes forces, mode 2 adds to them.
 // MIXED: the displacement, the cutoff test and every sum stay FP64; the pair
 // terms (erfc, exp, the LJ powers) are evaluated in FP32.
+// 128-thread blocks (kRealBlock); the FP64 variant fits six per SM in 78
+// registers without spilling, the FP32 one five.
 template <int TPA, bool MIXED>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(128, MIXED ? 5 : 6)
 k_ewald_real(const double4* __restrict__ pos, const double* __restrict__ q,
              const int64_t* __restrict__ mol, const int* __restrict__ nbr,
              const int* __restrict__ count, int stride, int64_t n, Box3 box, RealArgs a,
@@ -579,8 +581,8 @@ int real_tpa(const md_context* ctx, int64_t n) {
     return tpa;
 }
 
-// 128-thread blocks: at the kernel's ~96 registers five fit on an SM (20 warps)
-// where two 256-thread blocks would (16).
+// 128-thread blocks: six (FP64) or five (FP32 pair terms) fit on an SM, 24 or 20
+// warps, where two 256-thread blocks at ~96 registers would give 16.
 constexpr int kRealBlock = 128;
 
 template <int TPA, bool MIXED>
