@@ -220,8 +220,8 @@ public:
             const double* f[11] = {h_.x.data(), h_.y.data(), h_.z.data(), h_.vx.data(),
                                    h_.vy.data(), h_.vz.data(), h_.fx.data(), h_.fy.data(),
                                    h_.fz.data(), h_.mass.data(), h_.charge.data()};
-            for (int k = 0; k < 11; ++k)
-                if (size()) detail::check(md_system_set(dev_, k, f[k]));
+            static const int fields[11] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
+            if (size()) detail::check(md_system_set_fields(dev_, 11, fields, f));
             if (size()) detail::check(md_system_set_molecule_ids(dev_, h_.mol.data()));
             host_dirty_ = false;
         }
@@ -241,8 +241,8 @@ private:
         if (!device_ahead_ || !dev_) return;
         double* f[9] = {h_.x.data(), h_.y.data(), h_.z.data(), h_.vx.data(), h_.vy.data(),
                         h_.vz.data(), h_.fx.data(), h_.fy.data(), h_.fz.data()};
-        for (int k = 0; k < 9; ++k)
-            if (size()) detail::check(md_system_get(dev_, k, f[k]));
+        static const int fields[9] = {0, 1, 2, 3, 4, 5, 6, 7, 8};
+        if (size()) detail::check(md_system_get_fields(dev_, 9, fields, f));
         device_ahead_ = false;
     }
     void edit() {
