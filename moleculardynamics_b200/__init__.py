@@ -215,6 +215,7 @@ def _load():
         "md_batch_destroy": (C.c_int, [_vp]),
         "md_batch_add": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int)]),
         "md_batch_size": (C.c_int, [_vp]),
+        "md_batch_set_batched": (C.c_int, [_vp, C.c_int]),
         "md_batch_run": (C.c_int, [_vp, C.c_int64, _d]),
         "md_adjoint_create": (C.c_int, [_vp, C.POINTER(_vp)]),
         "md_adjoint_destroy": (C.c_int, [_vp]),
@@ -1189,6 +1190,11 @@ class Batch:
                                   lj.handle, C.byref(idx)))
         self._keep.append((integrator, sys, verlet, lj))
         return idx.value
+
+    def set_batched(self, on=True):
+        """Stage kernels shared by all replicas (default) or a graph of
+        per-replica kernels; every replica's trajectory is the same either way."""
+        _check(lib().md_batch_set_batched(self._h, 1 if on else 0))
 
     def __len__(self):
         return lib().md_batch_size(self._h)

@@ -17,6 +17,7 @@
 
 namespace mdb {
 int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
+int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 }
 
 struct md_batch {
@@ -28,6 +29,7 @@ struct md_batch {
     };
     std::vector<Replica> reps;
     int device = -1;
+    int batched = 1;  // batched stage kernels when the replicas allow them
 };
 
 using namespace mdb;
@@ -62,6 +64,103 @@ int read_rebuilds(md_verlet* v, cudaStream_t s, int* out) {
     return MD_OK;
 }
 
+// Captures work() from `stream` into graph g after deps; leaves (optional) gets
+// the last captured nodes.  The stream leaves capture whatever happened.
+template <class F>
+int capture_to(cudaStream_t stream, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
+               F&& work, std::vector<cudaGraphNode_t>* leaves) {
+    MDB_CUDA(cudaStreamBeginCaptureToGraph(stream, g, deps, nullptr, ndeps,
+                                           cudaStreamCaptureModeThreadLocal));
+    int rc = work();
+    if (rc == MD_OK && leaves) {
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* out = nullptr;
+        size_t nout = 0;
+        if (cudaStreamGetCaptureInfo(stream, &st, nullptr, nullptr, &out, &nout) != cudaSuccess)
+            rc = fail(MD_ERR_CUDA, "md_batch_run: capture info");
+        else leaves->assign(out, out + nout);
+    }
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(stream, &captured);
+    if (rc != MD_OK) return rc;
+    if (e != cudaSuccess) return fail(MD_ERR_CUDA, "md_batch_run: capture: %s", cudaGetErrorString(e));
+    return MD_OK;
+}
+
+// The step graph of batched stage kernels: the chain halves and kick/drift of
+// every replica in one launch (its rebuild test sets each replica's branch),
+// one conditional rebuild branch per replica, then the force pass and the
+// kick, kinetic energy, chain half and thermo row of every replica in three
+// launches.  Per replica the work and its order are those of its solo step.
+struct BatchedStep {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BatchKick* kick = nullptr;
+    BatchForce* force = nullptr;
+    int64_t lead_launches = 0;
+    std::vector<int64_t> body_launches;
+    ~BatchedStep() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        batch_kick_destroy(kick);
+        batch_force_destroy(force);
+    }
+};
+
+// Builds the batched step graph, or leaves bs.exec null when the replicas need
+// the per-replica graph (kernels that cannot share a launch).
+int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
+    const size_t nr = b->reps.size();
+    if (cudaGraphCreate(&bs.graph, 0) != cudaSuccess) return fail(MD_ERR_CUDA, "cudaGraphCreate");
+    std::vector<BatchRepView> views(nr);
+    for (size_t k = 0; k < nr; ++k) {
+        const auto& r = b->reps[k];
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, bs.graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+            return fail(MD_ERR_CUDA, "md_batch_run: conditional handle");
+        views[k] = BatchRepView{r.it, r.sys, r.list, r.lj, run[k].rows.as<double>(),
+                                run[k].idx.as<int>(), h};
+    }
+    if (batch_force_create(views.data(), static_cast<int>(nr), &bs.force) != MD_OK ||
+        batch_kick_create(views.data(), static_cast<int>(nr), &bs.kick) != MD_OK) {
+        cudaGetLastError();
+        return MD_OK;  // not batchable: the caller uses the per-replica graph
+    }
+    cudaStream_t lead = b->reps[0].sys->ctx->stream;
+    std::vector<cudaGraphNode_t> pre;
+    MDB_TRY(capture_to(lead, bs.graph, nullptr, 0,
+                       [&]() { return batch_kick_pre(bs.kick, lead, &bs.lead_launches); }, &pre));
+    std::vector<cudaGraphNode_t> conds(nr);
+    bs.body_launches.assign(nr, 0);
+    for (size_t k = 0; k < nr; ++k) {
+        auto& r = b->reps[k];
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = views[k].cond;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        const cudaError_t e = cudaGraphAddNode(&conds[k], bs.graph, pre.data(), pre.size(), &cp);
+        if (e != cudaSuccess) return fail(MD_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
+        md_context* ctx = r.sys->ctx;
+        const int64_t l0 = ctx->launches;
+        MDB_TRY(capture_to(ctx->stream, cp.conditional.phGraph_out[0], nullptr, 0, [&]() -> int {
+            MDB_TRY(verlet_build(r.list, r.sys, true));
+            return lj_quantize_async(r.lj, r.sys, r.list->d_rebuild_flag);
+        }, nullptr));
+        bs.body_launches[k] = ctx->launches - l0;
+        ctx->launches = l0;  // counted per rebuild by the caller
+    }
+    MDB_TRY(capture_to(lead, bs.graph, conds.data(), conds.size(), [&]() -> int {
+        MDB_TRY(batch_force_launch(bs.force, lead, &bs.lead_launches));
+        return batch_kick_post(bs.kick, lead, &bs.lead_launches);
+    }, nullptr));
+    if (cudaGraphInstantiate(&bs.exec, bs.graph, 0) != cudaSuccess) {
+        bs.exec = nullptr;
+        return fail(MD_ERR_CUDA, "md_batch_run: batched graph instantiation failed");
+    }
+    return MD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -91,6 +190,12 @@ int md_batch_add(md_batch* b, md_integrator* it, md_system* sys, md_verlet* list
 }
 
 int md_batch_size(const md_batch* b) { return b ? static_cast<int>(b->reps.size()) : 0; }
+
+int md_batch_set_batched(md_batch* b, int on) {
+    if (!b) return fail(MD_ERR_INVALID_ARGUMENT, "md_batch_set_batched: NULL batch");
+    b->batched = on ? 1 : 0;
+    return MD_OK;
+}
 
 int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     if (!b) return fail(MD_ERR_INVALID_ARGUMENT, "md_batch_run: NULL batch");
@@ -123,7 +228,24 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     cudaStream_t lead = b->reps[0].sys->ctx->stream;
     int rc = MD_OK;
     std::vector<int64_t> main_l(nr, 0), body_l(nr, 0);
-    if (steps > 1) {
+    BatchedStep bs;
+    if (steps > 1 && b->batched) {
+        MDB_TRY(build_batched_step(b, run, bs));
+        if (bs.exec) {
+            for (size_t k = 0; k < nr; ++k) {
+                md_context* ctx = b->reps[k].sys->ctx;
+                MDB_TRY(read_rebuilds(b->reps[k].list, ctx->stream, &run[k].rebuilt0));
+                MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+            }
+            for (int64_t s = 1; s < steps; ++s)
+                if (cudaGraphLaunch(bs.exec, lead) != cudaSuccess)
+                    return fail(MD_ERR_CUDA, "md_batch_run: graph launch failed");
+            MDB_CUDA(cudaStreamSynchronize(lead));
+            b->reps[0].sys->ctx->launches += (steps - 1) * bs.lead_launches;
+            for (size_t k = 0; k < nr; ++k) body_l[k] = bs.body_launches[k];
+        }
+    }
+    if (steps > 1 && !bs.exec) {
         if (cudaGraphCreate(&graph, 0) != cudaSuccess) return fail(MD_ERR_CUDA, "cudaGraphCreate");
         for (size_t k = 0; k < nr && rc == MD_OK; ++k) {
             auto& r = b->reps[k];

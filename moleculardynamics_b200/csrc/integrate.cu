@@ -54,8 +54,10 @@ __device__ __forceinline__ double disp2(const Fold3& f3, double4 p, double4 q) {
 // CHECK the kernel also reduces the top-2 displacement since the last Verlet build
 // and writes the device rebuild flag (verlet_list.cpp:44-63), saving a pass.
 template <bool CHECK>
-__global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc, DispArgs d) {
-    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+__device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const StepArgs& s,
+                                                const NhcState* nhc, const DispArgs& d,
+                                                unsigned block, unsigned nblocks) {
+    const int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     double a1 = 0.0;
     if (k < n) {
         double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
@@ -82,7 +84,12 @@ __global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* 
         if (s.q) s.q[k] = quantize_position(p, s.qs[0], s.qs[1], s.qs[2]);
         if (CHECK) a1 = disp2(f3, p, d.ref[k]);
     }
-    if (CHECK) top2_grid(a1, 0.0, d);
+    if (CHECK) top2_grid_at(a1, 0.0, d, block, nblocks);
+}
+
+template <bool CHECK>
+__global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc, DispArgs d) {
+    kick_drift_body<CHECK>(a, n, s, nhc, d, blockIdx.x, gridDim.x);
 }
 
 // langevin.hpp:55-80: B, A (wrap), O, A (wrap).
@@ -137,11 +144,12 @@ __global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s, DispArgs d) {
 }
 
 // Second half-kick (velocity_verlet.hpp:70-73), fused with the kinetic-energy sum.
-__global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsigned* ticket,
-                          double* out, uint32_t* status) {
+__device__ __forceinline__ void kick_ke_body(md_atoms a, int64_t n, const StepArgs& s, double* part,
+                                             unsigned* ticket, double* out, uint32_t* status,
+                                             unsigned block, unsigned nblocks) {
     double ke[1] = {0.0};
-    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    for (int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(nblocks) * blockDim.x) {
         const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
         const double vx = fma(c, a.fx[k], a.vx[k]);
         const double vy = fma(c, a.fy[k], a.vy[k]);
@@ -151,7 +159,12 @@ __global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsig
         a.vz[k] = vz;
         ke[0] += 0.5 * a.mass[k] * (vx * vx + vy * vy + vz * vz);
     }
-    grid_reduce<1>(ke, part, ticket, out, status);  // a NaN anywhere reaches the kinetic energy
+    grid_reduce_at<1>(ke, part, ticket, out, status, block, nblocks);  // a NaN reaches the KE
+}
+
+__global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsigned* ticket,
+                          double* out, uint32_t* status) {
+    kick_ke_body(a, n, s, part, ticket, out, status, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_scale(md_atoms a, int64_t n, NhcState* nhc) {
@@ -199,7 +212,7 @@ struct Weights {
 };
 
 // Start-of-step chain half: KE of the current velocities (pending scale included).
-__global__ void k_nhc_pre(NhcState* st, const double* ke_now, Weights w) {
+__device__ __forceinline__ void nhc_pre_body(NhcState* st, const double* ke_now, const Weights& w) {
     NhcState c = *st;
     double ke = ke_now ? *ke_now * c.scale * c.scale : c.ke;
     const double f = nhc_half(c, 0.5 * c.dt, w.w, ke);
@@ -208,14 +221,18 @@ __global__ void k_nhc_pre(NhcState* st, const double* ke_now, Weights w) {
     *st = c;
 }
 
+__global__ void k_nhc_pre(NhcState* st, const double* ke_now, Weights w) { nhc_pre_body(st, ke_now, w); }
+
 // End-of-step chain half using the freshly summed KE; leaves its scale pending.
-__global__ void k_nhc_post(NhcState* st, const double* ke_sum, Weights w) {
+__device__ __forceinline__ void nhc_post_body(NhcState* st, const double* ke_sum, const Weights& w) {
     NhcState c = *st;
     double ke = *ke_sum;
     c.scale = nhc_half(c, 0.5 * c.dt, w.w, ke);
     c.ke = ke;
     *st = c;
 }
+
+__global__ void k_nhc_post(NhcState* st, const double* ke_sum, Weights w) { nhc_post_body(st, ke_sum, w); }
 
 __device__ double nhc_conserved(const NhcState& c) {
     // nose_hoover.cpp:45-54
@@ -578,6 +595,187 @@ int record_async(md_context* ctx, const double* ev, const double* ke, const NhcS
 
 int constrained_pre_force(md_integrator* it, md_system* sys);
 int constrained_post_force(md_integrator* it, md_system* sys, bool apply_scale);
+
+// ------------------------------------------------------------ batched replicas
+// One replica's arguments of the batched kick kernels: what pre_force (no fresh
+// kinetic energy, the rebuild test fused in) and post_force_async give its solo
+// kernels, plus its thermo row.
+struct BatchKickRep {
+    md_atoms a;
+    int64_t n;
+    StepArgs s;
+    NhcState* nhc;
+    DispArgs d;
+    double* ke_part;
+    unsigned* ke_ticket;
+    double* ke_out;
+    uint32_t* status;
+    const double* ev;
+    double* rows;
+    int* idx;
+};
+
+namespace {
+
+__device__ __forceinline__ int replica_of_block(const int* __restrict__ off, int nrep, int b) {
+    int lo = 0, hi = nrep;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Start-of-step chain halves, one thread per replica (k_nhc_pre without a fresh KE).
+__global__ void k_batch_nhc_pre(const BatchKickRep* __restrict__ reps, int nrep, Weights w) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep && reps[r].nhc) nhc_pre_body(reps[r].nhc, nullptr, w);
+}
+
+// Kick/drift with the rebuild test of every replica; a replica's last block also
+// sets its rebuild branch's conditional.
+__global__ void k_batch_kick_drift(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
+                                   int nrep) {
+    const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
+    const BatchKickRep& d = reps[r];
+    const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
+    kick_drift_body<true>(d.a, d.n, d.s, d.nhc, d.d, blockIdx.x - b0, b1 - b0);
+}
+
+__global__ void k_batch_kick_ke(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
+                                int nrep) {
+    const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
+    const BatchKickRep& d = reps[r];
+    const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
+    kick_ke_body(d.a, d.n, d.s, d.ke_part, d.ke_ticket, d.ke_out, d.status, blockIdx.x - b0, b1 - b0);
+}
+
+// End-of-step chain halves and thermo rows (k_nhc_post, k_record_at), one thread per replica.
+__global__ void k_batch_nhc_post(const BatchKickRep* __restrict__ reps, int nrep, Weights w) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrep) return;
+    const BatchKickRep& d = reps[r];
+    if (d.nhc) nhc_post_body(d.nhc, d.ke_out, w);
+    if (d.rows) {
+        double* row = d.rows + 4 * static_cast<int64_t>(*d.idx);
+        row[0] = d.ev[0];
+        row[1] = d.ev[1];
+        row[2] = d.nhc ? d.nhc->ke : *d.ke_out;
+        row[3] = d.nhc ? nhc_conserved(*d.nhc) : 0.0;
+        ++*d.idx;
+    }
+}
+
+}  // namespace
+
+struct BatchKick {
+    DevBuf reps, kick_off, ke_off;
+    int nrep = 0, kick_total = 0, ke_total = 0;
+    bool any_nhc = false, any_rows = false;
+};
+
+int batch_kick_create(const BatchRepView* v, int nrep, BatchKick** out) {
+    if (nrep < 1) return fail(MD_ERR_INVALID_ARGUMENT, "batch_kick_create: no replicas");
+    std::vector<BatchKickRep> h(static_cast<size_t>(nrep));
+    std::vector<int> ko(static_cast<size_t>(nrep) + 1, 0), eo(static_cast<size_t>(nrep) + 1, 0);
+    bool any_nhc = false, any_rows = false;
+    for (int r = 0; r < nrep; ++r) {
+        md_integrator* it = v[r].it;
+        md_system* sys = v[r].sys;
+        md_context* ctx = sys->ctx;
+        if ((it->kind != 0 && it->kind != 2) || sys->n <= 0)
+            return fail(MD_ERR_INVALID_ARGUMENT, "batch_kick_create: velocity Verlet or NHC replicas");
+        BatchKickRep& d = h[static_cast<size_t>(r)];
+        d.a = sys->cur;
+        d.n = sys->n;
+        d.s = step_args(it, sys);
+        int4* q = nullptr;
+        MDB_TRY(step_quantize_target(it, sys, v[r].lj, &q));
+        if (q) {
+            d.s.q = q;
+            for (int k = 0; k < 3; ++k) d.s.qs[k] = 4294967296.0 / sys->box[k];
+        }
+        const int blocks = grid_for(sys->n, kBlock);
+        double* part;
+        MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+        d.d = disp_args(v[r].list, ctx, part);
+        d.d.cond = v[r].cond;
+        d.d.set_cond = 1;
+        d.nhc = nhc_of(it);
+        const int g = kick_grid(sys);
+        MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
+        d.ke_part = part;
+        d.ke_ticket = ctx_counter(ctx, 3);
+        d.ke_out = ctx_result(ctx, kResKE);
+        d.status = ctx->d_status;
+        d.ev = ctx_result(ctx, kResEnergy);
+        d.rows = v[r].rows;
+        d.idx = v[r].idx;
+        any_nhc = any_nhc || d.nhc;
+        any_rows = any_rows || d.rows;
+        ko[static_cast<size_t>(r) + 1] = ko[static_cast<size_t>(r)] + blocks;
+        eo[static_cast<size_t>(r) + 1] = eo[static_cast<size_t>(r)] + g;
+    }
+    BatchKick* b = new (std::nothrow) BatchKick();
+    if (!b) return fail(MD_ERR_OUT_OF_MEMORY, "batch_kick_create: host allocation");
+    b->nrep = nrep;
+    b->kick_total = ko.back();
+    b->ke_total = eo.back();
+    b->any_nhc = any_nhc;
+    b->any_rows = any_rows;
+    int rc = b->reps.ensure(sizeof(BatchKickRep) * h.size());
+    if (rc == MD_OK) rc = b->kick_off.ensure(sizeof(int) * ko.size());
+    if (rc == MD_OK) rc = b->ke_off.ensure(sizeof(int) * eo.size());
+    if (rc == MD_OK &&
+        (cudaMemcpy(b->reps.ptr, h.data(), sizeof(BatchKickRep) * h.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess ||
+         cudaMemcpy(b->kick_off.ptr, ko.data(), sizeof(int) * ko.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess ||
+         cudaMemcpy(b->ke_off.ptr, eo.data(), sizeof(int) * eo.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess))
+        rc = fail(MD_ERR_CUDA, "batch_kick_create: descriptor upload");
+    if (rc != MD_OK) {
+        batch_kick_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return MD_OK;
+}
+
+int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches) {
+    if (b->any_nhc) {
+        k_batch_nhc_pre<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                                   b->nrep, yoshida());
+        if (launches) ++*launches;
+    }
+    k_batch_kick_drift<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                             b->kick_off.as<int>(), b->nrep);
+    if (launches) ++*launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches) {
+    k_batch_kick_ke<<<b->ke_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                        b->ke_off.as<int>(), b->nrep);
+    if (launches) ++*launches;
+    if (b->any_nhc || b->any_rows) {
+        k_batch_nhc_post<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                                    b->nrep, yoshida());
+        if (launches) ++*launches;
+    }
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+void batch_kick_destroy(BatchKick* b) {
+    if (!b) return;
+    b->reps.release();
+    b->kick_off.release();
+    b->ke_off.release();
+    delete b;
+}
 
 }  // namespace mdb
 

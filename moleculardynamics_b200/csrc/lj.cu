@@ -258,14 +258,17 @@ struct PosOf<true> {
     static __device__ __forceinline__ T load(const T* p) { return __ldg(p); }
 };
 
+// The Verlet-list force pass of one system, for block `block` of `nblocks`
+// (a batched launch gives each system's blocks their own rank and count).
 template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
-__global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
-k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
-            const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
-            Box3 box, LJArgs a, double* __restrict__ fxo, double* __restrict__ fyo,
-            double* __restrict__ fzo, double* part, unsigned* ticket, double* out) {
+__device__ __forceinline__ void lj_verlet_body(
+    const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
+    const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
+    const Box3& box, const LJArgs& a, double* __restrict__ fxo, double* __restrict__ fyo,
+    double* __restrict__ fzo, double* part, unsigned* ticket, double* out, unsigned block,
+    unsigned nblocks) {
     using P = PosOf<MIXED>;
-    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t t = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t i = t / TPA;
     const int g = static_cast<int>(t % TPA);
     const Fold3 f3 = fold3_of(box);
@@ -337,7 +340,62 @@ k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __r
         fzo[i] = fz;
     }
     double v[2] = {e, vir};
-    grid_reduce<2>(v, part, ticket, out);
+    grid_reduce_at<2>(v, part, ticket, out, nullptr, block, nblocks);
+}
+
+template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
+__global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
+k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
+            const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
+            Box3 box, LJArgs a, double* __restrict__ fxo, double* __restrict__ fyo,
+            double* __restrict__ fzo, double* part, unsigned* ticket, double* out) {
+    lj_verlet_body<TPA, MIXED, LFS, U, CUBIC>(pos, pd, nbr, count, stride, n, box, a, fxo, fyo, fzo,
+                                              part, ticket, out, blockIdx.x, gridDim.x);
+}
+
+// One system's arguments of the batched force pass.
+struct BatchForceRep {
+    const void* pos;  // int4 fixed-point (mixed) or double4 positions
+    const double4* pd;
+    const int* nbr;
+    const int* count;
+    int stride;
+    int64_t n;
+    Box3 box;
+    LJArgs a;
+    double *fx, *fy, *fz;
+    double* part;
+    unsigned* ticket;
+    double* out;
+};
+
+// The system whose blocks [off[r], off[r + 1]) hold block b.
+__device__ __forceinline__ int system_of_block(const int* __restrict__ off, int nrep, int b) {
+    int lo = 0, hi = nrep;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The force pass of many systems in one launch: each block finds its system in
+// the block-offset table and runs exactly the blocks a launch of that system
+// alone would, so every system's forces and sums equal its solo pass.
+template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
+__global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
+k_lj_verlet_batch(const BatchForceRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
+    // the system's arguments are read from shared memory as the solo kernel reads
+    // its parameters, rather than held in registers
+    __shared__ BatchForceRep d;
+    const int r = system_of_block(off, nrep, static_cast<int>(blockIdx.x));
+    if (threadIdx.x == 0) d = reps[r];
+    __syncthreads();
+    const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
+    lj_verlet_body<TPA, MIXED, LFS, U, CUBIC>(
+        static_cast<const typename PosOf<MIXED>::T*>(d.pos), d.pd, d.nbr, d.count, d.stride, d.n,
+        d.box, d.a, d.fx, d.fy, d.fz, d.part, d.ticket, d.out, blockIdx.x - b0, b1 - b0);
 }
 
 // One thread's share of a row (entries g, g + TPA, ...): U position loads in
@@ -706,8 +764,11 @@ void launch_verlet_tpa(int tpa, int unroll, md_system* sys, md_verlet* v, const 
 int g_lj_tpa = 2;     // threads per atom of the Verlet force kernel (tunable)
 int g_lj_unroll = 2;  // independent gather chains per thread (tunable)
 
-int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q_gate) {
-    md_context* ctx = sys->ctx;
+namespace {
+
+// The pair-kernel arguments of one system: the potential plus the fixed-point
+// resolution and the exact band of the mixed path (box-dependent).
+LJArgs verlet_lj_args(const md_lj* lj, const md_system* sys) {
     LJArgs a = make_lj_args(lj);
     double res_max = 0.0;
     for (int d = 0; d < 3; ++d) {
@@ -719,6 +780,27 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     a.res2 = a.res[0] * a.res[0];
     a.rc2_lo = a.rc2 - a.band;
     a.rc2_hi = a.rc2 + a.band;
+    return a;
+}
+
+}  // namespace
+
+int lj_quantize_async(md_lj* lj, md_system* sys, const int* gate) {
+    if (lj->precision != MD_PRECISION_MIXED || sys->n == 0) return MD_OK;
+    md_context* ctx = sys->ctx;
+    MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(sys->n)));
+    const double two32 = 4294967296.0;
+    k_quantize<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(
+        sys->cur.pos, sys->n, two32 / sys->box[0], two32 / sys->box[1], two32 / sys->box[2],
+        sys->qpos.as<int4>(), gate);
+    ++ctx->launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q_gate) {
+    md_context* ctx = sys->ctx;
+    const LJArgs a = verlet_lj_args(lj, sys);
     const int tpa = lj->tpa ? lj->tpa : g_lj_tpa, unroll = lj->unroll ? lj->unroll : g_lj_unroll;
     const int64_t threads = std::max<int64_t>(sys->n * tpa, 1);
     const int64_t blocks = std::max<int64_t>(grid_for(threads, kBlock), halo_blocks(sys->n));
@@ -728,14 +810,7 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     double* out = ctx_result(ctx, kResEnergy);
     const bool lfs = lj->truncation == MD_LINEAR_FORCE_SHIFT;
     const bool mixed = lj->precision == MD_PRECISION_MIXED;
-    if (mixed && sys->n > 0) {
-        MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(sys->n)));
-        const double two32 = 4294967296.0;
-        k_quantize<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(
-            sys->cur.pos, sys->n, two32 / sys->box[0], two32 / sys->box[1], two32 / sys->box[2],
-            sys->qpos.as<int4>(), q_gate);
-        ++ctx->launches;
-    }
+    MDB_TRY(lj_quantize_async(lj, sys, q_gate));
     // halo tiles, when the list keeps them (fused runs of large systems turn them on,
     // or md_verlet_set_halo)
     const bool halo = mixed && lj->halo && sys->n > 0 && v->halo_on && v->stride % 8 == 0;
@@ -754,6 +829,123 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;
+}
+
+struct BatchForce {
+    DevBuf reps, off;
+    int nrep = 0, total = 0, tpa = 2;
+    bool mixed = false, lfs = false, cubic = false;
+};
+
+int batch_force_create(const BatchRepView* v, int nrep, BatchForce** out) {
+    if (nrep < 1) return fail(MD_ERR_INVALID_ARGUMENT, "batch_force_create: no replicas");
+    const md_lj* l0 = v[0].lj;
+    const int tpa0 = l0->tpa ? l0->tpa : g_lj_tpa, unroll0 = l0->unroll ? l0->unroll : g_lj_unroll;
+    std::vector<BatchForceRep> h(static_cast<size_t>(nrep));
+    std::vector<int> off(static_cast<size_t>(nrep) + 1, 0);
+    bool cubic = true, any_cubic = false;
+    for (int r = 0; r < nrep; ++r) {
+        md_lj* lj = v[r].lj;
+        md_system* sys = v[r].sys;
+        md_verlet* list = v[r].list;
+        const int tpa = lj->tpa ? lj->tpa : g_lj_tpa, unroll = lj->unroll ? lj->unroll : g_lj_unroll;
+        const bool mixed = lj->precision == MD_PRECISION_MIXED;
+        if (lj->precision != l0->precision || lj->truncation != l0->truncation || tpa != tpa0 ||
+            unroll != unroll0 || unroll != 2 || (tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8) ||
+            (mixed && lj->halo && list->halo_on))
+            return fail(MD_ERR_INVALID_ARGUMENT, "batch_force_create: force kernels differ");
+        md_context* ctx = sys->ctx;
+        const LJArgs a = verlet_lj_args(lj, sys);
+        const bool c = a.res[0] == a.res[1] && a.res[0] == a.res[2];
+        cubic = cubic && c;
+        any_cubic = any_cubic || c;
+        const int64_t blocks = grid_for(std::max<int64_t>(sys->n * tpa, 1), kBlock);
+        double* part;
+        MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+        if (mixed) MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(sys->n)));
+        BatchForceRep& d = h[static_cast<size_t>(r)];
+        d.pos = mixed ? static_cast<const void*>(sys->qpos.as<int4>())
+                      : static_cast<const void*>(sys->cur.pos);
+        d.pd = sys->cur.pos;
+        d.nbr = list->nbr.as<int>();
+        d.count = list->count.as<int>();
+        d.stride = list->stride;
+        d.n = sys->n;
+        d.box = box_of(sys);
+        d.a = a;
+        d.fx = sys->cur.fx;
+        d.fy = sys->cur.fy;
+        d.fz = sys->cur.fz;
+        d.part = part;
+        d.ticket = ctx_counter(ctx, 2);
+        d.out = ctx_result(ctx, kResEnergy);
+        off[static_cast<size_t>(r) + 1] = off[static_cast<size_t>(r)] + static_cast<int>(blocks);
+    }
+    // the mixed kernel specialises on a cubic box: one specialisation for all
+    if (l0->precision == MD_PRECISION_MIXED && any_cubic && !cubic)
+        return fail(MD_ERR_INVALID_ARGUMENT, "batch_force_create: cubic and non-cubic boxes mixed");
+    BatchForce* b = new (std::nothrow) BatchForce();
+    if (!b) return fail(MD_ERR_OUT_OF_MEMORY, "batch_force_create: host allocation");
+    b->nrep = nrep;
+    b->total = off.back();
+    b->tpa = tpa0;
+    b->mixed = l0->precision == MD_PRECISION_MIXED;
+    b->lfs = l0->truncation == MD_LINEAR_FORCE_SHIFT;
+    b->cubic = b->mixed && cubic;
+    int rc = b->reps.ensure(sizeof(BatchForceRep) * h.size());
+    if (rc == MD_OK) rc = b->off.ensure(sizeof(int) * off.size());
+    if (rc == MD_OK &&
+        (cudaMemcpy(b->reps.ptr, h.data(), sizeof(BatchForceRep) * h.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess ||
+         cudaMemcpy(b->off.ptr, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess))
+        rc = fail(MD_ERR_CUDA, "batch_force_create: descriptor upload");
+    if (rc != MD_OK) {
+        batch_force_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return MD_OK;
+}
+
+namespace {
+
+template <int TPA, bool MIXED, bool LFS, bool CUBIC>
+void batch_force_t(BatchForce* b, cudaStream_t s) {
+    k_lj_verlet_batch<TPA, MIXED, LFS, 2, CUBIC><<<b->total, kBlock, 0, s>>>(
+        b->reps.as<BatchForceRep>(), b->off.as<int>(), b->nrep);
+}
+
+template <int TPA>
+void batch_force_tpa(BatchForce* b, cudaStream_t s) {
+    if (b->mixed) {
+        if (b->lfs) b->cubic ? batch_force_t<TPA, true, true, true>(b, s) : batch_force_t<TPA, true, true, false>(b, s);
+        else b->cubic ? batch_force_t<TPA, true, false, true>(b, s) : batch_force_t<TPA, true, false, false>(b, s);
+    } else {
+        if (b->lfs) batch_force_t<TPA, false, true, false>(b, s);
+        else batch_force_t<TPA, false, false, false>(b, s);
+    }
+}
+
+}  // namespace
+
+int batch_force_launch(BatchForce* b, cudaStream_t s, int64_t* launches) {
+    switch (b->tpa) {
+        case 1: batch_force_tpa<1>(b, s); break;
+        case 4: batch_force_tpa<4>(b, s); break;
+        case 8: batch_force_tpa<8>(b, s); break;
+        default: batch_force_tpa<2>(b, s); break;
+    }
+    if (launches) ++*launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+void batch_force_destroy(BatchForce* b) {
+    if (!b) return;
+    b->reps.release();
+    b->off.release();
+    delete b;
 }
 
 int lj_forces_brute_async(md_lj* lj, md_system* sys, bool forces) {

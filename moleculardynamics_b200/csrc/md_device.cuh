@@ -118,9 +118,11 @@ __device__ __forceinline__ int4 quantize_position(const double4& p, double sx, d
                      static_cast<int>(p.w));
 }
 
+// grid_reduce over an explicit block index and block count: a batched launch
+// that runs many systems gives each system's blocks their own rank and count.
 template <int K>
-__device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out,
-                            uint32_t* status = nullptr) {
+__device__ void grid_reduce_at(double (&v)[K], double* part, unsigned* ticket, double* out,
+                               uint32_t* status, unsigned block, unsigned nblocks) {
     __shared__ double sm[K][32];
     __shared__ bool is_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -135,13 +137,13 @@ __device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, doub
         for (int k = 0; k < K; ++k) {
             double s = lane < nw ? sm[k][lane] : 0.0;
             s = warp_sum(s);
-            if (lane == 0) part[static_cast<size_t>(blockIdx.x) * K + k] = s;
+            if (lane == 0) part[static_cast<size_t>(block) * K + k] = s;
         }
     }
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned t = atomicAdd(ticket, 1u);
-        is_last = (t == gridDim.x - 1);
+        is_last = (t == nblocks - 1);
     }
     __syncthreads();
     if (!is_last) return;
@@ -149,7 +151,7 @@ __device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, doub
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    for (unsigned b = threadIdx.x; b < nblocks; b += blockDim.x) {
 #pragma unroll
         for (int k = 0; k < K; ++k) acc[k] += __ldcg(part + static_cast<size_t>(b) * K + k);
     }
@@ -172,6 +174,12 @@ __device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, doub
         }
     }
     if (threadIdx.x == 0) *ticket = 0u;
+}
+
+template <int K>
+__device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out,
+                            uint32_t* status = nullptr) {
+    grid_reduce_at<K>(v, part, ticket, out, status, blockIdx.x, gridDim.x);
 }
 
 // Top-2 of a multiset (verlet_list.cpp:44-63): (a1 >= a2), merge with (b1 >= b2).
@@ -206,9 +214,13 @@ struct DispArgs {
     unsigned* ticket;
     int* flag;
     double* top2;
+    // inside a step graph: the rebuild branch's conditional, set with the flag
+    cudaGraphConditionalHandle cond = 0;
+    int set_cond = 0;
 };
 
-__device__ inline void top2_grid(double a1, double a2, const DispArgs& d) {
+__device__ inline void top2_grid_at(double a1, double a2, const DispArgs& d, unsigned block,
+                                    unsigned nblocks) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const double b1 = __shfl_xor_sync(0xffffffffu, a1, o);
@@ -226,17 +238,17 @@ __device__ inline void top2_grid(double a1, double a2, const DispArgs& d) {
     if (threadIdx.x == 0) {
         double b1 = s1[0], b2 = s2[0];
         for (int w = 1; w < nw; ++w) top2_merge(b1, b2, s1[w], s2[w]);
-        d.part[2 * blockIdx.x] = b1;
-        d.part[2 * blockIdx.x + 1] = b2;
+        d.part[2 * block] = b1;
+        d.part[2 * block + 1] = b2;
         __threadfence();
-        last = atomicAdd(d.ticket, 1u) == gridDim.x - 1;
+        last = atomicAdd(d.ticket, 1u) == nblocks - 1;
     }
     __syncthreads();
     if (!last) return;
     // the last block merges all partials with every thread, then a tree
     __threadfence();
     double c1 = 0.0, c2 = 0.0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (unsigned b = threadIdx.x; b < nblocks; b += blockDim.x)
         top2_merge(c1, c2, __ldcg(d.part + 2 * b), __ldcg(d.part + 2 * b + 1));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -255,9 +267,15 @@ __device__ inline void top2_grid(double a1, double a2, const DispArgs& d) {
         const double r1 = __dsqrt_rn(c1), r2 = __dsqrt_rn(c2);
         d.top2[0] = r1;
         d.top2[1] = r2;
-        *d.flag = (d.criterion == 0 ? (r1 + r2) > d.skin : r1 > 0.5 * d.skin) ? 1 : 0;
+        const int rebuild = (d.criterion == 0 ? (r1 + r2) > d.skin : r1 > 0.5 * d.skin) ? 1 : 0;
+        *d.flag = rebuild;
+        if (d.set_cond) cudaGraphSetConditional(d.cond, rebuild ? 1u : 0u);
         *d.ticket = 0u;
     }
+}
+
+__device__ inline void top2_grid(double a1, double a2, const DispArgs& d) {
+    top2_grid_at(a1, a2, d, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- Philox

@@ -178,6 +178,32 @@ int rdf_sync(const md_rdf* r);
 int rdf_frame_launch(md_rdf* r, md_system* sys, int64_t first, int64_t stride);
 void rdf_frame_note(md_rdf* r, const md_system* sys, int64_t first, int64_t stride);
 
+// Replicas stepped by batched kernels: one launch per stage of the step covers
+// every replica, each block finding its replica in a block-offset table.  The
+// per-replica work inside is exactly that replica's solo step.
+struct BatchRepView {
+    md_integrator* it;
+    md_system* sys;
+    md_verlet* list;
+    md_lj* lj;
+    double* rows;                     // thermo rows at a device-held index, or null
+    int* idx;
+    cudaGraphConditionalHandle cond;  // the replica's rebuild branch in the step graph
+};
+struct BatchKick;   // integrate.cu: chain halves, kick/drift (+ rebuild test), kick + KE
+struct BatchForce;  // lj.cu: the Verlet-list force pass
+int batch_kick_create(const BatchRepView* reps, int nrep, BatchKick** out);
+int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches);
+int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches);
+void batch_kick_destroy(BatchKick* b);
+// MD_ERR_INVALID_ARGUMENT when the replicas' force kernels cannot share a launch
+// (different precision, truncation, threads per atom or unrolling, halo tiles).
+int batch_force_create(const BatchRepView* reps, int nrep, BatchForce** out);
+int batch_force_launch(BatchForce* b, cudaStream_t stream, int64_t* launches);
+void batch_force_destroy(BatchForce* b);
+// Mixed precision: the fixed-point positions (after a rebuild re-sorted the atoms).
+int lj_quantize_async(md_lj* lj, md_system* sys, const int* gate);
+
 // Smooth particle-mesh Ewald reciprocal term (pme.cu): grid and cuFFT plans of
 // one Ewald handle.  pme_eval_async writes the reciprocal energy and virial trace
 // to out[0..1] (device) and, for mode != 0, adds the k-space forces.

@@ -61,3 +61,40 @@ def test_batch_rejects_shared_context_and_langevin(md):
     ctx3, s3, v3, lj3, _ = replica(md, 4, 0.8, 1.0, 5, "vv", 0)
     with pytest.raises(md.InvalidArgument, match="Nose-Hoover"):
         batch.add(md.LangevinBAOAB(0.005, 1.0, 1.0, 7), s3, v3, lj3)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_batched_stage_kernels_equal_solo_runs(md, prec):
+    """Replicas that share one force kernel (same precision, cubic boxes) step
+    through the batched stage kernels -- one launch per stage for all replicas,
+    blocks mapped to replicas through a block-offset table, one conditional
+    rebuild branch per replica.  Each replica still follows its solo
+    trajectory bit for bit, as with the per-replica graph, with a fraction of
+    the launches."""
+    reps = [(4, 0.9, 1.3, 21, "nhc", prec), (5, 0.1, 1.8, 22, "nhc", prec),
+            (6, 0.8, 1.0, 23, "vv", prec), (7, 0.5, 1.5, 24, "nhc", prec),
+            (3, 0.8, 1.0, 25, "vv", prec)]  # the last: 2 cells per side, brute-force builds
+    steps = 80
+    alone = []
+    for r in reps:
+        ctx, s, v, lj, integ = replica(md, *r)
+        th = integ.run(s, v, lj, steps, thermo=True)
+        alone.append((s.positions, s.velocities, th, v.rebuild_count()))
+    launches = {}
+    for batched in (True, False):
+        batch = md.Batch()
+        parts = [replica(md, *r) for r in reps]
+        for ctx, s, v, lj, integ in parts:
+            batch.add(integ, s, v, lj)
+        batch.set_batched(batched)
+        before = sum(p[0].launch_count() for p in parts)
+        th = batch.run(steps, thermo=True)
+        launches[batched] = sum(p[0].launch_count() for p in parts) - before
+        for k, (ctx, s, v, lj, integ) in enumerate(parts):
+            pos, vel, th_alone, rebuilds = alone[k]
+            assert np.array_equal(s.positions, pos), (batched, k)
+            assert np.array_equal(s.velocities, vel), (batched, k)
+            assert np.array_equal(th[k], th_alone), (batched, k)
+            assert v.rebuild_count() == rebuilds, (batched, k)
+    assert sum(a[3] for a in alone) > len(reps)
+    assert launches[True] * 3 < launches[False]
