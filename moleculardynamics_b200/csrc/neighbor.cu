@@ -102,9 +102,12 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
     return excl;
 }
 
+// single: the grid is one block, whose scan is already the whole exclusive scan;
+// it then also writes the end sentinel start[m] (k_scan_top and k_scan_add would
+// write it and add nothing), saving their launches.
 __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int* __restrict__ counts,
                                                             int* start, int m, int* bsum,
-                                                            const int* flag) {
+                                                            const int* flag, int single) {
     if (!gate(flag)) return;
     const int base = blockIdx.x * kScanBlock * kScanItems;
     int v[kScanItems];
@@ -126,7 +129,10 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int* __restric
         sum += v[u];
     }
     (void)sum;
-    if (threadIdx.x == 0) bsum[blockIdx.x] = run_base;
+    if (threadIdx.x == 0) {
+        bsum[blockIdx.x] = run_base;
+        if (single) start[m] = run_base;
+    }
 }
 
 __global__ void __launch_bounds__(kScanBlock) k_scan_top(int* bsum, int nb, int* start, int m,
@@ -764,10 +770,12 @@ int cell_sort_gated(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_
                                                                counts, flag);
     const int nb = (m + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
     int* bsum = fill + m;  // scratch tail (sort_scratch reserves it)
-    k_scan_blocks<<<nb, kScanBlock, 0, ctx->stream>>>(counts, d_start, m, bsum, flag);
-    k_scan_top<<<1, kScanBlock, 0, ctx->stream>>>(bsum, nb, d_start, m, flag);
-    k_scan_add<<<nb, kScanBlock, 0, ctx->stream>>>(d_start, m, bsum, flag);
-    ctx->launches += 2;
+    k_scan_blocks<<<nb, kScanBlock, 0, ctx->stream>>>(counts, d_start, m, bsum, flag, nb == 1 ? 1 : 0);
+    if (nb > 1) {
+        k_scan_top<<<1, kScanBlock, 0, ctx->stream>>>(bsum, nb, d_start, m, flag);
+        k_scan_add<<<nb, kScanBlock, 0, ctx->stream>>>(d_start, m, bsum, flag);
+        ctx->launches += 2;
+    }
     if (n > 0)
         k_scatter<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(atom_rank, n, d_start, fill,
                                                                    d_sorted, flag);
