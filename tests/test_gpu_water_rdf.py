@@ -229,3 +229,33 @@ def test_python_cli_writes_the_csv(md, tmp_path, capsys):
     text = out.read_text().splitlines()
     assert text[3] == "# model: SPC/E, rigid (SETTLE), Ewald alpha=5.6/L kmax=5 rcut=10 A"
     assert text[12] == "# rdf_frames: 10" and text[22] == "r_angstrom,g_oo" and len(text) == 223
+
+
+def test_graph_replay_equals_host_launches(md):
+    """md_water_rdf_run and md_run_spce replay captured blocks as CUDA graphs by
+    default; with graphs off every kernel launches from the host.  Both give the
+    same positions, velocities, histogram, mean temperature and thermo rows."""
+    import ctypes as C
+    out = {}
+    for graphs in (True, False):
+        ctx = md.Context(0)
+        ctx.set_graphs(graphs)
+        from moleculardynamics_b200 import water_rdf as W
+        pos, types, box, molecules = W.state_point(*config3())
+        s = md.build_spce_system(pos, types, box, ctx=ctx)
+        rigid = md.RigidWater(1.0, 109.47)
+        s.velocities = W.thermal_velocities(s.masses, 298.0, 7001)
+        s.remove_center_of_mass_motion()
+        rigid.constrain_velocities(s)
+        dof = md.RigidWater.degrees_of_freedom(molecules, True)
+        integ = md.ConstrainedVelocityVerlet(md.units.femtoseconds(2.0), rigid)
+        ff = md.SpceForceField(ctx=ctx)
+        rdf = md.Rdf(10.0, 200, ctx=ctx)
+        mean_t = C.c_double()
+        md._check(md.lib().md_water_rdf_run(integ.handle, s.handle, ff.handle, rdf.handle, 298.0,
+                                            dof, 120, 50, 45, 10, C.byref(mean_t)))
+        th = integ.run(s, ff, 12, thermo=True)
+        out[graphs] = (s.positions, s.velocities, rdf.histogram(), mean_t.value, th)
+    a, b = out[True], out[False]
+    for x, y in zip(a, b):
+        assert np.array_equal(np.asarray(x), np.asarray(y))
