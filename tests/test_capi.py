@@ -95,3 +95,19 @@ def test_cxx_api_header_compiles_and_links(tmp_path):
                     f"-L{libdir}", "-lmoldyn_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
                    check=True)
     assert exe.exists()
+
+
+def test_cxx_header_compiles_cleanly():
+    """The reference-shaped C++ API (include/moldyn_b200.hpp) and the programs
+    written against it -- the moldyn_run-style shims and the water_rdf app --
+    compile with -Wall -Wextra -Werror (syntax and types only; no GPU)."""
+    import os
+    import subprocess
+    from conftest import ROOT
+    srcs = [os.path.join(ROOT, "tests", "cpp", f) for f in ("shim_run.cpp", "shim_analyze.cpp")]
+    srcs.append(os.path.join(ROOT, "moleculardynamics_b200", "apps", "water_rdf.cpp"))
+    for src in srcs:
+        res = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                              "-I", os.path.join(ROOT, "include"), src],
+                             capture_output=True, text=True)
+        assert res.returncode == 0, (src, res.stderr[-2000:])
