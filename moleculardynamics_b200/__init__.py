@@ -641,7 +641,7 @@ class EwaldTerms(dict):
 def fft_size(at_least):
     """The smallest n >= at_least whose prime factors are 2, 3, 5 and 7 (sizes
     the 3-D FFTs of PME handle fastest)."""
-    n = max(1, int(at_least))
+    n = max(1, math.ceil(at_least))
     while True:
         m = n
         for p in (2, 3, 5, 7):

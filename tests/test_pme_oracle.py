@@ -46,3 +46,30 @@ def test_bspline_partition_of_unity_and_derivatives():
         cm, _ = O._bspline_weights(np.clip(w - h, 0, 1), p)
         inner = (w > 2 * h) & (w < 1 - 2 * h)
         assert np.allclose(((cp - cm) / (2 * h))[inner], d[inner], atol=1e-7)
+
+
+def test_pme_converges_in_a_non_cubic_box():
+    """Configuration 1 stretched by (1, 1.25, 1.1): unequal grids per axis at
+    about the same spacing converge to the Ewald sum as in a cubic box."""
+    scale = np.array([1.0, 1.25, 1.1])
+    pos, box = SPCE["pos1"] * scale, SPCE["box1"] * scale
+    q = np.where(SPCE["isO1"], -0.8476, 0.4238)
+    mol = np.arange(len(q)) // 3
+    alpha = 0.3
+    f1, t1, w1 = O.ewald(pos, box, q, mol, kmax=14, alpha=alpha)
+    f0, t0, w0 = O.ewald(pos, box, q, mol, kmax=0, alpha=alpha)
+    e_ref, f_ref = t1["reciprocal"], f1 - f0
+    errs = []
+    for h, p in ((1.25, 4), (0.8, 6), (0.5, 8)):
+        K = [int(np.ceil(L / h)) for L in box]
+        e, w, f = O.pme_recip(pos, box, q, alpha, K, p)
+        errs.append((abs(e - e_ref) / abs(e_ref), np.sqrt(np.mean((f - f_ref) ** 2) / np.mean(f_ref ** 2))))
+    errs = np.array(errs)
+    assert np.all(np.diff(errs, axis=0) < 0)
+    assert errs[-1, 0] < 1e-8 and errs[-1, 1] < 1e-7
+
+
+def test_fft_friendly_grid_sizes():
+    import moleculardynamics_b200 as md
+    assert [md.fft_size(k) for k in (1, 7, 11, 13, 47, 49.72, 63, 97, 121)] == \
+        [1, 7, 12, 14, 48, 50, 63, 98, 125]
