@@ -1,5 +1,5 @@
-"""Failure detection without a GPU fault (SURVEY's failure-detection row): device
-errors are status bits read at the next synchronising call, never traps.  A tiny
+"""Failure detection without a GPU fault: device errors are status bits read at
+the next synchronising call, never traps.  A tiny
 neighbour-row capacity overflows and is grown (or reported when fixed); SHAKE
 non-convergence is tested with the water tests; a NaN in the state is reported;
 positions far outside the box fold back (exactly as the reference folds them)."""
