@@ -1,12 +1,15 @@
 """Benchmark: atom-steps/s of the 1,048,576-atom Lennard-Jones NVE step on one B200,
-mixed precision vs FP64 (BASELINE metric), with the reference CPU path beside it.
+mixed precision vs FP64, with the reference CPU path beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Workload (per GPU): fcc 64^3 lattice (N = 1,048,576), rho* = 0.8442, T* = 0.722,
 rc = 2.5 sigma (truncated), skin 0.3 sigma, dt* = 0.005; seeded Maxwell-Boltzmann
-velocities, equilibrated by BAOAB Langevin (gamma* = 1) before timing, then NVE
-velocity-Verlet steps with device-decided Verlet rebuilds.  One "step" = one
+velocities, equilibrated by 2000 BAOAB Langevin steps (gamma* = 1) of the reference's
+own code (oracle/make_lj1m_state.py writes that state once; both arms load it), then
+NVE velocity-Verlet steps with device-decided Verlet rebuilds.  Outside the timed
+region the GPU arm also runs the full 10,000-step NVE window in both precisions and
+reports its energy drift per atom.  One "step" = one
 velocity-Verlet step over the whole system (kick+drift, displacement check and
 any rebuild, LJ forces, kick).  The per-step working set (positions, velocities,
 forces, neighbour rows ~ 0.4 GB) exceeds the 126 MB L2, so no L2 flush is used.
@@ -39,12 +42,40 @@ RHO, TEMP, RC, SKIN, DT = 0.8442, 0.722, 2.5, 0.3, 0.005
 SEED = 2026
 
 
-def config(equil):
+STATE_FILE = os.path.join(ROOT, "oracle", "_ref", "lj1m_baoab2000.npz")
+
+
+def reference_state():
+    """(box, pos, vel, steps) of the liquid the reference itself equilibrated
+    (2000 LangevinBAOAB steps from the seeded lattice, written once by
+    oracle/make_lj1m_state.py), or None when that build artefact is absent."""
+    try:
+        with np.load(STATE_FILE) as z:
+            if int(z["cells"]) != CELLS:
+                return None
+            return (np.array(z["box"]), np.array(z["pos"]), np.array(z["vel"]),
+                    int(z["steps"]))
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def equilibration_note(ref_steps, gpu_steps):
+    if ref_steps is not None:
+        return (f"{ref_steps} LangevinBAOAB steps (gamma*=1, T*=0.722, seed {SEED + 1}) of the "
+                f"reference's own code from the seeded lattice, COM momentum removed "
+                f"(state file oracle/_ref/lj1m_baoab2000.npz)")
+    if gpu_steps is None:
+        return "none: the seeded lattice (the reference-equilibrated state file is absent)"
+    return (f"{gpu_steps} BAOAB steps (gamma*=1) on the GPU from the seeded lattice "
+            f"(the reference-equilibrated state file is absent)")
+
+
+def config(equilibration):
     return {
         "workload": "1M-atom LJ NVE velocity-Verlet: fcc 64^3 (N=1048576), rho*=0.8442, "
                     "T*=0.722, rc=2.5 truncated, skin=0.3, dt*=0.005",
         "n_atoms": 4 * CELLS ** 3,
-        "equilibration": f"{equil} BAOAB steps (gamma*=1) from the seeded lattice",
+        "equilibration": equilibration,
         "neighbour": "Verlet list rebuilt on device when the two largest displacements "
                      "exceed the skin (reference criterion)",
         "l2_policy": "no flush: per-step working set ~0.4 GB > 126 MB L2",
@@ -183,6 +214,44 @@ def equilibrated_state(md, ctx, equil):
     s.remove_center_of_mass_motion()
     lj.compute_forces(s, v)
     return st["box"], s.positions, s.velocities, s.forces
+
+
+def forces_of(md, ctx, box, pos, vel):
+    """FP64 forces of a given state (the first half-kick of the NVE window needs them)."""
+    s = md.System.from_arrays(pos, box, vel=vel, ctx=ctx)
+    v = md.VerletList(box, RC, SKIN, ctx=ctx)
+    v.build(s)
+    md.LennardJones(1.0, 1.0, RC).compute_forces(s, v)
+    return s.forces
+
+
+def drift_run(md, ctx, box, pos, vel, frc, precision, steps):
+    """The full NVE window (outside the timed region): `steps` fused VV steps from
+    the state with thermo rows.  Returns the energy-conservation summary and the
+    window's device-timed atom-steps/s (list rebuilds included)."""
+    n = pos.shape[0]
+    s = md.System.from_arrays(pos, box, vel=vel, ctx=ctx)
+    s.forces = frc
+    lj = md.LennardJones(1.0, 1.0, RC, precision=precision)
+    v = md.VerletList(box, RC, SKIN, ctx=ctx)
+    v.build(s)
+    e0, _ = lj.compute_forces(s, v)
+    ke0 = 0.5 * float(np.sum(vel * vel))
+    integ = md.VelocityVerlet(DT)
+    L = md.lib()
+    md._check(L.md_context_span_begin(ctx.handle))
+    rows = integ.run(s, v, lj, steps, thermo=True)
+    ms = C.c_double()
+    md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+    etot = (rows[:, 0] + rows[:, 2]) / n
+    base = (e0 + ke0) / n
+    t = DT * np.arange(1, steps + 1)
+    slope = float(np.polyfit(t, etot - base, 1)[0])
+    return {"max_abs_dev_per_atom": float(np.max(np.abs(etot - base))),
+            "final_dev_per_atom": float(etot[-1] - base),
+            "drift_per_atom_per_time": slope,
+            "rebuilds": int(v.rebuild_count()),
+            "atom_steps_per_s": n * steps / (ms.value * 1e-3)}
 
 
 def timed_run(md, ctx, box, pos, vel, frc, precision, steps, warmup, group, clocks=None):
@@ -348,19 +417,36 @@ def run_reference_arm(args):
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
+    import oracle as O
+    O.ref()  # the compiled reference, loaded here as well as in the workers
     steps = max(1, min(args.steps, args.ref_steps))
     procs = max(1, min(os.cpu_count() or 1, args.ref_procs))
-    pos, vel, box = lattice_state()
-    kind, value, rates = cpu_reference(pos, vel, box, steps, procs)
-    ms = 1e3 * 4 * CELLS ** 3 * procs / value
-    sample = (f"{procs} concurrent single-threaded reference processes, each its own "
-              f"{4 * CELLS ** 3}-atom system from the seeded lattice, {steps} NVE VV steps "
-              f"after its first Verlet build ({cpu_model()})")
+    rs = reference_state()
+    if rs is not None:
+        box, pos, vel, ref_steps = rs
+        where = "the reference-equilibrated liquid"
+    else:
+        pos, vel, box = lattice_state()
+        ref_steps = None
+        where = "the seeded lattice"
+    note = equilibration_note(ref_steps, None)
+    kind, _, rates = cpu_reference(pos, vel, box, steps, procs)
+    n = 4 * CELLS ** 3
+    # the processes run concurrently: the batch takes as long as its slowest one
+    wall = max(n * steps / r for r in rates)
+    ms = 1e3 * wall / steps
+    value = procs * n * steps / wall
+    sample = (f"{procs} concurrent single-threaded reference processes, each its own copy of "
+              f"{where} ({n} atoms), {steps} NVE VV steps after its first Verlet build "
+              f"({cpu_model()})")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fcc lattice)",
-        "config": config(0), "impl": "reference",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "requested_steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities, "
+                "reference-equilibrated liquid" if rs is not None else
+                "synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities",
+        "config": config(note), "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
                          "sample": sample, "per_process": rates},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -377,7 +463,18 @@ def run_gpu_arm(args):
     md.set_threads_per_atom(args.tpa)
     md.set_unroll(args.unroll)
     n = 4 * CELLS ** 3
-    box, pos, vel, frc = equilibrated_state(md, ctx, args.equil)
+    rs = None if args.gpu_equil else reference_state()
+    if rs is not None:
+        box, pos, vel, ref_steps = rs
+        frc = forces_of(md, ctx, box, pos, vel)
+        note = equilibration_note(ref_steps, None)
+        data = ("synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities, "
+                "reference-equilibrated liquid")
+    else:
+        box, pos, vel, frc = equilibrated_state(md, ctx, args.equil)
+        note = equilibration_note(None, args.equil)
+        data = ("synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities, "
+                f"{args.equil} BAOAB equilibration steps on the GPU")
     # identical starting state for both precisions
     clocks = ClockSampler(local)
     if args.precision == "mixed":
@@ -411,6 +508,15 @@ def run_gpu_arm(args):
     e2e_steps = max(3, min(args.steps, args.e2e_steps))
     sec, h2d, d2h = e2e_run(md, ctx, box, pos, vel, frc, e2e_steps, group)
     e2e_value = world * n * e2e_steps / sec
+    # the full NVE window of the configuration, both precisions, outside the timed region
+    drift = None
+    if args.drift_steps > 0:
+        d64 = drift_run(md, ctx, box, pos, vel, frc, md.PRECISION_FP64, args.drift_steps)
+        dmx = drift_run(md, ctx, box, pos, vel, frc, md.PRECISION_MIXED, args.drift_steps)
+        ratio = dmx["max_abs_dev_per_atom"] / max(d64["max_abs_dev_per_atom"], 1e-300)
+        drift = {"steps": args.drift_steps, "fp64": d64, "mixed": dmx,
+                 "mixed_over_fp64_max_dev": ratio, "within_2x_fp64": bool(ratio <= 2.0),
+                 "window_mixed_over_fp64": dmx["atom_steps_per_s"] / d64["atom_steps_per_s"]}
 
     if rank == 0:
         peaks, peak_src = measured_peaks()
@@ -436,9 +542,8 @@ def run_gpu_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": msmx / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 pair terms, f64 displacement/accumulation/integration (mixed)",
-            "data": "synthetic: seeded fcc lattice, Maxwell-Boltzmann velocities, "
-                    f"{args.equil} BAOAB equilibration steps",
-            "config": config(args.equil),
+            "data": data,
+            "config": config(note),
             "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
                      "force_kernel_ms": k64, "rebuilds": reb64},
             "mixed_over_fp64": valuemx / value64,
@@ -447,6 +552,7 @@ def run_gpu_arm(args):
             "virial_rel_err": abs(wmx - w64) / abs(w64),
             "nve_max_energy_dev_per_atom": {"fp64": drift64, "mixed": driftmx,
                                             "steps": args.steps},
+            "nve_drift_per_atom": drift,
             "neighbour_entries_per_atom": nbr,
             "rebuilds_in_timed_region": rebmx,
             "gpu_launches": int(launchmx),
@@ -1183,7 +1289,14 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--equil", type=int, default=2000)
+    ap.add_argument("--equil", type=int, default=2000,
+                    help="BAOAB steps on the GPU when the reference-equilibrated state is "
+                         "absent or --gpu-equil is given")
+    ap.add_argument("--gpu-equil", action="store_true",
+                    help="equilibrate on the GPU instead of loading the reference's state")
+    ap.add_argument("--drift-steps", type=int, default=10000,
+                    help="length of the NVE drift window run in both precisions after the "
+                         "timed region (0: skip)")
     ap.add_argument("--tpa", type=int, default=2)
     ap.add_argument("--unroll", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=20)

@@ -105,6 +105,12 @@ MD_API int md_context_device_name(const md_context* ctx, char* name, int len);
 MD_API int md_context_status(md_context* ctx, uint32_t* status, int clear);
 /* Number of kernels this context has launched (instrumentation). */
 MD_API int md_context_launch_count(md_context* ctx, int64_t* count);
+/* Step graphs captured by fused loops on this context (no reference counterpart).
+ * md_run_lj replays the step graph of an earlier call while the system, list and
+ * force field are the same handles and no device buffer was allocated, freed or
+ * permuted and no handle created, destroyed or reconfigured in between; each new
+ * capture adds one. */
+MD_API int md_context_graph_captures(md_context* ctx, int64_t* count);
 
 /* Instrumentation, no reference counterpart.  With timing enabled, launches of
  * the kernels below are bracketed by CUDA events on the context's stream;

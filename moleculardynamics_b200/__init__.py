@@ -84,6 +84,7 @@ def _load():
         "md_context_synchronize": (C.c_int, [_vp]),
         "md_context_status": (C.c_int, [_vp, C.POINTER(C.c_uint32), C.c_int]),
         "md_context_launch_count": (C.c_int, [_vp, _i64p]),
+        "md_context_graph_captures": (C.c_int, [_vp, _i64p]),
         "md_context_set_timing": (C.c_int, [_vp, C.c_int]),
         "md_context_set_graphs": (C.c_int, [_vp, C.c_int]),
         "md_context_device_name": (C.c_int, [_vp, C.c_char_p, C.c_int]),
@@ -283,6 +284,12 @@ class Context:
     def launch_count(self):
         c = C.c_int64()
         _check(lib().md_context_launch_count(self._h, C.byref(c)))
+        return c.value
+
+    def graph_captures(self):
+        """Step graphs fused loops have captured on this context."""
+        c = C.c_int64()
+        _check(lib().md_context_graph_captures(self._h, C.byref(c)))
         return c.value
 
     def device_name(self) -> str:

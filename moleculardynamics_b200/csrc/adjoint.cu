@@ -272,6 +272,7 @@ int segment_step(md_adjoint* a) {
 extern "C" {
 
 int md_adjoint_create(md_context* ctx, md_adjoint** out) {
+    graph_epoch_bump();
     if (!ctx || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_adjoint_create: NULL");
     md_adjoint* a = new (std::nothrow) md_adjoint();
     if (!a) return fail(MD_ERR_OUT_OF_MEMORY, "md_adjoint_create: host allocation");
@@ -281,6 +282,7 @@ int md_adjoint_create(md_context* ctx, md_adjoint** out) {
 }
 
 int md_adjoint_destroy(md_adjoint* a) {
+    graph_epoch_bump();
     if (!a) return MD_OK;
     if (a->ctx) cudaStreamSynchronize(a->ctx->stream);
     if (a->list) md_verlet_destroy(a->list);

@@ -365,6 +365,7 @@ extern "C" {
 
 // ------------------------------------------------------------------------ RDF
 int md_rdf_create(md_context* ctx, double rmax, int64_t bins, md_rdf** out) {
+    graph_epoch_bump();
     if (!ctx || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_create: NULL argument");
     if (bins < 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_rdf_create: bins must be >= 0");
     md_rdf* r = new (std::nothrow) md_rdf;
@@ -386,6 +387,7 @@ int md_rdf_create(md_context* ctx, double rmax, int64_t bins, md_rdf** out) {
 }
 
 int md_rdf_destroy(md_rdf* r) {
+    graph_epoch_bump();
     if (!r) return MD_OK;
     if (r->ctx) cudaStreamSynchronize(r->ctx->stream);
     r->hist.release();
@@ -541,6 +543,7 @@ int md_rdf_frames(const md_rdf* r, int64_t* frames) {
 
 // ------------------------------------------------------------------------ MSD
 int md_msd_create(md_context* ctx, int64_t natoms, int64_t max_lag, md_msd** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_msd_create: NULL argument");
     md_msd* m = new (std::nothrow) md_msd;
     if (!m) return fail(MD_ERR_RUNTIME, "md_msd_create: out of host memory");
@@ -554,6 +557,7 @@ int md_msd_create(md_context* ctx, int64_t natoms, int64_t max_lag, md_msd** out
 }
 
 int md_msd_destroy(md_msd* m) {
+    graph_epoch_bump();
     if (!m) return MD_OK;
     if (m->ctx) cudaStreamSynchronize(m->ctx->stream);
     m->prev.release();
@@ -602,6 +606,7 @@ int md_msd_diffusion(const md_msd* m, double dt, int64_t fit_from, int64_t fit_t
 
 // ----------------------------------------------------------------------- VACF
 int md_vacf_create(md_context* ctx, int64_t natoms, int64_t max_lag, md_vacf** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_vacf_create: NULL argument");
     md_vacf* v = new (std::nothrow) md_vacf;
     if (!v) return fail(MD_ERR_RUNTIME, "md_vacf_create: out of host memory");
@@ -615,6 +620,7 @@ int md_vacf_create(md_context* ctx, int64_t natoms, int64_t max_lag, md_vacf** o
 }
 
 int md_vacf_destroy(md_vacf* v) {
+    graph_epoch_bump();
     if (!v) return MD_OK;
     if (v->ctx) cudaStreamSynchronize(v->ctx->stream);
     v->ring.release();

@@ -166,6 +166,7 @@ int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
 extern "C" {
 
 int md_batch_create(md_batch** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_batch_create: NULL");
     md_batch* b = new (std::nothrow) md_batch();
     if (!b) return fail(MD_ERR_OUT_OF_MEMORY, "md_batch_create: host allocation");
@@ -174,6 +175,7 @@ int md_batch_create(md_batch** out) {
 }
 
 int md_batch_destroy(md_batch* b) {
+    graph_epoch_bump();
     delete b;
     return MD_OK;
 }
@@ -192,6 +194,7 @@ int md_batch_add(md_batch* b, md_integrator* it, md_system* sys, md_verlet* list
 int md_batch_size(const md_batch* b) { return b ? static_cast<int>(b->reps.size()) : 0; }
 
 int md_batch_set_batched(md_batch* b, int on) {
+    graph_epoch_bump();
     if (!b) return fail(MD_ERR_INVALID_ARGUMENT, "md_batch_set_batched: NULL batch");
     b->batched = on ? 1 : 0;
     return MD_OK;
@@ -205,7 +208,7 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     for (auto& r : b->reps) {
         MDB_TRY(verlet_ensure_ready(r.list, r.sys, "md_batch_run"));
         if (r.sys->n == 0) return fail(MD_ERR_INVALID_ARGUMENT, "md_batch_run: empty replica");
-        verlet_halo_for_run(r.list, r.sys, r.lj, steps);
+        verlet_halo_for_run(r.list, r.sys, r.lj);
     }
     MDB_CUDA(cudaSetDevice(b->device));
     std::vector<Run> run(nr);

@@ -712,6 +712,7 @@ extern "C" {
 
 int md_rigid_create(double oh, double hoh_degrees, double tolerance, int max_iterations,
                     md_rigid** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_create: NULL");
     // rigid_water.cpp:38-49
     if (!(oh > 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "RigidWater: ohDistance must be positive");
@@ -732,12 +733,14 @@ int md_rigid_create(double oh, double hoh_degrees, double tolerance, int max_ite
 }
 
 int md_rigid_set_settle(md_rigid* rw, int on) {
+    graph_epoch_bump();
     if (!rw) return fail(MD_ERR_INVALID_ARGUMENT, "md_rigid_set_settle: NULL");
     rw->settle = on != 0;
     return MD_OK;
 }
 
 int md_rigid_destroy(md_rigid* rw) {
+    graph_epoch_bump();
     delete rw;
     return MD_OK;
 }
@@ -811,6 +814,7 @@ int md_rigid_constrain_velocities(md_rigid* rw, md_system* sys, int* iterations)
 }
 
 int md_integrator_create_rattle(double dt, const md_rigid* rw, md_integrator** out) {
+    graph_epoch_bump();
     if (!rw || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_rattle: NULL");
     md_integrator* it = new (std::nothrow) md_integrator();
     if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_rattle: host allocation");
@@ -823,6 +827,7 @@ int md_integrator_create_rattle(double dt, const md_rigid* rw, md_integrator** o
 
 int md_integrator_create_rattle_nhc(double dt, const md_rigid* rw, double temperature, double tau,
                                     int chain_length, int64_t dof, md_integrator** out) {
+    graph_epoch_bump();
     if (!rw || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_rattle_nhc: NULL");
     MDB_TRY(md_integrator_create_nhc(dt, temperature, tau, chain_length, dof, out));
     (*out)->kind = 4;

@@ -1,4 +1,5 @@
 // context.cu -- error state, device context, scratch management.
+#include <atomic>
 #include <cstdio>
 #include <cstdarg>
 #include <cstring>
@@ -10,7 +11,11 @@ namespace mdb {
 
 namespace {
 thread_local std::string g_last_error;
+std::atomic<uint64_t> g_graph_epoch{1};
 }
+
+uint64_t graph_epoch() { return g_graph_epoch.load(std::memory_order_acquire); }
+void graph_epoch_bump() { g_graph_epoch.fetch_add(1, std::memory_order_acq_rel); }
 
 void set_error(const char* fmt, ...) {
     char buf[1024];
@@ -33,6 +38,7 @@ int fail(int code, const char* fmt, ...) {
 
 int DevBuf::ensure(size_t want) {
     if (want <= bytes && ptr) return MD_OK;
+    graph_epoch_bump();  // a captured graph may hold the old address
     if (ptr) {
         // Work already queued may still read the old buffer.
         cudaDeviceSynchronize();
@@ -53,7 +59,10 @@ int DevBuf::ensure(size_t want) {
 }
 
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        graph_epoch_bump();
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
 }
@@ -168,12 +177,14 @@ int md_context_create(int device, md_context** out) {
     MDB_CUDA(cudaMemset(ctx->result.ptr, 0, sizeof(double) * kMaxResults));
     MDB_CUDA(cudaMallocHost(&ctx->h_result, sizeof(double) * kMaxResults));
     MDB_CUDA(cudaDeviceSynchronize());
+    graph_epoch_bump();
     *out = ctx;
     return MD_OK;
 }
 
 int md_context_destroy(md_context* ctx) {
     if (!ctx) return MD_OK;
+    graph_epoch_bump();
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->partials.release();
@@ -218,12 +229,14 @@ int md_context_set_timing(md_context* ctx, int enable) {
     if (!ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_set_timing: NULL");
     MDB_TRY(ctx_collect(ctx));
     ctx->timing = enable != 0;
+    graph_epoch_bump();
     return MD_OK;
 }
 
 int md_context_set_graphs(md_context* ctx, int enable) {
     if (!ctx) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_set_graphs: NULL");
     ctx->graphs = enable != 0;
+    graph_epoch_bump();
     return MD_OK;
 }
 
@@ -281,6 +294,12 @@ int md_host_free(void* p) {
 int md_context_launch_count(md_context* ctx, int64_t* count) {
     if (!ctx || !count) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_launch_count: NULL");
     *count = ctx->launches;
+    return MD_OK;
+}
+
+int md_context_graph_captures(md_context* ctx, int64_t* count) {
+    if (!ctx || !count) return fail(MD_ERR_INVALID_ARGUMENT, "md_context_graph_captures: NULL");
+    *count = ctx->graph_captures;
     return MD_OK;
 }
 

@@ -966,10 +966,12 @@ extern "C" {
 double md_coulomb_prefactor(void) { return coulomb_prefactor(); }
 
 int md_ewald_create(md_context* ctx, double cutoff, int kmax, double alpha, md_ewald** out) {
+    graph_epoch_bump();
     return ewald_new(ctx, cutoff, kmax, alpha, out);
 }
 
 int md_ewald_destroy(md_ewald* ew) {
+    graph_epoch_bump();
     if (!ew) return MD_OK;
     if (ew->list) md_verlet_destroy(ew->list);
     if (ew->pme) {
@@ -989,6 +991,7 @@ int md_ewald_destroy(md_ewald* ew) {
 }
 
 int md_ewald_set_skin(md_ewald* ew, double skin) {
+    graph_epoch_bump();
     if (!ew || !(skin >= 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_skin: bad argument");
     ew->skin = skin;
     if (ew->list) {
@@ -1025,6 +1028,7 @@ int upload_vec(md_system* sys, const double* u, double4* dev_orig, double4* dev)
 }  // namespace
 
 int md_ewald_set_pme(md_ewald* ew, int kx, int ky, int kz, int order) {
+    graph_epoch_bump();
     if (!ew) return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_pme: NULL");
     if (kx == 0 && ky == 0 && kz == 0) {  // back to the k-vector sums
         if (ew->pme) {
@@ -1052,6 +1056,7 @@ int md_ewald_set_pme(md_ewald* ew, int kx, int ky, int kz, int order) {
 }
 
 int md_ewald_set_precision(md_ewald* ew, int precision) {
+    graph_epoch_bump();
     if (!ew || (precision != MD_PRECISION_FP64 && precision != MD_PRECISION_MIXED))
         return fail(MD_ERR_INVALID_ARGUMENT, "md_ewald_set_precision: MD_PRECISION_FP64 or _MIXED");
     ew->mixed = precision == MD_PRECISION_MIXED;
@@ -1155,6 +1160,7 @@ int md_ewald_kvector_count(const md_ewald* ew, int* count) {
 // ------------------------------------------------------------------- SPC/E
 int md_spce_create(md_context* ctx, double sigma_o, double epsilon_o, double cutoff, int kmax,
                    double alpha, md_ewald** out) {
+    graph_epoch_bump();
     MDB_TRY(ewald_new(ctx, cutoff, kmax, alpha, out));
     (*out)->spce = true;
     (*out)->sigma_o = sigma_o;
@@ -1163,6 +1169,7 @@ int md_spce_create(md_context* ctx, double sigma_o, double epsilon_o, double cut
 }
 
 int md_spce_set_lj_truncation(md_ewald* ew, int truncation) {
+    graph_epoch_bump();
     if (!ew || !ew->spce || (truncation != MD_TRUNCATED && truncation != MD_LINEAR_FORCE_SHIFT))
         return fail(MD_ERR_INVALID_ARGUMENT, "md_spce_set_lj_truncation: bad argument");
     ew->lj_truncation = truncation;

@@ -784,6 +784,7 @@ using namespace mdb;
 extern "C" {
 
 int md_integrator_create_vv(double dt, md_integrator** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_vv: NULL");
     md_integrator* it = new (std::nothrow) md_integrator();
     if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_vv: host allocation");
@@ -795,6 +796,7 @@ int md_integrator_create_vv(double dt, md_integrator** out) {
 
 int md_integrator_create_baoab(double dt, double friction, double temperature, uint64_t seed,
                                md_integrator** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_baoab: NULL");
     md_integrator* it = new (std::nothrow) md_integrator();
     if (!it) return fail(MD_ERR_OUT_OF_MEMORY, "md_integrator_create_baoab: host allocation");
@@ -809,6 +811,7 @@ int md_integrator_create_baoab(double dt, double friction, double temperature, u
 
 int md_integrator_create_nhc(double dt, double temperature, double tau, int chain_length,
                              int64_t dof, md_integrator** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_integrator_create_nhc: NULL");
     if (chain_length < 1)  // nose_hoover.cpp:36-38
         return fail(MD_ERR_INVALID_ARGUMENT, "NoseHooverChain: chainLength must be >= 1");
@@ -844,8 +847,18 @@ int md_integrator_create_nhc(double dt, double temperature, double tau, int chai
 }
 
 int md_integrator_destroy(md_integrator* it) {
+    graph_epoch_bump();
     if (!it) return MD_OK;
     cudaDeviceSynchronize();
+    if (it->run_graph) {
+        StepGraph* sg = static_cast<StepGraph*>(it->run_graph);
+        sg->release();
+        delete sg;
+    }
+    it->run_rows.release();
+    it->run_idx.release();
+    it->conserved.release();
+    if (it->h_rebuilt) cudaFreeHost(it->h_rebuilt);
     it->chain_state.release();
     it->noise.release();
     it->mol_state.release();
@@ -874,11 +887,9 @@ int md_integrator_conserved(md_integrator* it, double* value) {
     }
     // A tiny read on the default stream after all work on every stream finished.
     MDB_CUDA(cudaDeviceSynchronize());
-    double* d;
-    MDB_CUDA(cudaMalloc(&d, sizeof(double)));
-    k_conserved<<<1, 1>>>(it->chain_state.as<NhcState>(), d);
-    MDB_CUDA(cudaMemcpy(value, d, sizeof(double), cudaMemcpyDeviceToHost));
-    cudaFree(d);
+    MDB_TRY(it->conserved.ensure(sizeof(double)));
+    k_conserved<<<1, 1>>>(it->chain_state.as<NhcState>(), it->conserved.as<double>());
+    MDB_CUDA(cudaMemcpy(value, it->conserved.ptr, sizeof(double), cudaMemcpyDeviceToHost));
     return MD_OK;
 }
 
@@ -906,54 +917,78 @@ int md_run_lj(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, int64_
     if (it->kind >= 3)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_run_lj: constrained integrators run with md_run_spce");
     md_context* ctx = sys->ctx;
-    DevBuf rows, idx;
-    if (thermo && steps > 0) {
-        MDB_TRY(rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
-        MDB_TRY(idx.ensure(sizeof(int)));
-        MDB_CUDA(cudaMemsetAsync(idx.ptr, 0, sizeof(int), ctx->stream));
+    verlet_halo_for_run(v, sys, lj);
+    // Thermo rows persist on the integrator (a captured step graph writes them at a
+    // device-held index), grown in powers of two so that calls of similar length
+    // keep the same buffer.
+    if (steps > 0) {
+        size_t cap = 1024;
+        while (cap < static_cast<size_t>(steps)) cap *= 2;
+        MDB_TRY(it->run_rows.ensure(sizeof(double) * 4 * cap));
+        MDB_TRY(it->run_idx.ensure(sizeof(int)));
+        MDB_CUDA(cudaMemsetAsync(it->run_idx.ptr, 0, sizeof(int), ctx->stream));
+        if (!it->h_rebuilt) MDB_CUDA(cudaMallocHost(&it->h_rebuilt, 2 * sizeof(int)));
     }
+    double* rows = it->run_rows.as<double>();
+    int* idx = it->run_idx.as<int>();
     NhcState* nhc = nhc_of(it);
-    // The first step runs from the host: it sums the entry kinetic energy for
-    // the chain and sizes every buffer, so that the captured step graph needs
-    // no allocation.  Later steps replay the graph when that is possible
-    // (BAOAB's noise counter is a host-side launch argument, so it never is).
-    const bool want_graph = ctx->graphs && !ctx->timing && it->kind != 1 && steps >= 4 && sys->n > 0;
-    verlet_halo_for_run(v, sys, lj, steps);
-    StepGraph sg;
-    for (int64_t k = 0; k < steps; ++k) {
-        MDB_TRY(lj_fused_step(it, sys, v, lj, rows.as<double>(), idx.as<int>(), k == 0));
-        if (k == 0 && want_graph) {
-            if (capture_lj_step(it, sys, v, lj, rows.as<double>(), idx.as<int>(), sg) != MD_OK) {
-                cudaGetLastError();  // no graph: the remaining steps run from the host
-                continue;
-            }
-            const int64_t graph_steps = steps - 1;
-            int rebuilt0 = 0;
-            MDB_CUDA(cudaMemcpyAsync(&rebuilt0, v->d_rebuild_total, sizeof(int),
-                                     cudaMemcpyDeviceToHost, ctx->stream));
-            MDB_CUDA(cudaStreamSynchronize(ctx->stream));
-            for (int64_t g = 0; g < graph_steps; ++g) MDB_CUDA(cudaGraphLaunch(sg.exec, ctx->stream));
-            int rebuilt1 = 0;
-            MDB_CUDA(cudaMemcpyAsync(&rebuilt1, v->d_rebuild_total, sizeof(int),
-                                     cudaMemcpyDeviceToHost, ctx->stream));
-            MDB_CUDA(cudaStreamSynchronize(ctx->stream));
-            ctx->launches += graph_steps * sg.main_launches +
-                             static_cast<int64_t>(rebuilt1 - rebuilt0) * sg.body_launches;
-            break;
+    // Steps replay one captured step graph when that is possible (BAOAB's noise
+    // counter is a host-side launch argument, so it never is).  The graph of an
+    // earlier call is replayed while the system, list and force field are the same
+    // handles and nothing has been allocated, freed, permuted or reconfigured since
+    // (the graph epoch).  Otherwise the first step runs from the host -- it sizes
+    // every buffer -- and the step is captured afterwards.  A chain's first step
+    // always runs from the host: it sums the entry kinetic energy instead of using
+    // the tracked value, which the caller may have changed between calls.
+    const bool want_graph = ctx->graphs && !ctx->timing && it->kind != 1 && steps >= 1 && sys->n > 0;
+    StepGraph* sg = static_cast<StepGraph*>(it->run_graph);
+    const void* key[3] = {sys, v, lj};
+    bool cached = want_graph && sg && sg->exec && it->run_epoch == graph_epoch() &&
+                  key[0] == it->run_key[0] && key[1] == it->run_key[1] && key[2] == it->run_key[2];
+    int64_t k = 0;
+    if (steps > 0 && (!cached || nhc)) {
+        MDB_TRY(lj_fused_step(it, sys, v, lj, rows, idx, true));
+        k = 1;
+    }
+    if (want_graph && !cached) {
+        if (!sg) {
+            sg = new (std::nothrow) StepGraph();
+            if (!sg) return fail(MD_ERR_OUT_OF_MEMORY, "md_run_lj: host allocation");
+            it->run_graph = sg;
+        }
+        sg->release();
+        if (capture_lj_step(it, sys, v, lj, rows, idx, *sg) == MD_OK) {
+            ++ctx->graph_captures;
+            // anything the first step and the capture allocated is part of the key
+            it->run_epoch = graph_epoch();
+            for (int q = 0; q < 3; ++q) it->run_key[q] = key[q];
+            cached = true;
+        } else {
+            cudaGetLastError();  // no graph: the remaining steps run from the host
         }
     }
+    if (cached && k < steps) {
+        const int64_t graph_steps = steps - k;
+        MDB_CUDA(cudaMemcpyAsync(it->h_rebuilt, v->d_rebuild_total, sizeof(int),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+        for (int64_t g = 0; g < graph_steps; ++g) MDB_CUDA(cudaGraphLaunch(sg->exec, ctx->stream));
+        MDB_CUDA(cudaMemcpyAsync(it->h_rebuilt + 1, v->d_rebuild_total, sizeof(int),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+        MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->launches += graph_steps * sg->main_launches +
+                         static_cast<int64_t>(it->h_rebuilt[1] - it->h_rebuilt[0]) * sg->body_launches;
+        k = steps;
+    }
+    for (; k < steps; ++k) MDB_TRY(lj_fused_step(it, sys, v, lj, rows, idx, false));
     if (nhc && steps > 0 && sys->n > 0) {
         k_scale<<<grid_for(sys->n, kBlock), kBlock, 0, ctx->stream>>>(sys->cur, sys->n, nhc);
         k_reset_scale<<<1, 1, 0, ctx->stream>>>(nhc);
         ctx->launches += 2;
     }
-    if (rows.ptr)
-        MDB_CUDA(cudaMemcpyAsync(thermo, rows.ptr, sizeof(double) * 4 * static_cast<size_t>(steps),
+    if (thermo && steps > 0)
+        MDB_CUDA(cudaMemcpyAsync(thermo, rows, sizeof(double) * 4 * static_cast<size_t>(steps),
                                  cudaMemcpyDeviceToHost, ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
-    sg.release();
-    rows.release();
-    idx.release();
     MDB_TRY(ctx_check_status(ctx));
     double r[2];
     MDB_TRY(ctx_read_results(ctx, kResEnergy, 2, r));

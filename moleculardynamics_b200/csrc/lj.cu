@@ -1016,6 +1016,7 @@ extern "C" {
 
 int md_lj_create(double sigma, double epsilon, double cutoff, int truncation, int precision,
                  md_lj** out) {
+    graph_epoch_bump();
     if (!out) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_create: out is NULL");
     if (truncation != MD_TRUNCATED && truncation != MD_LINEAR_FORCE_SHIFT)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_create: unknown truncation %d", truncation);
@@ -1041,6 +1042,7 @@ int md_lj_create(double sigma, double epsilon, double cutoff, int truncation, in
 }
 
 int md_lj_destroy(md_lj* lj) {
+    graph_epoch_bump();
     delete lj;
     return MD_OK;
 }
@@ -1102,6 +1104,7 @@ int md_lj_lrc(const md_lj* lj, int64_t n, const double box[3], double* u_lrc, do
 
 // Threads per atom of the Verlet force kernel (1, 2, 4 or 8); autotuning hook.
 int md_lj_set_threads_per_atom(int tpa) {
+    graph_epoch_bump();
     if (tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_threads_per_atom: %d not in {1,2,4,8}", tpa);
     g_lj_tpa = tpa;
@@ -1110,6 +1113,7 @@ int md_lj_set_threads_per_atom(int tpa) {
 
 // Launch shape of one LJ object's Verlet force kernel (0 = the library default).
 int md_lj_set_launch(md_lj* lj, int tpa, int unroll) {
+    graph_epoch_bump();
     if (!lj) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: NULL");
     if (tpa != 0 && tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: tpa %d not in {0,1,2,4,8}", tpa);
@@ -1121,6 +1125,7 @@ int md_lj_set_launch(md_lj* lj, int tpa, int unroll) {
 }
 
 int md_lj_set_halo(md_lj* lj, int on) {
+    graph_epoch_bump();
     if (!lj) return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_halo: NULL");
     lj->halo = on != 0;
     return MD_OK;
@@ -1128,6 +1133,7 @@ int md_lj_set_halo(md_lj* lj, int on) {
 
 // Independent neighbour gathers in flight per thread (1, 2 or 4); autotuning hook.
 int md_lj_set_unroll(int unroll) {
+    graph_epoch_bump();
     if (unroll != 1 && unroll != 2 && unroll != 4)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_unroll: %d not in {1,2,4}", unroll);
     g_lj_unroll = unroll;

@@ -22,6 +22,13 @@ namespace mdb {
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 
+// Process-wide count of the events that can leave a captured step graph pointing
+// at stale memory or parameters: every device buffer allocated, grown or freed,
+// every atom permutation that swaps the system's arrays, every handle created,
+// destroyed or reconfigured.  A cached graph is replayed only while it is unchanged.
+uint64_t graph_epoch();
+void graph_epoch_bump();
+
 #define MDB_CUDA(call)                                                                   \
     do {                                                                                 \
         cudaError_t e_ = (call);                                                         \
@@ -73,6 +80,7 @@ struct md_context {
     mdb::DevBuf result;                  // small device results (energy, virial, ...)
     double* h_result = nullptr;          // pinned host mirror of `result`
     int64_t launches = 0;
+    int64_t graph_captures = 0;          // step graphs captured by fused loops
     int sm_count = 148;
     bool timing = false;
     bool graphs = true;                  // fused loops replay a captured step graph
@@ -264,17 +272,17 @@ constexpr int kHaloAtoms = 128;
 constexpr int kHaloRuns = 64;
 constexpr int kHaloCap = 2560;
 constexpr int kHaloSpan = 16;
-// Fused runs keep halo tiles for systems of at least this many atoms and runs of at
-// least kHaloMinSteps steps: below that, building the tiles at each rebuild costs
-// more than the faster force kernel saves.
+// Fused runs keep halo tiles for systems of at least this many atoms: below that,
+// building the tiles at each rebuild costs more than the faster force kernel saves.
+// The choice depends on the list and the force field only, never on the length of
+// one call, so short and long runs of the same system step with the same kernels.
 constexpr int64_t kHaloMinAtoms = 65536;
-constexpr int64_t kHaloMinSteps = 16;
 inline int64_t halo_blocks(int64_t n) { return (n + kHaloAtoms - 1) / kHaloAtoms; }
 // Turns the halo tiles on for this list (built right away from the current list
 // unless the stream is capturing); false when they cannot be used.
 bool verlet_halo_ready(md_verlet* v, md_system* sys);
 // The fused-run policy above, for a mixed-precision LJ force field.
-void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj, int64_t steps);
+void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 int verlet_check(md_verlet* v, md_system* sys);  // device flag <- needs rebuild
 int verlet_ensure_capacity(md_verlet* v, md_system* sys);
@@ -346,6 +354,15 @@ struct md_integrator {
     int64_t dof = 0;
     mdb::DevBuf chain_state;      // device: NhcState
     md_context* ctx = nullptr;
+    // md_run_lj: thermo rows that persist across calls (so a captured step graph
+    // keeps its record target) and the last captured step graph with the key it
+    // was captured under (system, list, force field, graph epoch).
+    mdb::DevBuf run_rows, run_idx;
+    mdb::DevBuf conserved;         // md_integrator_conserved's device result
+    void* run_graph = nullptr;     // mdb::StepGraph*
+    const void* run_key[3] = {nullptr, nullptr, nullptr};
+    uint64_t run_epoch = 0;
+    int* h_rebuilt = nullptr;      // pinned: device rebuild totals around the replays
 };
 
 namespace mdb {

@@ -955,12 +955,14 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
                             "than the fixed row capacity %d", mx, v->stride);
             }
             v->stride = ((mx + mx / 4 + 16) + 7) & ~7;
+            graph_epoch_bump();  // the stride is a captured launch argument
             MDB_TRY(v->nbr.ensure(sizeof(int) * static_cast<size_t>(sys->n) * v->stride));
             // positions are already sorted; the re-sort below is a no-op permutation
         }
         ++v->rebuilds;
         v->epoch = sys->epoch;
         v->sys = sys;
+        graph_epoch_bump();
         return MD_OK;
     }
     return verlet_build_impl(v, sys, v->d_rebuild_flag);
@@ -979,12 +981,12 @@ bool verlet_halo_ready(md_verlet* v, md_system* sys) {
         return false;
     }
     v->halo_on = true;
+    graph_epoch_bump();
     return true;
 }
 
-void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj, int64_t steps) {
-    if (lj->precision == MD_PRECISION_MIXED && lj->halo && sys->n >= kHaloMinAtoms &&
-        steps >= kHaloMinSteps)
+void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj) {
+    if (lj->precision == MD_PRECISION_MIXED && lj->halo && sys->n >= kHaloMinAtoms)
         verlet_halo_ready(v, sys);
 }
 
@@ -1148,6 +1150,7 @@ extern "C" {
 
 // ------------------------------------------------------------------ CellList
 int md_cells_create(md_context* ctx, const double box[3], double cutoff, md_cells** out) {
+    graph_epoch_bump();
     if (!ctx || !box || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_create: NULL argument");
     if (!(cutoff > 0.0)) return fail(MD_ERR_INVALID_ARGUMENT, "md_cells_create: cutoff must be > 0");
     md_cells* c = new (std::nothrow) md_cells();
@@ -1164,6 +1167,7 @@ int md_cells_create(md_context* ctx, const double box[3], double cutoff, md_cell
 }
 
 int md_cells_destroy(md_cells* c) {
+    graph_epoch_bump();
     if (!c) return MD_OK;
     c->grid.release();
     c->sorted_orig.release();
@@ -1207,6 +1211,7 @@ int md_cells_build(md_cells* c, md_system* sys) {
 // ---------------------------------------------------------------- VerletList
 int md_verlet_create(md_context* ctx, const double box[3], double cutoff, double skin,
                      md_verlet** out) {
+    graph_epoch_bump();
     if (!ctx || !box || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_create: NULL argument");
     if (!(cutoff > 0.0) || !(skin >= 0.0))
         return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_create: cutoff must be > 0 and skin >= 0");
@@ -1238,6 +1243,7 @@ int md_verlet_create(md_context* ctx, const double box[3], double cutoff, double
 }
 
 int md_verlet_destroy(md_verlet* v) {
+    graph_epoch_bump();
     if (!v) return MD_OK;
     if (v->ctx) cudaStreamSynchronize(v->ctx->stream);
     v->grid.release();
@@ -1291,6 +1297,7 @@ int md_verlet_rebuild_count(md_verlet* v, int64_t* count) {
 }
 
 int md_verlet_set_capacity(md_verlet* v, int capacity, int fixed) {
+    graph_epoch_bump();
     if (!v || capacity < 1) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_capacity: bad argument");
     if (v->ctx) MDB_CUDA(cudaStreamSynchronize(v->ctx->stream));
     v->stride = capacity;
@@ -1301,6 +1308,7 @@ int md_verlet_set_capacity(md_verlet* v, int capacity, int fixed) {
 }
 
 int md_verlet_set_halo(md_verlet* v, int on) {
+    graph_epoch_bump();
     if (!v) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_halo: NULL");
     if (!on) {
         v->halo_on = false;
@@ -1327,6 +1335,7 @@ int md_verlet_halo_tiles(md_verlet* v, int64_t* staged, int64_t* tiles) {
 }
 
 int md_verlet_set_criterion(md_verlet* v, int criterion) {
+    graph_epoch_bump();
     if (!v || (criterion != 0 && criterion != 1))
         return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_criterion: criterion must be 0 or 1");
     v->criterion = criterion;

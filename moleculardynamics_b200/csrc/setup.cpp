@@ -10,37 +10,9 @@
 #include <random>
 
 #include "../../include/moldyn_b200.h"
+#include "../../include/moldyn_b200_rng.hpp"
 
 namespace {
-
-// util/random.hpp:37-76
-class LatticeRng {
-public:
-    explicit LatticeRng(uint64_t seed) : engine_(seed) {}
-    double uniform() { return 1.0 - dist_(engine_); }
-    double normal() {
-        if (have_spare_) {
-            have_spare_ = false;
-            return spare_;
-        }
-        double u = 0.0, v = 0.0, s = 0.0;
-        do {
-            u = 2.0 * uniform() - 1.0;
-            v = 2.0 * uniform() - 1.0;
-            s = u * u + v * v;
-        } while (s >= 1.0 || s == 0.0);
-        const double m = std::sqrt(-2.0 * std::log(s) / s);
-        spare_ = v * m;
-        have_spare_ = true;
-        return u * m;
-    }
-
-private:
-    std::mt19937_64 engine_;
-    std::uniform_real_distribution<double> dist_{0.0, 1.0};
-    double spare_ = 0.0;
-    bool have_spare_ = false;
-};
 
 double fold(double v, double L) { return v - L * std::floor(v / L + 0.5); }
 
@@ -63,7 +35,7 @@ int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed,
     static const std::array<std::array<double, 3>, 4> basis = {
         {{0.0, 0.0, 0.0}, {0.0, 0.5, 0.5}, {0.5, 0.0, 0.5}, {0.5, 0.5, 0.0}}};
     box[0] = box[1] = box[2] = length;
-    LatticeRng rng(seed);
+    moldyn_b200::Rng rng(seed);
     const double sigma_v = std::sqrt(temperature / 1.0);
     int k = 0;
     for (int ix = 0; ix < cells; ++ix)
@@ -103,7 +75,7 @@ int md_fcc_lattice(int cells, double density, double temperature, uint64_t seed,
 // MD_ERR_INVALID_ARGUMENT.
 int64_t md_rng_normals(uint64_t seed, int64_t count, double* out) {
     if (count < 0 || (count > 0 && !out)) return MD_ERR_INVALID_ARGUMENT;
-    LatticeRng rng(seed);
+    moldyn_b200::Rng rng(seed);
     for (int64_t k = 0; k < count; ++k) out[k] = rng.normal();
     return count;
 }

@@ -190,6 +190,7 @@ int system_permute(md_system* sys, const int* d_perm) {
     sys->cur = sys->alt;
     sys->alt = t;
     ++sys->epoch;
+    graph_epoch_bump();  // the current arrays moved
     return MD_OK;
 }
 
@@ -212,6 +213,7 @@ using namespace mdb;
 extern "C" {
 
 int md_system_create(md_context* ctx, int64_t n, const double box[3], md_system** out) {
+    graph_epoch_bump();
     if (!ctx || !box || !out) return fail(MD_ERR_INVALID_ARGUMENT, "md_system_create: NULL argument");
     if (n < 0 || n > (int64_t(1) << 31) - 1)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_system_create: n=%lld out of range",
@@ -248,6 +250,7 @@ int md_system_create(md_context* ctx, int64_t n, const double box[3], md_system*
 }
 
 int md_system_destroy(md_system* sys) {
+    graph_epoch_bump();
     if (!sys) return MD_OK;
     if (sys->ctx) cudaStreamSynchronize(sys->ctx->stream);
     system_free_atoms(&sys->cur);
@@ -354,6 +357,7 @@ int md_system_get_fields(md_system* sys, int count, const int* fields, double* c
 }
 
 int md_system_set_molecule_ids(md_system* sys, const int64_t* ids) {
+    graph_epoch_bump();
     if (!sys || !ids) return fail(MD_ERR_INVALID_ARGUMENT, "md_system_set_molecule_ids: NULL");
     if (sys->n == 0) return MD_OK;
     md_context* ctx = sys->ctx;

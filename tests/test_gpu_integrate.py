@@ -133,6 +133,50 @@ def test_step_graph_replay_equals_host_launches(md, kind):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("kind,cells,precision", [("vv", 5, "fp64"), ("nhc", 5, "fp64"),
+                                                 ("vv", 26, "mixed")])
+def test_step_graph_cached_across_calls(md, kind, cells, precision):
+    """Calls of md_run_lj on the same handles replay the step graph the first call
+    captured (one capture in all), and give the same trajectory, thermo rows and
+    rebuilds as the same calls with every kernel launched from the host.  A
+    velocity-Verlet run split into calls also equals one call of the same length.
+    fcc 26^3 (70,304 atoms) in mixed precision runs on halo tiles."""
+    ctx = md.default_context()
+    lengths = [1, 5, 20, 74, 200]
+    prec = md.PRECISION_MIXED if precision == "mixed" else md.PRECISION_FP64
+
+    def run(split, graphs):
+        ctx.set_graphs(graphs)
+        try:
+            s, st = lattice_system(md, cells, 0.8442, 1.5, 7)
+            lj = md.LennardJones(1.0, 1.0, 2.5, precision=prec)
+            v = md.VerletList(st["box"], 2.5, 0.3)
+            v.build(s)
+            lj.compute_forces(s, v)
+            integ = (md.VelocityVerlet(0.005) if kind == "vv"
+                     else md.NoseHooverChain(0.005, 1.0, 0.5, 3, 3 * s.n - 3))
+            c0 = ctx.graph_captures()
+            rows = []
+            for k in (lengths if split else [sum(lengths)]):
+                rows.append(integ.run(s, v, lj, k, thermo=True))
+            caps = ctx.graph_captures() - c0
+            return s.positions, s.velocities, np.concatenate(rows), v.rebuild_count(), caps
+        finally:
+            ctx.set_graphs(True)
+
+    host = run(True, False)
+    cached = run(True, True)
+    assert cached[4] == 1 and host[4] == 0
+    assert host[3] == cached[3] and host[3] > 3
+    for a, b in zip(host[:3], cached[:3]):
+        assert np.array_equal(a, b)
+    if kind == "vv":
+        single = run(False, True)
+        assert single[3] == cached[3]
+        for a, b in zip(single[:3], cached[:3]):
+            assert np.array_equal(a, b)
+
+
 def test_nhc_fused_run_follows_host_steps(md):
     """The fused Nose-Hoover loop applies integrateChain(dt/2) exactly twice per
     step, as NoseHooverChain::step does (nose_hoover.hpp:37-42): it tracks the
