@@ -347,11 +347,20 @@ struct EnergyVirial {
     double virial = 0.0;  // raw sum of w(r), not divided by 3
 };
 
+// forcefield/forcefield.hpp:17-23: the interface LennardJones implements.
+class ForceField {
+public:
+    virtual ~ForceField() = default;
+    virtual EnergyVirial computeEnergyVirial(const System& sys) const = 0;
+    virtual double longRangeCorrection(const System& sys) const = 0;
+    virtual double longRangeCorrectionPressure(const System& sys) const = 0;
+};
+
 enum class Truncation { Truncated = MD_TRUNCATED, LinearForceShift = MD_LINEAR_FORCE_SHIFT };
 // Pair arithmetic: the reference's FP64 (default) or FP32 pair terms (extension).
 enum class Precision { FP64 = MD_PRECISION_FP64, Mixed = MD_PRECISION_MIXED };
 
-class LennardJones {
+class LennardJones : public ForceField {
 public:
     LennardJones(double sigma, double epsilon, double cutoff, Truncation truncation,
                  Precision precision = Precision::FP64)
@@ -361,9 +370,9 @@ public:
     }
     LennardJones(const LennardJones&) = delete;
     LennardJones& operator=(const LennardJones&) = delete;
-    ~LennardJones() { md_lj_destroy(h_); }
+    ~LennardJones() override { md_lj_destroy(h_); }
 
-    EnergyVirial computeEnergyVirial(const System& sys) const {
+    EnergyVirial computeEnergyVirial(const System& sys) const override {
         EnergyVirial ev;
         detail::check(md_lj_energy_virial(h_, sys.device(), &ev.energy, &ev.virial));
         return ev;
@@ -386,8 +395,8 @@ public:
         sys.deviceChanged();
         return ev;
     }
-    double longRangeCorrection(const System& sys) const { return lrc(sys).first; }
-    double longRangeCorrectionPressure(const System& sys) const { return lrc(sys).second; }
+    double longRangeCorrection(const System& sys) const override { return lrc(sys).first; }
+    double longRangeCorrectionPressure(const System& sys) const override { return lrc(sys).second; }
     double sigma() const { return sigma_; }
     double epsilon() const { return epsilon_; }
     double cutoff() const { return cutoff_; }
@@ -743,6 +752,58 @@ private:
     std::size_t lags_;
     md_vacf* h_ = nullptr;
 };
+
+// ------------------------------------------------------- analyze/block_average.hpp
+// Host-side statistics (no device work): the mean of a time series and its
+// standard error by the blocking method of Flyvbjerg and Petersen (J. Chem. Phys.
+// 91, 461 (1989)), as analyze/block_average.cpp applies it.  Level 0 is the
+// series itself; each further level halves it by averaging neighbouring pairs
+// (an odd last sample is dropped) while at least four blocks remain.  At every
+// level with n >= 2 blocks the standard error is sqrt(s^2 / n), s^2 the unbiased
+// block variance, with its own uncertainty se / sqrt(2 (n - 1)).  The result is
+// the first level whose error moved by no more than the previous level's
+// uncertainty (the plateau), else the last level.
+struct BlockResult {
+    double mean;
+    double standardError;
+    std::size_t blocks;
+};
+
+inline BlockResult blockAverage(const std::vector<double>& samples) {
+    if (samples.empty()) return BlockResult{0.0, 0.0, 0};
+    if (samples.size() == 1) return BlockResult{samples[0], 0.0, 1};
+    auto average = [](const std::vector<double>& v) {
+        double t = 0.0;
+        for (double x : v) t += x;
+        return t / static_cast<double>(v.size());
+    };
+    const double grand = average(samples);
+    std::vector<double> se, err;
+    std::vector<std::size_t> count;
+    std::vector<double> level(samples);
+    for (;;) {
+        const std::size_t n = level.size();
+        const double m = average(level);
+        double ss = 0.0;
+        for (double x : level) ss += (x - m) * (x - m);
+        const double e = std::sqrt(ss / static_cast<double>(n - 1) / static_cast<double>(n));
+        se.push_back(e);
+        err.push_back(e / std::sqrt(2.0 * static_cast<double>(n - 1)));
+        count.push_back(n);
+        if (n < 4) break;
+        std::vector<double> next(n / 2);
+        for (std::size_t k = 0; k < next.size(); ++k) next[k] = 0.5 * (level[2 * k] + level[2 * k + 1]);
+        level.swap(next);
+    }
+    std::size_t pick = se.size() - 1;
+    for (std::size_t k = 1; k < se.size(); ++k) {
+        if (std::fabs(se[k] - se[k - 1]) <= err[k - 1]) {
+            pick = k;
+            break;
+        }
+    }
+    return BlockResult{grand, se[pick], count[pick]};
+}
 
 // ------------------------------------------------------------------ core/units.hpp
 namespace units {

@@ -27,9 +27,12 @@ _d = C.POINTER(C.c_double)
 _i64 = C.POINTER(C.c_int64)
 
 
-def build(ref_root: str = "/root/reference") -> None:
-    """Compile the restatement (and the reference, when its sources exist)."""
-    env = dict(os.environ, REF_ROOT=ref_root)
+def build(ref_root: str | None = None) -> None:
+    """Compile the restatement (and the reference, when its sources exist under
+    ref_root, else under oracle/Makefile's REF_ROOT)."""
+    env = dict(os.environ)
+    if ref_root:
+        env["REF_ROOT"] = ref_root
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True, env=env)
 
 
@@ -190,6 +193,10 @@ def ref():
         R.ref_verlet_pairs.restype = C.c_int64
         R.ref_verlet_pairs.argtypes = [C.c_int64, _d, _d, _d, _d, C.c_double, C.c_double, _i64,
                                        _i64, C.c_int64]
+        R.ref_lj_verlet_all.restype = C.c_int64
+        R.ref_lj_verlet_all.argtypes = ([C.c_int64, _d, _d, _d, _d, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, C.c_double, _d, _d, _d, _d, _d,
+                                         _i64, _i64, C.c_int64])
         R.ref_verlet_needs_rebuild.restype = C.c_int
         R.ref_verlet_needs_rebuild.argtypes = [C.c_int64, _d, _d, _d, _d, _d, _d, _d, C.c_double,
                                                C.c_double]
@@ -220,6 +227,32 @@ def ref():
         R.ref_vacf.argtypes = [C.c_int64, C.c_int64, _d, _d, C.c_int64, _d, C.c_double, _d]
         _ref = R
     return _ref
+
+
+def ref_lj_verlet(pos, box, rc=2.5, skin=0.3, trunc=0, sigma=1.0, eps=1.0, cap=None):
+    """The compiled reference's moldyn_run ForceFn on one state: VerletList::build,
+    LennardJones::computeForces(sys, verlet) and the list's pairs.  Returns
+    (forces[N,3], energy, virial, pairs[M,2] in the reference's order)."""
+    R = ref()
+    if R is None:
+        raise RuntimeError("the compiled reference (oracle/_ref/libmoldyn_ref.so) is absent")
+    pos = _f64(pos)
+    n = pos.shape[0]
+    x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+    box = _f64(box)
+    f = [np.zeros(n) for _ in range(3)]
+    e, w = C.c_double(), C.c_double()
+    cap = cap or max(64, 48 * n)
+    while True:
+        pi = np.zeros(cap, dtype=np.int64)
+        pj = np.zeros(cap, dtype=np.int64)
+        m = R.ref_lj_verlet_all(n, _p(box), _p(x), _p(y), _p(z), sigma, eps, rc, trunc, skin,
+                                *[_p(a) for a in f], C.byref(e), C.byref(w), _p(pi), _p(pj), cap)
+        if m == -2:
+            raise ValueError("reference raised std::invalid_argument")
+        if m <= cap:
+            return np.stack(f, 1), e.value, w.value, np.stack([pi[:m], pj[:m]], 1)
+        cap = int(m)
 
 
 # ---------------------------------------------------------------------------

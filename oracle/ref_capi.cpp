@@ -15,6 +15,7 @@
 #include <utility>
 #include <vector>
 
+#include "moldyn/analyze/block_average.hpp"
 #include "moldyn/analyze/msd.hpp"
 #include "moldyn/analyze/rdf.hpp"
 #include "moldyn/analyze/vacf.hpp"
@@ -140,6 +141,38 @@ int64_t ref_verlet_pairs(int64_t n, const double* box, const double* x, const do
     System sys = makeSystem(n, box, x, y, z, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     VerletList verlet(sys.box(), cutoff, skin);
     verlet.build(sys);
+    int64_t count = 0;
+    verlet.forEachPair([&](std::size_t i, std::size_t j) {
+        if (count < cap) {
+            pi[count] = static_cast<int64_t>(i);
+            pj[count] = static_cast<int64_t>(j);
+        }
+        ++count;
+    });
+    return count;
+}
+
+// One VerletList build (verlet_list.cpp:8-42), then computeForces(sys, verlet)
+// (lennard_jones.cpp:116-119) and the list's pairs: the moldyn_run ForceFn's
+// outputs on one state.  Returns the pair count (pairs beyond cap are counted,
+// not stored), or -2 for std::invalid_argument.
+int64_t ref_lj_verlet_all(int64_t n, const double* box, const double* x, const double* y,
+                          const double* z, double sigma, double eps, double rc, int truncation,
+                          double skin, double* fx, double* fy, double* fz, double* energy,
+                          double* virial, int64_t* pi, int64_t* pj, int64_t cap) {
+    System sys = makeSystem(n, box, x, y, z, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    LennardJones lj(sigma, eps, rc, trunc(truncation));
+    EnergyVirial ev;
+    VerletList verlet(sys.box(), rc, skin);
+    try {
+        verlet.build(sys);
+        ev = lj.computeForces(sys, verlet);
+    } catch (const std::invalid_argument&) {
+        return -2;
+    }
+    *energy = ev.energy;
+    *virial = ev.virial;
+    dumpState(sys, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, fx, fy, fz);
     int64_t count = 0;
     verlet.forEachPair([&](std::size_t i, std::size_t j) {
         if (count < cap) {
@@ -361,6 +394,14 @@ void ref_vacf(int64_t frames, int64_t n, const double* box, const double* vel, i
     const std::vector<double> c = vacf.vacf();
     for (int64_t k = 0; k <= max_lag; ++k) out[k] = c[k];
     *d = vacf.diffusionCoefficient(dt);
+}
+
+// blockAverage (analyze/block_average.cpp): out[0..2] = mean, standard error, blocks.
+void ref_block_average(int64_t n, const double* samples, double* out) {
+    const BlockResult r = blockAverage(std::vector<double>(samples, samples + n));
+    out[0] = r.mean;
+    out[1] = r.standardError;
+    out[2] = static_cast<double>(r.blocks);
 }
 
 }  // extern "C"

@@ -1,9 +1,11 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference) and the
-reference library built by oracle/Makefile (oracle/_ref/libmoldyn_ref.so):
+Run in a container that has the reference tree (REF_ROOT, default /root/reference
+as in oracle/Makefile) and the reference built by oracle/Makefile
+(oracle/_ref/libmoldyn_ref.so and the reference's own apps oracle/_ref/moldyn_run,
+oracle/_ref/water_rdf):
 
-    python tests/golden/make_golden.py [REF_ROOT]
+    python tests/golden/make_golden.py [REF_ROOT [FIXTURE ...]]
 
 Inputs come from the reference's own data files (data/nist/...), the published
 NIST values are read out of the reference's own test sources
@@ -16,7 +18,9 @@ from __future__ import annotations
 import ctypes as C
 import os
 import re
+import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
@@ -261,6 +265,72 @@ def exp05_fixture(ref_root, R):
     return {"rows": rows}
 
 
+# moldyn_run command lines whose outputs the drop-in build of the same app must
+# reproduce: the 864-atom drop-in configuration (velocity Verlet, 1000 steps), the
+# same start under the Nose-Hoover chain, and linear-force-shift truncation.
+APP_RUNS = {
+    "c1_nve": ["--cells", "6", "--density", "0.8442", "--temperature", "0.722", "--cutoff", "2.5",
+               "--skin", "0.3", "--dt", "0.005", "--equilibrate", "0", "--production", "1000",
+               "--thermostat", "none", "--seed", "1"],
+    "c1_nhc": ["--cells", "6", "--density", "0.8442", "--temperature", "0.722", "--cutoff", "2.5",
+               "--skin", "0.3", "--dt", "0.005", "--equilibrate", "0", "--production", "500",
+               "--thermostat", "nose-hoover", "--seed", "1"],
+    "lfs_nve": ["--cells", "5", "--density", "0.8", "--temperature", "1.0", "--cutoff", "2.5",
+                "--skin", "0.3", "--dt", "0.005", "--equilibrate", "0", "--production", "500",
+                "--thermostat", "none", "--seed", "12345", "--truncation", "linear-force-shift"],
+}
+WATER_RDF_ARGS = ["--equilibrate", "200", "--production", "100", "--sample-every", "10"]
+
+
+def parse_csv(path):
+    """(comment lines minus the provenance ones that name the binary or host, rows)."""
+    comments, rows = [], []
+    for line in open(path):
+        line = line.rstrip("\n")
+        if line.startswith("#"):
+            if not line.startswith(("# command:", "# git_sha:", "# host:", "# wall_seconds:")):
+                comments.append(line)
+        elif line and not line[0].isalpha():
+            rows.append(line.split(","))
+    return comments, rows
+
+
+def apps_fixture(ref_root, R):
+    """Outputs of the reference's own apps (oracle/_ref/moldyn_run, water_rdf, built
+    from its sources by oracle/Makefile): moldyn_run's thermo, g(r) and MSD/VACF
+    CSVs for APP_RUNS, its NIST table (--nist-config data/nist/lj), and a short
+    water_rdf run (WATER_RDF_ARGS) on data/nist/spce configuration 3."""
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, args in APP_RUNS.items():
+            files = {k: os.path.join(tmp, f"{name}_{k}.csv") for k in ("thermo", "rdf", "msd")}
+            subprocess.run([os.path.join(ref, "moldyn_run"), *args, "--thermo-out", files["thermo"],
+                            "--rdf-out", files["rdf"], "--msd-out", files["msd"]], check=True,
+                           stdout=subprocess.DEVNULL)
+            for k, path in files.items():
+                comments, rows = parse_csv(path)
+                out[f"{name}_{k}_comments"] = np.array(comments)
+                if k == "thermo":
+                    out[f"{name}_thermo_phase"] = np.array([r[2] for r in rows])
+                    rows = [[r[0], r[1]] + r[3:] for r in rows]
+                out[f"{name}_{k}"] = np.array([[float(v) for v in r] for r in rows])
+        nist = subprocess.run([os.path.join(ref, "moldyn_run"), "--nist-config",
+                               os.path.join(ref_root, "data", "nist", "lj")], check=True,
+                              capture_output=True, text=True)
+        out["nist_table"] = np.array(nist.stdout)
+        csv = os.path.join(tmp, "water_rdf.csv")
+        subprocess.run([os.path.join(ref, "water_rdf"), "--data", os.path.join(ref_root, "data"),
+                        "--out", csv, *WATER_RDF_ARGS], check=True, stdout=subprocess.DEVNULL)
+        comments, rows = parse_csv(csv)
+        out["water_rdf_comments"] = np.array(comments)
+        out["water_rdf_g"] = np.array([[float(v) for v in r] for r in rows])
+    out["app_runs"] = np.array([" ".join(a) for a in APP_RUNS.values()])
+    out["app_run_names"] = np.array(list(APP_RUNS))
+    out["water_rdf_args"] = np.array(" ".join(WATER_RDF_ARGS))
+    return out
+
+
 FIXTURES = {
     "nist_lj.npz": lambda root, R: lj_fixture(root, R),
     "nist_spce.npz": lambda root, R: spce_fixture(root, R),
@@ -270,12 +340,13 @@ FIXTURES = {
     "exp03_ref.npz": exp03_fixture,
     "exp04_ref.npz": exp04_fixture,
     "exp05_ref.npz": exp05_fixture,
+    "apps_ref.npz": apps_fixture,
 }
 
 
 def main():
     """make_golden.py [REF_ROOT [FIXTURE ...]]: every fixture, or the named ones."""
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT", "/root/reference")
     names = sys.argv[2:] or sorted(FIXTURES)
     O.build(ref_root)
     R = O.ref()

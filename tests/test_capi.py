@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from conftest import ROOT, load_golden
 
@@ -98,16 +99,72 @@ def test_cxx_api_header_compiles_and_links(tmp_path):
 
 
 def test_cxx_header_compiles_cleanly():
-    """The reference-shaped C++ API (include/moldyn_b200.hpp) and the programs
-    written against it -- the moldyn_run-style shims and the water_rdf app --
-    compile with -Wall -Wextra -Werror (syntax and types only; no GPU)."""
+    """The reference-shaped C++ API (include/moldyn_b200.hpp) and the moldyn_run-style
+    shims written against it compile with -Wall -Wextra -Werror (syntax and types
+    only; no GPU)."""
     import os
     import subprocess
     from conftest import ROOT
     srcs = [os.path.join(ROOT, "tests", "cpp", f) for f in ("shim_run.cpp", "shim_analyze.cpp")]
-    srcs.append(os.path.join(ROOT, "moleculardynamics_b200", "apps", "water_rdf.cpp"))
     for src in srcs:
         res = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
                               "-I", os.path.join(ROOT, "include"), src],
                              capture_output=True, text=True)
         assert res.returncode == 0, (src, res.stderr[-2000:])
+
+
+def test_reference_apps_build_unchanged(tmp_path):
+    """The reference's own apps/moldyn_run.cpp and apps/water_rdf.cpp, read where
+    they lie and not edited, compile with -Wall -Wextra -Werror against
+    include/moldyn/ (the reference's header paths over this library) and link to
+    libmoldyn_b200.so, by the recipe that builds the shipped drop-in binaries
+    (moleculardynamics_b200/apps/Makefile).  Skipped where the reference tree is
+    absent (the recipe then builds nothing)."""
+    import os
+    import subprocess
+    from conftest import ROOT
+    res = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "moleculardynamics_b200", "apps"),
+                          f"BINDIR={tmp_path}", "CXXFLAGS=-std=c++17 -O0 -Wall -Wextra -Werror"],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr[-3000:]
+    built = sorted(os.listdir(tmp_path))
+    if not built:
+        pytest.skip("the reference's apps are not present here")
+    assert built == ["moldyn_run", "water_rdf"]
+
+
+
+
+def test_block_average_equals_reference(tmp_path):
+    """blockAverage (analyze/block_average.hpp, host-side statistics in the C++ layer)
+    gives the reference's mean, standard error and plateau block count bit for bit on
+    correlated series of several lengths, and its empty and one-sample answers."""
+    import subprocess
+
+    import oracle as O
+    R = O.ref()
+    if R is None:
+        pytest.skip("the compiled reference (oracle/_ref) is not present")
+    R.ref_block_average.argtypes = [C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    exe = tmp_path / "block_average"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp",
+                                                                "block_average.cpp"),
+                    "-o", str(exe)], check=True)
+    rng = np.random.default_rng(11)
+    cases = [np.zeros(0), np.array([2.5])]
+    for n in (2, 3, 7, 64, 1000, 4097):
+        x = np.empty(n)
+        x[0] = rng.normal()
+        for k in range(1, n):  # AR(1): correlated, so the plateau is not level 0
+            x[k] = 0.9 * x[k - 1] + rng.normal()
+        cases.append(x)
+    for x in cases:
+        out = subprocess.run([str(exe)], input=" ".join(repr(float(v)) for v in x),
+                             capture_output=True, text=True, check=True).stdout.split()
+        ref = np.zeros(3)
+        xs = np.ascontiguousarray(x, dtype=np.float64)
+        R.ref_block_average(len(xs), xs.ctypes.data_as(C.POINTER(C.c_double)),
+                            ref.ctypes.data_as(C.POINTER(C.c_double)))
+        assert float(out[0]) == ref[0] and float(out[1]) == ref[1], (len(x), out, ref)
+        assert int(out[2]) == int(ref[2]), (len(x), out, ref)

@@ -186,12 +186,13 @@ def test_units():
 
 
 def test_cxx_app_flag_errors():
-    """The C++ drop-in (moleculardynamics_b200/bin/water_rdf) rejects flags as
-    apps/water_rdf.cpp:120-142 does, before touching the device."""
+    """The reference's water_rdf app built unchanged on this library
+    (moleculardynamics_b200/bin/water_rdf) rejects flags as apps/water_rdf.cpp:120-142
+    does, before touching the device."""
     import os
     import subprocess
     exe = os.path.join(os.path.dirname(md.library_path()), "bin", "water_rdf")
-    assert os.path.exists(exe), "build the package first (make -C moleculardynamics_b200/csrc)"
+    assert os.path.exists(exe), "build the drop-in apps first (make -C moleculardynamics_b200/apps)"
     res = subprocess.run([exe, "--bogus", "1"], capture_output=True, text=True)
     assert res.returncode == 1 and "unknown flag --bogus" in res.stderr
     res = subprocess.run([exe, "--seed"], capture_output=True, text=True)
