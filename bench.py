@@ -510,11 +510,12 @@ def run_gpu_arm(args):
     e2e_value = world * n * e2e_steps / sec
     # the full NVE window of the configuration, both precisions, outside the timed region
     drift = None
-    if args.drift_steps > 0:
-        d64 = drift_run(md, ctx, box, pos, vel, frc, md.PRECISION_FP64, args.drift_steps)
-        dmx = drift_run(md, ctx, box, pos, vel, frc, md.PRECISION_MIXED, args.drift_steps)
+    drift_steps = 10000 if args.drift_steps is None else args.drift_steps
+    if drift_steps > 0:
+        d64 = drift_run(md, ctx, box, pos, vel, frc, md.PRECISION_FP64, drift_steps)
+        dmx = drift_run(md, ctx, box, pos, vel, frc, md.PRECISION_MIXED, drift_steps)
         ratio = dmx["max_abs_dev_per_atom"] / max(d64["max_abs_dev_per_atom"], 1e-300)
-        drift = {"steps": args.drift_steps, "fp64": d64, "mixed": dmx,
+        drift = {"steps": drift_steps, "fp64": d64, "mixed": dmx,
                  "mixed_over_fp64_max_dev": ratio, "within_2x_fp64": bool(ratio <= 2.0),
                  "window_mixed_over_fp64": dmx["atom_steps_per_s"] / d64["atom_steps_per_s"]}
 
@@ -636,6 +637,55 @@ def batch_cpu_reference(steps, procs):
     return total / max(r[2] for r in res), procs
 
 
+def make_batch(md, rows, device, precision, truncation):
+    """The replica table as one batch: each replica its own context, lattice,
+    list, force field and Nose-Hoover chain."""
+    batch = md.Batch()
+    parts = []
+    for r in rows:
+        ctx = md.Context(device)
+        st = md.fcc_lattice(r["cells"], r["density"], r["temperature"], r["seed"])
+        s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"], ctx=ctx)
+        lj = md.LennardJones(1.0, 1.0, RC, truncation, precision=precision)
+        v = md.VerletList(st["box"], RC, SKIN, ctx=ctx)
+        v.build(s)
+        pe, _ = lj.compute_forces(s, v)
+        integ = md.NoseHooverChain(DT, r["temperature"], 0.5, 3, 3 * s.n - 3)
+        parts.append((ctx, s, v, lj, integ, pe + s.kinetic_energy()))
+        batch.add(integ, s, v, lj)
+    return batch, parts
+
+
+def batch_drift_table(md, rows, device, steps):
+    """Extended-Hamiltonian conservation of every replica over `steps` NHC steps
+    from its lattice, outside the timed region: mixed and FP64 with the truncated
+    potential of the configuration, and mixed with linear-force-shift truncation
+    (no energy step when a pair crosses the cutoff) as the control.  Per replica:
+    max |H'(t) - H'(0)| / N and the same relative to |H'(0)|."""
+    cols = {}
+    for name, prec, trunc in (("mixed", md.PRECISION_MIXED, 0), ("fp64", md.PRECISION_FP64, 0),
+                              ("mixed_lfs", md.PRECISION_MIXED, 1)):
+        batch, parts = make_batch(md, rows, device, prec, trunc)
+        th = batch.run(steps, thermo=True)
+        h = th[:, :, 0] + th[:, :, 2] + th[:, :, 3]
+        h0 = np.array([p[5] for p in parts])  # H' before the first step (chain at rest)
+        dev = np.max(np.abs(h - h0[:, None]), axis=1)
+        n = np.array([p[1].n for p in parts], dtype=float)
+        cols[name] = (dev / n, dev / np.abs(h0))
+        del batch, parts
+    table = []
+    for k, r in enumerate(rows):
+        table.append({"atoms": r["atoms"], "density": r["density"],
+                      "temperature": r["temperature"],
+                      **{f"{name}_per_atom": float(v[0][k]) for name, v in cols.items()},
+                      **{f"{name}_relative": float(v[1][k]) for name, v in cols.items()}})
+    summary = {name: {"per_atom_max": float(v[0].max()), "per_atom_median": float(np.median(v[0])),
+                      "relative_max": float(v[1].max())} for name, v in cols.items()}
+    return {"steps": steps, "summary": summary, "replicas": table,
+            "mixed_over_fp64_per_atom_max": summary["mixed"]["per_atom_max"] /
+            max(summary["fp64"]["per_atom_max"], 1e-300)}
+
+
 def run_batch_arm(args):
     world, rank, local = dist_env()
     group = Group(world)
@@ -661,19 +711,7 @@ def run_batch_arm(args):
         return 0
     import moleculardynamics_b200 as md
     rows = batch_table()
-    batch = md.Batch()
-    parts = []
-    for r in rows:
-        ctx = md.Context(local)
-        st = md.fcc_lattice(r["cells"], r["density"], r["temperature"], r["seed"])
-        s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"], ctx=ctx)
-        lj = md.LennardJones(1.0, 1.0, RC, precision=md.PRECISION_MIXED)
-        v = md.VerletList(st["box"], RC, SKIN, ctx=ctx)
-        v.build(s)
-        pe, _ = lj.compute_forces(s, v)
-        integ = md.NoseHooverChain(DT, r["temperature"], 0.5, 3, 3 * s.n - 3)
-        parts.append((ctx, s, v, lj, integ, pe + s.kinetic_energy()))
-        batch.add(integ, s, v, lj)
+    batch, parts = make_batch(md, rows, local, md.PRECISION_MIXED, 0)
     n_atoms = sum(p[1].n for p in parts)
     batch.run(args.warmup)
     lead = parts[0][0]
@@ -709,6 +747,9 @@ def run_batch_arm(args):
                 "per_atom_max": float(per_atom.max()), "per_atom_median": float(np.median(per_atom))},
             "clocks": clocks.summary(),
         }
+        drift_steps = 5000 if args.drift_steps is None else args.drift_steps
+        if drift_steps > 0:
+            line["nhc_drift_per_replica"] = batch_drift_table(md, rows, local, drift_steps)
         if world == 1 and not args.no_cpu:
             cval, procs = batch_cpu_reference(max(1, args.cpu_steps), args.ref_procs)
             line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": procs,
@@ -733,6 +774,56 @@ def adjoint_config(steps, every, skin):
                         f"states saved every {every} steps, list skin {skin}",
             "loss": "(mean virial pressure - 1)^2 + (mean potential energy per atom + 5)^2",
             "n_atoms": 32000, "parallelism": "one system"}
+
+
+def adjoint_sweep(md, ctx, pos, vel, mass, box, every, skin, group, rank):
+    """Where the adjoint gradient of the trajectory loss stops agreeing with central
+    finite differences of the same forward code, as the trajectory grows: for each
+    length, d(loss)/d(epsilon) and d(loss)/d(sigma) by the adjoint, against
+    [L(p (1 + h)) - L(p (1 - h))] / 2h for h = 1e-5 ... 1e-10 (relative).  The loss
+    and the force-shifted potential are the benchmark's."""
+    n, vol = pos.shape[0], float(np.prod(box))
+    dof = 3 * n - 3
+
+    def loss_rows(rows):
+        p = n / vol * 2 * rows[:, 2] / dof + rows[:, 1] / (3 * vol)
+        u = rows[:, 0] / n
+        return (p.mean() - 1.0) ** 2 + (u.mean() + 5.0) ** 2, p.mean(), u.mean()
+
+    def forward(steps, sigma=1.0, eps=1.0):
+        s = md.System.from_arrays(pos, box, vel=vel, mass=mass, ctx=ctx)
+        traj = md.AdjointTrajectory(ctx)
+        lj = md.LennardJones(sigma, eps, RC, md.Truncation.LinearForceShift)
+        rows = traj.forward(s, lj, DT, steps, every, skin)
+        return rows, traj
+
+    hs = [1e-5, 1e-6, 1e-7, 1e-8, 1e-9, 1e-10]
+    table = []
+    for steps in (50, 100, 200, 400, 700, 1000):
+        rows, traj = forward(steps)
+        loss, pm, um = loss_rows(rows)
+        g = np.zeros_like(rows)
+        g[:, 0] = 2 * (um + 5.0) / (n * steps)
+        g[:, 1] = 2 * (pm - 1.0) / (3 * vol * steps)
+        g[:, 2] = 2 * (pm - 1.0) * (n / vol) * 2 / (dof * steps)
+        d_eps, d_sig, _, _ = traj.backward(g)
+        entry = {"steps": steps, "loss": loss, "d_epsilon": d_eps, "d_sigma": d_sig, "fd": []}
+        for h in hs:
+            fe = (loss_rows(forward(steps, eps=1 + h)[0])[0] -
+                  loss_rows(forward(steps, eps=1 - h)[0])[0]) / (2 * h)
+            fs = (loss_rows(forward(steps, sigma=1 + h)[0])[0] -
+                  loss_rows(forward(steps, sigma=1 - h)[0])[0]) / (2 * h)
+            entry["fd"].append({"h": h, "fd_epsilon": fe, "fd_sigma": fs,
+                                "rel_err_epsilon": abs(d_eps - fe) / abs(fe),
+                                "rel_err_sigma": abs(d_sig - fs) / abs(fs)})
+        entry["best_rel_err_epsilon"] = min(f["rel_err_epsilon"] for f in entry["fd"])
+        entry["best_rel_err_sigma"] = min(f["rel_err_sigma"] for f in entry["fd"])
+        table.append(entry)
+    if rank == 0:
+        print(json.dumps({"adjoint_sweep": table, "config": adjoint_config(1000, every, skin)}),
+              flush=True)
+    group.close()
+    return 0
 
 
 def run_adjoint_arm(args):
@@ -783,6 +874,8 @@ def run_adjoint_arm(args):
         return rows, traj, s, ms.value
 
     run_forward()  # warm-up: allocations, module load
+    if args.adj_sweep:
+        return adjoint_sweep(md, ctx, pos, vel, mass, box, every, skin, group, rank)
     rows, traj, s, fwd_ms = run_forward(timed=True)
     loss, pm, um = loss_rows(rows)
     g = np.zeros_like(rows)
@@ -1272,6 +1365,9 @@ def main():
                          "forward + backward of a 32,000-atom differentiable trajectory "
                          "(--steps is its length)")
     ap.add_argument("--adj-skin", type=float, default=2.0)
+    ap.add_argument("--adj-sweep", action="store_true",
+                    help="adjoint: the gradient against central differences over trajectory "
+                         "lengths and difference steps (a table, not the benchmark line)")
     ap.add_argument("--equil-water", type=int, default=1000)
     ap.add_argument("--settle", action="store_true",
                     help="water: SETTLE instead of SHAKE/RATTLE iterations")
@@ -1294,9 +1390,10 @@ def main():
                          "absent or --gpu-equil is given")
     ap.add_argument("--gpu-equil", action="store_true",
                     help="equilibrate on the GPU instead of loading the reference's state")
-    ap.add_argument("--drift-steps", type=int, default=10000,
-                    help="length of the NVE drift window run in both precisions after the "
-                         "timed region (0: skip)")
+    ap.add_argument("--drift-steps", type=int, default=None,
+                    help="length of the drift runs after the timed region: the NVE window in "
+                         "both precisions (lj1m, default 10000) or the per-replica NHC table "
+                         "(batch, default 5000); 0 skips them")
     ap.add_argument("--tpa", type=int, default=2)
     ap.add_argument("--unroll", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=20)

@@ -50,6 +50,7 @@ extern "C" {
 #define MD_STATUS_RATTLE_DIVERGED 0x4u   /* RATTLE did not converge in maxIterations */
 #define MD_STATUS_SHAKE_SINGULAR 0x8u    /* SHAKE denominator below 1e-30 */
 #define MD_STATUS_NONFINITE 0x10u        /* a position or the kinetic energy stopped being finite */
+#define MD_STATUS_WAIT_TIMEOUT 0x20u     /* a kernel's bounded wait on its own copies ran out */
 
 /* System fields (core/system.hpp:54-59). */
 #define MD_FIELD_X 0
@@ -370,9 +371,10 @@ MD_API int md_run_lj(md_integrator* integ, md_system* sys, md_verlet* list, md_l
 /* Lennard-Jones forces, energy and virial by brute force (the arithmetic of
  * md_lj_forces) for callers that must not allocate device memory -- no counterpart
  * in the reference.  Callers such as a host framework that owns all device memory
- * through its own pool, code running inside a stream capture, or latency-critical
- * loops that cannot afford cudaMalloc's device-wide synchronisation pass their
- * own device buffers: positions d_x/d_y/d_z (n doubles each, atom order), force
+ * through its own pool, or latency-critical loops that cannot afford cudaMalloc's
+ * device-wide synchronisation, pass their own device buffers: positions
+ * d_x/d_y/d_z (n doubles each, atom order; they need not be wrapped into the box:
+ * every displacement folds by the reference's minimum image), force
  * outputs d_fx/d_fy/d_fz and d_energy_virial (2 doubles: pair energy, virial),
  * and the CUDA stream to run on (NULL = legacy default stream).  The call
  * allocates nothing: its reduction scratch is a fixed 16 KiB array in the
@@ -380,9 +382,11 @@ MD_API int md_run_lj(md_integrator* integ, md_system* sys, md_verlet* list, md_l
  * process exits, which limits n to 262,144 atoms (larger n is rejected with
  * MD_ERR_INVALID_ARGUMENT).  The first call on each device looks up the array's
  * device address (cudaGetSymbolAddress), so make that first call before any
- * stream capture.  All calls share the array: calls that may overlap on the GPU
- * (different streams, or different host threads on one device) race and must be
- * serialised by the caller.  The call returns once the work is enqueued. */
+ * stream capture.  The address is kept for the life of the process: do not call
+ * this after a cudaDeviceReset.  All calls share the array: calls that may overlap
+ * on the GPU (different streams, or different host threads on one device) race
+ * and must be serialised by the caller.  The call returns once the work is
+ * enqueued. */
 MD_API int md_lj_forces_static(const double* d_x, const double* d_y, const double* d_z,
                                int64_t n, const double box[3], double sigma, double epsilon,
                                double cutoff, int truncation, double* d_fx, double* d_fy,

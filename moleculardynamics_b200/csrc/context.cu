@@ -97,12 +97,13 @@ int ctx_check_status(md_context* ctx) {
     // reported once: clear the word so the context can be used again
     MDB_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
     MDB_CUDA(cudaStreamSynchronize(ctx->stream));
-    return fail(MD_ERR_DEVICE, "device status 0x%x (%s%s%s%s%s)", st,
+    return fail(MD_ERR_DEVICE, "device status 0x%x (%s%s%s%s%s%s)", st,
                 (st & MD_STATUS_NEIGHBOR_OVERFLOW) ? "neighbour overflow " : "",
                 (st & MD_STATUS_SHAKE_DIVERGED) ? "SHAKE diverged " : "",
                 (st & MD_STATUS_RATTLE_DIVERGED) ? "RATTLE diverged " : "",
                 (st & MD_STATUS_SHAKE_SINGULAR) ? "SHAKE singular " : "",
-                (st & MD_STATUS_NONFINITE) ? "non-finite state" : "");
+                (st & MD_STATUS_NONFINITE) ? "non-finite state " : "",
+                (st & MD_STATUS_WAIT_TIMEOUT) ? "bounded wait ran out" : "");
 }
 
 void ctx_time_begin(md_context* ctx, int kernel) {

@@ -1,11 +1,9 @@
 // noalloc.cu -- a Lennard-Jones force entry point that allocates no device memory.
 //
 // Who needs it: callers that must not call cudaMalloc.  Examples are a host
-// framework that owns all device memory through its own pool allocator; code
-// running between a stream's begin/end capture, where allocation would break the
-// capture; and latency-critical loops, because cudaMalloc/cudaFree can synchronise
-// the whole device.  Such callers can still hand this library device buffers they
-// own.  md_lj_forces_static takes the positions and the output buffers from the
+// framework that owns all device memory through its own pool allocator, and
+// latency-critical loops, because cudaMalloc/cudaFree can synchronise the whole
+// device.  Such callers can still hand this library device buffers they own.  md_lj_forces_static takes the positions and the output buffers from the
 // caller.  Its only working memory (per-block reduction partials and the
 // completion ticket) lives in the file-scope array below, which every GPU that
 // loads the library holds until the process exits.
@@ -26,7 +24,9 @@ constexpr int64_t kStaticMaxAtoms = static_cast<int64_t>(kStaticMaxBlocks) * kSt
 constexpr int kScratchDoubles = 2 * kStaticMaxBlocks + 1;
 static __device__ __align__(256) double g_static_scratch[kScratchDoubles];
 
-// Device address of g_static_scratch for each device, resolved once.  The host
+// Device address of g_static_scratch for each device, resolved once and kept for
+// the life of the process (a cudaDeviceReset unloads the library's device image and
+// invalidates it, so the entry point must not be called after one).  The host
 // symbol g_static_scratch is only a stand-in for the device array and must never
 // be passed to a kernel itself.
 constexpr int kMaxDevices = 64;
@@ -137,7 +137,10 @@ int md_lj_forces_static(const double* d_x, const double* d_y, const double* d_z,
                         const double box[3], double sigma, double epsilon, double cutoff,
                         int truncation, double* d_fx, double* d_fy, double* d_fz,
                         double* d_energy_virial, void* stream) {
-    if (n < 0 || n > kStaticMaxAtoms)
+    if (n < 0)
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_forces_static: n = %lld, must be non-negative",
+                    static_cast<long long>(n));
+    if (n > kStaticMaxAtoms)
         return fail(MD_ERR_INVALID_ARGUMENT,
                     "md_lj_forces_static: n = %lld exceeds the static scratch limit of %lld atoms "
                     "(use md_lj_forces on an md_system for larger systems)",
