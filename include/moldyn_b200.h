@@ -205,6 +205,14 @@ MD_API int md_verlet_displacements(md_verlet* list, md_system* sys, double* larg
  * fused loop cannot grow it and reports MD_ERR_DEVICE (neighbour overflow).  The
  * list must be built again before its next use. */
 MD_API int md_verlet_set_capacity(md_verlet* list, int capacity, int fixed);
+/* Width of the cells the list is built from; no reference counterpart (the
+ * reference bins at the list cutoff rc + skin, cell_list.cpp:8-14, which 0
+ * restores).  Any width >= rc + skin gives the same pair set: wider cells mean
+ * more candidates per atom but fewer cells (a tuning axis).  The list must be
+ * built again before its next use. */
+MD_API int md_verlet_set_cell_width(md_verlet* list, double width);
+/* Cells per side of the list's grid (after md_verlet_set_cell_width). */
+MD_API int md_verlet_cells_per_side(const md_verlet* list, int dims[3]);
 
 /* ----------------------------------------------------------- Lennard-Jones */
 /* LennardJones(sigma, epsilon, cutoff, truncation) (lennard_jones.hpp:26,

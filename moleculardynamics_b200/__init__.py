@@ -123,6 +123,8 @@ def _load():
         "md_verlet_rebuild_count": (C.c_int, [_vp, _i64p]),
         "md_verlet_pairs": (C.c_int, [_vp, _i64p, _i64p, C.c_int64, _i64p]),
         "md_verlet_set_criterion": (C.c_int, [_vp, C.c_int]),
+        "md_verlet_set_cell_width": (C.c_int, [_vp, C.c_double]),
+        "md_verlet_cells_per_side": (C.c_int, [_vp, C.POINTER(C.c_int)]),
         "md_verlet_displacements": (C.c_int, [_vp, _vp, _d, _d]),
         "md_verlet_set_capacity": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_lj_create": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
@@ -530,6 +532,16 @@ class VerletList:
 
     def set_criterion(self, criterion: int):
         _check(lib().md_verlet_set_criterion(self._h, int(criterion)))
+
+    def set_cell_width(self, width: float):
+        """Cells at least `width` wide (>= cutoff + skin; 0: the reference's rule).
+        The pair set is unchanged; the list must be built again."""
+        _check(lib().md_verlet_set_cell_width(self._h, float(width)))
+
+    def cells_per_side(self):
+        d = (C.c_int * 3)()
+        _check(lib().md_verlet_cells_per_side(self._h, d))
+        return tuple(d)
 
     def set_capacity(self, capacity: int, fixed: bool = False):
         """Neighbours per atom the rows hold; host builds grow it on overflow

@@ -9,7 +9,10 @@ precision, so later runs of the same kind skip the search.
 
 `tune_skin` picks the Verlet skin that minimises the time of a fused step (a
 larger skin means a longer list but fewer rebuilds) by running a short fused
-segment from the same state for each candidate.
+segment from the same state for each candidate.  `tune_cell_width` does the same
+for the width of the cells the list is built from (the reference bins at the
+list cutoff; wider cells give the same pairs from more candidates per atom and
+fewer, fuller cells, which also reshapes the halo tiles of the mixed kernel).
 
 Cache: $MOLDYN_B200_TUNE_CACHE, else ~/.cache/moleculardynamics_b200/autotune.json.
 """
@@ -117,5 +120,34 @@ def tune_skin(box, pos, vel, mass, lj, make_integrator, skins=(0.2, 0.3, 0.4, 0.
     return min(times, key=times.get), times
 
 
+def tune_cell_width(box, pos, vel, mass, lj, skin, make_integrator,
+                    factors=(1.0, 1.1, 1.25, 1.5), steps=100, ctx=None):
+    """The cell width (a factor of the list cutoff rc + skin) with the shortest
+    fused step over `steps` steps from this state; returns (best width,
+    {width: ms per step}).  Factor 1.0 is the reference's own binning."""
+    ctx = ctx or md.default_context()
+    L = md.lib()
+    rl = lj.cutoff + skin
+    times = {}
+    for f in factors:
+        width = rl * f
+        s = md.System.from_arrays(pos, box, vel=vel, mass=mass, ctx=ctx)
+        v = md.VerletList(box, lj.cutoff, skin, ctx=ctx)
+        if f != 1.0:
+            v.set_cell_width(width)
+        if min(v.cells_per_side()) < 3:
+            continue  # too few cells: the list would be built by brute force
+        v.build(s)
+        lj.compute_forces(s, v)
+        integ = make_integrator()
+        integ.run(s, v, lj, 5)  # warm-up
+        ms = C.c_double()
+        md._check(L.md_context_span_begin(ctx.handle))
+        integ.run(s, v, lj, steps)
+        md._check(L.md_context_span_end(ctx.handle, C.byref(ms)))
+        times[width] = ms.value / steps
+    return min(times, key=times.get), times
+
+
 __all__ = ["SHAPES", "cache_path", "problem_key", "time_force_kernel", "tune_force_kernel",
-           "tune_skin"]
+           "tune_skin", "tune_cell_width"]

@@ -240,6 +240,7 @@ struct md_verlet {
     double box[3] = {0, 0, 0};
     double cutoff = 0.0, skin = 0.0;
     int criterion = 0;            // 0 reference top-2 sum, 1 max > skin/2
+    double cell_width = 0.0;      // 0: the reference's cells at the list cutoff
     mdb::CellGrid grid;
     mdb::DevBuf start;            // ncells + 1 (device order == sorted order)
     mdb::DevBuf perm;             // scratch for the sort

@@ -1342,6 +1342,30 @@ int md_verlet_set_criterion(md_verlet* v, int criterion) {
     return MD_OK;
 }
 
+int md_verlet_set_cell_width(md_verlet* v, double width) {
+    graph_epoch_bump();
+    if (!v) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_cell_width: NULL list");
+    const double rl = v->cutoff + v->skin;
+    if (!(width == 0.0 || width >= rl))
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "md_verlet_set_cell_width: width %g is below the list cutoff %g (0 restores "
+                    "the reference's rule)", width, rl);
+    if (v->ctx) cudaStreamSynchronize(v->ctx->stream);
+    MDB_TRY(v->grid.init(v->box, width == 0.0 ? rl : width));
+    MDB_TRY(v->start.ensure(sizeof(int) * static_cast<size_t>(v->grid.ncells + 1)));
+    v->cell_width = width;
+    v->sys = nullptr;  // the list must be built again on the new grid
+    return MD_OK;
+}
+
+int md_verlet_cells_per_side(const md_verlet* v, int dims[3]) {
+    if (!v || !dims) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_cells_per_side: NULL");
+    dims[0] = v->grid.nx;
+    dims[1] = v->grid.ny;
+    dims[2] = v->grid.nz;
+    return MD_OK;
+}
+
 int md_verlet_displacements(md_verlet* v, md_system* sys, double* largest, double* second) {
     if (!v || !sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_displacements: NULL");
     MDB_TRY(verlet_ready(v, sys, "md_verlet_displacements"));

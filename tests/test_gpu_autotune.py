@@ -33,3 +33,36 @@ def test_tune_force_kernel_applies_and_caches(md, tmp_path, monkeypatch):
     assert again == best and t2 == {}
     with pytest.raises(md.InvalidArgument):
         lj.set_launch(3, 1)
+
+
+def test_cell_width_keeps_the_pair_set_and_forces(md):
+    """Cells wider than the list cutoff (the cell-width axis of the tuner) give the
+    reference's pair set exactly and the same FP64 forces to summation order; a
+    width below the list cutoff is refused; tune_cell_width applies the fastest."""
+    st = md.fcc_lattice(10, 0.8442, 0.722, 5)
+    rng = np.random.default_rng(5)
+    pos = st["pos"] + rng.normal(scale=0.1, size=st["pos"].shape)
+    pos -= st["box"] * np.floor(pos / st["box"] + 0.5)
+    box = st["box"]
+    out = []
+    for factor in (0.0, 1.1, 1.3):
+        s = md.System.from_arrays(pos, box)
+        v = md.VerletList(box, 2.5, 0.3)
+        if factor:
+            v.set_cell_width(factor * 2.8)
+        v.build(s)
+        e, w = md.LennardJones(1.0, 1.0, 2.5).compute_forces(s, v)
+        out.append((v.cells_per_side(), v.pairs(), e, w, s.forces))
+    assert out[0][0] == (6, 6, 6) and out[1][0] == (5, 5, 5) and out[2][0] == (4, 4, 4)
+    for cells, pairs, e, w, f in out[1:]:
+        assert np.array_equal(pairs, out[0][1])
+        assert abs(e - out[0][2]) < 1e-12 * abs(out[0][2])
+        assert abs(w - out[0][3]) < 1e-12 * abs(out[0][3])
+        assert np.max(np.abs(f - out[0][4])) < 1e-12 * np.max(np.abs(out[0][4]))
+    with pytest.raises(md.InvalidArgument):
+        md.VerletList(box, 2.5, 0.3).set_cell_width(2.7)
+    lj = md.LennardJones(1.0, 1.0, 2.5)
+    best, times = T.tune_cell_width(box, pos, st["vel"], st["mass"], lj, 0.3,
+                                    lambda: md.VelocityVerlet(0.005), factors=(1.0, 1.2),
+                                    steps=20)
+    assert best in times and times[best] == min(times.values()) and len(times) == 2
