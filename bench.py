@@ -72,7 +72,8 @@ def equilibration_note(ref_steps, gpu_steps):
 
 def config(equilibration):
     return {
-        "workload": "1M-atom LJ NVE velocity-Verlet: fcc 64^3 (N=1048576), rho*=0.8442, "
+        "workload": ("1M-atom LJ NVE velocity-Verlet: " if CELLS == 64 else "LJ NVE velocity-Verlet: ")
+                    + f"fcc {CELLS}^3 (N={4 * CELLS ** 3}), rho*=0.8442, "
                     "T*=0.722, rc=2.5 truncated, skin=0.3, dt*=0.005",
         "n_atoms": 4 * CELLS ** 3,
         "equilibration": equilibration,
@@ -456,6 +457,12 @@ def run_reference_arm(args):
 
 
 def run_gpu_arm(args):
+    global CELLS
+    if args.cells != CELLS:
+        # profiling configuration: a smaller lattice of the same liquid, equilibrated
+        # on the GPU (the reference-equilibrated state is the 64^3 one)
+        CELLS = args.cells
+        args.gpu_equil = True
     world, rank, local = dist_env()
     group = Group(world)
     import moleculardynamics_b200 as md
@@ -1388,6 +1395,9 @@ def main():
     ap.add_argument("--equil", type=int, default=2000,
                     help="BAOAB steps on the GPU when the reference-equilibrated state is "
                          "absent or --gpu-equil is given")
+    ap.add_argument("--cells", type=int, default=CELLS,
+                    help="fcc cells per side (profiling configurations only; the metric is "
+                         "quoted on 64)")
     ap.add_argument("--gpu-equil", action="store_true",
                     help="equilibrate on the GPU instead of loading the reference's state")
     ap.add_argument("--drift-steps", type=int, default=None,

@@ -139,6 +139,7 @@ def _load():
         "md_lj_set_unroll": (C.c_int, [C.c_int]),
         "md_lj_set_launch": (C.c_int, [_vp, C.c_int, C.c_int]),
         "md_lj_set_halo": (C.c_int, [_vp, C.c_int]),
+        "md_lj_set_tile_threads": (C.c_int, [_vp, C.c_int]),
         "md_thermo_csv_open": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                         C.c_int64, C.c_int64, C.POINTER(_vp)]),
         "md_thermo_csv_append": (C.c_int, [_vp, _vp, C.c_int64, _d, C.c_int64, C.c_int64,
@@ -547,6 +548,10 @@ class VerletList:
         """Neighbours per atom the rows hold; host builds grow it on overflow
         unless fixed.  The list must be built again."""
         _check(lib().md_verlet_set_capacity(self._h, int(capacity), 1 if fixed else 0))
+
+    def set_tile_threads(self, tpa: int):
+        """Threads per atom of the mixed tile kernel (2, 4 or 8; 0: the default)."""
+        _check(lib().md_lj_set_tile_threads(self._h, int(tpa)))
 
     def set_halo(self, on=True):
         """Keep halo tiles for the mixed-precision force kernel (built now and at

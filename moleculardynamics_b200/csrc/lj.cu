@@ -610,13 +610,11 @@ k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
 //   d = qi - qj (int32 wrap-around, the minimum image), r^2 = d.d exactly in 64
 //   bits, rounded once to FP32 -- the quantity whose precision sets the force error
 //   (r^-14); r^-2, r^-6, energy, virial and w / r^2 in FP32; the force vector in
-//   FP32 from d rounded to FP32, summed per thread in chunks of 2 kTileChunk pairs
-//   that are added with Kahan compensation, and combined over an atom's threads in
+//   FP32 from d rounded to FP32, summed per thread in chunks of kTilePairsPerAdd
+//   pairs that are added with Kahan compensation, and combined over an atom's threads in
 //   FP64.  Pairs within the cutoff band are settled exactly (near_tile_pairs), as
 //   in the gathered mixed kernel, so the mixed path sums the FP64 path's pairs.
-constexpr int kTileTPA = 4;                      // threads per atom
-constexpr int kTileThreads = kHaloAtoms * kTileTPA;
-constexpr int kTileChunk = 4;                    // row words (8 pairs) per Kahan add
+constexpr int kTilePairsPerAdd = 8;  // pairs a thread sums in FP32 before a Kahan add
 constexpr long long kTileWaitCycles = 2000000000LL;  // ~1 s bound on a tile's copies
 
 struct TileArgs {
@@ -695,6 +693,50 @@ __device__ __forceinline__ unsigned ldg_row_word(const unsigned* p, uint64_t pol
                  : "l"(p), "l"(policy));
     return v;
 }
+
+// A tile kernel with TPA threads per atom reads each 8-entry chunk of a row as TPA
+// words of 8 / TPA 16-bit slots: thread g takes entries 8c + (8 / TPA) g + e.
+template <int TPA>
+struct TileRow;
+template <>
+struct TileRow<2> {
+    static constexpr int EPT = 4;
+    using W = uint2;
+    static __device__ __forceinline__ W load(const uint16_t* row, int c, int g, uint64_t pol) {
+        uint2 v;
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                     : "=r"(v.x), "=r"(v.y)
+                     : "l"(reinterpret_cast<const uint2*>(row) + 2 * c + g), "l"(pol));
+        return v;
+    }
+    static __device__ __forceinline__ unsigned slot(const W& w, int e) {
+        return ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffffu;
+    }
+};
+template <>
+struct TileRow<4> {
+    static constexpr int EPT = 2;
+    using W = unsigned;
+    static __device__ __forceinline__ W load(const uint16_t* row, int c, int g, uint64_t pol) {
+        return ldg_row_word(reinterpret_cast<const unsigned*>(row) + 4 * c + g, pol);
+    }
+    static __device__ __forceinline__ unsigned slot(const W& w, int e) {
+        return (w >> (16 * e)) & 0xffffu;
+    }
+};
+template <>
+struct TileRow<8> {
+    static constexpr int EPT = 1;
+    using W = unsigned;
+    static __device__ __forceinline__ W load(const uint16_t* row, int c, int g, uint64_t pol) {
+        unsigned short v;
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;"
+                     : "=h"(v)
+                     : "l"(row + 8 * c + g), "l"(pol));
+        return v;
+    }
+    static __device__ __forceinline__ unsigned slot(const W& w, int) { return w; }
+};
 
 // Warp 0 of the CTA queues the halo of tile t into `dst`: one bulk copy per run
 // (lane r takes run r), then lane 0 arrives on `bar` expecting the bytes.  A tile
@@ -793,20 +835,20 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
 // arithmetic on the FP64 positions, added with the main loop's arithmetic into
 // acc = {fx, fy, fz, e, w}.  The slot of an entry maps to its atom through the
 // tile's runs (read from global).
-template <bool LFS, int RM>
+template <bool LFS, int RM, int TPA>
 __device__ __noinline__ void near_tile_pairs(const TileArgs* ap, const Box3* boxp,
-                                             const double4* pd, const unsigned* row, int cnt,
+                                             const double4* pd, const uint16_t* row, int cnt,
                                              int g, int ii, int4 pi, const char* tile,
                                              const int2* runs, int nr, float* acc) {
+    constexpr int EPT = TileRow<TPA>::EPT;
     const TileArgs a = *ap;
     const Fold3 f3 = fold3_of(*boxp);
     for (int c = 0; 8 * c < cnt; ++c) {
-        const unsigned word = row[4 * c + g];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int k = 8 * c + 2 * g + h;
+        for (int e = 0; e < EPT; ++e) {
+            const int k = 8 * c + EPT * g + e;
             if (k >= cnt) continue;
-            const unsigned off = h ? (word >> 16) : (word & 0xffffu);
+            const unsigned off = row[k];
             const int4 qj = *reinterpret_cast<const int4*>(tile + off);
             const int dx = wrap_diff(pi.x, qj.x), dy = wrap_diff(pi.y, qj.y), dz = wrap_diff(pi.z, qj.z);
             const float r2 = r2_units<RM>(dx, dy, dz);
@@ -835,8 +877,8 @@ __device__ __noinline__ void near_tile_pairs(const TileArgs* ap, const Box3* box
     }
 }
 
-template <bool LFS, int RM>
-__global__ void __launch_bounds__(kTileThreads, 2)
+template <bool LFS, int RM, int TPA>
+__global__ void __launch_bounds__(kHaloAtoms * TPA, TPA == 8 ? 1 : 2)
 k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int* __restrict__ nbr,
           const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride, int64_t n,
           int ntiles, const int2* __restrict__ runs, const int2* __restrict__ meta,
@@ -847,7 +889,9 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
     extern __shared__ __align__(128) int4 s_buf[];  // 2 x kHaloCap slots
     __shared__ uint64_t s_bar[2];
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int g = tid & (kTileTPA - 1);
+    const int g = tid & (TPA - 1);
+    using R = TileRow<TPA>;
+    constexpr int EPT = R::EPT, WPA = kTilePairsPerAdd / EPT;
     const uint64_t pol_q = l2_evict_last_policy(), pol_row = l2_evict_first_policy();
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
@@ -876,7 +920,7 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
             timed_out = true;  // the copies never landed: flag it and stop using the buffers
             break;
         }
-        const int64_t i = static_cast<int64_t>(t) * kHaloAtoms + (tid / kTileTPA);
+        const int64_t i = static_cast<int64_t>(t) * kHaloAtoms + (tid / TPA);
         float fs[3] = {0.f, 0.f, 0.f}, fk[3] = {0.f, 0.f, 0.f};  // Kahan sums, force units
         float e = 0.f, vir = 0.f;
         double gx = 0.0, gy = 0.0, gz = 0.0;  // gathered rows (tiles that are not staged)
@@ -884,28 +928,28 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
             const int4 pi = __ldg(q + i);
             const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
             if (m.x > 0) {
-                // row i as 16-bit slot byte offsets; thread g takes entries 8c + 2g and
-                // 8c + 2g + 1 of each 8-entry chunk c (one 32-bit word)
-                const unsigned* row = reinterpret_cast<const unsigned*>(nbr16 + i * stride);
+                // row i as 16-bit slot byte offsets; thread g takes EPT consecutive
+                // entries of each 8-entry chunk c (one word)
+                const uint16_t* row = nbr16 + i * stride;
                 const char* tile = reinterpret_cast<const char*>(buf);
                 const int nch = (cnt + 7) >> 3;
                 bool near = false;
-                unsigned word = nch > 0 ? ldg_row_word(row + g, pol_row) : 0u;
-                for (int c0 = 0; c0 < nch; c0 += kTileChunk) {
+                typename R::W word = nch > 0 ? R::load(row, 0, g, pol_row) : typename R::W{};
+                for (int c0 = 0; c0 < nch; c0 += WPA) {
                     float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
-                    for (int u = 0; u < kTileChunk; ++u) {
+                    for (int u = 0; u < WPA; ++u) {
                         const int c = c0 + u;
-                        const unsigned cur = word;
-                        if (c + 1 < nch) word = ldg_row_word(row + 4 * (c + 1) + g, pol_row);
-                        const int k0 = 8 * c + 2 * g;
-                        const bool v0 = c < nch && k0 < cnt, v1 = c < nch && k0 + 1 < cnt;
-                        const unsigned o0 = v0 ? (cur & 0xffffu) : 0u;
-                        const unsigned o1 = v1 ? (cur >> 16) : 0u;
-                        const int4 q0 = *reinterpret_cast<const int4*>(tile + o0);
-                        const int4 q1 = *reinterpret_cast<const int4*>(tile + o1);
-                        pair_tile<LFS, RM>(a, pi, q0, v0, cx, cy, cz, e, vir, near);
-                        pair_tile<LFS, RM>(a, pi, q1, v1, cx, cy, cz, e, vir, near);
+                        const typename R::W cur = word;
+                        if (c + 1 < nch) word = R::load(row, c + 1, g, pol_row);
+#pragma unroll
+                        for (int h = 0; h < EPT; ++h) {
+                            const int kk = 8 * c + EPT * g + h;
+                            const bool valid = c < nch && kk < cnt;
+                            const unsigned off = valid ? R::slot(cur, h) : 0u;
+                            const int4 qj = *reinterpret_cast<const int4*>(tile + off);
+                            pair_tile<LFS, RM>(a, pi, qj, valid, cx, cy, cz, e, vir, near);
+                        }
                     }
                     kahan_add(fs[0], fk[0], cx);
                     kahan_add(fs[1], fk[1], cy);
@@ -913,7 +957,7 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
                 }
                 if (near) {  // rare: settle the pairs next to the cutoff
                     float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-                    near_tile_pairs<LFS, RM>(&a, &box, pd, row, cnt, g, static_cast<int>(i), pi,
+                    near_tile_pairs<LFS, RM, TPA>(&a, &box, pd, row, cnt, g, static_cast<int>(i), pi,
                                              tile, runs + static_cast<int64_t>(t) * kHaloRuns,
                                              m.x, acc);
                     kahan_add(fs[0], fk[0], acc[0]);
@@ -923,7 +967,7 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
                     vir += acc[4];
                 }
             } else {
-                const PairSums ps = gathered_row<LFS, true, 2, kTileTPA>(
+                const PairSums ps = gathered_row<LFS, true, 2, TPA>(
                     ga, box, pd, q, nbr + i * stride, cnt, g, static_cast<int>(i), pi);
                 gx = ps.fx;
                 gy = ps.fy;
@@ -937,7 +981,7 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
         double fy = (static_cast<double>(fs[1]) - static_cast<double>(fk[1])) * a.inv_scale + gy;
         double fz = (static_cast<double>(fs[2]) - static_cast<double>(fk[2])) * a.inv_scale + gz;
 #pragma unroll
-        for (int o = kTileTPA / 2; o > 0; o >>= 1) {
+        for (int o = TPA / 2; o > 0; o >>= 1) {
             fx += __shfl_xor_sync(0xffffffffu, fx, o);
             fy += __shfl_xor_sync(0xffffffffu, fy, o);
             fz += __shfl_xor_sync(0xffffffffu, fz, o);
@@ -1122,25 +1166,44 @@ TileArgs tile_args(const LJArgs& a) {
     return t;
 }
 
-template <bool LFS>
-void launch_tile(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
-                 double* out) {
+template <bool LFS, int RM, int TPA>
+void launch_tile_k(md_system* sys, md_verlet* v, const LJArgs& a, const TileArgs& t,
+                   double* part, unsigned* ticket, double* out) {
     const int ntiles = static_cast<int>(halo_blocks(sys->n));
-    const TileArgs t = tile_args(a);
-    auto kernel = t.rm ? k_lj_tile<LFS, 1> : k_lj_tile<LFS, 0>;
+    auto kernel = k_lj_tile<LFS, RM, TPA>;
     const size_t smem = 2 * kHaloCap * sizeof(int4);
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[t.rm]) {
+    static bool attr_set = false;
+    if (!attr_set) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
-        attr_set[t.rm] = true;
+        attr_set = true;
     }
-    const int grid = std::max(1, std::min(ntiles, 2 * sys->ctx->sm_count));
-    kernel<<<grid, kTileThreads, smem, sys->ctx->stream>>>(
+    const int per_sm = TPA == 8 ? 1 : 2;
+    const int grid = std::max(1, std::min(ntiles, per_sm * sys->ctx->sm_count));
+    kernel<<<grid, kHaloAtoms * TPA, smem, sys->ctx->stream>>>(
         sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
         v->count.as<int>(), v->stride, sys->n, ntiles, v->halo_runs.as<int2>(),
         v->halo_meta.as<int2>(), box_of(sys), a, t, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
         ticket, out, sys->ctx->d_status);
+}
+
+template <bool LFS, int TPA>
+void launch_tile_rm(md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                    unsigned* ticket, double* out) {
+    const TileArgs t = tile_args(a);
+    if (t.rm) launch_tile_k<LFS, 1, TPA>(sys, v, a, t, part, ticket, out);
+    else launch_tile_k<LFS, 0, TPA>(sys, v, a, t, part, ticket, out);
+}
+
+// tpa: threads per atom of the tile kernel (the tile shape: 2, 4 or 8; 0 = 4).
+template <bool LFS>
+void launch_tile(int tpa, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                 unsigned* ticket, double* out) {
+    switch (tpa) {
+        case 2: launch_tile_rm<LFS, 2>(sys, v, a, part, ticket, out); break;
+        case 8: launch_tile_rm<LFS, 8>(sys, v, a, part, ticket, out); break;
+        default: launch_tile_rm<LFS, 4>(sys, v, a, part, ticket, out); break;
+    }
 }
 
 template <bool LFS>
@@ -1232,8 +1295,8 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
     if (halo && cubic) {
-        if (lfs) launch_tile<true>(sys, v, a, part, ticket, out);
-        else launch_tile<false>(sys, v, a, part, ticket, out);
+        if (lfs) launch_tile<true>(lj->tile_tpa, sys, v, a, part, ticket, out);
+        else launch_tile<false>(lj->tile_tpa, sys, v, a, part, ticket, out);
     } else if (halo) {
         if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out);
         else launch_halo_u<false>(unroll, sys, v, a, part, ticket, out);
@@ -1540,6 +1603,14 @@ int md_lj_set_launch(md_lj* lj, int tpa, int unroll) {
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_launch: unroll %d not in {0,1,2,4}", unroll);
     lj->tpa = tpa;
     lj->unroll = unroll;
+    return MD_OK;
+}
+
+int md_lj_set_tile_threads(md_lj* lj, int tpa) {
+    graph_epoch_bump();
+    if (!lj || (tpa != 0 && tpa != 2 && tpa != 4 && tpa != 8))
+        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_tile_threads: threads per atom must be 0, 2, 4 or 8");
+    lj->tile_tpa = tpa;
     return MD_OK;
 }
 
