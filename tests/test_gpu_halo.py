@@ -116,6 +116,24 @@ def test_cubic_two_phase_box_mixes_staged_and_gathered_tiles(md):
     check_budget(ref, gathered, tiled)
 
 
+@pytest.mark.parametrize("tpa", [2, 8])
+def test_tile_shapes_within_budget(md, tpa):
+    """Every tile shape (threads per atom of the tile kernel) sums the same pairs:
+    within the error budget of FP64 and of the default shape, and deterministic."""
+    s, v, _ = melt(md, 12, 0.8442, 10)
+    ref, gathered, tiled = three_ways(md, s, v)
+    lj = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+    lj.set_tile_threads(tpa)
+    e, w = lj.compute_forces(s, v)
+    f = s.forces
+    e2, w2 = lj.compute_forces(s, v)
+    assert np.array_equal(s.forces, f) and e2 == e and w2 == w
+    check_budget(ref, gathered, (e, w, f))
+    assert rms_rel(f, tiled[2]) < 1e-6
+    with pytest.raises(md.InvalidArgument):
+        lj.set_tile_threads(3)
+
+
 def test_fused_run_with_rebuilds_replays_host_steps(md):
     s, v, st = melt(md, 10, 0.8442, 6, steps=50)
     x, vel = s.positions, s.velocities
