@@ -13,6 +13,7 @@ segment from the same state for each candidate.  `tune_cell_width` does the same
 for the width of the cells the list is built from (the reference bins at the
 list cutoff; wider cells give the same pairs from more candidates per atom and
 fewer, fuller cells, which also reshapes the halo tiles of the mixed kernel).
+`tune_tile_shape` times the mixed tile kernel over its threads per atom.
 
 Cache: $MOLDYN_B200_TUNE_CACHE, else ~/.cache/moleculardynamics_b200/autotune.json.
 """
@@ -120,6 +121,23 @@ def tune_skin(box, pos, vel, mass, lj, make_integrator, skins=(0.2, 0.3, 0.4, 0.
     return min(times, key=times.get), times
 
 
+TILE_SHAPES = (2, 4, 8)
+
+
+def tune_tile_shape(sys, lj, verlet, shapes=TILE_SHAPES, repeats=5):
+    """The fastest threads-per-atom of the mixed tile kernel (the tile shape) for a
+    list that keeps halo tiles; applies it and returns (best, {tpa: ms})."""
+    ctx = sys.ctx
+    verlet.set_halo(True)
+    timings = {}
+    for tpa in shapes:
+        lj.set_tile_threads(tpa)
+        timings[tpa] = time_force_kernel(ctx, sys, lj, verlet, repeats)
+    best = min(timings, key=timings.get)
+    lj.set_tile_threads(best)
+    return best, timings
+
+
 def tune_cell_width(box, pos, vel, mass, lj, skin, make_integrator,
                     factors=(1.0, 1.1, 1.25, 1.5), steps=100, ctx=None):
     """The cell width (a factor of the list cutoff rc + skin) with the shortest
@@ -150,4 +168,4 @@ def tune_cell_width(box, pos, vel, mass, lj, skin, make_integrator,
 
 
 __all__ = ["SHAPES", "cache_path", "problem_key", "time_force_kernel", "tune_force_kernel",
-           "tune_skin", "tune_cell_width"]
+           "tune_skin", "tune_cell_width", "TILE_SHAPES", "tune_tile_shape"]

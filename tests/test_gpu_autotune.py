@@ -66,3 +66,13 @@ def test_cell_width_keeps_the_pair_set_and_forces(md):
                                     lambda: md.VelocityVerlet(0.005), factors=(1.0, 1.2),
                                     steps=20)
     assert best in times and times[best] == min(times.values()) and len(times) == 2
+
+
+def test_tune_tile_shape_applies_the_fastest(md):
+    st = md.fcc_lattice(12, 0.8442, 0.722, 6)
+    s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"])
+    v = md.VerletList(st["box"], 2.5, 0.3)
+    v.build(s)
+    lj = md.LennardJones(1.0, 1.0, 2.5, precision=md.PRECISION_MIXED)
+    best, times = T.tune_tile_shape(s, lj, v, repeats=2)
+    assert best in T.TILE_SHAPES and times[best] == min(times.values())
