@@ -549,10 +549,6 @@ class VerletList:
         unless fixed.  The list must be built again."""
         _check(lib().md_verlet_set_capacity(self._h, int(capacity), 1 if fixed else 0))
 
-    def set_tile_threads(self, tpa: int):
-        """Threads per atom of the mixed tile kernel (2, 4 or 8; 0: the default)."""
-        _check(lib().md_lj_set_tile_threads(self._h, int(tpa)))
-
     def set_halo(self, on=True):
         """Keep halo tiles for the mixed-precision force kernel (built now and at
         every rebuild), or drop them.  Fused runs of large systems turn them on."""
@@ -616,6 +612,10 @@ class LennardJones:
         """Threads per atom and gathers in flight of this object's Verlet force
         kernel (0 = library default); see moleculardynamics_b200.autotune."""
         _check(lib().md_lj_set_launch(self._h, int(tpa), int(unroll)))
+
+    def set_tile_threads(self, tpa: int):
+        """Threads per atom of the mixed tile kernel (2, 4 or 8; 0: the default)."""
+        _check(lib().md_lj_set_tile_threads(self._h, int(tpa)))
 
     def set_halo(self, on=True):
         """Mixed precision: read neighbours through shared-memory halo tiles (the

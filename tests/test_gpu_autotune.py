@@ -45,7 +45,7 @@ def test_cell_width_keeps_the_pair_set_and_forces(md):
     pos -= st["box"] * np.floor(pos / st["box"] + 0.5)
     box = st["box"]
     out = []
-    for factor in (0.0, 1.1, 1.3):
+    for factor in (0.0, 1.25, 1.6):
         s = md.System.from_arrays(pos, box)
         v = md.VerletList(box, 2.5, 0.3)
         if factor:
@@ -53,7 +53,8 @@ def test_cell_width_keeps_the_pair_set_and_forces(md):
         v.build(s)
         e, w = md.LennardJones(1.0, 1.0, 2.5).compute_forces(s, v)
         out.append((v.cells_per_side(), v.pairs(), e, w, s.forces))
-    assert out[0][0] == (6, 6, 6) and out[1][0] == (5, 5, 5) and out[2][0] == (4, 4, 4)
+    # L = 16.79: 5 cells of the list cutoff 2.8 per side, 4 of 3.5, 3 of 4.48
+    assert out[0][0] == (5, 5, 5) and out[1][0] == (4, 4, 4) and out[2][0] == (3, 3, 3)
     for cells, pairs, e, w, f in out[1:]:
         assert np.array_equal(pairs, out[0][1])
         assert abs(e - out[0][2]) < 1e-12 * abs(out[0][2])
