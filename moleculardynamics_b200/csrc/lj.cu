@@ -600,32 +600,21 @@ k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
 // ------------------------------------------------------------ k_lj_tile
 // Mixed-precision forces over halo tiles, persistent and double-buffered (cubic
 // boxes).  Each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...: while
-// it computes one tile from one shared-memory buffer, the bulk-copy engine fills
-// the other with the next tile's halo -- one 1-D cp.async.bulk per run of cells,
-// completing on the buffer's mbarrier -- so no thread stages data or waits at a
-// staging barrier.  The source is this GPU's own fixed-point position array; no
-// copy is multicast.
+// its warps compute one tile from one shared-memory buffer, the bulk-copy engine
+// fills the other with the next tile's halo -- one 1-D cp.async.bulk per run of
+// cells, completing on the buffer's mbarrier.  The loop has no CTA-wide barrier:
+// each warp finishes a tile on its own, and the last warp to finish one queues
+// the copies of the tile after next into the buffer it frees.  The source is this
+// GPU's own fixed-point position array; no copy is multicast.
 //
-// Pair arithmetic, in integer units of the fixed-point grid (res = L / 2^32):
-//   d = qi - qj (int32 wrap-around, the minimum image), r^2 = d.d exactly in 64
-//   bits, rounded once to FP32 -- the quantity whose precision sets the force error
-//   (r^-14); r^-2, r^-6, energy, virial and w / r^2 in FP32; the force vector in
-//   FP32 from d rounded to FP32, summed per thread in chunks of kTilePairsPerAdd
-//   pairs that are added with Kahan compensation, and combined over an atom's threads in
-//   FP64.  Pairs within the cutoff band are settled exactly (near_tile_pairs), as
-//   in the gathered mixed kernel, so the mixed path sums the FP64 path's pairs.
-constexpr int kTilePairsPerAdd = 8;  // pairs a thread sums in FP32 before a Kahan add
+// Per list entry: one 16-bit slot read out of a row word, one shared-memory load,
+// and the arithmetic of the gathered mixed kernel (pair_mixed): the exact integer
+// displacement as FP64, r^2 formed in FP64 and rounded to FP32 once, FP32 pair
+// terms, the force vector accumulated in FP64.  Rows of staged tiles are padded to
+// whole 8-entry chunks with the atom's own slot (r^2 = 0, skipped), so entries are
+// read without a count test.  Pairs within the cutoff band are settled by the
+// reference arithmetic on the FP64 positions, as in the gathered kernel.
 constexpr long long kTileWaitCycles = 2000000000LL;  // ~1 s bound on a tile's copies
-
-struct TileArgs {
-    float sig2u;          // sigma^2 in r^2 units
-    float lo, hi;         // band around rc^2 in r^2 units (decided exactly inside)
-    float four_eps, tf_eps;
-    float ucf, dudr_u, rc_dudr;  // LFS: u(rc); length per sqrt(unit) * du/dr(rc); rc du/dr(rc)
-    double inv_scale;     // force units -> force
-    double rc2;           // the exact cutoff test of pairs inside the band
-    int rm;               // 1: r^2 converted by parts (interacting pairs have r^2 < 2^55 units)
-};
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -654,13 +643,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-// Waits for the phase of `bar` with the given parity; false after ~1 s.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-    if (mbar_try_wait(bar, parity)) return true;
+// Every lane of the warp waits for the phase of `bar` with the given parity (each
+// then sees the copied data); the warp gives up together after ~1 s.
+__device__ __forceinline__ bool warp_wait_bounded(uint64_t* bar, unsigned parity) {
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kTileWaitCycles) return false;
-    return true;
+    for (;;) {
+        if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+        const long long el = __shfl_sync(0xffffffffu, clock64() - t0, 0);
+        if (el > kTileWaitCycles) return false;
+    }
 }
 
 __device__ __forceinline__ uint64_t l2_evict_last_policy() {
@@ -684,14 +676,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
         "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
         "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
-}
-
-__device__ __forceinline__ unsigned ldg_row_word(const unsigned* p, uint64_t policy) {
-    unsigned v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
-                 : "=r"(v)
-                 : "l"(p), "l"(policy));
-    return v;
 }
 
 // A tile kernel with TPA threads per atom reads each 8-entry chunk of a row as TPA
@@ -718,7 +702,11 @@ struct TileRow<4> {
     static constexpr int EPT = 2;
     using W = unsigned;
     static __device__ __forceinline__ W load(const uint16_t* row, int c, int g, uint64_t pol) {
-        return ldg_row_word(reinterpret_cast<const unsigned*>(row) + 4 * c + g, pol);
+        unsigned v;
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+                     : "=r"(v)
+                     : "l"(reinterpret_cast<const unsigned*>(row) + 4 * c + g), "l"(pol));
+        return v;
     }
     static __device__ __forceinline__ unsigned slot(const W& w, int e) {
         return (w >> (16 * e)) & 0xffffu;
@@ -738,9 +726,9 @@ struct TileRow<8> {
     static __device__ __forceinline__ unsigned slot(const W& w, int) { return w; }
 };
 
-// Warp 0 of the CTA queues the halo of tile t into `dst`: one bulk copy per run
-// (lane r takes run r), then lane 0 arrives on `bar` expecting the bytes.  A tile
-// that is not staged arrives with none, so every tile completes one phase.
+// One warp queues the halo of tile t into `dst`: one bulk copy per run (lane r
+// takes run r), then lane 0 arrives on `bar` expecting the bytes.  A tile that is
+// not staged arrives with none, so every tile completes one phase.
 __device__ __forceinline__ void tile_issue(int t, int4* dst, uint64_t* bar, const int4* q,
                                            const int2* __restrict__ runs,
                                            const int2* __restrict__ meta, uint64_t policy) {
@@ -763,223 +751,148 @@ __device__ __forceinline__ void tile_issue(int t, int4* dst, uint64_t* bar, cons
     if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
 }
 
-// r^2 of an integer displacement, rounded once to FP32, in units res^2 (RM 0) or
-// 2^9 res^2 (RM 1: the 64-bit sum split into its high word and its low word shifted
-// by 9, both exact in FP32, joined by one fused multiply-add).  Each square is at
-// most 2^62, so three fit an unsigned 64-bit word.  With RM the high word
-// saturates below 2^23, which puts any entry that far apart (a stale list)
-// beyond the cutoff.
-template <int RM>
-__device__ __forceinline__ float r2_units(int dx, int dy, int dz) {
-    unsigned long long r2 = static_cast<unsigned long long>(static_cast<long long>(dx) * dx);
-    r2 += static_cast<unsigned long long>(static_cast<long long>(dy) * dy);
-    r2 += static_cast<unsigned long long>(static_cast<long long>(dz) * dz);
-    if constexpr (RM == 0) {
-        return __ull2float_rn(r2);
-    } else {
-        const unsigned hi = min(static_cast<unsigned>(r2 >> 32), 0x7FFFFFu);
-        const unsigned lo = static_cast<unsigned>(r2) >> 9;
-        const float fh = __int_as_float(0x4B000000 | hi) - 8388608.0f;
-        const float fl = __int_as_float(0x4B000000 | lo) - 8388608.0f;
-        return fmaf(fh, 8388608.0f, fl);
-    }
-}
-
-// The FP32 pair terms of r^2 (units): energy u, virial w and w / r^2.
+// One staged entry (pair_mixed's arithmetic, cubic box); r^2 = 0 is the row's
+// padding (the atom itself) and contributes nothing.
 template <bool LFS>
-__device__ __forceinline__ void terms_tile(const TileArgs& a, float r2, float& u, float& w,
-                                           float& sf) {
-    const float inv = rcp_approx(r2);
-    const float s2 = a.sig2u * inv;
+__device__ __forceinline__ void pair_tile(const LJArgs& a, int4 qi, int4 qj, double& fx,
+                                          double& fy, double& fz, float& e, float& vir,
+                                          bool& near) {
+    const double dx = diff_to_double(qi.x, qj.x);
+    const double dy = diff_to_double(qi.y, qj.y);
+    const double dz = diff_to_double(qi.z, qj.z);
+    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx)) * a.res2;
+    const bool in_range = r2 < a.rc2_hi;
+    const bool in_band = r2 > a.rc2_lo;
+    near = near || (in_range && in_band);
+    const bool take = in_range && !in_band && r2 > 0.0;
+    const float r2f = static_cast<float>(r2);
+    const float inv = rcp_approx(r2f);
+    const float s2 = a.sig2f * inv;
     const float s6 = s2 * s2 * s2;
     const float t6 = fmaf(s6, s6, -s6);
-    u = a.four_eps * t6;
-    w = a.tf_eps * fmaf(s6, s6, t6);
+    float u = a.four_epsf * t6;
+    float w = a.tf_epsf * fmaf(s6, s6, t6);
     if (LFS) {
-        const float r = sqrtf(r2);
-        u = u - a.ucf - fmaf(r, a.dudr_u, -a.rc_dudr);
-        w = fmaf(r, a.dudr_u, w);
+        const float r = sqrtf(r2f);
+        u = u - a.ucf - (r - a.rcf) * a.dudrcf;
+        w = w + r * a.dudrcf;
     }
-    sf = w * inv;
-}
-
-// One list entry of the tile kernel (branch-free; invalid entries contribute 0).
-template <bool LFS, int RM>
-__device__ __forceinline__ void pair_tile(const TileArgs& a, int4 qi, int4 qj, bool valid,
-                                          float& fx, float& fy, float& fz, float& e, float& vir,
-                                          bool& near) {
-    const int dx = wrap_diff(qi.x, qj.x), dy = wrap_diff(qi.y, qj.y), dz = wrap_diff(qi.z, qj.z);
-    const float r2 = r2_units<RM>(dx, dy, dz);
-    const bool in_range = valid && r2 < a.hi;
-    const bool in_band = r2 > a.lo;
-    near = near || (in_range && in_band);
-    const bool take = in_range && !in_band;
-    float u, w, sf;
-    terms_tile<LFS>(a, r2, u, w, sf);
-    sf = take ? sf : 0.0f;
-    e += take ? u : 0.0f;
-    vir += take ? w : 0.0f;
-    fx = fmaf(__int2float_rn(dx), sf, fx);
-    fy = fmaf(__int2float_rn(dy), sf, fy);
-    fz = fmaf(__int2float_rn(dz), sf, fz);
-}
-
-__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
-    const float y = x - c;
-    const float t = s + y;
-    c = (t - s) - y;
-    s = t;
-}
-
-// The pairs of a staged row next to the cutoff (rare): decided by the reference
-// arithmetic on the FP64 positions, added with the main loop's arithmetic into
-// acc = {fx, fy, fz, e, w}.  The slot of an entry maps to its atom through the
-// tile's runs (read from global).
-template <bool LFS, int RM, int TPA>
-__device__ __noinline__ void near_tile_pairs(const TileArgs* ap, const Box3* boxp,
-                                             const double4* pd, const uint16_t* row, int cnt,
-                                             int g, int ii, int4 pi, const char* tile,
-                                             const int2* runs, int nr, float* acc) {
-    constexpr int EPT = TileRow<TPA>::EPT;
-    const TileArgs a = *ap;
-    const Fold3 f3 = fold3_of(*boxp);
-    for (int c = 0; 8 * c < cnt; ++c) {
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const int k = 8 * c + EPT * g + e;
-            if (k >= cnt) continue;
-            const unsigned off = row[k];
-            const int4 qj = *reinterpret_cast<const int4*>(tile + off);
-            const int dx = wrap_diff(pi.x, qj.x), dy = wrap_diff(pi.y, qj.y), dz = wrap_diff(pi.z, qj.z);
-            const float r2 = r2_units<RM>(dx, dy, dz);
-            if (!(r2 < a.hi) || !(r2 > a.lo)) continue;
-            const int sl = static_cast<int>(off >> 4);
-            int lo = 0, hi = nr;  // the last run whose first slot is <= sl
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (runs[mid].y <= sl) lo = mid;
-                else hi = mid;
-            }
-            const int j = runs[lo].x + (sl - runs[lo].y);
-            const double4 p = ldg4(pd + ii), q2 = ldg4(pd + j);
-            double ex, ey, ez;
-            if (p.w < q2.w) min_image_wrapped(f3, p.x, p.y, p.z, q2.x, q2.y, q2.z, ex, ey, ez);
-            else min_image_wrapped(f3, q2.x, q2.y, q2.z, p.x, p.y, p.z, ex, ey, ez);
-            if (!(norm2_exact(ex, ey, ez) < a.rc2)) continue;
-            float u, w, sf;
-            terms_tile<LFS>(a, r2, u, w, sf);
-            acc[0] = fmaf(__int2float_rn(dx), sf, acc[0]);
-            acc[1] = fmaf(__int2float_rn(dy), sf, acc[1]);
-            acc[2] = fmaf(__int2float_rn(dz), sf, acc[2]);
-            acc[3] += u;
-            acc[4] += w;
-        }
+    float sf = 0.f;
+    if (take) {
+        sf = w * inv;
+        e += u;
+        vir += w;
     }
+    const double sd = static_cast<double>(sf) * a.res[0];
+    fx = fma(dx, sd, fx);
+    fy = fma(dy, sd, fy);
+    fz = fma(dz, sd, fz);
 }
 
-template <bool LFS, int RM, int TPA>
+template <bool LFS, int TPA>
 __global__ void __launch_bounds__(kHaloAtoms * TPA, TPA == 8 ? 1 : 2)
 k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int* __restrict__ nbr,
           const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride, int64_t n,
           int ntiles, const int2* __restrict__ runs, const int2* __restrict__ meta,
-          const __grid_constant__ Box3 box, const __grid_constant__ LJArgs ga,
-          const __grid_constant__ TileArgs a, double* __restrict__ fxo, double* __restrict__ fyo,
-          double* __restrict__ fzo, double* part, unsigned* ticket, double* out,
-          uint32_t* status) {
+          const __grid_constant__ Box3 box, const __grid_constant__ LJArgs a,
+          double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
+          double* part, unsigned* ticket, double* out, uint32_t* status) {
+    using R = TileRow<TPA>;
+    constexpr int EPT = R::EPT;
+    constexpr int kWarps = kHaloAtoms * TPA / 32;
     extern __shared__ __align__(128) int4 s_buf[];  // 2 x kHaloCap slots
     __shared__ uint64_t s_bar[2];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ int s_done[2];  // warps finished with each buffer's current tile
+    const int tid = threadIdx.x, lane = tid & 31;
     const int g = tid & (TPA - 1);
-    using R = TileRow<TPA>;
-    constexpr int EPT = R::EPT, WPA = kTilePairsPerAdd / EPT;
     const uint64_t pol_q = l2_evict_last_policy(), pol_row = l2_evict_first_policy();
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
+        s_done[0] = s_done[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     const int stride_t = static_cast<int>(gridDim.x);
-    if (warp == 0) {
+    if (tid < 32) {
         if (static_cast<int>(blockIdx.x) < ntiles)
             tile_issue(blockIdx.x, s_buf, &s_bar[0], q, runs, meta, pol_q);
         if (static_cast<int>(blockIdx.x) + stride_t < ntiles)
             tile_issue(blockIdx.x + stride_t, s_buf + kHaloCap, &s_bar[1], q, runs, meta, pol_q);
     }
+    const Fold3 f3 = fold3_of(box);
     double e_tot = 0.0, w_tot = 0.0;
     bool timed_out = false;
     int k = 0;
     for (int t = blockIdx.x; t < ntiles; t += stride_t, ++k) {
         const int b = k & 1;
         int4* buf = s_buf + b * kHaloCap;
-        const int2 m = meta[t];
-        // every thread waits (each then sees the copied data); the decision to give up
-        // is taken by the whole CTA, so that no thread leaves the loop alone
-        const bool landed = mbar_wait_bounded(&s_bar[b], static_cast<unsigned>((k >> 1) & 1));
-        if (__syncthreads_or(!landed)) {
-            timed_out = true;  // the copies never landed: flag it and stop using the buffers
+        if (!warp_wait_bounded(&s_bar[b], static_cast<unsigned>((k >> 1) & 1))) {
+            timed_out = true;  // the copies never landed: flag it and leave the loop
             break;
         }
+        const int2 m = meta[t];
         const int64_t i = static_cast<int64_t>(t) * kHaloAtoms + (tid / TPA);
-        float fs[3] = {0.f, 0.f, 0.f}, fk[3] = {0.f, 0.f, 0.f};  // Kahan sums, force units
+        const int ii = static_cast<int>(i);
+        double fx = 0.0, fy = 0.0, fz = 0.0;
         float e = 0.f, vir = 0.f;
-        double gx = 0.0, gy = 0.0, gz = 0.0;  // gathered rows (tiles that are not staged)
         if (i < n) {
             const int4 pi = __ldg(q + i);
             const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
             if (m.x > 0) {
-                // row i as 16-bit slot byte offsets; thread g takes EPT consecutive
-                // entries of each 8-entry chunk c (one word)
                 const uint16_t* row = nbr16 + i * stride;
                 const char* tile = reinterpret_cast<const char*>(buf);
-                const int nch = (cnt + 7) >> 3;
+                const int nch = (cnt + 7) >> 3;  // whole chunks: the last one is padded
                 bool near = false;
                 typename R::W word = nch > 0 ? R::load(row, 0, g, pol_row) : typename R::W{};
-                for (int c0 = 0; c0 < nch; c0 += WPA) {
-                    float cx = 0.f, cy = 0.f, cz = 0.f;
+                for (int c = 0; c < nch; ++c) {
+                    const typename R::W cur = word;
+                    if (c + 1 < nch) word = R::load(row, c + 1, g, pol_row);
 #pragma unroll
-                    for (int u = 0; u < WPA; ++u) {
-                        const int c = c0 + u;
-                        const typename R::W cur = word;
-                        if (c + 1 < nch) word = R::load(row, c + 1, g, pol_row);
+                    for (int h = 0; h < EPT; ++h) {
+                        const int4 qj = *reinterpret_cast<const int4*>(tile + R::slot(cur, h));
+                        pair_tile<LFS>(a, pi, qj, fx, fy, fz, e, vir, near);
+                    }
+                }
+                if (near) {
+                    // rare: the pairs next to the cutoff, decided by the reference
+                    // arithmetic on the FP64 positions (the slot maps to its atom
+                    // through the tile's runs)
+                    const int2* tr = runs + static_cast<int64_t>(t) * kHaloRuns;
+                    for (int c = 0; c < nch; ++c) {
 #pragma unroll
                         for (int h = 0; h < EPT; ++h) {
                             const int kk = 8 * c + EPT * g + h;
-                            const bool valid = c < nch && kk < cnt;
-                            const unsigned off = valid ? R::slot(cur, h) : 0u;
-                            const int4 qj = *reinterpret_cast<const int4*>(tile + off);
-                            pair_tile<LFS, RM>(a, pi, qj, valid, cx, cy, cz, e, vir, near);
+                            if (kk >= cnt) continue;
+                            const unsigned off = row[kk];
+                            const int sl = static_cast<int>(off >> 4);
+                            int lo = 0, hi = m.x;  // the last run whose first slot is <= sl
+                            while (hi - lo > 1) {
+                                const int mid = (lo + hi) >> 1;
+                                if (tr[mid].y <= sl) lo = mid;
+                                else hi = mid;
+                            }
+                            near_pair<LFS>(a, f3, pd, ii, tr[lo].x + (sl - tr[lo].y), pi,
+                                           *reinterpret_cast<const int4*>(tile + off), fx, fy, fz,
+                                           e, vir);
                         }
                     }
-                    kahan_add(fs[0], fk[0], cx);
-                    kahan_add(fs[1], fk[1], cy);
-                    kahan_add(fs[2], fk[2], cz);
-                }
-                if (near) {  // rare: settle the pairs next to the cutoff
-                    float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-                    near_tile_pairs<LFS, RM, TPA>(&a, &box, pd, row, cnt, g, static_cast<int>(i), pi,
-                                             tile, runs + static_cast<int64_t>(t) * kHaloRuns,
-                                             m.x, acc);
-                    kahan_add(fs[0], fk[0], acc[0]);
-                    kahan_add(fs[1], fk[1], acc[1]);
-                    kahan_add(fs[2], fk[2], acc[2]);
-                    e += acc[3];
-                    vir += acc[4];
                 }
             } else {
-                const PairSums ps = gathered_row<LFS, true, 2, TPA>(
-                    ga, box, pd, q, nbr + i * stride, cnt, g, static_cast<int>(i), pi);
-                gx = ps.fx;
-                gy = ps.fy;
-                gz = ps.fz;
-                e = ps.e;
-                vir = ps.vir;
+                // a tile that is not staged: its int32 row, positions gathered
+                const int* row = nbr + i * stride;
+                bool near = false;
+                for (int kk = g; kk < cnt; kk += TPA)
+                    pair_mixed<LFS, true>(a, pi, __ldg(q + __ldg(row + kk)), fx, fy, fz, e, vir,
+                                          near);
+                if (near) {
+                    for (int kk = g; kk < cnt; kk += TPA) {
+                        const int j = __ldg(row + kk);
+                        near_pair<LFS>(a, f3, pd, ii, j, pi, __ldg(q + j), fx, fy, fz, e, vir);
+                    }
+                }
             }
         }
-        // the atom's threads combine in FP64; compensated sums enter with their error
-        double fx = (static_cast<double>(fs[0]) - static_cast<double>(fk[0])) * a.inv_scale + gx;
-        double fy = (static_cast<double>(fs[1]) - static_cast<double>(fk[1])) * a.inv_scale + gy;
-        double fz = (static_cast<double>(fs[2]) - static_cast<double>(fk[2])) * a.inv_scale + gz;
 #pragma unroll
         for (int o = TPA / 2; o > 0; o >>= 1) {
             fx += __shfl_xor_sync(0xffffffffu, fx, o);
@@ -993,18 +906,29 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
         }
         e_tot += 0.5 * static_cast<double>(e);  // every pair was taken from both sides
         w_tot += 0.5 * static_cast<double>(vir);
-        __syncthreads();  // every thread is done with this buffer
-        if (warp == 0 && t + 2 * stride_t < ntiles) {
+        // this warp is done with the buffer; the last warp to finish queues the
+        // tile after next into it
+        __syncwarp();
+        int done = 0;
+        if (lane == 0) {
+            __threadfence_block();
+            done = atomicAdd(&s_done[b], 1) + 1;
+        }
+        done = __shfl_sync(0xffffffffu, done, 0);
+        if (done == kWarps) {
+            if (lane == 0) s_done[b] = 0;
+            __threadfence_block();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tile_issue(t + 2 * stride_t, buf, &s_bar[b], q, runs, meta, pol_q);
+            if (t + 2 * stride_t < ntiles)
+                tile_issue(t + 2 * stride_t, buf, &s_bar[b], q, runs, meta, pol_q);
         }
     }
     if (timed_out) {
-        if (tid == 0) atomicOr(status, MD_STATUS_WAIT_TIMEOUT);
-        // before the CTA exits, give the copies still queued into its buffers a
-        // bounded time to land
-        mbar_wait_bounded(&s_bar[k & 1], static_cast<unsigned>((k >> 1) & 1));
-        mbar_wait_bounded(&s_bar[(k + 1) & 1], static_cast<unsigned>(((k + 1) >> 1) & 1));
+        if (lane == 0) atomicOr(status, MD_STATUS_WAIT_TIMEOUT);
+        // before the CTA exits, give the copies that may still be queued into its
+        // buffers a bounded time to land
+        warp_wait_bounded(&s_bar[k & 1], static_cast<unsigned>((k >> 1) & 1));
+        warp_wait_bounded(&s_bar[(k + 1) & 1], static_cast<unsigned>(((k + 1) >> 1) & 1));
     }
     double v[2] = {e_tot, w_tot};
     grid_reduce<2>(v, part, ticket, out);
@@ -1141,36 +1065,11 @@ void launch_halo(md_system* sys, md_verlet* v, const LJArgs& a, double* part, un
         box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
 }
 
-// Integer-unit constants of k_lj_tile for a cubic box.
-TileArgs tile_args(const LJArgs& a) {
-    TileArgs t;
-    const double res = a.res[0];
-    // Split conversion when every pair that can interact (r^2 within the cutoff band)
-    // has r^2 < 2^55 units; farther entries saturate beyond the cutoff.
-    const double rcu = 1.01 * a.rc / res;
-    t.rm = rcu * rcu < 36028797018963968.0 ? 1 : 0;
-    const double unit = t.rm ? res * res * 512.0 : res * res;  // r^2 unit
-    t.sig2u = static_cast<float>(a.sig2 / unit);
-    // the band must also cover the FP32 rounding of r^2 (two ulps of rc^2)
-    const double band = a.band + 2.0 * 5.9604644775390625e-08 * a.rc2;
-    t.lo = static_cast<float>((a.rc2 - band) / unit);
-    t.hi = static_cast<float>((a.rc2 + band) / unit);
-    t.four_eps = a.four_epsf;
-    t.tf_eps = a.tf_epsf;
-    t.ucf = a.ucf;
-    const double ru = t.rm ? res * 22.627416997969522 : res;  // length per sqrt(r^2 unit)
-    t.dudr_u = static_cast<float>(ru * a.dudrc);
-    t.rc_dudr = static_cast<float>(a.rc * a.dudrc);
-    t.inv_scale = (t.rm ? 1.0 / 512.0 : 1.0) / res;
-    t.rc2 = a.rc2;
-    return t;
-}
-
-template <bool LFS, int RM, int TPA>
-void launch_tile_k(md_system* sys, md_verlet* v, const LJArgs& a, const TileArgs& t,
-                   double* part, unsigned* ticket, double* out) {
+template <bool LFS, int TPA>
+void launch_tile_k(md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                   unsigned* ticket, double* out) {
     const int ntiles = static_cast<int>(halo_blocks(sys->n));
-    auto kernel = k_lj_tile<LFS, RM, TPA>;
+    auto kernel = k_lj_tile<LFS, TPA>;
     const size_t smem = 2 * kHaloCap * sizeof(int4);
     static bool attr_set = false;
     if (!attr_set) {
@@ -1183,26 +1082,19 @@ void launch_tile_k(md_system* sys, md_verlet* v, const LJArgs& a, const TileArgs
     kernel<<<grid, kHaloAtoms * TPA, smem, sys->ctx->stream>>>(
         sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
         v->count.as<int>(), v->stride, sys->n, ntiles, v->halo_runs.as<int2>(),
-        v->halo_meta.as<int2>(), box_of(sys), a, t, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
+        v->halo_meta.as<int2>(), box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part,
         ticket, out, sys->ctx->d_status);
 }
 
-template <bool LFS, int TPA>
-void launch_tile_rm(md_system* sys, md_verlet* v, const LJArgs& a, double* part,
-                    unsigned* ticket, double* out) {
-    const TileArgs t = tile_args(a);
-    if (t.rm) launch_tile_k<LFS, 1, TPA>(sys, v, a, t, part, ticket, out);
-    else launch_tile_k<LFS, 0, TPA>(sys, v, a, t, part, ticket, out);
-}
-
-// tpa: threads per atom of the tile kernel (the tile shape: 2, 4 or 8; 0 = 4).
+// tpa: threads per atom of the tile kernel (the tile shape: 2, 4 or 8; 0 = the
+// default, 2).
 template <bool LFS>
 void launch_tile(int tpa, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
                  unsigned* ticket, double* out) {
     switch (tpa) {
-        case 2: launch_tile_rm<LFS, 2>(sys, v, a, part, ticket, out); break;
-        case 8: launch_tile_rm<LFS, 8>(sys, v, a, part, ticket, out); break;
-        default: launch_tile_rm<LFS, 4>(sys, v, a, part, ticket, out); break;
+        case 4: launch_tile_k<LFS, 4>(sys, v, a, part, ticket, out); break;
+        case 8: launch_tile_k<LFS, 8>(sys, v, a, part, ticket, out); break;
+        default: launch_tile_k<LFS, 2>(sys, v, a, part, ticket, out); break;
     }
 }
 

@@ -611,7 +611,8 @@ k_halo_plan(const int* __restrict__ start, GridArgs g, int64_t n, int64_t tiles,
 }
 
 // Rows of a planned tile as 16-bit byte offsets of 16-byte slots (slot = base of
-// the run holding j + j - the run's first atom; kHaloCap * 16 < 2^16): four
+// the run holding j + j - the run's first atom; kHaloCap * 16 < 2^16), the last
+// 8-entry chunk padded with the atom's own slot: four
 // threads per atom, eight entries per 16-byte access, two accesses in flight.  A
 // neighbour outside the tile's runs (not possible for a list built from the same
 // cells) un-stages the tile.
@@ -656,6 +657,9 @@ k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stri
         const int c = min(count[i], stride);
         const int4* src = reinterpret_cast<const int4*>(nbr + i * stride);
         uint4* dst = reinterpret_cast<uint4*>(nbr16 + i * stride);
+        // the last chunk is padded with the atom's own slot (r^2 = 0), which the
+        // force kernels skip, so they read whole chunks without a count test
+        const unsigned self = halo_slot(static_cast<int>(i), nr, s_beg, s_base, bad);
         for (int ch = tid & 3; 8 * ch < c; ch += 8) {
             const int ch2 = ch + 4;
             const bool two = 8 * ch2 < c;
@@ -671,7 +675,7 @@ k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stri
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
                 const int e = 8 * (k < 8 ? ch : ch2) + (k & 7);
-                off[k] = e < c ? halo_slot(js[k], nr, s_beg, s_base, bad) : 0u;
+                off[k] = e < c ? halo_slot(js[k], nr, s_beg, s_base, bad) : self;
             }
             dst[ch] = make_uint4(off[0] | (off[1] << 16), off[2] | (off[3] << 16),
                                  off[4] | (off[5] << 16), off[6] | (off[7] << 16));
