@@ -40,6 +40,7 @@ UNIT = "atom-steps/s"
 CELLS = 64
 RHO, TEMP, RC, SKIN, DT = 0.8442, 0.722, 2.5, 0.3, 0.005
 SEED = 2026
+TILE_THREADS = 0  # the mixed tile kernel's default shape unless --tile-threads
 
 
 STATE_FILE = os.path.join(ROOT, "oracle", "_ref", "lj1m_baoab2000.npz")
@@ -262,6 +263,8 @@ def timed_run(md, ctx, box, pos, vel, frc, precision, steps, warmup, group, cloc
     s = md.System.from_arrays(pos, box, vel=vel, ctx=ctx)
     s.forces = frc
     lj = md.LennardJones(1.0, 1.0, RC, precision=precision)
+    if TILE_THREADS:
+        lj.set_tile_threads(TILE_THREADS)
     v = md.VerletList(box, RC, SKIN, ctx=ctx)
     v.build(s)
     lj.compute_forces(s, v)
@@ -457,7 +460,8 @@ def run_reference_arm(args):
 
 
 def run_gpu_arm(args):
-    global CELLS
+    global CELLS, TILE_THREADS
+    TILE_THREADS = args.tile_threads
     if args.cells != CELLS:
         # profiling configuration: a smaller lattice of the same liquid, equilibrated
         # on the GPU (the reference-equilibrated state is the 64^3 one)
@@ -1398,6 +1402,8 @@ def main():
     ap.add_argument("--cells", type=int, default=CELLS,
                     help="fcc cells per side (profiling configurations only; the metric is "
                          "quoted on 64)")
+    ap.add_argument("--tile-threads", type=int, default=0,
+                    help="mixed tile kernel shape (md_lj_set_tile_threads; profiling)")
     ap.add_argument("--gpu-equil", action="store_true",
                     help="equilibrate on the GPU instead of loading the reference's state")
     ap.add_argument("--drift-steps", type=int, default=None,

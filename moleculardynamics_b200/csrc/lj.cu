@@ -643,23 +643,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-// The warp waits for the phase of `bar` with the given parity: lane 0 polls (the
-// hardware suspends it between tries), then every lane tests the completed phase
-// once, so each sees the copied data.  The warp gives up together after ~1 s.
+// Every lane of the warp waits for the phase of `bar` with the given parity (each
+// then sees the copied data); the warp gives up together after ~1 s.
 __device__ __forceinline__ bool warp_wait_bounded(uint64_t* bar, unsigned parity) {
-    int ok = 1;
-    if ((threadIdx.x & 31) == 0 && !mbar_try_wait(bar, parity)) {
-        const long long t0 = clock64();
-        while (!mbar_try_wait(bar, parity)) {
-            if (clock64() - t0 > kTileWaitCycles) {
-                ok = 0;
-                break;
-            }
-        }
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+    const long long t0 = clock64();
+    for (;;) {
+        if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+        const long long el = __shfl_sync(0xffffffffu, clock64() - t0, 0);
+        if (el > kTileWaitCycles) return false;
     }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (!ok) return false;
-    return __all_sync(0xffffffffu, mbar_try_wait(bar, parity));
 }
 
 __device__ __forceinline__ uint64_t l2_evict_last_policy() {
@@ -758,23 +751,15 @@ __device__ __forceinline__ void tile_issue(int t, int4* dst, uint64_t* bar, cons
     if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
 }
 
-// The constants of the tile kernel's pair term, read once into registers.
-struct TileConst {
-    double res2, res, rc2_lo, rc2_hi;
-    float sig2f, four_epsf, tf_epsf, ucf, rcf, dudrcf;
-};
-
-// One staged entry: pair_mixed's arithmetic in a cubic box (the integer
-// displacement converted exactly to FP64, r^2 formed in FP64 and rounded to FP32
-// once, FP32 pair terms, the force vector accumulated in FP64), branch-free.
-// r^2 = 0 is the row's padding (the atom itself) and contributes nothing.
+// One staged entry (pair_mixed's arithmetic, cubic box); r^2 = 0 is the row's
+// padding (the atom itself) and contributes nothing.
 template <bool LFS>
-__device__ __forceinline__ void pair_tile(const TileConst& a, int4 qi, int4 qj, double& fx,
+__device__ __forceinline__ void pair_tile(const LJArgs& a, int4 qi, int4 qj, double& fx,
                                           double& fy, double& fz, float& e, float& vir,
                                           bool& near) {
-    const double dx = __int2double_rn(wrap_diff(qi.x, qj.x));
-    const double dy = __int2double_rn(wrap_diff(qi.y, qj.y));
-    const double dz = __int2double_rn(wrap_diff(qi.z, qj.z));
+    const double dx = diff_to_double(qi.x, qj.x);
+    const double dy = diff_to_double(qi.y, qj.y);
+    const double dz = diff_to_double(qi.z, qj.z);
     const double r2 = fma(dz, dz, fma(dy, dy, dx * dx)) * a.res2;
     const bool in_range = r2 < a.rc2_hi;
     const bool in_band = r2 > a.rc2_lo;
@@ -792,10 +777,13 @@ __device__ __forceinline__ void pair_tile(const TileConst& a, int4 qi, int4 qj, 
         u = u - a.ucf - (r - a.rcf) * a.dudrcf;
         w = w + r * a.dudrcf;
     }
-    const float sf = take ? w * inv : 0.f;
-    e += take ? u : 0.f;
-    vir += take ? w : 0.f;
-    const double sd = static_cast<double>(sf) * a.res;
+    float sf = 0.f;
+    if (take) {
+        sf = w * inv;
+        e += u;
+        vir += w;
+    }
+    const double sd = static_cast<double>(sf) * a.res[0];
     fx = fma(dx, sd, fx);
     fy = fma(dy, sd, fy);
     fz = fma(dz, sd, fz);
@@ -833,59 +821,24 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
             tile_issue(blockIdx.x + stride_t, s_buf + kHaloCap, &s_bar[1], q, runs, meta, pol_q);
     }
     const Fold3 f3 = fold3_of(box);
-    TileConst tc;
-    tc.res2 = a.res2;
-    tc.res = a.res[0];
-    tc.rc2_lo = a.rc2_lo;
-    tc.rc2_hi = a.rc2_hi;
-    tc.sig2f = a.sig2f;
-    tc.four_epsf = a.four_epsf;
-    tc.tf_epsf = a.tf_epsf;
-    tc.ucf = a.ucf;
-    tc.rcf = a.rcf;
-    tc.dudrcf = a.dudrcf;
     double e_tot = 0.0, w_tot = 0.0;
     bool timed_out = false;
     int k = 0;
-    // this thread's atom of the first tile, loaded ahead of its halo
-    int t = blockIdx.x;
-    int64_t i_next = static_cast<int64_t>(t) * kHaloAtoms + (tid / TPA);
-    int4 pi_next = make_int4(0, 0, 0, 0);
-    int cnt_next = 0;
-    int2 m_next = make_int2(0, 0);
-    if (t < ntiles) {
-        m_next = meta[t];
-        if (i_next < n) {
-            pi_next = __ldg(q + i_next);
-            cnt_next = min(count[i_next], stride);  // an overflowed row is flagged, never over-read
-        }
-    }
-    for (; t < ntiles; t += stride_t, ++k) {
+    for (int t = blockIdx.x; t < ntiles; t += stride_t, ++k) {
         const int b = k & 1;
         int4* buf = s_buf + b * kHaloCap;
-        const int64_t i = i_next;
-        const int ii = static_cast<int>(i);
-        const int4 pi = pi_next;
-        const int cnt = cnt_next;
-        const int2 m = m_next;
-        {  // the next tile's atom, in flight while this one is computed
-            const int tn = t + stride_t;
-            i_next = static_cast<int64_t>(tn) * kHaloAtoms + (tid / TPA);
-            if (tn < ntiles) {
-                m_next = meta[tn];
-                if (i_next < n) {
-                    pi_next = __ldg(q + i_next);
-                    cnt_next = min(count[i_next], stride);
-                }
-            }
-        }
         if (!warp_wait_bounded(&s_bar[b], static_cast<unsigned>((k >> 1) & 1))) {
             timed_out = true;  // the copies never landed: flag it and leave the loop
             break;
         }
+        const int2 m = meta[t];
+        const int64_t i = static_cast<int64_t>(t) * kHaloAtoms + (tid / TPA);
+        const int ii = static_cast<int>(i);
         double fx = 0.0, fy = 0.0, fz = 0.0;
         float e = 0.f, vir = 0.f;
         if (i < n) {
+            const int4 pi = __ldg(q + i);
+            const int cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
             if (m.x > 0) {
                 const uint16_t* row = nbr16 + i * stride;
                 const char* tile = reinterpret_cast<const char*>(buf);
@@ -898,7 +851,7 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
 #pragma unroll
                     for (int h = 0; h < EPT; ++h) {
                         const int4 qj = *reinterpret_cast<const int4*>(tile + R::slot(cur, h));
-                        pair_tile<LFS>(tc, pi, qj, fx, fy, fz, e, vir, near);
+                        pair_tile<LFS>(a, pi, qj, fx, fy, fz, e, vir, near);
                     }
                 }
                 if (near) {
@@ -1233,7 +1186,7 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     const bool halo = mixed && lj->halo && sys->n > 0 && v->halo_on && v->stride % 8 == 0;
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
-    if (halo && cubic) {
+    if (halo && cubic && lj->tile_tpa != 1) {
         if (lfs) launch_tile<true>(lj->tile_tpa, sys, v, a, part, ticket, out);
         else launch_tile<false>(lj->tile_tpa, sys, v, a, part, ticket, out);
     } else if (halo) {
@@ -1547,8 +1500,9 @@ int md_lj_set_launch(md_lj* lj, int tpa, int unroll) {
 
 int md_lj_set_tile_threads(md_lj* lj, int tpa) {
     graph_epoch_bump();
-    if (!lj || (tpa != 0 && tpa != 2 && tpa != 4 && tpa != 8))
-        return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_set_tile_threads: threads per atom must be 0, 2, 4 or 8");
+    if (!lj || (tpa != 0 && tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8))
+        return fail(MD_ERR_INVALID_ARGUMENT,
+                    "md_lj_set_tile_threads: threads per atom must be 0, 1, 2, 4 or 8");
     lj->tile_tpa = tpa;
     return MD_OK;
 }

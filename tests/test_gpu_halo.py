@@ -119,7 +119,7 @@ def test_cubic_two_phase_box_mixes_staged_and_gathered_tiles(md):
     check_budget(ref, gathered, tiled, e_tol=1e-6)
 
 
-@pytest.mark.parametrize("tpa", [4, 8])
+@pytest.mark.parametrize("tpa", [1, 4, 8])
 def test_tile_shapes_within_budget(md, tpa):
     """Every tile shape (threads per atom of the tile kernel) sums the same pairs:
     within the error budget of FP64 and of the default shape, and deterministic."""
