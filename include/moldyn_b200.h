@@ -249,10 +249,10 @@ MD_API int md_lj_set_launch(md_lj* lj, int tpa, int unroll);
  * cells around them in shared memory; rows then also exist as 16-bit tile slots.
  * Forces are identical either way.  No reference counterpart. */
 MD_API int md_lj_set_halo(md_lj* lj, int on);
-/* Threads per atom of the mixed tile kernel (the tile shape: 2, 4 or 8 for the
- * persistent double-buffered kernel; 1 for the single-buffer kernel, one CTA per
- * tile with two threads per atom; 0 restores the default, 2); no reference
- * counterpart, a tuning axis.  Every shape sums the
+/* Shape of the mixed tile kernel: 0 (the default) one CTA per tile with two threads
+ * per atom, the halo queued by bulk copies; 1 the same with per-thread staging and
+ * the FP64-unit arithmetic of the gathered kernel; 2, 4 or 8 threads per atom in
+ * the persistent double-buffered kernel.  No reference counterpart, a tuning axis.  Every shape sums the
  * same pairs with the same arithmetic, in a different order. */
 MD_API int md_lj_set_tile_threads(md_lj* lj, int tpa);
 /* Halo tiles of a Verlet list: built now from the current list and again at

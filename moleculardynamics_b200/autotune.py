@@ -121,7 +121,7 @@ def tune_skin(box, pos, vel, mass, lj, make_integrator, skins=(0.2, 0.3, 0.4, 0.
     return min(times, key=times.get), times
 
 
-TILE_SHAPES = (1, 2, 4, 8)
+TILE_SHAPES = (0, 1, 2, 4)
 
 
 def tune_tile_shape(sys, lj, verlet, shapes=TILE_SHAPES, repeats=5):

@@ -934,6 +934,169 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
     grid_reduce<2>(v, part, ticket, out);
 }
 
+// ------------------------------------------------------------ k_lj_tile1
+// The single-buffer form of the tile kernel (the default shape): one CTA per tile,
+// two threads per atom, four CTAs per SM, so that while one CTA waits for its
+// halo the others compute.  Warp 0 queues the halo with one bulk copy per run
+// (tile_issue) and every thread waits on the CTA's mbarrier; no thread copies
+// data and no CTA barrier precedes the pairs.  Rows are padded to whole 8-entry
+// chunks (the atom's own slot), so each thread reads its 4 slots of a chunk with
+// one 8-byte load and evaluates them without a count test.  The arithmetic is the
+// gathered kernel's in integer units of the fixed-point grid: d exact, r^2 formed
+// in FP64 and rounded to FP32 once, FP32 pair terms, the force accumulated in
+// FP64 and scaled by 1 / res at the end; pairs in the cutoff band are settled by
+// the reference arithmetic as there.
+struct UnitConst {
+    double lo, hi;        // rc^2 -/+ band in units res^2
+    float sig2u;          // sigma^2 in units res^2
+    float four_epsf, tf_epsf, ucf, rcf, dudrcf, res_f;
+};
+
+template <bool LFS>
+__device__ __forceinline__ void pair_unit(const UnitConst& c, int4 qi, int4 qj, double& fx,
+                                          double& fy, double& fz, float& e, float& vir,
+                                          bool& near) {
+    const double dx = diff_to_double(qi.x, qj.x);
+    const double dy = diff_to_double(qi.y, qj.y);
+    const double dz = diff_to_double(qi.z, qj.z);
+    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));  // exact up to one rounding
+    const bool below = r2 < c.lo;
+    near = near || (!below && r2 < c.hi);
+    const float m = (below && r2 > 0.0) ? 1.f : 0.f;  // r^2 = 0: the row's padding
+    const float r2f = static_cast<float>(r2);
+    const float inv = rcp_approx(r2f);
+    const float s2 = c.sig2u * inv;
+    const float s6 = s2 * s2 * s2;
+    const float t6 = fmaf(s6, s6, -s6);
+    float u = c.four_epsf * t6;
+    float w = c.tf_epsf * fmaf(s6, s6, t6);
+    if (LFS) {
+        const float r = sqrtf(r2f) * c.res_f;
+        u = u - c.ucf - (r - c.rcf) * c.dudrcf;
+        w = w + r * c.dudrcf;
+    }
+    e = fmaf(u, m, e);
+    vir = fmaf(w, m, vir);
+    const double sd = static_cast<double>((w * m) * inv);
+    fx = fma(dx, sd, fx);
+    fy = fma(dy, sd, fy);
+    fz = fma(dz, sd, fz);
+}
+
+// Word c of a row for thread g of the two an atom has (4 slots), streamed past L1.
+__device__ __forceinline__ uint2 row_word2(const uint16_t* row, int c, int g) {
+    uint2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];"
+                 : "=r"(v.x), "=r"(v.y)
+                 : "l"(reinterpret_cast<const uint2*>(row) + 2 * c + g));
+    return v;
+}
+
+template <bool LFS>
+__global__ void __launch_bounds__(kHaloAtoms * 2, 4)
+k_lj_tile1(const int4* __restrict__ q, const double4* __restrict__ pd, const int* __restrict__ nbr,
+           const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride, int64_t n,
+           const int2* __restrict__ runs, const int2* __restrict__ meta,
+           const __grid_constant__ Box3 box, const __grid_constant__ LJArgs a,
+           const __grid_constant__ UnitConst uc, double* __restrict__ fxo,
+           double* __restrict__ fyo, double* __restrict__ fzo, double* part, unsigned* ticket,
+           double* out, uint32_t* status) {
+    constexpr int TPA = 2;
+    extern __shared__ __align__(128) int4 s_tile[];  // kHaloCap slots
+    __shared__ uint64_t s_bar;
+    const int tid = threadIdx.x, t = blockIdx.x;
+    const int g = tid & 1;
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid < 32) tile_issue(t, s_tile, &s_bar, q, runs, meta, l2_evict_last_policy());
+    // the atom's own data and first row word travel while the halo lands
+    const int2 m = meta[t];
+    const int64_t i = static_cast<int64_t>(t) * kHaloAtoms + (tid >> 1);
+    const int ii = static_cast<int>(i);
+    int4 pi = make_int4(0, 0, 0, 0);
+    int cnt = 0;
+    if (i < n) {
+        pi = __ldg(q + i);
+        cnt = min(count[i], stride);  // an overflowed row is flagged, never over-read
+    }
+    const uint16_t* row = nbr16 + i * stride;
+    const int nch = (i < n && m.x > 0) ? (cnt + 7) >> 3 : 0;
+    uint2 word = nch > 0 ? row_word2(row, 0, g) : make_uint2(0u, 0u);
+    const bool landed = warp_wait_bounded(&s_bar, 0u);
+    double fx = 0.0, fy = 0.0, fz = 0.0;  // grid units in the main loop, then real units
+    float e = 0.f, vir = 0.f;
+    if (!landed) {
+        if ((tid & 31) == 0) atomicOr(status, MD_STATUS_WAIT_TIMEOUT);
+    } else if (i < n) {
+        const Fold3 f3 = fold3_of(box);
+        if (m.x > 0) {
+            const char* tile = reinterpret_cast<const char*>(s_tile);
+            bool near = false;
+            for (int c = 0; c < nch; ++c) {
+                const uint2 cur = word;
+                if (c + 1 < nch) word = row_word2(row, c + 1, g);
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const int4 qj = *reinterpret_cast<const int4*>(tile + TileRow<2>::slot(cur, h));
+                    pair_unit<LFS>(uc, pi, qj, fx, fy, fz, e, vir, near);
+                }
+            }
+            const double inv_res = 1.0 / a.res[0];
+            fx *= inv_res;
+            fy *= inv_res;
+            fz *= inv_res;
+            if (near) {
+                // rare: the pairs next to the cutoff, decided by the reference
+                // arithmetic on the FP64 positions (the slot maps to its atom
+                // through the tile's runs)
+                const int2* tr = runs + static_cast<int64_t>(t) * kHaloRuns;
+                for (int c = 0; c < nch; ++c) {
+                    for (int h = 0; h < 4; ++h) {
+                        const int kk = 8 * c + 4 * g + h;
+                        if (kk >= cnt) continue;
+                        const unsigned off = row[kk];
+                        const int sl = static_cast<int>(off >> 4);
+                        int lo = 0, hi = m.x;  // the last run whose first slot is <= sl
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (tr[mid].y <= sl) lo = mid;
+                            else hi = mid;
+                        }
+                        near_pair<LFS>(a, f3, pd, ii, tr[lo].x + (sl - tr[lo].y), pi,
+                                       *reinterpret_cast<const int4*>(tile + off), fx, fy, fz, e,
+                                       vir);
+                    }
+                }
+            }
+        } else {
+            // a tile that is not staged: its int32 row, positions gathered
+            const int* r32 = nbr + i * stride;
+            bool near = false;
+            for (int kk = g; kk < cnt; kk += TPA)
+                pair_mixed<LFS, true>(a, pi, __ldg(q + __ldg(r32 + kk)), fx, fy, fz, e, vir, near);
+            if (near) {
+                for (int kk = g; kk < cnt; kk += TPA) {
+                    const int j = __ldg(r32 + kk);
+                    near_pair<LFS>(a, f3, pd, ii, j, pi, __ldg(q + j), fx, fy, fz, e, vir);
+                }
+            }
+        }
+    }
+    fx += __shfl_xor_sync(0xffffffffu, fx, 1);
+    fy += __shfl_xor_sync(0xffffffffu, fy, 1);
+    fz += __shfl_xor_sync(0xffffffffu, fz, 1);
+    if (i < n && g == 0) {
+        fxo[i] = fx;
+        fyo[i] = fy;
+        fzo[i] = fz;
+    }
+    double v[2] = {0.5 * static_cast<double>(e), 0.5 * static_cast<double>(vir)};  // both sides
+    grid_reduce<2>(v, part, ticket, out);
+}
+
 // Brute force (lennard_jones.cpp:90-97): every atom against every other atom,
 // positions staged through shared memory in tiles.
 template <bool LFS>
@@ -1065,6 +1228,33 @@ void launch_halo(md_system* sys, md_verlet* v, const LJArgs& a, double* part, un
         box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
 }
 
+UnitConst unit_const(const LJArgs& a) {
+    UnitConst c;
+    const double res2 = a.res2;
+    c.lo = a.rc2_lo / res2;
+    c.hi = a.rc2_hi / res2;
+    c.sig2u = static_cast<float>(a.sig2 / res2);
+    c.four_epsf = a.four_epsf;
+    c.tf_epsf = a.tf_epsf;
+    c.ucf = a.ucf;
+    c.rcf = a.rcf;
+    c.dudrcf = a.dudrcf;
+    c.res_f = static_cast<float>(a.res[0]);
+    return c;
+}
+
+template <bool LFS>
+void launch_tile1(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
+                  double* out) {
+    const unsigned blocks = static_cast<unsigned>(halo_blocks(sys->n));
+    const size_t smem = kHaloCap * sizeof(int4);
+    k_lj_tile1<LFS><<<blocks, kHaloAtoms * 2, smem, sys->ctx->stream>>>(
+        sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
+        v->count.as<int>(), v->stride, sys->n, v->halo_runs.as<int2>(), v->halo_meta.as<int2>(),
+        box_of(sys), a, unit_const(a), sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out,
+        sys->ctx->d_status);
+}
+
 template <bool LFS, int TPA>
 void launch_tile_k(md_system* sys, md_verlet* v, const LJArgs& a, double* part,
                    unsigned* ticket, double* out) {
@@ -1186,9 +1376,12 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     const bool halo = mixed && lj->halo && sys->n > 0 && v->halo_on && v->stride % 8 == 0;
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
-    if (halo && cubic && lj->tile_tpa != 1) {
+    if (halo && cubic && lj->tile_tpa > 1) {
         if (lfs) launch_tile<true>(lj->tile_tpa, sys, v, a, part, ticket, out);
         else launch_tile<false>(lj->tile_tpa, sys, v, a, part, ticket, out);
+    } else if (halo && cubic && lj->tile_tpa == 0) {
+        if (lfs) launch_tile1<true>(sys, v, a, part, ticket, out);
+        else launch_tile1<false>(sys, v, a, part, ticket, out);
     } else if (halo) {
         if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out);
         else launch_halo_u<false>(unroll, sys, v, a, part, ticket, out);

@@ -297,7 +297,7 @@ struct md_lj {
     double u_at_cutoff = 0, dudr_at_cutoff = 0;
     int tpa = 0, unroll = 0;   // launch shape of the Verlet force kernel (0: library default)
     bool halo = true;          // mixed precision: staged halo tiles where the list allows
-    int tile_tpa = 0;          // threads per atom of the tile kernel (0: its default, 2)
+    int tile_tpa = 0;          // tile kernel shape (0 default, 1 single-buffer per-thread staging, 2/4/8 persistent)
 };
 
 namespace mdb {
