@@ -250,9 +250,10 @@ MD_API int md_lj_set_launch(md_lj* lj, int tpa, int unroll);
  * Forces are identical either way.  No reference counterpart. */
 MD_API int md_lj_set_halo(md_lj* lj, int on);
 /* Shape of the mixed tile kernel: 0 (the default) one CTA per tile with two threads
- * per atom, the halo queued by bulk copies; 1 the same with per-thread staging and
- * the FP64-unit arithmetic of the gathered kernel; 2, 4 or 8 threads per atom in
- * the persistent double-buffered kernel.  No reference counterpart, a tuning axis.  Every shape sums the
+ * per atom, the halo staged by the threads; 1 the same with the halo queued by bulk
+ * copies on an mbarrier and the rows read in whole padded chunks; 2, 4 or 8 threads
+ * per atom in the persistent double-buffered kernel.  No reference counterpart, a
+ * tuning axis.  Every shape sums the
  * same pairs with the same arithmetic, in a different order. */
 MD_API int md_lj_set_tile_threads(md_lj* lj, int tpa);
 /* Halo tiles of a Verlet list: built now from the current list and again at

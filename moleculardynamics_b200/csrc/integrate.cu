@@ -519,13 +519,18 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
         if (e != cudaSuccess) rc = fail(MD_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
         else body = cp.conditional.phGraph_out[0];
     }
+    // the rebuild branch also re-quantizes the re-sorted positions, so that the
+    // main path launches no gated no-op
     if (rc == MD_OK)
-        rc = capture_into(ctx, body, nullptr, 0, [&]() -> int { return verlet_build(v, sys, true); },
-                          nullptr);
+        rc = capture_into(ctx, body, nullptr, 0, [&]() -> int {
+            MDB_TRY(verlet_build(v, sys, true));
+            if (q) MDB_TRY(lj_quantize_async(lj, sys, v->d_rebuild_flag));
+            return MD_OK;
+        }, nullptr);
     const int64_t l2 = ctx->launches;
     if (rc == MD_OK)
         rc = capture_into(ctx, graph, &cond, 1, [&]() -> int {
-            MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr));
+            MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr, q != nullptr));
             MDB_TRY(post_force_async(it, sys, false));
             if (rows) {
                 k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy),

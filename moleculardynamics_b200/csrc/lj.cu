@@ -935,7 +935,7 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
 }
 
 // ------------------------------------------------------------ k_lj_tile1
-// The single-buffer form of the tile kernel (the default shape): one CTA per tile,
+// A single-buffer form of the tile kernel (shape 1): one CTA per tile,
 // two threads per atom, four CTAs per SM, so that while one CTA waits for its
 // halo the others compute.  Warp 0 queues the halo with one bulk copy per run
 // (tile_issue) and every thread waits on the CTA's mbarrier; no thread copies
@@ -962,8 +962,10 @@ __device__ __forceinline__ void pair_unit(const UnitConst& c, int4 qi, int4 qj, 
     const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));  // exact up to one rounding
     const bool below = r2 < c.lo;
     near = near || (!below && r2 < c.hi);
-    const float m = (below && r2 > 0.0) ? 1.f : 0.f;  // r^2 = 0: the row's padding
-    const float r2f = static_cast<float>(r2);
+    const bool pad = !(r2 > 0.0);  // r^2 = 0: the row's padding (the atom itself)
+    const float m = (below && !pad) ? 1.f : 0.f;
+    // the padding's r^2 is replaced by a far one, so its (masked) terms stay finite
+    const float r2f = pad ? 1.0e30f : static_cast<float>(r2);
     const float inv = rcp_approx(r2f);
     const float s2 = c.sig2u * inv;
     const float s6 = s2 * s2 * s2;
@@ -1358,7 +1360,8 @@ int lj_quantize_async(md_lj* lj, md_system* sys, const int* gate) {
     return MD_OK;
 }
 
-int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q_gate) {
+int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q_gate,
+                           bool q_current) {
     md_context* ctx = sys->ctx;
     const LJArgs a = verlet_lj_args(lj, sys);
     const int tpa = lj->tpa ? lj->tpa : g_lj_tpa, unroll = lj->unroll ? lj->unroll : g_lj_unroll;
@@ -1370,7 +1373,7 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     double* out = ctx_result(ctx, kResEnergy);
     const bool lfs = lj->truncation == MD_LINEAR_FORCE_SHIFT;
     const bool mixed = lj->precision == MD_PRECISION_MIXED;
-    MDB_TRY(lj_quantize_async(lj, sys, q_gate));
+    if (!q_current) MDB_TRY(lj_quantize_async(lj, sys, q_gate));
     // halo tiles, when the list keeps them (fused runs of large systems turn them on,
     // or md_verlet_set_halo)
     const bool halo = mixed && lj->halo && sys->n > 0 && v->halo_on && v->stride % 8 == 0;
@@ -1379,7 +1382,7 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     if (halo && cubic && lj->tile_tpa > 1) {
         if (lfs) launch_tile<true>(lj->tile_tpa, sys, v, a, part, ticket, out);
         else launch_tile<false>(lj->tile_tpa, sys, v, a, part, ticket, out);
-    } else if (halo && cubic && lj->tile_tpa == 0) {
+    } else if (halo && cubic && lj->tile_tpa == 1) {
         if (lfs) launch_tile1<true>(sys, v, a, part, ticket, out);
         else launch_tile1<false>(sys, v, a, part, ticket, out);
     } else if (halo) {

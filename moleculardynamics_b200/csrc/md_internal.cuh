@@ -297,7 +297,7 @@ struct md_lj {
     double u_at_cutoff = 0, dudr_at_cutoff = 0;
     int tpa = 0, unroll = 0;   // launch shape of the Verlet force kernel (0: library default)
     bool halo = true;          // mixed precision: staged halo tiles where the list allows
-    int tile_tpa = 0;          // tile kernel shape (0 default, 1 single-buffer per-thread staging, 2/4/8 persistent)
+    int tile_tpa = 0;          // tile kernel shape (0 single-buffer, 1 single-buffer bulk copies, 2/4/8 persistent)
 };
 
 namespace mdb {
@@ -323,8 +323,10 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
 // q_gate: the fixed-point positions were written by the step's kick/drift; they
 // are re-quantized only when this device flag says a rebuild re-sorted the atoms
 // (null: always quantize).
+// q_current: the fixed-point positions are known to be current (a step graph
+// re-quantizes inside its rebuild branch), so no quantize launch at all.
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v,
-                           const int* q_gate = nullptr);
+                           const int* q_gate = nullptr, bool q_current = false);
 int lj_forces_brute_async(md_lj* lj, md_system* sys, bool forces);
 int lj_forces_cells_async(md_lj* lj, md_system* sys, md_cells* cells);
 int system_kinetic_async(md_system* sys, int slot);
