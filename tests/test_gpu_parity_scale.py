@@ -67,7 +67,7 @@ def test_fp64_1m_liquid_forces_and_pairs_equal_reference(md):
     fr, er, wr, pr = O.ref_lj_verlet(pos, box, rc=2.5, skin=0.3, trunc=0)
     assert approx_eq(e, er, 1e-12) and approx_eq(w, wr, 1e-12), (e, er, w, wr)
     assert approx_eq(f, fr, 1e-12), np.max(np.abs(f - fr))
-    assert len(pairs) == len(pr) and len(pr) > 38 * n
+    assert len(pairs) == len(pr) and len(pr) > 35 * n  # ~38 half pairs per atom at rc + skin
     assert np.array_equal(pair_keys(pairs, n), pair_keys(pr, n))
 
 
