@@ -478,48 +478,6 @@ __device__ __noinline__ PairSums gathered_row(LJArgs a, Box3 box, const double4*
     return acc;
 }
 
-// Constants of the integer-unit pair term (cubic boxes): lengths in units of the
-// fixed-point resolution res, so r^2 needs no scaling and the force vector is
-// scaled by 1 / res once per atom.
-struct UnitConst {
-    double lo, hi;        // rc^2 -/+ band in units res^2
-    float sig2u;          // sigma^2 in units res^2
-    float four_epsf, tf_epsf, ucf, rcf, dudrcf, res_f;
-};
-
-template <bool LFS>
-__device__ __forceinline__ void pair_unit(const UnitConst& c, int4 qi, int4 qj, double& fx,
-                                          double& fy, double& fz, float& e, float& vir,
-                                          bool& near) {
-    const double dx = diff_to_double(qi.x, qj.x);
-    const double dy = diff_to_double(qi.y, qj.y);
-    const double dz = diff_to_double(qi.z, qj.z);
-    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));  // exact up to one rounding
-    const bool below = r2 < c.lo;
-    near = near || (!below && r2 < c.hi);
-    const bool pad = !(r2 > 0.0);  // r^2 = 0: the row's padding (the atom itself)
-    const float m = (below && !pad) ? 1.f : 0.f;
-    // the padding's r^2 is replaced by a far one, so its (masked) terms stay finite
-    const float r2f = pad ? 1.0e30f : static_cast<float>(r2);
-    const float inv = rcp_approx(r2f);
-    const float s2 = c.sig2u * inv;
-    const float s6 = s2 * s2 * s2;
-    const float t6 = fmaf(s6, s6, -s6);
-    float u = c.four_epsf * t6;
-    float w = c.tf_epsf * fmaf(s6, s6, t6);
-    if (LFS) {
-        const float r = sqrtf(r2f) * c.res_f;
-        u = u - c.ucf - (r - c.rcf) * c.dudrcf;
-        w = w + r * c.dudrcf;
-    }
-    e = fmaf(u, m, e);
-    vir = fmaf(w, m, vir);
-    const double sd = static_cast<double>((w * m) * inv);
-    fx = fma(dx, sd, fx);
-    fy = fma(dy, sd, fy);
-    fz = fma(dz, sd, fz);
-}
-
 // Mixed-precision forces over halo tiles (one CTA per tile of kHaloAtoms sorted
 // atoms, two threads per atom).  The CTA copies the fixed-point positions of its
 // tile's cell runs into shared memory -- contiguous, coalesced reads of an array
@@ -534,8 +492,8 @@ __global__ void __launch_bounds__(kBlock, 4)
 k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int* __restrict__ nbr,
           const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride, int64_t n,
           const int2* __restrict__ runs, const int2* __restrict__ meta, Box3 box, LJArgs a,
-          UnitConst uc, double* __restrict__ fxo, double* __restrict__ fyo,
-          double* __restrict__ fzo, double* part, unsigned* ticket, double* out) {
+          double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
+          double* part, unsigned* ticket, double* out) {
     constexpr int TPA = kBlock / kHaloAtoms;
     extern __shared__ int4 s_q[];  // kHaloCap slots
     __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
@@ -583,62 +541,36 @@ k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
             const int nfull = cnt >> 3, nch = (cnt + 7) >> 3;
             bool near = false;
             uint4 cur = nch > 0 ? __ldg(rowv) : make_uint4(0u, 0u, 0u, 0u);
-            if constexpr (CUBIC) {
-                // integer units and whole chunks: the rows of staged tiles are padded
-                // to 8 entries with the atom's own slot, which pair_unit skips
-                auto chunk = [&](const uint4& v) {
-                    const unsigned w4[4] = {v.x, v.y, v.z, v.w};
+            auto chunk = [&](const uint4& v) {
+                const unsigned w4[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-                    for (int t = 0; t < 4; ++t)
-                        pair_unit<LFS>(
-                            uc, pi,
+                for (int t = 0; t < 4; ++t)
+                    pair_mixed<LFS, CUBIC>(
+                        a, pi, *reinterpret_cast<const int4*>(tile + __byte_perm(w4[t], 0u, sel)),
+                        acc.fx, acc.fy, acc.fz, acc.e, acc.vir, near);
+            };
+            int c = 0;
+            for (; c + 1 < nfull; c += 2) {  // two chunks per trip: no register copies
+                const uint4 nxt = __ldg(rowv + c + 1);
+                chunk(cur);
+                cur = c + 2 < nch ? __ldg(rowv + c + 2) : nxt;
+                chunk(nxt);
+            }
+            if (c < nfull) {
+                const uint4 nxt = c + 1 < nch ? __ldg(rowv + c + 1) : cur;
+                chunk(cur);
+                cur = nxt;
+            }
+            const int rem = cnt & 7;  // the last, partial chunk
+            if (rem > g) {
+                const unsigned w4[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (g + 2 * t < rem)
+                        pair_mixed<LFS, CUBIC>(
+                            a, pi,
                             *reinterpret_cast<const int4*>(tile + __byte_perm(w4[t], 0u, sel)),
                             acc.fx, acc.fy, acc.fz, acc.e, acc.vir, near);
-                };
-                int c = 0;
-                for (; c + 1 < nch; c += 2) {  // two chunks per trip: no register copies
-                    const uint4 nxt = __ldg(rowv + c + 1);
-                    chunk(cur);
-                    cur = c + 2 < nch ? __ldg(rowv + c + 2) : nxt;
-                    chunk(nxt);
-                }
-                if (c < nch) chunk(cur);
-                const double inv_res = 1.0 / a.res[0];
-                acc.fx *= inv_res;
-                acc.fy *= inv_res;
-                acc.fz *= inv_res;
-            } else {
-                auto chunk = [&](const uint4& v) {
-                    const unsigned w4[4] = {v.x, v.y, v.z, v.w};
-    #pragma unroll
-                    for (int t = 0; t < 4; ++t)
-                        pair_mixed<LFS, CUBIC>(
-                            a, pi, *reinterpret_cast<const int4*>(tile + __byte_perm(w4[t], 0u, sel)),
-                            acc.fx, acc.fy, acc.fz, acc.e, acc.vir, near);
-                };
-                int c = 0;
-                for (; c + 1 < nfull; c += 2) {  // two chunks per trip: no register copies
-                    const uint4 nxt = __ldg(rowv + c + 1);
-                    chunk(cur);
-                    cur = c + 2 < nch ? __ldg(rowv + c + 2) : nxt;
-                    chunk(nxt);
-                }
-                if (c < nfull) {
-                    const uint4 nxt = c + 1 < nch ? __ldg(rowv + c + 1) : cur;
-                    chunk(cur);
-                    cur = nxt;
-                }
-                const int rem = cnt & 7;  // the last, partial chunk
-                if (rem > g) {
-                    const unsigned w4[4] = {cur.x, cur.y, cur.z, cur.w};
-    #pragma unroll
-                    for (int t = 0; t < 4; ++t)
-                        if (g + 2 * t < rem)
-                            pair_mixed<LFS, CUBIC>(
-                                a, pi,
-                                *reinterpret_cast<const int4*>(tile + __byte_perm(w4[t], 0u, sel)),
-                                acc.fx, acc.fy, acc.fz, acc.e, acc.vir, near);
-                }
             }
             if (near)  // rare: settle the pairs next to the cutoff
                 acc = near_pairs_tile<LFS>(a, box, pd, row, cnt, g, ii, pi, s_q, s_beg, s_base, m.x,
@@ -1014,6 +946,45 @@ k_lj_tile(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
 // in FP64 and rounded to FP32 once, FP32 pair terms, the force accumulated in
 // FP64 and scaled by 1 / res at the end; pairs in the cutoff band are settled by
 // the reference arithmetic as there.
+struct UnitConst {
+    double lo, hi;        // rc^2 -/+ band in units res^2
+    float sig2u;          // sigma^2 in units res^2
+    float four_epsf, tf_epsf, ucf, rcf, dudrcf, res_f;
+};
+
+template <bool LFS>
+__device__ __forceinline__ void pair_unit(const UnitConst& c, int4 qi, int4 qj, double& fx,
+                                          double& fy, double& fz, float& e, float& vir,
+                                          bool& near) {
+    const double dx = diff_to_double(qi.x, qj.x);
+    const double dy = diff_to_double(qi.y, qj.y);
+    const double dz = diff_to_double(qi.z, qj.z);
+    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));  // exact up to one rounding
+    const bool below = r2 < c.lo;
+    near = near || (!below && r2 < c.hi);
+    const bool pad = !(r2 > 0.0);  // r^2 = 0: the row's padding (the atom itself)
+    const float m = (below && !pad) ? 1.f : 0.f;
+    // the padding's r^2 is replaced by a far one, so its (masked) terms stay finite
+    const float r2f = pad ? 1.0e30f : static_cast<float>(r2);
+    const float inv = rcp_approx(r2f);
+    const float s2 = c.sig2u * inv;
+    const float s6 = s2 * s2 * s2;
+    const float t6 = fmaf(s6, s6, -s6);
+    float u = c.four_epsf * t6;
+    float w = c.tf_epsf * fmaf(s6, s6, t6);
+    if (LFS) {
+        const float r = sqrtf(r2f) * c.res_f;
+        u = u - c.ucf - (r - c.rcf) * c.dudrcf;
+        w = w + r * c.dudrcf;
+    }
+    e = fmaf(u, m, e);
+    vir = fmaf(w, m, vir);
+    const double sd = static_cast<double>((w * m) * inv);
+    fx = fma(dx, sd, fx);
+    fy = fma(dy, sd, fy);
+    fz = fma(dz, sd, fz);
+}
+
 // Word c of a row for thread g of the two an atom has (4 slots), streamed past L1.
 __device__ __forceinline__ uint2 row_word2(const uint16_t* row, int c, int g) {
     uint2 v;
@@ -1247,6 +1218,18 @@ __global__ void k_quantize(const double4* __restrict__ pos, int64_t n, double sx
     q[k] = quantize_position(pos[k], sx, sy, sz);
 }
 
+template <bool LFS, int U>
+void launch_halo(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
+                 double* out) {
+    const unsigned blocks = static_cast<unsigned>(halo_blocks(sys->n));
+    const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
+    auto kernel = cubic ? k_lj_halo<LFS, U, true> : k_lj_halo<LFS, U, false>;
+    kernel<<<blocks, kBlock, kHaloCap * sizeof(int4), sys->ctx->stream>>>(
+        sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
+        v->count.as<int>(), v->stride, sys->n, v->halo_runs.as<int2>(), v->halo_meta.as<int2>(),
+        box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+}
+
 UnitConst unit_const(const LJArgs& a) {
     UnitConst c;
     const double res2 = a.res2;
@@ -1261,19 +1244,6 @@ UnitConst unit_const(const LJArgs& a) {
     c.res_f = static_cast<float>(a.res[0]);
     return c;
 }
-
-template <bool LFS, int U>
-void launch_halo(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
-                 double* out) {
-    const unsigned blocks = static_cast<unsigned>(halo_blocks(sys->n));
-    const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
-    auto kernel = cubic ? k_lj_halo<LFS, U, true> : k_lj_halo<LFS, U, false>;
-    kernel<<<blocks, kBlock, kHaloCap * sizeof(int4), sys->ctx->stream>>>(
-        sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
-        v->count.as<int>(), v->stride, sys->n, v->halo_runs.as<int2>(), v->halo_meta.as<int2>(),
-        box_of(sys), a, unit_const(a), sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
-}
-
 
 template <bool LFS>
 void launch_tile1(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
