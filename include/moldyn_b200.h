@@ -454,7 +454,8 @@ MD_API int md_batch_run(md_batch* batch, int64_t steps, double* thermo);
  * more often).  md_adjoint_backward takes dL/d(row) (steps x 3), recomputes each
  * segment from its saved state and returns dL/d(epsilon, sigma), and optionally
  * dL/d(initial positions) and dL/d(initial velocities) (n x 3, caller's order).
- * The system is left where the forward left it. */
+ * The system is left where the forward left it.  md_adjoint_backward replays
+ * on the system the forward ran on: it must not be destroyed in between. */
 MD_API int md_adjoint_create(md_context* ctx, md_adjoint** out);
 MD_API int md_adjoint_destroy(md_adjoint* adj);
 MD_API int md_adjoint_forward(md_adjoint* adj, md_system* sys, const md_lj* lj, double dt,

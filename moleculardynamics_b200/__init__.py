@@ -1169,6 +1169,7 @@ class AdjointTrajectory:
         self._h = h
         self.n = 0
         self.steps = 0
+        self._sys = None
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -1180,6 +1181,7 @@ class AdjointTrajectory:
         _check(lib().md_adjoint_forward(self._h, sys.handle, lj.handle, float(dt), int(steps),
                                         int(every), float(skin), _ptr(rows)))
         self.n, self.steps = sys.n, int(steps)
+        self._sys = sys  # backward() replays on this system: keep it alive
         return rows
 
     def backward(self, grad_rows):

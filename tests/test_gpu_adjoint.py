@@ -141,3 +141,31 @@ def test_backward_leaves_forward_state_and_checks_skin(md):
     s2 = md.System.from_arrays(pos, box, vel=vel * 3.0, mass=mass)
     with pytest.raises(md.MDError, match="larger skin"):
         md.AdjointTrajectory().forward(s2, md.LennardJones(1.0, 1.0, 2.5, 1), DT, 60, 60, 0.05)
+
+
+def test_adjoint_long_trajectory_matches_differences(md):
+    """A 400-step trajectory of the 32,000-atom lattice (fcc 20^3, force-shifted LJ,
+    list skin 2.0, states saved every 50 steps): the adjoint d loss / d(epsilon,
+    sigma) against central differences at h = 1e-7.  Longer trajectories diverge
+    (the differences themselves stop converging near 1000 steps).  The forward's
+    system is not kept by the caller: backward() must still replay on it."""
+    import gc
+    st = md.fcc_lattice(20, 0.8442, 0.722, 2026)
+    pos, vel, mass, box = st["pos"], st["vel"], st["mass"], st["box"]
+    n, vol = pos.shape[0], float(np.prod(box))
+    steps, every, skin, h = 400, 50, 2.0, 1e-7
+
+    def run(sigma=1.0, eps=1.0):
+        traj = md.AdjointTrajectory()
+        rows = traj.forward(md.System.from_arrays(pos, box, vel=vel, mass=mass),
+                            md.LennardJones(sigma, eps, 2.5, 1), DT, steps, every, skin)
+        return rows, traj
+
+    rows, traj = run()
+    gc.collect()
+    d_eps, d_sig, _, _ = traj.backward(loss_grad_rows(rows, n, vol))
+    fd_eps = (loss_of(run(eps=1 + h)[0], n, vol)[0] - loss_of(run(eps=1 - h)[0], n, vol)[0]) / (2 * h)
+    fd_sig = (loss_of(run(sigma=1 + h)[0], n, vol)[0] -
+              loss_of(run(sigma=1 - h)[0], n, vol)[0]) / (2 * h)
+    assert rel(d_eps, fd_eps) < 1e-6, (d_eps, fd_eps)
+    assert rel(d_sig, fd_sig) < 1e-6, (d_sig, fd_sig)
