@@ -494,7 +494,6 @@ int md_lj_hvp(const md_lj* lj, md_system* sys, md_verlet* list, const double* u,
     if (!lj || !sys || !list || !u || !out)
         return fail(MD_ERR_INVALID_ARGUMENT, "md_lj_hvp: NULL argument");
     MDB_TRY(verlet_ensure_ready(list, sys, "md_lj_hvp"));
-    MDB_TRY(verlet_int_rows_async(list, sys));  // the pair loop reads int32 rows
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     if (n == 0) {

@@ -1377,7 +1377,6 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
     // halo tiles, when the list keeps them (fused runs of large systems turn them on,
     // or md_verlet_set_halo)
     const bool halo = mixed && lj->halo && sys->n > 0 && v->halo_on && v->stride % 8 == 0;
-    if (!halo && v->halo_on) MDB_TRY(verlet_int_rows_async(v, sys));
     ctx_time_begin(ctx, MD_KERNEL_LJ_FORCE);
     const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
     if (halo && cubic && lj->tile_tpa > 1) {

@@ -256,7 +256,6 @@ struct md_verlet {
     int* d_rebuild_flag = nullptr; // device: set by the displacement check
     int* d_rebuild_total = nullptr; // device: rebuilds done inside fused loops
     int* d_max_count = nullptr;     // device: largest row seen by the last build
-    int* d_rows_state = nullptr;    // device: 1 = int32 rows of staged tiles not current
     // Halo tiles (mixed-precision force path): per block of kHaloAtoms sorted
     // atoms, runs of the cells around them and the rows as 16-bit halo slots.
     bool halo_on = false;
@@ -286,10 +285,6 @@ bool verlet_halo_ready(md_verlet* v, md_system* sys);
 // The fused-run policy above, for a mixed-precision LJ force field.
 void verlet_halo_for_run(md_verlet* v, md_system* sys, const md_lj* lj);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
-// A list with halo tiles keeps the rows of staged tiles as 16-bit slots only; this
-// restores their int32 rows (a gated no-op when they are current).  Every user of
-// the int32 rows of such a list calls it first.
-int verlet_int_rows_async(md_verlet* v, md_system* sys);
 int verlet_check(md_verlet* v, md_system* sys);  // device flag <- needs rebuild
 int verlet_ensure_capacity(md_verlet* v, md_system* sys);
 }  // namespace mdb

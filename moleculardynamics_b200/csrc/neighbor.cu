@@ -24,7 +24,7 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kBuildWarps = 4;
-constexpr int kMaxCand = 512;    // candidates staged per warp window (even)
+constexpr int kMaxCand = 576;    // candidates staged per warp window (even)
 
 __device__ __forceinline__ bool gate(const int* flag) { return flag == nullptr || *flag != 0; }
 
@@ -299,49 +299,16 @@ __device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, do
 // pair set (forEachPair) applies the reference's exact test to the positions of
 // the build and is bit-identical to the reference's.
 // Rows list candidates in stencil order, atoms of a cell in sorted order.
-//
-// With halo tiles (HaloRows.meta set, the tiles planned before the build), an atom
-// of a staged tile gets its row as 16-bit byte offsets of the candidates' slots in
-// its tile (nbr16) instead of int32 indices: slot = the slot of the candidate
-// cell's first atom in that tile + the candidate's offset in its cell.  A lane
-// keeps its atom's last 8 slots in shared memory and writes them with one 16-byte
-// store; the row's last chunk is padded with the atom's own slot.  Atoms of tiles
-// that are not staged get int32 rows.  *rows_state = 1 then says that the int32
-// rows of staged tiles are not current (verlet_int_rows rebuilds them on demand).
-struct HaloRows {
-    const int2* meta = nullptr;   // per tile: runs (or <= 0: not staged), slots
-    const int2* runs = nullptr;   // per tile kHaloRuns: (first atom, first slot)
-    uint16_t* nbr16 = nullptr;
-    int* rows_state = nullptr;
-};
-
-// Byte offset (slot * 16) of the first atom `beg` of a cell within tile t's halo.
-__device__ __forceinline__ unsigned cell_slot_offset(const HaloRows& h, int t, int nr, int beg) {
-    const int2* tr = h.runs + static_cast<int64_t>(t) * kHaloRuns;
-    int lo = 0, hi = nr;  // the last run whose first atom is <= beg
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(&tr[mid].x) <= beg) lo = mid;
-        else hi = mid;
-    }
-    const int2 r = tr[lo];
-    return static_cast<unsigned>(r.y + (beg - r.x)) << 4;
-}
-
 __global__ void __launch_bounds__(kBuildWarps * 32)
 k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
                double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
-               uint32_t* status, int* max_count, const int* flag, int groups, HaloRows hr) {
+               uint32_t* status, int* max_count, const int* flag, int groups) {
     if (!gate(flag)) return;
     // Candidates in pairs, structure-of-arrays within a pair so that two
     // candidates are tested with one packed FP32x2 instruction per step:
     // s_a[p] = (-x0, -x1, -y0, -y1), s_b[p] = (-z0, -z1, j0, j1).
     __shared__ float4 s_a[kBuildWarps][kMaxCand / 2];
     __shared__ float4 s_b[kBuildWarps][kMaxCand / 2];
-    // halo rows: the candidates' slot offsets in the cell's first and last tile (low
-    // and high 16 bits), and each lane's last 8 slots
-    __shared__ unsigned s_s[kBuildWarps][kMaxCand];
-    __shared__ uint4 s_ring[kBuildWarps][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // `groups` warps share a crowded cell, each taking every groups-th run of 32 atoms
     const int wid = blockIdx.x * kBuildWarps + warp;
@@ -379,21 +346,6 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     const int excl = incl - cnt;
     const int a0 = start[r], a1 = start[r + 1];
     int local_max = 0;
-    // halo rows: the tiles of the cell's first and last atom, whether each is staged,
-    // and (lane q) the slot offset of stencil cell q's first atom in each
-    const bool halo = hr.meta != nullptr && a1 > a0;
-    const int t_lo = a0 / kHaloAtoms, t_hi = halo ? (a1 - 1) / kHaloAtoms : t_lo;
-    const int2 m_lo = halo ? hr.meta[t_lo] : make_int2(0, 0);
-    const int2 m_hi = halo ? hr.meta[t_hi] : make_int2(0, 0);
-    const bool st_lo = halo && m_lo.x > 0, st_hi = halo && m_hi.x > 0;
-    unsigned cs_lo = 0u, cs_hi = 0u;
-    if (lane < 27) {
-        if (st_lo) cs_lo = cell_slot_offset(hr, t_lo, m_lo.x, beg);
-        if (st_hi) cs_hi = cell_slot_offset(hr, t_hi, m_hi.x, beg);
-    }
-    // one atom per lane (the usual cell): the ring holds its slots across windows
-    const bool ring_ok = groups == 1 && a1 - a0 <= 32;
-    if (hr.meta && hr.rows_state && lane == 0 && blockIdx.x == 0 && warp == 0) *hr.rows_state = 1;
     for (int wb = 0; wb < total; wb += kMaxCand) {
         const int wlen = min(kMaxCand, total - wb);
         __syncwarp();
@@ -405,8 +357,6 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
             const int qb = __shfl_sync(0xffffffffu, beg, q);
             const int qo = __shfl_sync(0xffffffffu, excl, q);
             const int qc = __shfl_sync(0xffffffffu, cnt, q);
-            const unsigned qcs_lo = __shfl_sync(0xffffffffu, cs_lo, q);
-            const unsigned qcs_hi = __shfl_sync(0xffffffffu, cs_hi, q);
             const int lo = max(qo, wb), hi = min(qo + qc, wb + wlen);
             for (int gb = lo; gb < hi; gb += 32) {
                 const int gt = gb + lane;
@@ -435,10 +385,6 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                     A[2 + h] = -static_cast<float>(vy);
                     B[h] = -static_cast<float>(vz);
                     B[2 + h] = __int_as_float(j);
-                    if (halo) {
-                        const unsigned d = static_cast<unsigned>(gt - qo) << 4;
-                        s_s[warp][tt] = ((qcs_lo + d) & 0xffffu) | ((qcs_hi + d) << 16);
-                    }
                 }
                 ns += __popc(m);
             }
@@ -468,98 +414,28 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
                 c = wb == 0 ? 0 : count[i];
             }
             int* row = nbr + static_cast<int64_t>(active ? i : 0) * stride;
-            // this atom's tile: staged ones take 16-bit slot rows
-            const int ti = i / kHaloAtoms;
-            const bool slots = active && ((ti == t_lo && st_lo) || (ti == t_hi && st_hi));
-            const int shift = ti == t_lo ? 0 : 16;
-            uint16_t* row16 = slots ? hr.nbr16 + static_cast<int64_t>(i) * stride : nullptr;
-            uint16_t* ring = reinterpret_cast<uint16_t*>(&s_ring[warp][lane]);
             // Per candidate pair: packed FP32x2 distances and predicated appends.
             const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy),
                          fz2 = make_float2(fz, fz);
             const int npairs = (ns + 1) >> 1;
-            if (!slots) {
 #pragma unroll 2
-                for (int pr = 0; pr < npairs; ++pr) {
-                    const float4 A = s_a[warp][pr], B = s_b[warp][pr];
-                    const float2 dx = __fadd2_rn(fx2, make_float2(A.x, A.y));
-                    const float2 dy = __fadd2_rn(fy2, make_float2(A.z, A.w));
-                    const float2 dz = __fadd2_rn(fz2, make_float2(B.x, B.y));
-                    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                    const int j0 = __float_as_int(B.z), j1 = __float_as_int(B.w);
-                    const bool h0 = active && r2.x < hi_thr && j0 != i;
-                    const bool h1 = active && r2.y < hi_thr && j1 != i;
-                    if (h0 && c < stride) row[c] = j0;
-                    c += h0 ? 1 : 0;
-                    if (h1 && c < stride) row[c] = j1;
-                    c += h1 ? 1 : 0;
-                }
-            } else {
-                const uint2* sw = reinterpret_cast<const uint2*>(s_s[warp]);
-#pragma unroll 2
-                for (int pr = 0; pr < npairs; ++pr) {
-                    const float4 A = s_a[warp][pr], B = s_b[warp][pr];
-                    const float2 dx = __fadd2_rn(fx2, make_float2(A.x, A.y));
-                    const float2 dy = __fadd2_rn(fy2, make_float2(A.z, A.w));
-                    const float2 dz = __fadd2_rn(fz2, make_float2(B.x, B.y));
-                    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                    const int j0 = __float_as_int(B.z), j1 = __float_as_int(B.w);
-                    const bool h0 = r2.x < hi_thr && j0 != i;
-                    const bool h1 = r2.y < hi_thr && j1 != i;
-                    if (h0 || h1) {
-                        const uint2 w = sw[pr];
-                        const uint16_t o0 = static_cast<uint16_t>(w.x >> shift);
-                        const uint16_t o1 = static_cast<uint16_t>(w.y >> shift);
-                        if (ring_ok) {
-                            if (h0 && c < stride) {
-                                ring[c & 7] = o0;
-                                if ((c & 7) == 7)
-                                    reinterpret_cast<uint4*>(row16)[c >> 3] = s_ring[warp][lane];
-                            }
-                            c += h0 ? 1 : 0;
-                            if (h1 && c < stride) {
-                                ring[c & 7] = o1;
-                                if ((c & 7) == 7)
-                                    reinterpret_cast<uint4*>(row16)[c >> 3] = s_ring[warp][lane];
-                            }
-                            c += h1 ? 1 : 0;
-                        } else {
-                            if (h0 && c < stride) row16[c] = o0;
-                            c += h0 ? 1 : 0;
-                            if (h1 && c < stride) row16[c] = o1;
-                            c += h1 ? 1 : 0;
-                        }
-                    }
-                }
+            for (int pr = 0; pr < npairs; ++pr) {
+                const float4 A = s_a[warp][pr], B = s_b[warp][pr];
+                const float2 dx = __fadd2_rn(fx2, make_float2(A.x, A.y));
+                const float2 dy = __fadd2_rn(fy2, make_float2(A.z, A.w));
+                const float2 dz = __fadd2_rn(fz2, make_float2(B.x, B.y));
+                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                const int j0 = __float_as_int(B.z), j1 = __float_as_int(B.w);
+                const bool h0 = active && r2.x < hi_thr && j0 != i;
+                const bool h1 = active && r2.y < hi_thr && j1 != i;
+                if (h0 && c < stride) row[c] = j0;
+                c += h0 ? 1 : 0;
+                if (h1 && c < stride) row[c] = j1;
+                c += h1 ? 1 : 0;
             }
             if (active) {
                 count[i] = c;
                 local_max = max(local_max, c);
-            }
-        }
-    }
-    if (halo && (st_lo || st_hi)) {
-        // pad the last 8-entry chunk of each slot row with the atom's own slot
-        // (stencil cell 13 is the home cell)
-        const unsigned self_lo = __shfl_sync(0xffffffffu, cs_lo, 13);
-        const unsigned self_hi = __shfl_sync(0xffffffffu, cs_hi, 13);
-        for (int ib = a0 + 32 * grp; ib < a1; ib += 32 * groups) {
-            const int i = ib + lane;
-            if (i >= a1) continue;
-            const int ti = i / kHaloAtoms;
-            const bool slots = (ti == t_lo && st_lo) || (ti == t_hi && st_hi);
-            if (!slots) continue;
-            const int c = min(count[i], stride);
-            if ((c & 7) == 0) continue;
-            const uint16_t self = static_cast<uint16_t>(
-                (ti == t_lo ? self_lo : self_hi) + (static_cast<unsigned>(i - a0) << 4));
-            uint16_t* row16 = hr.nbr16 + static_cast<int64_t>(i) * stride;
-            if (ring_ok) {
-                uint16_t* ring = reinterpret_cast<uint16_t*>(&s_ring[warp][lane]);
-                for (int e = c & 7; e < 8; ++e) ring[e] = self;
-                reinterpret_cast<uint4*>(row16)[c >> 3] = s_ring[warp][lane];
-            } else {
-                for (int e = c; e < ((c + 7) & ~7); ++e) row16[e] = self;
             }
         }
     }
@@ -811,43 +687,6 @@ k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stri
     if (__syncthreads_or(bad) && tid == 0) meta[b].x = -1;
 }
 
-// The int32 rows of staged tiles back from their 16-bit slot rows (the build of a
-// list with halo tiles writes only the slots there), when *state says they are
-// not current: slot -> the run holding it -> atom.  One CTA per tile.
-__global__ void __launch_bounds__(kRowsThreads)
-k_rows_from_slots(const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride,
-                  int64_t n, const int2* __restrict__ runs, const int2* __restrict__ meta,
-                  int* __restrict__ nbr, const int* state) {
-    if (*state == 0) return;
-    __shared__ int s_beg[kHaloRuns], s_base[kHaloRuns];
-    const int b = blockIdx.x, tid = threadIdx.x;
-    const int2 m = meta[b];
-    if (m.x <= 0) return;
-    if (tid < m.x) {
-        const int2 r = runs[static_cast<int64_t>(b) * kHaloRuns + tid];
-        s_beg[tid] = r.x;
-        s_base[tid] = r.y;
-    }
-    __syncthreads();
-    const int64_t i = static_cast<int64_t>(b) * kHaloAtoms + (tid >> 2);
-    if (i >= n) return;
-    const int c = min(count[i], stride);
-    const uint16_t* src = nbr16 + i * stride;
-    int* dst = nbr + i * stride;
-    for (int e = tid & 3; e < c; e += 4) {
-        const int sl = src[e] >> 4;
-        int t = 0;
-#pragma unroll
-        for (int step = kHaloRuns / 2; step > 0; step >>= 1) {
-            const int mid = t + step;
-            t = mid < m.x && s_base[mid] <= sl ? mid : t;
-        }
-        dst[e] = s_beg[t] + (sl - s_base[t]);
-    }
-}
-
-__global__ void k_clear_int(int* p) { *p = 0; }
-
 __global__ void k_store_ref(const double4* __restrict__ pos, double4* ref, int64_t n,
                             const int* flag, int* total) {
     if (!gate(flag)) return;
@@ -1080,26 +919,11 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
         const double mean = static_cast<double>(n) / v->grid.ncells;
         const int groups = static_cast<int>(std::min(16.0, std::max(1.0, std::ceil(1.5 * mean / 32.0))));
         const int64_t warps = static_cast<int64_t>(v->grid.ncells) * groups;
-        // With halo tiles the tiles are planned first, so that the build writes the
-        // rows of staged tiles as 16-bit slots itself (no conversion pass).
-        HaloRows hr;
-        if (v->halo_on && n > 0) {
-            if (v->stride % 8 != 0) {  // slot rows are read 16 bytes at a time
-                v->halo_on = false;
-                graph_epoch_bump();
-            } else {
-                MDB_TRY(halo_alloc(v, n));
-                halo_plan(v, sys, flag);
-                hr.meta = v->halo_meta.as<int2>();
-                hr.runs = v->halo_runs.as<int2>();
-                hr.nbr16 = v->nbr16.as<uint16_t>();
-                hr.rows_state = v->d_rows_state;
-            }
-        }
         k_verlet_cells<<<grid_for(warps, kBuildWarps), kBuildWarps * 32, 0, ctx->stream>>>(
             sys->cur.pos, start, g, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
-            ctx->d_status, v->d_max_count, flag, groups, hr);
+            ctx->d_status, v->d_max_count, flag, groups);
         ++ctx->launches;
+        if (v->halo_on && n > 0) MDB_TRY(halo_build(v, sys, flag));
     } else if (n > 0) {
         k_verlet_brute<<<grid_for(n * 32, kBlock), kBlock, 0, ctx->stream>>>(
             sys->cur.pos, n, box, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
@@ -1120,7 +944,10 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
     if (!conditional) {
         // Host-driven build: retry with a larger stride until no row overflows.
         for (int attempt = 0; attempt < 8; ++attempt) {
-            MDB_TRY(verlet_build_impl(v, sys, nullptr));
+            ctx_time_begin(sys->ctx, MD_KERNEL_NEIGHBOR);
+            const int rc = verlet_build_impl(v, sys, nullptr);
+            ctx_time_end(sys->ctx, MD_KERNEL_NEIGHBOR);
+            MDB_TRY(rc);
             int mx = 0;
             MDB_CUDA(cudaMemcpyAsync(&mx, v->d_max_count, sizeof(int), cudaMemcpyDeviceToHost,
                                      sys->ctx->stream));
@@ -1146,18 +973,6 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
         return MD_OK;
     }
     return verlet_build_impl(v, sys, v->d_rebuild_flag);
-}
-
-int verlet_int_rows_async(md_verlet* v, md_system* sys) {
-    if (!v->halo_on || sys->n <= 0 || !v->halo_meta.ptr) return MD_OK;
-    md_context* ctx = sys->ctx;
-    k_rows_from_slots<<<static_cast<unsigned>(halo_blocks(sys->n)), kRowsThreads, 0, ctx->stream>>>(
-        v->nbr16.as<uint16_t>(), v->count.as<int>(), v->stride, sys->n, v->halo_runs.as<int2>(),
-        v->halo_meta.as<int2>(), v->nbr.as<int>(), v->d_rows_state);
-    k_clear_int<<<1, 1, 0, ctx->stream>>>(v->d_rows_state);
-    ctx->launches += 2;
-    MDB_CHECK_LAUNCH();
-    return MD_OK;
 }
 
 bool verlet_halo_ready(md_verlet* v, md_system* sys) {
@@ -1424,7 +1239,6 @@ int md_verlet_create(md_context* ctx, const double box[3], double cutoff, double
             v->d_rebuild_flag = flags;
             v->d_rebuild_total = flags + 1;
             v->d_max_count = flags + 2;
-            v->d_rows_state = flags + 3;
         }
     }
     if (rc != MD_OK) {
@@ -1504,9 +1318,6 @@ int md_verlet_set_halo(md_verlet* v, int on) {
     graph_epoch_bump();
     if (!v) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_set_halo: NULL");
     if (!on) {
-        // the int32 rows of staged tiles are current again before the slots go
-        if (v->halo_on && v->sys && verlet_ready(v, v->sys, "md_verlet_set_halo") == MD_OK)
-            MDB_TRY(verlet_int_rows_async(v, v->sys));
         v->halo_on = false;
         return MD_OK;
     }
@@ -1583,7 +1394,6 @@ int md_verlet_pairs(md_verlet* v, int64_t* pi, int64_t* pj, int64_t cap, int64_t
     md_system* sys = v->sys;
     if (!sys) return fail(MD_ERR_INVALID_ARGUMENT, "md_verlet_pairs: list was never built");
     MDB_TRY(verlet_ready(v, sys, "md_verlet_pairs"));
-    MDB_TRY(verlet_int_rows_async(v, sys));
     md_context* ctx = v->ctx;
     const int64_t n = sys->n;
     if (n == 0) {
