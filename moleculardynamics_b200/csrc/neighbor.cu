@@ -12,6 +12,7 @@
 // uses the reference's exact min-image r^2 with the pair ordered by original index
 // (r_lo - r_hi), so the pair set is bit-identical to the reference's.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <new>
 
@@ -612,44 +613,58 @@ k_halo_plan(const int* __restrict__ start, GridArgs g, int64_t n, int64_t tiles,
 
 // Rows of a planned tile as 16-bit byte offsets of 16-byte slots (slot = base of
 // the run holding j + j - the run's first atom; kHaloCap * 16 < 2^16), the last
-// 8-entry chunk padded with the atom's own slot: four
-// threads per atom, eight entries per 16-byte access, two accesses in flight.  A
-// neighbour outside the tile's runs (not possible for a list built from the same
-// cells) un-stages the tile.
+// 8-entry chunk padded with the atom's own slot (r^2 = 0, which the force kernels
+// skip, so they read whole chunks without a count test).  Four threads per atom,
+// one 8-entry chunk (two 16-byte loads, one 16-byte store) per step.  A neighbour
+// outside the tile's runs (not possible for a list built from the same cells)
+// un-stages the tile.
 constexpr int kRowsThreads = 4 * kHaloAtoms;
 
-// The run holding j by a fixed six-step search (kHaloRuns = 64), predicated rather
-// than branched so that the lanes of a warp stay together.
-__device__ __forceinline__ unsigned halo_slot(int j, int nr, const int* s_beg, const int* s_base,
-                                              bool& bad) {
+struct HaloRun {
+    int shift;  // first atom - first slot: slot = j - shift
+    int base;   // first slot
+    int len;    // atoms in the run
+    int pad;
+};
+
+// The run holding j: six fixed steps over first atoms padded with INT_MAX to
+// kHaloRuns entries (no bounds test), then one 16-byte read of the run.
+__device__ __forceinline__ unsigned halo_slot(int j, const int* s_beg, const HaloRun* s_run,
+                                              bool& ok) {
     int t = 0;
 #pragma unroll
-    for (int step = kHaloRuns / 2; step > 0; step >>= 1) {
-        const int mid = t + step;
-        t = mid < nr && s_beg[mid] <= j ? mid : t;
-    }
-    const int off = j - s_beg[t];
-    const bool ok = off >= 0 && off < s_base[t + 1] - s_base[t];
-    bad = bad || !ok;
-    return ok ? static_cast<unsigned>(s_base[t] + off) << 4 : 0u;
+    for (int step = kHaloRuns / 2; step > 0; step >>= 1) t += s_beg[t + step] <= j ? step : 0;
+    const HaloRun r = s_run[t];
+    const int slot = j - r.shift;
+    ok = static_cast<unsigned>(slot - r.base) < static_cast<unsigned>(r.len);
+    return static_cast<unsigned>(slot) << 4;
 }
 
 __global__ void __launch_bounds__(kRowsThreads)
 k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
             const int2* __restrict__ runs, int2* meta, uint16_t* __restrict__ nbr16,
             const int* flag) {
+    static_assert(kRowsThreads >= kHaloRuns, "one thread per run");
     if (!gate(flag)) return;
-    __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
+    __shared__ int s_beg[kHaloRuns];
+    __shared__ HaloRun s_run[kHaloRuns];
     const int b = blockIdx.x, tid = threadIdx.x;
     const int2 m = meta[b];
     if (m.x <= 0) return;
     const int nr = m.x;
-    if (tid < nr) {
-        const int2 r = runs[static_cast<int64_t>(b) * kHaloRuns + tid];
-        s_beg[tid] = r.x;
-        s_base[tid] = r.y;
+    if (tid < kHaloRuns) {
+        const int2* tr = runs + static_cast<int64_t>(b) * kHaloRuns;
+        int beg = INT_MAX;
+        HaloRun hr{0, 0, 0, 0};
+        if (tid < nr) {
+            const int2 r = tr[tid];
+            const int next = tid + 1 < nr ? tr[tid + 1].y : m.y;
+            beg = r.x;
+            hr = HaloRun{r.x - r.y, r.y, next - r.y, 0};
+        }
+        s_beg[tid] = beg;
+        s_run[tid] = hr;
     }
-    if (tid == 0) s_base[nr] = m.y;
     __syncthreads();
     const int64_t i = static_cast<int64_t>(b) * kHaloAtoms + (tid >> 2);
     bool bad = false;
@@ -657,31 +672,23 @@ k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stri
         const int c = min(count[i], stride);
         const int4* src = reinterpret_cast<const int4*>(nbr + i * stride);
         uint4* dst = reinterpret_cast<uint4*>(nbr16 + i * stride);
-        // the last chunk is padded with the atom's own slot (r^2 = 0), which the
-        // force kernels skip, so they read whole chunks without a count test
-        const unsigned self = halo_slot(static_cast<int>(i), nr, s_beg, s_base, bad);
-        for (int ch = tid & 3; 8 * ch < c; ch += 8) {
-            const int ch2 = ch + 4;
-            const bool two = 8 * ch2 < c;
+        bool ok_self;
+        const unsigned self = halo_slot(static_cast<int>(i), s_beg, s_run, ok_self);
+        bad = !ok_self;
+        for (int ch = tid & 3; 8 * ch < c; ch += 4) {
             const int4 a0 = __ldg(src + 2 * ch), a1 = __ldg(src + 2 * ch + 1);
-            int4 b0 = make_int4(0, 0, 0, 0), b1 = b0;
-            if (two) {
-                b0 = __ldg(src + 2 * ch2);
-                b1 = __ldg(src + 2 * ch2 + 1);
-            }
-            const int js[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
-                                b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-            unsigned off[16];
+            const int js[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            unsigned off[8];
 #pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const int e = 8 * (k < 8 ? ch : ch2) + (k & 7);
-                off[k] = e < c ? halo_slot(js[k], nr, s_beg, s_base, bad) : self;
+            for (int k = 0; k < 8; ++k) {
+                const bool in_row = 8 * ch + k < c;
+                bool ok;
+                const unsigned o = halo_slot(in_row ? js[k] : static_cast<int>(i), s_beg, s_run, ok);
+                off[k] = in_row ? o : self;
+                bad = bad || (in_row && !ok);
             }
             dst[ch] = make_uint4(off[0] | (off[1] << 16), off[2] | (off[3] << 16),
                                  off[4] | (off[5] << 16), off[6] | (off[7] << 16));
-            if (two)
-                dst[ch2] = make_uint4(off[8] | (off[9] << 16), off[10] | (off[11] << 16),
-                                      off[12] | (off[13] << 16), off[14] | (off[15] << 16));
         }
     }
     if (__syncthreads_or(bad) && tid == 0) meta[b].x = -1;
