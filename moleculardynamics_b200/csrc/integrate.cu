@@ -357,14 +357,29 @@ int pre_force(md_integrator* it, md_system* sys, md_verlet* check, bool fresh_ke
     return MD_OK;
 }
 
-int post_force_async(md_integrator* it, md_system* sys, bool apply_scale) {
+// The closing half-kick for a force kernel to apply (the kick of post_force_async).
+KickArgs kick_args(const md_integrator* it, md_system* sys) {
+    KickArgs k;
+    k.vx = sys->cur.vx;
+    k.vy = sys->cur.vy;
+    k.vz = sys->cur.vz;
+    k.mass = sys->cur.mass;
+    k.inv_mass = sys->cur.inv_mass;
+    k.half_dt = step_args(it, sys).half_dt;
+    k.status = sys->ctx->d_status;
+    return k;
+}
+
+// The step's end: the closing half-kick with the kinetic energy (unless the force
+// kernel took it: `kicked`), then the chain half of a Nose-Hoover integrator.
+int post_force_async(md_integrator* it, md_system* sys, bool apply_scale, bool kicked = false) {
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     StepArgs s = step_args(it, sys);
     const int g = kick_grid(sys);
     double* part;
     MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
-    if (n > 0) {
+    if (n > 0 && !kicked) {
         k_kick_ke<<<g, kBlock, 0, ctx->stream>>>(sys->cur, n, s, part, ctx_counter(ctx, 3),
                                                 ctx_result(ctx, kResKE), ctx->d_status);
         ++ctx->launches;
@@ -475,8 +490,11 @@ int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, do
     MDB_TRY(step_quantize_target(it, sys, lj, &q));
     MDB_TRY(pre_force(it, sys, v, first, q));
     MDB_TRY(verlet_build(v, sys, true));
-    MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr));
-    MDB_TRY(post_force_async(it, sys, false));
+    const KickArgs ka = kick_args(it, sys);
+    bool kicked = false;
+    MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr, false, &ka,
+                                   &kicked));
+    MDB_TRY(post_force_async(it, sys, false, kicked));
     if (rows) {
         k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy), ctx_result(ctx, kResKE),
                                               nhc_of(it), rows, idx);
@@ -530,8 +548,11 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
     const int64_t l2 = ctx->launches;
     if (rc == MD_OK)
         rc = capture_into(ctx, graph, &cond, 1, [&]() -> int {
-            MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr, q != nullptr));
-            MDB_TRY(post_force_async(it, sys, false));
+            const KickArgs ka = kick_args(it, sys);
+            bool kicked = false;
+            MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr,
+                                           q != nullptr, &ka, &kicked));
+            MDB_TRY(post_force_async(it, sys, false, kicked));
             if (rows) {
                 k_record_at<<<1, 1, 0, ctx->stream>>>(ctx_result(ctx, kResEnergy),
                                                       ctx_result(ctx, kResKE), nhc, rows, idx);

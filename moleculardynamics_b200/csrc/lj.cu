@@ -487,13 +487,13 @@ __device__ __noinline__ PairSums gathered_row(LJArgs a, Box3 box, const double4*
 // around it) walks its int32 row with global gathers.  Pair arithmetic, the
 // exact decision of pairs next to the cutoff and the accumulation order are
 // those of k_lj_verlet's mixed path.
-template <bool LFS, int U, bool CUBIC>
+template <bool LFS, int U, bool CUBIC, bool KICK>
 __global__ void __launch_bounds__(kBlock, 4)
 k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int* __restrict__ nbr,
           const uint16_t* __restrict__ nbr16, const int* __restrict__ count, int stride, int64_t n,
           const int2* __restrict__ runs, const int2* __restrict__ meta, Box3 box, LJArgs a,
           double* __restrict__ fxo, double* __restrict__ fyo, double* __restrict__ fzo,
-          double* part, unsigned* ticket, double* out) {
+          double* part, unsigned* ticket, double* out, KickArgs kick) {
     constexpr int TPA = kBlock / kHaloAtoms;
     extern __shared__ int4 s_q[];  // kHaloCap slots
     __shared__ int s_beg[kHaloRuns + 1], s_base[kHaloRuns + 1];
@@ -588,13 +588,29 @@ k_lj_halo(const int4* __restrict__ q, const double4* __restrict__ pd, const int*
         fy += __shfl_xor_sync(0xffffffffu, fy, o);
         fz += __shfl_xor_sync(0xffffffffu, fz, o);
     }
+    double ke = 0.0;
     if (i < n && g == 0) {
         fxo[i] = fx;
         fyo[i] = fy;
         fzo[i] = fz;
+        if constexpr (KICK) {  // the closing half-kick, as the separate kick kernel does it
+            const double c = __dmul_rn(kick.half_dt, kick.inv_mass[i]);
+            const double vx = fma(c, fx, kick.vx[i]);
+            const double vy = fma(c, fy, kick.vy[i]);
+            const double vz = fma(c, fz, kick.vz[i]);
+            kick.vx[i] = vx;
+            kick.vy[i] = vy;
+            kick.vz[i] = vz;
+            ke = 0.5 * kick.mass[i] * (vx * vx + vy * vy + vz * vz);
+        }
     }
-    double v[2] = {e, vir};
-    grid_reduce<2>(v, part, ticket, out);
+    if constexpr (KICK) {  // energy, virial and kinetic energy (result slots 0, 1, 2)
+        double v[3] = {e, vir, ke};
+        grid_reduce<3>(v, part, ticket, out, kick.status);
+    } else {
+        double v[2] = {e, vir};
+        grid_reduce<2>(v, part, ticket, out);
+    }
 }
 
 // ------------------------------------------------------------ k_lj_tile
@@ -1220,14 +1236,16 @@ __global__ void k_quantize(const double4* __restrict__ pos, int64_t n, double sx
 
 template <bool LFS, int U>
 void launch_halo(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
-                 double* out) {
+                 double* out, const KickArgs* kick) {
     const unsigned blocks = static_cast<unsigned>(halo_blocks(sys->n));
     const bool cubic = a.res[0] == a.res[1] && a.res[0] == a.res[2];
-    auto kernel = cubic ? k_lj_halo<LFS, U, true> : k_lj_halo<LFS, U, false>;
+    auto kernel = kick ? (cubic ? k_lj_halo<LFS, U, true, true> : k_lj_halo<LFS, U, false, true>)
+                       : (cubic ? k_lj_halo<LFS, U, true, false> : k_lj_halo<LFS, U, false, false>);
     kernel<<<blocks, kBlock, kHaloCap * sizeof(int4), sys->ctx->stream>>>(
         sys->qpos.as<int4>(), sys->cur.pos, v->nbr.as<int>(), v->nbr16.as<uint16_t>(),
         v->count.as<int>(), v->stride, sys->n, v->halo_runs.as<int2>(), v->halo_meta.as<int2>(),
-        box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+        box_of(sys), a, sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out,
+        kick ? *kick : KickArgs{});
 }
 
 UnitConst unit_const(const LJArgs& a) {
@@ -1292,11 +1310,11 @@ void launch_tile(int tpa, md_system* sys, md_verlet* v, const LJArgs& a, double*
 
 template <bool LFS>
 void launch_halo_u(int unroll, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
-                   unsigned* ticket, double* out) {
+                   unsigned* ticket, double* out, const KickArgs* kick) {
     switch (unroll) {
-        case 1: launch_halo<LFS, 1>(sys, v, a, part, ticket, out); break;
-        case 4: launch_halo<LFS, 4>(sys, v, a, part, ticket, out); break;
-        default: launch_halo<LFS, 2>(sys, v, a, part, ticket, out); break;
+        case 1: launch_halo<LFS, 1>(sys, v, a, part, ticket, out, kick); break;
+        case 4: launch_halo<LFS, 4>(sys, v, a, part, ticket, out, kick); break;
+        default: launch_halo<LFS, 2>(sys, v, a, part, ticket, out, kick); break;
     }
 }
 
@@ -1361,14 +1379,15 @@ int lj_quantize_async(md_lj* lj, md_system* sys, const int* gate) {
 }
 
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q_gate,
-                           bool q_current) {
+                           bool q_current, const KickArgs* kick, bool* kicked) {
+    if (kicked) *kicked = false;
     md_context* ctx = sys->ctx;
     const LJArgs a = verlet_lj_args(lj, sys);
     const int tpa = lj->tpa ? lj->tpa : g_lj_tpa, unroll = lj->unroll ? lj->unroll : g_lj_unroll;
     const int64_t threads = std::max<int64_t>(sys->n * tpa, 1);
     const int64_t blocks = std::max<int64_t>(grid_for(threads, kBlock), halo_blocks(sys->n));
     double* part;
-    MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+    MDB_TRY(ctx_partials(ctx, 3 * static_cast<size_t>(blocks), &part));
     unsigned* ticket = ctx_counter(ctx, 2);
     double* out = ctx_result(ctx, kResEnergy);
     const bool lfs = lj->truncation == MD_LINEAR_FORCE_SHIFT;
@@ -1386,8 +1405,10 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
         if (lfs) launch_tile1<true>(sys, v, a, part, ticket, out);
         else launch_tile1<false>(sys, v, a, part, ticket, out);
     } else if (halo) {
-        if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out);
-        else launch_halo_u<false>(unroll, sys, v, a, part, ticket, out);
+        // the default halo kernel also takes the closing half-kick when asked
+        if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out, kick);
+        else launch_halo_u<false>(unroll, sys, v, a, part, ticket, out, kick);
+        if (kick && kicked) *kicked = true;
     } else if (mixed) {
         if (lfs) launch_verlet_tpa<true, true>(tpa, unroll, sys, v, a, part, ticket, out);
         else launch_verlet_tpa<true, false>(tpa, unroll, sys, v, a, part, ticket, out);

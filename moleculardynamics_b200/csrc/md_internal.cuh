@@ -325,8 +325,22 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
 // (null: always quantize).
 // q_current: the fixed-point positions are known to be current (a step graph
 // re-quantizes inside its rebuild branch), so no quantize launch at all.
+// The closing half-kick of a step (velocity_verlet.hpp:70-73) and the kinetic
+// energy after it, for a force kernel that applies the kick to each atom as it
+// writes the atom's force (the kinetic energy lands in result slot kResKE).
+struct KickArgs {
+    double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    const double* mass = nullptr;
+    const double* inv_mass = nullptr;
+    double half_dt = 0.0;
+    uint32_t* status = nullptr;  // MD_STATUS_NONFINITE when a sum is not finite
+};
+// Verlet-list LJ forces, energy and virial.  With `kick`, a force kernel that can
+// apply it does, and sets *kicked; otherwise *kicked stays false and the caller
+// kicks.
 int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v,
-                           const int* q_gate = nullptr, bool q_current = false);
+                           const int* q_gate = nullptr, bool q_current = false,
+                           const KickArgs* kick = nullptr, bool* kicked = nullptr);
 int lj_forces_brute_async(md_lj* lj, md_system* sys, bool forces);
 int lj_forces_cells_async(md_lj* lj, md_system* sys, md_cells* cells);
 int system_kinetic_async(md_system* sys, int slot);
