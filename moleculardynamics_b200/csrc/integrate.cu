@@ -87,8 +87,11 @@ __device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const Ste
     if (CHECK) top2_grid_at(a1, 0.0, d, block, nblocks);
 }
 
+// At most 48 registers: five 256-thread blocks per SM keep enough loads in flight
+// (the kernel streams ~190 bytes per atom and waits on memory, not arithmetic).
 template <bool CHECK>
-__global__ void k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc, DispArgs d) {
+__global__ void __launch_bounds__(kBlock, 5)
+k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc, DispArgs d) {
     kick_drift_body<CHECK>(a, n, s, nhc, d, blockIdx.x, gridDim.x);
 }
 
@@ -349,8 +352,10 @@ int pre_force(md_integrator* it, md_system* sys, md_verlet* check, bool fresh_ke
                                                 yoshida());
             ctx->launches += 1;
         }
+        ctx_time_begin(ctx, MD_KERNEL_INTEGRATE);
         if (check) k_kick_drift<true><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
         else k_kick_drift<false><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
+        ctx_time_end(ctx, MD_KERNEL_INTEGRATE);
     }
     ++ctx->launches;
     MDB_CHECK_LAUNCH();
@@ -380,8 +385,10 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale, bool k
     double* part;
     MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));
     if (n > 0 && !kicked) {
+        ctx_time_begin(ctx, MD_KERNEL_INTEGRATE);
         k_kick_ke<<<g, kBlock, 0, ctx->stream>>>(sys->cur, n, s, part, ctx_counter(ctx, 3),
                                                 ctx_result(ctx, kResKE), ctx->d_status);
+        ctx_time_end(ctx, MD_KERNEL_INTEGRATE);
         ++ctx->launches;
     }
     NhcState* nhc = nhc_of(it);
