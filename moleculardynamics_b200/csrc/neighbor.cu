@@ -628,13 +628,18 @@ struct HaloRun {
 };
 
 // The run holding j: six fixed steps over first atoms padded with INT_MAX to
-// kHaloRuns entries (no bounds test), then one 16-byte read of the run.
+// kHaloRuns entries (no bounds test), the position carried as a byte offset so
+// that each step is one shared load at a constant offset, one compare and one
+// predicated add; then one 16-byte read of the run.  Any j (also one read past
+// the row's end, whose result is not used) stays inside the table.
 __device__ __forceinline__ unsigned halo_slot(int j, const int* s_beg, const HaloRun* s_run,
                                               bool& ok) {
-    int t = 0;
+    const char* sb = reinterpret_cast<const char*>(s_beg);
+    unsigned tb = 0u;  // 4 * run index
 #pragma unroll
-    for (int step = kHaloRuns / 2; step > 0; step >>= 1) t += s_beg[t + step] <= j ? step : 0;
-    const HaloRun r = s_run[t];
+    for (int step = kHaloRuns / 2; step > 0; step >>= 1)
+        if (*reinterpret_cast<const int*>(sb + tb + 4 * step) <= j) tb += 4u * step;
+    const HaloRun r = *reinterpret_cast<const HaloRun*>(reinterpret_cast<const char*>(s_run) + 4u * tb);
     const int slot = j - r.shift;
     ok = static_cast<unsigned>(slot - r.base) < static_cast<unsigned>(r.len);
     return static_cast<unsigned>(slot) << 4;
@@ -678,14 +683,14 @@ k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stri
         for (int ch = tid & 3; 8 * ch < c; ch += 4) {
             const int4 a0 = __ldg(src + 2 * ch), a1 = __ldg(src + 2 * ch + 1);
             const int js[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const int rem = c - 8 * ch;  // entries of this chunk inside the row
             unsigned off[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                const bool in_row = 8 * ch + k < c;
                 bool ok;
-                const unsigned o = halo_slot(in_row ? js[k] : static_cast<int>(i), s_beg, s_run, ok);
-                off[k] = in_row ? o : self;
-                bad = bad || (in_row && !ok);
+                const unsigned o = halo_slot(js[k], s_beg, s_run, ok);
+                off[k] = k < rem ? o : self;
+                bad = bad || (k < rem && !ok);
             }
             dst[ch] = make_uint4(off[0] | (off[1] << 16), off[2] | (off[3] << 16),
                                  off[4] | (off[5] << 16), off[6] | (off[7] << 16));
