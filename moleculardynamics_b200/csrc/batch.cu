@@ -20,6 +20,18 @@ int verlet_ensure_ready(md_verlet* v, md_system* sys, const char* who);
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 }
 
+namespace mdb {
+// Per replica: its thermo rows (kept across runs, grown by doubling) and the
+// device-held row index.
+struct BatchRun {
+    DevBuf rows, idx;
+    int64_t cap = 0;
+    int rebuilt0 = 0, rebuilt1 = 0;
+};
+struct BatchCache;  // the batched step graph kept across runs (below)
+void batch_cache_destroy(BatchCache* c);
+}  // namespace mdb
+
 struct md_batch {
     struct Replica {
         md_integrator* it;
@@ -30,16 +42,16 @@ struct md_batch {
     std::vector<Replica> reps;
     int device = -1;
     int batched = 1;  // batched stage kernels when the replicas allow them
+    std::vector<mdb::BatchRun> runs;
+    mdb::BatchCache* cache = nullptr;
+    ~md_batch() { mdb::batch_cache_destroy(cache); }
 };
 
 using namespace mdb;
 
 namespace {
 
-struct Run {
-    DevBuf rows, idx;
-    int rebuilt0 = 0, rebuilt1 = 0;
-};
+using Run = BatchRun;
 
 int check_replica(const md_batch* b, const md_batch::Replica& r) {
     if (!r.it || !r.sys || !r.list || !r.lj)
@@ -88,15 +100,18 @@ int capture_to(cudaStream_t stream, cudaGraph_t g, const cudaGraphNode_t* deps, 
 }
 
 // The step graph of batched stage kernels: the chain halves and kick/drift of
-// every replica in one launch (its rebuild test sets each replica's branch),
-// one conditional rebuild branch per replica, then the force pass and the
+// every replica in one launch (with each replica's rebuild test), the gated
+// rebuild of every replica as one launch per stage (each replica's blocks leave
+// at once unless its own test asked for a rebuild), then the force pass and the
 // kick, kinetic energy, chain half and thermo row of every replica in three
-// launches.  Per replica the work and its order are those of its solo step.
+// launches: about fifteen kernel nodes and no conditional node.  Per replica the
+// work and its order are those of its solo step.
 struct BatchedStep {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     BatchKick* kick = nullptr;
     BatchForce* force = nullptr;
+    BatchRebuild* rebuild = nullptr;
     int64_t lead_launches = 0;
     std::vector<int64_t> body_launches;
     ~BatchedStep() {
@@ -104,8 +119,29 @@ struct BatchedStep {
         if (graph) cudaGraphDestroy(graph);
         batch_kick_destroy(kick);
         batch_force_destroy(force);
+        batch_rebuild_destroy(rebuild);
     }
 };
+
+}  // namespace
+
+// The batched step graph of the last run, replayed by later runs while nothing it
+// captured has changed: the process-wide graph epoch (any device buffer moved or
+// a launch setting changed), the batched switch and the replica list.
+struct mdb::BatchCache {
+    BatchedStep step;
+    std::vector<cudaEvent_t> ready;  // each replica's first step done, for the lead stream
+    uint64_t epoch = 0;
+    size_t nrep = 0;
+    ~BatchCache() {
+        for (cudaEvent_t e : ready)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+void mdb::batch_cache_destroy(BatchCache* c) { delete c; }
+
+namespace {
 
 // Builds the batched step graph, or leaves bs.exec null when the replicas need
 // the per-replica graph (kernels that cannot share a launch).
@@ -115,42 +151,20 @@ int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
     std::vector<BatchRepView> views(nr);
     for (size_t k = 0; k < nr; ++k) {
         const auto& r = b->reps[k];
-        cudaGraphConditionalHandle h;
-        if (cudaGraphConditionalHandleCreate(&h, bs.graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
-            return fail(MD_ERR_CUDA, "md_batch_run: conditional handle");
         views[k] = BatchRepView{r.it, r.sys, r.list, r.lj, run[k].rows.as<double>(),
-                                run[k].idx.as<int>(), h};
+                                run[k].idx.as<int>()};
     }
-    if (batch_force_create(views.data(), static_cast<int>(nr), &bs.force) != MD_OK ||
+    if (batch_rebuild_create(views.data(), static_cast<int>(nr), &bs.rebuild) != MD_OK ||
+        batch_force_create(views.data(), static_cast<int>(nr), &bs.force) != MD_OK ||
         batch_kick_create(views.data(), static_cast<int>(nr), &bs.kick) != MD_OK) {
         cudaGetLastError();
         return MD_OK;  // not batchable: the caller uses the per-replica graph
     }
     cudaStream_t lead = b->reps[0].sys->ctx->stream;
-    std::vector<cudaGraphNode_t> pre;
-    MDB_TRY(capture_to(lead, bs.graph, nullptr, 0,
-                       [&]() { return batch_kick_pre(bs.kick, lead, &bs.lead_launches); }, &pre));
-    std::vector<cudaGraphNode_t> conds(nr);
     bs.body_launches.assign(nr, 0);
-    for (size_t k = 0; k < nr; ++k) {
-        auto& r = b->reps[k];
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = views[k].cond;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        const cudaError_t e = cudaGraphAddNode(&conds[k], bs.graph, pre.data(), pre.size(), &cp);
-        if (e != cudaSuccess) return fail(MD_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
-        md_context* ctx = r.sys->ctx;
-        const int64_t l0 = ctx->launches;
-        MDB_TRY(capture_to(ctx->stream, cp.conditional.phGraph_out[0], nullptr, 0, [&]() -> int {
-            MDB_TRY(verlet_build(r.list, r.sys, true));
-            return lj_quantize_async(r.lj, r.sys, r.list->d_rebuild_flag);
-        }, nullptr));
-        bs.body_launches[k] = ctx->launches - l0;
-        ctx->launches = l0;  // counted per rebuild by the caller
-    }
-    MDB_TRY(capture_to(lead, bs.graph, conds.data(), conds.size(), [&]() -> int {
+    MDB_TRY(capture_to(lead, bs.graph, nullptr, 0, [&]() -> int {
+        MDB_TRY(batch_kick_pre(bs.kick, lead, &bs.lead_launches));
+        MDB_TRY(batch_rebuild_launch(bs.rebuild, lead, &bs.lead_launches));
         MDB_TRY(batch_force_launch(bs.force, lead, &bs.lead_launches));
         return batch_kick_post(bs.kick, lead, &bs.lead_launches);
     }, nullptr));
@@ -187,6 +201,8 @@ int md_batch_add(md_batch* b, md_integrator* it, md_system* sys, md_verlet* list
     MDB_TRY(check_replica(b, r));
     if (b->device < 0) b->device = sys->ctx->device;
     b->reps.push_back(r);
+    batch_cache_destroy(b->cache);  // the replica list is part of the cached graph
+    b->cache = nullptr;
     if (index) *index = static_cast<int>(b->reps.size()) - 1;
     return MD_OK;
 }
@@ -211,18 +227,27 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
         verlet_halo_for_run(r.list, r.sys, r.lj);
     }
     MDB_CUDA(cudaSetDevice(b->device));
-    std::vector<Run> run(nr);
+    if (b->runs.size() != nr) {
+        batch_cache_destroy(b->cache);
+        b->cache = nullptr;
+        b->runs.clear();
+        b->runs.resize(nr);
+    }
+    std::vector<Run>& run = b->runs;
     // Step 0 of every replica from the host, on the replica's own stream: it sizes
     // every buffer (the captured graph must not allocate) and sums the chains'
-    // entry kinetic energies.
+    // entry kinetic energies.  Thermo rows persist across runs, grown by doubling
+    // (a move invalidates a cached graph through the graph epoch).
     for (size_t k = 0; k < nr; ++k) {
         auto& r = b->reps[k];
         md_context* ctx = r.sys->ctx;
-        if (thermo) {
-            MDB_TRY(run[k].rows.ensure(sizeof(double) * 4 * static_cast<size_t>(steps)));
-            MDB_TRY(run[k].idx.ensure(sizeof(int)));
-            MDB_CUDA(cudaMemsetAsync(run[k].idx.ptr, 0, sizeof(int), ctx->stream));
+        if (run[k].cap < steps) {
+            const int64_t cap = std::max<int64_t>(steps, 2 * run[k].cap);
+            MDB_TRY(run[k].rows.ensure(sizeof(double) * 4 * static_cast<size_t>(cap)));
+            run[k].cap = cap;
         }
+        MDB_TRY(run[k].idx.ensure(sizeof(int)));
+        MDB_CUDA(cudaMemsetAsync(run[k].idx.ptr, 0, sizeof(int), ctx->stream));
         MDB_TRY(lj_fused_step(r.it, r.sys, r.list, r.lj, run[k].rows.as<double>(),
                               run[k].idx.as<int>(), true));
     }
@@ -231,24 +256,38 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     cudaStream_t lead = b->reps[0].sys->ctx->stream;
     int rc = MD_OK;
     std::vector<int64_t> main_l(nr, 0), body_l(nr, 0);
-    BatchedStep bs;
+    bool batched_done = false;
     if (steps > 1 && b->batched) {
-        MDB_TRY(build_batched_step(b, run, bs));
-        if (bs.exec) {
+        // the batched step graph of an earlier run while nothing it captured moved
+        BatchCache* c = b->cache;
+        if (!(c && c->step.exec && c->epoch == graph_epoch() && c->nrep == nr)) {
+            batch_cache_destroy(c);
+            c = b->cache = new (std::nothrow) BatchCache();
+            if (!c) return fail(MD_ERR_OUT_OF_MEMORY, "md_batch_run: host allocation");
+            c->nrep = nr;
+            MDB_TRY(build_batched_step(b, run, c->step));
+            if (c->step.exec) {
+                c->ready.assign(nr, nullptr);
+                for (size_t k = 0; k < nr; ++k)
+                    MDB_CUDA(cudaEventCreateWithFlags(&c->ready[k], cudaEventDisableTiming));
+            }
+            c->epoch = graph_epoch();
+        }
+        if (c->step.exec) {
+            // the lead stream replays the graph once every replica's first step is done
             for (size_t k = 0; k < nr; ++k) {
-                md_context* ctx = b->reps[k].sys->ctx;
-                MDB_TRY(read_rebuilds(b->reps[k].list, ctx->stream, &run[k].rebuilt0));
-                MDB_CUDA(cudaStreamSynchronize(ctx->stream));
+                MDB_CUDA(cudaEventRecord(c->ready[k], b->reps[k].sys->ctx->stream));
+                MDB_CUDA(cudaStreamWaitEvent(lead, c->ready[k], 0));
             }
             for (int64_t s = 1; s < steps; ++s)
-                if (cudaGraphLaunch(bs.exec, lead) != cudaSuccess)
+                if (cudaGraphLaunch(c->step.exec, lead) != cudaSuccess)
                     return fail(MD_ERR_CUDA, "md_batch_run: graph launch failed");
             MDB_CUDA(cudaStreamSynchronize(lead));
-            b->reps[0].sys->ctx->launches += (steps - 1) * bs.lead_launches;
-            for (size_t k = 0; k < nr; ++k) body_l[k] = bs.body_launches[k];
+            b->reps[0].sys->ctx->launches += (steps - 1) * c->step.lead_launches;
+            batched_done = true;
         }
     }
-    if (steps > 1 && !bs.exec) {
+    if (steps > 1 && !batched_done) {
         if (cudaGraphCreate(&graph, 0) != cudaSuccess) return fail(MD_ERR_CUDA, "cudaGraphCreate");
         for (size_t k = 0; k < nr && rc == MD_OK; ++k) {
             auto& r = b->reps[k];
@@ -276,7 +315,7 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     for (size_t k = 0; k < nr; ++k) {
         auto& r = b->reps[k];
         md_context* ctx = r.sys->ctx;
-        if (steps > 1) {
+        if (steps > 1 && !batched_done) {
             MDB_TRY(read_rebuilds(r.list, ctx->stream, &run[k].rebuilt1));
             MDB_CUDA(cudaStreamSynchronize(ctx->stream));
             ctx->launches += (steps - 1) * main_l[k] +
@@ -291,8 +330,6 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     for (size_t k = 0; k < nr; ++k) {
         auto& r = b->reps[k];
         MDB_CUDA(cudaStreamSynchronize(r.sys->ctx->stream));
-        run[k].rows.release();
-        run[k].idx.release();
         MDB_TRY(ctx_check_status(r.sys->ctx));
         double e[2];
         MDB_TRY(ctx_read_results(r.sys->ctx, kResEnergy, 2, e));

@@ -196,10 +196,10 @@ struct BatchRepView {
     md_lj* lj;
     double* rows;                     // thermo rows at a device-held index, or null
     int* idx;
-    cudaGraphConditionalHandle cond;  // the replica's rebuild branch in the step graph
 };
-struct BatchKick;   // integrate.cu: chain halves, kick/drift (+ rebuild test), kick + KE
-struct BatchForce;  // lj.cu: the Verlet-list force pass
+struct BatchKick;     // integrate.cu: chain halves, kick/drift (+ rebuild test), kick + KE
+struct BatchForce;    // lj.cu: the Verlet-list force pass
+struct BatchRebuild;  // neighbor.cu: the gated rebuild of every replica, stage by stage
 int batch_kick_create(const BatchRepView* reps, int nrep, BatchKick** out);
 int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches);
 int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches);
@@ -209,6 +209,11 @@ void batch_kick_destroy(BatchKick* b);
 int batch_force_create(const BatchRepView* reps, int nrep, BatchForce** out);
 int batch_force_launch(BatchForce* b, cudaStream_t stream, int64_t* launches);
 void batch_force_destroy(BatchForce* b);
+// MD_ERR_INVALID_ARGUMENT when a replica's rebuild cannot join the batched stages
+// (a list with halo tiles).
+int batch_rebuild_create(const BatchRepView* reps, int nrep, BatchRebuild** out);
+int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches);
+void batch_rebuild_destroy(BatchRebuild* b);
 // Mixed precision: the fixed-point positions (after a rebuild re-sorted the atoms).
 int lj_quantize_async(md_lj* lj, md_system* sys, const int* gate);
 

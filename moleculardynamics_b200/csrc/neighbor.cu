@@ -52,23 +52,35 @@ struct GridArgs {
     const int* cell_of_rank;
 };
 
-__global__ void k_zero_int(int* a, int64_t n, const int* flag) {
-    if (!gate(flag)) return;
-    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+// Kernel bodies take their block index (and count) explicitly: a batched launch
+// gives each replica's blocks their own rank, and each replica runs exactly the
+// blocks of its solo launch.
+__device__ __forceinline__ void zero_int_body(int* a, int64_t n, unsigned block, unsigned nblocks) {
+    for (int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(nblocks) * blockDim.x)
         a[k] = 0;
 }
 
-__global__ void k_bin(const double4* __restrict__ pos, int64_t n, GridArgs g, int* atom_rank,
-                      int* counts, const int* flag) {
+__global__ void k_zero_int(int* a, int64_t n, const int* flag) {
     if (!gate(flag)) return;
-    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    zero_int_body(a, n, blockIdx.x, gridDim.x);
+}
+
+__device__ __forceinline__ void bin_body(const double4* __restrict__ pos, int64_t n, const GridArgs& g,
+                                         int* atom_rank, int* counts, unsigned block) {
+    const int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (k >= n) return;
     const double4 p = pos[k];
     const int c = cell_of(p.x, p.y, p.z, g.box, g.wx, g.wy, g.wz, g.nx, g.ny, g.nz);
     const int r = g.rank_of_cell[c];
     atom_rank[k] = r;
     atomicAdd(counts + r, 1);
+}
+
+__global__ void k_bin(const double4* __restrict__ pos, int64_t n, GridArgs g, int* atom_rank,
+                      int* counts, const int* flag) {
+    if (!gate(flag)) return;
+    bin_body(pos, n, g, atom_rank, counts, blockIdx.x);
 }
 
 // Exclusive scan of counts[0..m) into start[0..m] (start[m] = total) in three
@@ -106,11 +118,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
 // single: the grid is one block, whose scan is already the whole exclusive scan;
 // it then also writes the end sentinel start[m] (k_scan_top and k_scan_add would
 // write it and add nothing), saving their launches.
-__global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int* __restrict__ counts,
-                                                            int* start, int m, int* bsum,
-                                                            const int* flag, int single) {
-    if (!gate(flag)) return;
-    const int base = blockIdx.x * kScanBlock * kScanItems;
+__device__ __forceinline__ void scan_blocks_body(const int* __restrict__ counts, int* start, int m,
+                                                 int* bsum, int single, unsigned block) {
+    const int base = block * kScanBlock * kScanItems;
     int v[kScanItems];
     int sum = 0;
 #pragma unroll
@@ -131,14 +141,19 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int* __restric
     }
     (void)sum;
     if (threadIdx.x == 0) {
-        bsum[blockIdx.x] = run_base;
+        bsum[block] = run_base;
         if (single) start[m] = run_base;
     }
 }
 
-__global__ void __launch_bounds__(kScanBlock) k_scan_top(int* bsum, int nb, int* start, int m,
-                                                         const int* flag) {
+__global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int* __restrict__ counts,
+                                                            int* start, int m, int* bsum,
+                                                            const int* flag, int single) {
     if (!gate(flag)) return;
+    scan_blocks_body(counts, start, m, bsum, single, blockIdx.x);
+}
+
+__device__ __forceinline__ void scan_top_body(int* bsum, int nb, int* start, int m) {
     int carry = 0;
     for (int b0 = 0; b0 < nb; b0 += kScanBlock) {
         const int b = b0 + threadIdx.x;
@@ -151,11 +166,16 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_top(int* bsum, int nb, int*
     if (threadIdx.x == 0) start[m] = carry;
 }
 
-__global__ void __launch_bounds__(kScanBlock) k_scan_add(int* start, int m, const int* __restrict__ bsum,
+__global__ void __launch_bounds__(kScanBlock) k_scan_top(int* bsum, int nb, int* start, int m,
                                                          const int* flag) {
     if (!gate(flag)) return;
-    const int base = blockIdx.x * kScanBlock * kScanItems;
-    const int off = bsum[blockIdx.x];
+    scan_top_body(bsum, nb, start, m);
+}
+
+__device__ __forceinline__ void scan_add_body(int* start, int m, const int* __restrict__ bsum,
+                                              unsigned block) {
+    const int base = block * kScanBlock * kScanItems;
+    const int off = bsum[block];
 #pragma unroll
     for (int u = 0; u < kScanItems; ++u) {
         const int i = base + u * kScanBlock + threadIdx.x;
@@ -163,14 +183,26 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add(int* start, int m, cons
     }
 }
 
-__global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const int* __restrict__ start,
-                          int* fill, int* sorted, const int* flag) {
+__global__ void __launch_bounds__(kScanBlock) k_scan_add(int* start, int m, const int* __restrict__ bsum,
+                                                         const int* flag) {
     if (!gate(flag)) return;
-    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    scan_add_body(start, m, bsum, blockIdx.x);
+}
+
+__device__ __forceinline__ void scatter_body(const int* __restrict__ atom_rank, int64_t n,
+                                             const int* __restrict__ start, int* fill, int* sorted,
+                                             unsigned block) {
+    const int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (k >= n) return;
     const int r = atom_rank[k];
     const int at = atomicAdd(fill + r, 1);
     sorted[start[r] + at] = static_cast<int>(k);
+}
+
+__global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const int* __restrict__ start,
+                          int* fill, int* sorted, const int* flag) {
+    if (!gate(flag)) return;
+    scatter_body(atom_rank, n, start, fill, sorted, blockIdx.x);
 }
 
 // Within each cell, order atoms by original index.  One warp per cell: each atom's
@@ -180,12 +212,10 @@ __global__ void k_scatter(const int* __restrict__ atom_rank, int64_t n, const in
 constexpr int kOrderWarps = 8;   // k_cell_order runs 256-thread blocks
 constexpr int kOrderMax = 512;   // atoms per cell ordered in shared memory
 
-__global__ void __launch_bounds__(32 * kOrderWarps)
-k_cell_order(int* sorted, const int* __restrict__ start, int m,
-                             const int* __restrict__ orig, const int* flag) {
-    if (!gate(flag)) return;
+__device__ __forceinline__ void cell_order_body(int* sorted, const int* __restrict__ start, int m,
+                                                const int* __restrict__ orig, unsigned block) {
     const int lane = threadIdx.x & 31;
-    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int r = static_cast<int>((block * blockDim.x + threadIdx.x) >> 5);
     if (r >= m) return;
     const int s0 = start[r], s1 = start[r + 1], c = s1 - s0;
     if (c <= 1) return;
@@ -230,12 +260,19 @@ k_cell_order(int* sorted, const int* __restrict__ start, int m,
     }
 }
 
+__global__ void __launch_bounds__(32 * kOrderWarps)
+k_cell_order(int* sorted, const int* __restrict__ start, int m,
+                             const int* __restrict__ orig, const int* flag) {
+    if (!gate(flag)) return;
+    cell_order_body(sorted, start, m, orig, blockIdx.x);
+}
+
 // Gathers every per-atom array into the new order.  Forces are skipped when the
 // caller recomputes them right after the rebuild (fused stepping loops).
-__global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restrict__ perm,
-                                int* slot, int64_t n, const int* flag, int with_forces) {
-    if (!gate(flag)) return;
-    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+__device__ __forceinline__ void permute_body(const md_atoms& src, const md_atoms& dst,
+                                             const int* __restrict__ perm, int* slot, int64_t n,
+                                             int with_forces, unsigned block) {
+    const int64_t s = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (s >= n) return;
     const int k = perm[s];
     dst.pos[s] = src.pos[k];
@@ -256,10 +293,15 @@ __global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restric
     slot[o] = static_cast<int>(s);
 }
 
-__global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* flag,
-                             int with_forces) {
+__global__ void k_permute_gated(md_atoms src, md_atoms dst, const int* __restrict__ perm,
+                                int* slot, int64_t n, const int* flag, int with_forces) {
     if (!gate(flag)) return;
-    const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    permute_body(src, dst, perm, slot, n, with_forces, blockIdx.x);
+}
+
+__device__ __forceinline__ void copy_atoms_body(const md_atoms& src, const md_atoms& dst, int64_t n,
+                                                int with_forces, unsigned block) {
+    const int64_t s = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (s >= n) return;
     dst.pos[s] = src.pos[s];
     dst.vx[s] = src.vx[s];
@@ -275,6 +317,12 @@ __global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* f
     dst.charge[s] = src.charge[s];
     dst.mol[s] = src.mol[s];
     dst.orig[s] = src.orig[s];
+}
+
+__global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* flag,
+                             int with_forces) {
+    if (!gate(flag)) return;
+    copy_atoms_body(src, dst, n, with_forces, blockIdx.x);
 }
 
 // Exact candidate test with the pair ordered by original index.
@@ -300,11 +348,12 @@ __device__ __forceinline__ bool within(const Box3& b, double4 pi, double4 pj, do
 // pair set (forEachPair) applies the reference's exact test to the positions of
 // the build and is bit-identical to the reference's.
 // Rows list candidates in stencil order, atoms of a cell in sorted order.
-__global__ void __launch_bounds__(kBuildWarps * 32)
-k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
-               double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
-               uint32_t* status, int* max_count, const int* flag, int groups) {
-    if (!gate(flag)) return;
+__device__ __forceinline__ void verlet_cells_body(const double4* __restrict__ pos,
+                                                  const int* __restrict__ start, const GridArgs& g,
+                                                  double rl2, int* __restrict__ nbr,
+                                                  int* __restrict__ count, int stride,
+                                                  uint32_t* status, int* max_count, int groups,
+                                                  unsigned block) {
     // Candidates in pairs, structure-of-arrays within a pair so that two
     // candidates are tested with one packed FP32x2 instruction per step:
     // s_a[p] = (-x0, -x1, -y0, -y1), s_b[p] = (-z0, -z1, j0, j1).
@@ -312,7 +361,7 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     __shared__ float4 s_b[kBuildWarps][kMaxCand / 2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // `groups` warps share a crowded cell, each taking every groups-th run of 32 atoms
-    const int wid = blockIdx.x * kBuildWarps + warp;
+    const int wid = static_cast<int>(block) * kBuildWarps + warp;
     const int r = wid / groups, grp = wid % groups;
     if (r >= g.ncells) return;
     const int cell = g.cell_of_rank[r];
@@ -447,14 +496,22 @@ k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, G
     }
 }
 
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_verlet_cells(const double4* __restrict__ pos, const int* __restrict__ start, GridArgs g,
+               double rl2, int* __restrict__ nbr, int* __restrict__ count, int stride,
+               uint32_t* status, int* max_count, const int* flag, int groups) {
+    if (!gate(flag)) return;
+    verlet_cells_body(pos, start, g, rl2, nbr, count, stride, status, max_count, groups, blockIdx.x);
+}
+
 // Boxes with fewer than 3 cells per side (verlet_list.cpp:26-33): one warp per atom
 // scans every other atom.
-__global__ void k_verlet_brute(const double4* __restrict__ pos, int64_t n, Box3 box, double rl2,
-                               int* __restrict__ nbr, int* __restrict__ count, int stride,
-                               uint32_t* status, int* max_count, const int* flag) {
-    if (!gate(flag)) return;
+__device__ __forceinline__ void brute_body(const double4* __restrict__ pos, int64_t n,
+                                           const Box3& box, double rl2, int* __restrict__ nbr,
+                                           int* __restrict__ count, int stride, uint32_t* status,
+                                           int* max_count, unsigned block) {
     const int lane = threadIdx.x & 31;
-    const int64_t i = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t i = (block * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
     if (i >= n) return;
     const double4 pi = pos[i];
     int base = 0;
@@ -474,6 +531,13 @@ __global__ void k_verlet_brute(const double4* __restrict__ pos, int64_t n, Box3 
         atomicMax(max_count, base);
         if (base > stride) atomicOr(status, MD_STATUS_NEIGHBOR_OVERFLOW);
     }
+}
+
+__global__ void k_verlet_brute(const double4* __restrict__ pos, int64_t n, Box3 box, double rl2,
+                               int* __restrict__ nbr, int* __restrict__ count, int stride,
+                               uint32_t* status, int* max_count, const int* flag) {
+    if (!gate(flag)) return;
+    brute_body(pos, n, box, rl2, nbr, count, stride, status, max_count, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- halo tiles
@@ -699,12 +763,17 @@ k_halo_rows(const int* __restrict__ nbr, const int* __restrict__ count, int stri
     if (__syncthreads_or(bad) && tid == 0) meta[b].x = -1;
 }
 
+__device__ __forceinline__ void store_ref_body(const double4* __restrict__ pos, double4* ref,
+                                               int64_t n, int* total, unsigned block) {
+    const int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k < n) ref[k] = pos[k];
+    if (k == 0 && total) ++*total;
+}
+
 __global__ void k_store_ref(const double4* __restrict__ pos, double4* ref, int64_t n,
                             const int* flag, int* total) {
     if (!gate(flag)) return;
-    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (k < n) ref[k] = pos[k];
-    if (k == 0 && total) ++*total;
+    store_ref_body(pos, ref, n, total, blockIdx.x);
 }
 
 // verlet_list.cpp:44-63: top-2 min-image displacements; decides on device.
@@ -800,6 +869,109 @@ int cell_sort_gated(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_
     ctx->launches += 3 + (n > 0 ? 2 : 0);
     MDB_CHECK_LAUNCH();
     return MD_OK;
+}
+
+
+// ------------------------------------------------------------ batched rebuilds
+// The gated rebuild of many replicas, one launch per stage (the counting sort, the
+// re-sort of the system, the list build, the reference positions and, for a mixed
+// force, the fixed-point copy).  Each block serves the replica the stage's
+// block-offset table assigns it and leaves at once when that replica's rebuild
+// flag is clear; a replica's blocks are those of its solo gated rebuild.
+struct RebuildRep {
+    const int* flag;
+    int64_t n;
+    int m;       // cells (0 for a brute-force build)
+    int nb;      // scan blocks
+    int groups;  // warps per cell in the list build
+    GridArgs g;
+    md_atoms cur, alt;
+    int* slot;
+    int *atom_rank, *counts, *fill;
+    int* start;
+    int* perm;
+    double rl2;
+    int* nbr;
+    int* count;
+    int stride;
+    uint32_t* status;
+    int* max_count;
+    double4* ref;
+    int* total;
+    int4* q;      // the fixed-point copy for a mixed force, or null
+    double qs[3];  // 2^32 / L per axis
+};
+
+enum RebuildStage : int {
+    kStZero, kStBin, kStScan, kStScanTop, kStScanAdd, kStScatter, kStOrder, kStPermute, kStCopy,
+    kStCells, kStBrute, kStRef, kStQuant, kRebuildStages
+};
+
+__device__ __forceinline__ int rebuild_rep_of(const int* __restrict__ off, int nrep, int b) {
+    int lo = 0, hi = nrep;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The stages on 256-thread blocks.
+template <int STAGE>
+__global__ void __launch_bounds__(kBlock)
+k_batch_rebuild(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
+    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
+    const RebuildRep& d = reps[r];
+    if (!gate(d.flag)) return;
+    const unsigned b = blockIdx.x - __ldg(off + r), nb = __ldg(off + r + 1) - __ldg(off + r);
+    if constexpr (STAGE == kStZero) {
+        zero_int_body(d.counts, 2 * static_cast<int64_t>(d.m), b, nb);
+        if (b == 0 && threadIdx.x == 0) *d.max_count = 0;
+    } else if constexpr (STAGE == kStBin) {
+        bin_body(d.cur.pos, d.n, d.g, d.atom_rank, d.counts, b);
+    } else if constexpr (STAGE == kStScatter) {
+        scatter_body(d.atom_rank, d.n, d.start, d.fill, d.perm, b);
+    } else if constexpr (STAGE == kStOrder) {
+        cell_order_body(d.perm, d.start, d.m, d.cur.orig, b);
+    } else if constexpr (STAGE == kStPermute) {
+        permute_body(d.cur, d.alt, d.perm, d.slot, d.n, 0, b);
+    } else if constexpr (STAGE == kStCopy) {
+        copy_atoms_body(d.alt, d.cur, d.n, 0, b);
+    } else if constexpr (STAGE == kStBrute) {
+        brute_body(d.cur.pos, d.n, d.g.box, d.rl2, d.nbr, d.count, d.stride, d.status, d.max_count, b);
+    } else if constexpr (STAGE == kStRef) {
+        store_ref_body(d.cur.pos, d.ref, d.n, d.total, b);
+    } else if constexpr (STAGE == kStQuant) {
+        const int64_t k = b * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+        if (d.q && k < d.n) d.q[k] = quantize_position(d.cur.pos[k], d.qs[0], d.qs[1], d.qs[2]);
+    }
+}
+
+// The cell-count scan on 1024-thread blocks: block scans (the whole scan where
+// one block covers the grid), then, for larger grids, the scan of the block
+// totals and their addition.
+template <int STAGE>
+__global__ void __launch_bounds__(kScanBlock)
+k_batch_rebuild_scan(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
+    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
+    const RebuildRep& d = reps[r];
+    if (!gate(d.flag)) return;
+    const unsigned b = blockIdx.x - __ldg(off + r);
+    int* bsum = d.fill + d.m;  // the sort scratch's tail
+    if constexpr (STAGE == kStScan) scan_blocks_body(d.counts, d.start, d.m, bsum, d.nb == 1 ? 1 : 0, b);
+    else if constexpr (STAGE == kStScanTop) scan_top_body(bsum, d.nb, d.start, d.m);
+    else scan_add_body(d.start, d.m, bsum, b);
+}
+
+// The list build, on the build's own 128-thread blocks.
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_batch_rebuild_cells(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
+    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
+    const RebuildRep& d = reps[r];
+    if (!gate(d.flag)) return;
+    verlet_cells_body(d.cur.pos, d.start, d.g, d.rl2, d.nbr, d.count, d.stride, d.status,
+                      d.max_count, d.groups, blockIdx.x - __ldg(off + r));
 }
 
 }  // namespace
@@ -1034,6 +1206,131 @@ int verlet_check(md_verlet* v, md_system* sys) {
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
+
+
+// ------------------------------------------------------------ batched rebuilds
+struct BatchRebuild {
+    DevBuf reps, off;  // off: kRebuildStages tables of nrep + 1 block offsets
+    int nrep = 0;
+    int blocks[kRebuildStages] = {};
+};
+
+int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
+    *out = nullptr;
+    if (nrep < 1) return fail(MD_ERR_INVALID_ARGUMENT, "batch_rebuild_create: no replicas");
+    std::vector<RebuildRep> h(static_cast<size_t>(nrep));
+    std::vector<int> off(static_cast<size_t>(kRebuildStages) * (nrep + 1), 0);
+    for (int r = 0; r < nrep; ++r) {
+        md_system* sys = v[r].sys;
+        md_verlet* lst = v[r].list;
+        md_context* ctx = sys->ctx;
+        const int64_t n = sys->n;
+        const bool cells = lst->grid.usable;
+        const int m = cells ? lst->grid.ncells : 0;
+        if (lst->halo_on || n <= 0 || (cells && (!lst->start.ptr || !lst->perm.ptr || !sys->alt.pos)))
+            return fail(MD_ERR_INVALID_ARGUMENT, "batch_rebuild_create: replica %d rebuilds alone", r);
+        RebuildRep& d = h[static_cast<size_t>(r)];
+        d.flag = lst->d_rebuild_flag;
+        d.n = n;
+        d.m = m;
+        d.nb = (m + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
+        const double mean = cells ? static_cast<double>(n) / m : 0.0;  // as verlet_build_impl
+        d.groups = static_cast<int>(std::min(16.0, std::max(1.0, std::ceil(1.5 * mean / 32.0))));
+        d.g = make_args(lst->grid, sys);
+        d.cur = sys->cur;
+        d.alt = sys->alt;
+        d.slot = sys->slot;
+        d.atom_rank = d.counts = d.fill = nullptr;
+        if (cells) MDB_TRY(sort_scratch(ctx, n, m, &d.atom_rank, &d.counts, &d.fill));
+        d.start = lst->start.as<int>();
+        d.perm = lst->perm.as<int>();
+        d.rl2 = (lst->cutoff + lst->skin) * (lst->cutoff + lst->skin);  // verlet_list.cpp:11
+        d.nbr = lst->nbr.as<int>();
+        d.count = lst->count.as<int>();
+        d.stride = lst->stride;
+        d.status = ctx->d_status;
+        d.max_count = lst->d_max_count;
+        d.ref = lst->ref.as<double4>();
+        d.total = lst->d_rebuild_total;
+        d.q = nullptr;
+        if (v[r].lj->precision == MD_PRECISION_MIXED) {
+            MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(n)));
+            d.q = sys->qpos.as<int4>();
+        }
+        for (int k = 0; k < 3; ++k) d.qs[k] = 4294967296.0 / sys->box[k];
+        // blocks of each stage: those of the solo gated rebuild
+        const int nblk = grid_for(n, kBlock), c = cells ? 1 : 0;
+        const int per[kRebuildStages] = {
+            cells ? static_cast<int>(std::min<int64_t>(grid_for(2 * static_cast<int64_t>(m), kBlock), 4096))
+                  : 1,
+            c * nblk, c * d.nb, d.nb > 1 ? 1 : 0, d.nb > 1 ? d.nb : 0, c * nblk,
+            c * grid_for(32 * static_cast<int64_t>(m), 256), c * nblk, c * nblk,
+            c * grid_for(static_cast<int64_t>(m) * d.groups, kBuildWarps),
+            cells ? 0 : grid_for(n * 32, kBlock), nblk, d.q ? nblk : 0};
+        for (int st = 0; st < kRebuildStages; ++st) {
+            int* o = off.data() + static_cast<size_t>(st) * (nrep + 1);
+            o[r + 1] = o[r] + per[st];
+        }
+    }
+    BatchRebuild* b = new (std::nothrow) BatchRebuild();
+    if (!b) return fail(MD_ERR_OUT_OF_MEMORY, "batch_rebuild_create: host allocation");
+    b->nrep = nrep;
+    for (int st = 0; st < kRebuildStages; ++st)
+        b->blocks[st] = off[static_cast<size_t>(st) * (nrep + 1) + nrep];
+    int rc = b->reps.ensure(sizeof(RebuildRep) * h.size());
+    if (rc == MD_OK) rc = b->off.ensure(sizeof(int) * off.size());
+    if (rc == MD_OK && (cudaMemcpy(b->reps.ptr, h.data(), sizeof(RebuildRep) * h.size(),
+                                   cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(b->off.ptr, off.data(), sizeof(int) * off.size(),
+                                   cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = fail(MD_ERR_CUDA, "batch_rebuild_create: upload");
+    if (rc != MD_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return MD_OK;
+}
+
+int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches) {
+    const RebuildRep* reps = b->reps.as<RebuildRep>();
+    const int* off = b->off.as<int>();
+    const int nr = b->nrep;
+    auto table = [&](int st) { return off + static_cast<size_t>(st) * (nr + 1); };
+    int64_t l = 0;
+    auto stage = [&](int st, auto kernel) {
+        if (b->blocks[st] == 0) return;
+        kernel<<<static_cast<unsigned>(b->blocks[st]), kBlock, 0, stream>>>(reps, table(st), nr);
+        ++l;
+    };
+    auto scan = [&](int st, auto kernel) {
+        if (b->blocks[st] == 0) return;
+        kernel<<<static_cast<unsigned>(b->blocks[st]), kScanBlock, 0, stream>>>(reps, table(st), nr);
+        ++l;
+    };
+    stage(kStZero, k_batch_rebuild<kStZero>);
+    stage(kStBin, k_batch_rebuild<kStBin>);
+    scan(kStScan, k_batch_rebuild_scan<kStScan>);
+    scan(kStScanTop, k_batch_rebuild_scan<kStScanTop>);
+    scan(kStScanAdd, k_batch_rebuild_scan<kStScanAdd>);
+    stage(kStScatter, k_batch_rebuild<kStScatter>);
+    stage(kStOrder, k_batch_rebuild<kStOrder>);
+    stage(kStPermute, k_batch_rebuild<kStPermute>);
+    stage(kStCopy, k_batch_rebuild<kStCopy>);
+    if (b->blocks[kStCells] > 0) {
+        k_batch_rebuild_cells<<<static_cast<unsigned>(b->blocks[kStCells]), kBuildWarps * 32, 0,
+                                stream>>>(reps, table(kStCells), nr);
+        ++l;
+    }
+    stage(kStBrute, k_batch_rebuild<kStBrute>);
+    stage(kStRef, k_batch_rebuild<kStRef>);
+    stage(kStQuant, k_batch_rebuild<kStQuant>);
+    if (launches) *launches += l;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+void batch_rebuild_destroy(BatchRebuild* b) { delete b; }
 
 }  // namespace mdb
 
