@@ -874,8 +874,8 @@ int cell_sort_gated(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_
 
 // ------------------------------------------------------------ batched rebuilds
 // The gated rebuild of many replicas, one launch per stage (the counting sort, the
-// re-sort of the system, the list build, the reference positions and, for a mixed
-// force, the fixed-point copy).  Each block serves the replica the stage's
+// re-sort of the system with the reference positions and, for a mixed force, the
+// fixed-point copy, the list build).  Each block serves the replica the stage's
 // block-offset table assigns it and leaves at once when that replica's rebuild
 // flag is clear; a replica's blocks are those of its solo gated rebuild.
 struct RebuildRep {
@@ -904,7 +904,7 @@ struct RebuildRep {
 
 enum RebuildStage : int {
     kStZero, kStBin, kStScan, kStScanTop, kStScanAdd, kStScatter, kStOrder, kStPermute, kStCopy,
-    kStCells, kStBrute, kStRef, kStQuant, kRebuildStages
+    kStCells, kStBrute, kStRef, kRebuildStages
 };
 
 __device__ __forceinline__ int rebuild_rep_of(const int* __restrict__ off, int nrep, int b) {
@@ -937,12 +937,21 @@ k_batch_rebuild(const RebuildRep* __restrict__ reps, const int* __restrict__ off
     } else if constexpr (STAGE == kStPermute) {
         permute_body(d.cur, d.alt, d.perm, d.slot, d.n, 0, b);
     } else if constexpr (STAGE == kStCopy) {
+        // the copy back also writes what the solo rebuild writes from the same
+        // positions after the list build: the reference positions of the rebuild
+        // test and the fixed-point copy
         copy_atoms_body(d.alt, d.cur, d.n, 0, b);
+        const int64_t k = b * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+        if (k < d.n) {
+            const double4 p = d.alt.pos[k];
+            d.ref[k] = p;
+            if (d.q) d.q[k] = quantize_position(p, d.qs[0], d.qs[1], d.qs[2]);
+        }
+        if (k == 0) ++*d.total;
     } else if constexpr (STAGE == kStBrute) {
         brute_body(d.cur.pos, d.n, d.g.box, d.rl2, d.nbr, d.count, d.stride, d.status, d.max_count, b);
-    } else if constexpr (STAGE == kStRef) {
+    } else if constexpr (STAGE == kStRef) {  // brute-force builds (no re-sort)
         store_ref_body(d.cur.pos, d.ref, d.n, d.total, b);
-    } else if constexpr (STAGE == kStQuant) {
         const int64_t k = b * static_cast<int64_t>(blockDim.x) + threadIdx.x;
         if (d.q && k < d.n) d.q[k] = quantize_position(d.cur.pos[k], d.qs[0], d.qs[1], d.qs[2]);
     }
@@ -1266,7 +1275,7 @@ int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
             c * nblk, c * d.nb, d.nb > 1 ? 1 : 0, d.nb > 1 ? d.nb : 0, c * nblk,
             c * grid_for(32 * static_cast<int64_t>(m), 256), c * nblk, c * nblk,
             c * grid_for(static_cast<int64_t>(m) * d.groups, kBuildWarps),
-            cells ? 0 : grid_for(n * 32, kBlock), nblk, d.q ? nblk : 0};
+            cells ? 0 : grid_for(n * 32, kBlock), cells ? 0 : nblk};
         for (int st = 0; st < kRebuildStages; ++st) {
             int* o = off.data() + static_cast<size_t>(st) * (nrep + 1);
             o[r + 1] = o[r] + per[st];
@@ -1324,7 +1333,6 @@ int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches
     }
     stage(kStBrute, k_batch_rebuild<kStBrute>);
     stage(kStRef, k_batch_rebuild<kStRef>);
-    stage(kStQuant, k_batch_rebuild<kStQuant>);
     if (launches) *launches += l;
     MDB_CHECK_LAUNCH();
     return MD_OK;
