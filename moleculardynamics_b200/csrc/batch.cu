@@ -131,11 +131,13 @@ struct BatchedStep {
 struct mdb::BatchCache {
     BatchedStep step;
     std::vector<cudaEvent_t> ready;  // each replica's first step done, for the lead stream
+    uint32_t* h_status = nullptr;    // pinned: each replica's status word after a run
     uint64_t epoch = 0;
     size_t nrep = 0;
     ~BatchCache() {
         for (cudaEvent_t e : ready)
             if (e) cudaEventDestroy(e);
+        if (h_status) cudaFreeHost(h_status);
     }
 };
 
@@ -270,6 +272,7 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
                 c->ready.assign(nr, nullptr);
                 for (size_t k = 0; k < nr; ++k)
                     MDB_CUDA(cudaEventCreateWithFlags(&c->ready[k], cudaEventDisableTiming));
+                MDB_CUDA(cudaMallocHost(&c->h_status, sizeof(uint32_t) * nr));
             }
             c->epoch = graph_epoch();
         }
@@ -282,9 +285,37 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
             for (int64_t s = 1; s < steps; ++s)
                 if (cudaGraphLaunch(c->step.exec, lead) != cudaSuccess)
                     return fail(MD_ERR_CUDA, "md_batch_run: graph launch failed");
+            md_context* lctx = b->reps[0].sys->ctx;
+            lctx->launches += (steps - 1) * c->step.lead_launches;
+            // The end of the run on the lead stream: the chains' pending scales, then
+            // every replica's thermo rows, status word and energy/virial slots read
+            // back, one synchronisation for all.
+            MDB_TRY(batch_kick_finish(c->step.kick, lead, &lctx->launches));
+            for (size_t k = 0; k < nr; ++k) {
+                md_context* ctx = b->reps[k].sys->ctx;
+                if (thermo)
+                    MDB_CUDA(cudaMemcpyAsync(thermo + 4 * steps * static_cast<int64_t>(k),
+                                             run[k].rows.ptr,
+                                             sizeof(double) * 4 * static_cast<size_t>(steps),
+                                             cudaMemcpyDeviceToHost, lead));
+                MDB_CUDA(cudaMemcpyAsync(c->h_status + k, ctx->d_status, sizeof(uint32_t),
+                                         cudaMemcpyDeviceToHost, lead));
+                MDB_CUDA(cudaMemcpyAsync(ctx->h_result + kResEnergy, ctx_result(ctx, kResEnergy),
+                                         2 * sizeof(double), cudaMemcpyDeviceToHost, lead));
+            }
             MDB_CUDA(cudaStreamSynchronize(lead));
-            b->reps[0].sys->ctx->launches += (steps - 1) * c->step.lead_launches;
-            batched_done = true;
+            int st = MD_OK;
+            for (size_t k = 0; k < nr; ++k) {
+                md_system* sys = b->reps[k].sys;
+                if (c->h_status[k] != 0) {  // reported (and cleared) as ctx_check_status does
+                    const int e = ctx_check_status(sys->ctx);
+                    if (st == MD_OK) st = e;
+                    continue;
+                }
+                sys->last_energy = sys->ctx->h_result[kResEnergy];
+                sys->last_virial = sys->ctx->h_result[kResVirial];
+            }
+            return st;
         }
     }
     if (steps > 1 && !batched_done) {

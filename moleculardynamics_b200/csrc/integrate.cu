@@ -53,16 +53,16 @@ __device__ __forceinline__ double disp2(const Fold3& f3, double4 p, double4 q) {
 // velocity_verlet.hpp:55-65 (+ an optional NHC pending scale applied first).  With
 // CHECK the kernel also reduces the top-2 displacement since the last Verlet build
 // and writes the device rebuild flag (verlet_list.cpp:44-63), saving a pass.
+// `scaled`: a chain's pending velocity scale `sc` is applied first.
 template <bool CHECK>
-__device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const StepArgs& s,
-                                                const NhcState* nhc, const DispArgs& d,
-                                                unsigned block, unsigned nblocks) {
+__device__ __forceinline__ void kick_drift_scaled(md_atoms a, int64_t n, const StepArgs& s,
+                                                  bool scaled, double sc, const DispArgs& d,
+                                                  unsigned block, unsigned nblocks) {
     const int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     double a1 = 0.0;
     if (k < n) {
         double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
-        if (nhc) {
-            const double sc = nhc->scale;
+        if (scaled) {
             vx = __dmul_rn(vx, sc);
             vy = __dmul_rn(vy, sc);
             vz = __dmul_rn(vz, sc);
@@ -85,6 +85,13 @@ __device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const Ste
         if (CHECK) a1 = disp2(f3, p, d.ref[k]);
     }
     if (CHECK) top2_grid_at(a1, 0.0, d, block, nblocks);
+}
+
+template <bool CHECK>
+__device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const StepArgs& s,
+                                                const NhcState* nhc, const DispArgs& d,
+                                                unsigned block, unsigned nblocks) {
+    kick_drift_scaled<CHECK>(a, n, s, nhc != nullptr, nhc ? nhc->scale : 1.0, d, block, nblocks);
 }
 
 // At most 48 registers: five 256-thread blocks per SM keep enough loads in flight
@@ -146,8 +153,9 @@ __global__ void k_baoab_pre(md_atoms a, int64_t n, StepArgs s, DispArgs d) {
     if (CHECK) top2_grid(a1, 0.0, d);
 }
 
-// Second half-kick (velocity_verlet.hpp:70-73), fused with the kinetic-energy sum.
-__device__ __forceinline__ void kick_ke_body(md_atoms a, int64_t n, const StepArgs& s, double* part,
+// Second half-kick (velocity_verlet.hpp:70-73), fused with the kinetic-energy sum;
+// true in the block that finished the sum.
+__device__ __forceinline__ bool kick_ke_body(md_atoms a, int64_t n, const StepArgs& s, double* part,
                                              unsigned* ticket, double* out, uint32_t* status,
                                              unsigned block, unsigned nblocks) {
     double ke[1] = {0.0};
@@ -162,7 +170,7 @@ __device__ __forceinline__ void kick_ke_body(md_atoms a, int64_t n, const StepAr
         a.vz[k] = vz;
         ke[0] += 0.5 * a.mass[k] * (vx * vx + vy * vy + vz * vz);
     }
-    grid_reduce_at<1>(ke, part, ticket, out, status, block, nblocks);  // a NaN reaches the KE
+    return grid_reduce_at<1>(ke, part, ticket, out, status, block, nblocks);  // a NaN reaches the KE
 }
 
 __global__ void k_kick_ke(md_atoms a, int64_t n, StepArgs s, double* part, unsigned* ticket,
@@ -215,24 +223,30 @@ struct Weights {
 };
 
 // Start-of-step chain half: KE of the current velocities (pending scale included).
-__device__ __forceinline__ void nhc_pre_body(NhcState* st, const double* ke_now, const Weights& w) {
-    NhcState c = *st;
-    double ke = ke_now ? *ke_now * c.scale * c.scale : c.ke;
+// The start-of-step chain half on a copy of the state, from the kinetic energy ke.
+__device__ __forceinline__ NhcState nhc_pre_state(NhcState c, double ke, const Weights& w) {
     const double f = nhc_half(c, 0.5 * c.dt, w.w, ke);
     c.scale *= f;
     c.ke = ke;
-    *st = c;
+    return c;
+}
+
+__device__ __forceinline__ void nhc_pre_body(NhcState* st, const double* ke_now, const Weights& w) {
+    const NhcState c = *st;
+    *st = nhc_pre_state(c, ke_now ? *ke_now * c.scale * c.scale : c.ke, w);
 }
 
 __global__ void k_nhc_pre(NhcState* st, const double* ke_now, Weights w) { nhc_pre_body(st, ke_now, w); }
 
 // End-of-step chain half using the freshly summed KE; leaves its scale pending.
-__device__ __forceinline__ void nhc_post_body(NhcState* st, const double* ke_sum, const Weights& w) {
-    NhcState c = *st;
-    double ke = *ke_sum;
+__device__ __forceinline__ NhcState nhc_post_state(NhcState c, double ke, const Weights& w) {
     c.scale = nhc_half(c, 0.5 * c.dt, w.w, ke);
     c.ke = ke;
-    *st = c;
+    return c;
+}
+
+__device__ __forceinline__ void nhc_post_body(NhcState* st, const double* ke_sum, const Weights& w) {
+    *st = nhc_post_state(*st, *ke_sum, w);
 }
 
 __global__ void k_nhc_post(NhcState* st, const double* ke_sum, Weights w) { nhc_post_body(st, ke_sum, w); }
@@ -661,13 +675,15 @@ __device__ __forceinline__ int replica_of_block(const int* __restrict__ off, int
 }
 
 // Start-of-step chain halves, one thread per replica (k_nhc_pre without a fresh KE).
+// (The chain half is serial FP64 work, exp-bound; computing it in every kick block
+// instead, or both halves in the block that ends the kinetic-energy sum, measured
+// slower: each block then waits on that chain before its atoms.)
 __global__ void k_batch_nhc_pre(const BatchKickRep* __restrict__ reps, int nrep, Weights w) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nrep && reps[r].nhc) nhc_pre_body(reps[r].nhc, nullptr, w);
 }
 
-// Kick/drift with the rebuild test of every replica; a replica's last block also
-// sets its rebuild branch's conditional.
+// Kick/drift with the rebuild test of every replica.
 __global__ void k_batch_kick_drift(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
                                    int nrep) {
     const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
@@ -698,6 +714,27 @@ __global__ void k_batch_nhc_post(const BatchKickRep* __restrict__ reps, int nrep
         row[3] = d.nhc ? nhc_conserved(*d.nhc) : 0.0;
         ++*d.idx;
     }
+}
+
+// The end of a batched run: every chain's pending velocity scale applied (k_scale)
+// and reset (k_reset_scale), two launches for all replicas.
+__global__ void k_batch_scale(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
+                              int nrep) {
+    const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
+    const BatchKickRep& d = reps[r];
+    if (!d.nhc) return;
+    const int64_t k = (blockIdx.x - __ldg(off + r)) * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const double sc = d.nhc->scale;
+    if (k < d.n) {
+        d.a.vx[k] = __dmul_rn(d.a.vx[k], sc);
+        d.a.vy[k] = __dmul_rn(d.a.vy[k], sc);
+        d.a.vz[k] = __dmul_rn(d.a.vz[k], sc);
+    }
+}
+
+__global__ void k_batch_reset_scale(const BatchKickRep* __restrict__ reps, int nrep) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep && reps[r].nhc) reps[r].nhc->scale = 1.0;
 }
 
 }  // namespace
@@ -797,6 +834,17 @@ int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches) {
                                                                     b->nrep, yoshida());
         if (launches) ++*launches;
     }
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int batch_kick_finish(BatchKick* b, cudaStream_t stream, int64_t* launches) {
+    if (!b->any_nhc) return MD_OK;
+    k_batch_scale<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                        b->kick_off.as<int>(), b->nrep);
+    k_batch_reset_scale<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                                    b->nrep);
+    if (launches) *launches += 2;
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }

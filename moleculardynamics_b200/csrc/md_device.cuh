@@ -121,7 +121,7 @@ __device__ __forceinline__ int4 quantize_position(const double4& p, double sx, d
 // grid_reduce over an explicit block index and block count: a batched launch
 // that runs many systems gives each system's blocks their own rank and count.
 template <int K>
-__device__ void grid_reduce_at(double (&v)[K], double* part, unsigned* ticket, double* out,
+__device__ bool grid_reduce_at(double (&v)[K], double* part, unsigned* ticket, double* out,
                                uint32_t* status, unsigned block, unsigned nblocks) {
     __shared__ double sm[K][32];
     __shared__ bool is_last;
@@ -146,7 +146,7 @@ __device__ void grid_reduce_at(double (&v)[K], double* part, unsigned* ticket, d
         is_last = (t == nblocks - 1);
     }
     __syncthreads();
-    if (!is_last) return;
+    if (!is_last) return false;
     __threadfence();
     double acc[K];
 #pragma unroll
@@ -174,12 +174,13 @@ __device__ void grid_reduce_at(double (&v)[K], double* part, unsigned* ticket, d
         }
     }
     if (threadIdx.x == 0) *ticket = 0u;
+    return true;  // this was the last block: `out` holds the sums
 }
 
 template <int K>
-__device__ void grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out,
+__device__ bool grid_reduce(double (&v)[K], double* part, unsigned* ticket, double* out,
                             uint32_t* status = nullptr) {
-    grid_reduce_at<K>(v, part, ticket, out, status, blockIdx.x, gridDim.x);
+    return grid_reduce_at<K>(v, part, ticket, out, status, blockIdx.x, gridDim.x);
 }
 
 // Top-2 of a multiset (verlet_list.cpp:44-63): (a1 >= a2), merge with (b1 >= b2).

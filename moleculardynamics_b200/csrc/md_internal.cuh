@@ -203,6 +203,8 @@ struct BatchRebuild;  // neighbor.cu: the gated rebuild of every replica, stage 
 int batch_kick_create(const BatchRepView* reps, int nrep, BatchKick** out);
 int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches);
 int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches);
+// After the last step of a batched run: every chain's pending scale applied.
+int batch_kick_finish(BatchKick* b, cudaStream_t stream, int64_t* launches);
 void batch_kick_destroy(BatchKick* b);
 // MD_ERR_INVALID_ARGUMENT when the replicas' force kernels cannot share a launch
 // (different precision, truncation, threads per atom or unrolling, halo tiles).
