@@ -425,6 +425,7 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale, bool k
 }  // namespace
 
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
+int verlet_build_q(md_verlet* v, md_system* sys, int4* q, bool* quantized);
 
 // ------------------------------------------------------------ step graphs
 namespace {
@@ -510,10 +511,12 @@ int lj_fused_step(md_integrator* it, md_system* sys, md_verlet* v, md_lj* lj, do
     int4* q = nullptr;
     MDB_TRY(step_quantize_target(it, sys, lj, &q));
     MDB_TRY(pre_force(it, sys, v, first, q));
-    MDB_TRY(verlet_build(v, sys, true));
+    // a rebuild that re-sorts the atoms also re-quantizes them (q stays current)
+    bool requantized = false;
+    MDB_TRY(verlet_build_q(v, sys, q, &requantized));
     const KickArgs ka = kick_args(it, sys);
     bool kicked = false;
-    MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr, false, &ka,
+    MDB_TRY(lj_forces_verlet_async(lj, sys, v, q ? v->d_rebuild_flag : nullptr, requantized, &ka,
                                    &kicked));
     MDB_TRY(post_force_async(it, sys, false, kicked));
     if (rows) {
@@ -562,8 +565,9 @@ int capture_lj_step_into(md_integrator* it, md_system* sys, md_verlet* v, md_lj*
     // main path launches no gated no-op
     if (rc == MD_OK)
         rc = capture_into(ctx, body, nullptr, 0, [&]() -> int {
-            MDB_TRY(verlet_build(v, sys, true));
-            if (q) MDB_TRY(lj_quantize_async(lj, sys, v->d_rebuild_flag));
+            bool requantized = false;
+            MDB_TRY(verlet_build_q(v, sys, q, &requantized));
+            if (q && !requantized) MDB_TRY(lj_quantize_async(lj, sys, v->d_rebuild_flag));
             return MD_OK;
         }, nullptr);
     const int64_t l2 = ctx->launches;

@@ -319,10 +319,21 @@ __device__ __forceinline__ void copy_atoms_body(const md_atoms& src, const md_at
     dst.orig[s] = src.orig[s];
 }
 
+// The copy back also writes what the rebuild needs from the same positions after
+// the list build: the reference positions of the rebuild test (and the rebuild
+// count), and for a mixed force the fixed-point copy (q, or none).
 __global__ void k_copy_atoms(md_atoms src, md_atoms dst, int64_t n, const int* flag,
-                             int with_forces) {
+                             int with_forces, double4* ref, int* total, int4* q, double sx,
+                             double sy, double sz) {
     if (!gate(flag)) return;
     copy_atoms_body(src, dst, n, with_forces, blockIdx.x);
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k < n) {
+        const double4 p = src.pos[k];
+        ref[k] = p;
+        if (q) q[k] = quantize_position(p, sx, sy, sz);
+    }
+    if (k == 0 && total) ++*total;
 }
 
 // Exact candidate test with the pair ordered by original index.
@@ -1088,7 +1099,9 @@ int halo_build(md_verlet* v, md_system* sys, const int* flag) {
     return MD_OK;
 }
 
-int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
+int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag, int4* q = nullptr,
+                      bool* quantized = nullptr) {
+    if (quantized) *quantized = false;
     md_context* ctx = sys->ctx;
     const int64_t n = sys->n;
     const Box3 box = make_box(sys);
@@ -1103,9 +1116,12 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
             const int with_forces = flag ? 0 : 1;  // fused loops recompute forces next
             k_permute_gated<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
                 sys->cur, sys->alt, v->perm.as<int>(), sys->slot, n, flag, with_forces);
-            k_copy_atoms<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(sys->alt, sys->cur, n,
-                                                                         flag, with_forces);
+            k_copy_atoms<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
+                sys->alt, sys->cur, n, flag, with_forces, v->ref.as<double4>(),
+                flag ? v->d_rebuild_total : nullptr, q, 4294967296.0 / sys->box[0],
+                4294967296.0 / sys->box[1], 4294967296.0 / sys->box[2]);
             ctx->launches += 2;
+            if (quantized) *quantized = q != nullptr;
         }
         const GridArgs g = make_args(v->grid, sys);
         // warps per cell from the mean occupancy (crowded cells, e.g. a long cutoff)
@@ -1122,8 +1138,7 @@ int verlet_build_impl(md_verlet* v, md_system* sys, const int* flag) {
             sys->cur.pos, n, box, rl2, v->nbr.as<int>(), v->count.as<int>(), v->stride,
             ctx->d_status, v->d_max_count, flag);
         ++ctx->launches;
-    }
-    if (n > 0) {
+        // no re-sort: the reference positions straight from the system
         k_store_ref<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(
             sys->cur.pos, v->ref.as<double4>(), n, flag, flag ? v->d_rebuild_total : nullptr);
         ++ctx->launches;
@@ -1166,6 +1181,13 @@ int verlet_build(md_verlet* v, md_system* sys, bool conditional) {
         return MD_OK;
     }
     return verlet_build_impl(v, sys, v->d_rebuild_flag);
+}
+
+// The gated (conditional) build of a fused step for a mixed force: the rebuild also
+// writes the fixed-point copy q when it re-sorts the system (*quantized then true).
+int verlet_build_q(md_verlet* v, md_system* sys, int4* q, bool* quantized) {
+    MDB_TRY(verlet_alloc(v, sys));
+    return verlet_build_impl(v, sys, v->d_rebuild_flag, q, quantized);
 }
 
 bool verlet_halo_ready(md_verlet* v, md_system* sys) {
