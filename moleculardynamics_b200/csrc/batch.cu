@@ -282,6 +282,7 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
                 MDB_CUDA(cudaEventRecord(c->ready[k], b->reps[k].sys->ctx->stream));
                 MDB_CUDA(cudaStreamWaitEvent(lead, c->ready[k], 0));
             }
+            MDB_TRY(batch_rebuild_prime(c->step.rebuild, lead, &b->reps[0].sys->ctx->launches));
             for (int64_t s = 1; s < steps; ++s)
                 if (cudaGraphLaunch(c->step.exec, lead) != cudaSuccess)
                     return fail(MD_ERR_CUDA, "md_batch_run: graph launch failed");

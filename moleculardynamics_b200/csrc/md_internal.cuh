@@ -215,6 +215,8 @@ void batch_force_destroy(BatchForce* b);
 // (a list with halo tiles).
 int batch_rebuild_create(const BatchRepView* reps, int nrep, BatchRebuild** out);
 int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches);
+// Once per run before the first replay: every replica's cell counts cleared.
+int batch_rebuild_prime(BatchRebuild* b, cudaStream_t stream, int64_t* launches);
 void batch_rebuild_destroy(BatchRebuild* b);
 // Mixed precision: the fixed-point positions (after a rebuild re-sorted the atoms).
 int lj_quantize_async(md_lj* lj, md_system* sys, const int* gate);

@@ -893,7 +893,6 @@ struct RebuildRep {
     const int* flag;
     int64_t n;
     int m;       // cells (0 for a brute-force build)
-    int nb;      // scan blocks
     int groups;  // warps per cell in the list build
     GridArgs g;
     md_atoms cur, alt;
@@ -914,8 +913,8 @@ struct RebuildRep {
 };
 
 enum RebuildStage : int {
-    kStZero, kStBin, kStScan, kStScanTop, kStScanAdd, kStScatter, kStOrder, kStPermute, kStCopy,
-    kStCells, kStBrute, kStRef, kRebuildStages
+    kStZero, kStBin, kStScan, kStScatter, kStOrder, kStPermute, kStCopy, kStCells, kStBrute,
+    kRebuildStages
 };
 
 __device__ __forceinline__ int rebuild_rep_of(const int* __restrict__ off, int nrep, int b) {
@@ -936,15 +935,16 @@ k_batch_rebuild(const RebuildRep* __restrict__ reps, const int* __restrict__ off
     const RebuildRep& d = reps[r];
     if (!gate(d.flag)) return;
     const unsigned b = blockIdx.x - __ldg(off + r), nb = __ldg(off + r + 1) - __ldg(off + r);
-    if constexpr (STAGE == kStZero) {
-        zero_int_body(d.counts, 2 * static_cast<int64_t>(d.m), b, nb);
-        if (b == 0 && threadIdx.x == 0) *d.max_count = 0;
-    } else if constexpr (STAGE == kStBin) {
+    if constexpr (STAGE == kStBin) {
         bin_body(d.cur.pos, d.n, d.g, d.atom_rank, d.counts, b);
     } else if constexpr (STAGE == kStScatter) {
         scatter_body(d.atom_rank, d.n, d.start, d.fill, d.perm, b);
     } else if constexpr (STAGE == kStOrder) {
         cell_order_body(d.perm, d.start, d.m, d.cur.orig, b);
+        // the counts are used up: cleared here for the next rebuild, and the row
+        // maximum for this one's build
+        zero_int_body(d.counts, 2 * static_cast<int64_t>(d.m), b, nb);
+        if (b == 0 && threadIdx.x == 0) *d.max_count = 0;
     } else if constexpr (STAGE == kStPermute) {
         permute_body(d.cur, d.alt, d.perm, d.slot, d.n, 0, b);
     } else if constexpr (STAGE == kStCopy) {
@@ -959,29 +959,55 @@ k_batch_rebuild(const RebuildRep* __restrict__ reps, const int* __restrict__ off
             if (d.q) d.q[k] = quantize_position(p, d.qs[0], d.qs[1], d.qs[2]);
         }
         if (k == 0) ++*d.total;
-    } else if constexpr (STAGE == kStBrute) {
+    } else if constexpr (STAGE == kStBrute) {  // no re-sort: one warp per atom
         brute_body(d.cur.pos, d.n, d.g.box, d.rl2, d.nbr, d.count, d.stride, d.status, d.max_count, b);
-    } else if constexpr (STAGE == kStRef) {  // brute-force builds (no re-sort)
-        store_ref_body(d.cur.pos, d.ref, d.n, d.total, b);
-        const int64_t k = b * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-        if (d.q && k < d.n) d.q[k] = quantize_position(d.cur.pos[k], d.qs[0], d.qs[1], d.qs[2]);
+        const int64_t i = (b * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+        if ((threadIdx.x & 31) == 0 && i < d.n) {  // the reference and fixed-point copies
+            const double4 p = d.cur.pos[i];
+            d.ref[i] = p;
+            if (d.q) d.q[i] = quantize_position(p, d.qs[0], d.qs[1], d.qs[2]);
+        }
+        if (b == 0 && threadIdx.x == 0) ++*d.total;
     }
 }
 
-// The cell-count scan on 1024-thread blocks: block scans (the whole scan where
-// one block covers the grid), then, for larger grids, the scan of the block
-// totals and their addition.
-template <int STAGE>
+// Once per run, before the first replay: every replica's cell counts cleared (a
+// rebuild launched from the host leaves them set; the replays clear them as they
+// use them).
+__global__ void __launch_bounds__(kBlock)
+k_batch_rebuild_prime(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
+    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
+    const RebuildRep& d = reps[r];
+    const unsigned b = blockIdx.x - __ldg(off + r), nb = __ldg(off + r + 1) - __ldg(off + r);
+    zero_int_body(d.counts, 2 * static_cast<int64_t>(d.m), b, nb);
+}
+
+// The cell-count scan, one 1024-thread block per replica over its whole grid:
+// chunks of kScanBlock * kScanItems counts scanned in turn with a running carry
+// (the same exclusive sums as the solo multi-block scan).
 __global__ void __launch_bounds__(kScanBlock)
 k_batch_rebuild_scan(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
     const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
     const RebuildRep& d = reps[r];
     if (!gate(d.flag)) return;
-    const unsigned b = blockIdx.x - __ldg(off + r);
-    int* bsum = d.fill + d.m;  // the sort scratch's tail
-    if constexpr (STAGE == kStScan) scan_blocks_body(d.counts, d.start, d.m, bsum, d.nb == 1 ? 1 : 0, b);
-    else if constexpr (STAGE == kStScanTop) scan_top_body(bsum, d.nb, d.start, d.m);
-    else scan_add_body(d.start, d.m, bsum, b);
+    int carry = 0;
+    for (int base = 0; base < d.m; base += kScanBlock * kScanItems) {
+        int v[kScanItems];
+#pragma unroll
+        for (int u = 0; u < kScanItems; ++u) {
+            const int i = base + u * kScanBlock + threadIdx.x;  // coalesced
+            v[u] = i < d.m ? d.counts[i] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kScanItems; ++u) {
+            int tot;
+            const int ex = block_exclusive_scan(v[u], &tot);
+            const int i = base + u * kScanBlock + threadIdx.x;
+            if (i < d.m) d.start[i] = carry + ex;
+            carry += tot;
+        }
+    }
+    if (threadIdx.x == 0) d.start[d.m] = carry;
 }
 
 // The list build, on the build's own 128-thread blocks.
@@ -1264,7 +1290,6 @@ int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
         d.flag = lst->d_rebuild_flag;
         d.n = n;
         d.m = m;
-        d.nb = (m + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
         const double mean = cells ? static_cast<double>(n) / m : 0.0;  // as verlet_build_impl
         d.groups = static_cast<int>(std::min(16.0, std::max(1.0, std::ceil(1.5 * mean / 32.0))));
         d.g = make_args(lst->grid, sys);
@@ -1292,12 +1317,11 @@ int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
         // blocks of each stage: those of the solo gated rebuild
         const int nblk = grid_for(n, kBlock), c = cells ? 1 : 0;
         const int per[kRebuildStages] = {
-            cells ? static_cast<int>(std::min<int64_t>(grid_for(2 * static_cast<int64_t>(m), kBlock), 4096))
-                  : 1,
-            c * nblk, c * d.nb, d.nb > 1 ? 1 : 0, d.nb > 1 ? d.nb : 0, c * nblk,
-            c * grid_for(32 * static_cast<int64_t>(m), 256), c * nblk, c * nblk,
-            c * grid_for(static_cast<int64_t>(m) * d.groups, kBuildWarps),
-            cells ? 0 : grid_for(n * 32, kBlock), cells ? 0 : nblk};
+            c * static_cast<int>(std::min<int64_t>(grid_for(2 * static_cast<int64_t>(m), kBlock), 4096)),
+            c * nblk, c, c * nblk,
+            cells ? grid_for(32 * static_cast<int64_t>(m), 256) : 1,  // + clearing the row maximum
+            c * nblk, c * nblk, c * grid_for(static_cast<int64_t>(m) * d.groups, kBuildWarps),
+            cells ? 0 : grid_for(n * 32, kBlock)};
         for (int st = 0; st < kRebuildStages; ++st) {
             int* o = off.data() + static_cast<size_t>(st) * (nrep + 1);
             o[r + 1] = o[r] + per[st];
@@ -1334,16 +1358,12 @@ int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches
         kernel<<<static_cast<unsigned>(b->blocks[st]), kBlock, 0, stream>>>(reps, table(st), nr);
         ++l;
     };
-    auto scan = [&](int st, auto kernel) {
-        if (b->blocks[st] == 0) return;
-        kernel<<<static_cast<unsigned>(b->blocks[st]), kScanBlock, 0, stream>>>(reps, table(st), nr);
-        ++l;
-    };
-    stage(kStZero, k_batch_rebuild<kStZero>);
     stage(kStBin, k_batch_rebuild<kStBin>);
-    scan(kStScan, k_batch_rebuild_scan<kStScan>);
-    scan(kStScanTop, k_batch_rebuild_scan<kStScanTop>);
-    scan(kStScanAdd, k_batch_rebuild_scan<kStScanAdd>);
+    if (b->blocks[kStScan] > 0) {
+        k_batch_rebuild_scan<<<static_cast<unsigned>(b->blocks[kStScan]), kScanBlock, 0, stream>>>(
+            reps, table(kStScan), nr);
+        ++l;
+    }
     stage(kStScatter, k_batch_rebuild<kStScatter>);
     stage(kStOrder, k_batch_rebuild<kStOrder>);
     stage(kStPermute, k_batch_rebuild<kStPermute>);
@@ -1354,8 +1374,17 @@ int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches
         ++l;
     }
     stage(kStBrute, k_batch_rebuild<kStBrute>);
-    stage(kStRef, k_batch_rebuild<kStRef>);
     if (launches) *launches += l;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int batch_rebuild_prime(BatchRebuild* b, cudaStream_t stream, int64_t* launches) {
+    if (b->blocks[kStZero] == 0) return MD_OK;
+    k_batch_rebuild_prime<<<static_cast<unsigned>(b->blocks[kStZero]), kBlock, 0, stream>>>(
+        b->reps.as<RebuildRep>(), b->off.as<int>() + static_cast<size_t>(kStZero) * (b->nrep + 1),
+        b->nrep);
+    if (launches) ++*launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
