@@ -109,6 +109,10 @@ int capture_to(cudaStream_t stream, cudaGraph_t g, const cudaGraphNode_t* deps, 
 struct BatchedStep {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // the first step of a run (the chains' entry kinetic energies summed afresh)
+    cudaGraph_t first_graph = nullptr;
+    cudaGraphExec_t first_exec = nullptr;
+    int64_t first_launches = 0;
     BatchKick* kick = nullptr;
     BatchForce* force = nullptr;
     BatchRebuild* rebuild = nullptr;
@@ -117,6 +121,8 @@ struct BatchedStep {
     ~BatchedStep() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (first_exec) cudaGraphExecDestroy(first_exec);
+        if (first_graph) cudaGraphDestroy(first_graph);
         batch_kick_destroy(kick);
         batch_force_destroy(force);
         batch_rebuild_destroy(rebuild);
@@ -173,6 +179,17 @@ int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
     if (cudaGraphInstantiate(&bs.exec, bs.graph, 0) != cudaSuccess) {
         bs.exec = nullptr;
         return fail(MD_ERR_CUDA, "md_batch_run: batched graph instantiation failed");
+    }
+    if (cudaGraphCreate(&bs.first_graph, 0) != cudaSuccess) return fail(MD_ERR_CUDA, "cudaGraphCreate");
+    MDB_TRY(capture_to(lead, bs.first_graph, nullptr, 0, [&]() -> int {
+        MDB_TRY(batch_kick_first(bs.kick, lead, &bs.first_launches));
+        MDB_TRY(batch_rebuild_launch(bs.rebuild, lead, &bs.first_launches));
+        MDB_TRY(batch_force_launch(bs.force, lead, &bs.first_launches));
+        return batch_kick_post(bs.kick, lead, &bs.first_launches);
+    }, nullptr));
+    if (cudaGraphInstantiate(&bs.first_exec, bs.first_graph, 0) != cudaSuccess) {
+        bs.first_exec = nullptr;
+        return fail(MD_ERR_CUDA, "md_batch_run: batched first-step graph instantiation failed");
     }
     return MD_OK;
 }
@@ -236,22 +253,29 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
         b->runs.resize(nr);
     }
     std::vector<Run>& run = b->runs;
-    // Step 0 of every replica from the host, on the replica's own stream: it sizes
-    // every buffer (the captured graph must not allocate) and sums the chains'
-    // entry kinetic energies.  Thermo rows persist across runs, grown by doubling
-    // (a move invalidates a cached graph through the graph epoch).
+    // Thermo rows persist across runs, grown by doubling (a move invalidates a cached
+    // graph through the graph epoch).
     for (size_t k = 0; k < nr; ++k) {
-        auto& r = b->reps[k];
-        md_context* ctx = r.sys->ctx;
         if (run[k].cap < steps) {
             const int64_t cap = std::max<int64_t>(steps, 2 * run[k].cap);
             MDB_TRY(run[k].rows.ensure(sizeof(double) * 4 * static_cast<size_t>(cap)));
             run[k].cap = cap;
         }
         MDB_TRY(run[k].idx.ensure(sizeof(int)));
-        MDB_CUDA(cudaMemsetAsync(run[k].idx.ptr, 0, sizeof(int), ctx->stream));
-        MDB_TRY(lj_fused_step(r.it, r.sys, r.list, r.lj, run[k].rows.as<double>(),
-                              run[k].idx.as<int>(), true));
+    }
+    // A run whose batched graphs are cached replays its first step too (that graph
+    // sums the chains' entry kinetic energies afresh).  Otherwise step 0 of every
+    // replica runs from the host, on the replica's own stream: it sizes every buffer
+    // (the captured graphs must not allocate) and sums the chains' entry energies.
+    const bool warm = b->batched && b->cache && b->cache->step.exec && b->cache->step.first_exec &&
+                      b->cache->epoch == graph_epoch() && b->cache->nrep == nr;
+    if (!warm) {
+        for (size_t k = 0; k < nr; ++k) {
+            auto& r = b->reps[k];
+            MDB_CUDA(cudaMemsetAsync(run[k].idx.ptr, 0, sizeof(int), r.sys->ctx->stream));
+            MDB_TRY(lj_fused_step(r.it, r.sys, r.list, r.lj, run[k].rows.as<double>(),
+                                  run[k].idx.as<int>(), true));
+        }
     }
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -259,10 +283,10 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
     int rc = MD_OK;
     std::vector<int64_t> main_l(nr, 0), body_l(nr, 0);
     bool batched_done = false;
-    if (steps > 1 && b->batched) {
+    if ((steps > 1 || warm) && b->batched) {
         // the batched step graph of an earlier run while nothing it captured moved
         BatchCache* c = b->cache;
-        if (!(c && c->step.exec && c->epoch == graph_epoch() && c->nrep == nr)) {
+        if (!warm) {
             batch_cache_destroy(c);
             c = b->cache = new (std::nothrow) BatchCache();
             if (!c) return fail(MD_ERR_OUT_OF_MEMORY, "md_batch_run: host allocation");
@@ -277,16 +301,21 @@ int md_batch_run(md_batch* b, int64_t steps, double* thermo) {
             c->epoch = graph_epoch();
         }
         if (c->step.exec) {
-            // the lead stream replays the graph once every replica's first step is done
+            // the lead stream starts once every replica's stream has caught up
             for (size_t k = 0; k < nr; ++k) {
                 MDB_CUDA(cudaEventRecord(c->ready[k], b->reps[k].sys->ctx->stream));
                 MDB_CUDA(cudaStreamWaitEvent(lead, c->ready[k], 0));
             }
-            MDB_TRY(batch_rebuild_prime(c->step.rebuild, lead, &b->reps[0].sys->ctx->launches));
+            md_context* lctx = b->reps[0].sys->ctx;
+            MDB_TRY(batch_rebuild_prime(c->step.rebuild, lead, &lctx->launches));
+            if (warm) {
+                if (cudaGraphLaunch(c->step.first_exec, lead) != cudaSuccess)
+                    return fail(MD_ERR_CUDA, "md_batch_run: graph launch failed");
+                lctx->launches += c->step.first_launches;
+            }
             for (int64_t s = 1; s < steps; ++s)
                 if (cudaGraphLaunch(c->step.exec, lead) != cudaSuccess)
                     return fail(MD_ERR_CUDA, "md_batch_run: graph launch failed");
-            md_context* lctx = b->reps[0].sys->ctx;
             lctx->launches += (steps - 1) * c->step.lead_launches;
             // The end of the run on the lead stream: the chains' pending scales, then
             // every replica's thermo rows, status word and energy/virial slots read

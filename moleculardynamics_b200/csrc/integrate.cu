@@ -687,6 +687,17 @@ __global__ void k_batch_nhc_pre(const BatchKickRep* __restrict__ reps, int nrep,
     if (r < nrep && reps[r].nhc) nhc_pre_body(reps[r].nhc, nullptr, w);
 }
 
+// The first step of a run: every row index back to 0, and a chain's start-of-step
+// half from the kinetic energy summed just before (k_nhc_pre with a fresh KE, as
+// the first step of md_run_lj runs it).
+__global__ void k_batch_first_pre(const BatchKickRep* __restrict__ reps, int nrep, Weights w) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrep) return;
+    const BatchKickRep& d = reps[r];
+    if (d.idx) *d.idx = 0;
+    if (d.nhc) nhc_pre_body(d.nhc, d.ke_out, w);
+}
+
 // Kick/drift with the rebuild test of every replica.
 __global__ void k_batch_kick_drift(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
                                    int nrep) {
@@ -745,14 +756,17 @@ __global__ void k_batch_reset_scale(const BatchKickRep* __restrict__ reps, int n
 
 struct BatchKick {
     DevBuf reps, kick_off, ke_off;
-    int nrep = 0, kick_total = 0, ke_total = 0;
+    DevBuf kin_reps, kin_off;  // the chains' entry kinetic energies (first step of a run)
+    int nrep = 0, kick_total = 0, ke_total = 0, kin_total = 0;
     bool any_nhc = false, any_rows = false;
 };
 
 int batch_kick_create(const BatchRepView* v, int nrep, BatchKick** out) {
     if (nrep < 1) return fail(MD_ERR_INVALID_ARGUMENT, "batch_kick_create: no replicas");
     std::vector<BatchKickRep> h(static_cast<size_t>(nrep));
-    std::vector<int> ko(static_cast<size_t>(nrep) + 1, 0), eo(static_cast<size_t>(nrep) + 1, 0);
+    std::vector<BatchKineticRep> kh(static_cast<size_t>(nrep));
+    std::vector<int> ko(static_cast<size_t>(nrep) + 1, 0), eo(static_cast<size_t>(nrep) + 1, 0),
+        kn(static_cast<size_t>(nrep) + 1, 0);
     bool any_nhc = false, any_rows = false;
     for (int r = 0; r < nrep; ++r) {
         md_integrator* it = v[r].it;
@@ -789,17 +803,30 @@ int batch_kick_create(const BatchRepView* v, int nrep, BatchKick** out) {
         any_rows = any_rows || d.rows;
         ko[static_cast<size_t>(r) + 1] = ko[static_cast<size_t>(r)] + blocks;
         eo[static_cast<size_t>(r) + 1] = eo[static_cast<size_t>(r)] + g;
+        // system_kinetic_async's launch for a chain (reduce_grid blocks: kick_grid's count)
+        kh[static_cast<size_t>(r)] = BatchKineticRep{sys->cur, sys->n, part, ctx_counter(ctx, 0),
+                                                     ctx_result(ctx, kResKE)};
+        kn[static_cast<size_t>(r) + 1] = kn[static_cast<size_t>(r)] + (d.nhc ? g : 0);
     }
     BatchKick* b = new (std::nothrow) BatchKick();
     if (!b) return fail(MD_ERR_OUT_OF_MEMORY, "batch_kick_create: host allocation");
     b->nrep = nrep;
     b->kick_total = ko.back();
     b->ke_total = eo.back();
+    b->kin_total = kn.back();
     b->any_nhc = any_nhc;
     b->any_rows = any_rows;
     int rc = b->reps.ensure(sizeof(BatchKickRep) * h.size());
     if (rc == MD_OK) rc = b->kick_off.ensure(sizeof(int) * ko.size());
     if (rc == MD_OK) rc = b->ke_off.ensure(sizeof(int) * eo.size());
+    if (rc == MD_OK) rc = b->kin_reps.ensure(sizeof(BatchKineticRep) * kh.size());
+    if (rc == MD_OK) rc = b->kin_off.ensure(sizeof(int) * kn.size());
+    if (rc == MD_OK &&
+        (cudaMemcpy(b->kin_reps.ptr, kh.data(), sizeof(BatchKineticRep) * kh.size(),
+                    cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(b->kin_off.ptr, kn.data(), sizeof(int) * kn.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess))
+        rc = fail(MD_ERR_CUDA, "batch_kick_create: upload");
     if (rc == MD_OK &&
         (cudaMemcpy(b->reps.ptr, h.data(), sizeof(BatchKickRep) * h.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess ||
@@ -825,6 +852,18 @@ int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches) {
     k_batch_kick_drift<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
                                                              b->kick_off.as<int>(), b->nrep);
     if (launches) ++*launches;
+    MDB_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+int batch_kick_first(BatchKick* b, cudaStream_t stream, int64_t* launches) {
+    MDB_TRY(batch_kinetic_launch(b->kin_reps.as<BatchKineticRep>(), b->kin_off.as<int>(), b->nrep,
+                                 b->kin_total, stream));
+    k_batch_first_pre<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                                 b->nrep, yoshida());
+    k_batch_kick_drift<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                             b->kick_off.as<int>(), b->nrep);
+    if (launches) *launches += (b->kin_total > 0 ? 1 : 0) + 2;
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
@@ -858,6 +897,8 @@ void batch_kick_destroy(BatchKick* b) {
     b->reps.release();
     b->kick_off.release();
     b->ke_off.release();
+    b->kin_reps.release();
+    b->kin_off.release();
     delete b;
 }
 

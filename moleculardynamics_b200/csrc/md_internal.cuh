@@ -197,11 +197,25 @@ struct BatchRepView {
     double* rows;                     // thermo rows at a device-held index, or null
     int* idx;
 };
+// system.cu: the kinetic energy of many systems in one launch, each with the blocks
+// of its own system_kinetic_async (reduce_grid), into `out`.
+struct BatchKineticRep {
+    md_atoms a;
+    int64_t n;
+    double* part;
+    unsigned* ticket;
+    double* out;
+};
+int batch_kinetic_launch(const BatchKineticRep* reps, const int* off, int nrep, int blocks,
+                         cudaStream_t stream);
 struct BatchKick;     // integrate.cu: chain halves, kick/drift (+ rebuild test), kick + KE
 struct BatchForce;    // lj.cu: the Verlet-list force pass
 struct BatchRebuild;  // neighbor.cu: the gated rebuild of every replica, stage by stage
 int batch_kick_create(const BatchRepView* reps, int nrep, BatchKick** out);
 int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches);
+// The first step of a run instead of batch_kick_pre: row indices reset, the chains'
+// entry kinetic energies summed afresh, then the same kick/drift.
+int batch_kick_first(BatchKick* b, cudaStream_t stream, int64_t* launches);
 int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches);
 // After the last step of a batched run: every chain's pending scale applied.
 int batch_kick_finish(BatchKick* b, cudaStream_t stream, int64_t* launches);

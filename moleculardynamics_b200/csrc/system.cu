@@ -102,14 +102,36 @@ __global__ void k_zero_forces(md_atoms a, int64_t n) {
 }
 
 // system.cpp:124-131: sum 0.5*m*v^2, v^2 = vx*vx + vy*vy + vz*vz.
-__global__ void k_kinetic(md_atoms a, int64_t n, double* part, unsigned* ticket, double* out) {
+__device__ __forceinline__ void kinetic_body(const md_atoms& a, int64_t n, double* part,
+                                             unsigned* ticket, double* out, unsigned block,
+                                             unsigned nblocks) {
     double v[1] = {0.0};
-    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    for (int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(nblocks) * blockDim.x) {
         const double v2 = a.vx[k] * a.vx[k] + a.vy[k] * a.vy[k] + a.vz[k] * a.vz[k];
         v[0] += 0.5 * a.mass[k] * v2;
     }
-    grid_reduce<1>(v, part, ticket, out);
+    grid_reduce_at<1>(v, part, ticket, out, nullptr, block, nblocks);
+}
+
+__global__ void k_kinetic(md_atoms a, int64_t n, double* part, unsigned* ticket, double* out) {
+    kinetic_body(a, n, part, ticket, out, blockIdx.x, gridDim.x);
+}
+
+// The kinetic energy of many systems in one launch: each block sums for the system
+// its block-offset table assigns it, with that system's solo blocks (reduce_grid).
+__global__ void k_batch_kinetic(const BatchKineticRep* __restrict__ reps, const int* __restrict__ off,
+                                int nrep) {
+    int lo = 0, hi = nrep;
+    const int b = static_cast<int>(blockIdx.x);
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    const BatchKineticRep& d = reps[lo];
+    kinetic_body(d.a, d.n, d.part, d.ticket, d.out, b - __ldg(off + lo),
+                 __ldg(off + lo + 1) - __ldg(off + lo));
 }
 
 // system.cpp:137-145 plus the total mass (system.cpp:148-151).
@@ -191,6 +213,14 @@ int system_permute(md_system* sys, const int* d_perm) {
     sys->alt = t;
     ++sys->epoch;
     graph_epoch_bump();  // the current arrays moved
+    return MD_OK;
+}
+
+int batch_kinetic_launch(const BatchKineticRep* reps, const int* off, int nrep, int blocks,
+                         cudaStream_t stream) {
+    if (blocks <= 0) return MD_OK;
+    k_batch_kinetic<<<static_cast<unsigned>(blocks), kBlock, 0, stream>>>(reps, off, nrep);
+    MDB_CHECK_LAUNCH();
     return MD_OK;
 }
 
