@@ -788,7 +788,6 @@ int batch_kick_create(const BatchRepView* v, int nrep, BatchKick** out) {
         double* part;
         MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
         d.d = disp_args(v[r].list, ctx, part);
-        d.d.set_cond = 0;  // the batched rebuild reads the flag itself
         d.nhc = nhc_of(it);
         const int g = kick_grid(sys);
         MDB_TRY(ctx_partials(ctx, static_cast<size_t>(g), &part));

@@ -215,9 +215,6 @@ struct DispArgs {
     unsigned* ticket;
     int* flag;
     double* top2;
-    // inside a step graph: the rebuild branch's conditional, set with the flag
-    cudaGraphConditionalHandle cond = 0;
-    int set_cond = 0;
 };
 
 __device__ inline void top2_grid_at(double a1, double a2, const DispArgs& d, unsigned block,
@@ -270,7 +267,6 @@ __device__ inline void top2_grid_at(double a1, double a2, const DispArgs& d, uns
         d.top2[1] = r2;
         const int rebuild = (d.criterion == 0 ? (r1 + r2) > d.skin : r1 > 0.5 * d.skin) ? 1 : 0;
         *d.flag = rebuild;
-        if (d.set_cond) cudaGraphSetConditional(d.cond, rebuild ? 1u : 0u);
         *d.ticket = 0u;
     }
 }
