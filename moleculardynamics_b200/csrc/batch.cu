@@ -162,8 +162,10 @@ int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
         views[k] = BatchRepView{r.it, r.sys, r.list, r.lj, run[k].rows.as<double>(),
                                 run[k].idx.as<int>()};
     }
+    std::vector<KickArgs> kicks(nr);
+    for (size_t k = 0; k < nr; ++k) kicks[k] = integrator_kick_args(b->reps[k].it, b->reps[k].sys);
     if (batch_rebuild_create(views.data(), static_cast<int>(nr), &bs.rebuild) != MD_OK ||
-        batch_force_create(views.data(), static_cast<int>(nr), &bs.force) != MD_OK ||
+        batch_force_create(views.data(), static_cast<int>(nr), kicks.data(), &bs.force) != MD_OK ||
         batch_kick_create(views.data(), static_cast<int>(nr), &bs.kick) != MD_OK) {
         cudaGetLastError();
         return MD_OK;  // not batchable: the caller uses the per-replica graph
@@ -174,7 +176,7 @@ int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
         MDB_TRY(batch_kick_pre(bs.kick, lead, &bs.lead_launches));
         MDB_TRY(batch_rebuild_launch(bs.rebuild, lead, &bs.lead_launches));
         MDB_TRY(batch_force_launch(bs.force, lead, &bs.lead_launches));
-        return batch_kick_post(bs.kick, lead, &bs.lead_launches);
+        return batch_kick_post(bs.kick, lead, &bs.lead_launches, batch_force_kicks(bs.force));
     }, nullptr));
     if (cudaGraphInstantiate(&bs.exec, bs.graph, 0) != cudaSuccess) {
         bs.exec = nullptr;
@@ -185,7 +187,7 @@ int build_batched_step(md_batch* b, std::vector<Run>& run, BatchedStep& bs) {
         MDB_TRY(batch_kick_first(bs.kick, lead, &bs.first_launches));
         MDB_TRY(batch_rebuild_launch(bs.rebuild, lead, &bs.first_launches));
         MDB_TRY(batch_force_launch(bs.force, lead, &bs.first_launches));
-        return batch_kick_post(bs.kick, lead, &bs.first_launches);
+        return batch_kick_post(bs.kick, lead, &bs.first_launches, batch_force_kicks(bs.force));
     }, nullptr));
     if (cudaGraphInstantiate(&bs.first_exec, bs.first_graph, 0) != cudaSuccess) {
         bs.first_exec = nullptr;

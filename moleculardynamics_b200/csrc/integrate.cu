@@ -190,63 +190,93 @@ __global__ void k_scale(md_atoms a, int64_t n, NhcState* nhc) {
 
 __global__ void k_reset_scale(NhcState* nhc) { nhc->scale = 1.0; }
 
-// nose_hoover.cpp:89-108 for link j; ke is the current kinetic energy.
-__device__ void nhc_link(NhcState& c, int j, double d2, double d4, double ke) {
-    const bool next = j < c.chain - 1;
-    if (next) c.pxi[j] *= exp(-d4 * c.pxi[j + 1] / c.Q[j + 1]);
-    double g;
-    if (j == 0) g = 2.0 * ke - c.dof * c.temperature;
-    else g = c.pxi[j - 1] * c.pxi[j - 1] / c.Q[j - 1] - c.temperature;
-    c.pxi[j] += d2 * g;
-    if (next) c.pxi[j] *= exp(-d4 * c.pxi[j + 1] / c.Q[j + 1]);
-}
-
-// integrateChain(delta) (nose_hoover.cpp:59-124) with weights w[3]; returns the
-// product of the velocity scale factors and updates ke to KE * scale^2.
-__device__ double nhc_half(NhcState& c, double delta, const double* w, double& ke) {
-    double total = 1.0;
-    for (int s = 0; s < 3; ++s) {
-        const double d = w[s] * delta;
-        const double d2 = 0.5 * d, d4 = 0.25 * d;
-        for (int j = c.chain - 1; j >= 0; --j) nhc_link(c, j, d2, d4, ke);
-        for (int k = 0; k < c.chain; ++k) c.xi[k] += d * c.pxi[k] / c.Q[k];
-        const double f = exp(-d * c.pxi[0] / c.Q[0]);
-        total *= f;
-        ke = ke * f * f;
-        for (int j = 0; j < c.chain; ++j) nhc_link(c, j, d2, d4, ke);
-    }
-    return total;
-}
-
 struct Weights {
     double w[3];
 };
 
-// Start-of-step chain half: KE of the current velocities (pending scale included).
-// The start-of-step chain half on a copy of the state, from the kinetic energy ke.
-__device__ __forceinline__ NhcState nhc_pre_state(NhcState c, double ke, const Weights& w) {
-    const double f = nhc_half(c, 0.5 * c.dt, w.w, ke);
-    c.scale *= f;
-    c.ke = ke;
-    return c;
+// nose_hoover.cpp:89-108 for link j of a chain in arrays of C slots (m links in use);
+// ke is the current kinetic energy.  Explicit round-to-nearest products and sums (no
+// contraction into FMAs; the division is IEEE), in the reference's order of
+// operations.  Both damping factors of a link use p[j + 1] before the link changes
+// p[j], so one exponential serves both.
+template <int C>
+__device__ __forceinline__ void chain_link(const double (&Q)[C], double (&p)[C], int j, int m,
+                                           double d2, double d4, double ke, double dof,
+                                           double temp) {
+    const int up = j + 1 < C ? j + 1 : j;  // read only when j + 1 < m <= C
+    const int dn = j > 0 ? j - 1 : 0;
+    const bool next = j < m - 1;
+    const double damp = next ? exp(__dmul_rn(-d4, p[up]) / Q[up]) : 1.0;
+    if (next) p[j] = __dmul_rn(p[j], damp);
+    const double g = j == 0 ? __dsub_rn(__dmul_rn(2.0, ke), __dmul_rn(dof, temp))
+                            : __dsub_rn(__dmul_rn(p[dn], p[dn]) / Q[dn], temp);
+    p[j] = __dadd_rn(p[j], __dmul_rn(d2, g));
+    if (next) p[j] = __dmul_rn(p[j], damp);
 }
 
+// integrateChain(delta) (nose_hoover.cpp:59-124) with weights w on the chain of *st.
+// With C > 0 the chain has exactly C links, held in registers: every loop unrolls,
+// so no array is indexed at run time.  C = 0 takes any length up to kMaxChain, in
+// arrays indexed at run time (local memory).  Returns the product of the velocity
+// scale factors and updates ke to KE * scale^2.
+template <int C>
+__device__ double chain_half(NhcState* st, double delta, Weights w, double& ke) {
+    constexpr int kSlots = C > 0 ? C : kMaxChain;
+    constexpr int kUnroll = C > 0 ? C : 1;  // link loops: whole for C > 0, rolled for C = 0
+    const int m = C > 0 ? C : st->chain;
+    const double dof = st->dof, temp = st->temperature;
+    double Q[kSlots], xi[kSlots], p[kSlots];
+#pragma unroll kUnroll
+    for (int k = 0; k < m; ++k) {
+        Q[k] = st->Q[k];
+        xi[k] = st->xi[k];
+        p[k] = st->pxi[k];
+    }
+    double total = 1.0;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const double d = __dmul_rn(w.w[s], delta);
+        const double d2 = 0.5 * d, d4 = 0.25 * d;
+#pragma unroll kUnroll
+        for (int j = m - 1; j >= 0; --j) chain_link(Q, p, j, m, d2, d4, ke, dof, temp);
+#pragma unroll kUnroll
+        for (int k = 0; k < m; ++k) xi[k] = __dadd_rn(xi[k], __dmul_rn(d, p[k]) / Q[k]);
+        const double f = exp(__dmul_rn(-d, p[0]) / Q[0]);
+        total = __dmul_rn(total, f);
+        ke = __dmul_rn(__dmul_rn(ke, f), f);
+#pragma unroll kUnroll
+        for (int j = 0; j < m; ++j) chain_link(Q, p, j, m, d2, d4, ke, dof, temp);
+    }
+#pragma unroll kUnroll
+    for (int k = 0; k < m; ++k) {
+        st->xi[k] = xi[k];
+        st->pxi[k] = p[k];
+    }
+    return total;
+}
+
+// The usual three-link chain in registers; other lengths through C = 0.
+__device__ __forceinline__ double nhc_half(NhcState* st, double delta, const Weights& w, double& ke) {
+    return st->chain == 3 ? chain_half<3>(st, delta, w, ke) : chain_half<0>(st, delta, w, ke);
+}
+
+// Start-of-step chain half, from the kinetic energy of the current velocities (ke_now,
+// pending scale included) or, with ke_now null, the one the last chain half left.
 __device__ __forceinline__ void nhc_pre_body(NhcState* st, const double* ke_now, const Weights& w) {
-    const NhcState c = *st;
-    *st = nhc_pre_state(c, ke_now ? *ke_now * c.scale * c.scale : c.ke, w);
+    const double scale = st->scale;
+    double ke = ke_now ? *ke_now * scale * scale : st->ke;
+    const double f = nhc_half(st, 0.5 * st->dt, w, ke);
+    st->scale = scale * f;
+    st->ke = ke;
 }
 
 __global__ void k_nhc_pre(NhcState* st, const double* ke_now, Weights w) { nhc_pre_body(st, ke_now, w); }
 
 // End-of-step chain half using the freshly summed KE; leaves its scale pending.
-__device__ __forceinline__ NhcState nhc_post_state(NhcState c, double ke, const Weights& w) {
-    c.scale = nhc_half(c, 0.5 * c.dt, w.w, ke);
-    c.ke = ke;
-    return c;
-}
-
 __device__ __forceinline__ void nhc_post_body(NhcState* st, const double* ke_sum, const Weights& w) {
-    *st = nhc_post_state(*st, *ke_sum, w);
+    double ke = *ke_sum;
+    st->scale = nhc_half(st, 0.5 * st->dt, w, ke);
+    st->ke = ke;
 }
 
 __global__ void k_nhc_post(NhcState* st, const double* ke_sum, Weights w) { nhc_post_body(st, ke_sum, w); }
@@ -423,6 +453,8 @@ int post_force_async(md_integrator* it, md_system* sys, bool apply_scale, bool k
 }
 
 }  // namespace
+
+KickArgs integrator_kick_args(const md_integrator* it, md_system* sys) { return kick_args(it, sys); }
 
 int verlet_build(md_verlet* v, md_system* sys, bool conditional);
 int verlet_build_q(md_verlet* v, md_system* sys, int4* q, bool* quantized);
@@ -867,10 +899,12 @@ int batch_kick_first(BatchKick* b, cudaStream_t stream, int64_t* launches) {
     return MD_OK;
 }
 
-int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches) {
-    k_batch_kick_ke<<<b->ke_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
-                                                        b->ke_off.as<int>(), b->nrep);
-    if (launches) ++*launches;
+int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches, bool kicked) {
+    if (!kicked) {
+        k_batch_kick_ke<<<b->ke_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
+                                                            b->ke_off.as<int>(), b->nrep);
+        if (launches) ++*launches;
+    }
     if (b->any_nhc || b->any_rows) {
         k_batch_nhc_post<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
                                                                     b->nrep, yoshida());

@@ -259,14 +259,17 @@ struct PosOf<true> {
 };
 
 // The Verlet-list force pass of one system, for block `block` of `nblocks`
-// (a batched launch gives each system's blocks their own rank and count).
-template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
+// (a batched launch gives each system's blocks their own rank and count).  With
+// KICK the pass also applies the closing half-kick to each atom once its force is
+// summed, and reduces the kinetic energy with the energy and virial (result slots
+// 0, 1, 2), so no separate kick pass re-reads the forces and velocities.
+template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC, bool KICK = false>
 __device__ __forceinline__ void lj_verlet_body(
     const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
     const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
     const Box3& box, const LJArgs& a, double* __restrict__ fxo, double* __restrict__ fyo,
     double* __restrict__ fzo, double* part, unsigned* ticket, double* out, unsigned block,
-    unsigned nblocks) {
+    unsigned nblocks, const KickArgs& kick) {
     using P = PosOf<MIXED>;
     const int64_t t = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t i = t / TPA;
@@ -334,24 +337,45 @@ __device__ __forceinline__ void lj_verlet_body(
         fy += __shfl_xor_sync(0xffffffffu, fy, o);
         fz += __shfl_xor_sync(0xffffffffu, fz, o);
     }
+    double ke = 0.0;
     if (i < n && g == 0) {
         fxo[i] = fx;
         fyo[i] = fy;
         fzo[i] = fz;
+        if constexpr (KICK) {  // the closing half-kick, as the separate kick kernel does it
+            const double c = __dmul_rn(kick.half_dt, kick.inv_mass[i]);
+            const double vx = fma(c, fx, kick.vx[i]);
+            const double vy = fma(c, fy, kick.vy[i]);
+            const double vz = fma(c, fz, kick.vz[i]);
+            kick.vx[i] = vx;
+            kick.vy[i] = vy;
+            kick.vz[i] = vz;
+            ke = 0.5 * kick.mass[i] * (vx * vx + vy * vy + vz * vz);
+        }
     }
-    double v[2] = {e, vir};
-    grid_reduce_at<2>(v, part, ticket, out, nullptr, block, nblocks);
+    if constexpr (KICK) {
+        double v[3] = {e, vir, ke};
+        grid_reduce_at<3>(v, part, ticket, out, kick.status, block, nblocks);
+    } else {
+        double v[2] = {e, vir};
+        grid_reduce_at<2>(v, part, ticket, out, nullptr, block, nblocks);
+    }
 }
 
-template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
+template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC, bool KICK>
 __global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
 k_lj_verlet(const typename PosOf<MIXED>::T* __restrict__ pos, const double4* __restrict__ pd,
             const int* __restrict__ nbr, const int* __restrict__ count, int stride, int64_t n,
             Box3 box, LJArgs a, double* __restrict__ fxo, double* __restrict__ fyo,
-            double* __restrict__ fzo, double* part, unsigned* ticket, double* out) {
-    lj_verlet_body<TPA, MIXED, LFS, U, CUBIC>(pos, pd, nbr, count, stride, n, box, a, fxo, fyo, fzo,
-                                              part, ticket, out, blockIdx.x, gridDim.x);
+            double* __restrict__ fzo, double* part, unsigned* ticket, double* out, KickArgs kick) {
+    lj_verlet_body<TPA, MIXED, LFS, U, CUBIC, KICK>(pos, pd, nbr, count, stride, n, box, a, fxo,
+                                                    fyo, fzo, part, ticket, out, blockIdx.x,
+                                                    gridDim.x, kick);
 }
+
+// The gathered kernel shape that also takes the closing half-kick (the default
+// shape; other shapes leave the kick to the integrator's own pass).
+constexpr bool verlet_kicks(int tpa, int unroll) { return tpa == 2 && unroll == 2; }
 
 // One system's arguments of the batched force pass.
 struct BatchForceRep {
@@ -367,6 +391,7 @@ struct BatchForceRep {
     double* part;
     unsigned* ticket;
     double* out;
+    KickArgs kick;  // used by the kernel that takes the closing half-kick
 };
 
 // The system whose blocks [off[r], off[r + 1]) hold block b.
@@ -383,7 +408,7 @@ __device__ __forceinline__ int system_of_block(const int* __restrict__ off, int 
 // The force pass of many systems in one launch: each block finds its system in
 // the block-offset table and runs exactly the blocks a launch of that system
 // alone would, so every system's forces and sums equal its solo pass.
-template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC>
+template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC, bool KICK>
 __global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
 k_lj_verlet_batch(const BatchForceRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
     // the system's arguments are read from shared memory as the solo kernel reads
@@ -393,9 +418,9 @@ k_lj_verlet_batch(const BatchForceRep* __restrict__ reps, const int* __restrict_
     if (threadIdx.x == 0) d = reps[r];
     __syncthreads();
     const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
-    lj_verlet_body<TPA, MIXED, LFS, U, CUBIC>(
+    lj_verlet_body<TPA, MIXED, LFS, U, CUBIC, KICK>(
         static_cast<const typename PosOf<MIXED>::T*>(d.pos), d.pd, d.nbr, d.count, d.stride, d.n,
-        d.box, d.a, d.fx, d.fy, d.fz, d.part, d.ticket, d.out, blockIdx.x - b0, b1 - b0);
+        d.box, d.a, d.fx, d.fy, d.fz, d.part, d.ticket, d.out, blockIdx.x - b0, b1 - b0, d.kick);
 }
 
 // One thread's share of a row (entries g, g + TPA, ...): U position loads in
@@ -1209,18 +1234,27 @@ Box3 box_of(const md_system* sys) {
 }
 
 template <int TPA, bool MIXED, bool LFS, int U>
-void launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
-                   double* out) {
+bool launch_verlet(md_system* sys, md_verlet* v, const LJArgs& a, double* part, unsigned* ticket,
+                   double* out, const KickArgs* kick) {
     const int64_t threads = sys->n * TPA;
     const typename PosOf<MIXED>::T* pos;
     if constexpr (MIXED) pos = sys->qpos.as<int4>();
     else pos = sys->cur.pos;
     const bool cubic = MIXED && a.res[0] == a.res[1] && a.res[0] == a.res[2];
-    auto kernel = cubic ? k_lj_verlet<TPA, MIXED, LFS, U, MIXED>
-                        : k_lj_verlet<TPA, MIXED, LFS, U, false>;
+    auto kernel = cubic ? k_lj_verlet<TPA, MIXED, LFS, U, MIXED, false>
+                        : k_lj_verlet<TPA, MIXED, LFS, U, false, false>;
+    bool kicks = false;
+    if constexpr (verlet_kicks(TPA, U)) {
+        if (kick) {
+            kernel = cubic ? k_lj_verlet<TPA, MIXED, LFS, U, MIXED, true>
+                           : k_lj_verlet<TPA, MIXED, LFS, U, false, true>;
+            kicks = true;
+        }
+    }
     kernel<<<grid_for(threads, kBlock), kBlock, 0, sys->ctx->stream>>>(
         pos, sys->cur.pos, v->nbr.as<int>(), v->count.as<int>(), v->stride, sys->n, box_of(sys), a,
-        sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out);
+        sys->cur.fx, sys->cur.fy, sys->cur.fz, part, ticket, out, kicks ? *kick : KickArgs{});
+    return kicks;
 }
 
 // Fixed-point positions for the mixed pair kernels (quantize_position), skipped
@@ -1319,23 +1353,23 @@ void launch_halo_u(int unroll, md_system* sys, md_verlet* v, const LJArgs& a, do
 }
 
 template <int TPA, bool MIXED, bool LFS>
-void launch_verlet_u(int unroll, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
-                     unsigned* ticket, double* out) {
+bool launch_verlet_u(int unroll, md_system* sys, md_verlet* v, const LJArgs& a, double* part,
+                     unsigned* ticket, double* out, const KickArgs* kick) {
     switch (unroll) {
-        case 1: launch_verlet<TPA, MIXED, LFS, 1>(sys, v, a, part, ticket, out); break;
-        case 4: launch_verlet<TPA, MIXED, LFS, 4>(sys, v, a, part, ticket, out); break;
-        default: launch_verlet<TPA, MIXED, LFS, 2>(sys, v, a, part, ticket, out); break;
+        case 1: return launch_verlet<TPA, MIXED, LFS, 1>(sys, v, a, part, ticket, out, kick);
+        case 4: return launch_verlet<TPA, MIXED, LFS, 4>(sys, v, a, part, ticket, out, kick);
+        default: return launch_verlet<TPA, MIXED, LFS, 2>(sys, v, a, part, ticket, out, kick);
     }
 }
 
 template <bool MIXED, bool LFS>
-void launch_verlet_tpa(int tpa, int unroll, md_system* sys, md_verlet* v, const LJArgs& a,
-                       double* part, unsigned* ticket, double* out) {
+bool launch_verlet_tpa(int tpa, int unroll, md_system* sys, md_verlet* v, const LJArgs& a,
+                       double* part, unsigned* ticket, double* out, const KickArgs* kick) {
     switch (tpa) {
-        case 1: launch_verlet_u<1, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
-        case 4: launch_verlet_u<4, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
-        case 8: launch_verlet_u<8, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
-        default: launch_verlet_u<2, MIXED, LFS>(unroll, sys, v, a, part, ticket, out); break;
+        case 1: return launch_verlet_u<1, MIXED, LFS>(unroll, sys, v, a, part, ticket, out, kick);
+        case 4: return launch_verlet_u<4, MIXED, LFS>(unroll, sys, v, a, part, ticket, out, kick);
+        case 8: return launch_verlet_u<8, MIXED, LFS>(unroll, sys, v, a, part, ticket, out, kick);
+        default: return launch_verlet_u<2, MIXED, LFS>(unroll, sys, v, a, part, ticket, out, kick);
     }
 }
 
@@ -1409,12 +1443,17 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
         if (lfs) launch_halo_u<true>(unroll, sys, v, a, part, ticket, out, kick);
         else launch_halo_u<false>(unroll, sys, v, a, part, ticket, out, kick);
         if (kick && kicked) *kicked = true;
-    } else if (mixed) {
-        if (lfs) launch_verlet_tpa<true, true>(tpa, unroll, sys, v, a, part, ticket, out);
-        else launch_verlet_tpa<true, false>(tpa, unroll, sys, v, a, part, ticket, out);
     } else {
-        if (lfs) launch_verlet_tpa<false, true>(tpa, unroll, sys, v, a, part, ticket, out);
-        else launch_verlet_tpa<false, false>(tpa, unroll, sys, v, a, part, ticket, out);
+        // the default gathered shape also takes the closing half-kick when asked
+        bool k;
+        if (mixed) {
+            k = lfs ? launch_verlet_tpa<true, true>(tpa, unroll, sys, v, a, part, ticket, out, kick)
+                    : launch_verlet_tpa<true, false>(tpa, unroll, sys, v, a, part, ticket, out, kick);
+        } else {
+            k = lfs ? launch_verlet_tpa<false, true>(tpa, unroll, sys, v, a, part, ticket, out, kick)
+                    : launch_verlet_tpa<false, false>(tpa, unroll, sys, v, a, part, ticket, out, kick);
+        }
+        if (k && kicked) *kicked = true;
     }
     ctx_time_end(ctx, MD_KERNEL_LJ_FORCE);
     ++ctx->launches;
@@ -1426,9 +1465,10 @@ struct BatchForce {
     DevBuf reps, off;
     int nrep = 0, total = 0, tpa = 2;
     bool mixed = false, lfs = false, cubic = false;
+    bool kick = false;  // the kernel takes each replica's closing half-kick
 };
 
-int batch_force_create(const BatchRepView* v, int nrep, BatchForce** out) {
+int batch_force_create(const BatchRepView* v, int nrep, const KickArgs* kicks, BatchForce** out) {
     if (nrep < 1) return fail(MD_ERR_INVALID_ARGUMENT, "batch_force_create: no replicas");
     const md_lj* l0 = v[0].lj;
     const int tpa0 = l0->tpa ? l0->tpa : g_lj_tpa, unroll0 = l0->unroll ? l0->unroll : g_lj_unroll;
@@ -1452,7 +1492,7 @@ int batch_force_create(const BatchRepView* v, int nrep, BatchForce** out) {
         any_cubic = any_cubic || c;
         const int64_t blocks = grid_for(std::max<int64_t>(sys->n * tpa, 1), kBlock);
         double* part;
-        MDB_TRY(ctx_partials(ctx, 2 * static_cast<size_t>(blocks), &part));
+        MDB_TRY(ctx_partials(ctx, 3 * static_cast<size_t>(blocks), &part));
         if (mixed) MDB_TRY(sys->qpos.ensure(sizeof(int4) * static_cast<size_t>(sys->n)));
         BatchForceRep& d = h[static_cast<size_t>(r)];
         d.pos = mixed ? static_cast<const void*>(sys->qpos.as<int4>())
@@ -1470,6 +1510,7 @@ int batch_force_create(const BatchRepView* v, int nrep, BatchForce** out) {
         d.part = part;
         d.ticket = ctx_counter(ctx, 2);
         d.out = ctx_result(ctx, kResEnergy);
+        d.kick = kicks ? kicks[r] : KickArgs{};
         off[static_cast<size_t>(r) + 1] = off[static_cast<size_t>(r)] + static_cast<int>(blocks);
     }
     // the mixed kernel specialises on a cubic box: one specialisation for all
@@ -1483,6 +1524,7 @@ int batch_force_create(const BatchRepView* v, int nrep, BatchForce** out) {
     b->mixed = l0->precision == MD_PRECISION_MIXED;
     b->lfs = l0->truncation == MD_LINEAR_FORCE_SHIFT;
     b->cubic = b->mixed && cubic;
+    b->kick = kicks && verlet_kicks(tpa0, unroll0);  // as each replica's solo pass
     int rc = b->reps.ensure(sizeof(BatchForceRep) * h.size());
     if (rc == MD_OK) rc = b->off.ensure(sizeof(int) * off.size());
     if (rc == MD_OK &&
@@ -1503,8 +1545,10 @@ namespace {
 
 template <int TPA, bool MIXED, bool LFS, bool CUBIC>
 void batch_force_t(BatchForce* b, cudaStream_t s) {
-    k_lj_verlet_batch<TPA, MIXED, LFS, 2, CUBIC><<<b->total, kBlock, 0, s>>>(
-        b->reps.as<BatchForceRep>(), b->off.as<int>(), b->nrep);
+    auto kernel = k_lj_verlet_batch<TPA, MIXED, LFS, 2, CUBIC, false>;
+    if constexpr (verlet_kicks(TPA, 2))
+        if (b->kick) kernel = k_lj_verlet_batch<TPA, MIXED, LFS, 2, CUBIC, true>;
+    kernel<<<b->total, kBlock, 0, s>>>(b->reps.as<BatchForceRep>(), b->off.as<int>(), b->nrep);
 }
 
 template <int TPA>
@@ -1531,6 +1575,8 @@ int batch_force_launch(BatchForce* b, cudaStream_t s, int64_t* launches) {
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
+
+bool batch_force_kicks(const BatchForce* b) { return b && b->kick; }
 
 void batch_force_destroy(BatchForce* b) {
     if (!b) return;

@@ -99,14 +99,6 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Deterministic grid reduction of K doubles per thread.  Each block reduces its
-// values with a fixed shuffle tree and writes part[block*K + k]; the last block
-// to arrive (atomic ticket) re-reduces all partials in block order and writes
-// out[k], then resets the ticket.  Must be called by every thread of the block;
-// blockDim.x must be a multiple of 32 and <= 1024.
-// Deterministic grid-wide sums: per-block partials, then the last block to
-// arrive (ticket) sums them in block order into out[0..K).  With `status`, a
-// non-finite sum (an atom that blew up) also sets MD_STATUS_NONFINITE there.
 // Fixed-point position for the mixed pair kernels: q = round(x 2^32 / L) taken
 // modulo 2^32 (so unwrapped coordinates land on their periodic image), w = the
 // original index.
@@ -118,8 +110,14 @@ __device__ __forceinline__ int4 quantize_position(const double4& p, double sx, d
                      static_cast<int>(p.w));
 }
 
-// grid_reduce over an explicit block index and block count: a batched launch
-// that runs many systems gives each system's blocks their own rank and count.
+// Deterministic grid reduction of K doubles per thread.  Each block reduces its
+// values with a fixed shuffle tree and writes part[block*K + k]; the last block
+// to arrive (atomic ticket) re-reduces all partials in block order and writes
+// out[k], then resets the ticket.  With `status`, a non-finite sum (an atom that
+// blew up) also sets MD_STATUS_NONFINITE there.  Must be called by every thread
+// of the block; blockDim.x must be a multiple of 32 and <= 1024.  Returns true in
+// the last block.  The block index and count are explicit: a batched launch that
+// runs many systems gives each system's blocks their own rank and count.
 template <int K>
 __device__ bool grid_reduce_at(double (&v)[K], double* part, unsigned* ticket, double* out,
                                uint32_t* status, unsigned block, unsigned nblocks) {

@@ -208,6 +208,9 @@ struct BatchKineticRep {
 };
 int batch_kinetic_launch(const BatchKineticRep* reps, const int* off, int nrep, int blocks,
                          cudaStream_t stream);
+struct KickArgs;
+// The closing half-kick of integrator `it` on `sys` for a force kernel to apply.
+KickArgs integrator_kick_args(const md_integrator* it, md_system* sys);
 struct BatchKick;     // integrate.cu: chain halves, kick/drift (+ rebuild test), kick + KE
 struct BatchForce;    // lj.cu: the Verlet-list force pass
 struct BatchRebuild;  // neighbor.cu: the gated rebuild of every replica, stage by stage
@@ -216,14 +219,19 @@ int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches);
 // The first step of a run instead of batch_kick_pre: row indices reset, the chains'
 // entry kinetic energies summed afresh, then the same kick/drift.
 int batch_kick_first(BatchKick* b, cudaStream_t stream, int64_t* launches);
-int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches);
+// The step's end: the closing half-kick with the kinetic energy (unless the force
+// kernel took it: `kicked`), then the chain halves and thermo rows.
+int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches, bool kicked);
 // After the last step of a batched run: every chain's pending scale applied.
 int batch_kick_finish(BatchKick* b, cudaStream_t stream, int64_t* launches);
 void batch_kick_destroy(BatchKick* b);
 // MD_ERR_INVALID_ARGUMENT when the replicas' force kernels cannot share a launch
 // (different precision, truncation, threads per atom or unrolling, halo tiles).
-int batch_force_create(const BatchRepView* reps, int nrep, BatchForce** out);
+// With `kicks` (one per replica), a force kernel shape that can take the closing
+// half-kick does (batch_force_kicks), as each replica's solo pass would.
+int batch_force_create(const BatchRepView* reps, int nrep, const KickArgs* kicks, BatchForce** out);
 int batch_force_launch(BatchForce* b, cudaStream_t stream, int64_t* launches);
+bool batch_force_kicks(const BatchForce* b);
 void batch_force_destroy(BatchForce* b);
 // MD_ERR_INVALID_ARGUMENT when a replica's rebuild cannot join the batched stages
 // (a list with halo tiles).

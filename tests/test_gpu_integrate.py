@@ -362,9 +362,11 @@ def test_baoab_relaxes_hot_start(md):
     assert 0.9 < final_t < 1.1 and final_t < 1.5
 
 
-def test_nhc_matches_oracle_short(md):
-    """A few NHC steps track the oracle's (analytic KE*s^2 vs re-summed KE only
-    changes rounding)."""
+@pytest.mark.parametrize("chain,fused", [(3, False), (3, True), (1, True), (5, False), (5, True)])
+def test_nhc_matches_oracle_short(md, chain, fused):
+    """A few NHC steps, host-driven or one fused run, track the oracle's (analytic
+    KE*s^2 vs re-summed KE only changes rounding), for the three-link chain the
+    kernels hold in registers and for other lengths."""
     s, st = lattice_system(md, 3, 0.80, 3.0, 55)
     n = len(st["mass"])
     dof = 3 * n - 3
@@ -372,16 +374,19 @@ def test_nhc_matches_oracle_short(md):
     v = md.VerletList(st["box"], 2.5, 0.3)
     v.build(s)
     lj.compute_forces(s, v)
-    integ = md.NoseHooverChain(0.002, 1.0, 0.5, 3, dof)
+    integ = md.NoseHooverChain(0.002, 1.0, 0.5, chain, dof)
 
     def forces(sys_):
         v.rebuild_if_needed(sys_)
         return lj.compute_forces(sys_, v)[0]
 
-    for _ in range(30):
-        integ.step(s, forces)
+    if fused:
+        integ.run(s, v, lj, 30)
+    else:
+        for _ in range(30):
+            integ.step(s, forces)
     sim = O.Sim(st["pos"], st["vel"], st["mass"], st["box"], rc=2.5, trunc=1, skin=0.3, dt=0.002)
-    sim.set_nhc(1.0, 0.5, 3, dof)
+    sim.set_nhc(1.0, 0.5, chain, dof)
     sim.prime()
     sim.run("nhc", 30)
     p, vel, _ = sim.state()
