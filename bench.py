@@ -108,6 +108,13 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, ValueError):
             self.proc = None
+        # the timed region starts once nvidia-smi has written its first sample (its
+        # start-up, not the sampling, is what could delay this process's launches)
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 5.0:
+            if os.path.getsize(self.path) > 0 or self.proc.poll() is not None:
+                break
+            time.sleep(0.05)
         time.sleep(0.3)
         return self
 

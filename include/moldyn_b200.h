@@ -435,8 +435,8 @@ MD_API int md_batch_add(md_batch* batch, md_integrator* integ, md_system* sys, m
                         md_lj* lj, int* index);
 MD_API int md_batch_size(const md_batch* batch);
 /* Stage kernels shared by all replicas (default, 1): each stage of the step is
- * one launch over every replica through a block-offset table, with one
- * conditional rebuild branch per replica; 0, or replicas whose force kernels
+ * one launch over every replica through a per-block table of replicas, the
+ * rebuild stages gated per replica on the device; 0, or replicas whose force kernels
  * differ (precision, truncation, threads per atom, unrolling, halo tiles, cubic
  * and non-cubic boxes in one mixed batch), replay a graph of per-replica
  * kernels.  Each replica's trajectory is its solo run's either way. */

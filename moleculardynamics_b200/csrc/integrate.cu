@@ -53,45 +53,55 @@ __device__ __forceinline__ double disp2(const Fold3& f3, double4 p, double4 q) {
 // velocity_verlet.hpp:55-65 (+ an optional NHC pending scale applied first).  With
 // CHECK the kernel also reduces the top-2 displacement since the last Verlet build
 // and writes the device rebuild flag (verlet_list.cpp:44-63), saving a pass.
-// `scaled`: a chain's pending velocity scale `sc` is applied first.
-template <bool CHECK>
+// `scaled`: a chain's pending velocity scale `sc` is applied first.  A block moves
+// ATOMS * blockDim.x atoms, each thread every blockDim.x-th of them; the top-2
+// displacement is exact whatever the blocking.
+template <bool CHECK, int ATOMS = 1>
 __device__ __forceinline__ void kick_drift_scaled(md_atoms a, int64_t n, const StepArgs& s,
                                                   bool scaled, double sc, const DispArgs& d,
                                                   unsigned block, unsigned nblocks) {
-    const int64_t k = block * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    double a1 = 0.0;
-    if (k < n) {
-        double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
-        if (scaled) {
-            vx = __dmul_rn(vx, sc);
-            vy = __dmul_rn(vy, sc);
-            vz = __dmul_rn(vz, sc);
+    double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+    for (int u = 0; u < ATOMS; ++u) {
+        const int64_t k = (block * static_cast<int64_t>(ATOMS) + u) * blockDim.x + threadIdx.x;
+        if (k < n) {
+            double vx = a.vx[k], vy = a.vy[k], vz = a.vz[k];
+            if (scaled) {
+                vx = __dmul_rn(vx, sc);
+                vy = __dmul_rn(vy, sc);
+                vz = __dmul_rn(vz, sc);
+            }
+            const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
+            vx = fma(c, a.fx[k], vx);
+            vy = fma(c, a.fy[k], vy);
+            vz = fma(c, a.fz[k], vz);
+            const Fold3 f3 = fold3_of(s.box);
+            double4 p = a.pos[k];
+            p.x = fold_wrapped(fma(s.dt, vx, p.x), f3.b[0]);
+            p.y = fold_wrapped(fma(s.dt, vy, p.y), f3.b[1]);
+            p.z = fold_wrapped(fma(s.dt, vz, p.z), f3.b[2]);
+            check_finite(p, s.status);
+            a.pos[k] = p;
+            a.vx[k] = vx;
+            a.vy[k] = vy;
+            a.vz[k] = vz;
+            if (s.q) s.q[k] = quantize_position(p, s.qs[0], s.qs[1], s.qs[2]);
+            if (CHECK) {
+                const double x = disp2(f3, p, d.ref[k]);
+                if (u == 0) a1 = x;
+                else top2_insert(a1, a2, x);
+            }
         }
-        const double c = __dmul_rn(s.half_dt, a.inv_mass[k]);
-        vx = fma(c, a.fx[k], vx);
-        vy = fma(c, a.fy[k], vy);
-        vz = fma(c, a.fz[k], vz);
-        const Fold3 f3 = fold3_of(s.box);
-        double4 p = a.pos[k];
-        p.x = fold_wrapped(fma(s.dt, vx, p.x), f3.b[0]);
-        p.y = fold_wrapped(fma(s.dt, vy, p.y), f3.b[1]);
-        p.z = fold_wrapped(fma(s.dt, vz, p.z), f3.b[2]);
-        check_finite(p, s.status);
-        a.pos[k] = p;
-        a.vx[k] = vx;
-        a.vy[k] = vy;
-        a.vz[k] = vz;
-        if (s.q) s.q[k] = quantize_position(p, s.qs[0], s.qs[1], s.qs[2]);
-        if (CHECK) a1 = disp2(f3, p, d.ref[k]);
     }
-    if (CHECK) top2_grid_at(a1, 0.0, d, block, nblocks);
+    if (CHECK) top2_grid_at(a1, a2, d, block, nblocks);
 }
 
-template <bool CHECK>
+template <bool CHECK, int ATOMS = 1>
 __device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const StepArgs& s,
                                                 const NhcState* nhc, const DispArgs& d,
                                                 unsigned block, unsigned nblocks) {
-    kick_drift_scaled<CHECK>(a, n, s, nhc != nullptr, nhc ? nhc->scale : 1.0, d, block, nblocks);
+    kick_drift_scaled<CHECK, ATOMS>(a, n, s, nhc != nullptr, nhc ? nhc->scale : 1.0, d, block,
+                                    nblocks);
 }
 
 // At most 48 registers: five 256-thread blocks per SM keep enough loads in flight
@@ -683,6 +693,9 @@ int constrained_post_force(md_integrator* it, md_system* sys, bool apply_scale);
 // One replica's arguments of the batched kick kernels: what pre_force (no fresh
 // kinetic energy, the rebuild test fused in) and post_force_async give its solo
 // kernels, plus its thermo row.
+// Atoms per thread of the batched kick/drift and chain-scale launches.
+constexpr int kBatchKickAtoms = 2;
+
 struct BatchKickRep {
     md_atoms a;
     int64_t n;
@@ -699,16 +712,6 @@ struct BatchKickRep {
 };
 
 namespace {
-
-__device__ __forceinline__ int replica_of_block(const int* __restrict__ off, int nrep, int b) {
-    int lo = 0, hi = nrep;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= b) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
 
 // Start-of-step chain halves, one thread per replica (k_nhc_pre without a fresh KE).
 // (The chain half is serial FP64 work, exp-bound; computing it in every kick block
@@ -730,21 +733,18 @@ __global__ void k_batch_first_pre(const BatchKickRep* __restrict__ reps, int nre
     if (d.nhc) nhc_pre_body(d.nhc, d.ke_out, w);
 }
 
-// Kick/drift with the rebuild test of every replica.
-__global__ void k_batch_kick_drift(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
-                                   int nrep) {
-    const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
-    const BatchKickRep& d = reps[r];
-    const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
-    kick_drift_body<true>(d.a, d.n, d.s, d.nhc, d.d, blockIdx.x - b0, b1 - b0);
+// Kick/drift with the rebuild test of every replica, kBatchKickAtoms atoms per
+// thread: the batch's many small replicas then fill fewer, fuller blocks.
+__global__ void k_batch_kick_drift(const BatchKickRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const BatchKickRep& d = reps[e.x];
+    kick_drift_body<true, kBatchKickAtoms>(d.a, d.n, d.s, d.nhc, d.d, e.y, e.z);
 }
 
-__global__ void k_batch_kick_ke(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
-                                int nrep) {
-    const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
-    const BatchKickRep& d = reps[r];
-    const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
-    kick_ke_body(d.a, d.n, d.s, d.ke_part, d.ke_ticket, d.ke_out, d.status, blockIdx.x - b0, b1 - b0);
+__global__ void k_batch_kick_ke(const BatchKickRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const BatchKickRep& d = reps[e.x];
+    kick_ke_body(d.a, d.n, d.s, d.ke_part, d.ke_ticket, d.ke_out, d.status, e.y, e.z);
 }
 
 // End-of-step chain halves and thermo rows (k_nhc_post, k_record_at), one thread per replica.
@@ -765,17 +765,19 @@ __global__ void k_batch_nhc_post(const BatchKickRep* __restrict__ reps, int nrep
 
 // The end of a batched run: every chain's pending velocity scale applied (k_scale)
 // and reset (k_reset_scale), two launches for all replicas.
-__global__ void k_batch_scale(const BatchKickRep* __restrict__ reps, const int* __restrict__ off,
-                              int nrep) {
-    const int r = replica_of_block(off, nrep, static_cast<int>(blockIdx.x));
-    const BatchKickRep& d = reps[r];
+__global__ void k_batch_scale(const BatchKickRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const BatchKickRep& d = reps[e.x];
     if (!d.nhc) return;
-    const int64_t k = (blockIdx.x - __ldg(off + r)) * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const double sc = d.nhc->scale;
-    if (k < d.n) {
-        d.a.vx[k] = __dmul_rn(d.a.vx[k], sc);
-        d.a.vy[k] = __dmul_rn(d.a.vy[k], sc);
-        d.a.vz[k] = __dmul_rn(d.a.vz[k], sc);
+#pragma unroll
+    for (int u = 0; u < kBatchKickAtoms; ++u) {
+        const int64_t k = (e.y * static_cast<int64_t>(kBatchKickAtoms) + u) * blockDim.x + threadIdx.x;
+        if (k < d.n) {
+            d.a.vx[k] = __dmul_rn(d.a.vx[k], sc);
+            d.a.vy[k] = __dmul_rn(d.a.vy[k], sc);
+            d.a.vz[k] = __dmul_rn(d.a.vz[k], sc);
+        }
     }
 }
 
@@ -787,8 +789,8 @@ __global__ void k_batch_reset_scale(const BatchKickRep* __restrict__ reps, int n
 }  // namespace
 
 struct BatchKick {
-    DevBuf reps, kick_off, ke_off;
-    DevBuf kin_reps, kin_off;  // the chains' entry kinetic energies (first step of a run)
+    DevBuf reps, kick_blk, ke_blk;  // block tables (block_table) of the kick launches
+    DevBuf kin_reps, kin_blk;  // the chains' entry kinetic energies (first step of a run)
     int nrep = 0, kick_total = 0, ke_total = 0, kin_total = 0;
     bool any_nhc = false, any_rows = false;
 };
@@ -832,7 +834,8 @@ int batch_kick_create(const BatchRepView* v, int nrep, BatchKick** out) {
         d.idx = v[r].idx;
         any_nhc = any_nhc || d.nhc;
         any_rows = any_rows || d.rows;
-        ko[static_cast<size_t>(r) + 1] = ko[static_cast<size_t>(r)] + blocks;
+        ko[static_cast<size_t>(r) + 1] =
+            ko[static_cast<size_t>(r)] + grid_for(sys->n, kBatchKickAtoms * kBlock);
         eo[static_cast<size_t>(r) + 1] = eo[static_cast<size_t>(r)] + g;
         // system_kinetic_async's launch for a chain (reduce_grid blocks: kick_grid's count)
         kh[static_cast<size_t>(r)] = BatchKineticRep{sys->cur, sys->n, part, ctx_counter(ctx, 0),
@@ -847,23 +850,25 @@ int batch_kick_create(const BatchRepView* v, int nrep, BatchKick** out) {
     b->kin_total = kn.back();
     b->any_nhc = any_nhc;
     b->any_rows = any_rows;
+    const std::vector<int4> kt = block_table(ko.data(), nrep), et = block_table(eo.data(), nrep),
+                            nt = block_table(kn.data(), nrep);
     int rc = b->reps.ensure(sizeof(BatchKickRep) * h.size());
-    if (rc == MD_OK) rc = b->kick_off.ensure(sizeof(int) * ko.size());
-    if (rc == MD_OK) rc = b->ke_off.ensure(sizeof(int) * eo.size());
+    if (rc == MD_OK) rc = b->kick_blk.ensure(sizeof(int4) * kt.size());
+    if (rc == MD_OK) rc = b->ke_blk.ensure(sizeof(int4) * et.size());
     if (rc == MD_OK) rc = b->kin_reps.ensure(sizeof(BatchKineticRep) * kh.size());
-    if (rc == MD_OK) rc = b->kin_off.ensure(sizeof(int) * kn.size());
+    if (rc == MD_OK) rc = b->kin_blk.ensure(sizeof(int4) * std::max<size_t>(nt.size(), 1));
     if (rc == MD_OK &&
         (cudaMemcpy(b->kin_reps.ptr, kh.data(), sizeof(BatchKineticRep) * kh.size(),
                     cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(b->kin_off.ptr, kn.data(), sizeof(int) * kn.size(), cudaMemcpyHostToDevice) !=
+         cudaMemcpy(b->kin_blk.ptr, nt.data(), sizeof(int4) * nt.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess))
         rc = fail(MD_ERR_CUDA, "batch_kick_create: upload");
     if (rc == MD_OK &&
         (cudaMemcpy(b->reps.ptr, h.data(), sizeof(BatchKickRep) * h.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess ||
-         cudaMemcpy(b->kick_off.ptr, ko.data(), sizeof(int) * ko.size(), cudaMemcpyHostToDevice) !=
+         cudaMemcpy(b->kick_blk.ptr, kt.data(), sizeof(int4) * kt.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess ||
-         cudaMemcpy(b->ke_off.ptr, eo.data(), sizeof(int) * eo.size(), cudaMemcpyHostToDevice) !=
+         cudaMemcpy(b->ke_blk.ptr, et.data(), sizeof(int4) * et.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess))
         rc = fail(MD_ERR_CUDA, "batch_kick_create: descriptor upload");
     if (rc != MD_OK) {
@@ -881,19 +886,19 @@ int batch_kick_pre(BatchKick* b, cudaStream_t stream, int64_t* launches) {
         if (launches) ++*launches;
     }
     k_batch_kick_drift<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
-                                                             b->kick_off.as<int>(), b->nrep);
+                                                             b->kick_blk.as<int4>());
     if (launches) ++*launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
 
 int batch_kick_first(BatchKick* b, cudaStream_t stream, int64_t* launches) {
-    MDB_TRY(batch_kinetic_launch(b->kin_reps.as<BatchKineticRep>(), b->kin_off.as<int>(), b->nrep,
+    MDB_TRY(batch_kinetic_launch(b->kin_reps.as<BatchKineticRep>(), b->kin_blk.as<int4>(),
                                  b->kin_total, stream));
     k_batch_first_pre<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
                                                                  b->nrep, yoshida());
     k_batch_kick_drift<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
-                                                             b->kick_off.as<int>(), b->nrep);
+                                                             b->kick_blk.as<int4>());
     if (launches) *launches += (b->kin_total > 0 ? 1 : 0) + 2;
     MDB_CHECK_LAUNCH();
     return MD_OK;
@@ -902,7 +907,7 @@ int batch_kick_first(BatchKick* b, cudaStream_t stream, int64_t* launches) {
 int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches, bool kicked) {
     if (!kicked) {
         k_batch_kick_ke<<<b->ke_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
-                                                            b->ke_off.as<int>(), b->nrep);
+                                                            b->ke_blk.as<int4>());
         if (launches) ++*launches;
     }
     if (b->any_nhc || b->any_rows) {
@@ -917,7 +922,7 @@ int batch_kick_post(BatchKick* b, cudaStream_t stream, int64_t* launches, bool k
 int batch_kick_finish(BatchKick* b, cudaStream_t stream, int64_t* launches) {
     if (!b->any_nhc) return MD_OK;
     k_batch_scale<<<b->kick_total, kBlock, 0, stream>>>(b->reps.as<BatchKickRep>(),
-                                                        b->kick_off.as<int>(), b->nrep);
+                                                        b->kick_blk.as<int4>());
     k_batch_reset_scale<<<grid_for(b->nrep, 128), 128, 0, stream>>>(b->reps.as<BatchKickRep>(),
                                                                     b->nrep);
     if (launches) *launches += 2;
@@ -928,10 +933,10 @@ int batch_kick_finish(BatchKick* b, cudaStream_t stream, int64_t* launches) {
 void batch_kick_destroy(BatchKick* b) {
     if (!b) return;
     b->reps.release();
-    b->kick_off.release();
-    b->ke_off.release();
+    b->kick_blk.release();
+    b->ke_blk.release();
     b->kin_reps.release();
-    b->kin_off.release();
+    b->kin_blk.release();
     delete b;
 }
 

@@ -394,33 +394,21 @@ struct BatchForceRep {
     KickArgs kick;  // used by the kernel that takes the closing half-kick
 };
 
-// The system whose blocks [off[r], off[r + 1]) hold block b.
-__device__ __forceinline__ int system_of_block(const int* __restrict__ off, int nrep, int b) {
-    int lo = 0, hi = nrep;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= b) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // The force pass of many systems in one launch: each block finds its system in
-// the block-offset table and runs exactly the blocks a launch of that system
-// alone would, so every system's forces and sums equal its solo pass.
+// the block table and runs exactly the blocks a launch of that system alone
+// would, so every system's forces and sums equal its solo pass.
 template <int TPA, bool MIXED, bool LFS, int U, bool CUBIC, bool KICK>
 __global__ void __launch_bounds__(kBlock, UnrollBlocks<U, MIXED>::value)
-k_lj_verlet_batch(const BatchForceRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
+k_lj_verlet_batch(const BatchForceRep* __restrict__ reps, const int4* __restrict__ blk) {
     // the system's arguments are read from shared memory as the solo kernel reads
     // its parameters, rather than held in registers
     __shared__ BatchForceRep d;
-    const int r = system_of_block(off, nrep, static_cast<int>(blockIdx.x));
-    if (threadIdx.x == 0) d = reps[r];
+    const int4 e = __ldg(blk + blockIdx.x);
+    if (threadIdx.x == 0) d = reps[e.x];
     __syncthreads();
-    const int b0 = __ldg(off + r), b1 = __ldg(off + r + 1);
     lj_verlet_body<TPA, MIXED, LFS, U, CUBIC, KICK>(
         static_cast<const typename PosOf<MIXED>::T*>(d.pos), d.pd, d.nbr, d.count, d.stride, d.n,
-        d.box, d.a, d.fx, d.fy, d.fz, d.part, d.ticket, d.out, blockIdx.x - b0, b1 - b0, d.kick);
+        d.box, d.a, d.fx, d.fy, d.fz, d.part, d.ticket, d.out, e.y, e.z, d.kick);
 }
 
 // One thread's share of a row (entries g, g + TPA, ...): U position loads in
@@ -1462,7 +1450,7 @@ int lj_forces_verlet_async(md_lj* lj, md_system* sys, md_verlet* v, const int* q
 }
 
 struct BatchForce {
-    DevBuf reps, off;
+    DevBuf reps, blk;  // blk: the launch's block table (block_table)
     int nrep = 0, total = 0, tpa = 2;
     bool mixed = false, lfs = false, cubic = false;
     bool kick = false;  // the kernel takes each replica's closing half-kick
@@ -1525,12 +1513,13 @@ int batch_force_create(const BatchRepView* v, int nrep, const KickArgs* kicks, B
     b->lfs = l0->truncation == MD_LINEAR_FORCE_SHIFT;
     b->cubic = b->mixed && cubic;
     b->kick = kicks && verlet_kicks(tpa0, unroll0);  // as each replica's solo pass
+    const std::vector<int4> t = block_table(off.data(), nrep);
     int rc = b->reps.ensure(sizeof(BatchForceRep) * h.size());
-    if (rc == MD_OK) rc = b->off.ensure(sizeof(int) * off.size());
+    if (rc == MD_OK) rc = b->blk.ensure(sizeof(int4) * t.size());
     if (rc == MD_OK &&
         (cudaMemcpy(b->reps.ptr, h.data(), sizeof(BatchForceRep) * h.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess ||
-         cudaMemcpy(b->off.ptr, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice) !=
+         cudaMemcpy(b->blk.ptr, t.data(), sizeof(int4) * t.size(), cudaMemcpyHostToDevice) !=
              cudaSuccess))
         rc = fail(MD_ERR_CUDA, "batch_force_create: descriptor upload");
     if (rc != MD_OK) {
@@ -1548,7 +1537,7 @@ void batch_force_t(BatchForce* b, cudaStream_t s) {
     auto kernel = k_lj_verlet_batch<TPA, MIXED, LFS, 2, CUBIC, false>;
     if constexpr (verlet_kicks(TPA, 2))
         if (b->kick) kernel = k_lj_verlet_batch<TPA, MIXED, LFS, 2, CUBIC, true>;
-    kernel<<<b->total, kBlock, 0, s>>>(b->reps.as<BatchForceRep>(), b->off.as<int>(), b->nrep);
+    kernel<<<b->total, kBlock, 0, s>>>(b->reps.as<BatchForceRep>(), b->blk.as<int4>());
 }
 
 template <int TPA>
@@ -1581,7 +1570,7 @@ bool batch_force_kicks(const BatchForce* b) { return b && b->kick; }
 void batch_force_destroy(BatchForce* b) {
     if (!b) return;
     b->reps.release();
-    b->off.release();
+    b->blk.release();
     delete b;
 }
 

@@ -45,6 +45,17 @@ void graph_epoch_bump();
         if (rc_ != MD_OK) return rc_; \
     } while (0)
 
+// One entry per block of a batched launch, {system, rank of the block among that
+// system's blocks, their count, 0}, from the systems' block offsets off[0..nrep]:
+// a block finds its system with one load.
+inline std::vector<int4> block_table(const int* off, int nrep) {
+    std::vector<int4> t(static_cast<size_t>(off[nrep]));
+    for (int r = 0; r < nrep; ++r)
+        for (int b = off[r]; b < off[r + 1]; ++b)
+            t[static_cast<size_t>(b)] = make_int4(r, b - off[r], off[r + 1] - off[r], 0);
+    return t;
+}
+
 // ------------------------------------------------------------ device buffers
 // Grow-only device allocation (bytes), freed by the owner.
 struct DevBuf {
@@ -187,7 +198,7 @@ int rdf_frame_launch(md_rdf* r, md_system* sys, int64_t first, int64_t stride);
 void rdf_frame_note(md_rdf* r, const md_system* sys, int64_t first, int64_t stride);
 
 // Replicas stepped by batched kernels: one launch per stage of the step covers
-// every replica, each block finding its replica in a block-offset table.  The
+// every replica, each block finding its replica in a per-block table.  The
 // per-replica work inside is exactly that replica's solo step.
 struct BatchRepView {
     md_integrator* it;
@@ -206,7 +217,7 @@ struct BatchKineticRep {
     unsigned* ticket;
     double* out;
 };
-int batch_kinetic_launch(const BatchKineticRep* reps, const int* off, int nrep, int blocks,
+int batch_kinetic_launch(const BatchKineticRep* reps, const int4* blk, int blocks,
                          cudaStream_t stream);
 struct KickArgs;
 // The closing half-kick of integrator `it` on `sys` for a force kernel to apply.

@@ -887,7 +887,7 @@ int cell_sort_gated(md_system* sys, const CellGrid& grid, int* d_sorted, int* d_
 // The gated rebuild of many replicas, one launch per stage (the counting sort, the
 // re-sort of the system with the reference positions and, for a mixed force, the
 // fixed-point copy, the list build).  Each block serves the replica the stage's
-// block-offset table assigns it and leaves at once when that replica's rebuild
+// block table assigns it and leaves at once when that replica's rebuild
 // flag is clear; a replica's blocks are those of its solo gated rebuild.
 struct RebuildRep {
     const int* flag;
@@ -917,24 +917,14 @@ enum RebuildStage : int {
     kRebuildStages
 };
 
-__device__ __forceinline__ int rebuild_rep_of(const int* __restrict__ off, int nrep, int b) {
-    int lo = 0, hi = nrep;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= b) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // The stages on 256-thread blocks.
 template <int STAGE>
 __global__ void __launch_bounds__(kBlock)
-k_batch_rebuild(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
-    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
-    const RebuildRep& d = reps[r];
+k_batch_rebuild(const RebuildRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const RebuildRep& d = reps[e.x];
     if (!gate(d.flag)) return;
-    const unsigned b = blockIdx.x - __ldg(off + r), nb = __ldg(off + r + 1) - __ldg(off + r);
+    const unsigned b = e.y, nb = e.z;
     if constexpr (STAGE == kStBin) {
         bin_body(d.cur.pos, d.n, d.g, d.atom_rank, d.counts, b);
     } else if constexpr (STAGE == kStScatter) {
@@ -975,20 +965,18 @@ k_batch_rebuild(const RebuildRep* __restrict__ reps, const int* __restrict__ off
 // rebuild launched from the host leaves them set; the replays clear them as they
 // use them).
 __global__ void __launch_bounds__(kBlock)
-k_batch_rebuild_prime(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
-    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
-    const RebuildRep& d = reps[r];
-    const unsigned b = blockIdx.x - __ldg(off + r), nb = __ldg(off + r + 1) - __ldg(off + r);
-    zero_int_body(d.counts, 2 * static_cast<int64_t>(d.m), b, nb);
+k_batch_rebuild_prime(const RebuildRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const RebuildRep& d = reps[e.x];
+    zero_int_body(d.counts, 2 * static_cast<int64_t>(d.m), e.y, e.z);
 }
 
 // The cell-count scan, one 1024-thread block per replica over its whole grid:
 // chunks of kScanBlock * kScanItems counts scanned in turn with a running carry
 // (the same exclusive sums as the solo multi-block scan).
 __global__ void __launch_bounds__(kScanBlock)
-k_batch_rebuild_scan(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
-    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
-    const RebuildRep& d = reps[r];
+k_batch_rebuild_scan(const RebuildRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const RebuildRep& d = reps[__ldg(blk + blockIdx.x).x];
     if (!gate(d.flag)) return;
     int carry = 0;
     for (int base = 0; base < d.m; base += kScanBlock * kScanItems) {
@@ -1010,14 +998,17 @@ k_batch_rebuild_scan(const RebuildRep* __restrict__ reps, const int* __restrict_
     if (threadIdx.x == 0) d.start[d.m] = carry;
 }
 
-// The list build, on the build's own 128-thread blocks.
+// The list build, on the build's own 128-thread blocks.  (Blocks that each take two
+// or four of the solo build's blocks in turn, so that a step in which few replicas
+// rebuild places fewer blocks, measured slower: the rebuilding replicas' builds
+// lose more parallelism than the skipped blocks cost.)
 __global__ void __launch_bounds__(kBuildWarps * 32)
-k_batch_rebuild_cells(const RebuildRep* __restrict__ reps, const int* __restrict__ off, int nrep) {
-    const int r = rebuild_rep_of(off, nrep, static_cast<int>(blockIdx.x));
-    const RebuildRep& d = reps[r];
+k_batch_rebuild_cells(const RebuildRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const RebuildRep& d = reps[e.x];
     if (!gate(d.flag)) return;
     verlet_cells_body(d.cur.pos, d.start, d.g, d.rl2, d.nbr, d.count, d.stride, d.status,
-                      d.max_count, d.groups, blockIdx.x - __ldg(off + r));
+                      d.max_count, d.groups, e.y);
 }
 
 }  // namespace
@@ -1267,9 +1258,10 @@ int verlet_check(md_verlet* v, md_system* sys) {
 
 // ------------------------------------------------------------ batched rebuilds
 struct BatchRebuild {
-    DevBuf reps, off;  // off: kRebuildStages tables of nrep + 1 block offsets
+    DevBuf reps, blk;  // blk: the stages' block tables (block_table), one after another
     int nrep = 0;
     int blocks[kRebuildStages] = {};
+    int base[kRebuildStages] = {};  // first entry of each stage's table in blk
 };
 
 int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
@@ -1330,13 +1322,18 @@ int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
     BatchRebuild* b = new (std::nothrow) BatchRebuild();
     if (!b) return fail(MD_ERR_OUT_OF_MEMORY, "batch_rebuild_create: host allocation");
     b->nrep = nrep;
-    for (int st = 0; st < kRebuildStages; ++st)
-        b->blocks[st] = off[static_cast<size_t>(st) * (nrep + 1) + nrep];
+    std::vector<int4> t;
+    for (int st = 0; st < kRebuildStages; ++st) {
+        const std::vector<int4> ts = block_table(off.data() + static_cast<size_t>(st) * (nrep + 1), nrep);
+        b->blocks[st] = static_cast<int>(ts.size());
+        b->base[st] = static_cast<int>(t.size());
+        t.insert(t.end(), ts.begin(), ts.end());
+    }
     int rc = b->reps.ensure(sizeof(RebuildRep) * h.size());
-    if (rc == MD_OK) rc = b->off.ensure(sizeof(int) * off.size());
+    if (rc == MD_OK) rc = b->blk.ensure(sizeof(int4) * std::max<size_t>(t.size(), 1));
     if (rc == MD_OK && (cudaMemcpy(b->reps.ptr, h.data(), sizeof(RebuildRep) * h.size(),
                                    cudaMemcpyHostToDevice) != cudaSuccess ||
-                        cudaMemcpy(b->off.ptr, off.data(), sizeof(int) * off.size(),
+                        cudaMemcpy(b->blk.ptr, t.data(), sizeof(int4) * t.size(),
                                    cudaMemcpyHostToDevice) != cudaSuccess))
         rc = fail(MD_ERR_CUDA, "batch_rebuild_create: upload");
     if (rc != MD_OK) {
@@ -1349,19 +1346,17 @@ int batch_rebuild_create(const BatchRepView* v, int nrep, BatchRebuild** out) {
 
 int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches) {
     const RebuildRep* reps = b->reps.as<RebuildRep>();
-    const int* off = b->off.as<int>();
-    const int nr = b->nrep;
-    auto table = [&](int st) { return off + static_cast<size_t>(st) * (nr + 1); };
+    auto table = [&](int st) { return b->blk.as<int4>() + b->base[st]; };
     int64_t l = 0;
     auto stage = [&](int st, auto kernel) {
         if (b->blocks[st] == 0) return;
-        kernel<<<static_cast<unsigned>(b->blocks[st]), kBlock, 0, stream>>>(reps, table(st), nr);
+        kernel<<<static_cast<unsigned>(b->blocks[st]), kBlock, 0, stream>>>(reps, table(st));
         ++l;
     };
     stage(kStBin, k_batch_rebuild<kStBin>);
     if (b->blocks[kStScan] > 0) {
         k_batch_rebuild_scan<<<static_cast<unsigned>(b->blocks[kStScan]), kScanBlock, 0, stream>>>(
-            reps, table(kStScan), nr);
+            reps, table(kStScan));
         ++l;
     }
     stage(kStScatter, k_batch_rebuild<kStScatter>);
@@ -1370,7 +1365,7 @@ int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches
     stage(kStCopy, k_batch_rebuild<kStCopy>);
     if (b->blocks[kStCells] > 0) {
         k_batch_rebuild_cells<<<static_cast<unsigned>(b->blocks[kStCells]), kBuildWarps * 32, 0,
-                                stream>>>(reps, table(kStCells), nr);
+                                stream>>>(reps, table(kStCells));
         ++l;
     }
     stage(kStBrute, k_batch_rebuild<kStBrute>);
@@ -1382,8 +1377,7 @@ int batch_rebuild_launch(BatchRebuild* b, cudaStream_t stream, int64_t* launches
 int batch_rebuild_prime(BatchRebuild* b, cudaStream_t stream, int64_t* launches) {
     if (b->blocks[kStZero] == 0) return MD_OK;
     k_batch_rebuild_prime<<<static_cast<unsigned>(b->blocks[kStZero]), kBlock, 0, stream>>>(
-        b->reps.as<RebuildRep>(), b->off.as<int>() + static_cast<size_t>(kStZero) * (b->nrep + 1),
-        b->nrep);
+        b->reps.as<RebuildRep>(), b->blk.as<int4>() + b->base[kStZero]);
     if (launches) ++*launches;
     MDB_CHECK_LAUNCH();
     return MD_OK;

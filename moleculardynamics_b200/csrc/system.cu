@@ -119,19 +119,11 @@ __global__ void k_kinetic(md_atoms a, int64_t n, double* part, unsigned* ticket,
 }
 
 // The kinetic energy of many systems in one launch: each block sums for the system
-// its block-offset table assigns it, with that system's solo blocks (reduce_grid).
-__global__ void k_batch_kinetic(const BatchKineticRep* __restrict__ reps, const int* __restrict__ off,
-                                int nrep) {
-    int lo = 0, hi = nrep;
-    const int b = static_cast<int>(blockIdx.x);
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= b) lo = mid;
-        else hi = mid;
-    }
-    const BatchKineticRep& d = reps[lo];
-    kinetic_body(d.a, d.n, d.part, d.ticket, d.out, b - __ldg(off + lo),
-                 __ldg(off + lo + 1) - __ldg(off + lo));
+// its block table entry names, with that system's solo blocks (reduce_grid).
+__global__ void k_batch_kinetic(const BatchKineticRep* __restrict__ reps, const int4* __restrict__ blk) {
+    const int4 e = __ldg(blk + blockIdx.x);
+    const BatchKineticRep& d = reps[e.x];
+    kinetic_body(d.a, d.n, d.part, d.ticket, d.out, e.y, e.z);
 }
 
 // system.cpp:137-145 plus the total mass (system.cpp:148-151).
@@ -216,10 +208,10 @@ int system_permute(md_system* sys, const int* d_perm) {
     return MD_OK;
 }
 
-int batch_kinetic_launch(const BatchKineticRep* reps, const int* off, int nrep, int blocks,
+int batch_kinetic_launch(const BatchKineticRep* reps, const int4* blk, int blocks,
                          cudaStream_t stream) {
     if (blocks <= 0) return MD_OK;
-    k_batch_kinetic<<<static_cast<unsigned>(blocks), kBlock, 0, stream>>>(reps, off, nrep);
+    k_batch_kinetic<<<static_cast<unsigned>(blocks), kBlock, 0, stream>>>(reps, blk);
     MDB_CHECK_LAUNCH();
     return MD_OK;
 }
