@@ -495,15 +495,25 @@ def run_gpu_arm(args):
                 f"{args.equil} BAOAB equilibration steps on the GPU")
     # identical starting state for both precisions
     clocks = ClockSampler(local)
+    def one_arm_line(precision, ms, kms, reb):
+        # profiling configuration (one precision alone): a short line, not the contract's
+        if rank == 0:
+            print(json.dumps({"precision": precision, "steps": args.steps,
+                              "ms_per_step": ms / args.steps,
+                              "atom_steps_per_s": world * n * args.steps / (ms * 1e-3),
+                              "force_kernel_ms": kms, "rebuilds": reb}), flush=True)
+
     if args.precision == "mixed":
-        # profiling configuration: the mixed path alone
-        timed_run(md, ctx, box, pos, vel, frc, md.PRECISION_MIXED, args.steps, args.warmup, group)
+        ms, _, kms, _, _, reb = timed_run(md, ctx, box, pos, vel, frc, md.PRECISION_MIXED,
+                                          args.steps, args.warmup, group)
+        one_arm_line("mixed", ms, kms, reb)
         group.close()
         return 0
     ms64, rows64, k64, launch64, nbr, reb64 = timed_run(md, ctx, box, pos, vel, frc,
                                                         md.PRECISION_FP64, args.steps,
                                                         args.warmup, group)
     if args.precision == "fp64":
+        one_arm_line("fp64", ms64, k64, reb64)
         group.close()
         return 0
     msmx, rowsmx, kmx, launchmx, _, rebmx = timed_run(md, ctx, box, pos, vel, frc,

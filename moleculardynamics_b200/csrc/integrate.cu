@@ -105,11 +105,14 @@ __device__ __forceinline__ void kick_drift_body(md_atoms a, int64_t n, const Ste
 }
 
 // At most 48 registers: five 256-thread blocks per SM keep enough loads in flight
-// (the kernel streams ~190 bytes per atom and waits on memory, not arithmetic).
+// (the kernel streams ~190 bytes per atom and waits on memory, not arithmetic);
+// kKickAtoms atoms per thread.
+constexpr int kKickAtoms = 2;
+
 template <bool CHECK>
 __global__ void __launch_bounds__(kBlock, 5)
 k_kick_drift(md_atoms a, int64_t n, StepArgs s, const NhcState* nhc, DispArgs d) {
-    kick_drift_body<CHECK>(a, n, s, nhc, d, blockIdx.x, gridDim.x);
+    kick_drift_body<CHECK, kKickAtoms>(a, n, s, nhc, d, blockIdx.x, gridDim.x);
 }
 
 // langevin.hpp:55-80: B, A (wrap), O, A (wrap).
@@ -407,8 +410,9 @@ int pre_force(md_integrator* it, md_system* sys, md_verlet* check, bool fresh_ke
             ctx->launches += 1;
         }
         ctx_time_begin(ctx, MD_KERNEL_INTEGRATE);
-        if (check) k_kick_drift<true><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
-        else k_kick_drift<false><<<blocks, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
+        const int kd = grid_for(n, kKickAtoms * kBlock);
+        if (check) k_kick_drift<true><<<kd, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
+        else k_kick_drift<false><<<kd, kBlock, 0, ctx->stream>>>(sys->cur, n, s, nhc, d);
         ctx_time_end(ctx, MD_KERNEL_INTEGRATE);
     }
     ++ctx->launches;
