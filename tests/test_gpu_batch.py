@@ -12,7 +12,7 @@ REPLICAS = [(4, 0.9, 1.3, 11, "nhc", 0), (5, 0.1, 1.8, 12, "nhc", 0), (6, 0.8, 1
             (8, 0.5, 1.5, 14, "nhc", 1), (7, 0.3, 2.0, 15, "vv", 0)]
 
 
-def replica(md, cells, rho, temp, seed, kind, prec):
+def replica(md, cells, rho, temp, seed, kind, prec, chain=3):
     ctx = md.Context(0)
     st = md.fcc_lattice(cells, rho, temp, seed)
     s = md.System.from_arrays(st["pos"], st["box"], vel=st["vel"], mass=st["mass"], ctx=ctx)
@@ -20,7 +20,7 @@ def replica(md, cells, rho, temp, seed, kind, prec):
     v = md.VerletList(st["box"], 2.5, 0.3, ctx=ctx)
     v.build(s)
     lj.compute_forces(s, v)
-    integ = (md.NoseHooverChain(0.005, temp, 0.5, 3, 3 * s.n - 3) if kind == "nhc"
+    integ = (md.NoseHooverChain(0.005, temp, 0.5, chain, 3 * s.n - 3) if kind == "nhc"
              else md.VelocityVerlet(0.005))
     return ctx, s, v, lj, integ
 
@@ -67,7 +67,7 @@ def test_batch_rejects_shared_context_and_langevin(md):
 def test_batched_stage_kernels_equal_solo_runs(md, prec):
     """Replicas that share one force kernel (same precision, cubic boxes) step
     through the batched stage kernels -- one launch per stage for all replicas,
-    blocks mapped to replicas through a block-offset table, the rebuild stages
+    blocks mapped to replicas through a per-block table, the rebuild stages
     gated per replica (here with a brute-force build beside the cell builds).
     Each replica still follows its solo trajectory bit for bit, as with the
     per-replica graph, with a fraction of the launches."""
@@ -151,6 +151,34 @@ def test_batch_graph_kept_across_runs(md):
         alone.append((s.positions, s.velocities, th1, th2))
     batch = md.Batch()
     parts = [replica(md, *r) for r in reps]
+    for ctx, s, v, lj, integ in parts:
+        batch.add(integ, s, v, lj)
+    th1 = batch.run(30, thermo=True)
+    th2 = batch.run(50, thermo=True)
+    for k, (ctx, s, v, lj, integ) in enumerate(parts):
+        pos, vel, a1, a2 = alone[k]
+        assert np.array_equal(th1[k], a1), k
+        assert np.array_equal(th2[k], a2), k
+        assert np.array_equal(s.positions, pos), k
+        assert np.array_equal(s.velocities, vel), k
+
+
+def test_batched_chains_of_any_length_equal_solo_runs(md):
+    """Nose-Hoover replicas with chains of 1, 3 and 5 links in one batched run (the
+    three-link chain's halves run in registers, other lengths through the general
+    path), beside a velocity-Verlet replica: each follows its solo trajectory and
+    thermo rows bit for bit, over a first run and a second that replays the cached
+    graphs."""
+    reps = [((5, 0.8, 1.0, 51, "nhc", 1), 1), ((6, 0.3, 1.5, 52, "nhc", 1), 3),
+            ((7, 0.9, 1.2, 53, "nhc", 1), 5), ((5, 0.5, 1.8, 54, "vv", 1), 3)]
+    alone = []
+    for r, chain in reps:
+        ctx, s, v, lj, integ = replica(md, *r, chain=chain)
+        th1 = integ.run(s, v, lj, 30, thermo=True)
+        th2 = integ.run(s, v, lj, 50, thermo=True)
+        alone.append((s.positions, s.velocities, th1, th2))
+    batch = md.Batch()
+    parts = [replica(md, *r, chain=chain) for r, chain in reps]
     for ctx, s, v, lj, integ in parts:
         batch.add(integ, s, v, lj)
     th1 = batch.run(30, thermo=True)
